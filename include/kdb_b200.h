@@ -1,0 +1,131 @@
+/* kdb_b200.h -- C ABI of the B200 execution backend for KushDB's relational
+ * hot path (ScanSelect -> HashJoin -> GroupByAggregate -> OrderBy, plus
+ * SkinnerJoin).
+ *
+ * The reference calls its runtime per tuple from JIT-generated code through
+ * raw function pointers (DeclareExternalFunction in compile/proxy).  Per-
+ * tuple calls cannot cross to a GPU, so this boundary sits one level higher,
+ * at operator-tree / operator-batch granularity:
+ *
+ *   reference                                        here
+ *   -----------------------------------------------  --------------------------
+ *   runtime::ColumnData::{Open,Size,Get}              kdb_table_add_column,
+ *     (runtime/column_data.h:60-92),                  kdb_table_add_text_column,
+ *     FileManager::Open (runtime/file_manager.cc:22)  kdb_column_open_kdb
+ *   runtime::Enum::EnumManager::Register/GetKey       kdb_enum_register,
+ *     (runtime/enum.h:17-40)                          kdb_enum_open_kdbenum
+ *   compile::TranslateQuery + ExecutableQuery::      kdb_query_execute
+ *     Execute (compile/query_translator.h:12,
+ *     execution/executable_query.cc:199-255)
+ *   runtime::HashTable::{Create,Insert,GetBucket}    kdb_hash_build / kdb_hash_probe
+ *     (runtime/hash_table.h:22-38)
+ *   runtime::AggregateHashTable::* + aggregators     kdb_group_by_aggregate
+ *     (runtime/aggregate_hash_table.h:28-49,
+ *      compile/proxy/aggregator.cc)
+ *   runtime::Vector::Sort (runtime/vector.cc:105)    kdb_sort
+ *   runtime::ExecutePermutableSkinnerJoin            kdb_query_execute with a
+ *     (runtime/skinner_join_executor.h:16-25)         SKINNER_JOIN plan
+ *   runtime::Printer (runtime/printer.cc)            kdb_result_format
+ *
+ * Conventions: every function returns 0 on success and a negative code on
+ * error (no exceptions cross the ABI); kdb_last_error() describes the last
+ * failure on a context.  Objects are opaque handles owned by a kdb_ctx (one
+ * CUDA device, one stream).  A context is used by one host thread at a time.
+ * Plans are passed as JSON text in the plan::Operator shape (see
+ * kushdb_b200/plan.py for the serialiser).
+ */
+#ifndef KDB_B200_H_
+#define KDB_B200_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define KDB_OK 0
+#define KDB_ERR_INVALID -1      /* bad argument / plan */
+#define KDB_ERR_CUDA -2         /* CUDA runtime / driver error */
+#define KDB_ERR_COMPILE -3      /* NVRTC compilation failed */
+#define KDB_ERR_CAPACITY -4     /* a device table or buffer ran out of room */
+#define KDB_ERR_UNSUPPORTED -5  /* plan feature not supported */
+#define KDB_ERR_TIMEOUT -6      /* a bounded device wait gave up */
+
+typedef struct kdb_ctx kdb_ctx;
+typedef struct kdb_result kdb_result;
+
+/* ---- context ------------------------------------------------------------ */
+/* Creates a context on CUDA device `device`.  Replaces QueryState/
+ * FileManager ownership (execution/query_state.h:15-37). */
+int kdb_ctx_create(int device, kdb_ctx** out);
+int kdb_ctx_destroy(kdb_ctx* ctx);
+const char* kdb_last_error(kdb_ctx* ctx);
+/* Number of kernels this context launched since creation (all kinds). */
+int64_t kdb_ctx_kernel_launches(kdb_ctx* ctx);
+/* Bytes of device memory the context currently holds for columns. */
+int64_t kdb_ctx_column_bytes(kdb_ctx* ctx);
+/* The cudaStream_t all of the context's work is issued on (for callers that
+ * time or order work around it with their own CUDA events). */
+void* kdb_ctx_stream(kdb_ctx* ctx);
+/* When enabled, every kernel launch of a query is bracketed by CUDA events;
+ * kdb_last_query_kernels then reports them. */
+int kdb_ctx_set_profiling(kdb_ctx* ctx, int enabled);
+/* Per-kernel device times of the last query as JSON
+ * [{"tag":"...","ms":x},...]; returns the size needed including the NUL. */
+int64_t kdb_last_query_kernels(kdb_ctx* ctx, char* buf, int64_t cap);
+
+/* ---- columns (runtime/column_data.h:20-92) -------------------------------
+ * Type strings: "SMALLINT" "INT" "BIGINT" "REAL" "DATE" "TEXT" "BOOLEAN"
+ * "ENUM:<id>".  Fixed-width data uses the type's physical width (int8
+ * BOOLEAN, int16 SMALLINT, int32 INT/DATE/ENUM, int64 BIGINT, f64 REAL);
+ * `nulls` (optional) holds one int8 per row, 1 = NULL (the reference's
+ * `_null.kdb` BOOLEAN column).  Data is copied into HBM and stays resident
+ * until the table is dropped or the context destroyed. */
+int kdb_table_add_column(kdb_ctx* ctx, const char* table, const char* column, const char* type,
+                         const void* host_data, int64_t n, const int8_t* host_nulls);
+/* TEXT: value r is chars[offsets[r] .. offsets[r+1]) (offsets: n+1 int64). */
+int kdb_table_add_text_column(kdb_ctx* ctx, const char* table, const char* column,
+                              const int64_t* offsets, const char* chars, int64_t n,
+                              const int8_t* host_nulls);
+/* Reads a reference .kdb column file (runtime/column_data.cc:121-229 layout)
+ * and, when `null_path` is non-empty, its BOOLEAN null file. */
+int kdb_column_open_kdb(kdb_ctx* ctx, const char* table, const char* column, const char* type,
+                        const char* path, const char* null_path);
+int kdb_table_drop(kdb_ctx* ctx, const char* table);
+int64_t kdb_table_num_rows(kdb_ctx* ctx, const char* table);
+
+/* ---- enums (runtime/enum.cc) --------------------------------------------- */
+/* Key k's string is chars[offsets[k] .. offsets[k+1]). */
+int kdb_enum_register(kdb_ctx* ctx, int32_t enum_id, const int64_t* offsets, const char* chars,
+                      int32_t n);
+/* Reads a reference .kdbenum dictionary (runtime/enum.cc:38-131). */
+int kdb_enum_open_kdbenum(kdb_ctx* ctx, int32_t enum_id, const char* path);
+
+/* ---- queries -------------------------------------------------------------- */
+/* Translates the plan into device pipelines (compiled for sm_100a through
+ * NVRTC and cached by plan shape) and runs them; the result stays on the
+ * host in `out`. */
+int kdb_query_execute(kdb_ctx* ctx, const char* plan_json, kdb_result** out);
+/* Device time (ms, CUDA events) of the last kdb_query_execute's pipelines,
+ * excluding result download, and the bytes read from table columns. */
+double kdb_last_query_device_ms(kdb_ctx* ctx);
+
+/* ---- results (runtime/printer.cc output format) ------------------------ */
+int64_t kdb_result_num_rows(const kdb_result* r);
+int32_t kdb_result_num_cols(const kdb_result* r);
+int kdb_result_col_type(const kdb_result* r, int32_t col, char* buf, int32_t cap);
+int kdb_result_get_i64(const kdb_result* r, int32_t col, int64_t* out);
+int kdb_result_get_f64(const kdb_result* r, int32_t col, double* out);
+int kdb_result_get_nulls(const kdb_result* r, int32_t col, int8_t* out);
+int64_t kdb_result_get_text(const kdb_result* r, int32_t col, int64_t row, char* buf, int64_t cap);
+/* Whole result in the reference printer format ("v|v|...|\n" per row);
+ * returns the size needed including the terminating NUL. */
+int64_t kdb_result_format(kdb_ctx* ctx, const kdb_result* r, char* buf, int64_t cap);
+void kdb_result_free(kdb_result* r);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* KDB_B200_H_ */

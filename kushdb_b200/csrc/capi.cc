@@ -1,0 +1,264 @@
+// extern "C" boundary (include/kdb_b200.h): no exceptions cross it.
+#include <cstring>
+#include <fstream>
+#include <sstream>
+
+#include "../../include/kdb_b200.h"
+#include "engine.h"
+
+struct kdb_ctx {
+  std::unique_ptr<kdb::Context> c;
+  std::string err;
+};
+
+struct kdb_result {
+  kdb::HostResult r;
+};
+
+namespace {
+
+template <typename F>
+int Guard(kdb_ctx* ctx, F&& f) {
+  if (!ctx) return KDB_ERR_INVALID;
+  try {
+    f();
+    return KDB_OK;
+  } catch (const kdb::Error& e) {
+    ctx->err = e.what();
+    return e.code;
+  } catch (const std::exception& e) {
+    ctx->err = e.what();
+    return KDB_ERR_INVALID;
+  }
+}
+
+std::vector<char> ReadFile(const std::string& path) {
+  std::ifstream in(path, std::ios::binary);
+  if (!in) throw kdb::Error(KDB_ERR_INVALID, "cannot open " + path);
+  return std::vector<char>((std::istreambuf_iterator<char>(in)), std::istreambuf_iterator<char>());
+}
+
+}  // namespace
+
+extern "C" {
+
+int kdb_ctx_create(int device, kdb_ctx** out) {
+  if (!out) return KDB_ERR_INVALID;
+  *out = nullptr;
+  auto* ctx = new kdb_ctx();
+  try {
+    ctx->c = std::make_unique<kdb::Context>(device);
+  } catch (const std::exception& e) {
+    static thread_local std::string last;
+    last = e.what();
+    delete ctx;
+    return KDB_ERR_CUDA;
+  }
+  *out = ctx;
+  return KDB_OK;
+}
+
+int kdb_ctx_destroy(kdb_ctx* ctx) {
+  delete ctx;
+  return KDB_OK;
+}
+
+const char* kdb_last_error(kdb_ctx* ctx) { return ctx ? ctx->err.c_str() : "null context"; }
+
+int64_t kdb_ctx_kernel_launches(kdb_ctx* ctx) { return ctx ? ctx->c->kernel_launches : -1; }
+
+int64_t kdb_ctx_column_bytes(kdb_ctx* ctx) { return ctx ? ctx->c->ColumnBytes() : -1; }
+
+void* kdb_ctx_stream(kdb_ctx* ctx) { return ctx ? static_cast<void*>(ctx->c->stream) : nullptr; }
+
+int kdb_ctx_set_profiling(kdb_ctx* ctx, int enabled) {
+  return Guard(ctx, [&] { ctx->c->profile = enabled != 0; });
+}
+
+int64_t kdb_last_query_kernels(kdb_ctx* ctx, char* buf, int64_t cap) {
+  if (!ctx) return KDB_ERR_INVALID;
+  std::ostringstream o;
+  o << "[";
+  bool firstk = true;
+  for (const auto& [tag, ms] : ctx->c->last_kernels) {
+    o << (firstk ? "" : ",") << "{\"tag\":\"" << tag << "\",\"ms\":" << ms << "}";
+    firstk = false;
+  }
+  o << "]";
+  std::string s = o.str();
+  if (buf && cap > 0) {
+    int64_t n = std::min<int64_t>(cap - 1, s.size());
+    std::memcpy(buf, s.data(), n);
+    buf[n] = 0;
+  }
+  return static_cast<int64_t>(s.size()) + 1;
+}
+
+int kdb_table_add_column(kdb_ctx* ctx, const char* table, const char* column, const char* type,
+                         const void* host_data, int64_t n, const int8_t* host_nulls) {
+  return Guard(ctx, [&] {
+    if (!table || !column || !type || (n > 0 && !host_data))
+      throw kdb::Error(KDB_ERR_INVALID, "null argument");
+    ctx->c->AddColumn(table, column, kdb::plan::ParseType(type), host_data, n, host_nulls);
+  });
+}
+
+int kdb_table_add_text_column(kdb_ctx* ctx, const char* table, const char* column,
+                              const int64_t* offsets, const char* chars, int64_t n,
+                              const int8_t* host_nulls) {
+  return Guard(ctx, [&] {
+    if (!table || !column || !offsets) throw kdb::Error(KDB_ERR_INVALID, "null argument");
+    ctx->c->AddTextColumn(table, column, offsets, chars, n, host_nulls);
+  });
+}
+
+// runtime/column_data.cc:121-229 file layout.
+int kdb_column_open_kdb(kdb_ctx* ctx, const char* table, const char* column, const char* type,
+                        const char* path, const char* null_path) {
+  return Guard(ctx, [&] {
+    kdb::plan::Type t = kdb::plan::ParseType(type);
+    std::vector<char> raw = ReadFile(path);
+    std::vector<char> nulls;
+    if (null_path && *null_path) nulls = ReadFile(null_path);
+    const int8_t* np = nulls.empty() ? nullptr : reinterpret_cast<const int8_t*>(nulls.data());
+    if (t.id == kdb::plan::TypeId::TEXT) {
+      if (raw.size() < 8) throw kdb::Error(KDB_ERR_INVALID, "short TEXT file");
+      int32_t card;
+      std::memcpy(&card, raw.data(), 4);
+      std::vector<int64_t> off(card + 1, 0);
+      std::string chars;
+      for (int32_t r = 0; r < card; r++) {
+        int32_t len;
+        uint64_t o;
+        std::memcpy(&len, raw.data() + 8 + 16 * r, 4);
+        std::memcpy(&o, raw.data() + 8 + 16 * r + 8, 8);
+        if (o + len > raw.size()) throw kdb::Error(KDB_ERR_INVALID, "corrupt TEXT file");
+        chars.append(raw.data() + o, len);
+        off[r + 1] = static_cast<int64_t>(chars.size());
+      }
+      ctx->c->AddTextColumn(table, column, off.data(), chars.data(), card, np);
+    } else {
+      int w = kdb::plan::TypeWidth(t.id);
+      int64_t n = static_cast<int64_t>(raw.size()) / w;
+      if (np && static_cast<int64_t>(nulls.size()) != n)
+        throw kdb::Error(KDB_ERR_INVALID, "null file length differs from column length");
+      ctx->c->AddColumn(table, column, t, raw.data(), n, np);
+    }
+  });
+}
+
+int kdb_table_drop(kdb_ctx* ctx, const char* table) {
+  return Guard(ctx, [&] { ctx->c->DropTable(table); });
+}
+
+int64_t kdb_table_num_rows(kdb_ctx* ctx, const char* table) {
+  if (!ctx) return -1;
+  auto it = ctx->c->tables.find(table);
+  return it == ctx->c->tables.end() ? -1 : it->second.rows;
+}
+
+int kdb_enum_register(kdb_ctx* ctx, int32_t enum_id, const int64_t* offsets, const char* chars,
+                      int32_t n) {
+  return Guard(ctx, [&] {
+    std::vector<std::string> v;
+    for (int32_t k = 0; k < n; k++) v.emplace_back(chars + offsets[k], offsets[k + 1] - offsets[k]);
+    ctx->c->RegisterEnum(enum_id, std::move(v));
+  });
+}
+
+// runtime/enum.cc:19-131: EnumData{u64 entry_offset; u64 mask; u64 array[]}
+// then EnumEntry{u64 str_offset; u32 str_len; u32 value} indexed by key.
+int kdb_enum_open_kdbenum(kdb_ctx* ctx, int32_t enum_id, const char* path) {
+  return Guard(ctx, [&] {
+    std::vector<char> raw = ReadFile(path);
+    if (raw.size() < 16) throw kdb::Error(KDB_ERR_INVALID, "short .kdbenum file");
+    uint64_t entry_offset;
+    std::memcpy(&entry_offset, raw.data(), 8);
+    std::vector<std::string> values;
+    uint64_t first_str = UINT64_MAX;
+    for (uint64_t pos = entry_offset; pos + 16 <= raw.size() && pos < first_str; pos += 16) {
+      uint64_t so;
+      uint32_t sl, v;
+      std::memcpy(&so, raw.data() + pos, 8);
+      std::memcpy(&sl, raw.data() + pos + 8, 4);
+      std::memcpy(&v, raw.data() + pos + 12, 4);
+      if (first_str == UINT64_MAX) first_str = so;
+      if (so + sl > raw.size()) throw kdb::Error(KDB_ERR_INVALID, "corrupt .kdbenum file");
+      if (v >= values.size()) values.resize(v + 1);
+      values[v] = std::string(raw.data() + so, sl);
+    }
+    ctx->c->RegisterEnum(enum_id, std::move(values));
+  });
+}
+
+int kdb_query_execute(kdb_ctx* ctx, const char* plan_json, kdb_result** out) {
+  if (out) *out = nullptr;
+  return Guard(ctx, [&] {
+    if (!plan_json || !out) throw kdb::Error(KDB_ERR_INVALID, "null argument");
+    auto plan = kdb::plan::ParsePlan(plan_json);
+    auto res = std::make_unique<kdb_result>();
+    res->r = kdb::ExecutePlan(*ctx->c, *plan);
+    *out = res.release();
+  });
+}
+
+double kdb_last_query_device_ms(kdb_ctx* ctx) { return ctx ? ctx->c->last_device_ms : -1; }
+
+int64_t kdb_result_num_rows(const kdb_result* r) { return r ? r->r.rows : -1; }
+int32_t kdb_result_num_cols(const kdb_result* r) { return r ? static_cast<int32_t>(r->r.cols.size()) : -1; }
+
+int kdb_result_col_type(const kdb_result* r, int32_t col, char* buf, int32_t cap) {
+  if (!r || col < 0 || col >= static_cast<int32_t>(r->r.cols.size()) || !buf) return KDB_ERR_INVALID;
+  const auto& t = r->r.cols[col].type;
+  std::string s = t.id == kdb::plan::TypeId::ENUM ? "ENUM:" + std::to_string(t.enum_id)
+                                                  : kdb::plan::TypeName(t.id);
+  std::snprintf(buf, cap, "%s", s.c_str());
+  return KDB_OK;
+}
+
+int kdb_result_get_i64(const kdb_result* r, int32_t col, int64_t* out) {
+  if (!r || col < 0 || col >= static_cast<int32_t>(r->r.cols.size())) return KDB_ERR_INVALID;
+  const auto& c = r->r.cols[col];
+  if (c.i.size() != static_cast<size_t>(r->r.rows)) return KDB_ERR_INVALID;
+  std::memcpy(out, c.i.data(), sizeof(int64_t) * c.i.size());
+  return KDB_OK;
+}
+
+int kdb_result_get_f64(const kdb_result* r, int32_t col, double* out) {
+  if (!r || col < 0 || col >= static_cast<int32_t>(r->r.cols.size())) return KDB_ERR_INVALID;
+  const auto& c = r->r.cols[col];
+  if (c.f.size() != static_cast<size_t>(r->r.rows)) return KDB_ERR_INVALID;
+  std::memcpy(out, c.f.data(), sizeof(double) * c.f.size());
+  return KDB_OK;
+}
+
+int kdb_result_get_nulls(const kdb_result* r, int32_t col, int8_t* out) {
+  if (!r || col < 0 || col >= static_cast<int32_t>(r->r.cols.size())) return KDB_ERR_INVALID;
+  const auto& c = r->r.cols[col];
+  std::memcpy(out, c.null.data(), c.null.size());
+  return KDB_OK;
+}
+
+int64_t kdb_result_get_text(const kdb_result* r, int32_t col, int64_t row, char* buf, int64_t cap) {
+  if (!r || col < 0 || col >= static_cast<int32_t>(r->r.cols.size())) return KDB_ERR_INVALID;
+  const auto& c = r->r.cols[col];
+  if (row < 0 || row >= static_cast<int64_t>(c.s.size())) return KDB_ERR_INVALID;
+  const std::string& s = c.s[row];
+  if (buf && cap > 0) std::memcpy(buf, s.data(), std::min<int64_t>(cap, s.size()));
+  return static_cast<int64_t>(s.size());
+}
+
+int64_t kdb_result_format(kdb_ctx* ctx, const kdb_result* r, char* buf, int64_t cap) {
+  if (!ctx || !r) return KDB_ERR_INVALID;
+  std::string s = kdb::FormatResult(r->r, ctx->c->HostEnums());
+  if (buf && cap > 0) {
+    int64_t n = std::min<int64_t>(cap - 1, s.size());
+    std::memcpy(buf, s.data(), n);
+    buf[n] = 0;
+  }
+  return static_cast<int64_t>(s.size()) + 1;
+}
+
+void kdb_result_free(kdb_result* r) { delete r; }
+
+}  // extern "C"

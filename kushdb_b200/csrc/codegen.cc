@@ -1,0 +1,1752 @@
+// Plan executor + pipeline code generator.
+//
+// Follows the reference's produce/consume translation
+// (compile/translators/operator_translator.h:13-38): a plan is cut into
+// pipelines at the same breakers the reference uses -- hash-join build side
+// (hash_join_translator.cc:34-55), group-by / aggregate
+// (group_by_aggregate_translator.cc:36-111, aggregate_translator.cc:34-126),
+// order-by materialisation (order_by_translator.cc:35-110) and Skinner
+// children (permutable_skinner_join_translator.cc:111-204).  Each pipeline
+// becomes ONE CUDA kernel (the reference's body_N becomes a grid-stride loop
+// over the source rows): streaming operators (scan-select filters,
+// projections, hash-join probes, Skinner index lookups) are fused into the
+// loop body, and the sink (materialisation, aggregate, group table, join
+// table) is written into the same kernel.  Kernels are compiled for sm_100a by
+// NVRTC with -fmad=false so per-row float arithmetic rounds exactly like the
+// reference's mulsd/addsd (khir/asm/asm_backend.cc:1834-1864).
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <functional>
+#include <set>
+#include <sstream>
+
+#include "engine.h"
+
+namespace kdb {
+namespace {
+
+using namespace plan;
+
+// ---------------------------------------------------------------------------
+// Source building
+// ---------------------------------------------------------------------------
+
+std::string CType(TypeId t) {
+  switch (t) {
+    case TypeId::SMALLINT: return "int16_t";
+    case TypeId::INT:
+    case TypeId::DATE:
+    case TypeId::ENUM: return "int32_t";
+    case TypeId::BIGINT: return "int64_t";
+    case TypeId::REAL: return "double";
+    case TypeId::BOOLEAN: return "bool";
+    case TypeId::TEXT: return "kdb_str";
+  }
+  return "void";
+}
+
+// Storage type of a materialised column.
+std::string StoreType(TypeId t) {
+  switch (t) {
+    case TypeId::BOOLEAN: return "int8_t";
+    case TypeId::TEXT: return "kdb_str";
+    default: return CType(t);
+  }
+}
+
+size_t StoreWidth(TypeId t) {
+  switch (t) {
+    case TypeId::BOOLEAN: return 1;
+    case TypeId::SMALLINT: return 2;
+    case TypeId::INT:
+    case TypeId::DATE:
+    case TypeId::ENUM: return 4;
+    case TypeId::BIGINT:
+    case TypeId::REAL: return 8;
+    case TypeId::TEXT: return 16;
+  }
+  return 8;
+}
+
+bool IsIntLike(TypeId t) {
+  return t == TypeId::SMALLINT || t == TypeId::INT || t == TypeId::BIGINT || t == TypeId::DATE ||
+         t == TypeId::ENUM || t == TypeId::BOOLEAN;
+}
+
+std::string F64Lit(double d) {
+  if (std::isnan(d)) return "__longlong_as_double(0x7ff8000000000000LL)";
+  if (std::isinf(d)) return d > 0 ? "__longlong_as_double(0x7ff0000000000000LL)"
+                                  : "__longlong_as_double((long long)0xfff0000000000000ULL)";
+  char buf[64];
+  std::snprintf(buf, sizeof(buf), "%.17g", d);
+  std::string s = buf;
+  if (s.find_first_of(".eE") == std::string::npos) s += ".0";
+  return s;
+}
+
+std::string I64Lit(int64_t v) {
+  if (v == INT64_MIN) return "(-9223372036854775807LL - 1)";
+  return "(" + std::to_string(v) + "LL)";
+}
+
+struct CVal {
+  Type type;
+  std::string v;  // C expression / variable holding the value
+  std::string n;  // C bool expression: is NULL ("false" when never NULL)
+};
+
+struct Scope {
+  std::vector<std::vector<CVal>> child;
+  std::vector<CVal> virt;
+  const std::vector<CVal>& Child(int i) const {
+    if (i < 0 || i >= static_cast<int>(child.size()) || child[i].empty())
+      throw Error(-1, "column reference to unbound child " + std::to_string(i));
+    return child[i];
+  }
+};
+
+class KernelSource {
+ public:
+  std::ostringstream globals;
+  std::ostringstream pre;
+  std::ostringstream body;
+  std::vector<uint64_t> args;
+  int indent = 1;
+  int tmp = 0;
+  int lits = 0;
+
+  std::string Fresh(const char* p) { return std::string(p) + std::to_string(tmp++); }
+
+  void L(const std::string& s) { body << std::string(indent * 2, ' ') << s << "\n"; }
+  void Open(const std::string& s) {
+    L(s + " {");
+    indent++;
+  }
+  void Close() {
+    indent--;
+    L("}");
+  }
+
+  int Arg(uint64_t w) {
+    if (args.size() >= 384) throw Error(-5, "pipeline needs more than 384 kernel argument words");
+    args.push_back(w);
+    return static_cast<int>(args.size()) - 1;
+  }
+  std::string Word(uint64_t w) { return "a.w[" + std::to_string(Arg(w)) + "]"; }
+  // Declares a typed device pointer local in the prologue.
+  std::string Ptr(const void* p, const std::string& type, bool is_const = false) {
+    std::string name = "p" + std::to_string(tmp++);
+    pre << "  " << (is_const ? "const " : "") << type << "* __restrict__ " << name << " = ("
+        << (is_const ? "const " : "") << type << "*)a.w[" << Arg(reinterpret_cast<uint64_t>(p))
+        << "];\n";
+    return name;
+  }
+  std::string Lit(const std::string& s) {
+    std::string name = "kdb_lit" + std::to_string(lits++);
+    globals << "__device__ const char " << name << "[" << (s.size() + 1) << "] = {";
+    for (unsigned char c : s) globals << static_cast<int>(c) << ",";
+    globals << "0};\n";
+    return "kdb_mkstr(" + name + ", " + std::to_string(s.size()) + ")";
+  }
+
+  std::string Kernel(const std::string& name, int block) const {
+    std::ostringstream o;
+    o << globals.str() << "\nextern \"C\" __global__ void __launch_bounds__(" << block << ") "
+      << name << "(KArgs a) {\n"
+      << pre.str() << body.str() << "}\n";
+    return o.str();
+  }
+
+  KArgs Args() const {
+    KArgs k;
+    std::memset(&k, 0, sizeof(k));
+    for (size_t i = 0; i < args.size(); i++) k.w[i] = args[i];
+    return k;
+  }
+};
+
+// ---------------------------------------------------------------------------
+// Expression emission (mirrors compile/translators/expression_translator.cc
+// and compile/proxy/evaluate.cc; NULL rules as in the oracle)
+// ---------------------------------------------------------------------------
+
+class ExprGen {
+ public:
+  ExprGen(Context& ctx, KernelSource& ks) : ctx_(ctx), ks_(ks) {}
+
+  CVal Bind(const Type& t, const std::string& v, const std::string& n) {
+    CVal out{t, ks_.Fresh("v"), ks_.Fresh("n")};
+    ks_.L(CType(t.id) + " " + out.v + " = " + v + ";");
+    if (n == "false" || n == "true") {
+      out.n = n;
+      ks_.tmp--;
+    } else {
+      ks_.L("bool " + out.n + " = " + n + ";");
+    }
+    return out;
+  }
+
+  const DevEnum& EnumOf(const Type& t) { return ctx_.Enum(t.enum_id); }
+
+  std::string EnumRank(const Type& t, const std::string& key) {
+    auto it = rank_ptr_.find(t.enum_id);
+    if (it == rank_ptr_.end())
+      it = rank_ptr_.emplace(t.enum_id, ks_.Ptr(EnumOf(t).d_rank, "int32_t", true)).first;
+    return it->second + "[" + key + "]";
+  }
+  std::string EnumString(const Type& t, const std::string& key) {
+    auto it = str_ptr_.find(t.enum_id);
+    if (it == str_ptr_.end()) {
+      const DevEnum& e = EnumOf(t);
+      std::string off = ks_.Ptr(e.d_off, "int64_t", true);
+      std::string ch = ks_.Ptr(e.d_chars, "char", true);
+      it = str_ptr_.emplace(t.enum_id, std::make_pair(off, ch)).first;
+    }
+    return "kdb_enum_str(" + it->second.first + ", " + it->second.second + ", " + key + ")";
+  }
+
+  std::string HashOf(const CVal& c) {
+    switch (c.type.id) {
+      case TypeId::REAL: return "kdb_mix64(kdb_dbits(" + c.v + "))";
+      case TypeId::TEXT: return "kdb_hash_str(" + c.v + ")";
+      case TypeId::BOOLEAN: return "kdb_mix64((uint64_t)(" + c.v + " ? 1 : 0))";
+      default: return "kdb_mix64((uint64_t)(int64_t)" + c.v + ")";
+    }
+  }
+
+  std::string EqOf(const CVal& a, const CVal& b) {
+    switch (a.type.id) {
+      case TypeId::TEXT: return "kdb_str_eq(" + a.v + ", " + b.v + ")";
+      case TypeId::BOOLEAN: return "(" + a.v + " == " + b.v + ")";
+      default: return "(" + a.v + " == " + b.v + ")";
+    }
+  }
+
+  CVal Emit(const Expr& e, const Scope& s) {
+    switch (e.kind) {
+      case ExprKind::ColRef: return s.Child(e.child_idx).at(e.column_idx);
+      case ExprKind::VirtColRef: return s.virt.at(e.column_idx);
+      case ExprKind::Literal: {
+        std::string v;
+        switch (e.type.id) {
+          case TypeId::REAL: v = F64Lit(e.fval); break;
+          case TypeId::TEXT: v = ks_.Lit(e.sval); break;
+          case TypeId::BOOLEAN: v = e.ival ? "true" : "false"; break;
+          case TypeId::BIGINT: v = I64Lit(e.ival); break;
+          case TypeId::SMALLINT: v = "(int16_t)" + std::to_string(e.ival); break;
+          default: v = "(int32_t)(" + std::to_string(e.ival) + "LL)"; break;
+        }
+        return CVal{e.type, v, e.lit_null ? "true" : "false"};
+      }
+      case ExprKind::Unary: {
+        CVal c = Emit(e.kid(0), s);
+        if (e.uop == UnOp::IS_NULL) return Bind(e.type, c.n, "false");
+        return Bind(e.type, "!" + c.v, c.n);
+      }
+      case ExprKind::Case: {
+        CVal c = Emit(e.kid(0), s);
+        CVal t = Emit(e.kid(1), s);
+        CVal f = Emit(e.kid(2), s);
+        std::string take = "(!(" + c.n + ") && " + c.v + ")";
+        return Bind(e.type, take + " ? " + t.v + " : " + f.v, take + " ? " + t.n + " : " + f.n);
+      }
+      case ExprKind::IntToFloat: {
+        CVal c = Emit(e.kid(0), s);
+        return Bind(e.type, "(" + c.n + ") ? 0.0 : (double)" + c.v, "false");
+      }
+      case ExprKind::Extract: {
+        CVal c = Emit(e.kid(0), s);
+        return Bind(e.type, "kdb_extract_year(" + c.v + ")", c.n);
+      }
+      case ExprKind::EnumIn: {
+        CVal c = Emit(e.kid(0), s);
+        std::string cond = "false";
+        for (int32_t x : e.in_values) cond += " || " + c.v + " == " + std::to_string(x);
+        return Bind(e.type, "!(" + c.n + ") && (" + cond + ")", "false");
+      }
+      case ExprKind::Agg: throw Error(-1, "Aggregate expression can't be derived");
+      case ExprKind::Binary: break;
+    }
+    CVal l = Emit(e.kid(0), s);
+    CVal r = Emit(e.kid(1), s);
+    if (e.bop == BinOp::AND) {
+      // expression_translator.cc:74-91
+      return Bind(e.type, "(" + l.n + ") ? false : (" + l.v + " ? " + r.v + " : false)",
+                  "(" + l.n + ") ? true : (" + l.v + " ? (" + r.n + ") : false)");
+    }
+    if (e.bop == BinOp::OR) {
+      // expression_translator.cc:93-108
+      return Bind(e.type, "(" + l.n + ") ? " + r.v + " : (" + l.v + " ? true : " + r.v + ")",
+                  "(" + l.n + ") ? (" + r.n + ") : (" + l.v + " ? false : (" + r.n + "))");
+    }
+    std::string n = "(" + l.n + ") || (" + r.n + ")";
+    if (l.n == "false" && r.n == "false") n = "false";
+    const Type& lt = l.type;
+    auto cmp = [&](const std::string& a, const std::string& b) -> std::string {
+      switch (e.bop) {
+        case BinOp::EQ: return "(" + a + " == " + b + ")";
+        case BinOp::NEQ: return "(" + a + " != " + b + ")";
+        case BinOp::LT: return "(" + a + " < " + b + ")";
+        case BinOp::LEQ: return "(" + a + " <= " + b + ")";
+        case BinOp::GT: return "(" + a + " > " + b + ")";
+        case BinOp::GEQ: return "(" + a + " >= " + b + ")";
+        default: throw Error(-1, "bad comparison");
+      }
+    };
+    switch (lt.id) {
+      case TypeId::BOOLEAN: return Bind(e.type, cmp(l.v, r.v), n);
+      case TypeId::SMALLINT:
+      case TypeId::INT:
+      case TypeId::BIGINT:
+      case TypeId::DATE: {
+        if (e.bop == BinOp::ADD || e.bop == BinOp::SUB || e.bop == BinOp::MUL) {
+          // arithmetic in the column type, two's-complement wrap (evaluate.cc:84-113)
+          std::string ut = lt.id == TypeId::SMALLINT ? "uint16_t"
+                           : lt.id == TypeId::BIGINT ? "uint64_t"
+                                                     : "uint32_t";
+          const char* op = e.bop == BinOp::ADD ? " + " : e.bop == BinOp::SUB ? " - " : " * ";
+          std::string expr = "(" + CType(lt.id) + ")(" + ut + ")((" + ut + ")" + l.v + op + "(" +
+                             ut + ")" + r.v + ")";
+          if (lt.id == TypeId::SMALLINT)
+            expr = "(int16_t)(uint16_t)((uint32_t)(uint16_t)" + l.v + op + "(uint32_t)(uint16_t)" +
+                   r.v + ")";
+          return Bind(e.type, expr, n);
+        }
+        if (e.bop == BinOp::DIV) throw Error(-1, "Invalid arguments to div");
+        return Bind(e.type, cmp(l.v, r.v), n);
+      }
+      case TypeId::REAL: {
+        switch (e.bop) {
+          case BinOp::ADD: return Bind(e.type, "__dadd_rn(" + l.v + ", " + r.v + ")", n);
+          case BinOp::SUB: return Bind(e.type, "__dsub_rn(" + l.v + ", " + r.v + ")", n);
+          case BinOp::MUL: return Bind(e.type, "__dmul_rn(" + l.v + ", " + r.v + ")", n);
+          case BinOp::DIV: return Bind(e.type, "__ddiv_rn(" + l.v + ", " + r.v + ")", n);
+          default: return Bind(e.type, cmp(l.v, r.v), n);
+        }
+      }
+      case TypeId::TEXT: {
+        switch (e.bop) {
+          case BinOp::STARTS_WITH:
+            return Bind(e.type, "kdb_str_starts_with(" + l.v + ", " + r.v + ")", n);
+          case BinOp::ENDS_WITH:
+            return Bind(e.type, "kdb_str_ends_with(" + l.v + ", " + r.v + ")", n);
+          case BinOp::CONTAINS:
+            return Bind(e.type, "kdb_str_contains(" + l.v + ", " + r.v + ")", n);
+          case BinOp::EQ: return Bind(e.type, "kdb_str_eq(" + l.v + ", " + r.v + ")", n);
+          case BinOp::NEQ: return Bind(e.type, "!kdb_str_eq(" + l.v + ", " + r.v + ")", n);
+          default: return Bind(e.type, cmp("kdb_str_cmp(" + l.v + ", " + r.v + ")", "0"), n);
+        }
+      }
+      case TypeId::ENUM: {
+        // evaluate.cc:186-268: EQ/NEQ on keys, ordering and string ops on the
+        // key's string (ranks when both sides are the same enum)
+        if (e.bop == BinOp::EQ || e.bop == BinOp::NEQ) return Bind(e.type, cmp(l.v, r.v), n);
+        if (r.type.id == TypeId::ENUM && r.type.enum_id == lt.enum_id &&
+            (e.bop == BinOp::LT || e.bop == BinOp::LEQ || e.bop == BinOp::GT || e.bop == BinOp::GEQ))
+          return Bind(e.type, cmp(EnumRank(lt, l.v), EnumRank(lt, r.v)), n);
+        std::string ls = EnumString(lt, l.v);
+        std::string rs = r.type.id == TypeId::ENUM ? EnumString(r.type, r.v) : r.v;
+        switch (e.bop) {
+          case BinOp::STARTS_WITH: return Bind(e.type, "kdb_str_starts_with(" + ls + ", " + rs + ")", n);
+          case BinOp::ENDS_WITH: return Bind(e.type, "kdb_str_ends_with(" + ls + ", " + rs + ")", n);
+          case BinOp::CONTAINS: return Bind(e.type, "kdb_str_contains(" + ls + ", " + rs + ")", n);
+          default: return Bind(e.type, cmp("kdb_str_cmp(" + ls + ", " + rs + ")", "0"), n);
+        }
+      }
+    }
+    throw Error(-1, "unhandled binary expression");
+  }
+
+ private:
+  Context& ctx_;
+  KernelSource& ks_;
+  std::map<int32_t, std::string> rank_ptr_;
+  std::map<int32_t, std::pair<std::string, std::string>> str_ptr_;
+};
+
+// ---------------------------------------------------------------------------
+// Aggregate state layout (compile/proxy/aggregator.cc semantics)
+// ---------------------------------------------------------------------------
+
+enum class StateKind { SumF64, SumI64, AvgF64, Count, MinMaxKey, MinMaxText };
+
+struct AggPlan {
+  const Expr* agg;
+  StateKind kind;
+  bool is_min = false;
+  bool child_nullable = false;
+  int count_flag = -1;  // bit in the first-row flags (COUNT(col) quirk)
+};
+
+AggPlan PlanAgg(const Expr& a, int& flags) {
+  AggPlan p{&a, StateKind::Count};
+  const Type& ct = a.kid(0).type;
+  p.child_nullable = a.kid(0).nullable;
+  switch (a.agg) {
+    case AggType::SUM: p.kind = ct.id == TypeId::REAL ? StateKind::SumF64 : StateKind::SumI64; break;
+    case AggType::AVG: p.kind = StateKind::AvgF64; break;
+    case AggType::COUNT:
+      p.kind = StateKind::Count;
+      // COUNT initialises to 1 on the group's first row even when that row's
+      // value is NULL (aggregator.cc:285-287)
+      if (p.child_nullable) {
+        if (flags >= 8) throw Error(-5, "more than 8 nullable COUNT(col) aggregates");
+        p.count_flag = flags++;
+      }
+      break;
+    case AggType::MIN:
+    case AggType::MAX:
+      p.is_min = a.agg == AggType::MIN;
+      if (ct.id == TypeId::BOOLEAN) throw Error(-1, "cannot compute min of non-numeric col");
+      p.kind = ct.id == TypeId::TEXT ? StateKind::MinMaxText : StateKind::MinMaxKey;
+      break;
+  }
+  return p;
+}
+
+// Order-preserving 64-bit key of a MIN/MAX input value.
+std::string OKey(ExprGen& eg, const CVal& c) {
+  switch (c.type.id) {
+    case TypeId::REAL: return "kdb_dord(" + c.v + ")";
+    case TypeId::ENUM:
+      return "(((uint64_t)(uint32_t)" + eg.EnumRank(c.type, c.v) + " << 32) | (uint64_t)(uint32_t)" +
+             c.v + ")";
+    default: return "((uint64_t)(int64_t)" + c.v + " ^ 0x8000000000000000ULL)";
+  }
+}
+
+// Value from an order-preserving key.
+std::string OKeyInv(const Type& t, const std::string& k) {
+  switch (t.id) {
+    case TypeId::REAL: return "kdb_dord_inv(" + k + ")";
+    case TypeId::ENUM: return "(int32_t)(uint32_t)(" + k + " & 0xffffffffULL)";
+    default: return "(" + CType(t.id) + ")(int64_t)(" + k + " ^ 0x8000000000000000ULL)";
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Executor
+// ---------------------------------------------------------------------------
+
+using Consume = std::function<void(const std::vector<CVal>&, const std::string& pos)>;
+
+struct JoinTable {
+  MatBuffer build;
+  uint64_t* slots = nullptr;
+  uint64_t mask = 0;
+};
+
+class Executor {
+ public:
+  Executor(Context& ctx, Arena& arena) : ctx_(ctx), arena_(arena) {}
+
+  HostResult Run(const Operator& root);
+  int64_t bytes_scanned = 0;
+
+ private:
+  Context& ctx_;
+  Arena& arena_;
+  std::map<const Operator*, MatBuffer> mats_;
+  std::map<const Operator*, JoinTable> joins_;
+  std::map<std::pair<const Operator*, int>, JoinTable> skinner_idx_;
+
+  // --- helpers -----------------------------------------------------------
+  static bool Streamable(const Operator& op) {
+    return op.kind == OpKind::SCAN || op.kind == OpKind::SCAN_SELECT || op.kind == OpKind::SELECT ||
+           op.kind == OpKind::HASH_JOIN || op.kind == OpKind::SKINNER_JOIN;
+  }
+
+  // Reads a device counter.  In a compile-only context it reports 2 rows so
+  // the downstream pipelines (sorts, outputs) are still generated.
+  int64_t ReadU64(const uint64_t* d) {
+    uint64_t h = 0;
+    ctx_.D2H(&h, d, sizeof(h));
+    if (ctx_.dry) h = 2;
+    return static_cast<int64_t>(h);
+  }
+
+  MatBuffer AllocMat(const std::vector<SchemaCol>& schema, int64_t cap) {
+    MatBuffer m;
+    m.cap = std::max<int64_t>(cap, 1);
+    for (const auto& c : schema) {
+      MatCol mc;
+      mc.type = c.expr->type;
+      mc.nullable = c.expr->nullable;
+      mc.data = arena_.Alloc(StoreWidth(mc.type.id) * m.cap);
+      if (mc.nullable) mc.nulls = arena_.AllocT<int8_t>(m.cap);
+      m.cols.push_back(mc);
+    }
+    m.pos = arena_.AllocT<uint64_t>(m.cap);
+    return m;
+  }
+
+  // Prepare everything a stream over `op` needs: materialise non-streamable
+  // inputs, build hash-join tables and Skinner indexes.
+  void Prepare(const Operator& op) {
+    switch (op.kind) {
+      case OpKind::SCAN:
+      case OpKind::SCAN_SELECT: return;
+      case OpKind::SELECT:
+        PrepareInput(op.child());
+        return;
+      case OpKind::HASH_JOIN:
+        BuildJoin(op);
+        PrepareInput(op.child(1));
+        return;
+      case OpKind::SKINNER_JOIN:
+        PrepareSkinner(op);
+        return;
+      default: return;
+    }
+  }
+  void PrepareInput(const Operator& op) {
+    if (Streamable(op)) Prepare(op);
+    else if (!mats_.count(&op)) mats_[&op] = Materialize(op);
+  }
+
+  // --- stream emission ---------------------------------------------------
+  void EmitStream(KernelSource& ks, ExprGen& eg, const Operator& op, const Consume& consume,
+                  int64_t& src_rows);
+  void EmitMatScan(KernelSource& ks, const MatBuffer& m, const uint32_t* indirection,
+                   const Consume& consume, int64_t& src_rows);
+  std::vector<CVal> LoadMatRow(KernelSource& ks, ExprGen& eg, const MatBuffer& m,
+                               const std::string& row, std::vector<std::string>* col_ptrs_cache);
+
+  // --- pipelines ---------------------------------------------------------
+  MatBuffer Materialize(const Operator& op);
+  MatBuffer MaterializeStream(const Operator& op, const uint32_t* order = nullptr,
+                              const MatBuffer* ordered_src = nullptr);
+  MatBuffer RunAggregate(const Operator& op);
+  MatBuffer RunGroupBy(const Operator& op);
+  MatBuffer RunOrderBy(const Operator& op);
+  void BuildJoin(const Operator& op);
+  void PrepareSkinner(const Operator& op);
+  JoinTable BuildIndex(const MatBuffer& m, const std::vector<int>& key_cols);
+  void EmitProbe(KernelSource& ks, ExprGen& eg, const JoinTable& jt,
+                 const std::vector<int>& build_key_cols, const std::vector<CVal>& probe_keys,
+                 const std::function<void(const std::vector<CVal>&, const std::string&)>& on_match);
+  std::string JoinHash(ExprGen& eg, const std::vector<CVal>& keys);
+
+  void LaunchPipeline(KernelSource& ks, int64_t src_rows, const char* what, int block = 256) {
+    std::string src = ks.Kernel("kdb_pipeline", block);
+    CUfunction f = ctx_.Kernel(src, "kdb_pipeline");
+    int grid = ctx_.GridFor(std::max<int64_t>(src_rows, 1), block);
+    ctx_.Launch(f, grid, block, ks.Args(), 0, what);
+  }
+};
+
+std::string Executor::JoinHash(ExprGen& eg, const std::vector<CVal>& keys) {
+  std::string h = "0x51ed270b27f1a0c9ULL";
+  for (const auto& k : keys) h = "kdb_hash_combine(" + h + ", " + eg.HashOf(k) + ")";
+  return "(uint32_t)((" + h + ") >> 32)";
+}
+
+std::vector<CVal> Executor::LoadMatRow(KernelSource& ks, ExprGen& eg, const MatBuffer& m,
+                                       const std::string& row, std::vector<std::string>* cache) {
+  std::vector<CVal> vals;
+  for (size_t c = 0; c < m.cols.size(); c++) {
+    const MatCol& mc = m.cols[c];
+    std::string dp, np;
+    if (cache && (*cache).size() > 2 * c && !(*cache)[2 * c].empty()) {
+      dp = (*cache)[2 * c];
+      np = (*cache)[2 * c + 1];
+    } else {
+      dp = ks.Ptr(mc.data, StoreType(mc.type.id), true);
+      np = mc.nullable ? ks.Ptr(mc.nulls, "int8_t", true) : "";
+      if (cache) {
+        if (cache->size() < 2 * m.cols.size()) cache->resize(2 * m.cols.size());
+        (*cache)[2 * c] = dp;
+        (*cache)[2 * c + 1] = np;
+      }
+    }
+    std::string v = dp + "[" + row + "]";
+    if (mc.type.id == TypeId::BOOLEAN) v = "(" + v + " != 0)";
+    vals.push_back(eg.Bind(mc.type, v, mc.nullable ? "(" + np + "[" + row + "] != 0)" : "false"));
+  }
+  return vals;
+}
+
+void Executor::EmitMatScan(KernelSource& ks, const MatBuffer& m, const uint32_t* indirection,
+                           const Consume& consume, int64_t& src_rows) {
+  ExprGen eg(ctx_, ks);
+  src_rows = m.rows;
+  std::string n = ks.Word(static_cast<uint64_t>(m.rows));
+  std::string ind = indirection ? ks.Ptr(indirection, "uint32_t", true) : "";
+  std::string pos = ks.Ptr(m.pos, "uint64_t", true);
+  ks.Open("for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < (int64_t)" + n +
+          "; r += (int64_t)gridDim.x * blockDim.x)");
+  std::string row = "r";
+  if (indirection) {
+    ks.L("int64_t rr = (int64_t)" + ind + "[r];");
+    row = "rr";
+  }
+  auto vals = LoadMatRow(ks, eg, m, row, nullptr);
+  // ordered sources (ORDER BY output) emit in sorted order: position = r
+  consume(vals, indirection ? "(uint64_t)r" : pos + "[" + row + "]");
+  ks.Close();
+}
+
+void Executor::EmitStream(KernelSource& ks, ExprGen& eg, const Operator& op, const Consume& consume,
+                          int64_t& src_rows) {
+  switch (op.kind) {
+    case OpKind::SCAN:
+    case OpKind::SCAN_SELECT: {
+      // scan_translator.cc:140-168 / scan_select_translator.cc:92-156
+      const DevTable* t = nullptr;
+      auto it = ctx_.tables.find(op.relation);
+      if (it == ctx_.tables.end()) throw Error(-1, "unknown relation " + op.relation);
+      t = &it->second;
+      int64_t rows = std::max<int64_t>(t->rows, 0);
+      src_rows = rows;
+      std::string n = ks.Word(static_cast<uint64_t>(rows));
+      // columns used by the filters load first, the rest only for rows that
+      // pass (scan_select_translator.cc:115-134 loads lazily the same way)
+      std::set<int> filter_cols;
+      std::function<void(const Expr&)> collect = [&](const Expr& e) {
+        if (e.kind == ExprKind::VirtColRef || e.kind == ExprKind::ColRef) filter_cols.insert(e.column_idx);
+        for (const auto& k : e.kids) collect(*k);
+      };
+      for (const auto& f : op.filters) collect(*f);
+      std::vector<const DevColumn*> cols;
+      std::vector<std::string> dp, np, tp;
+      for (const auto& sc : op.scan_columns) {
+        const DevColumn& c = ctx_.Column(op.relation, sc.name);
+        if (c.type.id != sc.type.id) throw Error(-1, "column " + sc.name + " type mismatch");
+        cols.push_back(&c);
+        if (c.type.id == TypeId::TEXT) {
+          dp.push_back(ks.Ptr(c.toff, "int64_t", true));
+          tp.push_back(ks.Ptr(c.tchars, "char", true));
+        } else {
+          dp.push_back(ks.Ptr(c.data, StoreType(c.type.id), true));
+          tp.push_back("");
+        }
+        np.push_back(c.nulls ? ks.Ptr(c.nulls, "int8_t", true) : "");
+        bytes_scanned += static_cast<int64_t>(c.bytes);
+      }
+      ks.Open("for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < (int64_t)" + n +
+              "; r += (int64_t)gridDim.x * blockDim.x)");
+      std::vector<CVal> scan(cols.size());
+      auto load = [&](size_t k) {
+        const DevColumn& c = *cols[k];
+        std::string v;
+        if (c.type.id == TypeId::TEXT) v = "kdb_text_at(" + dp[k] + ", " + tp[k] + ", r)";
+        else if (c.type.id == TypeId::BOOLEAN) v = "(" + dp[k] + "[r] != 0)";
+        else v = dp[k] + "[r]";
+        scan[k] = eg.Bind(c.type, v, np[k].empty() ? "false" : "(" + np[k] + "[r] != 0)");
+      };
+      Scope s;
+      if (op.kind == OpKind::SCAN) {
+        for (size_t k = 0; k < cols.size(); k++) load(k);
+        s.child.push_back(scan);
+        std::vector<CVal> out;
+        for (const auto& c : op.output) out.push_back(eg.Emit(*c.expr, s));
+        consume(out, "(uint64_t)r");
+        ks.Close();
+        return;
+      }
+      for (int k : filter_cols)
+        if (k < static_cast<int>(cols.size())) load(k);
+      int opened = 0;
+      for (const auto& f : op.filters) {
+        s.virt = scan;
+        CVal v = eg.Emit(*f, s);
+        ks.Open("if (!(" + v.n + ") && " + v.v + ")");
+        opened++;
+      }
+      for (size_t k = 0; k < cols.size(); k++)
+        if (!filter_cols.count(static_cast<int>(k))) load(k);
+      s.virt = scan;
+      std::vector<CVal> out;
+      for (const auto& c : op.output) out.push_back(eg.Emit(*c.expr, s));
+      consume(out, "(uint64_t)r");
+      for (int i = 0; i < opened; i++) ks.Close();
+      ks.Close();
+      return;
+    }
+    case OpKind::SELECT: {
+      // select_translator.cc:19-37
+      auto body = [&](const std::vector<CVal>& in, const std::string& pos) {
+        Scope s;
+        s.child.push_back(in);
+        CVal v = eg.Emit(*op.filters[0], s);
+        ks.Open("if (!(" + v.n + ") && " + v.v + ")");
+        std::vector<CVal> out;
+        for (const auto& c : op.output) out.push_back(eg.Emit(*c.expr, s));
+        consume(out, pos);
+        ks.Close();
+      };
+      if (Streamable(op.child())) EmitStream(ks, eg, op.child(), body, src_rows);
+      else EmitMatScan(ks, mats_.at(&op.child()), nullptr, body, src_rows);
+      return;
+    }
+    case OpKind::HASH_JOIN: {
+      // probe side: hash_join_translator.cc:106-138
+      const JoinTable& jt = joins_.at(&op);
+      std::vector<int> bkeys;
+      for (const auto& k : op.left_keys) bkeys.push_back(k->column_idx);
+      auto body = [&](const std::vector<CVal>& right, const std::string& pos) {
+        Scope s;
+        s.child.resize(2);
+        s.child[1] = right;
+        std::vector<CVal> pk;
+        for (const auto& k : op.right_keys) pk.push_back(eg.Emit(*k, s));
+        EmitProbe(ks, eg, jt, bkeys, pk, [&](const std::vector<CVal>& left, const std::string& bpos) {
+          Scope s2;
+          s2.child.push_back(left);
+          s2.child.push_back(right);
+          std::vector<CVal> out;
+          for (const auto& c : op.output) out.push_back(eg.Emit(*c.expr, s2));
+          consume(out, "((" + pos + ") << 32) | ((" + bpos + ") & 0xffffffffULL)");
+        });
+      };
+      if (Streamable(op.child(1))) EmitStream(ks, eg, op.child(1), body, src_rows);
+      else EmitMatScan(ks, mats_.at(&op.child(1)), nullptr, body, src_rows);
+      return;
+    }
+    case OpKind::SKINNER_JOIN: {
+      // Fused index-nested-loop over the children in child order: each next
+      // child is reached through a hash index on a column equated with an
+      // already bound child, and every condition is checked as soon as all
+      // its children are bound.  The result set equals the reference's
+      // (permutable_skinner_join_translator.cc:329-912): join order changes
+      // only the emission order.
+      size_t nt = op.children.size();
+      std::vector<std::set<int>> cond_tables(op.conditions.size());
+      std::function<void(const Expr&, std::set<int>&)> collect = [&](const Expr& e, std::set<int>& st) {
+        if (e.kind == ExprKind::ColRef) st.insert(e.child_idx);
+        for (const auto& k : e.kids) collect(*k, st);
+      };
+      for (size_t c = 0; c < op.conditions.size(); c++) collect(*op.conditions[c], cond_tables[c]);
+      Scope s;
+      s.child.resize(nt);
+      std::function<void(size_t, const std::string&)> rec = [&](size_t t, const std::string& pos) {
+        if (t == nt) {
+          std::vector<CVal> out;
+          for (const auto& c : op.output) out.push_back(eg.Emit(*c.expr, s));
+          consume(out, pos);
+          return;
+        }
+        auto bound = [&](const std::vector<CVal>& vals, const std::string& p2) {
+          s.child[t] = vals;
+          int opened = 0;
+          for (size_t c = 0; c < op.conditions.size(); c++) {
+            if (cond_tables[c].empty() || *cond_tables[c].rbegin() != static_cast<int>(t)) continue;
+            CVal v = eg.Emit(*op.conditions[c], s);
+            ks.Open("if (!(" + v.n + ") && " + v.v + ")");
+            opened++;
+          }
+          rec(t + 1, p2);
+          for (int i = 0; i < opened; i++) ks.Close();
+          s.child[t].clear();
+        };
+        const MatBuffer& m = mats_.at(&op.child(t));
+        if (t == 0) {
+          EmitMatScan(ks, m, nullptr, [&](const std::vector<CVal>& vals, const std::string& p) { bound(vals, p); },
+                      src_rows);
+          return;
+        }
+        // an equality condition linking t to a bound child
+        for (size_t c = 0; c < op.conditions.size(); c++) {
+          const Expr& e = *op.conditions[c];
+          if (e.kind != ExprKind::Binary || e.bop != BinOp::EQ) continue;
+          const Expr& a = e.kid(0);
+          const Expr& b = e.kid(1);
+          if (a.kind != ExprKind::ColRef || b.kind != ExprKind::ColRef) continue;
+          const Expr* mine = nullptr;
+          const Expr* other = nullptr;
+          if (a.child_idx == static_cast<int>(t) && b.child_idx < static_cast<int>(t)) {
+            mine = &a;
+            other = &b;
+          } else if (b.child_idx == static_cast<int>(t) && a.child_idx < static_cast<int>(t)) {
+            mine = &b;
+            other = &a;
+          }
+          if (!mine) continue;
+          const JoinTable& jt = skinner_idx_.at({&op, static_cast<int>(t) * 1000 + mine->column_idx});
+          CVal key = s.child[other->child_idx].at(other->column_idx);
+          EmitProbe(ks, eg, jt, {mine->column_idx}, {key},
+                    [&](const std::vector<CVal>& vals, const std::string& bpos) {
+                      bound(vals, "((" + pos + ") * 1000003ULL + (" + bpos + "))");
+                    });
+          return;
+        }
+        // no equality link: nested loop over all rows of child t
+        std::string n = ks.Word(static_cast<uint64_t>(m.rows));
+        std::string it = ks.Fresh("t");
+        ks.Open("for (int64_t " + it + " = 0; " + it + " < (int64_t)" + n + "; " + it + "++)");
+        auto vals = LoadMatRow(ks, eg, m, it, nullptr);
+        bound(vals, "((" + pos + ") * 1000003ULL + (uint64_t)" + it + ")");
+        ks.Close();
+      };
+      rec(0, "0ULL");
+      return;
+    }
+    default: {
+      EmitMatScan(ks, mats_.at(&op), nullptr, consume, src_rows);
+      return;
+    }
+  }
+}
+
+void Executor::EmitProbe(KernelSource& ks, ExprGen& eg, const JoinTable& jt,
+                         const std::vector<int>& bkeys, const std::vector<CVal>& pk,
+                         const std::function<void(const std::vector<CVal>&, const std::string&)>& on_match) {
+  // NULL probe keys never equal a (non-NULL) build key
+  std::string nn = "true";
+  for (const auto& k : pk) nn += " && !(" + k.n + ")";
+  ks.Open("if (" + nn + ")");
+  std::string h = ks.Fresh("h");
+  ks.L("uint32_t " + h + " = " + JoinHash(eg, pk) + ";");
+  std::string slots = ks.Ptr(jt.slots, "uint64_t", true);
+  std::string mask = ks.Word(jt.mask);
+  std::string i = ks.Fresh("i"), k = ks.Fresh("k"), e = ks.Fresh("e");
+  ks.L("uint64_t " + i + " = kdb_mix64(" + h + ") & " + mask + ";");
+  ks.Open("for (uint64_t " + k + " = 0; " + k + " <= " + mask + "; " + k + "++, " + i + " = (" + i +
+          " + 1) & " + mask + ")");
+  ks.L("uint64_t " + e + " = " + slots + "[" + i + "];");
+  ks.L("if (" + e + " == 0) break;");
+  ks.Open("if ((uint32_t)(" + e + " >> 32) == " + h + ")");
+  std::string br = ks.Fresh("br");
+  ks.L("int64_t " + br + " = (int64_t)(uint32_t)" + e + " - 1;");
+  auto left = LoadMatRow(ks, eg, jt.build, br, nullptr);
+  std::string eq = "true";
+  for (size_t j = 0; j < bkeys.size(); j++) eq += " && " + eg.EqOf(left.at(bkeys[j]), pk[j]);
+  ks.Open("if (" + eq + ")");
+  std::string bpos = ks.Ptr(jt.build.pos, "uint64_t", true) + "[" + br + "]";
+  on_match(left, bpos);
+  ks.Close();
+  ks.Close();
+  ks.Close();
+  ks.Close();
+}
+
+// Join table over materialised rows (runtime::HashTable equivalent,
+// runtime/hash_table.cc:13-36): build rows with a NULL key are skipped
+// (hash_join_translator.cc:86-101).
+JoinTable Executor::BuildIndex(const MatBuffer& m, const std::vector<int>& key_cols) {
+  JoinTable jt;
+  jt.build = m;
+  uint64_t cap = 1024;
+  while (cap < static_cast<uint64_t>(m.rows) * 2) cap <<= 1;
+  jt.mask = cap - 1;
+  jt.slots = arena_.AllocT<uint64_t>(cap);
+  ctx_.Memset(jt.slots, 0, cap * sizeof(uint64_t));
+  if (m.rows == 0) return jt;
+  KernelSource ks;
+  ExprGen eg(ctx_, ks);
+  std::string n = ks.Word(static_cast<uint64_t>(m.rows));
+  std::string slots = ks.Ptr(jt.slots, "uint64_t");
+  std::string mask = ks.Word(jt.mask);
+  ks.Open("for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < (int64_t)" + n +
+          "; r += (int64_t)gridDim.x * blockDim.x)");
+  auto vals = LoadMatRow(ks, eg, m, "r", nullptr);
+  std::vector<CVal> keys;
+  std::string nn = "true";
+  for (int c : key_cols) {
+    keys.push_back(vals.at(c));
+    nn += " && !(" + vals.at(c).n + ")";
+  }
+  ks.Open("if (" + nn + ")");
+  ks.L("kdb_join_insert(" + slots + ", " + mask + ", " + JoinHash(eg, keys) + ", (uint32_t)r);");
+  ks.Close();
+  ks.Close();
+  LaunchPipeline(ks, m.rows, "join build");
+  return jt;
+}
+
+void Executor::BuildJoin(const Operator& op) {
+  if (joins_.count(&op)) return;
+  MatBuffer left = Materialize(op.child(0));
+  std::vector<int> keys;
+  for (const auto& k : op.left_keys) {
+    if (k->kind != ExprKind::ColRef) throw Error(-5, "hash join keys must be column references");
+    keys.push_back(k->column_idx);
+  }
+  joins_[&op] = BuildIndex(left, keys);
+}
+
+void Executor::PrepareSkinner(const Operator& op) {
+  for (size_t t = 0; t < op.children.size(); t++)
+    if (!mats_.count(&op.child(t))) mats_[&op.child(t)] = Materialize(op.child(t));
+  for (size_t t = 1; t < op.children.size(); t++) {
+    for (const auto& cp : op.conditions) {
+      const Expr& e = *cp;
+      if (e.kind != ExprKind::Binary || e.bop != BinOp::EQ) continue;
+      const Expr& a = e.kid(0);
+      const Expr& b = e.kid(1);
+      if (a.kind != ExprKind::ColRef || b.kind != ExprKind::ColRef) continue;
+      const Expr* mine = nullptr;
+      if (a.child_idx == static_cast<int>(t) && b.child_idx < static_cast<int>(t)) mine = &a;
+      else if (b.child_idx == static_cast<int>(t) && a.child_idx < static_cast<int>(t)) mine = &b;
+      if (!mine) continue;
+      auto key = std::make_pair(&op, static_cast<int>(t) * 1000 + mine->column_idx);
+      if (!skinner_idx_.count(key))
+        skinner_idx_[key] = BuildIndex(mats_.at(&op.child(t)), {mine->column_idx});
+      break;
+    }
+  }
+}
+
+// Materialise a streamable operator's rows (with stream positions), or, when
+// `ordered_src` is given, project `op.output` over that buffer read in
+// `order`.  Capacity: exact bound for scans; join outputs are counted and the
+// pipeline reruns once at the counted size if the first guess was short.
+MatBuffer Executor::MaterializeStream(const Operator& op, const uint32_t* order,
+                                      const MatBuffer* ordered_src) {
+  if (!ordered_src) Prepare(op);
+  std::function<int64_t(const Operator&)> bound = [&](const Operator& o) -> int64_t {
+    switch (o.kind) {
+      case OpKind::SCAN:
+      case OpKind::SCAN_SELECT: {
+        auto it = ctx_.tables.find(o.relation);
+        return it == ctx_.tables.end() ? 0 : std::max<int64_t>(it->second.rows, 0);
+      }
+      case OpKind::SELECT: return bound(o.child());
+      case OpKind::HASH_JOIN:
+        return 2 * std::max<int64_t>(bound(o.child(1)), joins_.count(&o) ? joins_.at(&o).build.rows : 0);
+      default: {
+        auto it = mats_.find(&o);
+        return it == mats_.end() ? 1024 : it->second.rows;
+      }
+    }
+  };
+  int64_t cap = ordered_src ? ordered_src->rows : bound(op);
+  for (int attempt = 0; attempt < 3; attempt++) {
+    KernelSource ks;
+    ExprGen eg(ctx_, ks);
+    const auto& schema = op.output;
+    MatBuffer out = AllocMat(schema, cap);
+    uint64_t* counter = arena_.AllocT<uint64_t>(1);
+    ctx_.Memset(counter, 0, sizeof(uint64_t));
+    std::vector<std::string> optr, onull;
+    for (const auto& c : out.cols) {
+      optr.push_back(ks.Ptr(c.data, StoreType(c.type.id)));
+      onull.push_back(c.nullable ? ks.Ptr(c.nulls, "int8_t") : "");
+    }
+    std::string posp = ks.Ptr(out.pos, "uint64_t");
+    std::string cnt = ks.Ptr(counter, "uint64_t");
+    std::string capw = "(uint64_t)" + ks.Word(static_cast<uint64_t>(out.cap));
+    auto sink = [&](const std::vector<CVal>& vals, const std::string& pos) {
+      ks.Open("");
+      ks.L("uint64_t slot = kdb_alloc_slot((unsigned long long*)" + cnt + ");");
+      ks.Open("if (slot < " + capw + ")");
+      for (size_t c = 0; c < vals.size(); c++) {
+        const CVal& v = vals[c];
+        std::string val = v.type.id == TypeId::BOOLEAN ? "(int8_t)(" + v.v + " ? 1 : 0)" : v.v;
+        ks.L(optr[c] + "[slot] = " + val + ";");
+        if (!onull[c].empty()) ks.L(onull[c] + "[slot] = (" + v.n + ") ? 1 : 0;");
+      }
+      ks.L(posp + "[slot] = " + pos + ";");
+      ks.Close();
+      ks.Close();
+    };
+    int64_t src_rows = 0;
+    if (ordered_src) {
+      auto body = [&](const std::vector<CVal>& in, const std::string& pos) {
+        Scope s;
+        s.child.push_back(in);
+        std::vector<CVal> vals;
+        for (const auto& c : schema) vals.push_back(eg.Emit(*c.expr, s));
+        sink(vals, pos);
+      };
+      EmitMatScan(ks, *ordered_src, order, body, src_rows);
+    } else {
+      EmitStream(ks, eg, op, sink, src_rows);
+    }
+    LaunchPipeline(ks, src_rows, "materialize");
+    int64_t produced = ReadU64(counter);
+    ctx_.CheckDeviceError("materialize");
+    if (produced <= out.cap) {
+      out.rows = produced;
+      return out;
+    }
+    if (ordered_src) throw Error(-4, "ordered materialisation overflow");
+    cap = produced;
+  }
+  throw Error(-4, "materialisation did not converge");
+}
+
+MatBuffer Executor::Materialize(const Operator& op) {
+  switch (op.kind) {
+    case OpKind::OUTPUT: return Materialize(op.child());
+    case OpKind::AGGREGATE: return RunAggregate(op);
+    case OpKind::GROUP_BY_AGGREGATE: return RunGroupBy(op);
+    case OpKind::ORDER_BY: return RunOrderBy(op);
+    default: return MaterializeStream(op);
+  }
+}
+
+// Emits the per-row update of one aggregate at group slot `g` (atomics).
+void EmitGroupUpdate(KernelSource& ks, ExprGen& eg, const AggPlan& p, const CVal& c,
+                     const std::string& sv, const std::string& sc, const std::string& g) {
+  ks.Open("if (!(" + c.n + "))");
+  switch (p.kind) {
+    case StateKind::SumF64: ks.L("atomicAdd((double*)&" + sv + "[" + g + "], " + c.v + ");"); break;
+    case StateKind::AvgF64: ks.L("atomicAdd((double*)&" + sv + "[" + g + "], (double)" + c.v + ");"); break;
+    case StateKind::SumI64:
+      ks.L("atomicAdd((unsigned long long*)&" + sv + "[" + g + "], (unsigned long long)(int64_t)" + c.v + ");");
+      break;
+    case StateKind::MinMaxKey:
+      ks.L(std::string(p.is_min ? "kdb_atomic_min_u64(&" : "kdb_atomic_max_u64(&") + sv + "[" + g + "], " +
+           OKey(eg, c) + ");");
+      break;
+    case StateKind::MinMaxText:
+      ks.L("kdb_atomic_str_minmax(&" + sv + "[" + g + "], " + c.v + ", " + (p.is_min ? "true" : "false") + ");");
+      break;
+    case StateKind::Count: break;
+  }
+  ks.L("atomicAdd((unsigned long long*)&" + sc + "[" + g + "], 1ULL);");
+  ks.Close();
+}
+
+// The aggregate's result value from its state at slot `g`.
+CVal GroupResult(ExprGen& eg, const AggPlan& p, const std::string& sv, const std::string& sc,
+                 const std::string& g, const std::string& first) {
+  const Type& rt = p.agg->type;
+  const Type& ct = p.agg->kid(0).type;
+  std::string v = sv + "[" + g + "]", c = "(int64_t)" + sc + "[" + g + "]";
+  switch (p.kind) {
+    case StateKind::SumF64: return eg.Bind(rt, "__longlong_as_double((long long)" + v + ")", c + " == 0");
+    case StateKind::SumI64: return eg.Bind(rt, "(" + CType(rt.id) + ")(int64_t)" + v, c + " == 0");
+    case StateKind::AvgF64:
+      return eg.Bind(rt, "__ddiv_rn(__longlong_as_double((long long)" + v + "), (double)" + c + ")", c + " == 0");
+    case StateKind::Count: {
+      std::string val = c;
+      if (p.count_flag >= 0) val = "(" + c + " + (int64_t)((" + first + " >> " + std::to_string(p.count_flag) + ") & 1ULL))";
+      return eg.Bind(rt, val, "false");
+    }
+    case StateKind::MinMaxKey: return eg.Bind(rt, OKeyInv(ct, v), c + " == 0");
+    case StateKind::MinMaxText: return eg.Bind(rt, "kdb_str_from_handle(" + v + ")", c + " == 0");
+  }
+  throw Error(-1, "bad aggregate");
+}
+
+// ---------------------------------------------------------------------------
+// Ungrouped aggregate (aggregate_translator.cc:34-126): per-thread register
+// state, block reduction to per-block partials, one finalize thread that
+// combines the partials in block order and evaluates the output schema.
+// ---------------------------------------------------------------------------
+
+MatBuffer Executor::RunAggregate(const Operator& op) {
+  PrepareInput(op.child());
+  int flags = 0;
+  std::vector<AggPlan> plans;
+  for (const auto& a : op.aggs) plans.push_back(PlanAgg(*a, flags));
+  const int nw = static_cast<int>(plans.size()) * 2 + 2;  // per agg: value, count; + rows, first
+  const int block = 256;
+
+  KernelSource ks;
+  ExprGen eg(ctx_, ks);
+  int64_t src_rows = 0;
+  for (size_t j = 0; j < plans.size(); j++) {
+    const AggPlan& p = plans[j];
+    std::string J = std::to_string(j);
+    switch (p.kind) {
+      case StateKind::SumF64:
+      case StateKind::AvgF64: ks.L("double s" + J + " = 0.0;"); break;
+      case StateKind::MinMaxKey: ks.L("uint64_t s" + J + " = " + (p.is_min ? "~0ULL;" : "0ULL;")); break;
+      default: ks.L("int64_t s" + J + " = 0;"); break;
+    }
+    ks.L("int64_t c" + J + " = 0;");
+  }
+  ks.L("int64_t rows = 0;");
+  ks.L("uint64_t first = ~0ULL;");
+  uint64_t* text_state = arena_.AllocT<uint64_t>(plans.size() + 1);
+  ctx_.Memset(text_state, 0, sizeof(uint64_t) * (plans.size() + 1));
+  std::string tsp = ks.Ptr(text_state, "uint64_t");
+  auto consume = [&](const std::vector<CVal>& in, const std::string& pos) {
+    Scope s;
+    s.child.push_back(in);
+    std::string fl = "0ULL";
+    for (size_t j = 0; j < plans.size(); j++) {
+      const AggPlan& p = plans[j];
+      CVal c = eg.Emit(p.agg->kid(0), s);
+      std::string J = std::to_string(j);
+      if (p.count_flag >= 0) fl += " | ((" + c.n + ") ? " + std::to_string(1 << p.count_flag) + "ULL : 0ULL)";
+      ks.Open("if (!(" + c.n + "))");
+      switch (p.kind) {
+        case StateKind::SumF64: ks.L("s" + J + " = __dadd_rn(s" + J + ", " + c.v + ");"); break;
+        case StateKind::AvgF64: ks.L("s" + J + " = __dadd_rn(s" + J + ", (double)" + c.v + ");"); break;
+        case StateKind::SumI64:
+          ks.L("s" + J + " = (int64_t)((uint64_t)s" + J + " + (uint64_t)(int64_t)" + c.v + ");");
+          break;
+        case StateKind::MinMaxKey:
+          ks.L("{ uint64_t k = " + OKey(eg, c) + "; s" + J + " = " + (p.is_min ? "(k < s" : "(k > s") + J +
+               ") ? k : s" + J + "; }");
+          break;
+        case StateKind::MinMaxText:
+          ks.L("kdb_atomic_str_minmax(&" + tsp + "[" + J + "], " + c.v + ", " + (p.is_min ? "true" : "false") + ");");
+          break;
+        case StateKind::Count: break;
+      }
+      ks.L("c" + J + "++;");
+      ks.Close();
+    }
+    ks.L("rows++;");
+    ks.L("{ uint64_t f = ((uint64_t)(" + pos + ") << 8) | (" + fl + "); first = f < first ? f : first; }");
+  };
+  if (Streamable(op.child())) EmitStream(ks, eg, op.child(), consume, src_rows);
+  else EmitMatScan(ks, mats_.at(&op.child()), nullptr, consume, src_rows);
+
+  int grid = ctx_.GridFor(std::max<int64_t>(src_rows, 1), block);
+  uint64_t* part = arena_.AllocT<uint64_t>(static_cast<size_t>(grid) * nw);
+  std::string pp = ks.Ptr(part, "uint64_t");
+  ks.L("__shared__ uint64_t red_u[32];");
+  ks.L("__shared__ double red_d[32];");
+  ks.L("__shared__ int64_t red_i[32];");
+  auto store = [&](int w, const std::string& val) {
+    ks.L("if (threadIdx.x == 0) " + pp + "[(int64_t)blockIdx.x * " + std::to_string(nw) + " + " +
+         std::to_string(w) + "] = " + val + ";");
+  };
+  for (size_t j = 0; j < plans.size(); j++) {
+    const AggPlan& p = plans[j];
+    std::string J = std::to_string(j);
+    switch (p.kind) {
+      case StateKind::SumF64:
+      case StateKind::AvgF64:
+        ks.Open("");
+        ks.L("double t = kdb_block_reduce(s" + J + ", KdbAddF64(), red_d);");
+        store(static_cast<int>(j) * 2, "(uint64_t)__double_as_longlong(t)");
+        ks.Close();
+        break;
+      case StateKind::SumI64:
+        ks.Open("");
+        ks.L("int64_t t = kdb_block_reduce(s" + J + ", KdbAddI64(), red_i);");
+        store(static_cast<int>(j) * 2, "(uint64_t)t");
+        ks.Close();
+        break;
+      case StateKind::MinMaxKey:
+        ks.Open("");
+        ks.L("uint64_t t = kdb_block_reduce(s" + J + (p.is_min ? ", KdbMinU64(), red_u);" : ", KdbMaxU64(), red_u);"));
+        store(static_cast<int>(j) * 2, "t");
+        ks.Close();
+        break;
+      default: break;
+    }
+    ks.Open("");
+    ks.L("int64_t t = kdb_block_reduce(c" + J + ", KdbAddI64(), red_i);");
+    store(static_cast<int>(j) * 2 + 1, "(uint64_t)t");
+    ks.Close();
+  }
+  ks.Open("");
+  ks.L("int64_t t = kdb_block_reduce(rows, KdbAddI64(), red_i);");
+  store(nw - 2, "(uint64_t)t");
+  ks.Close();
+  ks.Open("");
+  ks.L("uint64_t t = kdb_block_reduce(first, KdbMinU64(), red_u);");
+  store(nw - 1, "t");
+  ks.Close();
+  {
+    std::string src = ks.Kernel("kdb_pipeline", block);
+    CUfunction f = ctx_.Kernel(src, "kdb_pipeline");
+    ctx_.Launch(f, grid, block, ks.Args(), 0, "aggregate");
+  }
+
+  // Finalize.  Every output column gets a NULL array: an empty input emits a
+  // single all-NULL row even for COUNT (aggregate_translator.cc:82-89).
+  MatBuffer out = AllocMat(op.output, 1);
+  for (auto& mc : out.cols)
+    if (!mc.nulls) {
+      mc.nullable = true;
+      mc.nulls = arena_.AllocT<int8_t>(1);
+    }
+  KernelSource fk;
+  ExprGen fg(ctx_, fk);
+  std::string fp = fk.Ptr(part, "uint64_t", true);
+  std::string ftp = fk.Ptr(text_state, "uint64_t", true);
+  std::string G = fk.Word(static_cast<uint64_t>(grid));
+  fk.Open("if (blockIdx.x == 0 && threadIdx.x == 0)");
+  for (size_t j = 0; j < plans.size(); j++) {
+    const AggPlan& p = plans[j];
+    std::string J = std::to_string(j);
+    switch (p.kind) {
+      case StateKind::SumF64:
+      case StateKind::AvgF64: fk.L("double s" + J + " = 0.0;"); break;
+      case StateKind::MinMaxKey: fk.L("uint64_t s" + J + " = " + (p.is_min ? "~0ULL;" : "0ULL;")); break;
+      default: fk.L("int64_t s" + J + " = 0;"); break;
+    }
+    fk.L("int64_t c" + J + " = 0;");
+  }
+  fk.L("int64_t rows = 0;");
+  fk.L("uint64_t first = ~0ULL;");
+  fk.Open("for (int64_t b = 0; b < (int64_t)" + G + "; b++)");
+  fk.L("const uint64_t* q = " + fp + " + b * " + std::to_string(nw) + ";");
+  for (size_t j = 0; j < plans.size(); j++) {
+    const AggPlan& p = plans[j];
+    std::string J = std::to_string(j), W = std::to_string(j * 2);
+    switch (p.kind) {
+      case StateKind::SumF64:
+      case StateKind::AvgF64:
+        fk.L("s" + J + " = __dadd_rn(s" + J + ", __longlong_as_double((long long)q[" + W + "]));");
+        break;
+      case StateKind::SumI64: fk.L("s" + J + " = (int64_t)((uint64_t)s" + J + " + q[" + W + "]);"); break;
+      case StateKind::MinMaxKey:
+        fk.L("s" + J + " = (q[" + W + "] " + (p.is_min ? "<" : ">") + " s" + J + ") ? q[" + W + "] : s" + J + ";");
+        break;
+      default: break;
+    }
+    fk.L("c" + J + " += (int64_t)q[" + std::to_string(j * 2 + 1) + "];");
+  }
+  fk.L("rows += (int64_t)q[" + std::to_string(nw - 2) + "];");
+  fk.L("first = q[" + std::to_string(nw - 1) + "] < first ? q[" + std::to_string(nw - 1) + "] : first;");
+  fk.Close();
+  std::vector<CVal> virt;
+  for (size_t j = 0; j < plans.size(); j++) {
+    const AggPlan& p = plans[j];
+    std::string J = std::to_string(j);
+    const Type& rt = p.agg->type;
+    const Type& ct = p.agg->kid(0).type;
+    switch (p.kind) {
+      case StateKind::SumF64: virt.push_back(fg.Bind(rt, "s" + J, "c" + J + " == 0")); break;
+      case StateKind::SumI64: virt.push_back(fg.Bind(rt, "(" + CType(rt.id) + ")s" + J, "c" + J + " == 0")); break;
+      case StateKind::AvgF64:
+        virt.push_back(fg.Bind(rt, "__ddiv_rn(s" + J + ", (double)c" + J + ")", "c" + J + " == 0"));
+        break;
+      case StateKind::Count: {
+        std::string v = "c" + J;
+        if (p.count_flag >= 0) v = "(c" + J + " + (int64_t)((first >> " + std::to_string(p.count_flag) + ") & 1ULL))";
+        virt.push_back(fg.Bind(rt, v, "false"));
+        break;
+      }
+      case StateKind::MinMaxKey: virt.push_back(fg.Bind(rt, OKeyInv(ct, "s" + J), "c" + J + " == 0")); break;
+      case StateKind::MinMaxText:
+        virt.push_back(fg.Bind(rt, "kdb_str_from_handle(" + ftp + "[" + J + "])", "c" + J + " == 0"));
+        break;
+    }
+  }
+  Scope s;
+  s.virt = virt;
+  std::vector<CVal> vals;
+  for (const auto& c : op.output) vals.push_back(fg.Emit(*c.expr, s));
+  for (size_t c = 0; c < out.cols.size(); c++) {
+    const MatCol& mc = out.cols[c];
+    std::string dp = fk.Ptr(mc.data, StoreType(mc.type.id));
+    std::string val = mc.type.id == TypeId::BOOLEAN ? "(int8_t)(" + vals[c].v + " ? 1 : 0)" : vals[c].v;
+    fk.L(dp + "[0] = " + val + ";");
+    std::string np = fk.Ptr(mc.nulls, "int8_t");
+    fk.L(np + "[0] = (rows == 0 || (" + vals[c].n + ")) ? 1 : 0;");
+  }
+  std::string posp = fk.Ptr(out.pos, "uint64_t");
+  fk.L(posp + "[0] = 0;");
+  fk.Close();
+  {
+    std::string src = fk.Kernel("kdb_finalize", 32);
+    CUfunction f = ctx_.Kernel(src, "kdb_finalize");
+    ctx_.Launch(f, 1, 32, fk.Args(), 0, "aggregate finalize");
+  }
+  ctx_.CheckDeviceError("aggregate");
+  out.rows = 1;
+  return out;
+}
+
+// ---------------------------------------------------------------------------
+// Group-by (group_by_aggregate_translator.cc:36-111 + AggregateHashTable):
+// a device open-addressing table updated with atomics, then compaction of the
+// occupied slots, a radix sort on each group's first stream position (the
+// reference's ForEach emits groups in insertion order,
+// compile/proxy/aggregate_hash_table.cc:245-291) and one output kernel.
+// ---------------------------------------------------------------------------
+
+struct KeyLayout {
+  bool packed = true;
+  std::vector<int> offset, width;
+  std::vector<bool> nullable;
+  int bits = 0;
+  uint64_t domain = 1;  // number of distinct keys when all keys are enum/bool
+  bool small_domain = true;
+};
+
+KeyLayout PlanKeys(Context& ctx, const std::vector<std::unique_ptr<Expr>>& keys) {
+  KeyLayout kl;
+  for (const auto& k : keys) {
+    int w = 0;
+    uint64_t card = 0;
+    switch (k->type.id) {
+      case TypeId::ENUM: {
+        uint64_t n = ctx.Enum(k->type.enum_id).values.size();
+        w = 1;
+        while ((1ULL << w) < n) w++;
+        card = n;
+        break;
+      }
+      case TypeId::BOOLEAN: w = 1; card = 2; break;
+      case TypeId::SMALLINT: w = 16; break;
+      case TypeId::INT:
+      case TypeId::DATE: w = 32; break;
+      case TypeId::BIGINT:
+      case TypeId::REAL: w = 64; break;
+      case TypeId::TEXT: w = 1000; break;
+    }
+    kl.offset.push_back(kl.bits);
+    kl.width.push_back(w);
+    kl.nullable.push_back(k->nullable);
+    kl.bits += w + (k->nullable ? 1 : 0);
+    if (card == 0) kl.small_domain = false;
+    else if (kl.small_domain) kl.domain *= card + (k->nullable ? 1 : 0);
+  }
+  kl.packed = kl.bits <= 63;
+  return kl;
+}
+
+MatBuffer Executor::RunGroupBy(const Operator& op) {
+  PrepareInput(op.child());
+  int flags = 0;
+  std::vector<AggPlan> plans;
+  for (const auto& a : op.aggs) plans.push_back(PlanAgg(*a, flags));
+  KeyLayout kl = PlanKeys(ctx_, op.group_by);
+  const size_t nk = op.group_by.size();
+
+  uint64_t cap = 1024;
+  if (kl.small_domain) {
+    while (cap < 2 * kl.domain) cap <<= 1;
+  } else {
+    cap = 1 << 16;
+  }
+  for (int attempt = 0; attempt < 8; attempt++) {
+    uint64_t mask = cap - 1;
+    uint64_t* slots = arena_.AllocT<uint64_t>(cap);
+    uint64_t* first = arena_.AllocT<uint64_t>(cap);
+    uint64_t* gcount = arena_.AllocT<uint64_t>(1);
+    std::vector<uint64_t*> kw(nk), sv(plans.size()), sc(plans.size());
+    std::vector<int32_t*> klen(nk);
+    std::vector<int8_t*> kn(nk);
+    if (!kl.packed)
+      for (size_t k = 0; k < nk; k++) {
+        kw[k] = arena_.AllocT<uint64_t>(cap);
+        klen[k] = arena_.AllocT<int32_t>(cap);
+        kn[k] = arena_.AllocT<int8_t>(cap);
+      }
+    for (size_t j = 0; j < plans.size(); j++) {
+      sv[j] = arena_.AllocT<uint64_t>(cap);
+      sc[j] = arena_.AllocT<uint64_t>(cap);
+    }
+    ctx_.Memset(gcount, 0, sizeof(uint64_t));
+    // init kernel
+    {
+      KernelSource ks;
+      std::string S = ks.Ptr(slots, "uint64_t"), F = ks.Ptr(first, "uint64_t");
+      std::string C = ks.Word(cap);
+      ks.Open("for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < (int64_t)" + C +
+              "; i += (int64_t)gridDim.x * blockDim.x)");
+      ks.L(S + "[i] = 0; " + F + "[i] = ~0ULL;");
+      for (size_t j = 0; j < plans.size(); j++) {
+        std::string V = ks.Ptr(sv[j], "uint64_t"), N = ks.Ptr(sc[j], "uint64_t");
+        bool min_init = plans[j].kind == StateKind::MinMaxKey && plans[j].is_min;
+        ks.L(V + "[i] = " + (min_init ? "~0ULL" : "0ULL") + "; " + N + "[i] = 0;");
+      }
+      ks.Close();
+      LaunchPipeline(ks, static_cast<int64_t>(cap), "group init");
+    }
+    // aggregation pipeline
+    {
+      KernelSource ks;
+      ExprGen eg(ctx_, ks);
+      std::string S = ks.Ptr(slots, "uint64_t"), F = ks.Ptr(first, "uint64_t");
+      std::string M = "(uint64_t)" + ks.Word(mask), GC = ks.Ptr(gcount, "unsigned long long");
+      std::string LIM = "(uint64_t)" + ks.Word(cap / 2);
+      std::string ERR = ks.Ptr(ctx_.d_err, "int");
+      std::vector<std::string> KW(nk), KL(nk), KN(nk), SV(plans.size()), SC(plans.size());
+      if (!kl.packed)
+        for (size_t k = 0; k < nk; k++) {
+          KW[k] = ks.Ptr(kw[k], "uint64_t");
+          KL[k] = ks.Ptr(klen[k], "int32_t");
+          KN[k] = ks.Ptr(kn[k], "int8_t");
+        }
+      for (size_t j = 0; j < plans.size(); j++) {
+        SV[j] = ks.Ptr(sv[j], "uint64_t");
+        SC[j] = ks.Ptr(sc[j], "uint64_t");
+      }
+      int64_t src_rows = 0;
+      auto consume = [&](const std::vector<CVal>& in, const std::string& pos) {
+        Scope s;
+        s.child.push_back(in);
+        std::vector<CVal> keys;
+        for (const auto& g : op.group_by) keys.push_back(eg.Emit(*g, s));
+        std::string g = ks.Fresh("g");
+        if (kl.packed) {
+          std::string pk = "0x8000000000000000ULL";
+          for (size_t k = 0; k < nk; k++) {
+            const CVal& c = keys[k];
+            std::string bits;
+            switch (c.type.id) {
+              case TypeId::REAL: bits = "kdb_dbits(" + c.v + ")"; break;
+              case TypeId::BOOLEAN: bits = "(uint64_t)(" + c.v + " ? 1 : 0)"; break;
+              case TypeId::SMALLINT: bits = "(uint64_t)(uint16_t)" + c.v; break;
+              case TypeId::BIGINT: bits = "(uint64_t)" + c.v; break;
+              default: bits = "(uint64_t)(uint32_t)" + c.v; break;
+            }
+            uint64_t m = kl.width[k] >= 64 ? ~0ULL : ((1ULL << kl.width[k]) - 1);
+            std::string field = "((" + c.n + ") ? 0ULL : ((" + bits + ") & " + std::to_string(m) + "ULL))";
+            pk += " | (" + field + " << " + std::to_string(kl.offset[k]) + ")";
+            if (kl.nullable[k])
+              pk += " | ((" + c.n + ") ? (1ULL << " + std::to_string(kl.offset[k] + kl.width[k]) + ") : 0ULL)";
+          }
+          ks.L("int64_t " + g + " = kdb_group_find_packed(" + S + ", " + M + ", " + pk + ", " + GC + ", " + LIM +
+               ", " + ERR + ");");
+        } else {
+          std::string h = "0x2545f4914f6cdd1dULL";
+          for (size_t k = 0; k < nk; k++)
+            h = "kdb_hash_combine(" + h + ", (" + keys[k].n + ") ? 0x9e3779b97f4a7c15ULL : " + eg.HashOf(keys[k]) + ")";
+          std::string eq = "true", init;
+          for (size_t k = 0; k < nk; k++) {
+            const CVal& c = keys[k];
+            std::string stored_null = "(__ldcg(&" + KN[k] + "[i]) != 0)";
+            std::string w = "__ldcg((const unsigned long long*)&" + KW[k] + "[i])";
+            std::string veq;
+            switch (c.type.id) {
+              case TypeId::TEXT:
+                veq = "kdb_str_eq(kdb_mkstr((const char*)" + w + ", __ldcg(&" + KL[k] + "[i])), " + c.v + ")";
+                init += KW[k] + "[i] = (uint64_t)" + c.v + ".p; " + KL[k] + "[i] = " + c.v + ".len; ";
+                break;
+              case TypeId::REAL:
+                veq = "(__longlong_as_double((long long)" + w + ") == " + c.v + ")";
+                init += KW[k] + "[i] = (uint64_t)__double_as_longlong(" + c.v + "); ";
+                break;
+              case TypeId::BOOLEAN:
+                veq = "((" + w + " != 0) == " + c.v + ")";
+                init += KW[k] + "[i] = " + c.v + " ? 1ULL : 0ULL; ";
+                break;
+              default:
+                veq = "((int64_t)" + w + " == (int64_t)" + c.v + ")";
+                init += KW[k] + "[i] = (uint64_t)(int64_t)" + c.v + "; ";
+                break;
+            }
+            init += KN[k] + "[i] = (" + c.n + ") ? 1 : 0; ";
+            eq += " && (" + stored_null + " == (" + c.n + ")) && ((" + c.n + ") || " + veq + ")";
+          }
+          ks.L("int64_t " + g + " = kdb_group_find(" + S + ", " + M + ", (" + h +
+               ") | 0x8000000000000000ULL, [&](uint64_t i) { return " + eq + "; }, [&](uint64_t i) { " + init +
+               "}, " + GC + ", " + LIM + ", " + ERR + ");");
+        }
+        ks.Open("if (" + g + " >= 0)");
+        std::string fl = "0ULL";
+        for (size_t j = 0; j < plans.size(); j++) {
+          CVal c = eg.Emit(plans[j].agg->kid(0), s);
+          if (plans[j].count_flag >= 0)
+            fl += " | ((" + c.n + ") ? " + std::to_string(1 << plans[j].count_flag) + "ULL : 0ULL)";
+          EmitGroupUpdate(ks, eg, plans[j], c, SV[j], SC[j], g);
+        }
+        ks.L("kdb_atomic_min_u64(&" + F + "[" + g + "], ((uint64_t)(" + pos + ") << 8) | (" + fl + "));");
+        ks.Close();
+      };
+      if (Streamable(op.child())) EmitStream(ks, eg, op.child(), consume, src_rows);
+      else EmitMatScan(ks, mats_.at(&op.child()), nullptr, consume, src_rows);
+      LaunchPipeline(ks, src_rows, "group by");
+    }
+    try {
+      ctx_.CheckDeviceError("group by");
+    } catch (const Error& e) {
+      if (e.code == -4 && !kl.small_domain) {
+        cap <<= 3;
+        continue;
+      }
+      throw;
+    }
+    // compact occupied slots: (first position, slot)
+    uint64_t* keys = arena_.AllocT<uint64_t>(cap);
+    uint32_t* vals = arena_.AllocT<uint32_t>(cap);
+    uint64_t* ngroups = arena_.AllocT<uint64_t>(1);
+    ctx_.Memset(ngroups, 0, sizeof(uint64_t));
+    {
+      KernelSource ks;
+      std::string S = ks.Ptr(slots, "uint64_t", true), F = ks.Ptr(first, "uint64_t", true);
+      std::string K = ks.Ptr(keys, "uint64_t"), V = ks.Ptr(vals, "uint32_t");
+      std::string NG = ks.Ptr(ngroups, "unsigned long long");
+      std::string C = ks.Word(cap);
+      ks.Open("for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < (int64_t)" + C +
+              "; i += (int64_t)gridDim.x * blockDim.x)");
+      ks.Open("if (" + S + "[i] >= 2)");
+      ks.L("uint64_t o = kdb_alloc_slot(" + NG + ");");
+      ks.L(K + "[o] = " + F + "[i]; " + V + "[o] = (uint32_t)i;");
+      ks.Close();
+      ks.Close();
+      LaunchPipeline(ks, static_cast<int64_t>(cap), "group compact");
+    }
+    int64_t ng = ReadU64(ngroups);
+    ctx_.RadixSortPairs(keys, vals, ng, arena_, 64);
+    // output kernel
+    MatBuffer out = AllocMat(op.output, ng);
+    if (ng > 0) {
+      KernelSource ks;
+      ExprGen eg(ctx_, ks);
+      std::string S = ks.Ptr(slots, "uint64_t", true), F = ks.Ptr(first, "uint64_t", true);
+      std::string V = ks.Ptr(vals, "uint32_t", true);
+      std::string NGW = ks.Word(static_cast<uint64_t>(ng));
+      std::vector<std::string> KW(nk), KL(nk), KN(nk), SV(plans.size()), SC(plans.size());
+      if (!kl.packed)
+        for (size_t k = 0; k < nk; k++) {
+          KW[k] = ks.Ptr(kw[k], "uint64_t", true);
+          KL[k] = ks.Ptr(klen[k], "int32_t", true);
+          KN[k] = ks.Ptr(kn[k], "int8_t", true);
+        }
+      for (size_t j = 0; j < plans.size(); j++) {
+        SV[j] = ks.Ptr(sv[j], "uint64_t", true);
+        SC[j] = ks.Ptr(sc[j], "uint64_t", true);
+      }
+      std::vector<std::string> optr, onull;
+      for (const auto& c : out.cols) {
+        optr.push_back(ks.Ptr(c.data, StoreType(c.type.id)));
+        onull.push_back(c.nullable ? ks.Ptr(c.nulls, "int8_t") : "");
+      }
+      std::string posp = ks.Ptr(out.pos, "uint64_t");
+      ks.Open("for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < (int64_t)" + NGW +
+              "; r += (int64_t)gridDim.x * blockDim.x)");
+      ks.L("uint64_t i = " + V + "[r];");
+      ks.L("uint64_t fst = " + F + "[i];");
+      std::vector<CVal> virt;
+      for (size_t k = 0; k < nk; k++) {
+        const Type& t = op.group_by[k]->type;
+        if (kl.packed) {
+          uint64_t m = kl.width[k] >= 64 ? ~0ULL : ((1ULL << kl.width[k]) - 1);
+          std::string bits = "((" + S + "[i] >> " + std::to_string(kl.offset[k]) + ") & " + std::to_string(m) + "ULL)";
+          std::string v;
+          switch (t.id) {
+            case TypeId::REAL: v = "__longlong_as_double((long long)" + bits + ")"; break;
+            case TypeId::BOOLEAN: v = "(" + bits + " != 0)"; break;
+            case TypeId::SMALLINT: v = "(int16_t)(uint16_t)" + bits; break;
+            case TypeId::BIGINT: v = "(int64_t)" + bits; break;
+            default: v = "(int32_t)(uint32_t)" + bits; break;
+          }
+          std::string n = kl.nullable[k]
+                              ? "(((" + S + "[i] >> " + std::to_string(kl.offset[k] + kl.width[k]) + ") & 1ULL) != 0)"
+                              : "false";
+          virt.push_back(eg.Bind(t, v, n));
+        } else {
+          std::string w = KW[k] + "[i]";
+          std::string v;
+          switch (t.id) {
+            case TypeId::TEXT: v = "kdb_mkstr((const char*)" + w + ", " + KL[k] + "[i])"; break;
+            case TypeId::REAL: v = "__longlong_as_double((long long)" + w + ")"; break;
+            case TypeId::BOOLEAN: v = "(" + w + " != 0)"; break;
+            default: v = "(" + CType(t.id) + ")(int64_t)" + w; break;
+          }
+          virt.push_back(eg.Bind(t, v, "(" + KN[k] + "[i] != 0)"));
+        }
+      }
+      for (size_t j = 0; j < plans.size(); j++) virt.push_back(GroupResult(eg, plans[j], SV[j], SC[j], "i", "fst"));
+      Scope s;
+      s.virt = virt;
+      for (size_t c = 0; c < op.output.size(); c++) {
+        CVal v = eg.Emit(*op.output[c].expr, s);
+        std::string val = v.type.id == TypeId::BOOLEAN ? "(int8_t)(" + v.v + " ? 1 : 0)" : v.v;
+        ks.L(optr[c] + "[r] = " + val + ";");
+        if (!onull[c].empty()) ks.L(onull[c] + "[r] = (" + v.n + ") ? 1 : 0;");
+      }
+      ks.L(posp + "[r] = (uint64_t)r;");
+      ks.Close();
+      LaunchPipeline(ks, ng, "group output");
+    }
+    ctx_.CheckDeviceError("group output");
+    out.rows = ng;
+    return out;
+  }
+  throw Error(-4, "group table did not fit");
+}
+
+// ---------------------------------------------------------------------------
+// Order-by (order_by_translator.cc:35-110): materialise the child, then
+// stable radix passes -- stream order, the reference merge sort's tie key,
+// then every sort key from the least significant (NULL flag after value so
+// NULL sorts last ascending, LessThan in evaluate.cc:339-402).
+// ---------------------------------------------------------------------------
+
+MatBuffer Executor::RunOrderBy(const Operator& op) {
+  MatBuffer m = Materialize(op.child());
+  int64_t n = m.rows;
+  uint64_t* keys = arena_.AllocT<uint64_t>(std::max<int64_t>(n, 1));
+  uint32_t* idx = arena_.AllocT<uint32_t>(std::max<int64_t>(n, 1));
+  auto keygen = [&](const std::function<std::string(KernelSource&, ExprGen&, const std::string&)>& body) {
+    KernelSource ks;
+    ExprGen eg(ctx_, ks);
+    std::string K = ks.Ptr(keys, "uint64_t");
+    std::string I = ks.Ptr(idx, "uint32_t");
+    std::string N = ks.Word(static_cast<uint64_t>(n));
+    ks.Open("for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < (int64_t)" + N +
+            "; i += (int64_t)gridDim.x * blockDim.x)");
+    std::string expr = body(ks, eg, I);
+    ks.L(K + "[i] = " + expr + ";");
+    ks.Close();
+    LaunchPipeline(ks, n, "order key");
+  };
+  if (n > 1) {
+    // stream order
+    std::string dummy;
+    keygen([&](KernelSource& ks, ExprGen&, const std::string& I) {
+      std::string P = ks.Ptr(m.pos, "uint64_t", true);
+      ks.L(I + "[i] = (uint32_t)i;");
+      return P + "[i]";
+    });
+    ctx_.RadixSortPairs(keys, idx, n, arena_, 64);
+    keygen([&](KernelSource&, ExprGen&, const std::string&) {
+      return "kdb_tie_path((uint64_t)i, " + std::to_string(n) + "ULL)";
+    });
+    ctx_.RadixSortPairs(keys, idx, n, arena_, 64);
+    const auto& child_schema = SchemaOf(op.child());
+    for (int k = static_cast<int>(op.sort_keys.size()) - 1; k >= 0; k--) {
+      int col = op.sort_keys[k]->column_idx;
+      const MatCol& mc = m.cols.at(col);
+      bool asc = op.asc[k];
+      (void)child_schema;
+      const std::string inv = asc ? "" : "~";
+      auto load = [&](KernelSource& ks, ExprGen& eg, const std::string& I) {
+        std::string D = ks.Ptr(mc.data, StoreType(mc.type.id), true);
+        return std::make_pair(D + "[" + I + "[i]]", std::string());
+      };
+      if (mc.type.id == TypeId::BOOLEAN) throw Error(-1, "Can't be less than.");
+      if (mc.type.id == TypeId::TEXT) {
+        // max length over the rows decides the number of 8-byte chunks
+        uint64_t* mx = arena_.AllocT<uint64_t>(1);
+        ctx_.Memset(mx, 0, sizeof(uint64_t));
+        {
+          KernelSource ks;
+          std::string D = ks.Ptr(mc.data, "kdb_str", true), MX = ks.Ptr(mx, "unsigned long long");
+          std::string N = ks.Word(static_cast<uint64_t>(n));
+          ks.Open("for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < (int64_t)" + N +
+                  "; i += (int64_t)gridDim.x * blockDim.x)");
+          ks.L("atomicMax(" + MX + ", (unsigned long long)" + D + "[i].len);");
+          ks.Close();
+          LaunchPipeline(ks, n, "text max len");
+        }
+        int64_t maxlen = ReadU64(mx);
+        keygen([&](KernelSource& ks, ExprGen& eg, const std::string& I) {
+          return inv + "(uint64_t)" + load(ks, eg, I).first + ".len";
+        });
+        ctx_.RadixSortPairs(keys, idx, n, arena_, 64);
+        for (int64_t c = (maxlen + 7) / 8 - 1; c >= 0; c--) {
+          keygen([&](KernelSource& ks, ExprGen& eg, const std::string& I) {
+            return inv + "kdb_str_chunk(" + load(ks, eg, I).first + ", " + std::to_string(c) + ")";
+          });
+          ctx_.RadixSortPairs(keys, idx, n, arena_, 64);
+        }
+      } else {
+        keygen([&](KernelSource& ks, ExprGen& eg, const std::string& I) {
+          std::string v = load(ks, eg, I).first;
+          std::string norm;
+          switch (mc.type.id) {
+            case TypeId::REAL: norm = "kdb_dord(" + v + ")"; break;
+            case TypeId::ENUM: norm = "(uint64_t)(uint32_t)" + eg.EnumRank(mc.type, v); break;
+            default: norm = "((uint64_t)(int64_t)" + v + " ^ 0x8000000000000000ULL)"; break;
+          }
+          return inv + "(" + norm + ")";
+        });
+        ctx_.RadixSortPairs(keys, idx, n, arena_, 64);
+      }
+      if (mc.nullable) {
+        keygen([&](KernelSource& ks, ExprGen&, const std::string& I) {
+          std::string NP = ks.Ptr(mc.nulls, "int8_t", true);
+          std::string isnull = "(uint64_t)(" + NP + "[" + I + "[i]] != 0)";
+          return asc ? isnull : "(1ULL - " + isnull + ")";
+        });
+        ctx_.RadixSortPairs(keys, idx, n, arena_, 8);
+      }
+    }
+  } else if (n == 1) {
+    ctx_.Memset(idx, 0, sizeof(uint32_t));
+  }
+  return MaterializeStream(op, idx, &m);
+}
+
+// ---------------------------------------------------------------------------
+// Result download (runtime/printer.cc formats it on the host)
+// ---------------------------------------------------------------------------
+
+HostResult Executor::Run(const Operator& root) {
+  MatBuffer m = Materialize(root);
+  const auto& schema = SchemaOf(root);
+  HostResult res;
+  res.rows = m.rows;
+  for (size_t c = 0; c < m.cols.size(); c++) {
+    const MatCol& mc = m.cols[c];
+    HostColumn hc;
+    hc.name = schema[c].name;
+    hc.type = mc.type;
+    hc.null.assign(m.rows, 0);
+    if (mc.nulls && m.rows) ctx_.D2H(hc.null.data(), mc.nulls, m.rows);
+    size_t w = StoreWidth(mc.type.id);
+    std::vector<char> raw(w * m.rows);
+    if (m.rows) ctx_.D2H(raw.data(), mc.data, raw.size());
+    switch (mc.type.id) {
+      case TypeId::REAL: {
+        hc.f.resize(m.rows);
+        std::memcpy(hc.f.data(), raw.data(), raw.size());
+        break;
+      }
+      case TypeId::TEXT: {
+        const DevStr* ds = reinterpret_cast<const DevStr*>(raw.data());
+        std::vector<int64_t> off(m.rows + 1, 0);
+        for (int64_t r = 0; r < m.rows; r++) off[r + 1] = off[r] + (hc.null[r] ? 0 : ds[r].len);
+        int64_t total = off[m.rows];
+        hc.s.resize(m.rows);
+        if (total > 0) {
+          int64_t* d_off = arena_.AllocT<int64_t>(m.rows + 1);
+          char* d_chars = arena_.AllocT<char>(total);
+          ctx_.H2D(d_off, off.data(), sizeof(int64_t) * (m.rows + 1));
+          KernelSource ks;
+          std::string D = ks.Ptr(mc.data, "kdb_str", true), O = ks.Ptr(d_off, "int64_t", true);
+          std::string CH = ks.Ptr(d_chars, "char");
+          std::string N = ks.Word(static_cast<uint64_t>(m.rows));
+          ks.Open("for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < (int64_t)" + N +
+                  "; r += (int64_t)gridDim.x * blockDim.x)");
+          ks.L("int64_t len = " + O + "[r + 1] - " + O + "[r];");
+          ks.L("for (int64_t b = 0; b < len; b++) " + CH + "[" + O + "[r] + b] = " + D + "[r].p[b];");
+          ks.Close();
+          LaunchPipeline(ks, m.rows, "text download");
+          std::vector<char> chars(total);
+          ctx_.D2H(chars.data(), d_chars, total);
+          for (int64_t r = 0; r < m.rows; r++) hc.s[r].assign(chars.data() + off[r], off[r + 1] - off[r]);
+        }
+        break;
+      }
+      default: {
+        hc.i.resize(m.rows);
+        for (int64_t r = 0; r < m.rows; r++) {
+          const char* p = raw.data() + w * r;
+          switch (mc.type.id) {
+            case TypeId::BOOLEAN: hc.i[r] = *reinterpret_cast<const int8_t*>(p); break;
+            case TypeId::SMALLINT: hc.i[r] = *reinterpret_cast<const int16_t*>(p); break;
+            case TypeId::BIGINT: hc.i[r] = *reinterpret_cast<const int64_t*>(p); break;
+            default: hc.i[r] = *reinterpret_cast<const int32_t*>(p); break;
+          }
+        }
+        break;
+      }
+    }
+    res.cols.push_back(std::move(hc));
+  }
+  return res;
+}
+
+}  // namespace
+
+HostResult ExecutePlan(Context& ctx, const plan::Operator& root) {
+  Arena arena(ctx);
+  Executor ex(ctx, arena);
+  if (ctx.dry) return ex.Run(root);
+  ctx.BeginQueryProfile();
+  cudaEvent_t e0, e1;
+  KDB_CUDA(cudaEventCreate(&e0));
+  KDB_CUDA(cudaEventCreate(&e1));
+  KDB_CUDA(cudaEventRecord(e0, ctx.stream));
+  HostResult r;
+  try {
+    r = ex.Run(root);
+  } catch (...) {
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    cudaStreamSynchronize(ctx.stream);
+    throw;
+  }
+  KDB_CUDA(cudaEventRecord(e1, ctx.stream));
+  KDB_CUDA(cudaEventSynchronize(e1));
+  float ms = 0;
+  KDB_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+  ctx.last_device_ms = ms;
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  ctx.EndQueryProfile();
+  return r;
+}
+
+}  // namespace kdb

@@ -1,0 +1,416 @@
+// Context: device residency of columns and enums, the NVRTC pipeline cache
+// and kernel launch plumbing.
+#include "engine.h"
+
+#include <nvrtc.h>
+
+#include <algorithm>
+#include <cstdlib>
+#include <cstring>
+#include <fstream>
+#include <numeric>
+#include <sstream>
+
+namespace kdb {
+
+namespace {
+
+const char* kDeviceRuntime =
+#include "device_runtime.inc"
+    ;
+
+// Driver API entry points, resolved through the runtime so the library does
+// not link libcuda directly (it must load on machines without a driver).
+struct Driver {
+  CUresult (*ModuleLoadData)(CUmodule*, const void*) = nullptr;
+  CUresult (*ModuleGetFunction)(CUfunction*, CUmodule, const char*) = nullptr;
+  CUresult (*LaunchKernel)(CUfunction, unsigned, unsigned, unsigned, unsigned, unsigned, unsigned,
+                           unsigned, CUstream, void**, void**) = nullptr;
+  CUresult (*ModuleUnload)(CUmodule) = nullptr;
+  CUresult (*FuncSetAttribute)(CUfunction, CUfunction_attribute, int) = nullptr;
+  bool loaded = false;
+
+  template <typename F>
+  void Get(const char* name, F& fn) {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    KDB_CUDA(cudaGetDriverEntryPoint(name, &p, cudaEnableDefault, &q));
+    if (!p || q != cudaDriverEntryPointSuccess)
+      throw Error(-2, std::string("driver entry point missing: ") + name);
+    fn = reinterpret_cast<F>(p);
+  }
+  void Load() {
+    if (loaded) return;
+    Get("cuModuleLoadData", ModuleLoadData);
+    Get("cuModuleGetFunction", ModuleGetFunction);
+    Get("cuLaunchKernel", LaunchKernel);
+    Get("cuModuleUnload", ModuleUnload);
+    Get("cuFuncSetAttribute", FuncSetAttribute);
+    loaded = true;
+  }
+};
+Driver g_drv;
+
+void CuCheck(CUresult r, const char* what) {
+  if (r != CUDA_SUCCESS) throw Error(-2, std::string(what) + " failed (CUresult " + std::to_string(r) + ")");
+}
+
+void NvrtcCheck(nvrtcResult r, const char* what) {
+  if (r != NVRTC_SUCCESS) throw Error(-3, std::string(what) + ": " + nvrtcGetErrorString(r));
+}
+
+}  // namespace
+
+void CudaCheck(cudaError_t e, const char* what) {
+  if (e != cudaSuccess) throw Error(-2, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+// ---------------------------------------------------------------------------
+// Arena
+// ---------------------------------------------------------------------------
+
+Arena::~Arena() {
+  if (ctx_.dry) return;
+  for (void* p : ptrs_) cudaFreeAsync(p, ctx_.stream);
+}
+
+void* Arena::Alloc(size_t bytes) {
+  if (bytes == 0) bytes = 16;
+  if (ctx_.dry) return ctx_.DevAlloc(bytes);
+  void* p = nullptr;
+  KDB_CUDA(cudaMallocAsync(&p, bytes, ctx_.stream));
+  ptrs_.push_back(p);
+  return p;
+}
+
+namespace {
+uint64_t g_fake_next = 0x7f0000000000ULL;
+}
+
+void* Context::DevAlloc(size_t bytes) {
+  if (dry) {
+    void* p = reinterpret_cast<void*>(g_fake_next);
+    g_fake_next += (bytes + 255) & ~size_t(255);
+    return p;
+  }
+  void* p = nullptr;
+  KDB_CUDA(cudaMalloc(&p, std::max<size_t>(bytes, 16)));
+  return p;
+}
+
+void Context::DevFree(void* p) {
+  if (!dry && p) cudaFree(p);
+}
+
+void Context::Memset(void* d, int v, size_t bytes) {
+  if (!dry && bytes) KDB_CUDA(cudaMemsetAsync(d, v, bytes, stream));
+}
+
+void Context::H2D(void* d, const void* h, size_t bytes) {
+  if (!dry && bytes) KDB_CUDA(cudaMemcpyAsync(d, h, bytes, cudaMemcpyHostToDevice, stream));
+}
+
+void Context::D2H(void* h, const void* d, size_t bytes) {
+  if (dry) {
+    std::memset(h, 0, bytes);
+    return;
+  }
+  if (bytes) KDB_CUDA(cudaMemcpyAsync(h, d, bytes, cudaMemcpyDeviceToHost, stream));
+  KDB_CUDA(cudaStreamSynchronize(stream));
+}
+
+// ---------------------------------------------------------------------------
+// Context
+// ---------------------------------------------------------------------------
+
+Context::Context(int dev) : device(dev) {
+  if (dev < 0) {
+    dry = true;
+    d_err = static_cast<int*>(DevAlloc(16));
+    return;
+  }
+  KDB_CUDA(cudaSetDevice(dev));
+  KDB_CUDA(cudaFree(nullptr));
+  KDB_CUDA(cudaDeviceGetAttribute(&num_sms, cudaDevAttrMultiProcessorCount, dev));
+  KDB_CUDA(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
+  // keep freed stream-ordered memory in the pool between queries
+  cudaMemPool_t pool;
+  KDB_CUDA(cudaDeviceGetDefaultMemPool(&pool, dev));
+  uint64_t threshold = UINT64_MAX;
+  KDB_CUDA(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &threshold));
+  KDB_CUDA(cudaMalloc(&d_err, sizeof(int) * 4));
+  KDB_CUDA(cudaMemset(d_err, 0, sizeof(int) * 4));
+  g_drv.Load();
+}
+
+Context::~Context() {
+  if (dry) return;
+  cudaSetDevice(device);
+  cudaStreamSynchronize(stream);
+  for (auto& [n, t] : tables)
+    for (auto& [cn, c] : t.cols) FreeColumn(c);
+  for (auto& [id, e] : enums) {
+    cudaFree(e.d_off);
+    cudaFree(e.d_chars);
+    cudaFree(e.d_rank);
+  }
+  for (auto& [k, p] : programs_)
+    if (p->module) g_drv.ModuleUnload(p->module);
+  cudaFree(d_err);
+  cudaStreamDestroy(stream);
+}
+
+void Context::FreeColumn(DevColumn& c) {
+  DevFree(c.data);
+  DevFree(c.toff);
+  DevFree(c.tchars);
+  DevFree(c.nulls);
+  c = DevColumn();
+}
+
+static void CheckRows(DevTable& t, int64_t n, const std::string& name) {
+  if (t.rows >= 0 && t.rows != n)
+    throw Error(-1, "column " + name + " has " + std::to_string(n) + " rows, table has " +
+                        std::to_string(t.rows));
+  t.rows = n;
+}
+
+void Context::AddColumn(const std::string& table, const std::string& column, const plan::Type& type,
+                        const void* data, int64_t n, const int8_t* nulls) {
+  if (type.id == plan::TypeId::TEXT) throw Error(-1, "TEXT columns use kdb_table_add_text_column");
+  if (n < 0) throw Error(-1, "negative row count");
+  DevTable& t = tables[table];
+  CheckRows(t, n, column);
+  auto it = t.cols.find(column);
+  if (it != t.cols.end()) FreeColumn(it->second);
+  DevColumn c;
+  c.type = type;
+  c.n = n;
+  size_t w = plan::TypeWidth(type.id);
+  c.bytes = w * n;
+  c.data = DevAlloc(std::max<size_t>(c.bytes, 16));
+  H2D(c.data, data, c.bytes);
+  if (nulls) {
+    c.nulls = static_cast<int8_t*>(DevAlloc(std::max<int64_t>(n, 16)));
+    H2D(c.nulls, nulls, n);
+    c.bytes += n;
+  }
+  if (!dry) KDB_CUDA(cudaStreamSynchronize(stream));
+  t.cols[column] = c;
+}
+
+void Context::AddTextColumn(const std::string& table, const std::string& column,
+                            const int64_t* offsets, const char* chars, int64_t n,
+                            const int8_t* nulls) {
+  if (n < 0) throw Error(-1, "negative row count");
+  DevTable& t = tables[table];
+  CheckRows(t, n, column);
+  auto it = t.cols.find(column);
+  if (it != t.cols.end()) FreeColumn(it->second);
+  DevColumn c;
+  c.type = plan::Type{plan::TypeId::TEXT, 0};
+  c.n = n;
+  int64_t nbytes = offsets[n] - offsets[0];
+  std::vector<int64_t> off(offsets, offsets + n + 1);
+  int64_t base = off[0];
+  for (auto& o : off) o -= base;
+  for (int64_t r = 0; r < n; r++)
+    c.max_text_len = std::max<int32_t>(c.max_text_len, static_cast<int32_t>(off[r + 1] - off[r]));
+  c.toff = static_cast<int64_t*>(DevAlloc(sizeof(int64_t) * (n + 1)));
+  H2D(c.toff, off.data(), sizeof(int64_t) * (n + 1));
+  c.tchars = static_cast<char*>(DevAlloc(std::max<int64_t>(nbytes, 16)));
+  H2D(c.tchars, chars + base, nbytes);
+  c.bytes = sizeof(int64_t) * (n + 1) + nbytes;
+  if (nulls) {
+    c.nulls = static_cast<int8_t*>(DevAlloc(std::max<int64_t>(n, 16)));
+    H2D(c.nulls, nulls, n);
+    c.bytes += n;
+  }
+  if (!dry) KDB_CUDA(cudaStreamSynchronize(stream));
+  t.cols[column] = c;
+}
+
+void Context::DropTable(const std::string& table) {
+  auto it = tables.find(table);
+  if (it == tables.end()) return;
+  if (!dry) KDB_CUDA(cudaStreamSynchronize(stream));
+  for (auto& [n, c] : it->second.cols) FreeColumn(c);
+  tables.erase(it);
+}
+
+void Context::RegisterEnum(int32_t id, std::vector<std::string> values) {
+  auto it = enums.find(id);
+  if (it != enums.end()) {
+    if (it->second.values == values) return;
+    DevFree(it->second.d_off);
+    DevFree(it->second.d_chars);
+    DevFree(it->second.d_rank);
+    enums.erase(it);
+  }
+  DevEnum e;
+  e.values = std::move(values);
+  int32_t n = static_cast<int32_t>(e.values.size());
+  std::vector<int64_t> off(n + 1, 0);
+  std::string chars;
+  for (int32_t k = 0; k < n; k++) {
+    chars += e.values[k];
+    off[k + 1] = static_cast<int64_t>(chars.size());
+  }
+  std::vector<int32_t> order(n);
+  std::iota(order.begin(), order.end(), 0);
+  std::stable_sort(order.begin(), order.end(),
+                   [&](int32_t a, int32_t b) { return e.values[a] < e.values[b]; });
+  e.rank.assign(n, 0);
+  for (int32_t r = 0; r < n; r++) e.rank[order[r]] = r;
+  e.d_off = static_cast<int64_t*>(DevAlloc(sizeof(int64_t) * (n + 1)));
+  H2D(e.d_off, off.data(), sizeof(int64_t) * (n + 1));
+  e.d_chars = static_cast<char*>(DevAlloc(std::max<size_t>(chars.size(), 16)));
+  H2D(e.d_chars, chars.data(), chars.size());
+  e.d_rank = static_cast<int32_t*>(DevAlloc(sizeof(int32_t) * std::max(n, 1)));
+  H2D(e.d_rank, e.rank.data(), sizeof(int32_t) * n);
+  if (!dry) KDB_CUDA(cudaStreamSynchronize(stream));
+  enums[id] = std::move(e);
+}
+
+int64_t Context::ColumnBytes() const {
+  int64_t b = 0;
+  for (auto& [n, t] : tables)
+    for (auto& [cn, c] : t.cols) b += static_cast<int64_t>(c.bytes);
+  return b;
+}
+
+const DevColumn& Context::Column(const std::string& table, const std::string& column) const {
+  auto t = tables.find(table);
+  if (t == tables.end()) throw Error(-1, "unknown relation " + table);
+  auto c = t->second.cols.find(column);
+  if (c == t->second.cols.end()) throw Error(-1, "unknown column " + table + "." + column);
+  return c->second;
+}
+
+const DevEnum& Context::Enum(int32_t id) const {
+  auto it = enums.find(id);
+  if (it == enums.end()) throw Error(-1, "enum " + std::to_string(id) + " not registered");
+  return it->second;
+}
+
+EnumDicts Context::HostEnums() const {
+  EnumDicts d;
+  for (auto& [id, e] : enums) d[id] = e.values;
+  return d;
+}
+
+CUfunction Context::Kernel(const std::string& source, const std::string& name) {
+  auto it = programs_.find(source);
+  if (it == programs_.end()) {
+    auto prog = std::make_unique<Program>();
+    std::string full = std::string(kDeviceRuntime) + "\n" + source;
+    nvrtcProgram p;
+    NvrtcCheck(nvrtcCreateProgram(&p, full.c_str(), "kdb_pipeline.cu", 0, nullptr, nullptr),
+               "nvrtcCreateProgram");
+    const char* opts[] = {"--gpu-architecture=sm_100a", "--std=c++17", "--fmad=false",
+                          "-lineinfo", "-DNDEBUG"};
+    nvrtcResult cr = nvrtcCompileProgram(p, 5, opts);
+    size_t log_size = 0;
+    nvrtcGetProgramLogSize(p, &log_size);
+    std::string log(log_size, '\0');
+    if (log_size) nvrtcGetProgramLog(p, &log[0]);
+    if (cr != NVRTC_SUCCESS) {
+      nvrtcDestroyProgram(&p);
+      if (const char* dump = std::getenv("KDB_DUMP_FAILED_SOURCE")) {
+        std::ofstream(dump) << full;
+      }
+      throw Error(-3, "NVRTC compile failed: " + log.substr(0, 4000));
+    }
+    size_t cubin_size = 0;
+    NvrtcCheck(nvrtcGetCUBINSize(p, &cubin_size), "nvrtcGetCUBINSize");
+    std::vector<char> cubin(cubin_size);
+    NvrtcCheck(nvrtcGetCUBIN(p, cubin.data()), "nvrtcGetCUBIN");
+    nvrtcDestroyProgram(&p);
+    if (!dry) CuCheck(g_drv.ModuleLoadData(&prog->module, cubin.data()), "cuModuleLoadData");
+    prog->log = log;
+    it = programs_.emplace(source, std::move(prog)).first;
+  }
+  Program& prog = *it->second;
+  if (dry) return nullptr;
+  auto f = prog.fns.find(name);
+  if (f == prog.fns.end()) {
+    CUfunction fn;
+    CuCheck(g_drv.ModuleGetFunction(&fn, prog.module, name.c_str()), "cuModuleGetFunction");
+    f = prog.fns.emplace(name, fn).first;
+  }
+  return f->second;
+}
+
+int Context::GridFor(int64_t n, int block) const {
+  int64_t want = (n + block - 1) / block;
+  int64_t cap = static_cast<int64_t>(num_sms) * (2048 / block);
+  return static_cast<int>(std::max<int64_t>(1, std::min(want, cap)));
+}
+
+void Context::Launch(CUfunction f, int grid, int block, const KArgs& args, size_t smem,
+                     const char* tag) {
+  kernel_launches++;
+  if (dry) return;
+  void* params[] = {const_cast<KArgs*>(&args)};
+  if (smem > 48 * 1024)
+    CuCheck(g_drv.FuncSetAttribute(f, CU_FUNC_ATTRIBUTE_MAX_DYNAMIC_SHARED_SIZE_BYTES,
+                                   static_cast<int>(smem)),
+            "cuFuncSetAttribute");
+  TimedStart(tag);
+  CuCheck(g_drv.LaunchKernel(f, grid, 1, 1, block, 1, 1, static_cast<unsigned>(smem),
+                             reinterpret_cast<CUstream>(stream), params, nullptr),
+          "cuLaunchKernel");
+  TimedStop();
+}
+
+void Context::TimedStart(const char* tag) {
+  if (!profile || dry) return;
+  LaunchTiming t;
+  t.tag = tag;
+  KDB_CUDA(cudaEventCreate(&t.start));
+  KDB_CUDA(cudaEventCreate(&t.stop));
+  KDB_CUDA(cudaEventRecord(t.start, stream));
+  timings.push_back(t);
+}
+
+void Context::TimedStop() {
+  if (!profile || dry || timings.empty()) return;
+  KDB_CUDA(cudaEventRecord(timings.back().stop, stream));
+}
+
+void Context::BeginQueryProfile() {
+  for (auto& t : timings) {
+    cudaEventDestroy(t.start);
+    cudaEventDestroy(t.stop);
+  }
+  timings.clear();
+}
+
+void Context::EndQueryProfile() {
+  last_kernels.clear();
+  if (!profile || dry) return;
+  KDB_CUDA(cudaStreamSynchronize(stream));
+  for (auto& t : timings) {
+    float ms = 0;
+    KDB_CUDA(cudaEventElapsedTime(&ms, t.start, t.stop));
+    last_kernels.emplace_back(t.tag, ms);
+    cudaEventDestroy(t.start);
+    cudaEventDestroy(t.stop);
+  }
+  timings.clear();
+}
+
+void Context::CheckDeviceError(const char* what) {
+  if (dry) return;
+  int err[4] = {0, 0, 0, 0};
+  KDB_CUDA(cudaMemcpyAsync(err, d_err, sizeof(err), cudaMemcpyDeviceToHost, stream));
+  KDB_CUDA(cudaStreamSynchronize(stream));
+  if (err[0]) {
+    KDB_CUDA(cudaMemsetAsync(d_err, 0, sizeof(int) * 4, stream));
+    if (err[0] == 1) throw Error(-4, std::string(what) + ": device table capacity exceeded");
+    if (err[0] == 2) throw Error(-6, std::string(what) + ": bounded device wait gave up");
+    throw Error(-5, std::string(what) + ": unsupported value on device");
+  }
+}
+
+}  // namespace kdb

@@ -1,0 +1,188 @@
+// Host-side engine: device-resident tables, compiled-pipeline cache, and the
+// plan executor that turns plan::Operator trees into device pipelines.
+//
+// Replaces, for the hot path, the reference's compile + execution layers
+// (compile/query_translator.cc:16-34, execution/executable_query.cc:199-255)
+// and the runtime structures its generated code calls per tuple
+// (runtime/column_data, hash_table, aggregate_hash_table, vector).
+#pragma once
+
+#include <cuda.h>
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <map>
+#include <memory>
+#include <stdexcept>
+#include <string>
+#include <unordered_map>
+#include <vector>
+
+#include "host_result.h"
+#include "plan.h"
+
+namespace kdb {
+
+// Error with a KDB_ERR_* code.
+struct Error : std::runtime_error {
+  int code;
+  Error(int c, const std::string& m) : std::runtime_error(m), code(c) {}
+};
+
+void CudaCheck(cudaError_t e, const char* what);
+#define KDB_CUDA(x) ::kdb::CudaCheck((x), #x)
+
+// A TEXT value in a materialised buffer (same layout as device kdb_str).
+struct DevStr {
+  const char* p;
+  int32_t len;
+  int32_t pad;
+};
+static_assert(sizeof(DevStr) == 16, "DevStr layout");
+
+// One HBM-resident base-table column (runtime::ColumnData equivalent).
+struct DevColumn {
+  plan::Type type;
+  int64_t n = 0;
+  void* data = nullptr;      // fixed width values
+  int64_t* toff = nullptr;   // TEXT: offsets[n+1]
+  char* tchars = nullptr;    // TEXT: bytes
+  int8_t* nulls = nullptr;   // optional NULL flags
+  size_t bytes = 0;
+  int32_t max_text_len = 0;
+};
+
+struct DevTable {
+  std::map<std::string, DevColumn> cols;
+  int64_t rows = -1;
+};
+
+// Enum dictionary mirrored on the device; `rank[k]` is key k's position in
+// string order, so ORDER BY / MIN / MAX / < on enums compare ranks
+// (compile/proxy/aggregator.cc:163-171, evaluate.cc:203-250).
+struct DevEnum {
+  std::vector<std::string> values;
+  int64_t* d_off = nullptr;
+  char* d_chars = nullptr;
+  int32_t* d_rank = nullptr;
+  std::vector<int32_t> rank;
+};
+
+// A materialised intermediate: columnar, device resident.  TEXT columns
+// hold DevStr (pointers into base columns or kernel literals).
+struct MatCol {
+  plan::Type type;
+  bool nullable = false;
+  void* data = nullptr;
+  int8_t* nulls = nullptr;
+};
+
+struct MatBuffer {
+  std::vector<MatCol> cols;
+  uint64_t* pos = nullptr;   // stream position of each row (reference emission order key)
+  int64_t rows = 0;
+  int64_t cap = 0;
+};
+
+// A compiled pipeline program (one CUDA module from NVRTC).
+struct Program {
+  CUmodule module = nullptr;
+  std::map<std::string, CUfunction> fns;
+  std::string log;
+};
+
+// Host mirror of the device KArgs struct (passed by value).
+struct KArgs {
+  uint64_t w[384];
+};
+
+class Context;
+
+// Stream-ordered device allocations owned by one query execution.
+class Arena {
+ public:
+  explicit Arena(Context& ctx) : ctx_(ctx) {}
+  ~Arena();
+  void* Alloc(size_t bytes);
+  template <typename T>
+  T* AllocT(size_t count) {
+    return static_cast<T*>(Alloc(count * sizeof(T) + 16));
+  }
+
+ private:
+  Context& ctx_;
+  std::vector<void*> ptrs_;
+};
+
+class Context {
+ public:
+  // device < 0: compile-only context (no GPU needed): every pipeline is
+  // generated and compiled by NVRTC, nothing is allocated, copied or run,
+  // and device reads return zeros.
+  explicit Context(int device);
+  ~Context();
+
+  int device = 0;
+  bool dry = false;
+  int num_sms = 148;
+  cudaStream_t stream = nullptr;
+  std::map<std::string, DevTable> tables;
+  std::map<int32_t, DevEnum> enums;
+  std::string last_error;
+  int64_t kernel_launches = 0;
+  double last_device_ms = 0;
+
+  // device error word shared by all launches of a query
+  int* d_err = nullptr;
+
+  void AddColumn(const std::string& table, const std::string& column, const plan::Type& type,
+                 const void* data, int64_t n, const int8_t* nulls);
+  void AddTextColumn(const std::string& table, const std::string& column, const int64_t* offsets,
+                     const char* chars, int64_t n, const int8_t* nulls);
+  void DropTable(const std::string& table);
+  void RegisterEnum(int32_t id, std::vector<std::string> values);
+  int64_t ColumnBytes() const;
+
+  const DevColumn& Column(const std::string& table, const std::string& column) const;
+  const DevEnum& Enum(int32_t id) const;
+
+  // NVRTC compile (cached by source text) and kernel lookup.
+  CUfunction Kernel(const std::string& source, const std::string& name);
+  void Launch(CUfunction f, int grid, int block, const KArgs& args, size_t smem = 0,
+              const char* tag = "pipeline");
+  // Per-launch CUDA-event timing (enabled by kdb_ctx_set_profiling).
+  bool profile = false;
+  struct LaunchTiming {
+    std::string tag;
+    cudaEvent_t start, stop;
+  };
+  std::vector<LaunchTiming> timings;
+  std::vector<std::pair<std::string, float>> last_kernels;
+  void BeginQueryProfile();
+  void EndQueryProfile();
+  void TimedStart(const char* tag);
+  void TimedStop();
+  int GridFor(int64_t n, int block) const;
+
+  // Device memory / copies that honour the compile-only mode.
+  void* DevAlloc(size_t bytes);
+  void DevFree(void* p);
+  void Memset(void* d, int v, size_t bytes);
+  void H2D(void* d, const void* h, size_t bytes);
+  void D2H(void* h, const void* d, size_t bytes);  // synchronous
+
+  // Static kernels (kernels.cu).
+  void RadixSortPairs(uint64_t* keys, uint32_t* vals, int64_t n, Arena& arena, int key_bits = 64);
+  void CheckDeviceError(const char* what);
+
+  EnumDicts HostEnums() const;
+
+ private:
+  std::unordered_map<std::string, std::unique_ptr<Program>> programs_;
+  void FreeColumn(DevColumn& c);
+};
+
+// Runs a plan on the device and returns the host result.
+HostResult ExecutePlan(Context& ctx, const plan::Operator& root);
+
+}  // namespace kdb

@@ -1,0 +1,180 @@
+"""Python host API over the C ABI (include/kdb_b200.h).
+
+``Engine`` owns one ``kdb_ctx``: tables registered with it stay resident in
+HBM (runtime::ColumnData replaced by device columns) and plans built with
+``kushdb_b200.plan`` run as generated sm_100a pipelines.  There is no CPU
+fallback: without the compiled library or a GPU the calls raise.
+"""
+
+from __future__ import annotations
+
+import ctypes
+import os
+from typing import Dict, Optional
+
+import numpy as np
+
+from .data import HostTable
+from .plan import EnumRegistry, Operator
+from .result import Result, declare_result_api
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libkdb_b200.so")
+
+# every symbol include/kdb_b200.h declares
+EXPORTS = [
+    "kdb_ctx_create", "kdb_ctx_destroy", "kdb_last_error", "kdb_ctx_kernel_launches",
+    "kdb_ctx_column_bytes", "kdb_ctx_stream", "kdb_ctx_set_profiling", "kdb_last_query_kernels", "kdb_table_add_column", "kdb_table_add_text_column",
+    "kdb_column_open_kdb", "kdb_table_drop", "kdb_table_num_rows", "kdb_enum_register",
+    "kdb_enum_open_kdbenum", "kdb_query_execute", "kdb_last_query_device_ms",
+    "kdb_result_num_rows", "kdb_result_num_cols", "kdb_result_col_type", "kdb_result_get_i64",
+    "kdb_result_get_f64", "kdb_result_get_nulls", "kdb_result_get_text", "kdb_result_format",
+    "kdb_result_free",
+]
+
+_lib = None
+
+
+class KdbError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"[{code}] {msg}")
+        self.code = code
+
+
+def load_library(path: str = LIB_PATH):
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise FileNotFoundError(
+            f"{path} is missing: build it with `python kushdb_b200/build.py` (no CPU fallback)")
+    L = ctypes.CDLL(path)
+    P, I32, I64 = ctypes.c_void_p, ctypes.c_int32, ctypes.c_int64
+    L.kdb_ctx_create.argtypes = [ctypes.c_int, ctypes.POINTER(P)]
+    L.kdb_ctx_destroy.argtypes = [P]
+    L.kdb_last_error.restype = ctypes.c_char_p
+    L.kdb_last_error.argtypes = [P]
+    L.kdb_ctx_kernel_launches.restype = I64
+    L.kdb_ctx_kernel_launches.argtypes = [P]
+    L.kdb_ctx_column_bytes.restype = I64
+    L.kdb_ctx_column_bytes.argtypes = [P]
+    L.kdb_ctx_stream.restype = P
+    L.kdb_ctx_stream.argtypes = [P]
+    L.kdb_ctx_set_profiling.argtypes = [P, ctypes.c_int]
+    L.kdb_last_query_kernels.restype = I64
+    L.kdb_last_query_kernels.argtypes = [P, ctypes.c_char_p, I64]
+    L.kdb_table_add_column.argtypes = [P, ctypes.c_char_p, ctypes.c_char_p, ctypes.c_char_p, P, I64, P]
+    L.kdb_table_add_text_column.argtypes = [P, ctypes.c_char_p, ctypes.c_char_p, P, P, I64, P]
+    L.kdb_column_open_kdb.argtypes = [P, ctypes.c_char_p, ctypes.c_char_p, ctypes.c_char_p,
+                                      ctypes.c_char_p, ctypes.c_char_p]
+    L.kdb_table_drop.argtypes = [P, ctypes.c_char_p]
+    L.kdb_table_num_rows.restype = I64
+    L.kdb_table_num_rows.argtypes = [P, ctypes.c_char_p]
+    L.kdb_enum_register.argtypes = [P, I32, P, P, I32]
+    L.kdb_enum_open_kdbenum.argtypes = [P, I32, ctypes.c_char_p]
+    L.kdb_query_execute.argtypes = [P, ctypes.c_char_p, ctypes.POINTER(P)]
+    L.kdb_last_query_device_ms.restype = ctypes.c_double
+    L.kdb_last_query_device_ms.argtypes = [P]
+    declare_result_api(L, "kdb_")
+    _lib = L
+    return L
+
+
+def _ptr(a):
+    return None if a is None else a.ctypes.data_as(ctypes.c_void_p)
+
+
+class Engine:
+    """One device context.  ``device=-1`` makes a compile-only context: every
+    pipeline is generated and compiled by NVRTC but nothing runs (no GPU
+    needed); results are then empty."""
+
+    def __init__(self, device: int = 0):
+        self.lib = load_library()
+        h = ctypes.c_void_p()
+        rc = self.lib.kdb_ctx_create(device, ctypes.byref(h))
+        if rc != 0:
+            raise KdbError(rc, f"kdb_ctx_create({device}) failed (no CUDA device?)")
+        self.ctx = h
+        self.device = device
+        self._enums_sent: Dict[int, int] = {}
+
+    def close(self):
+        if self.ctx:
+            self.lib.kdb_ctx_destroy(self.ctx)
+            self.ctx = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def _check(self, rc):
+        if rc != 0:
+            raise KdbError(rc, self.lib.kdb_last_error(self.ctx).decode())
+
+    def register_enums(self) -> None:
+        for k, vals in EnumRegistry.all().items():
+            if self._enums_sent.get(k) == id(vals) and False:
+                continue
+            enc = [v.encode() for v in vals]
+            off = np.zeros(len(enc) + 1, np.int64)
+            off[1:] = np.cumsum([len(b) for b in enc])
+            chars = np.frombuffer(b"".join(enc) or b"\0", np.uint8)
+            self._check(self.lib.kdb_enum_register(self.ctx, k, _ptr(off), _ptr(chars), len(enc)))
+
+    def register_table(self, table: HostTable, name: Optional[str] = None) -> None:
+        name = (name or table.name).encode()
+        for c in table.columns.values():
+            nulls = None if c.nulls is None else np.ascontiguousarray(c.nulls, np.int8)
+            if c.type.type_id == "TEXT":
+                off = np.ascontiguousarray(c.offsets, np.int64)
+                chars = np.ascontiguousarray(c.chars, np.uint8)
+                if chars.size == 0:
+                    chars = np.zeros(1, np.uint8)
+                self._check(self.lib.kdb_table_add_text_column(
+                    self.ctx, name, c.name.encode(), _ptr(off), _ptr(chars), len(off) - 1, _ptr(nulls)))
+            else:
+                v = np.ascontiguousarray(c.values)
+                self._check(self.lib.kdb_table_add_column(
+                    self.ctx, name, c.name.encode(), c.type.to_json().encode(), _ptr(v), len(v),
+                    _ptr(nulls)))
+
+    def drop_table(self, name: str) -> None:
+        self._check(self.lib.kdb_table_drop(self.ctx, name.encode()))
+
+    def execute(self, plan) -> Result:
+        text = plan.to_json() if isinstance(plan, Operator) else plan
+        self.register_enums()
+        h = ctypes.c_void_p()
+        self._check(self.lib.kdb_query_execute(self.ctx, text.encode(), ctypes.byref(h)))
+        try:
+            return Result.from_handle(self.lib, "kdb_", self.ctx, h)
+        finally:
+            self.lib.kdb_result_free(h)
+
+    def last_device_ms(self) -> float:
+        return self.lib.kdb_last_query_device_ms(self.ctx)
+
+    def kernel_launches(self) -> int:
+        return self.lib.kdb_ctx_kernel_launches(self.ctx)
+
+    def stream_handle(self) -> int:
+        return self.lib.kdb_ctx_stream(self.ctx) or 0
+
+    def set_profiling(self, on: bool) -> None:
+        self._check(self.lib.kdb_ctx_set_profiling(self.ctx, 1 if on else 0))
+
+    def last_kernels(self):
+        import json
+        n = self.lib.kdb_last_query_kernels(self.ctx, None, 0)
+        buf = ctypes.create_string_buffer(int(n))
+        self.lib.kdb_last_query_kernels(self.ctx, buf, n)
+        return json.loads(buf.value.decode())
