@@ -125,52 +125,56 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
-def cpu_baseline(name: str, steps: int = 1):
-    """Times the oracle (CPU restatement of the reference's generated code,
-    one thread) on a bounded sample of the same workload."""
-    from oracle import Oracle
-    scale = {"scan_agg": 1.0, "group_by": 0.1, "join_group": 0.1}[name]
-    tables, plan, rows, _, _, cfg = make_workload(name, scale)
-    o = Oracle()
-    for t in tables:
-        o.register_table(t)
-    o.execute(plan)
-    secs = []
-    for _ in range(steps):
-        o.execute(plan)
-        secs.append(o.last_exec_seconds())
-    s = min(secs)
-    o.close()
-    return rows / s, {"rows": rows, "seconds": s, "scale": scale}
+def _ranks(values):
+    order = sorted(range(len(values)), key=lambda k: values[k])
+    r = [0] * len(values)
+    for i, k in enumerate(order):
+        r[k] = i
+    return r
+
+
+def run_cpu_baseline(name: str, tables):
+    """One execution of the compiled CPU baseline loop for the workload
+    (oracle/baseline.cc: the reference's generated-code loop + runtime
+    structures, restated, one thread).  Returns seconds."""
+    import oracle
+    from kushdb_b200.plan import EPOCH_JDN
+    if name == "scan_agg":
+        return oracle.baseline_scan_agg(tables[0], 9300 + EPOCH_JDN, 0.05, 0.07)[0]
+    if name == "group_by":
+        return oracle.baseline_group_by(tables[0], 10471 + EPOCH_JDN, _ranks(wl.RF_VALUES),
+                                        _ranks(wl.LS_VALUES))[0]
+    return oracle.baseline_join_group(tables[0], tables[1], 9204 + EPOCH_JDN,
+                                      wl.SEG_VALUES.index("BUILDING"))[0]
+
+
+def cpu_baseline(name: str, tables, rows: int, repeats: int = 3):
+    """Times the compiled CPU baseline on the full workload (a few seconds of
+    CPU work at most); rows/s from the best of `repeats`."""
+    secs = min(run_cpu_baseline(name, tables) for _ in range(repeats))
+    return rows / secs, {"rows": rows, "seconds": secs, "repeats": repeats}
 
 
 def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
-    from oracle import Oracle
-    scale = {"scan_agg": 1.0, "group_by": 0.1, "join_group": 0.1}[args.workload]
-    tables, plan, rows, _, _, cfg = make_workload(args.workload, scale)
-    o = Oracle()
-    for t in tables:
-        o.register_table(t)
+    tables, plan, rows, _, _, cfg = make_workload(args.workload)
     for _ in range(args.warmup):
-        o.execute(plan)
+        run_cpu_baseline(args.workload, tables)
     total = 0.0
     for _ in range(args.steps):
-        o.execute(plan)
-        total += o.last_exec_seconds()
+        total += run_cpu_baseline(args.workload, tables)
     value = rows * args.steps / total
-    cfg = dict(cfg)
-    cfg["sample_scale"] = scale
     line = {
         "impl": "reference", "metric": "rows_per_second", "value": value, "unit": "rows/s",
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": total / args.steps * 1e3, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": cfg,
         "cpu_baseline": {"value": value, "unit": "rows/s", "cores": 1, "kind": "port",
-                         "sample": f"{rows} rows of the {args.workload} workload per step "
-                                   f"(scale {scale}), oracle restatement, one thread"},
+                         "sample": f"the full {args.workload} workload ({rows} rows) per step: "
+                                   "compiled restatement of the reference's generated loop and "
+                                   "runtime tables, one thread like the reference executor"},
         "e2e": {"value": value, "unit": "rows/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line))
@@ -301,10 +305,11 @@ def main():
     cpu = None
     if not args.no_cpu_baseline:
         try:
-            v, info = cpu_baseline(args.workload)
+            v, info = cpu_baseline(args.workload, tables, rows)
             cpu = {"value": v, "unit": "rows/s", "cores": 1, "kind": "port",
-                   "sample": f"{info['rows']} rows (scale {info['scale']} of the workload), "
-                             f"{info['seconds']:.3f} s, oracle restatement, one thread"}
+                   "sample": f"full workload ({info['rows']} rows), best of {info['repeats']}: "
+                             f"{info['seconds']:.4f} s; compiled restatement of the reference's "
+                             "generated loop + runtime tables (oracle/baseline.cc), one thread"}
         except Exception as ex:  # the oracle is a reported baseline, not the product
             cpu = {"value": None, "unit": "rows/s", "cores": 1, "kind": "port", "sample": f"failed: {ex}"}
 

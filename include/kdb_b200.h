@@ -17,14 +17,16 @@
  *   compile::TranslateQuery + ExecutableQuery::      kdb_query_execute
  *     Execute (compile/query_translator.h:12,
  *     execution/executable_query.cc:199-255)
- *   runtime::HashTable::{Create,Insert,GetBucket}    kdb_hash_build / kdb_hash_probe
- *     (runtime/hash_table.h:22-38)
- *   runtime::AggregateHashTable::* + aggregators     kdb_group_by_aggregate
- *     (runtime/aggregate_hash_table.h:28-49,
+ *   runtime::HashTable::{Create,Insert,GetBucket}    device join tables built and
+ *     (runtime/hash_table.h:22-38)                    probed inside the pipelines
+ *                                                     of a HASH_JOIN plan
+ *   runtime::AggregateHashTable::* + aggregators     device group tables of a
+ *     (runtime/aggregate_hash_table.h:28-49,          GROUP_BY_AGGREGATE plan
  *      compile/proxy/aggregator.cc)
- *   runtime::Vector::Sort (runtime/vector.cc:105)    kdb_sort
- *   runtime::ExecutePermutableSkinnerJoin            kdb_query_execute with a
- *     (runtime/skinner_join_executor.h:16-25)         SKINNER_JOIN plan
+ *   runtime::Vector::Sort (runtime/vector.cc:105)    device sort of an ORDER_BY
+ *                                                     plan
+ *   runtime::ExecutePermutableSkinnerJoin            SKINNER_JOIN plan
+ *     (runtime/skinner_join_executor.h:16-25)
  *   runtime::Printer (runtime/printer.cc)            kdb_result_format
  *
  * Conventions: every function returns 0 on success and a negative code on

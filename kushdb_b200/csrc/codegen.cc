@@ -16,6 +16,7 @@
 // reference's mulsd/addsd (khir/asm/asm_backend.cc:1834-1864).
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
 #include <cstdio>
 #include <cstring>
 #include <functional>
@@ -432,6 +433,18 @@ std::string OKeyInv(const Type& t, const std::string& k) {
 
 using Consume = std::function<void(const std::vector<CVal>&, const std::string& pos)>;
 
+constexpr int64_t kSmallOrder = 4096;
+
+struct KeyLayout {
+  bool packed = true;
+  std::vector<int> offset, width;
+  std::vector<bool> nullable;
+  std::vector<uint64_t> card;
+  int bits = 0;
+  uint64_t domain = 1;  // number of distinct keys when all keys are enum/bool
+  bool small_domain = true;
+};
+
 struct JoinTable {
   MatBuffer build;
   uint64_t* slots = nullptr;
@@ -521,6 +534,9 @@ class Executor {
   MatBuffer RunAggregate(const Operator& op);
   MatBuffer RunGroupBy(const Operator& op);
   MatBuffer RunOrderBy(const Operator& op);
+  MatBuffer SmallOrderBy(const Operator& op, MatBuffer& m);
+  MatBuffer LargeOrderBy(const Operator& op, MatBuffer& m);
+  MatBuffer RunGroupByDense(const Operator& op, const std::vector<AggPlan>& plans, const KeyLayout& kl);
   void BuildJoin(const Operator& op);
   void PrepareSkinner(const Operator& op);
   JoinTable BuildIndex(const MatBuffer& m, const std::vector<int>& key_cols);
@@ -1249,15 +1265,6 @@ MatBuffer Executor::RunAggregate(const Operator& op) {
 // compile/proxy/aggregate_hash_table.cc:245-291) and one output kernel.
 // ---------------------------------------------------------------------------
 
-struct KeyLayout {
-  bool packed = true;
-  std::vector<int> offset, width;
-  std::vector<bool> nullable;
-  int bits = 0;
-  uint64_t domain = 1;  // number of distinct keys when all keys are enum/bool
-  bool small_domain = true;
-};
-
 KeyLayout PlanKeys(Context& ctx, const std::vector<std::unique_ptr<Expr>>& keys) {
   KeyLayout kl;
   for (const auto& k : keys) {
@@ -1280,6 +1287,7 @@ KeyLayout PlanKeys(Context& ctx, const std::vector<std::unique_ptr<Expr>>& keys)
       case TypeId::TEXT: w = 1000; break;
     }
     kl.offset.push_back(kl.bits);
+    kl.card.push_back(card);
     kl.width.push_back(w);
     kl.nullable.push_back(k->nullable);
     kl.bits += w + (k->nullable ? 1 : 0);
@@ -1290,6 +1298,310 @@ KeyLayout PlanKeys(Context& ctx, const std::vector<std::unique_ptr<Expr>>& keys)
   return kl;
 }
 
+// Structural signature of an expression (identical signatures compute the
+// same value, so their accumulators can be shared).
+std::string ExprSig(const Expr& e) {
+  std::ostringstream o;
+  o << static_cast<int>(e.kind) << ":" << static_cast<int>(e.type.id) << "." << e.type.enum_id << ":"
+    << e.child_idx << "." << e.column_idx << ":" << static_cast<int>(e.bop) << static_cast<int>(e.uop)
+    << static_cast<int>(e.agg) << ":" << e.lit_null << "," << e.ival << "," << F64Lit(e.fval) << ","
+    << e.sval.size() << "'" << e.sval << "'(";
+  for (const auto& k : e.kids) o << ExprSig(*k) << ";";
+  for (int32_t v : e.in_values) o << v << ",";
+  o << ")";
+  return o.str();
+}
+
+// Small-domain group-by: every key is ENUM or BOOLEAN, so a group id is the
+// mixed-radix number of the key digits (NULL is one extra digit).  Each
+// thread keeps all groups' states in registers (selects, no atomics); at the
+// end a warp-shuffle + shared-memory reduction gives one partial per CTA and
+// a single finalize block combines the partials in a fixed order, orders the
+// present groups by their first stream position (the reference's insertion
+// order) and evaluates the output schema.  This is the pre-aggregation the
+// reference's AggregateHashTable::UpdateOrInsert hot loop
+// (compile/proxy/aggregate_hash_table.cc:187-243) turns into on a GPU when the
+// group count is tiny.
+enum class WordKind { AddF64, AddI64, MinU64, MaxU64 };
+
+struct DenseWord {
+  WordKind kind;
+  std::string init;   // C initialiser
+  std::string ctype;  // register type
+};
+
+MatBuffer Executor::RunGroupByDense(const Operator& op, const std::vector<AggPlan>& plans,
+                                    const KeyLayout& kl) {
+  const int64_t D = static_cast<int64_t>(kl.domain);
+  // words per group: per-agg value / count words (shared when identical),
+  // then rows and first position
+  std::vector<DenseWord> words;
+  std::map<std::string, int> word_of;
+  std::vector<int> vword(plans.size(), -1), cword(plans.size(), -1);
+  auto add_word = [&](const std::string& sig, WordKind k, const std::string& init, const std::string& ct) {
+    auto it = word_of.find(sig);
+    if (it != word_of.end()) return it->second;
+    words.push_back({k, init, ct});
+    word_of[sig] = static_cast<int>(words.size()) - 1;
+    return static_cast<int>(words.size()) - 1;
+  };
+  for (size_t j = 0; j < plans.size(); j++) {
+    const AggPlan& p = plans[j];
+    std::string csig = ExprSig(p.agg->kid(0));
+    switch (p.kind) {
+      case StateKind::SumF64:
+      case StateKind::AvgF64: vword[j] = add_word("fsum|" + csig, WordKind::AddF64, "0.0", "double"); break;
+      case StateKind::SumI64: vword[j] = add_word("isum|" + csig, WordKind::AddI64, "0", "int64_t"); break;
+      case StateKind::MinMaxKey:
+        vword[j] = p.is_min ? add_word("min|" + csig, WordKind::MinU64, "~0ULL", "uint64_t")
+                            : add_word("max|" + csig, WordKind::MaxU64, "0ULL", "uint64_t");
+        break;
+      default: break;
+    }
+    if (p.child_nullable) cword[j] = add_word("cnt|" + csig, WordKind::AddI64, "0", "int64_t");
+  }
+  const int rows_w = static_cast<int>(words.size());
+  words.push_back({WordKind::AddI64, "0", "int64_t"});
+  const int first_w = static_cast<int>(words.size());
+  words.push_back({WordKind::MinU64, "~0ULL", "uint64_t"});
+  const int W = static_cast<int>(words.size());
+  const int64_t K = D * W;
+  const int block = 256;
+
+  auto reg = [&](int64_t g, int w) { return "a" + std::to_string(g) + "_" + std::to_string(w); };
+  auto combine = [&](WordKind k, const std::string& a, const std::string& b) -> std::string {
+    switch (k) {
+      case WordKind::AddF64: return "__dadd_rn(" + a + ", " + b + ")";
+      case WordKind::AddI64: return "(int64_t)((uint64_t)" + a + " + (uint64_t)" + b + ")";
+      case WordKind::MinU64: return "(" + b + " < " + a + " ? " + b + " : " + a + ")";
+      case WordKind::MaxU64: return "(" + b + " > " + a + " ? " + b + " : " + a + ")";
+    }
+    return a;
+  };
+  auto to_bits = [&](const DenseWord& w, const std::string& v) {
+    return w.ctype == "double" ? "(uint64_t)__double_as_longlong(" + v + ")" : "(uint64_t)" + v;
+  };
+  auto from_bits = [&](const DenseWord& w, const std::string& v) {
+    return w.ctype == "double" ? "__longlong_as_double((long long)" + v + ")" : "(" + w.ctype + ")" + v;
+  };
+
+  KernelSource ks;
+  ExprGen eg(ctx_, ks);
+  for (int64_t g = 0; g < D; g++)
+    for (int w = 0; w < W; w++) ks.L(words[w].ctype + " " + reg(g, w) + " = " + words[w].init + ";");
+  int64_t src_rows = 0;
+  auto consume = [&](const std::vector<CVal>& in, const std::string& pos) {
+    Scope s;
+    s.child.push_back(in);
+    std::string gid = "0";
+    int64_t stride = 1;
+    for (size_t k = 0; k < op.group_by.size(); k++) {
+      CVal c = eg.Emit(*op.group_by[k], s);
+      std::string digit = c.type.id == TypeId::BOOLEAN ? "(" + c.v + " ? 1 : 0)" : "(int64_t)" + c.v;
+      if (kl.nullable[k]) digit = "((" + c.n + ") ? " + std::to_string(kl.card[k]) + " : " + digit + ")";
+      gid += " + " + digit + " * " + std::to_string(stride);
+      stride *= static_cast<int64_t>(kl.card[k] + (kl.nullable[k] ? 1 : 0));
+    }
+    std::string G = ks.Fresh("gid");
+    ks.L("int64_t " + G + " = " + gid + ";");
+    // per-row contributions of every word
+    std::vector<std::string> contrib(W), active(W, "true");
+    std::string fl = "0ULL";
+    for (size_t j = 0; j < plans.size(); j++) {
+      const AggPlan& p = plans[j];
+      CVal c = eg.Emit(p.agg->kid(0), s);
+      if (p.count_flag >= 0) fl += " | ((" + c.n + ") ? " + std::to_string(1 << p.count_flag) + "ULL : 0ULL)";
+      std::string nn = "!(" + c.n + ")";
+      if (vword[j] >= 0 && contrib[vword[j]].empty()) {
+        switch (p.kind) {
+          case StateKind::SumF64: contrib[vword[j]] = c.v; break;
+          case StateKind::AvgF64: contrib[vword[j]] = "(double)" + c.v; break;
+          case StateKind::SumI64: contrib[vword[j]] = "(int64_t)" + c.v; break;
+          default: contrib[vword[j]] = OKey(eg, c); break;
+        }
+        active[vword[j]] = nn;
+      }
+      if (cword[j] >= 0 && contrib[cword[j]].empty()) {
+        contrib[cword[j]] = "(int64_t)1";
+        active[cword[j]] = nn;
+      }
+    }
+    contrib[rows_w] = "(int64_t)1";
+    contrib[first_w] = "(((uint64_t)(" + pos + ") << 8) | (" + fl + "))";
+    std::vector<std::string> cv(W);
+    for (int w = 0; w < W; w++) {
+      cv[w] = ks.Fresh("c");
+      ks.L(words[w].ctype + " " + cv[w] + " = " + contrib[w] + ";");
+    }
+    for (int64_t g = 0; g < D; g++) {
+      std::string h = ks.Fresh("h");
+      ks.L("bool " + h + " = " + G + " == " + std::to_string(g) + ";");
+      for (int w = 0; w < W; w++) {
+        std::string cond = active[w] == "true" ? h : "(" + h + " && " + active[w] + ")";
+        ks.L(reg(g, w) + " = " + cond + " ? " + combine(words[w].kind, reg(g, w), cv[w]) + " : " + reg(g, w) + ";");
+      }
+    }
+  };
+  if (Streamable(op.child())) EmitStream(ks, eg, op.child(), consume, src_rows);
+  else EmitMatScan(ks, mats_.at(&op.child()), nullptr, consume, src_rows);
+
+  int grid = static_cast<int>(std::min<int64_t>(ctx_.GridFor(std::max<int64_t>(src_rows, 1), block),
+                                                static_cast<int64_t>(ctx_.num_sms) * 2));
+  uint64_t* part = arena_.AllocT<uint64_t>(static_cast<size_t>(grid) * K);
+  std::string PP = ks.Ptr(part, "uint64_t");
+  ks.L("__shared__ uint64_t red[" + std::to_string(block / 32) + "][" + std::to_string(K) + "];");
+  ks.L("const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;");
+  for (int64_t g = 0; g < D; g++)
+    for (int w = 0; w < W; w++) {
+      std::string r = reg(g, w);
+      ks.L("for (int o = 16; o > 0; o >>= 1) { " + words[w].ctype + " y = __shfl_xor_sync(0xffffffffu, " + r +
+           ", o); " + r + " = " + combine(words[w].kind, r, "y") + "; }");
+      ks.L("if (lane == 0) red[warp][" + std::to_string(g * W + w) + "] = " + to_bits(words[w], r) + ";");
+    }
+  ks.L("__syncthreads();");
+  ks.Open("for (int k = threadIdx.x; k < " + std::to_string(K) + "; k += blockDim.x)");
+  ks.L("int w = k % " + std::to_string(W) + ";");
+  ks.L("uint64_t acc = red[0][k];");
+  ks.Open("for (int wp = 1; wp < " + std::to_string(block / 32) + "; wp++)");
+  ks.L("uint64_t y = red[wp][k];");
+  ks.Open("switch (w)");
+  for (int w = 0; w < W; w++) {
+    ks.L("case " + std::to_string(w) + ": acc = " +
+         to_bits(words[w], combine(words[w].kind, from_bits(words[w], "acc"), from_bits(words[w], "y"))) + "; break;");
+  }
+  ks.Close();
+  ks.Close();
+  ks.L(PP + "[(int64_t)blockIdx.x * " + std::to_string(K) + " + k] = acc;");
+  ks.Close();
+  {
+    std::string src = ks.Kernel("kdb_pipeline", block);
+    CUfunction f = ctx_.Kernel(src, "kdb_pipeline");
+    ctx_.Launch(f, grid, block, ks.Args(), 0, "group by");
+  }
+
+  // finalize: one block combines the per-CTA partials (warp per word, fixed
+  // order), orders present groups by first position, evaluates the output
+  MatBuffer out = AllocMat(op.output, D);
+  uint64_t* ngroups = arena_.AllocT<uint64_t>(1);
+  KernelSource fk;
+  ExprGen fg(ctx_, fk);
+  std::string FP = fk.Ptr(part, "uint64_t", true);
+  std::string NG = fk.Ptr(ngroups, "uint64_t");
+  std::string GW = "(int64_t)" + fk.Word(static_cast<uint64_t>(grid));
+  fk.L("__shared__ uint64_t tot[" + std::to_string(K) + "];");
+  fk.L("__shared__ int32_t order[" + std::to_string(D) + "];");
+  fk.L("const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;");
+  fk.Open("for (int k = warp; k < " + std::to_string(K) + "; k += blockDim.x / 32)");
+  fk.L("int w = k % " + std::to_string(W) + ";");
+  fk.L("uint64_t acc = 0; bool have = false;");
+  fk.Open("for (int64_t b = lane; b < " + GW + "; b += 32)");
+  fk.L("uint64_t y = " + FP + "[b * " + std::to_string(K) + " + k];");
+  fk.Open("if (!have)");
+  fk.L("acc = y; have = true;");
+  fk.Close();
+  fk.Open("else");
+  fk.Open("switch (w)");
+  for (int w = 0; w < W; w++)
+    fk.L("case " + std::to_string(w) + ": acc = " +
+         to_bits(words[w], combine(words[w].kind, from_bits(words[w], "acc"), from_bits(words[w], "y"))) + "; break;");
+  fk.Close();
+  fk.Close();
+  fk.Close();
+  fk.Open("for (int o = 16; o > 0; o >>= 1)");
+  fk.L("uint64_t y = __shfl_down_sync(0xffffffffu, acc, o);");
+  fk.L("bool hy = __shfl_down_sync(0xffffffffu, have, o);");
+  fk.Open("if (hy && lane + o < 32)");
+  fk.Open("if (!have)");
+  fk.L("acc = y; have = true;");
+  fk.Close();
+  fk.Open("else");
+  fk.Open("switch (w)");
+  for (int w = 0; w < W; w++)
+    fk.L("case " + std::to_string(w) + ": acc = " +
+         to_bits(words[w], combine(words[w].kind, from_bits(words[w], "acc"), from_bits(words[w], "y"))) + "; break;");
+  fk.Close();
+  fk.Close();
+  fk.Close();
+  fk.Close();
+  fk.L("if (lane == 0) tot[k] = acc;");
+  fk.Close();
+  fk.L("__syncthreads();");
+  fk.Open("if (threadIdx.x == 0)");
+  fk.L("int32_t ng = 0;");
+  fk.Open("for (int32_t g = 0; g < " + std::to_string(D) + "; g++)");
+  fk.Open("if ((int64_t)tot[g * " + std::to_string(W) + " + " + std::to_string(rows_w) + "] > 0)");
+  // insertion by first position
+  fk.L("int32_t j = ng++;");
+  fk.L("uint64_t fg = tot[g * " + std::to_string(W) + " + " + std::to_string(first_w) + "];");
+  fk.L("while (j > 0 && tot[order[j - 1] * " + std::to_string(W) + " + " + std::to_string(first_w) +
+       "] > fg) { order[j] = order[j - 1]; j--; }");
+  fk.L("order[j] = g;");
+  fk.Close();
+  fk.Close();
+  fk.L("*" + NG + " = (uint64_t)ng;");
+  std::vector<std::string> optr, onull;
+  for (const auto& c : out.cols) {
+    optr.push_back(fk.Ptr(c.data, StoreType(c.type.id)));
+    onull.push_back(c.nullable ? fk.Ptr(c.nulls, "int8_t") : "");
+  }
+  std::string posp = fk.Ptr(out.pos, "uint64_t");
+  fk.Open("for (int32_t r = 0; r < ng; r++)");
+  fk.L("int64_t g = order[r];");
+  fk.L("const uint64_t* t = tot + g * " + std::to_string(W) + ";");
+  fk.L("int64_t rows = (int64_t)t[" + std::to_string(rows_w) + "];");
+  fk.L("uint64_t fst = t[" + std::to_string(first_w) + "];");
+  std::vector<CVal> virt;
+  int64_t stride = 1;
+  for (size_t k = 0; k < op.group_by.size(); k++) {
+    const Type& ty = op.group_by[k]->type;
+    int64_t base = static_cast<int64_t>(kl.card[k] + (kl.nullable[k] ? 1 : 0));
+    std::string digit = "((g / " + std::to_string(stride) + ") % " + std::to_string(base) + ")";
+    std::string v = ty.id == TypeId::BOOLEAN ? "(" + digit + " != 0)" : "(" + CType(ty.id) + ")" + digit;
+    std::string n = kl.nullable[k] ? "(" + digit + " == " + std::to_string(kl.card[k]) + ")" : "false";
+    virt.push_back(fg.Bind(ty, v, n));
+    stride *= base;
+  }
+  for (size_t j = 0; j < plans.size(); j++) {
+    const AggPlan& p = plans[j];
+    const Type& rt = p.agg->type;
+    const Type& ct = p.agg->kid(0).type;
+    std::string cnt = cword[j] >= 0 ? "(int64_t)t[" + std::to_string(cword[j]) + "]" : "rows";
+    std::string v = vword[j] >= 0 ? from_bits(words[vword[j]], "t[" + std::to_string(vword[j]) + "]") : "";
+    switch (p.kind) {
+      case StateKind::SumF64: virt.push_back(fg.Bind(rt, v, cnt + " == 0")); break;
+      case StateKind::SumI64: virt.push_back(fg.Bind(rt, "(" + CType(rt.id) + ")" + v, cnt + " == 0")); break;
+      case StateKind::AvgF64: virt.push_back(fg.Bind(rt, "__ddiv_rn(" + v + ", (double)" + cnt + ")", cnt + " == 0")); break;
+      case StateKind::Count: {
+        std::string val = cnt;
+        if (p.count_flag >= 0) val = "(" + cnt + " + (int64_t)((fst >> " + std::to_string(p.count_flag) + ") & 1ULL))";
+        virt.push_back(fg.Bind(rt, val, "false"));
+        break;
+      }
+      case StateKind::MinMaxKey: virt.push_back(fg.Bind(rt, OKeyInv(ct, v), cnt + " == 0")); break;
+      default: throw Error(-5, "dense group-by cannot hold TEXT MIN/MAX");
+    }
+  }
+  Scope sc;
+  sc.virt = virt;
+  for (size_t c = 0; c < op.output.size(); c++) {
+    CVal v = fg.Emit(*op.output[c].expr, sc);
+    std::string val = v.type.id == TypeId::BOOLEAN ? "(int8_t)(" + v.v + " ? 1 : 0)" : v.v;
+    fk.L(optr[c] + "[r] = " + val + ";");
+    if (!onull[c].empty()) fk.L(onull[c] + "[r] = (" + v.n + ") ? 1 : 0;");
+  }
+  fk.L(posp + "[r] = (uint64_t)r;");
+  fk.Close();
+  fk.Close();
+  {
+    std::string src = fk.Kernel("kdb_finalize", 256);
+    CUfunction f = ctx_.Kernel(src, "kdb_finalize");
+    ctx_.Launch(f, 1, 256, fk.Args(), 0, "group by finalize");
+  }
+  out.rows = ReadU64(ngroups);
+  ctx_.CheckDeviceError("group by");
+  return out;
+}
+
 MatBuffer Executor::RunGroupBy(const Operator& op) {
   PrepareInput(op.child());
   int flags = 0;
@@ -1297,6 +1609,17 @@ MatBuffer Executor::RunGroupBy(const Operator& op) {
   for (const auto& a : op.aggs) plans.push_back(PlanAgg(*a, flags));
   KeyLayout kl = PlanKeys(ctx_, op.group_by);
   const size_t nk = op.group_by.size();
+  {
+    // small key domain: register pre-aggregation (no atomics)
+    bool dense = kl.small_domain && kl.domain <= 32 && !op.group_by.empty();
+    int words = 2;
+    for (const auto& p : plans) {
+      if (p.kind == StateKind::MinMaxText) dense = false;
+      words += 2;
+    }
+    if (dense && static_cast<int64_t>(kl.domain) * words <= 96 && !std::getenv("KDB_NO_DENSE_GROUPBY"))
+      return RunGroupByDense(op, plans, kl);
+  }
 
   uint64_t cap = 1024;
   if (kl.small_domain) {
@@ -1554,6 +1877,78 @@ MatBuffer Executor::RunGroupBy(const Operator& op) {
 
 MatBuffer Executor::RunOrderBy(const Operator& op) {
   MatBuffer m = Materialize(op.child());
+  int64_t n = m.rows;
+  if (n <= kSmallOrder) return SmallOrderBy(op, m);
+  return LargeOrderBy(op, m);
+}
+
+// ORDER BY of at most kSmallOrder rows in one block: every row's final rank
+// is the number of rows that compare before it under the generated
+// comparator (sort keys, then the reference merge sort's tie key of the
+// row's stream index), so one launch replaces the radix passes.
+MatBuffer Executor::SmallOrderBy(const Operator& op, MatBuffer& m) {
+  int64_t n = m.rows;
+  uint32_t* idx = arena_.AllocT<uint32_t>(std::max<int64_t>(n, 1));
+  if (n > 0) {
+    KernelSource ks;
+    ExprGen eg(ctx_, ks);
+    std::string P = ks.Ptr(m.pos, "uint64_t", true);
+    std::string I = ks.Ptr(idx, "uint32_t");
+    std::string N = "nrows";
+    ks.L("__shared__ uint32_t sidx[" + std::to_string(kSmallOrder) + "];");
+    ks.L("const int64_t nrows = (int64_t)" + ks.Word(static_cast<uint64_t>(n)) + ";");
+    ks.Open("for (int64_t i = threadIdx.x; i < " + N + "; i += blockDim.x)");
+    ks.L("uint64_t p = " + P + "[i]; uint32_t c = 0;");
+    ks.L("for (int64_t j = 0; j < " + N + "; j++) c += " + P + "[j] < p;");
+    ks.L("sidx[i] = c;");
+    ks.Close();
+    ks.L("__syncthreads();");
+    // comparator over the materialised key columns
+    std::string less = "auto less = [&](int64_t ra, int64_t rb) -> bool {\n";
+    for (size_t k = 0; k < op.sort_keys.size(); k++) {
+      const MatCol& mc = m.cols.at(op.sort_keys[k]->column_idx);
+      if (mc.type.id == TypeId::BOOLEAN) throw Error(-1, "Can't be less than.");
+      std::string D = ks.Ptr(mc.data, StoreType(mc.type.id), true);
+      std::string NP = mc.nullable ? ks.Ptr(mc.nulls, "int8_t", true) : "";
+      std::string na = NP.empty() ? "false" : "(" + NP + "[ra] != 0)";
+      std::string nb = NP.empty() ? "false" : "(" + NP + "[rb] != 0)";
+      std::string ab, ba;
+      switch (mc.type.id) {
+        case TypeId::TEXT:
+          ab = "(kdb_str_cmp(" + D + "[ra], " + D + "[rb]) < 0)";
+          ba = "(kdb_str_cmp(" + D + "[rb], " + D + "[ra]) < 0)";
+          break;
+        case TypeId::ENUM:
+          ab = "(" + eg.EnumRank(mc.type, D + "[ra]") + " < " + eg.EnumRank(mc.type, D + "[rb]") + ")";
+          ba = "(" + eg.EnumRank(mc.type, D + "[rb]") + " < " + eg.EnumRank(mc.type, D + "[ra]") + ")";
+          break;
+        default:
+          ab = "(" + D + "[ra] < " + D + "[rb])";
+          ba = "(" + D + "[rb] < " + D + "[ra])";
+          break;
+      }
+      // proxy::LessThan: NULL sorts after every value
+      std::string lt_ab = "(!" + na + " && (" + nb + " || " + ab + "))";
+      std::string lt_ba = "(!" + nb + " && (" + na + " || " + ba + "))";
+      bool asc = op.asc[k];
+      less += "    if " + lt_ab + " return " + (asc ? "true" : "false") + ";\n";
+      less += "    if " + lt_ba + " return " + (asc ? "false" : "true") + ";\n";
+    }
+    less += "    return kdb_tie_path(sidx[ra], " + N + ") < kdb_tie_path(sidx[rb], " + N + ");\n  };";
+    ks.L(less);
+    ks.Open("for (int64_t i = threadIdx.x; i < " + N + "; i += blockDim.x)");
+    ks.L("uint32_t r = 0;");
+    ks.L("for (int64_t j = 0; j < " + N + "; j++) r += (j != i) && less(j, i);");
+    ks.L(I + "[r] = (uint32_t)i;");
+    ks.Close();
+    std::string src = ks.Kernel("kdb_pipeline", 1024);
+    CUfunction f = ctx_.Kernel(src, "kdb_pipeline");
+    ctx_.Launch(f, 1, 1024, ks.Args(), 0, "order by small");
+  }
+  return MaterializeStream(op, idx, &m);
+}
+
+MatBuffer Executor::LargeOrderBy(const Operator& op, MatBuffer& m) {
   int64_t n = m.rows;
   uint64_t* keys = arena_.AllocT<uint64_t>(std::max<int64_t>(n, 1));
   uint32_t* idx = arena_.AllocT<uint32_t>(std::max<int64_t>(n, 1));

@@ -28,7 +28,7 @@ typedef unsigned long long uint64_t;
 
 // Bounded spin: every device-side wait gives up after this many polls and
 // reports KDB_DEV_ERR_TIMEOUT instead of hanging the GPU.
-#define KDB_SPIN_LIMIT (1 << 22)
+#define KDB_SPIN_LIMIT (1 << 20)
 
 struct KArgs {
   uint64_t w[384];
@@ -268,8 +268,13 @@ KDB_DEV int64_t kdb_group_find(uint64_t* slots, uint64_t mask, uint64_t h, EQ eq
       s = prev;
     }
     if (s == 1) {
+      // the claiming thread may be a lane of this warp: back off so the
+      // scheduler runs it (independent thread scheduling), bounded
       int it = 0;
-      while ((s = *(volatile uint64_t*)&slots[i]) == 1 && it < KDB_SPIN_LIMIT) it++;
+      while ((s = *(volatile uint64_t*)&slots[i]) == 1 && it < KDB_SPIN_LIMIT) {
+        __nanosleep(64);
+        it++;
+      }
       if (s == 1) {
         kdb_set_error(err, KDB_DEV_ERR_TIMEOUT);
         return -1;
@@ -318,12 +323,12 @@ KDB_DEV T kdb_block_reduce(T v, OP op, T* scratch) {
   __syncthreads();
   int nw = (blockDim.x + 31) >> 5;
   if (warp == 0) {
-    T x = lane < nw ? scratch[lane] : v;
-    if (lane < nw) {
-      for (int o = 16; o > 0; o >>= 1) {
-        T y = __shfl_down_sync(0xffffffffu, x, o);
-        if (lane + o < nw) x = op(x, y);
-      }
+    // every lane of warp 0 takes part in each full-mask shuffle; lanes past
+    // the warp count only feed values that are never combined
+    T x = lane < nw ? scratch[lane] : scratch[0];
+    for (int o = 16; o > 0; o >>= 1) {
+      T y = __shfl_down_sync(0xffffffffu, x, o);
+      if (lane + o < nw) x = op(x, y);
     }
     v = x;
   }

@@ -304,6 +304,10 @@ CUfunction Context::Kernel(const std::string& source, const std::string& name) {
   if (it == programs_.end()) {
     auto prog = std::make_unique<Program>();
     std::string full = std::string(kDeviceRuntime) + "\n" + source;
+    if (const char* dir = std::getenv("KDB_DUMP_DIR")) {
+      // debugging aid: keep every generated pipeline source
+      std::ofstream(std::string(dir) + "/pipeline_" + std::to_string(programs_.size()) + ".cu") << source;
+    }
     nvrtcProgram p;
     NvrtcCheck(nvrtcCreateProgram(&p, full.c_str(), "kdb_pipeline.cu", 0, nullptr, nullptr),
                "nvrtcCreateProgram");

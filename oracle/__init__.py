@@ -50,6 +50,13 @@ def lib():
         L.kdbo_last_exec_seconds.restype = ctypes.c_double
         L.kdbo_last_exec_seconds.argtypes = [P]
         declare_result_api(L, "kdbo_")
+        D = ctypes.c_double
+        L.kdbo_baseline_scan_agg.restype = D
+        L.kdbo_baseline_scan_agg.argtypes = [P, P, P, I64, I32, D, D, P, P, P]
+        L.kdbo_baseline_group_by.restype = D
+        L.kdbo_baseline_group_by.argtypes = [P, P, P, P, P, P, P, I64, I32, P, P, P, I32, P]
+        L.kdbo_baseline_join_group.restype = D
+        L.kdbo_baseline_join_group.argtypes = [P, P, P, I64, I32, I32, P, P, P, I64, I32, P, P, P]
         _lib = L
     return _lib
 
@@ -129,3 +136,50 @@ def oracle_for(tables: Dict[str, HostTable]) -> Oracle:
     for t in tables.values():
         o.register_table(t)
     return o
+
+
+# ---------------------------------------------------------------------------
+# Compiled CPU baseline loops (oracle/baseline.cc): the benchmark plans as the
+# reference's generated code runs them, one thread.  Each returns
+# (seconds, result).
+# ---------------------------------------------------------------------------
+
+
+def baseline_scan_agg(table, date_lt_jdn: int, lo: float, hi: float):
+    L = lib()
+    c = table.columns
+    date = np.ascontiguousarray(c["s_date"].values)
+    disc = np.ascontiguousarray(c["s_discount"].values)
+    price = np.ascontiguousarray(c["s_price"].values)
+    s, n, e = ctypes.c_double(), ctypes.c_int64(), ctypes.c_int8()
+    secs = L.kdbo_baseline_scan_agg(_ptr(date), _ptr(disc), _ptr(price), len(date), date_lt_jdn, lo, hi,
+                                    ctypes.byref(s), ctypes.byref(n), ctypes.byref(e))
+    return secs, (None if e.value else s.value, None if e.value else n.value)
+
+
+def baseline_group_by(table, date_leq_jdn: int, rank_rf, rank_ls):
+    L = lib()
+    c = table.columns
+    arrs = [np.ascontiguousarray(c[k].values) for k in
+            ["l_shipdate", "l_returnflag", "l_linestatus", "l_quantity", "l_extendedprice", "l_discount", "l_tax"]]
+    rr = np.ascontiguousarray(rank_rf, np.int32)
+    rl = np.ascontiguousarray(rank_ls, np.int32)
+    out = np.zeros((64, 10), np.float64)
+    ng = ctypes.c_int32()
+    secs = L.kdbo_baseline_group_by(*[_ptr(a) for a in arrs], len(arrs[0]), date_leq_jdn, _ptr(rr), _ptr(rl),
+                                    _ptr(out), 64, ctypes.byref(ng))
+    return secs, out[:min(ng.value, 64)]
+
+
+def baseline_join_group(build, probe, date_lt_jdn: int, seg: int, top: int = 10):
+    L = lib()
+    b, p = build.columns, probe.columns
+    ck, cd, cs = (np.ascontiguousarray(b[k].values) for k in ["c_custkey", "c_date", "c_segment"])
+    ok, op, od = (np.ascontiguousarray(p[k].values) for k in ["o_custkey", "o_price", "o_discount"])
+    keys = np.zeros(top, np.int32)
+    sums = np.zeros(top, np.float64)
+    ng = ctypes.c_int32()
+    secs = L.kdbo_baseline_join_group(_ptr(ck), _ptr(cd), _ptr(cs), len(ck), date_lt_jdn, seg, _ptr(ok),
+                                      _ptr(op), _ptr(od), len(ok), top, _ptr(keys), _ptr(sums),
+                                      ctypes.byref(ng))
+    return secs, (ng.value, keys, sums)
