@@ -946,7 +946,10 @@ MatBuffer Executor::MaterializeStream(const Operator& op, const uint32_t* order,
     std::string capw = "(uint64_t)" + ks.Word(static_cast<uint64_t>(out.cap));
     auto sink = [&](const std::vector<CVal>& vals, const std::string& pos) {
       ks.Open("");
-      ks.L("uint64_t slot = kdb_alloc_slot((unsigned long long*)" + cnt + ");");
+      // an ordered source (ORDER BY output) writes row r at index r; other
+      // streams append through the warp-aggregated counter
+      if (ordered_src) ks.L("uint64_t slot = (uint64_t)r; if (r == 0) *(unsigned long long*)" + cnt + " = " + capw + ";");
+      else ks.L("uint64_t slot = kdb_alloc_slot((unsigned long long*)" + cnt + ");");
       ks.Open("if (slot < " + capw + ")");
       for (size_t c = 0; c < vals.size(); c++) {
         const CVal& v = vals[c];
@@ -1610,14 +1613,20 @@ MatBuffer Executor::RunGroupBy(const Operator& op) {
   KeyLayout kl = PlanKeys(ctx_, op.group_by);
   const size_t nk = op.group_by.size();
   {
-    // small key domain: register pre-aggregation (no atomics)
+    // small key domain: register pre-aggregation (no atomics) when the
+    // per-thread state (groups x distinct accumulator words) stays small
     bool dense = kl.small_domain && kl.domain <= 32 && !op.group_by.empty();
-    int words = 2;
+    std::set<std::string> distinct;
     for (const auto& p : plans) {
       if (p.kind == StateKind::MinMaxText) dense = false;
-      words += 2;
+      std::string csig = ExprSig(p.agg->kid(0));
+      if (p.kind == StateKind::SumF64 || p.kind == StateKind::AvgF64) distinct.insert("f|" + csig);
+      else if (p.kind == StateKind::SumI64) distinct.insert("i|" + csig);
+      else if (p.kind == StateKind::MinMaxKey) distinct.insert((p.is_min ? "n|" : "x|") + csig);
+      if (p.child_nullable) distinct.insert("c|" + csig);
     }
-    if (dense && static_cast<int64_t>(kl.domain) * words <= 96 && !std::getenv("KDB_NO_DENSE_GROUPBY"))
+    int64_t words = static_cast<int64_t>(distinct.size()) + 2;
+    if (dense && static_cast<int64_t>(kl.domain) * words <= 64 && !std::getenv("KDB_NO_DENSE_GROUPBY"))
       return RunGroupByDense(op, plans, kl);
   }
 

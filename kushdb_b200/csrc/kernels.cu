@@ -112,6 +112,31 @@ __global__ void __launch_bounds__(kSortBlock) RadixScatter(
   }
 }
 
+// Stable sort of at most kSmallSort pairs in one block: an element's rank is
+// the number of smaller keys plus the equal keys before it.
+constexpr int kSmallSort = 2048;
+
+__global__ void __launch_bounds__(1024) SmallRankSort(uint64_t* __restrict__ keys,
+                                                      uint32_t* __restrict__ vals, int n,
+                                                      uint64_t mask) {
+  __shared__ uint64_t sk[kSmallSort];
+  __shared__ uint64_t sfull[kSmallSort];
+  __shared__ uint32_t sv[kSmallSort];
+  for (int i = threadIdx.x; i < n; i += blockDim.x) {
+    sfull[i] = keys[i];
+    sk[i] = keys[i] & mask;
+    sv[i] = vals[i];
+  }
+  __syncthreads();
+  for (int i = threadIdx.x; i < n; i += blockDim.x) {
+    uint64_t k = sk[i];
+    int r = 0;
+    for (int j = 0; j < n; j++) r += (sk[j] < k) || (sk[j] == k && j < i);
+    keys[r] = sfull[i];
+    vals[r] = sv[i];
+  }
+}
+
 __global__ void CopyPairs(const uint64_t* __restrict__ ks, const uint32_t* __restrict__ vs,
                           uint64_t* __restrict__ kd, uint32_t* __restrict__ vd, int64_t n) {
   for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < n;
@@ -128,6 +153,15 @@ void Context::RadixSortPairs(uint64_t* keys, uint32_t* vals, int64_t n, Arena& a
                              int key_bits) {
   if (n <= 1 || dry) return;
   if (n > 0xffffffffLL) throw Error(-5, "sort of more than 2^32 rows");
+  if (n <= kSmallSort) {
+    uint64_t mask = key_bits >= 64 ? ~0ULL : ((1ULL << key_bits) - 1);
+    TimedStart("sort small");
+    SmallRankSort<<<1, 1024, 0, stream>>>(keys, vals, static_cast<int>(n), mask);
+    TimedStop();
+    kernel_launches++;
+    KDB_CUDA(cudaGetLastError());
+    return;
+  }
   int nblocks = static_cast<int>((n + kSortTile - 1) / kSortTile);
   uint64_t* k2 = arena.AllocT<uint64_t>(n);
   uint32_t* v2 = arena.AllocT<uint32_t>(n);

@@ -122,8 +122,10 @@ class Engine:
 
     def register_enums(self) -> None:
         for k, vals in EnumRegistry.all().items():
-            if self._enums_sent.get(k) == id(vals) and False:
+            key = tuple(vals)
+            if self._enums_sent.get(k) == key:
                 continue
+            self._enums_sent[k] = key
             enc = [v.encode() for v in vals]
             off = np.zeros(len(enc) + 1, np.int64)
             off[1:] = np.cumsum([len(b) for b in enc])
@@ -150,12 +152,17 @@ class Engine:
     def drop_table(self, name: str) -> None:
         self._check(self.lib.kdb_table_drop(self.ctx, name.encode()))
 
-    def execute(self, plan) -> Result:
+    def execute(self, plan, fetch: bool = True):
+        """Runs the plan; returns a Result (fetch=True) or the row count."""
         text = plan.to_json() if isinstance(plan, Operator) else plan
+        if isinstance(text, str):
+            text = text.encode()
         self.register_enums()
         h = ctypes.c_void_p()
-        self._check(self.lib.kdb_query_execute(self.ctx, text.encode(), ctypes.byref(h)))
+        self._check(self.lib.kdb_query_execute(self.ctx, text, ctypes.byref(h)))
         try:
+            if not fetch:
+                return self.lib.kdb_result_num_rows(h)
             return Result.from_handle(self.lib, "kdb_", self.ctx, h)
         finally:
             self.lib.kdb_result_free(h)
