@@ -2,6 +2,7 @@
 #include <cstring>
 #include <fstream>
 #include <sstream>
+#include <unordered_map>
 
 #include "../../include/kdb_b200.h"
 #include "engine.h"
@@ -9,6 +10,7 @@
 struct kdb_ctx {
   std::unique_ptr<kdb::Context> c;
   std::string err;
+  std::unordered_map<std::string, std::unique_ptr<kdb::plan::Operator>> plans;
 };
 
 struct kdb_result {
@@ -195,9 +197,15 @@ int kdb_query_execute(kdb_ctx* ctx, const char* plan_json, kdb_result** out) {
   if (out) *out = nullptr;
   return Guard(ctx, [&] {
     if (!plan_json || !out) throw kdb::Error(KDB_ERR_INVALID, "null argument");
-    auto plan = kdb::plan::ParsePlan(plan_json);
+    // parsed plans are cached by their text (a prepared statement's tree)
+    auto& cache = ctx->plans;
+    auto it = cache.find(plan_json);
+    if (it == cache.end()) {
+      if (cache.size() >= 256) cache.clear();
+      it = cache.emplace(plan_json, kdb::plan::ParsePlan(plan_json)).first;
+    }
     auto res = std::make_unique<kdb_result>();
-    res->r = kdb::ExecutePlan(*ctx->c, *plan);
+    res->r = kdb::ExecutePlan(*ctx->c, *it->second);
     *out = res.release();
   });
 }

@@ -373,6 +373,67 @@ class ExprGen {
 
 enum class StateKind { SumF64, SumI64, AvgF64, Count, MinMaxKey, MinMaxText };
 
+// How two partial states of one accumulator word combine.
+enum class WordKind { AddF64, AddI64, MinU64, MaxU64 };
+
+struct DenseWord {
+  WordKind kind;
+  std::string init;   // C initialiser
+  std::string ctype;  // register type
+};
+
+// C expression combining two uint64 bit patterns of a word of kind `k`.
+std::string CombineBits(WordKind k, const std::string& a, const std::string& b) {
+  switch (k) {
+    case WordKind::AddF64:
+      return "(uint64_t)__double_as_longlong(__dadd_rn(__longlong_as_double((long long)" + a +
+             "), __longlong_as_double((long long)" + b + ")))";
+    case WordKind::AddI64: return "(" + a + " + " + b + ")";
+    case WordKind::MinU64: return "(" + b + " < " + a + " ? " + b + " : " + a + ")";
+    case WordKind::MaxU64: return "(" + b + " > " + a + " ? " + b + " : " + a + ")";
+  }
+  return a;
+}
+
+// Emits a block-wide reduction of per-CTA partials part[b * nw + k] over
+// `G` blocks into shared tot[k]: one warp per word, lanes striding over the
+// blocks in a fixed order, then a shuffle tree (deterministic).
+void EmitPartialReduce(KernelSource& ks, const std::string& part, const std::string& G, int nw,
+                       const std::vector<WordKind>& kinds) {
+  ks.L("__shared__ uint64_t tot[" + std::to_string(nw) + "];");
+  ks.Open("");
+  ks.L("const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;");
+  ks.Open("for (int k = warp; k < " + std::to_string(nw) + "; k += blockDim.x / 32)");
+  ks.L("uint64_t acc = 0; bool have = false;");
+  ks.Open("for (int64_t b = lane; b < (int64_t)" + G + "; b += 32)");
+  ks.L("uint64_t y = " + part + "[b * " + std::to_string(nw) + " + k];");
+  ks.Open("if (!have)");
+  ks.L("acc = y; have = true;");
+  ks.Close();
+  ks.Open("else switch (k)");
+  for (int w = 0; w < nw; w++) ks.L("case " + std::to_string(w) + ": acc = " + CombineBits(kinds[w], "acc", "y") + "; break;");
+  ks.Close();
+  ks.Close();
+  ks.Open("for (int o = 16; o > 0; o >>= 1)");
+  ks.L("uint64_t y = __shfl_down_sync(0xffffffffu, acc, o);");
+  ks.L("bool hy = __shfl_down_sync(0xffffffffu, have, o);");
+  ks.Open("if (hy && lane + o < 32)");
+  ks.Open("if (!have)");
+  ks.L("acc = y; have = true;");
+  ks.Close();
+  ks.Open("else switch (k)");
+  for (int w = 0; w < nw; w++) ks.L("case " + std::to_string(w) + ": acc = " + CombineBits(kinds[w], "acc", "y") + "; break;");
+  ks.Close();
+  ks.Close();
+  ks.Close();
+  ks.L("if (lane == 0) tot[k] = acc;");
+  ks.Close();
+  ks.Close();
+  ks.L("__syncthreads();");
+}
+
+
+
 struct AggPlan {
   const Expr* agg;
   StateKind kind;
@@ -466,6 +527,23 @@ class Executor {
   std::map<std::pair<const Operator*, int>, JoinTable> skinner_idx_;
 
   // --- helpers -----------------------------------------------------------
+  // Upper bound (or, for joins, an estimate) of the rows a stream produces.
+  int64_t RowBound(const Operator& o) {
+    switch (o.kind) {
+      case OpKind::SCAN:
+      case OpKind::SCAN_SELECT: {
+        auto it = ctx_.tables.find(o.relation);
+        return it == ctx_.tables.end() ? 0 : std::max<int64_t>(it->second.rows, 0);
+      }
+      case OpKind::SELECT: return RowBound(o.child());
+      case OpKind::HASH_JOIN:
+        return 2 * std::max<int64_t>(RowBound(o.child(1)), joins_.count(&o) ? joins_.at(&o).build.rows : 0);
+      default: {
+        auto it = mats_.find(&o);
+        return it == mats_.end() ? 1024 : it->second.rows;
+      }
+    }
+  }
   static bool Streamable(const Operator& op) {
     return op.kind == OpKind::SCAN || op.kind == OpKind::SCAN_SELECT || op.kind == OpKind::SELECT ||
            op.kind == OpKind::HASH_JOIN || op.kind == OpKind::SKINNER_JOIN;
@@ -545,9 +623,17 @@ class Executor {
                  const std::function<void(const std::vector<CVal>&, const std::string&)>& on_match);
   std::string JoinHash(ExprGen& eg, const std::vector<CVal>& keys);
 
+  // Kernel symbol for a pipeline role: "group by" -> kdb_group_by.
+  static std::string KernelName(const char* what) {
+    std::string n = "kdb_";
+    for (const char* c = what; *c; c++) n += (*c == ' ') ? '_' : *c;
+    return n;
+  }
+
   void LaunchPipeline(KernelSource& ks, int64_t src_rows, const char* what, int block = 256) {
-    std::string src = ks.Kernel("kdb_pipeline", block);
-    CUfunction f = ctx_.Kernel(src, "kdb_pipeline");
+    std::string name = KernelName(what);
+    std::string src = ks.Kernel(name, block);
+    CUfunction f = ctx_.Kernel(src, name);
     int grid = ctx_.GridFor(std::max<int64_t>(src_rows, 1), block);
     ctx_.Launch(f, grid, block, ks.Args(), 0, what);
   }
@@ -912,23 +998,7 @@ void Executor::PrepareSkinner(const Operator& op) {
 MatBuffer Executor::MaterializeStream(const Operator& op, const uint32_t* order,
                                       const MatBuffer* ordered_src) {
   if (!ordered_src) Prepare(op);
-  std::function<int64_t(const Operator&)> bound = [&](const Operator& o) -> int64_t {
-    switch (o.kind) {
-      case OpKind::SCAN:
-      case OpKind::SCAN_SELECT: {
-        auto it = ctx_.tables.find(o.relation);
-        return it == ctx_.tables.end() ? 0 : std::max<int64_t>(it->second.rows, 0);
-      }
-      case OpKind::SELECT: return bound(o.child());
-      case OpKind::HASH_JOIN:
-        return 2 * std::max<int64_t>(bound(o.child(1)), joins_.count(&o) ? joins_.at(&o).build.rows : 0);
-      default: {
-        auto it = mats_.find(&o);
-        return it == mats_.end() ? 1024 : it->second.rows;
-      }
-    }
-  };
-  int64_t cap = ordered_src ? ordered_src->rows : bound(op);
+  int64_t cap = ordered_src ? ordered_src->rows : RowBound(op);
   for (int attempt = 0; attempt < 3; attempt++) {
     KernelSource ks;
     ExprGen eg(ctx_, ks);
@@ -1142,7 +1212,9 @@ MatBuffer Executor::RunAggregate(const Operator& op) {
         store(static_cast<int>(j) * 2, "t");
         ks.Close();
         break;
-      default: break;
+      default:
+        store(static_cast<int>(j) * 2, "0ULL");
+        break;
     }
     ks.Open("");
     ks.L("int64_t t = kdb_block_reduce(c" + J + ", KdbAddI64(), red_i);");
@@ -1158,8 +1230,8 @@ MatBuffer Executor::RunAggregate(const Operator& op) {
   store(nw - 1, "t");
   ks.Close();
   {
-    std::string src = ks.Kernel("kdb_pipeline", block);
-    CUfunction f = ctx_.Kernel(src, "kdb_pipeline");
+    std::string src = ks.Kernel("kdb_aggregate", block);
+    CUfunction f = ctx_.Kernel(src, "kdb_aggregate");
     ctx_.Launch(f, grid, block, ks.Args(), 0, "aggregate");
   }
 
@@ -1176,41 +1248,30 @@ MatBuffer Executor::RunAggregate(const Operator& op) {
   std::string fp = fk.Ptr(part, "uint64_t", true);
   std::string ftp = fk.Ptr(text_state, "uint64_t", true);
   std::string G = fk.Word(static_cast<uint64_t>(grid));
-  fk.Open("if (blockIdx.x == 0 && threadIdx.x == 0)");
+  {
+    std::vector<WordKind> kinds(nw, WordKind::AddI64);
+    for (size_t j = 0; j < plans.size(); j++) {
+      const AggPlan& p = plans[j];
+      if (p.kind == StateKind::SumF64 || p.kind == StateKind::AvgF64) kinds[j * 2] = WordKind::AddF64;
+      if (p.kind == StateKind::MinMaxKey) kinds[j * 2] = p.is_min ? WordKind::MinU64 : WordKind::MaxU64;
+    }
+    kinds[nw - 1] = WordKind::MinU64;
+    EmitPartialReduce(fk, fp, G, nw, kinds);
+  }
+  fk.Open("if (threadIdx.x == 0)");
   for (size_t j = 0; j < plans.size(); j++) {
     const AggPlan& p = plans[j];
-    std::string J = std::to_string(j);
+    std::string J = std::to_string(j), W = std::to_string(j * 2), C = std::to_string(j * 2 + 1);
     switch (p.kind) {
       case StateKind::SumF64:
-      case StateKind::AvgF64: fk.L("double s" + J + " = 0.0;"); break;
-      case StateKind::MinMaxKey: fk.L("uint64_t s" + J + " = " + (p.is_min ? "~0ULL;" : "0ULL;")); break;
-      default: fk.L("int64_t s" + J + " = 0;"); break;
+      case StateKind::AvgF64: fk.L("double s" + J + " = __longlong_as_double((long long)tot[" + W + "]);"); break;
+      case StateKind::MinMaxKey: fk.L("uint64_t s" + J + " = tot[" + W + "];"); break;
+      default: fk.L("int64_t s" + J + " = (int64_t)tot[" + W + "];"); break;
     }
-    fk.L("int64_t c" + J + " = 0;");
+    fk.L("int64_t c" + J + " = (int64_t)tot[" + C + "];");
   }
-  fk.L("int64_t rows = 0;");
-  fk.L("uint64_t first = ~0ULL;");
-  fk.Open("for (int64_t b = 0; b < (int64_t)" + G + "; b++)");
-  fk.L("const uint64_t* q = " + fp + " + b * " + std::to_string(nw) + ";");
-  for (size_t j = 0; j < plans.size(); j++) {
-    const AggPlan& p = plans[j];
-    std::string J = std::to_string(j), W = std::to_string(j * 2);
-    switch (p.kind) {
-      case StateKind::SumF64:
-      case StateKind::AvgF64:
-        fk.L("s" + J + " = __dadd_rn(s" + J + ", __longlong_as_double((long long)q[" + W + "]));");
-        break;
-      case StateKind::SumI64: fk.L("s" + J + " = (int64_t)((uint64_t)s" + J + " + q[" + W + "]);"); break;
-      case StateKind::MinMaxKey:
-        fk.L("s" + J + " = (q[" + W + "] " + (p.is_min ? "<" : ">") + " s" + J + ") ? q[" + W + "] : s" + J + ";");
-        break;
-      default: break;
-    }
-    fk.L("c" + J + " += (int64_t)q[" + std::to_string(j * 2 + 1) + "];");
-  }
-  fk.L("rows += (int64_t)q[" + std::to_string(nw - 2) + "];");
-  fk.L("first = q[" + std::to_string(nw - 1) + "] < first ? q[" + std::to_string(nw - 1) + "] : first;");
-  fk.Close();
+  fk.L("int64_t rows = (int64_t)tot[" + std::to_string(nw - 2) + "];");
+  fk.L("uint64_t first = tot[" + std::to_string(nw - 1) + "];");
   std::vector<CVal> virt;
   for (size_t j = 0; j < plans.size(); j++) {
     const AggPlan& p = plans[j];
@@ -1251,9 +1312,9 @@ MatBuffer Executor::RunAggregate(const Operator& op) {
   fk.L(posp + "[0] = 0;");
   fk.Close();
   {
-    std::string src = fk.Kernel("kdb_finalize", 32);
-    CUfunction f = ctx_.Kernel(src, "kdb_finalize");
-    ctx_.Launch(f, 1, 32, fk.Args(), 0, "aggregate finalize");
+    std::string src = fk.Kernel("kdb_aggregate_finalize", 256);
+    CUfunction f = ctx_.Kernel(src, "kdb_aggregate_finalize");
+    ctx_.Launch(f, 1, 256, fk.Args(), 0, "aggregate finalize");
   }
   ctx_.CheckDeviceError("aggregate");
   out.rows = 1;
@@ -1325,14 +1386,6 @@ std::string ExprSig(const Expr& e) {
 // reference's AggregateHashTable::UpdateOrInsert hot loop
 // (compile/proxy/aggregate_hash_table.cc:187-243) turns into on a GPU when the
 // group count is tiny.
-enum class WordKind { AddF64, AddI64, MinU64, MaxU64 };
-
-struct DenseWord {
-  WordKind kind;
-  std::string init;   // C initialiser
-  std::string ctype;  // register type
-};
-
 MatBuffer Executor::RunGroupByDense(const Operator& op, const std::vector<AggPlan>& plans,
                                     const KeyLayout& kl) {
   const int64_t D = static_cast<int64_t>(kl.domain);
@@ -1477,8 +1530,8 @@ MatBuffer Executor::RunGroupByDense(const Operator& op, const std::vector<AggPla
   ks.L(PP + "[(int64_t)blockIdx.x * " + std::to_string(K) + " + k] = acc;");
   ks.Close();
   {
-    std::string src = ks.Kernel("kdb_pipeline", block);
-    CUfunction f = ctx_.Kernel(src, "kdb_pipeline");
+    std::string src = ks.Kernel("kdb_group_by_dense", block);
+    CUfunction f = ctx_.Kernel(src, "kdb_group_by_dense");
     ctx_.Launch(f, grid, block, ks.Args(), 0, "group by");
   }
 
@@ -1596,8 +1649,8 @@ MatBuffer Executor::RunGroupByDense(const Operator& op, const std::vector<AggPla
   fk.Close();
   fk.Close();
   {
-    std::string src = fk.Kernel("kdb_finalize", 256);
-    CUfunction f = ctx_.Kernel(src, "kdb_finalize");
+    std::string src = fk.Kernel("kdb_group_by_finalize", 256);
+    CUfunction f = ctx_.Kernel(src, "kdb_group_by_finalize");
     ctx_.Launch(f, 1, 256, fk.Args(), 0, "group by finalize");
   }
   out.rows = ReadU64(ngroups);
@@ -1630,11 +1683,15 @@ MatBuffer Executor::RunGroupBy(const Operator& op) {
       return RunGroupByDense(op, plans, kl);
   }
 
+  // capacity: exact for small key domains; otherwise twice the input-row
+  // bound capped at 2^20 slots (regrown on overflow)
   uint64_t cap = 1024;
   if (kl.small_domain) {
     while (cap < 2 * kl.domain) cap <<= 1;
   } else {
-    cap = 1 << 16;
+    uint64_t want = std::min<uint64_t>(2 * static_cast<uint64_t>(std::max<int64_t>(RowBound(op.child()), 1)),
+                                       1ULL << 20);
+    while (cap < want) cap <<= 1;
   }
   for (int attempt = 0; attempt < 8; attempt++) {
     uint64_t mask = cap - 1;
@@ -1950,8 +2007,8 @@ MatBuffer Executor::SmallOrderBy(const Operator& op, MatBuffer& m) {
     ks.L("for (int64_t j = 0; j < " + N + "; j++) r += (j != i) && less(j, i);");
     ks.L(I + "[r] = (uint32_t)i;");
     ks.Close();
-    std::string src = ks.Kernel("kdb_pipeline", 1024);
-    CUfunction f = ctx_.Kernel(src, "kdb_pipeline");
+    std::string src = ks.Kernel("kdb_order_by_small", 1024);
+    CUfunction f = ctx_.Kernel(src, "kdb_order_by_small");
     ctx_.Launch(f, 1, 1024, ks.Args(), 0, "order by small");
   }
   return MaterializeStream(op, idx, &m);

@@ -226,10 +226,20 @@ KDB_DEV void kdb_join_insert(uint64_t* slots, uint64_t mask, uint32_t h, uint32_
 // `gcount` counts claimed slots; past `limit` (half the capacity) the table
 // reports KDB_DEV_ERR_CAPACITY so the host regrows it, while the remaining
 // free slots keep every probe of this launch short and bounded.
+// Probes stop after KDB_MAX_PROBE slots: with the load kept under one half
+// the expected run is a few slots, so a longer one means the table is
+// overfull and the host must regrow it (never a full-table scan per row).
+#define KDB_MAX_PROBE 4096
+
 KDB_DEV int64_t kdb_group_find_packed(uint64_t* slots, uint64_t mask, uint64_t key,
                                       unsigned long long* gcount, uint64_t limit, int* err) {
+  if (*(volatile unsigned long long*)gcount >= limit) {
+    // already overfull: this launch's result is discarded, stop early
+    kdb_set_error(err, KDB_DEV_ERR_CAPACITY);
+    return -1;
+  }
   uint64_t i = kdb_mix64(key) & mask;
-  for (uint64_t k = 0; k <= mask; k++) {
+  for (uint64_t k = 0; k <= mask && k < KDB_MAX_PROBE; k++) {
     uint64_t s = *(volatile uint64_t*)&slots[i];
     if (s == key) return (int64_t)i;
     if (s == 0) {
@@ -253,8 +263,12 @@ KDB_DEV int64_t kdb_group_find_packed(uint64_t* slots, uint64_t mask, uint64_t k
 template <typename EQ, typename INIT>
 KDB_DEV int64_t kdb_group_find(uint64_t* slots, uint64_t mask, uint64_t h, EQ eq, INIT init,
                                unsigned long long* gcount, uint64_t limit, int* err) {
+  if (*(volatile unsigned long long*)gcount >= limit) {
+    kdb_set_error(err, KDB_DEV_ERR_CAPACITY);
+    return -1;
+  }
   uint64_t i = h & mask;
-  for (uint64_t k = 0; k <= mask; k++) {
+  for (uint64_t k = 0; k <= mask && k < KDB_MAX_PROBE; k++) {
     uint64_t s = *(volatile uint64_t*)&slots[i];
     if (s == 0) {
       uint64_t prev = atomicCAS((unsigned long long*)&slots[i], 0ULL, 1ULL);

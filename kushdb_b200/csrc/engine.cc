@@ -182,11 +182,21 @@ void Context::AddColumn(const std::string& table, const std::string& column, con
   DevTable& t = tables[table];
   CheckRows(t, n, column);
   auto it = t.cols.find(column);
-  if (it != t.cols.end()) FreeColumn(it->second);
+  size_t w = plan::TypeWidth(type.id);
+  if (it != t.cols.end()) {
+    DevColumn& old = it->second;
+    if (old.type == type && old.n == n && (old.nulls != nullptr) == (nulls != nullptr)) {
+      // same shape: refresh the resident buffers in place
+      H2D(old.data, data, w * n);
+      if (nulls) H2D(old.nulls, nulls, n);
+      if (!dry) KDB_CUDA(cudaStreamSynchronize(stream));
+      return;
+    }
+    FreeColumn(old);
+  }
   DevColumn c;
   c.type = type;
   c.n = n;
-  size_t w = plan::TypeWidth(type.id);
   c.bytes = w * n;
   c.data = DevAlloc(std::max<size_t>(c.bytes, 16));
   H2D(c.data, data, c.bytes);
