@@ -113,6 +113,13 @@ int kdb_query_execute(kdb_ctx* ctx, const char* plan_json, kdb_result** out);
  * excluding result download, and the bytes read from table columns. */
 double kdb_last_query_device_ms(kdb_ctx* ctx);
 
+/* ---- device sort (runtime/vector.cc:45-110) ------------------------------
+ * Stable sort of n (key, value) pairs already in device memory by the low
+ * `key_bits` bits of the keys (ties keep their input order); the primitive
+ * under ORDER BY.  Scratch comes from the context's stream-ordered pool; the
+ * call returns when the sort is done. */
+int kdb_sort_pairs(kdb_ctx* ctx, uint64_t* d_keys, uint32_t* d_vals, int64_t n, int32_t key_bits);
+
 /* ---- results (runtime/printer.cc output format) ------------------------ */
 int64_t kdb_result_num_rows(const kdb_result* r);
 int32_t kdb_result_num_cols(const kdb_result* r);

@@ -210,6 +210,16 @@ int kdb_query_execute(kdb_ctx* ctx, const char* plan_json, kdb_result** out) {
   });
 }
 
+int kdb_sort_pairs(kdb_ctx* ctx, uint64_t* d_keys, uint32_t* d_vals, int64_t n, int32_t key_bits) {
+  return Guard(ctx, [&] {
+    if (n < 0 || (n > 0 && (!d_keys || !d_vals))) throw kdb::Error(KDB_ERR_INVALID, "bad sort arguments");
+    if (key_bits < 1 || key_bits > 64) throw kdb::Error(KDB_ERR_INVALID, "key_bits must be in [1, 64]");
+    kdb::Arena arena(*ctx->c);
+    ctx->c->RadixSortPairs(d_keys, d_vals, n, arena, key_bits);
+    if (!ctx->c->dry) KDB_CUDA(cudaStreamSynchronize(ctx->c->stream));
+  });
+}
+
 double kdb_last_query_device_ms(kdb_ctx* ctx) { return ctx ? ctx->c->last_device_ms : -1; }
 
 int64_t kdb_result_num_rows(const kdb_result* r) { return r ? r->r.rows : -1; }

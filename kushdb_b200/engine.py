@@ -29,7 +29,7 @@ EXPORTS = [
     "kdb_enum_open_kdbenum", "kdb_query_execute", "kdb_last_query_device_ms",
     "kdb_result_num_rows", "kdb_result_num_cols", "kdb_result_col_type", "kdb_result_get_i64",
     "kdb_result_get_f64", "kdb_result_get_nulls", "kdb_result_get_text", "kdb_result_format",
-    "kdb_result_free",
+    "kdb_result_free", "kdb_sort_pairs",
 ]
 
 _lib = None
@@ -75,6 +75,7 @@ def load_library(path: str = LIB_PATH):
     L.kdb_query_execute.argtypes = [P, ctypes.c_char_p, ctypes.POINTER(P)]
     L.kdb_last_query_device_ms.restype = ctypes.c_double
     L.kdb_last_query_device_ms.argtypes = [P]
+    L.kdb_sort_pairs.argtypes = [P, P, P, I64, I32]
     declare_result_api(L, "kdb_")
     _lib = L
     return L
@@ -172,6 +173,10 @@ class Engine:
 
     def kernel_launches(self) -> int:
         return self.lib.kdb_ctx_kernel_launches(self.ctx)
+
+    def sort_pairs(self, d_keys: int, d_vals: int, n: int, key_bits: int = 64) -> None:
+        """Stable device sort of n (uint64 key, uint32 value) pairs in place."""
+        self._check(self.lib.kdb_sort_pairs(self.ctx, ctypes.c_void_p(d_keys), ctypes.c_void_p(d_vals), n, key_bits))
 
     def stream_handle(self) -> int:
         return self.lib.kdb_ctx_stream(self.ctx) or 0
