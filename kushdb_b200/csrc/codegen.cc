@@ -152,10 +152,10 @@ class KernelSource {
     return "kdb_mkstr(" + name + ", " + std::to_string(s.size()) + ")";
   }
 
-  std::string Kernel(const std::string& name, int block) const {
+  std::string Kernel(const std::string& name, int block, int min_blocks = 1) const {
     std::ostringstream o;
-    o << globals.str() << "\nextern \"C\" __global__ void __launch_bounds__(" << block << ") "
-      << name << "(KArgs a) {\n"
+    o << globals.str() << "\nextern \"C\" __global__ void __launch_bounds__(" << block << ", " << min_blocks
+      << ") " << name << "(KArgs a) {\n"
       << pre.str() << body.str() << "}\n";
     return o.str();
   }
@@ -727,16 +727,60 @@ void Executor::EmitStream(KernelSource& ks, ExprGen& eg, const Operator& op, con
         np.push_back(c.nulls ? ks.Ptr(c.nulls, "int8_t", true) : "");
         bytes_scanned += static_cast<int64_t>(c.bytes);
       }
-      ks.Open("for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < (int64_t)" + n +
-              "; r += (int64_t)gridDim.x * blockDim.x)");
+      bool any_text = false;
+      for (const DevColumn* c : cols) any_text |= c->type.id == TypeId::TEXT;
+      const bool vec = !any_text && !std::getenv("KDB_NO_VECTOR_SCAN");
       std::vector<CVal> scan(cols.size());
-      auto load = [&](size_t k) {
-        const DevColumn& c = *cols[k];
-        std::string v;
-        if (c.type.id == TypeId::TEXT) v = "kdb_text_at(" + dp[k] + ", " + tp[k] + ", r)";
-        else if (c.type.id == TypeId::BOOLEAN) v = "(" + dp[k] + "[r] != 0)";
-        else v = dp[k] + "[r]";
-        scan[k] = eg.Bind(c.type, v, np[k].empty() ? "false" : "(" + np[k] + "[r] != 0)");
+      std::function<void(size_t)> load;
+      if (vec) {
+        // 4 consecutive rows per thread, every column loaded with vector
+        // loads up front (all loads of an iteration in flight together)
+        ks.L("const int64_t nrows = (int64_t)" + n + ";");
+        ks.Open("for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q * 4 < nrows; q += (int64_t)gridDim.x * blockDim.x)");
+        ks.L("const int64_t base = q * 4;");
+        ks.L("const bool full = base + 4 <= nrows;");
+        std::vector<std::string> arr(cols.size()), narr(cols.size());
+        for (size_t k = 0; k < cols.size(); k++) {
+          const DevColumn& c = *cols[k];
+          std::string st = StoreType(c.type.id);
+          arr[k] = ks.Fresh("L");
+          ks.L(st + " " + arr[k] + "[4];");
+          ks.L("if (full) kdb_ld4(" + dp[k] + ", base, " + arr[k] + "); else for (int u = 0; u < 4; u++) " + arr[k] +
+               "[u] = base + u < nrows ? " + dp[k] + "[base + u] : (" + st + ")0;");
+          if (!np[k].empty()) {
+            narr[k] = ks.Fresh("N");
+            ks.L("int8_t " + narr[k] + "[4];");
+            ks.L("if (full) kdb_ld4(" + np[k] + ", base, " + narr[k] + "); else for (int u = 0; u < 4; u++) " +
+                 narr[k] + "[u] = base + u < nrows ? " + np[k] + "[base + u] : (int8_t)0;");
+          }
+        }
+        ks.L("#pragma unroll");
+        ks.Open("for (int u = 0; u < 4; u++)");
+        ks.L("const int64_t r = base + u;");
+        ks.Open("if (r < nrows)");
+        load = [&, arr, narr](size_t k) {
+          const DevColumn& c = *cols[k];
+          std::string v = c.type.id == TypeId::BOOLEAN ? "(" + arr[k] + "[u] != 0)" : arr[k] + "[u]";
+          scan[k] = eg.Bind(c.type, v, narr[k].empty() ? "false" : "(" + narr[k] + "[u] != 0)");
+        };
+      } else {
+        ks.Open("for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < (int64_t)" + n +
+                "; r += (int64_t)gridDim.x * blockDim.x)");
+        load = [&](size_t k) {
+          const DevColumn& c = *cols[k];
+          std::string v;
+          if (c.type.id == TypeId::TEXT) v = "kdb_text_at(" + dp[k] + ", " + tp[k] + ", r)";
+          else if (c.type.id == TypeId::BOOLEAN) v = "(" + dp[k] + "[r] != 0)";
+          else v = dp[k] + "[r]";
+          scan[k] = eg.Bind(c.type, v, np[k].empty() ? "false" : "(" + np[k] + "[r] != 0)");
+        };
+      }
+      auto close_loop = [&]() {
+        if (vec) {
+          ks.Close();
+          ks.Close();
+        }
+        ks.Close();
       };
       Scope s;
       if (op.kind == OpKind::SCAN) {
@@ -745,7 +789,7 @@ void Executor::EmitStream(KernelSource& ks, ExprGen& eg, const Operator& op, con
         std::vector<CVal> out;
         for (const auto& c : op.output) out.push_back(eg.Emit(*c.expr, s));
         consume(out, "(uint64_t)r");
-        ks.Close();
+        close_loop();
         return;
       }
       for (int k : filter_cols)
@@ -764,7 +808,7 @@ void Executor::EmitStream(KernelSource& ks, ExprGen& eg, const Operator& op, con
       for (const auto& c : op.output) out.push_back(eg.Emit(*c.expr, s));
       consume(out, "(uint64_t)r");
       for (int i = 0; i < opened; i++) ks.Close();
-      ks.Close();
+      close_loop();
       return;
     }
     case OpKind::SELECT: {
@@ -1422,7 +1466,10 @@ MatBuffer Executor::RunGroupByDense(const Operator& op, const std::vector<AggPla
   words.push_back({WordKind::MinU64, "~0ULL", "uint64_t"});
   const int W = static_cast<int>(words.size());
   const int64_t K = D * W;
-  const int block = 256;
+  // block size and the launch-bounds occupancy hint (env overrides for tuning)
+  const int block = std::getenv("KDB_DENSE_BLOCK") ? std::atoi(std::getenv("KDB_DENSE_BLOCK")) : 256;
+  const int min_blocks = std::getenv("KDB_DENSE_MINB") ? std::atoi(std::getenv("KDB_DENSE_MINB")) : 1;
+  const int grid_per_sm = std::getenv("KDB_DENSE_GRID") ? std::atoi(std::getenv("KDB_DENSE_GRID")) : 2;
 
   auto reg = [&](int64_t g, int w) { return "a" + std::to_string(g) + "_" + std::to_string(w); };
   auto combine = [&](WordKind k, const std::string& a, const std::string& b) -> std::string {
@@ -1502,7 +1549,7 @@ MatBuffer Executor::RunGroupByDense(const Operator& op, const std::vector<AggPla
   else EmitMatScan(ks, mats_.at(&op.child()), nullptr, consume, src_rows);
 
   int grid = static_cast<int>(std::min<int64_t>(ctx_.GridFor(std::max<int64_t>(src_rows, 1), block),
-                                                static_cast<int64_t>(ctx_.num_sms) * 2));
+                                                static_cast<int64_t>(ctx_.num_sms) * grid_per_sm));
   uint64_t* part = arena_.AllocT<uint64_t>(static_cast<size_t>(grid) * K);
   std::string PP = ks.Ptr(part, "uint64_t");
   ks.L("__shared__ uint64_t red[" + std::to_string(block / 32) + "][" + std::to_string(K) + "];");
@@ -1530,7 +1577,7 @@ MatBuffer Executor::RunGroupByDense(const Operator& op, const std::vector<AggPla
   ks.L(PP + "[(int64_t)blockIdx.x * " + std::to_string(K) + " + k] = acc;");
   ks.Close();
   {
-    std::string src = ks.Kernel("kdb_group_by_dense", block);
+    std::string src = ks.Kernel("kdb_group_by_dense", block, min_blocks);
     CUfunction f = ctx_.Kernel(src, "kdb_group_by_dense");
     ctx_.Launch(f, grid, block, ks.Args(), 0, "group by");
   }

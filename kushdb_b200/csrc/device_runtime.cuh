@@ -116,6 +116,35 @@ KDB_DEV int32_t kdb_extract_year(int32_t jd) {
   return y - 4800;
 }
 
+// ---- 4-row vector loads ------------------------------------------------------
+// A scan thread loads 4 consecutive rows of each column with 128-bit (or
+// narrower, for 1-2 byte types) streaming loads: every column byte is read
+// exactly once, so evict-first (__ldcs) keeps them from displacing the hash
+// tables in L2.  `base` is a multiple of 4 and the columns are 256-byte
+// aligned, so every vector access is naturally aligned.
+KDB_DEV void kdb_ld4(const int32_t* p, int64_t base, int32_t* o) {
+  int4 v = __ldcs(reinterpret_cast<const int4*>(p + base));
+  o[0] = v.x; o[1] = v.y; o[2] = v.z; o[3] = v.w;
+}
+KDB_DEV void kdb_ld4(const double* p, int64_t base, double* o) {
+  double2 a = __ldcs(reinterpret_cast<const double2*>(p + base));
+  double2 b = __ldcs(reinterpret_cast<const double2*>(p + base + 2));
+  o[0] = a.x; o[1] = a.y; o[2] = b.x; o[3] = b.y;
+}
+KDB_DEV void kdb_ld4(const int64_t* p, int64_t base, int64_t* o) {
+  longlong2 a = __ldcs(reinterpret_cast<const longlong2*>(p + base));
+  longlong2 b = __ldcs(reinterpret_cast<const longlong2*>(p + base + 2));
+  o[0] = a.x; o[1] = a.y; o[2] = b.x; o[3] = b.y;
+}
+KDB_DEV void kdb_ld4(const int16_t* p, int64_t base, int16_t* o) {
+  short4 v = __ldcs(reinterpret_cast<const short4*>(p + base));
+  o[0] = v.x; o[1] = v.y; o[2] = v.z; o[3] = v.w;
+}
+KDB_DEV void kdb_ld4(const int8_t* p, int64_t base, int8_t* o) {
+  char4 v = __ldcs(reinterpret_cast<const char4*>(p + base));
+  o[0] = v.x; o[1] = v.y; o[2] = v.z; o[3] = v.w;
+}
+
 // ---- hashing ----------------------------------------------------------------
 KDB_DEV uint64_t kdb_mix64(uint64_t x) {
   // splitmix64 finaliser

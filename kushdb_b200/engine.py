@@ -161,12 +161,11 @@ class Engine:
         self.register_enums()
         h = ctypes.c_void_p()
         self._check(self.lib.kdb_query_execute(self.ctx, text, ctypes.byref(h)))
-        try:
-            if not fetch:
-                return self.lib.kdb_result_num_rows(h)
-            return Result.from_handle(self.lib, "kdb_", self.ctx, h)
-        finally:
+        if not fetch:
+            n = self.lib.kdb_result_num_rows(h)
             self.lib.kdb_result_free(h)
+            return n
+        return Result.from_handle(self.lib, "kdb_", self.ctx, h)
 
     def last_device_ms(self) -> float:
         return self.lib.kdb_last_query_device_ms(self.ctx)
@@ -190,3 +189,4 @@ class Engine:
         buf = ctypes.create_string_buffer(int(n))
         self.lib.kdb_last_query_kernels(self.ctx, buf, n)
         return json.loads(buf.value.decode())
+

@@ -24,22 +24,58 @@ class ResultColumn:
 
 
 class Result:
-    def __init__(self, columns: List[ResultColumn], lines: List[str]):
-        self.columns = columns
-        self.lines = lines
+    """A query result.  Columns and the printer-format lines are read from
+    the C result handle on first access; the handle is freed with the
+    object."""
+
+    def __init__(self, columns: List[ResultColumn] = None, lines: List[str] = None):
+        self._columns = columns
+        self._lines = lines
+        self._src = None
+
+    @property
+    def columns(self) -> List[ResultColumn]:
+        if self._columns is None:
+            self._columns = self._read_columns()
+        return self._columns
+
+    @property
+    def lines(self) -> List[str]:
+        if self._lines is None:
+            self._lines = self._read_lines()
+        return self._lines
 
     @property
     def num_rows(self) -> int:
+        if self._src is not None and self._columns is None:
+            lib, prefix, _ctx, h = self._src
+            return int(getattr(lib, prefix + "result_num_rows")(h))
         return len(self.columns[0].nulls) if self.columns else 0
 
     def row(self, r: int):
-        out = []
-        for c in self.columns:
-            out.append(None if c.nulls[r] else c.values[r])
-        return out
+        return [None if c.nulls[r] else c.values[r] for c in self.columns]
 
     @staticmethod
     def from_handle(lib, prefix: str, ctx, handle) -> "Result":
+        """Takes ownership of `handle`."""
+        res = Result()
+        res._src = (lib, prefix, ctx, ctypes.c_void_p(handle.value if hasattr(handle, "value") else handle))
+        return res
+
+    def close(self):
+        if self._src is not None:
+            lib, prefix, _ctx, h = self._src
+            getattr(lib, prefix + "result_free")(h)
+            self._src = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _read_columns(self) -> List[ResultColumn]:
+        lib, prefix, _ctx, handle = self._src
         f = lambda n: getattr(lib, prefix + n)  # noqa: E731
         nrows = f("result_num_rows")(handle)
         ncols = f("result_num_cols")(handle)
@@ -69,14 +105,18 @@ class Result:
                 vals = np.zeros(nrows, np.int64)
                 f("result_get_i64")(handle, c, vals.ctypes.data_as(ctypes.c_void_p))
             cols.append(ResultColumn(t, vals, nulls))
+        return cols
+
+    def _read_lines(self) -> List[str]:
+        lib, prefix, ctx, handle = self._src
+        f = lambda n: getattr(lib, prefix + n)  # noqa: E731
         need = f("result_format")(ctx, handle, None, 0)
         tbuf = ctypes.create_string_buffer(int(need))
         f("result_format")(ctx, handle, tbuf, need)
-        text = tbuf.value.decode()
-        lines = text.split("\n")
+        lines = tbuf.value.decode().split("\n")
         if lines and lines[-1] == "":
             lines.pop()
-        return Result(cols, lines)
+        return lines
 
 
 def declare_result_api(lib, prefix: str) -> None:

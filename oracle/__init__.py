@@ -122,10 +122,7 @@ class Oracle:
         self.register_enums()
         h = ctypes.c_void_p()
         self._check(self.lib.kdbo_execute(self.ctx, text.encode(), ctypes.byref(h)))
-        try:
-            return Result.from_handle(self.lib, "kdbo_", self.ctx, h)
-        finally:
-            self.lib.kdbo_result_free(h)
+        return Result.from_handle(self.lib, "kdbo_", self.ctx, h)
 
     def last_exec_seconds(self) -> float:
         return self.lib.kdbo_last_exec_seconds(self.ctx)
