@@ -120,6 +120,27 @@ double kdb_last_query_device_ms(kdb_ctx* ctx);
  * call returns when the sort is done. */
 int kdb_sort_pairs(kdb_ctx* ctx, uint64_t* d_keys, uint32_t* d_vals, int64_t n, int32_t key_bits);
 
+/* The same sort without any device allocation, for callers that cannot
+ * allocate when they sort: code recording a CUDA graph (cudaMalloc is not a
+ * stream operation and breaks the capture), host callbacks and other
+ * contexts where CUDA allocation calls are not allowed, and host engines that
+ * hand out every byte of HBM through their own allocator.  This entry point
+ * has no counterpart in the reference.
+ *
+ * Scratch is one static device array sized for KDB_SORT_NOALLOC_MAX_PAIRS
+ * pairs (12.25 MiB), held by every GPU that loads this library until the
+ * process exits.  n above that limit returns KDB_ERR_CAPACITY without
+ * launching anything.  The work is queued on `stream` (a cudaStream_t; NULL =
+ * legacy default stream) on the current device and the call returns without
+ * waiting.  The first call on each device looks up the array's device address
+ * once (cudaGetSymbolAddress): make that first call before any stream
+ * capture.  Every call shares the one array, so calls whose work overlaps on
+ * the GPU (different streams, or different host threads) race and must be
+ * ordered by the caller. */
+#define KDB_SORT_NOALLOC_MAX_PAIRS (1 << 20)
+int kdb_sort_pairs_noalloc(uint64_t* d_keys, uint32_t* d_vals, int64_t n, int32_t key_bits,
+                           void* stream);
+
 /* ---- results (runtime/printer.cc output format) ------------------------ */
 int64_t kdb_result_num_rows(const kdb_result* r);
 int32_t kdb_result_num_cols(const kdb_result* r);

@@ -11,8 +11,10 @@
 #include <cuda_runtime.h>
 
 #include <cstdint>
+#include <mutex>
 #include <vector>
 
+#include "../../include/kdb_b200.h"
 #include "engine.h"
 
 namespace kdb {
@@ -197,3 +199,94 @@ void Context::RadixSortPairs(uint64_t* keys, uint32_t* vals, int64_t n, Arena& a
 }
 
 }  // namespace kdb
+
+// ---------------------------------------------------------------------------
+// Allocation-free sort entry point.
+//
+// Some callers cannot allocate device memory at the moment they need a sort:
+// code recording a CUDA graph (cudaMalloc is not a stream operation and breaks
+// the capture), host callbacks and driver-owned threads where CUDA
+// allocation calls are not allowed, and host engines that budget every byte
+// of HBM through their own allocator and forbid hidden allocations from a
+// library.  kdb_sort_pairs_noalloc serves them: the radix passes' scratch (a
+// second key/value buffer and the per-block digit histograms) lives in one
+// file-scope __device__ array sized for KDB_SORT_NOALLOC_MAX_PAIRS pairs,
+// which each GPU that loads this library holds until the process exits.
+// ---------------------------------------------------------------------------
+namespace kdb {
+namespace {
+
+constexpr int64_t kNoAllocMaxPairs = KDB_SORT_NOALLOC_MAX_PAIRS;
+constexpr int64_t kNoAllocMaxBlocks = (kNoAllocMaxPairs + kSortTile - 1) / kSortTile;
+constexpr size_t kNoAllocKeyBytes = sizeof(uint64_t) * kNoAllocMaxPairs;
+constexpr size_t kNoAllocValBytes = sizeof(uint32_t) * kNoAllocMaxPairs;
+constexpr size_t kNoAllocHistBytes = sizeof(uint32_t) * 256 * kNoAllocMaxBlocks;
+constexpr size_t kNoAllocScratchBytes = kNoAllocKeyBytes + kNoAllocValBytes + kNoAllocHistBytes;
+
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
+
+// Device address of g_noalloc_scratch per device.  In host code the array's
+// name is only a host-side stand-in, so its device address is looked up once
+// per device, with that device current, through cudaGetSymbolAddress.
+constexpr int kMaxDevices = 64;
+std::mutex g_noalloc_mu;
+void* g_noalloc_addr[kMaxDevices] = {};
+
+int NoAllocScratch(unsigned char** out) {
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return KDB_ERR_CUDA;
+  std::lock_guard<std::mutex> lock(g_noalloc_mu);
+  if (!g_noalloc_addr[dev]) {
+    void* p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess || !p) return KDB_ERR_CUDA;
+    g_noalloc_addr[dev] = p;
+  }
+  *out = static_cast<unsigned char*>(g_noalloc_addr[dev]);
+  return KDB_OK;
+}
+
+}  // namespace
+}  // namespace kdb
+
+extern "C" int kdb_sort_pairs_noalloc(uint64_t* d_keys, uint32_t* d_vals, int64_t n,
+                                      int32_t key_bits, void* stream) {
+  using namespace kdb;
+  if (n < 0 || (n > 0 && (!d_keys || !d_vals)) || key_bits < 1 || key_bits > 64)
+    return KDB_ERR_INVALID;
+  if (n > kNoAllocMaxPairs) return KDB_ERR_CAPACITY;  // scratch holds at most this many pairs
+  unsigned char* scratch = nullptr;
+  int rc = NoAllocScratch(&scratch);
+  if (rc != KDB_OK) return rc;
+  if (n <= 1) return KDB_OK;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  if (n <= kSmallSort) {
+    uint64_t mask = key_bits >= 64 ? ~0ULL : ((1ULL << key_bits) - 1);
+    SmallRankSort<<<1, 1024, 0, s>>>(d_keys, d_vals, static_cast<int>(n), mask);
+    return cudaGetLastError() == cudaSuccess ? KDB_OK : KDB_ERR_CUDA;
+  }
+  int nblocks = static_cast<int>((n + kSortTile - 1) / kSortTile);
+  uint64_t* k2 = reinterpret_cast<uint64_t*>(scratch);
+  uint32_t* v2 = reinterpret_cast<uint32_t*>(scratch + kNoAllocKeyBytes);
+  uint32_t* hist = reinterpret_cast<uint32_t*>(scratch + kNoAllocKeyBytes + kNoAllocValBytes);
+  uint64_t* ka = d_keys;
+  uint32_t* va = d_vals;
+  uint64_t* kb = k2;
+  uint32_t* vb = v2;
+  int passes = (key_bits + 7) / 8;
+  for (int p = 0; p < passes; p++) {
+    int shift = 8 * p;
+    // every histogram entry is rewritten by each pass, so nothing left in the
+    // shared scratch by an earlier call is read
+    RadixHistogram<<<nblocks, kSortBlock, 0, s>>>(ka, n, shift, hist, nblocks);
+    ExclusiveScanSmall<<<1, 1024, 0, s>>>(hist, static_cast<int64_t>(nblocks) * 256);
+    RadixScatter<<<nblocks, kSortBlock, 0, s>>>(ka, va, kb, vb, n, shift, hist, nblocks);
+    std::swap(ka, kb);
+    std::swap(va, vb);
+  }
+  if (ka != d_keys) {
+    int grid = static_cast<int>(std::min<int64_t>((n + 255) / 256, 4096));
+    CopyPairs<<<grid, 256, 0, s>>>(ka, va, d_keys, d_vals, n);
+  }
+  return cudaGetLastError() == cudaSuccess ? KDB_OK : KDB_ERR_CUDA;
+}

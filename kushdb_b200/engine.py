@@ -29,7 +29,7 @@ EXPORTS = [
     "kdb_enum_open_kdbenum", "kdb_query_execute", "kdb_last_query_device_ms",
     "kdb_result_num_rows", "kdb_result_num_cols", "kdb_result_col_type", "kdb_result_get_i64",
     "kdb_result_get_f64", "kdb_result_get_nulls", "kdb_result_get_text", "kdb_result_format",
-    "kdb_result_free", "kdb_sort_pairs",
+    "kdb_result_free", "kdb_sort_pairs", "kdb_sort_pairs_noalloc",
 ]
 
 _lib = None
@@ -76,6 +76,7 @@ def load_library(path: str = LIB_PATH):
     L.kdb_last_query_device_ms.restype = ctypes.c_double
     L.kdb_last_query_device_ms.argtypes = [P]
     L.kdb_sort_pairs.argtypes = [P, P, P, I64, I32]
+    L.kdb_sort_pairs_noalloc.argtypes = [P, P, I64, I32, P]
     declare_result_api(L, "kdb_")
     _lib = L
     return L
@@ -190,3 +191,12 @@ class Engine:
         self.lib.kdb_last_query_kernels(self.ctx, buf, n)
         return json.loads(buf.value.decode())
 
+
+def sort_pairs_noalloc(d_keys: int, d_vals: int, n: int, key_bits: int = 64, stream: int = 0) -> int:
+    """kdb_sort_pairs_noalloc: the device sort with no device allocation
+    (scratch is a static array of KDB_SORT_NOALLOC_MAX_PAIRS pairs).  Queued on
+    `stream` of the current device; returns the C status code (0 = ok,
+    -4 = more pairs than the static scratch holds)."""
+    lib = load_library()
+    return lib.kdb_sort_pairs_noalloc(ctypes.c_void_p(d_keys), ctypes.c_void_p(d_vals), n, key_bits,
+                                      ctypes.c_void_p(stream) if stream else None)
