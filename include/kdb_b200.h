@@ -113,6 +113,14 @@ int kdb_query_execute(kdb_ctx* ctx, const char* plan_json, kdb_result** out);
  * excluding result download, and the bytes read from table columns. */
 double kdb_last_query_device_ms(kdb_ctx* ctx);
 
+/* ---- Skinner join options (runtime/skinner_join_executor.cc:20-22) ------
+ * Work budget per episode (tuples examined, the reference's
+ * --budget_per_episode) and the UCT random seed (--join_seed).  Join order
+ * changes only the emission order, never the result set. */
+int kdb_ctx_set_skinner(kdb_ctx* ctx, int64_t budget_per_episode, uint32_t seed);
+/* Episodes the last SKINNER_JOIN of the last query ran. */
+int64_t kdb_last_skinner_episodes(kdb_ctx* ctx);
+
 /* ---- device sort (runtime/vector.cc:45-110) ------------------------------
  * Stable sort of n (key, value) pairs already in device memory by the low
  * `key_bits` bits of the keys (ties keep their input order); the primitive

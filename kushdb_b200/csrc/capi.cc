@@ -210,6 +210,16 @@ int kdb_query_execute(kdb_ctx* ctx, const char* plan_json, kdb_result** out) {
   });
 }
 
+int kdb_ctx_set_skinner(kdb_ctx* ctx, int64_t budget_per_episode, uint32_t seed) {
+  return Guard(ctx, [&] {
+    if (budget_per_episode < 1) throw kdb::Error(KDB_ERR_INVALID, "budget must be positive");
+    ctx->c->skinner_budget = budget_per_episode;
+    ctx->c->skinner_seed = seed;
+  });
+}
+
+int64_t kdb_last_skinner_episodes(kdb_ctx* ctx) { return ctx ? ctx->c->last_skinner_episodes : -1; }
+
 int kdb_sort_pairs(kdb_ctx* ctx, uint64_t* d_keys, uint32_t* d_vals, int64_t n, int32_t key_bits) {
   return Guard(ctx, [&] {
     if (n < 0 || (n > 0 && (!d_keys || !d_vals))) throw kdb::Error(KDB_ERR_INVALID, "bad sort arguments");

@@ -20,6 +20,7 @@
 #include <cstdio>
 #include <cstring>
 #include <functional>
+#include <random>
 #include <set>
 #include <sstream>
 
@@ -524,7 +525,6 @@ class Executor {
   Arena& arena_;
   std::map<const Operator*, MatBuffer> mats_;
   std::map<const Operator*, JoinTable> joins_;
-  std::map<std::pair<const Operator*, int>, JoinTable> skinner_idx_;
 
   // --- helpers -----------------------------------------------------------
   // Upper bound (or, for joins, an estimate) of the rows a stream produces.
@@ -546,7 +546,7 @@ class Executor {
   }
   static bool Streamable(const Operator& op) {
     return op.kind == OpKind::SCAN || op.kind == OpKind::SCAN_SELECT || op.kind == OpKind::SELECT ||
-           op.kind == OpKind::HASH_JOIN || op.kind == OpKind::SKINNER_JOIN;
+           op.kind == OpKind::HASH_JOIN;
   }
 
   // Reads a device counter.  In a compile-only context it reports 2 rows so
@@ -586,9 +586,6 @@ class Executor {
         BuildJoin(op);
         PrepareInput(op.child(1));
         return;
-      case OpKind::SKINNER_JOIN:
-        PrepareSkinner(op);
-        return;
       default: return;
     }
   }
@@ -612,11 +609,11 @@ class Executor {
   MatBuffer RunAggregate(const Operator& op);
   MatBuffer RunGroupBy(const Operator& op);
   MatBuffer RunOrderBy(const Operator& op);
+  MatBuffer RunSkinner(const Operator& op);
   MatBuffer SmallOrderBy(const Operator& op, MatBuffer& m);
   MatBuffer LargeOrderBy(const Operator& op, MatBuffer& m);
   MatBuffer RunGroupByDense(const Operator& op, const std::vector<AggPlan>& plans, const KeyLayout& kl);
   void BuildJoin(const Operator& op);
-  void PrepareSkinner(const Operator& op);
   JoinTable BuildIndex(const MatBuffer& m, const std::vector<int>& key_cols);
   void EmitProbe(KernelSource& ks, ExprGen& eg, const JoinTable& jt,
                  const std::vector<int>& build_key_cols, const std::vector<CVal>& probe_keys,
@@ -851,84 +848,6 @@ void Executor::EmitStream(KernelSource& ks, ExprGen& eg, const Operator& op, con
       else EmitMatScan(ks, mats_.at(&op.child(1)), nullptr, body, src_rows);
       return;
     }
-    case OpKind::SKINNER_JOIN: {
-      // Fused index-nested-loop over the children in child order: each next
-      // child is reached through a hash index on a column equated with an
-      // already bound child, and every condition is checked as soon as all
-      // its children are bound.  The result set equals the reference's
-      // (permutable_skinner_join_translator.cc:329-912): join order changes
-      // only the emission order.
-      size_t nt = op.children.size();
-      std::vector<std::set<int>> cond_tables(op.conditions.size());
-      std::function<void(const Expr&, std::set<int>&)> collect = [&](const Expr& e, std::set<int>& st) {
-        if (e.kind == ExprKind::ColRef) st.insert(e.child_idx);
-        for (const auto& k : e.kids) collect(*k, st);
-      };
-      for (size_t c = 0; c < op.conditions.size(); c++) collect(*op.conditions[c], cond_tables[c]);
-      Scope s;
-      s.child.resize(nt);
-      std::function<void(size_t, const std::string&)> rec = [&](size_t t, const std::string& pos) {
-        if (t == nt) {
-          std::vector<CVal> out;
-          for (const auto& c : op.output) out.push_back(eg.Emit(*c.expr, s));
-          consume(out, pos);
-          return;
-        }
-        auto bound = [&](const std::vector<CVal>& vals, const std::string& p2) {
-          s.child[t] = vals;
-          int opened = 0;
-          for (size_t c = 0; c < op.conditions.size(); c++) {
-            if (cond_tables[c].empty() || *cond_tables[c].rbegin() != static_cast<int>(t)) continue;
-            CVal v = eg.Emit(*op.conditions[c], s);
-            ks.Open("if (!(" + v.n + ") && " + v.v + ")");
-            opened++;
-          }
-          rec(t + 1, p2);
-          for (int i = 0; i < opened; i++) ks.Close();
-          s.child[t].clear();
-        };
-        const MatBuffer& m = mats_.at(&op.child(t));
-        if (t == 0) {
-          EmitMatScan(ks, m, nullptr, [&](const std::vector<CVal>& vals, const std::string& p) { bound(vals, p); },
-                      src_rows);
-          return;
-        }
-        // an equality condition linking t to a bound child
-        for (size_t c = 0; c < op.conditions.size(); c++) {
-          const Expr& e = *op.conditions[c];
-          if (e.kind != ExprKind::Binary || e.bop != BinOp::EQ) continue;
-          const Expr& a = e.kid(0);
-          const Expr& b = e.kid(1);
-          if (a.kind != ExprKind::ColRef || b.kind != ExprKind::ColRef) continue;
-          const Expr* mine = nullptr;
-          const Expr* other = nullptr;
-          if (a.child_idx == static_cast<int>(t) && b.child_idx < static_cast<int>(t)) {
-            mine = &a;
-            other = &b;
-          } else if (b.child_idx == static_cast<int>(t) && a.child_idx < static_cast<int>(t)) {
-            mine = &b;
-            other = &a;
-          }
-          if (!mine) continue;
-          const JoinTable& jt = skinner_idx_.at({&op, static_cast<int>(t) * 1000 + mine->column_idx});
-          CVal key = s.child[other->child_idx].at(other->column_idx);
-          EmitProbe(ks, eg, jt, {mine->column_idx}, {key},
-                    [&](const std::vector<CVal>& vals, const std::string& bpos) {
-                      bound(vals, "((" + pos + ") * 1000003ULL + (" + bpos + "))");
-                    });
-          return;
-        }
-        // no equality link: nested loop over all rows of child t
-        std::string n = ks.Word(static_cast<uint64_t>(m.rows));
-        std::string it = ks.Fresh("t");
-        ks.Open("for (int64_t " + it + " = 0; " + it + " < (int64_t)" + n + "; " + it + "++)");
-        auto vals = LoadMatRow(ks, eg, m, it, nullptr);
-        bound(vals, "((" + pos + ") * 1000003ULL + (uint64_t)" + it + ")");
-        ks.Close();
-      };
-      rec(0, "0ULL");
-      return;
-    }
     default: {
       EmitMatScan(ks, mats_.at(&op), nullptr, consume, src_rows);
       return;
@@ -1013,27 +932,6 @@ void Executor::BuildJoin(const Operator& op) {
   joins_[&op] = BuildIndex(left, keys);
 }
 
-void Executor::PrepareSkinner(const Operator& op) {
-  for (size_t t = 0; t < op.children.size(); t++)
-    if (!mats_.count(&op.child(t))) mats_[&op.child(t)] = Materialize(op.child(t));
-  for (size_t t = 1; t < op.children.size(); t++) {
-    for (const auto& cp : op.conditions) {
-      const Expr& e = *cp;
-      if (e.kind != ExprKind::Binary || e.bop != BinOp::EQ) continue;
-      const Expr& a = e.kid(0);
-      const Expr& b = e.kid(1);
-      if (a.kind != ExprKind::ColRef || b.kind != ExprKind::ColRef) continue;
-      const Expr* mine = nullptr;
-      if (a.child_idx == static_cast<int>(t) && b.child_idx < static_cast<int>(t)) mine = &a;
-      else if (b.child_idx == static_cast<int>(t) && a.child_idx < static_cast<int>(t)) mine = &b;
-      if (!mine) continue;
-      auto key = std::make_pair(&op, static_cast<int>(t) * 1000 + mine->column_idx);
-      if (!skinner_idx_.count(key))
-        skinner_idx_[key] = BuildIndex(mats_.at(&op.child(t)), {mine->column_idx});
-      break;
-    }
-  }
-}
 
 // Materialise a streamable operator's rows (with stream positions), or, when
 // `ordered_src` is given, project `op.output` over that buffer read in
@@ -1107,6 +1005,7 @@ MatBuffer Executor::Materialize(const Operator& op) {
     case OpKind::AGGREGATE: return RunAggregate(op);
     case OpKind::GROUP_BY_AGGREGATE: return RunGroupBy(op);
     case OpKind::ORDER_BY: return RunOrderBy(op);
+    case OpKind::SKINNER_JOIN: return RunSkinner(op);
     default: return MaterializeStream(op);
   }
 }
@@ -2159,6 +2058,578 @@ MatBuffer Executor::LargeOrderBy(const Operator& op, MatBuffer& m) {
 // ---------------------------------------------------------------------------
 // Result download (runtime/printer.cc formats it on the host)
 // ---------------------------------------------------------------------------
+
+
+// ---------------------------------------------------------------------------
+// Skinner join: adaptive join ordering by UCT over budgeted episodes
+// (permutable_skinner_join_translator.cc:82-994,
+//  runtime/skinner_join_executor.cc:34-879).
+//
+// Reference: each table gets a generated "table function"; the executor's
+// UCT agent picks a join order per episode, runs it for a fixed step budget
+// and resumes it later from a progress tree, deduplicating result tuples in a
+// TupleIdxTable.  Here: one generated kernel whose join order is a runtime
+// argument (like the reference's permutable variant, no recompilation per
+// order) runs an episode as an index-nested-loop over a slice of the leftmost
+// table; the slice is sized so the episode's work (tuples examined) matches
+// the budget.  Exactly-once emission without a dedup table: every table t
+// keeps an offset (tuples of t fully processed while t was leftmost), and
+// every later episode skips those tuples of t in any position, so each result
+// combination is produced by the first episode whose leftmost slice covers
+// one of its tuples.  The join is complete when one table's offset reaches its
+// cardinality.  The UCT search below restates UctNode/UctJoinAgent
+// (skinner_join_executor.cc:559-838): exploration weight 1e-5, untried
+// actions first, connected-table heuristic below the root, random connected
+// playout; reward = 0.5 * progress + 0.5 * results / budget
+// (JoinEnvironment::Reward, :252-274).
+// ---------------------------------------------------------------------------
+
+class JoinEnv {
+ public:
+  virtual ~JoinEnv() = default;
+  virtual bool IsConnected(const std::set<int>& joined, int table) = 0;
+  virtual bool IsComplete() = 0;
+  virtual double Execute(const std::vector<int>& order) = 0;
+};
+
+class UctNode {
+ public:
+  UctNode(int round, int num_tables, JoinEnv& env, const std::vector<int>& already_joined, uint32_t seed)
+      : env_(env), created_in_(round), num_tables_(num_tables),
+        num_actions_(num_tables - static_cast<int>(already_joined.size())), children_(num_actions_),
+        tries_(num_actions_, 0), reward_(num_actions_, 0.0), table_of_action_(num_actions_), rng_(seed) {
+    for (int a = 0; a < num_actions_; a++) {
+      priority_.push_back(a);
+      recommended_.insert(a);
+    }
+    joined_.insert(already_joined.begin(), already_joined.end());
+    int a = 0;
+    for (int t = 0; t < num_tables_; t++)
+      if (!joined_.count(t)) {
+        unjoined_.push_back(t);
+        table_of_action_[a++] = t;
+      }
+  }
+
+  UctNode(int round, UctNode& parent, int joined_table, uint32_t seed)
+      : env_(parent.env_), created_in_(round), num_tables_(parent.num_tables_),
+        num_actions_(parent.num_actions_ - 1), children_(num_actions_), tries_(num_actions_, 0),
+        reward_(num_actions_, 0.0), joined_(parent.joined_), unjoined_(parent.unjoined_),
+        table_of_action_(num_actions_), rng_(seed) {
+    joined_.insert(joined_table);
+    unjoined_.erase(std::find(unjoined_.begin(), unjoined_.end(), joined_table));
+    for (int a = 0; a < num_actions_; a++) table_of_action_[a] = unjoined_[a];
+    // connected-table heuristic (skinner_join_executor.cc:617-630)
+    for (int a = 0; a < num_actions_; a++)
+      if (env_.IsConnected(joined_, table_of_action_[a])) recommended_.insert(a);
+    if (recommended_.empty())
+      for (int a = 0; a < num_actions_; a++) recommended_.insert(a);
+    for (int a = 0; a < num_actions_; a++)
+      if (recommended_.count(a)) priority_.push_back(a);
+  }
+
+  double Sample(int round, std::vector<int>& order) {
+    if (num_actions_ == 0) return env_.Execute(order);
+    int action = SelectAction();
+    int table = table_of_action_[action];
+    order[joined_.size()] = table;
+    if (created_in_ != round && !children_[action])
+      children_[action] = std::make_unique<UctNode>(round, *this, table, static_cast<uint32_t>(rng_()));
+    UctNode* child = children_[action].get();
+    double reward = child ? child->Sample(round, order) : Playout(order);
+    visits_++;
+    tries_[action]++;
+    reward_[action] += reward;
+    return reward;
+  }
+
+ private:
+  double Playout(std::vector<int>& order) {
+    int last = order[joined_.size()];
+    std::set<int> cur(joined_.begin(), joined_.end());
+    cur.insert(last);
+    std::vector<int> rest;
+    for (int t = 0; t < num_tables_; t++)
+      if (!joined_.count(t) && t != last) rest.push_back(t);
+    std::shuffle(rest.begin(), rest.end(), rng_);
+    for (int pos = static_cast<int>(joined_.size()) + 1; pos < num_tables_; pos++) {
+      int pick = -1;
+      for (int t : rest)
+        if (!cur.count(t) && env_.IsConnected(cur, t)) {
+          pick = t;
+          break;
+        }
+      if (pick < 0)
+        for (int t : rest)
+          if (!cur.count(t)) {
+            pick = t;
+            break;
+          }
+      order[pos] = pick;
+      cur.insert(pick);
+    }
+    return env_.Execute(order);
+  }
+
+  int SelectAction() {
+    if (!priority_.empty()) {
+      int idx = static_cast<int>(rng_() % priority_.size());
+      int action = priority_[idx];
+      priority_.erase(priority_.begin() + idx);
+      return action;
+    }
+    int offset = static_cast<int>(rng_() % num_actions_);
+    int best = -1;
+    double best_q = -1;
+    for (int i = 0; i < num_actions_; i++) {
+      int a = (offset + i) % num_actions_;
+      if (!recommended_.count(a)) continue;
+      double q = reward_[a] / tries_[a] + kExploration * std::sqrt(std::log(visits_) / tries_[a]);
+      if (q > best_q) {
+        best = a;
+        best_q = q;
+      }
+    }
+    return best;
+  }
+
+  static constexpr double kExploration = 1e-5;
+  JoinEnv& env_;
+  int created_in_, num_tables_, num_actions_;
+  std::vector<int> priority_;
+  std::vector<std::unique_ptr<UctNode>> children_;
+  int visits_ = 0;
+  std::vector<int> tries_;
+  std::vector<double> reward_;
+  std::set<int> joined_;
+  std::set<int> recommended_;
+  std::vector<int> unjoined_;
+  std::vector<int> table_of_action_;
+  std::default_random_engine rng_;
+};
+
+struct SkinnerPred {  // equality between two children's columns
+  int cond;
+  int ta, ca, tb, cb;
+};
+
+class SkinnerEngine : public JoinEnv {
+ public:
+  SkinnerEngine(Context& ctx, Arena& arena, const Operator& op, std::vector<const MatBuffer*> mats,
+                std::vector<std::vector<JoinTable>> index_for, const std::vector<SkinnerPred>& preds,
+                std::function<MatBuffer(int64_t)> alloc_out, int64_t budget, uint32_t seed)
+      : ctx_(ctx), arena_(arena), op_(op), mats_(std::move(mats)), preds_(preds),
+        alloc_out_(std::move(alloc_out)), budget_(budget), seed_(seed) {
+    T_ = static_cast<int>(mats_.size());
+    for (const MatBuffer* m : mats_) cards_.push_back(m->rows);
+    offsets_.assign(T_, 0);
+    slice_est_.assign(T_, 1024);
+    // tables each condition references
+    std::function<void(const Expr&, uint64_t&)> collect = [&](const Expr& e, uint64_t& m) {
+      if (e.kind == ExprKind::ColRef) m |= 1ULL << e.child_idx;
+      for (const auto& k : e.kids) collect(*k, m);
+    };
+    for (const auto& c : op_.conditions) {
+      uint64_t m = 0;
+      collect(*c, m);
+      cond_tables_.push_back(m);
+    }
+    for (const auto& pr : preds_) {
+      connected_.insert({pr.ta, pr.tb});
+      connected_.insert({pr.tb, pr.ta});
+    }
+    index_for_ = std::move(index_for);
+  }
+
+  bool IsConnected(const std::set<int>& joined, int table) override {
+    for (int t : joined)
+      if (connected_.count({t, table})) return true;
+    return false;
+  }
+  bool IsComplete() override {
+    for (int t = 0; t < T_; t++)
+      if (offsets_[t] >= cards_[t]) return true;
+    return false;
+  }
+
+  MatBuffer Run(const std::vector<int>& prefix) {
+    out_ = alloc_out_(1 << 12);
+    count_ = arena_.AllocT<uint64_t>(1);
+    work_ = arena_.AllocT<uint64_t>(1);
+    ctx_.Memset(count_, 0, sizeof(uint64_t));
+    ctx_.Memset(work_, 0, sizeof(uint64_t));
+    produced_ = 0;
+    bool empty = false;
+    for (int64_t c : cards_) empty |= c == 0;
+    if (!empty) {
+      Generate();
+      std::vector<int> order(T_);
+      for (size_t i = 0; i < prefix.size(); i++) order[i] = prefix[i];
+      UctNode root(0, T_, *this, prefix, seed_);
+      int round = 0;
+      while (!IsComplete() && episodes_ < (ctx_.dry ? 1 : (1 << 24))) {
+        round++;
+        root.Sample(round, order);
+      }
+    }
+    out_.rows = produced_;
+    return out_;
+  }
+
+  int64_t episodes() const { return episodes_; }
+
+  double Execute(const std::vector<int>& order) override {
+    episodes_++;
+    int L = order[0];
+    int64_t remaining = cards_[L] - offsets_[L];
+    int64_t len = std::max<int64_t>(1, std::min<int64_t>(slice_est_[L], remaining));
+    int64_t s0 = offsets_[L], s1 = s0 + len;
+    KArgs a = args_;
+    // order, lookup plan and condition schedule of this order
+    std::vector<int> pos_of(T_);
+    for (int p = 0; p < T_; p++) pos_of[order[p]] = p;
+    uint64_t bound = 0;
+    for (int p = 0; p < T_; p++) {
+      int t = order[p];
+      int lk = -1;
+      int used_pred = -1;
+      if (p > 0)
+        for (size_t j = 0; j < preds_.size() && lk < 0; j++) {
+          const SkinnerPred& pr = preds_[j];
+          if (pr.tb == t && (bound >> pr.ta & 1ULL)) {
+            lk = static_cast<int>(j) * 2;
+            used_pred = pr.cond;
+          } else if (pr.ta == t && (bound >> pr.tb & 1ULL)) {
+            lk = static_cast<int>(j) * 2 + 1;
+            used_pred = pr.cond;
+          }
+        }
+      uint64_t after = bound | (1ULL << t);
+      uint64_t sched = 0;
+      for (size_t c = 0; c < cond_tables_.size(); c++) {
+        uint64_t m = cond_tables_[c];
+        bool ready_now = (m & ~after) == 0 && (p == 0 ? true : (m & ~bound) != 0);
+        if (p == 0 && m == 0) ready_now = true;  // constant conditions at the first table
+        if (ready_now && static_cast<int>(c) != used_pred) sched |= 1ULL << c;
+      }
+      bound = after;
+      a.w[w_order_ + p] = static_cast<uint64_t>(t);
+      a.w[w_lookup_ + p] = static_cast<uint64_t>(static_cast<int64_t>(lk));
+      a.w[w_sched_ + p] = sched;
+    }
+    for (int t = 0; t < T_; t++) a.w[w_off_ + t] = static_cast<uint64_t>(offsets_[t]);
+    a.w[w_s0_] = static_cast<uint64_t>(s0);
+    a.w[w_s1_] = static_cast<uint64_t>(s1);
+    int64_t results = 0, work = 0;
+    for (int attempt = 0; attempt < 8; attempt++) {
+      a.w[w_cap_] = static_cast<uint64_t>(out_.cap);
+      PatchOut(a);
+      ctx_.Launch(fn_, ctx_.GridFor(len, 128), 128, a, 0, "skinner episode");
+      uint64_t cw[2] = {0, 0};
+      ctx_.D2H(&cw[0], count_, sizeof(uint64_t));
+      ctx_.D2H(&cw[1], work_, sizeof(uint64_t));
+      ctx_.CheckDeviceError("skinner episode");
+      int64_t total = static_cast<int64_t>(cw[0]);
+      if (total <= out_.cap || ctx_.dry) {
+        results = total - produced_;
+        work = static_cast<int64_t>(cw[1]);
+        produced_ = ctx_.dry ? 0 : total;
+        break;
+      }
+      Grow(total);  // the slice reruns into the larger buffer
+      uint64_t keep = static_cast<uint64_t>(produced_);
+      ctx_.H2D(count_, &keep, sizeof(uint64_t));
+      ctx_.Memset(work_, 0, sizeof(uint64_t));
+    }
+    ctx_.Memset(work_, 0, sizeof(uint64_t));
+    offsets_[L] = s1;
+    // size the next slice of L so its work matches the budget
+    double per_row = static_cast<double>(std::max<int64_t>(work, 1)) / len;
+    slice_est_[L] = std::max<int64_t>(32, std::min<int64_t>(int64_t(budget_ / per_row), 1LL << 26));
+    double progress = static_cast<double>(len) / static_cast<double>(remaining);
+    return 0.5 * progress + 0.5 * static_cast<double>(results) / static_cast<double>(budget_);
+  }
+
+ private:
+  // Generates the episode kernel once; per-episode values are patched into
+  // reserved argument words.
+  void Generate() {
+    KernelSource ks;
+    ExprGen eg(ctx_, ks);
+    const int T = T_;
+    w_order_ = ks.Arg(0);
+    for (int i = 1; i < T; i++) ks.Arg(0);
+    w_lookup_ = ks.Arg(0);
+    for (int i = 1; i < T; i++) ks.Arg(0);
+    w_sched_ = ks.Arg(0);
+    for (int i = 1; i < T; i++) ks.Arg(0);
+    w_off_ = ks.Arg(0);
+    for (int i = 1; i < T; i++) ks.Arg(0);
+    w_s0_ = ks.Arg(0);
+    w_s1_ = ks.Arg(0);
+    w_cap_ = ks.Arg(0);
+    std::string TS = std::to_string(T);
+    ks.L("int32_t ord[" + TS + "]; int32_t lk[" + TS + "]; uint64_t sched[" + TS + "]; int64_t off[" + TS + "];");
+    ks.L("for (int p = 0; p < " + TS + "; p++) { ord[p] = (int32_t)a.w[" + std::to_string(w_order_) +
+         " + p]; lk[p] = (int32_t)(int64_t)a.w[" + std::to_string(w_lookup_) + " + p]; sched[p] = a.w[" +
+         std::to_string(w_sched_) + " + p]; off[p] = (int64_t)a.w[" + std::to_string(w_off_) + " + p]; }");
+    ks.L("int64_t card[" + TS + "];");
+    for (int t = 0; t < T; t++) ks.L("card[" + std::to_string(t) + "] = (int64_t)" + ks.Word(static_cast<uint64_t>(cards_[t])) + ";");
+    ks.L("const int64_t s0 = (int64_t)a.w[" + std::to_string(w_s0_) + "], s1 = (int64_t)a.w[" + std::to_string(w_s1_) + "];");
+    ks.L("int64_t rows[" + TS + "]; uint64_t iti[" + TS + "]; uint32_t ith[" + TS + "]; int64_t itk[" + TS + "];");
+    ks.L("unsigned long long work = 0;");
+    std::vector<std::vector<std::string>> cache(T);
+    auto load = [&](int t, std::vector<CVal>& out) {
+      out = LoadMat(ks, eg, *mats_[t], "rows[" + std::to_string(t) + "]", &cache[t]);
+    };
+    // conditions
+    ks.Open("auto cond = [&](int c) -> bool");
+    ks.Open("switch (c)");
+    for (size_t c = 0; c < op_.conditions.size(); c++) {
+      ks.Open("case " + std::to_string(c) + ":");
+      Scope sc;
+      sc.child.resize(T);
+      for (int t = 0; t < T; t++)
+        if (cond_tables_[c] >> t & 1ULL) load(t, sc.child[t]);
+      CVal v = eg.Emit(*op_.conditions[c], sc);
+      ks.L("return !(" + v.n + ") && " + v.v + ";");
+      ks.Close();
+    }
+    ks.Close();
+    ks.L("return false;");
+    ks.indent--;
+    ks.L("};");
+    ks.L("auto conds_ok = [&](uint64_t m) -> bool { while (m) { int c = __ffsll((long long)m) - 1; m &= m - 1; if (!cond(c)) return false; } return true; };");
+    // lookups: case 2j probes table tb with the key of ta; 2j+1 the reverse
+    ks.Open("auto init = [&](int p)");
+    ks.Open("switch (lk[p])");
+    ks.L("case -1: iti[p] = 0; itk[p] = 0; break;");
+    for (size_t j = 0; j < preds_.size(); j++)
+      for (int side = 0; side < 2; side++) {
+        const SkinnerPred& pr = preds_[j];
+        int from = side == 0 ? pr.ta : pr.tb, fcol = side == 0 ? pr.ca : pr.cb;
+        int to = side == 0 ? pr.tb : pr.ta;
+        const JoinTable& jt = index_for_[to][side == 0 ? pr.cb : pr.ca];
+        ks.Open("case " + std::to_string(j * 2 + side) + ":");
+        std::vector<CVal> fv;
+        load(from, fv);
+        const CVal& key = fv.at(fcol);
+        ks.Open("if (" + key.n + ")");
+        ks.L("itk[p] = -1;");
+        ks.Close();
+        ks.Open("else");
+        ks.L("uint32_t h = " + JoinHash(eg, {key}) + ";");
+        ks.L("ith[p] = h; iti[p] = kdb_mix64(h) & " + ks.Word(jt.mask) + "; itk[p] = 0;");
+        ks.Close();
+        ks.L("break;");
+        ks.Close();
+      }
+    ks.Close();
+    ks.indent--;
+    ks.L("};");
+    ks.Open("auto next = [&](int p) -> int64_t");
+    ks.Open("switch (lk[p])");
+    ks.L("case -1: { int t = ord[p]; if (iti[p] < (uint64_t)card[t]) return (int64_t)(iti[p]++); return -1; }");
+    for (size_t j = 0; j < preds_.size(); j++)
+      for (int side = 0; side < 2; side++) {
+        const SkinnerPred& pr = preds_[j];
+        int from = side == 0 ? pr.ta : pr.tb, fcol = side == 0 ? pr.ca : pr.cb;
+        int to = side == 0 ? pr.tb : pr.ta, tcol = side == 0 ? pr.cb : pr.ca;
+        const JoinTable& jt = index_for_[to][tcol];
+        ks.Open("case " + std::to_string(j * 2 + side) + ":");
+        std::string slots = ks.Ptr(jt.slots, "uint64_t", true);
+        std::string mask = ks.Word(jt.mask);
+        ks.Open("while (itk[p] >= 0 && (uint64_t)itk[p] <= " + mask + ")");
+        ks.L("uint64_t e = " + slots + "[iti[p]];");
+        ks.Open("if (e == 0)");
+        ks.L("itk[p] = -1;");
+        ks.L("break;");
+        ks.Close();
+        ks.L("iti[p] = (iti[p] + 1) & " + mask + "; itk[p]++;");
+        ks.Open("if ((uint32_t)(e >> 32) == ith[p])");
+        ks.L("int64_t br = (int64_t)(uint32_t)e - 1;");
+        std::vector<CVal> fv;
+        load(from, fv);
+        std::vector<std::string> tcache;
+        auto tv = LoadMat(ks, eg, *mats_[to], "br", &cache[to]);
+        ks.L("if (" + eg.EqOf(tv.at(tcol), fv.at(fcol)) + ") return br;");
+        ks.Close();
+        ks.Close();
+        ks.L("return -1;");
+        ks.Close();
+      }
+    ks.Close();
+    ks.L("return -1;");
+    ks.indent--;
+    ks.L("};");
+    // emission of one result row (output schema over the bound children)
+    out_ptr_words_.clear();
+    ks.Open("auto emit = [&]()");
+    {
+      Scope sc;
+      sc.child.resize(T);
+      for (int t = 0; t < T; t++) load(t, sc.child[t]);
+      std::vector<CVal> vals;
+      for (const auto& c : op_.output) vals.push_back(eg.Emit(*c.expr, sc));
+      int wc = ks.Arg(0);
+      w_count_ = wc;
+      ks.L("uint64_t slot = kdb_alloc_slot((unsigned long long*)a.w[" + std::to_string(wc) + "]);");
+      ks.Open("if (slot < a.w[" + std::to_string(w_cap_) + "])");
+      for (size_t c = 0; c < vals.size(); c++) {
+        const MatCol& mc = out_.cols[c];
+        int wd = ks.Arg(0);
+        out_ptr_words_.push_back(wd);
+        std::string val = vals[c].type.id == TypeId::BOOLEAN ? "(int8_t)(" + vals[c].v + " ? 1 : 0)" : vals[c].v;
+        ks.L("((" + StoreType(mc.type.id) + "*)a.w[" + std::to_string(wd) + "])[slot] = " + val + ";");
+        int wn = ks.Arg(0);
+        out_ptr_words_.push_back(wn);
+        if (mc.nullable) ks.L("((int8_t*)a.w[" + std::to_string(wn) + "])[slot] = (" + vals[c].n + ") ? 1 : 0;");
+      }
+      w_pos_ = ks.Arg(0);
+      ks.L("((uint64_t*)a.w[" + std::to_string(w_pos_) + "])[slot] = slot;");
+      ks.Close();
+    }
+    ks.indent--;
+    ks.L("};");
+    // the episode: DFS over positions for each leftmost tuple of the slice
+    ks.Open("for (int64_t x = s0 + blockIdx.x * (int64_t)blockDim.x + threadIdx.x; x < s1; x += (int64_t)gridDim.x * blockDim.x)");
+    ks.L("rows[ord[0]] = x; work++;");
+    ks.L("if (!conds_ok(sched[0])) continue;");
+    if (T == 1) {
+      ks.L("emit();");
+    } else {
+      ks.L("int p = 1; init(1);");
+      ks.Open("while (p >= 1)");
+      ks.L("int64_t c = next(p);");
+      ks.Open("if (c < 0)");
+      ks.L("p--;");
+      ks.L("continue;");
+      ks.Close();
+      ks.L("int t = ord[p];");
+      ks.L("if (c < off[t]) continue;");
+      ks.L("rows[t] = c; work++;");
+      ks.L("if (!conds_ok(sched[p])) continue;");
+      ks.Open("if (p == " + std::to_string(T - 1) + ")");
+      ks.L("emit();");
+      ks.Close();
+      ks.Open("else");
+      ks.L("p++;");
+      ks.L("init(p);");
+      ks.Close();
+      ks.Close();
+    }
+    ks.Close();
+    std::string wk = ks.Ptr(work_, "unsigned long long");
+    ks.L("if (work) atomicAdd(" + wk + ", work);");
+    std::string src = ks.Kernel("kdb_skinner_episode", 128);
+    fn_ = ctx_.Kernel(src, "kdb_skinner_episode");
+    args_ = ks.Args();
+  }
+
+  void PatchOut(KArgs& a) {
+    a.w[w_count_] = reinterpret_cast<uint64_t>(count_);
+    for (size_t c = 0; c < out_.cols.size(); c++) {
+      a.w[out_ptr_words_[2 * c]] = reinterpret_cast<uint64_t>(out_.cols[c].data);
+      a.w[out_ptr_words_[2 * c + 1]] = reinterpret_cast<uint64_t>(out_.cols[c].nulls);
+    }
+    a.w[w_pos_] = reinterpret_cast<uint64_t>(out_.pos);
+  }
+
+  void Grow(int64_t need) {
+    MatBuffer bigger = alloc_out_(std::max<int64_t>(need, 2 * out_.cap));
+    for (size_t c = 0; c < out_.cols.size(); c++) {
+      size_t w = StoreWidth(out_.cols[c].type.id);
+      if (produced_ && !ctx_.dry)
+        KDB_CUDA(cudaMemcpyAsync(bigger.cols[c].data, out_.cols[c].data, w * produced_, cudaMemcpyDeviceToDevice,
+                                 ctx_.stream));
+      if (out_.cols[c].nulls && produced_ && !ctx_.dry)
+        KDB_CUDA(cudaMemcpyAsync(bigger.cols[c].nulls, out_.cols[c].nulls, produced_, cudaMemcpyDeviceToDevice,
+                                 ctx_.stream));
+    }
+    if (produced_ && !ctx_.dry)
+      KDB_CUDA(cudaMemcpyAsync(bigger.pos, out_.pos, 8 * produced_, cudaMemcpyDeviceToDevice, ctx_.stream));
+    out_ = bigger;
+  }
+
+  std::vector<CVal> LoadMat(KernelSource& ks, ExprGen& eg, const MatBuffer& m, const std::string& row,
+                            std::vector<std::string>* cache) {
+    std::vector<CVal> vals;
+    for (size_t c = 0; c < m.cols.size(); c++) {
+      const MatCol& mc = m.cols[c];
+      if (cache->size() < 2 * m.cols.size()) cache->resize(2 * m.cols.size());
+      if ((*cache)[2 * c].empty()) {
+        (*cache)[2 * c] = ks.Ptr(mc.data, StoreType(mc.type.id), true);
+        (*cache)[2 * c + 1] = mc.nullable ? ks.Ptr(mc.nulls, "int8_t", true) : "";
+      }
+      std::string dp = (*cache)[2 * c], np = (*cache)[2 * c + 1];
+      std::string v = dp + "[" + row + "]";
+      if (mc.type.id == TypeId::BOOLEAN) v = "(" + v + " != 0)";
+      vals.push_back(eg.Bind(mc.type, v, mc.nullable ? "(" + np + "[" + row + "] != 0)" : "false"));
+    }
+    return vals;
+  }
+
+  std::string JoinHash(ExprGen& eg, const std::vector<CVal>& keys) {
+    std::string h = "0x51ed270b27f1a0c9ULL";
+    for (const auto& k : keys) h = "kdb_hash_combine(" + h + ", " + eg.HashOf(k) + ")";
+    return "(uint32_t)((" + h + ") >> 32)";
+  }
+
+  Context& ctx_;
+  Arena& arena_;
+  const Operator& op_;
+  std::vector<const MatBuffer*> mats_;
+  std::vector<SkinnerPred> preds_;
+  std::function<MatBuffer(int64_t)> alloc_out_;
+  int64_t budget_;
+  uint32_t seed_;
+  int T_ = 0;
+  std::vector<int64_t> cards_, offsets_, slice_est_;
+  std::vector<uint64_t> cond_tables_;
+  std::set<std::pair<int, int>> connected_;
+  std::vector<std::vector<JoinTable>> index_for_;
+  MatBuffer out_;
+  uint64_t* count_ = nullptr;
+  uint64_t* work_ = nullptr;
+  int64_t produced_ = 0;
+  int64_t episodes_ = 0;
+  CUfunction fn_ = nullptr;
+  KArgs args_;
+  int w_order_ = 0, w_lookup_ = 0, w_sched_ = 0, w_off_ = 0, w_s0_ = 0, w_s1_ = 0, w_cap_ = 0, w_count_ = 0,
+      w_pos_ = 0;
+  std::vector<int> out_ptr_words_;
+};
+
+MatBuffer Executor::RunSkinner(const Operator& op) {
+  const int T = static_cast<int>(op.children.size());
+  if (T > 16) throw Error(-5, "Skinner join of more than 16 tables");
+  if (op.conditions.size() > 64) throw Error(-5, "Skinner join with more than 64 conditions");
+  for (int t = 0; t < T; t++)
+    if (!mats_.count(&op.child(t))) mats_[&op.child(t)] = Materialize(op.child(t));
+  std::vector<const MatBuffer*> mats;
+  for (int t = 0; t < T; t++) mats.push_back(&mats_.at(&op.child(t)));
+  // equality predicates between two children: the join graph and indexes
+  std::vector<SkinnerPred> preds;
+  for (size_t c = 0; c < op.conditions.size(); c++) {
+    const Expr& e = *op.conditions[c];
+    if (e.kind != ExprKind::Binary || e.bop != BinOp::EQ) continue;
+    const Expr& x = e.kid(0);
+    const Expr& y = e.kid(1);
+    if (x.kind != ExprKind::ColRef || y.kind != ExprKind::ColRef || x.child_idx == y.child_idx) continue;
+    preds.push_back({static_cast<int>(c), x.child_idx, x.column_idx, y.child_idx, y.column_idx});
+  }
+  std::vector<std::vector<JoinTable>> index_for(T);
+  for (int t = 0; t < T; t++) index_for[t].resize(mats[t]->cols.size());
+  for (const auto& pr : preds) {
+    if (!index_for[pr.tb][pr.cb].slots) index_for[pr.tb][pr.cb] = BuildIndex(*mats[pr.tb], {pr.cb});
+    if (!index_for[pr.ta][pr.ca].slots) index_for[pr.ta][pr.ca] = BuildIndex(*mats[pr.ta], {pr.ca});
+  }
+  auto alloc = [&](int64_t cap) { return AllocMat(op.output, cap); };
+  SkinnerEngine eng(ctx_, arena_, op, mats, index_for, preds, alloc, ctx_.skinner_budget, ctx_.skinner_seed);
+  MatBuffer out = eng.Run(op.prefix_order);
+  ctx_.last_skinner_episodes = eng.episodes();
+  return out;
+}
 
 HostResult Executor::Run(const Operator& root) {
   MatBuffer m = Materialize(root);

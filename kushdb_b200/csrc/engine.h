@@ -131,6 +131,11 @@ class Context {
   std::string last_error;
   int64_t kernel_launches = 0;
   double last_device_ms = 0;
+  // Skinner join: work budget per episode (tuples examined) and UCT seed
+  // (runtime/skinner_join_executor.cc:20-22 budget_per_episode / join_seed)
+  int64_t skinner_budget = 1 << 20;
+  uint32_t skinner_seed = 0;
+  int64_t last_skinner_episodes = 0;
 
   // device error word shared by all launches of a query
   int* d_err = nullptr;

@@ -29,7 +29,7 @@ EXPORTS = [
     "kdb_enum_open_kdbenum", "kdb_query_execute", "kdb_last_query_device_ms",
     "kdb_result_num_rows", "kdb_result_num_cols", "kdb_result_col_type", "kdb_result_get_i64",
     "kdb_result_get_f64", "kdb_result_get_nulls", "kdb_result_get_text", "kdb_result_format",
-    "kdb_result_free", "kdb_sort_pairs", "kdb_sort_pairs_noalloc",
+    "kdb_result_free", "kdb_sort_pairs", "kdb_ctx_set_skinner", "kdb_last_skinner_episodes", "kdb_sort_pairs_noalloc",
 ]
 
 _lib = None
@@ -76,6 +76,9 @@ def load_library(path: str = LIB_PATH):
     L.kdb_last_query_device_ms.restype = ctypes.c_double
     L.kdb_last_query_device_ms.argtypes = [P]
     L.kdb_sort_pairs.argtypes = [P, P, P, I64, I32]
+    L.kdb_ctx_set_skinner.argtypes = [P, I64, ctypes.c_uint32]
+    L.kdb_last_skinner_episodes.restype = I64
+    L.kdb_last_skinner_episodes.argtypes = [P]
     L.kdb_sort_pairs_noalloc.argtypes = [P, P, I64, I32, P]
     declare_result_api(L, "kdb_")
     _lib = L
@@ -177,6 +180,13 @@ class Engine:
     def sort_pairs(self, d_keys: int, d_vals: int, n: int, key_bits: int = 64) -> None:
         """Stable device sort of n (uint64 key, uint32 value) pairs in place."""
         self._check(self.lib.kdb_sort_pairs(self.ctx, ctypes.c_void_p(d_keys), ctypes.c_void_p(d_vals), n, key_bits))
+
+    def set_skinner(self, budget_per_episode: int = 1 << 20, seed: int = 0) -> None:
+        """Skinner join episode budget (tuples examined) and UCT seed."""
+        self._check(self.lib.kdb_ctx_set_skinner(self.ctx, budget_per_episode, seed))
+
+    def last_skinner_episodes(self) -> int:
+        return self.lib.kdb_last_skinner_episodes(self.ctx)
 
     def stream_handle(self) -> int:
         return self.lib.kdb_ctx_stream(self.ctx) or 0

@@ -240,3 +240,97 @@ WORKLOADS: Dict[str, str] = {
     "group_by": "Q1-shape group-by, 2 enum keys, 8 aggregates, ORDER BY keys",
     "join_group": "Q3-shape hash join + group-by + ORDER BY sum DESC",
 }
+
+
+# ---------------------------------------------------------------------------
+# Skinner multiway join (JOB-style): 6-8 tables, star or chain
+# ---------------------------------------------------------------------------
+
+PRINTABLE = np.frombuffer(b"abcdefghijklmnopqrstuvwxyzABCDEFGHIJKLMNOPQRSTUVWXYZ0123456789 _-", np.uint8)
+
+
+def random_text(seed: int, n: int, token: str, frac: float, lo: int = 8, hi: int = 40) -> HostColumn:
+    """n random printable strings of length [lo, hi]; a seeded `frac` of them
+    get the 3-char `token` planted (random 3-grams alone almost never match)."""
+    lens = uniform_int(seed, n, lo, hi)
+    off = np.zeros(n + 1, np.int64)
+    off[1:] = np.cumsum(lens)
+    chars = PRINTABLE[splitmix64(seed + 1, int(off[-1])) % np.uint64(len(PRINTABLE))].copy()
+    plant = uniform01(seed + 2, n) < frac
+    where = uniform_int(seed + 3, n, 0, 1 << 30)
+    tok = np.frombuffer(token.encode(), np.uint8)
+    for r in np.nonzero(plant)[0]:
+        L = int(lens[r])
+        p = int(off[r]) + int(where[r] % (L - len(tok) + 1))
+        chars[p:p + len(tok)] = tok
+    return HostColumn("", Type.Text(), offsets=off, chars=chars)
+
+
+def skinner_tables(shape: str = "star", n_tables: int = 6, min_rows: int = 10_000, max_rows: int = 3_000_000,
+                   zipf_s: float = 0.0, seed: int = 5, prefix: str = "j"):
+    """Tables for a multiway join.  star: table 0 is the fact table with a
+    foreign key into each other table's primary key; chain: table i+1 has a
+    foreign key into table i.  Every table has an int32 primary key, and a
+    text column with a planted token on a 2-10% share of rows."""
+    rng_sizes = np.exp(np.log(min_rows) + uniform01(seed, n_tables) * (np.log(max_rows) - np.log(min_rows)))
+    sizes = [int(x) for x in rng_sizes]
+    if shape == "star":  # the fact table is the largest
+        sizes.sort(reverse=True)
+    tables = []
+    tokens = []
+    for i in range(n_tables):
+        n = sizes[i]
+        t = HostTable(f"{prefix}{i}")
+        t.add(HostColumn("pk", Type.Int(), values=np.arange(n, dtype=np.int32)))
+        tok = "".join(chr(c) for c in PRINTABLE[splitmix64(seed + 100 + i, 3) % np.uint64(26)])
+        frac = 0.02 + 0.08 * float(uniform01(seed + 200 + i, 1)[0])
+        txt = random_text(seed + 300 + i, n, tok, frac)
+        txt.name = "note"
+        t.add(txt)
+        tables.append(t)
+        tokens.append(tok)
+    def fk(seed_, n, target_rows):
+        if zipf_s > 0:
+            return (zipf_keys(seed_, n, target_rows, zipf_s) - 1).astype(np.int32)
+        return uniform_int(seed_, n, 0, target_rows - 1).astype(np.int32)
+    if shape == "star":
+        for i in range(1, n_tables):
+            tables[0].add(HostColumn(f"fk{i}", Type.Int(), values=fk(seed + 400 + i, sizes[0], sizes[i])))
+    else:
+        for i in range(1, n_tables):
+            tables[i].add(HostColumn("fk", Type.Int(), values=fk(seed + 400 + i, sizes[i], sizes[i - 1])))
+    return tables, tokens
+
+
+def skinner_plan(tables, tokens, shape: str = "star", like_tables=(1, 2)):
+    """SkinnerJoin of ScanSelect children (LIKE '%tok%' -> CONTAINS on the
+    listed tables) with equality join predicates, under an aggregate
+    COUNT(*), MIN(pk of table 0)."""
+    from .plan import (AggregateOperator, Contains, Min, ScanSelectOperator as SSO, SkinnerJoinOperator)
+    db = catalog_of(tables)
+    children = []
+    for i, t in enumerate(tables):
+        rel = db[t.name]
+        cols = [c for c in t.columns if c != "note"]
+        scan = OperatorSchema()
+        scan.AddGeneratedColumns(rel, cols + (["note"] if i in like_tables else []))
+        filters = [Contains(VirtColRef(scan, "note"), Literal(tokens[i]))] if i in like_tables else []
+        out = OperatorSchema()
+        out.AddVirtualPassthroughColumns(scan, cols)
+        children.append(SSO(out, scan, rel, filters))
+    conds = []
+    if shape == "star":
+        for i in range(1, len(tables)):
+            conds.append(Eq(ColRef(children[0], f"fk{i}", 0), ColRef(children[i], "pk", i)))
+    else:
+        for i in range(1, len(tables)):
+            conds.append(Eq(ColRef(children[i], "fk", i), ColRef(children[i - 1], "pk", i - 1)))
+    js = OperatorSchema()
+    js.AddPassthroughColumns(children[0], ["pk"], 0)
+    join = SkinnerJoinOperator(js, children, conds)
+    cnt = Count()
+    mn = Min(ColRef(join, "pk"))
+    s = OperatorSchema()
+    s.AddDerivedColumn("count", VirtColRef(cnt, 0))
+    s.AddDerivedColumn("min_pk", VirtColRef(mn, 1))
+    return OutputOperator(AggregateOperator(s, join, [cnt, mn]))

@@ -52,6 +52,11 @@ def test_workload_plans_compile_for_sm100a():
     e.execute(wl.scan_agg_plan(t1))
     e.execute(wl.group_by_plan(t2))
     e.execute(wl.join_plan(b, p))
+    for shape in ("star", "chain"):
+        tables, tokens = wl.skinner_tables(shape, 6, min_rows=100, max_rows=1000, prefix=shape)
+        for t in tables:
+            e.register_table(t)
+        e.execute(wl.skinner_plan(tables, tokens, shape))
     assert e.kernel_launches() > 0
     e.close()
 
