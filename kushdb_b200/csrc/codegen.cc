@@ -405,27 +405,40 @@ void EmitPartialReduce(KernelSource& ks, const std::string& part, const std::str
   ks.Open("");
   ks.L("const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;");
   ks.Open("for (int k = warp; k < " + std::to_string(nw) + "; k += blockDim.x / 32)");
-  ks.L("uint64_t acc = 0; bool have = false;");
-  ks.Open("for (int64_t b = lane; b < (int64_t)" + G + "; b += 32)");
-  ks.L("uint64_t y = " + part + "[b * " + std::to_string(nw) + " + k];");
-  ks.Open("if (!have)");
-  ks.L("acc = y; have = true;");
-  ks.Close();
-  ks.Open("else switch (k)");
-  for (int w = 0; w < nw; w++) ks.L("case " + std::to_string(w) + ": acc = " + CombineBits(kinds[w], "acc", "y") + "; break;");
-  ks.Close();
-  ks.Close();
-  ks.Open("for (int o = 16; o > 0; o >>= 1)");
-  ks.L("uint64_t y = __shfl_down_sync(0xffffffffu, acc, o);");
-  ks.L("bool hy = __shfl_down_sync(0xffffffffu, have, o);");
-  ks.Open("if (hy && lane + o < 32)");
-  ks.Open("if (!have)");
-  ks.L("acc = y; have = true;");
-  ks.Close();
-  ks.Open("else switch (k)");
-  for (int w = 0; w < nw; w++) ks.L("case " + std::to_string(w) + ": acc = " + CombineBits(kinds[w], "acc", "y") + "; break;");
-  ks.Close();
-  ks.Close();
+  ks.L("uint64_t acc = 0;");
+  // the word's kind is warp-uniform: one tight loop per kind, identity
+  // elements for lanes past the last block
+  ks.Open("switch (k)");
+  for (int w = 0; w < nw; w++) {
+    ks.Open("case " + std::to_string(w) + ":");
+    switch (kinds[w]) {
+      case WordKind::AddF64:
+        ks.L("{ double x = 0.0; for (int64_t b = lane; b < (int64_t)" + G + "; b += 32) x = __dadd_rn(x, __longlong_as_double((long long)" +
+             part + "[b * " + std::to_string(nw) + " + k]));");
+        ks.L("for (int o = 16; o > 0; o >>= 1) x = __dadd_rn(x, __shfl_down_sync(0xffffffffu, x, o));");
+        ks.L("acc = (uint64_t)__double_as_longlong(x); }");
+        break;
+      case WordKind::AddI64:
+        ks.L("{ uint64_t x = 0; for (int64_t b = lane; b < (int64_t)" + G + "; b += 32) x += " + part + "[b * " +
+             std::to_string(nw) + " + k];");
+        ks.L("for (int o = 16; o > 0; o >>= 1) x += __shfl_down_sync(0xffffffffu, x, o);");
+        ks.L("acc = x; }");
+        break;
+      case WordKind::MinU64:
+      case WordKind::MaxU64: {
+        bool mn = kinds[w] == WordKind::MinU64;
+        std::string cmp = mn ? "<" : ">";
+        ks.L(std::string("{ uint64_t x = ") + (mn ? "~0ULL" : "0ULL") + "; for (int64_t b = lane; b < (int64_t)" + G +
+             "; b += 32) { uint64_t y = " + part + "[b * " + std::to_string(nw) + " + k]; x = y " + cmp + " x ? y : x; }");
+        ks.L("for (int o = 16; o > 0; o >>= 1) { uint64_t y = __shfl_down_sync(0xffffffffu, x, o); x = y " + cmp +
+             " x ? y : x; }");
+        ks.L("acc = x; }");
+        break;
+      }
+    }
+    ks.L("break;");
+    ks.Close();
+  }
   ks.Close();
   ks.L("if (lane == 0) tot[k] = acc;");
   ks.Close();
@@ -987,6 +1000,12 @@ MatBuffer Executor::MaterializeStream(const Operator& op, const uint32_t* order,
       EmitStream(ks, eg, op, sink, src_rows);
     }
     LaunchPipeline(ks, src_rows, "materialize");
+    if (ordered_src) {
+      // every row r is written at index r: the count is known without a
+      // read-back (device errors surface at the next synchronisation)
+      out.rows = ordered_src->rows;
+      return out;
+    }
     int64_t produced = ReadU64(counter);
     ctx_.CheckDeviceError("materialize");
     if (produced <= out.cap) {
@@ -1490,44 +1509,12 @@ MatBuffer Executor::RunGroupByDense(const Operator& op, const std::vector<AggPla
   std::string FP = fk.Ptr(part, "uint64_t", true);
   std::string NG = fk.Ptr(ngroups, "uint64_t");
   std::string GW = "(int64_t)" + fk.Word(static_cast<uint64_t>(grid));
-  fk.L("__shared__ uint64_t tot[" + std::to_string(K) + "];");
   fk.L("__shared__ int32_t order[" + std::to_string(D) + "];");
-  fk.L("const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;");
-  fk.Open("for (int k = warp; k < " + std::to_string(K) + "; k += blockDim.x / 32)");
-  fk.L("int w = k % " + std::to_string(W) + ";");
-  fk.L("uint64_t acc = 0; bool have = false;");
-  fk.Open("for (int64_t b = lane; b < " + GW + "; b += 32)");
-  fk.L("uint64_t y = " + FP + "[b * " + std::to_string(K) + " + k];");
-  fk.Open("if (!have)");
-  fk.L("acc = y; have = true;");
-  fk.Close();
-  fk.Open("else");
-  fk.Open("switch (w)");
-  for (int w = 0; w < W; w++)
-    fk.L("case " + std::to_string(w) + ": acc = " +
-         to_bits(words[w], combine(words[w].kind, from_bits(words[w], "acc"), from_bits(words[w], "y"))) + "; break;");
-  fk.Close();
-  fk.Close();
-  fk.Close();
-  fk.Open("for (int o = 16; o > 0; o >>= 1)");
-  fk.L("uint64_t y = __shfl_down_sync(0xffffffffu, acc, o);");
-  fk.L("bool hy = __shfl_down_sync(0xffffffffu, have, o);");
-  fk.Open("if (hy && lane + o < 32)");
-  fk.Open("if (!have)");
-  fk.L("acc = y; have = true;");
-  fk.Close();
-  fk.Open("else");
-  fk.Open("switch (w)");
-  for (int w = 0; w < W; w++)
-    fk.L("case " + std::to_string(w) + ": acc = " +
-         to_bits(words[w], combine(words[w].kind, from_bits(words[w], "acc"), from_bits(words[w], "y"))) + "; break;");
-  fk.Close();
-  fk.Close();
-  fk.Close();
-  fk.Close();
-  fk.L("if (lane == 0) tot[k] = acc;");
-  fk.Close();
-  fk.L("__syncthreads();");
+  {
+    std::vector<WordKind> kinds(K);
+    for (int64_t k = 0; k < K; k++) kinds[k] = words[k % W].kind;
+    EmitPartialReduce(fk, FP, GW, static_cast<int>(K), kinds);
+  }
   fk.Open("if (threadIdx.x == 0)");
   fk.L("int32_t ng = 0;");
   fk.Open("for (int32_t g = 0; g < " + std::to_string(D) + "; g++)");
@@ -2223,7 +2210,9 @@ class SkinnerEngine : public JoinEnv {
     T_ = static_cast<int>(mats_.size());
     for (const MatBuffer* m : mats_) cards_.push_back(m->rows);
     offsets_.assign(T_, 0);
-    slice_est_.assign(T_, 1024);
+    // first slice of each leftmost table: a share of the budget (later
+    // slices are sized from the measured work per leftmost tuple)
+    slice_est_.assign(T_, std::max<int64_t>(1, std::min<int64_t>(budget_ / 64, 65536)));
     // tables each condition references
     std::function<void(const Expr&, uint64_t&)> collect = [&](const Expr& e, uint64_t& m) {
       if (e.kind == ExprKind::ColRef) m |= 1ULL << e.child_idx;
@@ -2345,7 +2334,7 @@ class SkinnerEngine : public JoinEnv {
     offsets_[L] = s1;
     // size the next slice of L so its work matches the budget
     double per_row = static_cast<double>(std::max<int64_t>(work, 1)) / len;
-    slice_est_[L] = std::max<int64_t>(32, std::min<int64_t>(int64_t(budget_ / per_row), 1LL << 26));
+    slice_est_[L] = std::max<int64_t>(1, std::min<int64_t>(int64_t(budget_ / per_row), 1LL << 26));
     double progress = static_cast<double>(len) / static_cast<double>(remaining);
     return 0.5 * progress + 0.5 * static_cast<double>(results) / static_cast<double>(budget_);
   }
@@ -2636,31 +2625,53 @@ HostResult Executor::Run(const Operator& root) {
   const auto& schema = SchemaOf(root);
   HostResult res;
   res.rows = m.rows;
+  // one batch of device->host copies into the context's pinned staging
+  // buffer and a single synchronisation (not one per column)
+  std::vector<size_t> data_off(m.cols.size()), null_off(m.cols.size());
+  size_t total = 0;
+  for (size_t c = 0; c < m.cols.size(); c++) {
+    data_off[c] = total;
+    total += (StoreWidth(m.cols[c].type.id) * m.rows + 15) & ~size_t(15);
+    null_off[c] = total;
+    if (m.cols[c].nulls) total += (static_cast<size_t>(m.rows) + 15) & ~size_t(15);
+  }
+  char* stage = static_cast<char*>(ctx_.HostStage(total));
+  if (m.rows > 0 && !ctx_.dry) {
+    for (size_t c = 0; c < m.cols.size(); c++) {
+      const MatCol& mc = m.cols[c];
+      KDB_CUDA(cudaMemcpyAsync(stage + data_off[c], mc.data, StoreWidth(mc.type.id) * m.rows,
+                               cudaMemcpyDeviceToHost, ctx_.stream));
+      if (mc.nulls)
+        KDB_CUDA(cudaMemcpyAsync(stage + null_off[c], mc.nulls, m.rows, cudaMemcpyDeviceToHost, ctx_.stream));
+    }
+    KDB_CUDA(cudaStreamSynchronize(ctx_.stream));
+  } else if (total) {
+    std::memset(stage, 0, total);
+  }
   for (size_t c = 0; c < m.cols.size(); c++) {
     const MatCol& mc = m.cols[c];
     HostColumn hc;
     hc.name = schema[c].name;
     hc.type = mc.type;
-    hc.null.assign(m.rows, 0);
-    if (mc.nulls && m.rows) ctx_.D2H(hc.null.data(), mc.nulls, m.rows);
+    if (mc.nulls) hc.null.assign(stage + null_off[c], stage + null_off[c] + m.rows);
+    else hc.null.assign(m.rows, 0);
     size_t w = StoreWidth(mc.type.id);
-    std::vector<char> raw(w * m.rows);
-    if (m.rows) ctx_.D2H(raw.data(), mc.data, raw.size());
+    const char* raw = stage + data_off[c];
     switch (mc.type.id) {
       case TypeId::REAL: {
         hc.f.resize(m.rows);
-        std::memcpy(hc.f.data(), raw.data(), raw.size());
+        if (m.rows) std::memcpy(hc.f.data(), raw, w * m.rows);
         break;
       }
       case TypeId::TEXT: {
-        const DevStr* ds = reinterpret_cast<const DevStr*>(raw.data());
+        const DevStr* ds = reinterpret_cast<const DevStr*>(raw);
         std::vector<int64_t> off(m.rows + 1, 0);
         for (int64_t r = 0; r < m.rows; r++) off[r + 1] = off[r] + (hc.null[r] ? 0 : ds[r].len);
-        int64_t total = off[m.rows];
+        int64_t nbytes = off[m.rows];
         hc.s.resize(m.rows);
-        if (total > 0) {
+        if (nbytes > 0) {
           int64_t* d_off = arena_.AllocT<int64_t>(m.rows + 1);
-          char* d_chars = arena_.AllocT<char>(total);
+          char* d_chars = arena_.AllocT<char>(nbytes);
           ctx_.H2D(d_off, off.data(), sizeof(int64_t) * (m.rows + 1));
           KernelSource ks;
           std::string D = ks.Ptr(mc.data, "kdb_str", true), O = ks.Ptr(d_off, "int64_t", true);
@@ -2672,8 +2683,8 @@ HostResult Executor::Run(const Operator& root) {
           ks.L("for (int64_t b = 0; b < len; b++) " + CH + "[" + O + "[r] + b] = " + D + "[r].p[b];");
           ks.Close();
           LaunchPipeline(ks, m.rows, "text download");
-          std::vector<char> chars(total);
-          ctx_.D2H(chars.data(), d_chars, total);
+          std::vector<char> chars(nbytes);
+          ctx_.D2H(chars.data(), d_chars, nbytes);
           for (int64_t r = 0; r < m.rows; r++) hc.s[r].assign(chars.data() + off[r], off[r + 1] - off[r]);
         }
         break;
@@ -2681,7 +2692,7 @@ HostResult Executor::Run(const Operator& root) {
       default: {
         hc.i.resize(m.rows);
         for (int64_t r = 0; r < m.rows; r++) {
-          const char* p = raw.data() + w * r;
+          const char* p = raw + w * r;
           switch (mc.type.id) {
             case TypeId::BOOLEAN: hc.i[r] = *reinterpret_cast<const int8_t*>(p); break;
             case TypeId::SMALLINT: hc.i[r] = *reinterpret_cast<const int16_t*>(p); break;

@@ -119,6 +119,20 @@ void Context::D2H(void* h, const void* d, size_t bytes) {
   KDB_CUDA(cudaStreamSynchronize(stream));
 }
 
+void* Context::HostStage(size_t bytes) {
+  if (bytes <= stage_bytes_ && stage_) return stage_;
+  size_t want = std::max<size_t>(bytes, 1 << 20);
+  if (dry) {
+    std::free(stage_);
+    stage_ = std::malloc(want);
+  } else {
+    if (stage_) cudaFreeHost(stage_);
+    KDB_CUDA(cudaMallocHost(&stage_, want));
+  }
+  stage_bytes_ = want;
+  return stage_;
+}
+
 // ---------------------------------------------------------------------------
 // Context
 // ---------------------------------------------------------------------------
@@ -144,7 +158,11 @@ Context::Context(int dev) : device(dev) {
 }
 
 Context::~Context() {
-  if (dry) return;
+  if (dry) {
+    std::free(stage_);
+    return;
+  }
+  if (stage_) cudaFreeHost(stage_);
   cudaSetDevice(device);
   cudaStreamSynchronize(stream);
   for (auto& [n, t] : tables)

@@ -175,6 +175,8 @@ class Context {
   void Memset(void* d, int v, size_t bytes);
   void H2D(void* d, const void* h, size_t bytes);
   void D2H(void* h, const void* d, size_t bytes);  // synchronous
+  // Pinned host staging buffer of at least `bytes` (reused across queries).
+  void* HostStage(size_t bytes);
 
   // Static kernels (kernels.cu).
   void RadixSortPairs(uint64_t* keys, uint32_t* vals, int64_t n, Arena& arena, int key_bits = 64);
@@ -184,6 +186,8 @@ class Context {
 
  private:
   std::unordered_map<std::string, std::unique_ptr<Program>> programs_;
+  void* stage_ = nullptr;
+  size_t stage_bytes_ = 0;
   void FreeColumn(DevColumn& c);
 };
 
