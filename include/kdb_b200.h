@@ -149,6 +149,48 @@ int kdb_sort_pairs(kdb_ctx* ctx, uint64_t* d_keys, uint32_t* d_vals, int64_t n, 
 int kdb_sort_pairs_noalloc(uint64_t* d_keys, uint32_t* d_vals, int64_t n, int32_t key_bits,
                            void* stream);
 
+/* ---- batched form ----------------------------------------------------------
+ * Many queries of one template, run together as a captured CUDA graph of
+ * fused kernels (one launch per phase for all queries):
+ *   SELECT d.key, SUM(f.price * (1 - f.disc)) FROM dim d JOIN fact f
+ *   ON f.fk = d.key WHERE d.date < date_lt AND d.seg = seg GROUP BY d.key
+ * i.e. HashJoin(ScanSelect(dim), Scan(fact)) -> GroupByAggregate
+ * (hash_join_translator.cc:34-139, group_by_aggregate_translator.cc:36-111)
+ * with per-query constants.  The dimension key must be unique (a primary
+ * key); kdb_batch_run reports KDB_ERR_UNSUPPORTED otherwise.  Columns are
+ * registered tables' columns (int32 key/date/seg/fk, REAL price/disc). */
+typedef struct kdb_batch kdb_batch;
+typedef struct {
+  const char* dim_table;
+  const char* dim_key;
+  const char* dim_date;
+  const char* dim_seg;
+  const char* fact_table;
+  const char* fact_fk;
+  const char* fact_price;
+  const char* fact_disc;
+  int32_t date_lt;
+  int32_t seg;
+} kdb_batch_query;
+int kdb_batch_create(kdb_ctx* ctx, const kdb_batch_query* queries, int32_t n, kdb_batch** out);
+/* block in {128,256,512}, load factor of the join tables in (0.05, 0.95],
+ * fanout = power-of-two number of join sub-tables per query (radix
+ * partitioning by the key hash's top bits). */
+int kdb_batch_configure(kdb_batch* b, int32_t block, double load_factor, int32_t fanout);
+/* Autotuner: times every block x load factor {0.5,0.7,0.9} x fanout
+ * {1,64,256,1024} configuration (`reps` replays each), keeps the fastest;
+ * writes a JSON report of all timings into `report`. */
+int kdb_batch_tune(kdb_batch* b, int32_t reps, char* report, int64_t cap);
+int kdb_batch_config(kdb_batch* b, int32_t* block, double* load_factor, int32_t* fanout);
+/* Runs all queries (graph replay) and waits. */
+int kdb_batch_run(kdb_batch* b);
+/* Mean device ms per batch over `reps` replays (CUDA events), -1 on error. */
+double kdb_batch_run_timed(kdb_batch* b, int32_t reps);
+/* Query q's groups (key, sum) in the order the fact stream first reaches
+ * them; returns the group count (copies at most `cap`). */
+int64_t kdb_batch_result(kdb_batch* b, int32_t q, int32_t* keys, double* sums, int64_t cap);
+void kdb_batch_free(kdb_batch* b);
+
 /* ---- results (runtime/printer.cc output format) ------------------------ */
 int64_t kdb_result_num_rows(const kdb_result* r);
 int32_t kdb_result_num_cols(const kdb_result* r);

@@ -42,6 +42,11 @@ std::vector<char> ReadFile(const std::string& path) {
 
 }  // namespace
 
+kdb::Context* kdb_ctx_context(kdb_ctx* ctx) { return ctx->c.get(); }
+void kdb_ctx_set_error(kdb_ctx* ctx, const std::string& msg) {
+  if (ctx) ctx->err = msg;
+}
+
 extern "C" {
 
 int kdb_ctx_create(int device, kdb_ctx** out) {

@@ -231,14 +231,21 @@ class ExprGen {
       case ExprKind::ColRef: return s.Child(e.child_idx).at(e.column_idx);
       case ExprKind::VirtColRef: return s.virt.at(e.column_idx);
       case ExprKind::Literal: {
+        // numeric literals travel as kernel argument words, so queries that
+        // differ only in their constants share one compiled pipeline
         std::string v;
         switch (e.type.id) {
-          case TypeId::REAL: v = F64Lit(e.fval); break;
+          case TypeId::REAL: {
+            uint64_t bits;
+            std::memcpy(&bits, &e.fval, 8);
+            v = "__longlong_as_double((long long)" + ks_.Word(bits) + ")";
+            break;
+          }
           case TypeId::TEXT: v = ks_.Lit(e.sval); break;
-          case TypeId::BOOLEAN: v = e.ival ? "true" : "false"; break;
-          case TypeId::BIGINT: v = I64Lit(e.ival); break;
-          case TypeId::SMALLINT: v = "(int16_t)" + std::to_string(e.ival); break;
-          default: v = "(int32_t)(" + std::to_string(e.ival) + "LL)"; break;
+          case TypeId::BOOLEAN: v = "(" + ks_.Word(e.ival ? 1 : 0) + " != 0)"; break;
+          case TypeId::BIGINT: v = "(int64_t)" + ks_.Word(static_cast<uint64_t>(e.ival)); break;
+          case TypeId::SMALLINT: v = "(int16_t)(int64_t)" + ks_.Word(static_cast<uint64_t>(e.ival)); break;
+          default: v = "(int32_t)(int64_t)" + ks_.Word(static_cast<uint64_t>(e.ival)); break;
         }
         return CVal{e.type, v, e.lit_null ? "true" : "false"};
       }
@@ -1004,6 +1011,7 @@ MatBuffer Executor::MaterializeStream(const Operator& op, const uint32_t* order,
       // every row r is written at index r: the count is known without a
       // read-back (device errors surface at the next synchronisation)
       out.rows = ordered_src->rows;
+      out.pos_is_index = true;
       return out;
     }
     int64_t produced = ReadU64(counter);
@@ -1280,6 +1288,7 @@ MatBuffer Executor::RunAggregate(const Operator& op) {
   }
   ctx_.CheckDeviceError("aggregate");
   out.rows = 1;
+  out.pos_is_index = true;
   return out;
 }
 
@@ -1588,6 +1597,7 @@ MatBuffer Executor::RunGroupByDense(const Operator& op, const std::vector<AggPla
   }
   out.rows = ReadU64(ngroups);
   ctx_.CheckDeviceError("group by");
+  out.pos_is_index = true;
   return out;
 }
 
@@ -1630,7 +1640,6 @@ MatBuffer Executor::RunGroupBy(const Operator& op) {
     uint64_t mask = cap - 1;
     uint64_t* slots = arena_.AllocT<uint64_t>(cap);
     uint64_t* first = arena_.AllocT<uint64_t>(cap);
-    uint64_t* gcount = arena_.AllocT<uint64_t>(1);
     std::vector<uint64_t*> kw(nk), sv(plans.size()), sc(plans.size());
     std::vector<int32_t*> klen(nk);
     std::vector<int8_t*> kn(nk);
@@ -1644,7 +1653,6 @@ MatBuffer Executor::RunGroupBy(const Operator& op) {
       sv[j] = arena_.AllocT<uint64_t>(cap);
       sc[j] = arena_.AllocT<uint64_t>(cap);
     }
-    ctx_.Memset(gcount, 0, sizeof(uint64_t));
     // init kernel
     {
       KernelSource ks;
@@ -1666,8 +1674,7 @@ MatBuffer Executor::RunGroupBy(const Operator& op) {
       KernelSource ks;
       ExprGen eg(ctx_, ks);
       std::string S = ks.Ptr(slots, "uint64_t"), F = ks.Ptr(first, "uint64_t");
-      std::string M = "(uint64_t)" + ks.Word(mask), GC = ks.Ptr(gcount, "unsigned long long");
-      std::string LIM = "(uint64_t)" + ks.Word(cap / 2);
+      std::string M = "(uint64_t)" + ks.Word(mask);
       std::string ERR = ks.Ptr(ctx_.d_err, "int");
       std::vector<std::string> KW(nk), KL(nk), KN(nk), SV(plans.size()), SC(plans.size());
       if (!kl.packed)
@@ -1705,8 +1712,7 @@ MatBuffer Executor::RunGroupBy(const Operator& op) {
             if (kl.nullable[k])
               pk += " | ((" + c.n + ") ? (1ULL << " + std::to_string(kl.offset[k] + kl.width[k]) + ") : 0ULL)";
           }
-          ks.L("int64_t " + g + " = kdb_group_find_packed(" + S + ", " + M + ", " + pk + ", " + GC + ", " + LIM +
-               ", " + ERR + ");");
+          ks.L("int64_t " + g + " = kdb_group_find_packed(" + S + ", " + M + ", " + pk + ", " + ERR + ");");
         } else {
           std::string h = "0x2545f4914f6cdd1dULL";
           for (size_t k = 0; k < nk; k++)
@@ -1740,7 +1746,7 @@ MatBuffer Executor::RunGroupBy(const Operator& op) {
           }
           ks.L("int64_t " + g + " = kdb_group_find(" + S + ", " + M + ", (" + h +
                ") | 0x8000000000000000ULL, [&](uint64_t i) { return " + eq + "; }, [&](uint64_t i) { " + init +
-               "}, " + GC + ", " + LIM + ", " + ERR + ");");
+               "}, " + ERR + ");");
         }
         ks.Open("if (" + g + " >= 0)");
         std::string fl = "0ULL";
@@ -1862,6 +1868,7 @@ MatBuffer Executor::RunGroupBy(const Operator& op) {
     }
     ctx_.CheckDeviceError("group output");
     out.rows = ng;
+    out.pos_is_index = true;
     return out;
   }
   throw Error(-4, "group table did not fit");
@@ -1965,18 +1972,27 @@ MatBuffer Executor::LargeOrderBy(const Operator& op, MatBuffer& m) {
     LaunchPipeline(ks, n, "order key");
   };
   if (n > 1) {
-    // stream order
-    std::string dummy;
-    keygen([&](KernelSource& ks, ExprGen&, const std::string& I) {
-      std::string P = ks.Ptr(m.pos, "uint64_t", true);
-      ks.L(I + "[i] = (uint32_t)i;");
-      return P + "[i]";
-    });
-    ctx_.RadixSortPairs(keys, idx, n, arena_, 64);
+    // stream order (skipped when the rows already are in it)
+    if (m.pos_is_index) {
+      keygen([&](KernelSource& ks, ExprGen&, const std::string& I) {
+        ks.L(I + "[i] = (uint32_t)i;");
+        return std::string("0ULL");
+      });
+    } else {
+      keygen([&](KernelSource& ks, ExprGen&, const std::string& I) {
+        std::string P = ks.Ptr(m.pos, "uint64_t", true);
+        ks.L(I + "[i] = (uint32_t)i;");
+        return P + "[i]";
+      });
+      ctx_.RadixSortPairs(keys, idx, n, arena_, 64);
+    }
+    // the tie key uses at most depth = ceil(log2 n) + 1 leading bits
+    int depth = 1;
+    while ((1LL << (depth - 1)) < n) depth++;
     keygen([&](KernelSource&, ExprGen&, const std::string&) {
-      return "kdb_tie_path((uint64_t)i, " + std::to_string(n) + "ULL)";
+      return "(kdb_tie_path((uint64_t)i, " + std::to_string(n) + "ULL) >> " + std::to_string(64 - depth) + ")";
     });
-    ctx_.RadixSortPairs(keys, idx, n, arena_, 64);
+    ctx_.RadixSortPairs(keys, idx, n, arena_, depth);
     const auto& child_schema = SchemaOf(op.child());
     for (int k = static_cast<int>(op.sort_keys.size()) - 1; k >= 0; k--) {
       int col = op.sort_keys[k]->column_idx;

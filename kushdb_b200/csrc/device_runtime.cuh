@@ -252,32 +252,21 @@ KDB_DEV void kdb_join_insert(uint64_t* slots, uint64_t mask, uint32_t h, uint32_
 // ---- group tables ------------------------------------------------------------
 // Packed keys: the whole group key fits in 63 bits; the slot word holds
 // key | 1<<63 and is claimed by a single CAS (no wait on other threads).
-// `gcount` counts claimed slots; past `limit` (half the capacity) the table
-// reports KDB_DEV_ERR_CAPACITY so the host regrows it, while the remaining
-// free slots keep every probe of this launch short and bounded.
-// Probes stop after KDB_MAX_PROBE slots: with the load kept under one half
-// the expected run is a few slots, so a longer one means the table is
-// overfull and the host must regrow it (never a full-table scan per row).
-#define KDB_MAX_PROBE 4096
+// Overflow detection: tables are sized at most half full from the expected
+// group count, where a probe run averages about two slots; a run longer than
+// KDB_MAX_PROBE slots therefore means the estimate was wrong, and the lookup
+// reports KDB_DEV_ERR_CAPACITY (the host regrows the table and reruns).  No
+// shared counter is touched on the hot path.
+#define KDB_MAX_PROBE 256
 
-KDB_DEV int64_t kdb_group_find_packed(uint64_t* slots, uint64_t mask, uint64_t key,
-                                      unsigned long long* gcount, uint64_t limit, int* err) {
-  if (*(volatile unsigned long long*)gcount >= limit) {
-    // already overfull: this launch's result is discarded, stop early
-    kdb_set_error(err, KDB_DEV_ERR_CAPACITY);
-    return -1;
-  }
+KDB_DEV int64_t kdb_group_find_packed(uint64_t* slots, uint64_t mask, uint64_t key, int* err) {
   uint64_t i = kdb_mix64(key) & mask;
   for (uint64_t k = 0; k <= mask && k < KDB_MAX_PROBE; k++) {
     uint64_t s = *(volatile uint64_t*)&slots[i];
     if (s == key) return (int64_t)i;
     if (s == 0) {
       uint64_t prev = atomicCAS((unsigned long long*)&slots[i], 0ULL, (unsigned long long)key);
-      if (prev == 0) {
-        if (atomicAdd(gcount, 1ULL) >= limit) kdb_set_error(err, KDB_DEV_ERR_CAPACITY);
-        return (int64_t)i;
-      }
-      if (prev == key) return (int64_t)i;
+      if (prev == 0 || prev == key) return (int64_t)i;
     }
     i = (i + 1) & mask;
   }
@@ -290,12 +279,7 @@ KDB_DEV int64_t kdb_group_find_packed(uint64_t* slots, uint64_t mask, uint64_t k
 // and publishes the hash; others wait (bounded) while they see 1, then
 // compare keys with `eq` (which must read key columns with __ldcg).
 template <typename EQ, typename INIT>
-KDB_DEV int64_t kdb_group_find(uint64_t* slots, uint64_t mask, uint64_t h, EQ eq, INIT init,
-                               unsigned long long* gcount, uint64_t limit, int* err) {
-  if (*(volatile unsigned long long*)gcount >= limit) {
-    kdb_set_error(err, KDB_DEV_ERR_CAPACITY);
-    return -1;
-  }
+KDB_DEV int64_t kdb_group_find(uint64_t* slots, uint64_t mask, uint64_t h, EQ eq, INIT init, int* err) {
   uint64_t i = h & mask;
   for (uint64_t k = 0; k <= mask && k < KDB_MAX_PROBE; k++) {
     uint64_t s = *(volatile uint64_t*)&slots[i];
@@ -305,7 +289,6 @@ KDB_DEV int64_t kdb_group_find(uint64_t* slots, uint64_t mask, uint64_t h, EQ eq
         init(i);
         __threadfence();
         atomicExch((unsigned long long*)&slots[i], (unsigned long long)h);
-        if (atomicAdd(gcount, 1ULL) >= limit) kdb_set_error(err, KDB_DEV_ERR_CAPACITY);
         return (int64_t)i;
       }
       s = prev;

@@ -80,6 +80,7 @@ struct MatCol {
 struct MatBuffer {
   std::vector<MatCol> cols;
   uint64_t* pos = nullptr;   // stream position of each row (reference emission order key)
+  bool pos_is_index = false;  // pos[r] == r: rows are already in stream order
   int64_t rows = 0;
   int64_t cap = 0;
 };

@@ -29,7 +29,9 @@ EXPORTS = [
     "kdb_enum_open_kdbenum", "kdb_query_execute", "kdb_last_query_device_ms",
     "kdb_result_num_rows", "kdb_result_num_cols", "kdb_result_col_type", "kdb_result_get_i64",
     "kdb_result_get_f64", "kdb_result_get_nulls", "kdb_result_get_text", "kdb_result_format",
-    "kdb_result_free", "kdb_sort_pairs", "kdb_ctx_set_skinner", "kdb_last_skinner_episodes", "kdb_sort_pairs_noalloc",
+    "kdb_result_free", "kdb_sort_pairs", "kdb_ctx_set_skinner", "kdb_last_skinner_episodes",
+    "kdb_batch_create", "kdb_batch_configure", "kdb_batch_tune", "kdb_batch_config", "kdb_batch_run",
+    "kdb_batch_run_timed", "kdb_batch_result", "kdb_batch_free", "kdb_sort_pairs_noalloc",
 ]
 
 _lib = None
@@ -77,6 +79,16 @@ def load_library(path: str = LIB_PATH):
     L.kdb_last_query_device_ms.argtypes = [P]
     L.kdb_sort_pairs.argtypes = [P, P, P, I64, I32]
     L.kdb_ctx_set_skinner.argtypes = [P, I64, ctypes.c_uint32]
+    L.kdb_batch_create.argtypes = [P, P, I32, ctypes.POINTER(P)]
+    L.kdb_batch_configure.argtypes = [P, I32, ctypes.c_double, I32]
+    L.kdb_batch_tune.argtypes = [P, I32, ctypes.c_char_p, I64]
+    L.kdb_batch_config.argtypes = [P, P, P, P]
+    L.kdb_batch_run.argtypes = [P]
+    L.kdb_batch_run_timed.restype = ctypes.c_double
+    L.kdb_batch_run_timed.argtypes = [P, I32]
+    L.kdb_batch_result.restype = I64
+    L.kdb_batch_result.argtypes = [P, I32, P, P, I64]
+    L.kdb_batch_free.argtypes = [P]
     L.kdb_last_skinner_episodes.restype = I64
     L.kdb_last_skinner_episodes.argtypes = [P]
     L.kdb_sort_pairs_noalloc.argtypes = [P, P, I64, I32, P]
@@ -210,3 +222,71 @@ def sort_pairs_noalloc(d_keys: int, d_vals: int, n: int, key_bits: int = 64, str
     lib = load_library()
     return lib.kdb_sort_pairs_noalloc(ctypes.c_void_p(d_keys), ctypes.c_void_p(d_vals), n, key_bits,
                                       ctypes.c_void_p(stream) if stream else None)
+
+
+class BatchQuery(ctypes.Structure):
+    """kdb_batch_query: one query of the batched join + group-by template."""
+    _fields_ = [("dim_table", ctypes.c_char_p), ("dim_key", ctypes.c_char_p), ("dim_date", ctypes.c_char_p),
+                ("dim_seg", ctypes.c_char_p), ("fact_table", ctypes.c_char_p), ("fact_fk", ctypes.c_char_p),
+                ("fact_price", ctypes.c_char_p), ("fact_disc", ctypes.c_char_p), ("date_lt", ctypes.c_int32),
+                ("seg", ctypes.c_int32)]
+
+
+class Batch:
+    """Many join + group-by template queries run as one captured CUDA graph
+    (kdb_batch_*)."""
+
+    def __init__(self, engine: Engine, queries):
+        self.engine = engine
+        self.lib = engine.lib
+        arr = (BatchQuery * len(queries))()
+        self._keep = []
+        for i, q in enumerate(queries):
+            enc = {k: (v.encode() if isinstance(v, str) else v) for k, v in q.items()}
+            self._keep.append(enc)
+            arr[i] = BatchQuery(**enc)
+        h = ctypes.c_void_p()
+        engine._check(self.lib.kdb_batch_create(engine.ctx, ctypes.cast(arr, ctypes.c_void_p), len(queries),
+                                                ctypes.byref(h)))
+        self.h = h
+        self.n = len(queries)
+
+    def configure(self, block: int = 256, load_factor: float = 0.5, fanout: int = 1) -> None:
+        self.engine._check(self.lib.kdb_batch_configure(self.h, block, load_factor, fanout))
+
+    def tune(self, reps: int = 3):
+        import json
+        buf = ctypes.create_string_buffer(1 << 16)
+        self.engine._check(self.lib.kdb_batch_tune(self.h, reps, buf, 1 << 16))
+        return json.loads(buf.value.decode())
+
+    def config(self):
+        b, lf, f = ctypes.c_int32(), ctypes.c_double(), ctypes.c_int32()
+        self.lib.kdb_batch_config(self.h, ctypes.byref(b), ctypes.byref(lf), ctypes.byref(f))
+        return {"block": b.value, "load_factor": lf.value, "fanout": f.value}
+
+    def run(self) -> None:
+        self.engine._check(self.lib.kdb_batch_run(self.h))
+
+    def run_timed(self, reps: int = 10) -> float:
+        return self.lib.kdb_batch_run_timed(self.h, reps)
+
+    def result(self, q: int):
+        n = self.lib.kdb_batch_result(self.h, q, None, None, 0)
+        if n < 0:
+            raise KdbError(int(n), self.lib.kdb_last_error(self.engine.ctx).decode())
+        keys = np.zeros(n, np.int32)
+        sums = np.zeros(n, np.float64)
+        self.lib.kdb_batch_result(self.h, q, _ptr(keys), _ptr(sums), n)
+        return keys, sums
+
+    def close(self):
+        if self.h:
+            self.lib.kdb_batch_free(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -334,3 +334,69 @@ def skinner_plan(tables, tokens, shape: str = "star", like_tables=(1, 2)):
     s.AddDerivedColumn("count", VirtColRef(cnt, 0))
     s.AddDerivedColumn("min_pk", VirtColRef(mn, 1))
     return OutputOperator(AggregateOperator(s, join, [cnt, mn]))
+
+
+# ---------------------------------------------------------------------------
+# Batched form: many uneven join + group-by queries of one template
+# ---------------------------------------------------------------------------
+
+
+def batch_tables(n_queries: int = 256, min_fact: int = 10_000, max_fact: int = 6_000_000, seed: int = 21,
+                 prefix: str = "bq"):
+    """Per query: a dimension table (1/4 of the fact rows; unique int32 key,
+    date, segment) and a fact table (foreign key uniform over the dimension
+    keys, price, discount); fact rows log-uniform in [min_fact, max_fact].
+    The predicate constants give a dimension selectivity uniform in
+    [1%, 90%].  Returns [(dim, fact, date_lt_jdn, seg)]."""
+    out = []
+    sizes = np.exp(np.log(min_fact) + uniform01(seed, n_queries) * (np.log(max_fact) - np.log(min_fact)))
+    sel = 0.01 + 0.89 * uniform01(seed + 1, n_queries)
+    for q in range(n_queries):
+        nf = int(sizes[q])
+        nd = max(1, nf // 4)
+        s = seed * 1000 + 17 * q
+        d = HostTable(f"{prefix}_dim{q}")
+        d.add(HostColumn("d_key", Type.Int(), values=(np.arange(nd, dtype=np.int64) * 7 + q).astype(np.int32)))
+        d.add(HostColumn("d_date", Type.Date(), values=_dates(s + 1, nd)))
+        d.add(HostColumn("d_seg", Type.Int(), values=np.zeros(nd, np.int32)))
+        f = HostTable(f"{prefix}_fact{q}")
+        fk_idx = uniform_int(s + 2, nf, 0, nd - 1)
+        f.add(HostColumn("f_fk", Type.Int(), values=(fk_idx * 7 + q).astype(np.int32)))
+        f.add(HostColumn("f_price", Type.Real(), values=_price(s + 3, nf)))
+        f.add(HostColumn("f_disc", Type.Real(), values=_hundredths(s + 4, nf, 10)))
+        date_lt = EPOCH_JDN + 8035 + int(round(float(sel[q]) * (10591 - 8035 + 1)))
+        out.append((d, f, date_lt, 0))
+    return out
+
+
+def batch_plan(dim: HostTable, fact: HostTable, date_lt_jdn: int, seg: int) -> OutputOperator:
+    """The plain form of one batched query: HashJoin(ScanSelect(dim),
+    Scan(fact)) -> GROUP BY dim key, SUM(price * (1 - discount))."""
+    db = catalog_of([dim, fact])
+    drel, frel = db[dim.name], db[fact.name]
+    ds = OperatorSchema()
+    ds.AddGeneratedColumns(drel, ["d_key", "d_date", "d_seg"])
+    filt = [Lt(VirtColRef(ds, "d_date"), LiteralExpression(Type.Date(), date_lt_jdn)),
+            Eq(VirtColRef(ds, "d_seg"), Literal(int(seg)))]
+    dout = OperatorSchema()
+    dout.AddVirtualPassthroughColumns(ds, ["d_key"])
+    dsel = ScanSelectOperator(dout, ds, drel, filt)
+    fs = OperatorSchema()
+    fs.AddGeneratedColumns(frel, ["f_fk", "f_price", "f_disc"])
+    fscan = ScanOperator(fs, frel)
+    js = OperatorSchema()
+    js.AddPassthroughColumns(dsel, ["d_key"], 0)
+    js.AddPassthroughColumns(fscan, ["f_price", "f_disc"], 1)
+    join = HashJoinOperator(js, dsel, fscan, [ColRef(dsel, "d_key", 0)], [ColRef(fscan, "f_fk", 1)])
+    key = ColRefE(join, "d_key")
+    rev = Sum(Mul(ColRef(join, "f_price"), Sub(Literal(1.0), ColRef(join, "f_disc"))))
+    gs = OperatorSchema()
+    gs.AddDerivedColumn("d_key", VirtColRef(key, 0))
+    gs.AddDerivedColumn("revenue", VirtColRef(rev, 1))
+    return OutputOperator(GroupByAggregateOperator(gs, join, [key], [rev]))
+
+
+def batch_query_desc(dim: HostTable, fact: HostTable, date_lt_jdn: int, seg: int) -> dict:
+    return {"dim_table": dim.name, "dim_key": "d_key", "dim_date": "d_date", "dim_seg": "d_seg",
+            "fact_table": fact.name, "fact_fk": "f_fk", "fact_price": "f_price", "fact_disc": "f_disc",
+            "date_lt": int(date_lt_jdn), "seg": int(seg)}
