@@ -7,7 +7,7 @@ available).  Metric: rows/s (whole job), with the roofline of the dominant
 kernel against the measured HBM copy bandwidth.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--workload group_by|scan_agg|join_group]
+                    [--workload group_by|scan_agg|join_group|batched|serving]
 
 A step is one execution of the query over the resident table.  The timed
 region covers exactly K steps on the engine's CUDA stream (events), bracketed
@@ -240,6 +240,94 @@ def run_batched(args):
     print(json.dumps(line))
 
 
+def run_serving(args):
+    """Serving form: a stream of requests mixing four query shapes (scan +
+    aggregate, group-by, join + group-by + ORDER BY, Skinner multiway join)
+    arrives as a Poisson process; the server's slots run them concurrently.
+    Reports throughput and submission-to-completion latency (p50/p99), beside
+    the same request sequence run one at a time through the plain API."""
+    import random
+    import torch
+    from kushdb_b200.engine import Engine, Server
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    eng = Engine(local)
+    sa = wl.scan_agg_table(1_000_000, name="srv_sales")
+    gb = wl.group_by_table(6_000_000, name="srv_lineitem")
+    build, probe = wl.join_tables(1_500_000, 6_000_000)
+    sk, tokens = wl.skinner_tables("star", 6, min_rows=10_000, max_rows=1_000_000, seed=5, prefix="srv_sk")
+    for t in [sa, gb, build, probe] + sk:
+        eng.register_table(t)
+    shapes = {
+        "scan_agg": [wl.scan_agg_plan(sa, date_lt=d) for d in (9000, 9300, 9800)],
+        "group_by": [wl.group_by_plan(gb, date_leq=d) for d in (10000, 10471)],
+        "join_group": [wl.join_plan(build, probe, date_lt=d) for d in (9000, 9204)],
+        "skinner": [wl.skinner_plan(sk, tokens, "star")],
+    }
+    plans = [(k, p.to_json().encode()) for k, ps in shapes.items() for p in ps]
+    alone_ms = {}
+    for k, p in plans:  # compile and warm every pipeline
+        for _ in range(args.warmup):
+            eng.execute(p, fetch=False)
+    stream = torch.cuda.ExternalStream(eng.stream_handle())
+    rnd = random.Random(1234)
+    n = args.serving_requests
+    seq = [plans[rnd.randrange(len(plans))] for _ in range(n)]
+    # one at a time through the plain API (device time per request)
+    t0 = time.perf_counter()
+    for k, p in seq:
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        eng.execute(p, fetch=False)
+        e1.record(stream)
+        e1.synchronize()
+        alone_ms.setdefault(k, []).append(e0.elapsed_time(e1))
+    seq_s = time.perf_counter() - t0
+    out = {}
+    for mode in ("saturated", "poisson"):
+        with ClockSampler(local) as clocks, Server(eng, slots=args.serving_slots,
+                                                   hbm_budget_bytes=args.serving_budget_gb << 30) as srv:
+            tickets = []
+            t0 = time.perf_counter()
+            if mode == "saturated":
+                for _, p in seq:
+                    tickets.append(srv.submit(p))
+            else:
+                gaps = np.random.default_rng(7).exponential(1.0 / args.serving_rate, n)
+                t_next = t0
+                for (_, p), g in zip(seq, gaps):
+                    t_next += g
+                    while time.perf_counter() < t_next:
+                        pass
+                    tickets.append(srv.submit(p))
+            for t in tickets:
+                r = srv.wait(t)
+                r.close()
+            wall = time.perf_counter() - t0
+            st = srv.stats()
+        st["wall_s"] = wall
+        st["clocks"] = clocks.summary()
+        out[mode] = st
+    sat = out["saturated"]
+    line = {
+        "metric": "queries_per_second", "value": sat["queries_per_second"], "unit": "queries/s",
+        "n_gpus": 1, "steps": n, "warmup": args.warmup, "ms_per_step": 1e3 / sat["queries_per_second"],
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": "serving mix (scan_agg 1M rows, group_by 6M, join_group 1.5M x 6M, "
+                               "skinner star of 6 tables 10k-1M rows)", "requests": n,
+                   "slots": args.serving_slots, "hbm_budget_gb": args.serving_budget_gb,
+                   "poisson_rate_qps": args.serving_rate, "l2": "inputs larger than L2 (126 MB)"},
+        "saturated": sat,
+        "poisson": out["poisson"],
+        "one_at_a_time": {"queries_per_second": n / seq_s,
+                          "device_ms_p50_by_shape": {k: statistics.median(v) for k, v in alone_ms.items()}},
+        "speedup_vs_one_at_a_time": sat["queries_per_second"] / (n / seq_s),
+        "gpu_launches": sat["kernel_launches"] + out["poisson"]["kernel_launches"],
+        "clocks": sat["clocks"],
+    }
+    print(json.dumps(line))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -247,9 +335,13 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="group_by",
-                    choices=["group_by", "scan_agg", "join_group", "batched"])
+                    choices=["group_by", "scan_agg", "join_group", "batched", "serving"])
     ap.add_argument("--batch-queries", type=int, default=256)
     ap.add_argument("--batch-max-fact", type=int, default=6_000_000)
+    ap.add_argument("--serving-requests", type=int, default=2000)
+    ap.add_argument("--serving-slots", type=int, default=4)
+    ap.add_argument("--serving-rate", type=float, default=1000.0)
+    ap.add_argument("--serving-budget-gb", type=int, default=32)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     args = ap.parse_args()
@@ -260,6 +352,9 @@ def main():
         return
     if args.workload == "batched":
         run_batched(args)
+        return
+    if args.workload == "serving":
+        run_serving(args)
         return
 
     import torch

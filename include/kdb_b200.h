@@ -191,6 +191,31 @@ double kdb_batch_run_timed(kdb_batch* b, int32_t reps);
 int64_t kdb_batch_result(kdb_batch* b, int32_t q, int32_t* keys, double* sums, int64_t cap);
 void kdb_batch_free(kdb_batch* b);
 
+/* ---- serving ---------------------------------------------------------------
+ * A request loop over the context's resident tables (no reference
+ * counterpart: the reference runs one query per process,
+ * execution/executable_query.cc:199-255).  `slots` worker threads, each with
+ * its own CUDA stream, take queued plans as soon as a slot is free and the
+ * request's estimated device footprint fits `hbm_budget_bytes` beside the
+ * ones in flight, so queries of different shapes run concurrently.  Tables
+ * must not be added or dropped while a server runs. */
+typedef struct kdb_server kdb_server;
+int kdb_server_start(kdb_ctx* ctx, int32_t slots, int64_t hbm_budget_bytes, kdb_server** out);
+/* Queues a plan (same JSON as kdb_query_execute); returns a ticket > 0 or a
+ * negative KDB_ERR_* (a plan that does not parse is rejected here). */
+int64_t kdb_server_submit(kdb_server* s, const char* plan_json);
+/* 1 = still pending, 0 = done (the result is handed over in *out and the
+ * ticket retired), < 0 = the query failed (message in kdb_last_error of the
+ * owning context).  Waits up to wait_ms for completion. */
+int kdb_server_poll(kdb_server* s, int64_t ticket, int64_t wait_ms, kdb_result** out);
+/* JSON: completed, failed, p50_ms, p99_ms, max_ms (submission to completion),
+ * service_p50_ms, queries_per_second, peak_in_flight, slots, hbm_budget,
+ * kernel_launches.
+ * Returns the size needed including the NUL. */
+int64_t kdb_server_stats(kdb_server* s, char* buf, int64_t cap);
+/* Finishes the requests in flight, drops queued ones, joins the workers. */
+void kdb_server_stop(kdb_server* s);
+
 /* ---- results (runtime/printer.cc output format) ------------------------ */
 int64_t kdb_result_num_rows(const kdb_result* r);
 int32_t kdb_result_num_cols(const kdb_result* r);

@@ -12,34 +12,40 @@
 // with per-query predicate constants).  Plain execution pays a launch
 // sequence, host synchronisations and code-generation per query; here every
 // phase of all queries is one launch:
-//   1. build  -- every CTA range owns one query: filter its dimension rows
-//      and insert the survivors into that query's join table (CAS);
-//   2. probe  -- likewise over the fact rows: probe, and add the measure into
-//      the matched build row's accumulator (the dimension key is the
-//      table's primary key, so the build row is the group; duplicate build
-//      keys are detected and reported);
+//   1. build  -- filter each query's dimension rows and insert the survivors
+//      into that query's join table (CAS on (key, row) slots);
+//   2. probe  -- over the fact rows: probe, and add the measure into the
+//      matched build row's accumulator (the dimension key is the table's
+//      primary key, so the build row is the group; duplicate build keys are
+//      detected and reported);
 //   3. output -- compact each query's touched build rows into its result.
-// Capacities are sized from the table sizes, so no phase needs a read-back
-// and the whole batch is captured once into a CUDA graph and replayed.
-// Tunables (chosen by kdb_batch_tune): block size, join-table load factor,
-// and radix fan-out P -- with P > 1 each query's join table is split into P
-// sub-tables by the top bits of the key hash, so a probe's working set is one
-// sub-table (for build sides larger than L2).
+// Each CTA owns a fixed chunk of one query's rows (block x 16), and chunks
+// are numbered query after query, so the CTAs resident at any moment work on
+// a few queries and their join tables and accumulators stay in L2.
+// Capacities are sized when the batch is configured, so no phase needs a
+// read-back and the whole batch is captured once into a CUDA graph and
+// replayed.  Tunables (chosen by kdb_batch_tune): block size, join-table load
+// factor, and radix fan-out P -- with P > 1 each query's join table is split
+// into P sub-tables by the top bits of the key hash, so a probe's working set
+// is one sub-table (for build sides larger than L2).
 #include <cuda_runtime.h>
 
 #include <algorithm>
 #include <chrono>
+#include <climits>
 #include <cmath>
 #include <cstring>
 #include <sstream>
 #include <string>
 #include <vector>
 
-#include "../../include/kdb_b200.h"
-#include "engine.h"
+#include "capi_internal.h"
 
 namespace kdb {
 namespace {
+
+constexpr int kRowsPerThread = 16;  // rows of one chunk per thread
+constexpr int kProbeUnroll = 4;     // independent probes in flight per thread
 
 struct QueryDesc {
   // dimension side
@@ -54,7 +60,7 @@ struct QueryDesc {
   const double* f_price;
   const double* f_disc;
   int64_t nf;
-  // join table: P sub-tables of `sub_cap` slots each, slots[q_slot_base ...]
+  // join table: P sub-tables of `sub_cap` slots each, slots[slot_base ...]
   int64_t slot_base;
   uint32_t sub_cap;
   uint32_t pad;
@@ -62,17 +68,36 @@ struct QueryDesc {
   int64_t acc_base;
   // result region out[out_base ...] (capacity nd)
   int64_t out_base;
-  // CTA ranges of the three phases
+  // CTA ranges of the three phases (one chunk of rows per CTA)
   int32_t build_block0, build_blocks;
   int32_t probe_block0, probe_blocks;
   int32_t out_block0, out_blocks;
 };
 
-__device__ __forceinline__ uint32_t KeyHash(int32_t k) {
+// Per build row: the running sum and the complement of the first fact row
+// that reached it (0 = untouched; atomicMax of ~row keeps the smallest row).
+struct Acc {
+  double sum;
+  unsigned long long first_inv;
+};
+static_assert(sizeof(Acc) == 16, "Acc layout");
+
+// 64-bit mix of the key: the top bits choose the sub-table, the low 32 bits
+// the home slot inside it, so the two are independent.
+__device__ __forceinline__ uint64_t KeyHash(int32_t k) {
   uint64_t x = static_cast<uint64_t>(static_cast<uint32_t>(k)) * 0x9E3779B97F4A7C15ULL;
-  x ^= x >> 29;
+  x ^= x >> 31;
   x *= 0xBF58476D1CE4E5B9ULL;
-  return static_cast<uint32_t>(x >> 32) | 1u;
+  x ^= x >> 29;
+  return x;
+}
+
+__device__ __forceinline__ uint32_t SubTable(uint64_t h, int fanout_bits) {
+  return fanout_bits ? static_cast<uint32_t>(h >> (64 - fanout_bits)) : 0u;
+}
+
+__device__ __forceinline__ uint32_t HomeSlot(uint64_t h, uint32_t cap) {
+  return static_cast<uint32_t>((static_cast<uint64_t>(static_cast<uint32_t>(h)) * cap) >> 32);
 }
 
 // block -> query by binary search over the queries' first blocks
@@ -88,94 +113,139 @@ __device__ __forceinline__ int FindQuery(const QueryDesc* qs, int nq, int block)
   return lo;
 }
 
-// slot = (hash << 32) | (row + 1); 0 = empty
-__global__ void BatchBuild(const QueryDesc* __restrict__ qs, int nq, uint64_t* __restrict__ slots,
-                           int fanout_bits, int* __restrict__ err) {
+// Rows [r0, r1) of this CTA's chunk.
+template <int kPhase>
+__device__ __forceinline__ const QueryDesc& Chunk(const QueryDesc* qs, int nq, int64_t& r0, int64_t& r1) {
   __shared__ int sq;
-  if (threadIdx.x == 0) sq = FindQuery<0>(qs, nq, blockIdx.x);
+  if (threadIdx.x == 0) sq = FindQuery<kPhase>(qs, nq, blockIdx.x);
   __syncthreads();
   const QueryDesc& q = qs[sq];
-  const int64_t local = blockIdx.x - q.build_block0;
-  const int64_t stride = static_cast<int64_t>(q.build_blocks) * blockDim.x;
-  for (int64_t r = local * blockDim.x + threadIdx.x; r < q.nd; r += stride) {
+  const int b0 = kPhase == 0 ? q.build_block0 : kPhase == 1 ? q.probe_block0 : q.out_block0;
+  const int64_t chunk = static_cast<int64_t>(blockDim.x) * kRowsPerThread;
+  const int64_t n = kPhase == 1 ? q.nf : q.nd;
+  r0 = (blockIdx.x - b0) * chunk;
+  r1 = r0 + chunk < n ? r0 + chunk : n;
+  return q;
+}
+
+// Rows of every dimension table per (query, sub-table): sizes the
+// sub-tables so that none can overflow whatever the predicates select.
+__global__ void BatchPartCount(const QueryDesc* __restrict__ qs, int nq, int fanout_bits,
+                               unsigned* __restrict__ counts) {
+  extern __shared__ unsigned hist[];
+  const int parts = 1 << fanout_bits;
+  for (int i = threadIdx.x; i < parts; i += blockDim.x) hist[i] = 0;
+  int64_t r0, r1;
+  const QueryDesc& q = Chunk<0>(qs, nq, r0, r1);
+  const int qi = static_cast<int>(&q - qs);
+  for (int64_t r = r0 + threadIdx.x; r < r1; r += blockDim.x)
+    atomicAdd(&hist[SubTable(KeyHash(__ldcs(q.d_key + r)), fanout_bits)], 1u);
+  __syncthreads();
+  for (int i = threadIdx.x; i < parts; i += blockDim.x)
+    if (hist[i]) atomicAdd(&counts[static_cast<int64_t>(qi) * parts + i], hist[i]);
+}
+
+// slot = (key << 32) | (row + 1); 0 = empty
+__global__ void BatchBuild(const QueryDesc* __restrict__ qs, int nq, unsigned long long* __restrict__ slots,
+                           int fanout_bits, int* __restrict__ err) {
+  int64_t r0, r1;
+  const QueryDesc& q = Chunk<0>(qs, nq, r0, r1);
+  for (int64_t r = r0 + threadIdx.x; r < r1; r += blockDim.x) {
     if (!(__ldcs(q.d_date + r) < q.date_lt)) continue;
     if (!(__ldcs(q.d_seg + r) == q.seg)) continue;
-    int32_t k = __ldcs(q.d_key + r);
-    uint32_t h = KeyHash(k);
-    uint32_t part = fanout_bits ? (h >> (32 - fanout_bits)) : 0;
-    uint64_t* sub = slots + q.slot_base + static_cast<int64_t>(part) * q.sub_cap;
-    uint32_t i = static_cast<uint32_t>((static_cast<uint64_t>(h) * q.sub_cap) >> 32);
-    uint64_t e = (static_cast<uint64_t>(h) << 32) | static_cast<uint64_t>(r + 1);
+    const int32_t k = __ldcs(q.d_key + r);
+    const uint64_t h = KeyHash(k);
+    unsigned long long* sub = slots + q.slot_base + static_cast<int64_t>(SubTable(h, fanout_bits)) * q.sub_cap;
+    uint32_t i = HomeSlot(h, q.sub_cap);
+    const unsigned long long e =
+        (static_cast<unsigned long long>(static_cast<uint32_t>(k)) << 32) | static_cast<unsigned long long>(r + 1);
+    bool placed = false;
     for (uint32_t n = 0; n < q.sub_cap; n++) {
-      uint64_t prev = atomicCAS(reinterpret_cast<unsigned long long*>(sub + i), 0ULL,
-                                static_cast<unsigned long long>(e));
-      if (prev == 0) break;
-      if (static_cast<uint32_t>(prev >> 32) == h && q.d_key[static_cast<uint32_t>(prev) - 1] == k)
+      const unsigned long long prev = atomicCAS(sub + i, 0ULL, e);
+      if (prev == 0) {
+        placed = true;
+        break;
+      }
+      if (static_cast<uint32_t>(prev >> 32) == static_cast<uint32_t>(k))
         atomicCAS(err, 0, 3);  // duplicate dimension key: not a primary key
       if (++i == q.sub_cap) i = 0;
     }
+    if (!placed) atomicCAS(err, 0, 4);
   }
 }
 
-// sum / count / first fact row per build row
-__global__ void BatchProbe(const QueryDesc* __restrict__ qs, int nq, const uint64_t* __restrict__ slots,
-                           int fanout_bits, double* __restrict__ sum, unsigned long long* __restrict__ cnt,
-                           unsigned long long* __restrict__ first) {
-  __shared__ int sq;
-  if (threadIdx.x == 0) sq = FindQuery<1>(qs, nq, blockIdx.x);
-  __syncthreads();
-  const QueryDesc& q = qs[sq];
-  const int64_t local = blockIdx.x - q.probe_block0;
-  const int64_t stride = static_cast<int64_t>(q.probe_blocks) * blockDim.x;
-  for (int64_t r = local * blockDim.x + threadIdx.x; r < q.nf; r += stride) {
-    int32_t k = __ldcs(q.f_fk + r);
-    uint32_t h = KeyHash(k);
-    uint32_t part = fanout_bits ? (h >> (32 - fanout_bits)) : 0;
-    const uint64_t* sub = slots + q.slot_base + static_cast<int64_t>(part) * q.sub_cap;
-    uint32_t i = static_cast<uint32_t>((static_cast<uint64_t>(h) * q.sub_cap) >> 32);
-    for (uint32_t n = 0; n < q.sub_cap; n++) {
-      uint64_t e = sub[i];
-      if (e == 0) break;
-      if (static_cast<uint32_t>(e >> 32) == h) {
-        int64_t br = static_cast<int64_t>(static_cast<uint32_t>(e)) - 1;
-        if (q.d_key[br] == k) {
+// sum and first fact row per build row; kProbeUnroll rows per thread are
+// loaded and hashed together so their table reads overlap.
+__global__ void BatchProbe(const QueryDesc* __restrict__ qs, int nq, const unsigned long long* __restrict__ slots,
+                           int fanout_bits, Acc* __restrict__ acc) {
+  int64_t r0, r1;
+  const QueryDesc& q = Chunk<1>(qs, nq, r0, r1);
+  const int64_t step = blockDim.x;
+  for (int64_t base = r0 + threadIdx.x; base < r1; base += kProbeUnroll * step) {
+    int32_t k[kProbeUnroll];
+    uint32_t pos[kProbeUnroll];
+    const unsigned long long* sub[kProbeUnroll];
+    unsigned long long e[kProbeUnroll];
+#pragma unroll
+    for (int j = 0; j < kProbeUnroll; j++) {
+      const int64_t r = base + j * step;
+      k[j] = r < r1 ? __ldcs(q.f_fk + r) : 0;
+    }
+#pragma unroll
+    for (int j = 0; j < kProbeUnroll; j++) {
+      const uint64_t h = KeyHash(k[j]);
+      sub[j] = slots + q.slot_base + static_cast<int64_t>(SubTable(h, fanout_bits)) * q.sub_cap;
+      pos[j] = HomeSlot(h, q.sub_cap);
+      e[j] = base + j * step < r1 ? sub[j][pos[j]] : 0ULL;
+    }
+#pragma unroll
+    for (int j = 0; j < kProbeUnroll; j++) {
+      const int64_t r = base + j * step;
+      if (r >= r1) continue;
+      unsigned long long s = e[j];
+      uint32_t i = pos[j];
+      for (uint32_t n = 0; s != 0 && n < q.sub_cap; n++) {
+        if (static_cast<uint32_t>(s >> 32) == static_cast<uint32_t>(k[j])) {
+          Acc* a = acc + q.acc_base + (static_cast<int64_t>(static_cast<uint32_t>(s)) - 1);
           // plain per-row IEEE arithmetic, like the reference's generated code
-          double v = __dmul_rn(__ldcs(q.f_price + r), __dsub_rn(1.0, __ldcs(q.f_disc + r)));
-          atomicAdd(sum + q.acc_base + br, v);
-          atomicAdd(cnt + q.acc_base + br, 1ULL);
-          atomicMin(first + q.acc_base + br, static_cast<unsigned long long>(r));
+          const double v = __dmul_rn(__ldcs(q.f_price + r), __dsub_rn(1.0, __ldcs(q.f_disc + r)));
+          atomicAdd(&a->sum, v);
+          atomicMax(&a->first_inv, ~static_cast<unsigned long long>(r));
+          break;  // keys are unique on the build side
         }
+        if (++i == q.sub_cap) i = 0;
+        s = sub[j][i];
       }
-      if (++i == q.sub_cap) i = 0;
     }
   }
 }
 
-// per query: build rows with a match -> (key, sum, first fact row)
-__global__ void BatchOutput(const QueryDesc* __restrict__ qs, int nq, const double* __restrict__ sum,
-                            const unsigned long long* __restrict__ cnt,
-                            const unsigned long long* __restrict__ first, int32_t* __restrict__ out_key,
-                            double* __restrict__ out_sum, unsigned long long* __restrict__ out_first,
-                            unsigned long long* __restrict__ out_count) {
-  __shared__ int sq;
-  if (threadIdx.x == 0) sq = FindQuery<2>(qs, nq, blockIdx.x);
-  __syncthreads();
-  const QueryDesc& q = qs[sq];
-  const int64_t local = blockIdx.x - q.out_block0;
-  const int64_t stride = static_cast<int64_t>(q.out_blocks) * blockDim.x;
-  for (int64_t r = local * blockDim.x + threadIdx.x; r < q.nd; r += stride) {
-    if (cnt[q.acc_base + r] == 0) continue;
-    unsigned long long o = atomicAdd(out_count + sq, 1ULL);
-    out_key[q.out_base + o] = q.d_key[r];
-    out_sum[q.out_base + o] = sum[q.acc_base + r];
-    out_first[q.out_base + o] = first[q.acc_base + r];
+// per query: build rows with a match -> (key, sum, first fact row); one
+// counter atomic per warp
+__global__ void BatchOutput(const QueryDesc* __restrict__ qs, int nq, const Acc* __restrict__ acc,
+                            int32_t* __restrict__ out_key, double* __restrict__ out_sum,
+                            unsigned long long* __restrict__ out_first, unsigned long long* __restrict__ out_count) {
+  int64_t r0, r1;
+  const QueryDesc& q = Chunk<2>(qs, nq, r0, r1);
+  const int qi = static_cast<int>(&q - qs);
+  const unsigned lane = threadIdx.x & 31;
+  for (int64_t rb = r0; rb < r1; rb += blockDim.x) {  // uniform trip count per warp
+    const int64_t r = rb + threadIdx.x;
+    Acc a{0.0, 0ULL};
+    if (r < r1) a = acc[q.acc_base + r];
+    const bool hit = a.first_inv != 0;
+    const unsigned m = __ballot_sync(0xffffffffu, hit);
+    if (m == 0) continue;
+    unsigned long long o0 = 0;
+    if (lane == 0) o0 = atomicAdd(out_count + qi, static_cast<unsigned long long>(__popc(m)));
+    o0 = __shfl_sync(0xffffffffu, o0, 0);
+    if (hit) {
+      const int64_t o = q.out_base + static_cast<int64_t>(o0) + __popc(m & ((1u << lane) - 1));
+      out_key[o] = q.d_key[r];
+      out_sum[o] = a.sum;
+      out_first[o] = ~a.first_inv;
+    }
   }
-}
-
-__global__ void FillU64(unsigned long long* p, int64_t n, unsigned long long v) {
-  for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < n;
-       i += static_cast<int64_t>(gridDim.x) * blockDim.x)
-    p[i] = v;
 }
 
 }  // namespace
@@ -198,52 +268,68 @@ class Batch {
     int fbits = 0;
     while ((1 << fbits) < cfg.fanout) fbits++;
     fanout_bits_ = fbits;
+    const int parts = 1 << fbits;
     const int nq = static_cast<int>(host_qs_.size());
-    int64_t slot_total = 0, acc_total = 0;
-    int32_t bb = 0, pb = 0, ob = 0;
-    const int64_t per_sm = std::max(1, 2048 / cfg.block);
-    const int64_t max_blocks = static_cast<int64_t>(ctx_.num_sms) * per_sm;
-    int64_t total_nd = 0, total_nf = 0;
+    const int64_t chunk = static_cast<int64_t>(cfg.block) * kRowsPerThread;
+    int64_t bb = 0, pb = 0, ob = 0;
     for (auto& q : host_qs_) {
-      total_nd += q.nd;
-      total_nf += q.nf;
+      if (q.nd >= static_cast<int64_t>(UINT32_MAX))
+        throw Error(KDB_ERR_CAPACITY, "batch dimension table too large");
+      auto blocks = [&](int64_t rows) { return std::max<int64_t>(1, (rows + chunk - 1) / chunk); };
+      q.build_block0 = static_cast<int32_t>(bb);
+      q.build_blocks = static_cast<int32_t>(blocks(q.nd));
+      bb += q.build_blocks;
+      q.probe_block0 = static_cast<int32_t>(pb);
+      q.probe_blocks = static_cast<int32_t>(blocks(q.nf));
+      pb += q.probe_blocks;
+      q.out_block0 = static_cast<int32_t>(ob);
+      q.out_blocks = static_cast<int32_t>(blocks(q.nd));
+      ob += q.out_blocks;
+      if (bb > INT_MAX || pb > INT_MAX) throw Error(KDB_ERR_CAPACITY, "batch too large");
     }
-    for (auto& q : host_qs_) {
-      int parts = 1 << fbits;
-      double want = std::max<double>(1.0, static_cast<double>(q.nd) / cfg.load_factor / parts);
-      q.sub_cap = static_cast<uint32_t>(std::max<double>(32.0, std::ceil(want)));
+    build_grid_ = static_cast<int>(bb);
+    probe_grid_ = static_cast<int>(pb);
+    out_grid_ = static_cast<int>(ob);
+    KDB_CUDA(cudaMalloc(&d_qs_, sizeof(QueryDesc) * nq));
+    KDB_CUDA(cudaMemcpy(d_qs_, host_qs_.data(), sizeof(QueryDesc) * nq, cudaMemcpyHostToDevice));
+    // largest sub-table population per query (all dimension rows, so it
+    // bounds what any predicate lets through)
+    std::vector<unsigned> most(nq);
+    if (fbits > 0) {
+      unsigned* counts = nullptr;
+      const size_t nc = static_cast<size_t>(nq) * parts;
+      KDB_CUDA(cudaMalloc(&counts, sizeof(unsigned) * nc));
+      KDB_CUDA(cudaMemsetAsync(counts, 0, sizeof(unsigned) * nc, ctx_.stream));
+      BatchPartCount<<<build_grid_, cfg.block, sizeof(unsigned) * parts, ctx_.stream>>>(d_qs_, nq, fbits, counts);
+      KDB_CUDA(cudaGetLastError());
+      std::vector<unsigned> h(nc);
+      KDB_CUDA(cudaMemcpyAsync(h.data(), counts, sizeof(unsigned) * nc, cudaMemcpyDeviceToHost, ctx_.stream));
+      KDB_CUDA(cudaStreamSynchronize(ctx_.stream));
+      cudaFree(counts);
+      for (int q = 0; q < nq; q++)
+        most[q] = *std::max_element(h.begin() + static_cast<int64_t>(q) * parts,
+                                    h.begin() + static_cast<int64_t>(q + 1) * parts);
+    } else {
+      for (int q = 0; q < nq; q++) most[q] = static_cast<unsigned>(host_qs_[q].nd);
+    }
+    int64_t slot_total = 0, acc_total = 0;
+    for (int qi = 0; qi < nq; qi++) {
+      auto& q = host_qs_[qi];
+      // capacity above the most rows a sub-table can receive: probes always
+      // end at an empty slot
+      const double want = std::ceil(static_cast<double>(most[qi]) / cfg.load_factor) + 1;
+      q.sub_cap = static_cast<uint32_t>(std::max(8.0, want));
       q.slot_base = slot_total;
       slot_total += static_cast<int64_t>(q.sub_cap) * parts;
       q.acc_base = acc_total;
       q.out_base = acc_total;
       acc_total += std::max<int64_t>(q.nd, 1);
-      // CTAs in proportion to the rows of each phase, at least one
-      auto share = [&](int64_t rows, int64_t total) {
-        int64_t b = total > 0 ? (rows * max_blocks + total - 1) / total : 1;
-        b = std::min<int64_t>(b, (rows + cfg.block - 1) / cfg.block);
-        return static_cast<int32_t>(std::max<int64_t>(1, b));
-      };
-      q.build_block0 = bb;
-      q.build_blocks = share(q.nd, total_nd);
-      bb += q.build_blocks;
-      q.probe_block0 = pb;
-      q.probe_blocks = share(q.nf, total_nf);
-      pb += q.probe_blocks;
-      q.out_block0 = ob;
-      q.out_blocks = share(q.nd, total_nd);
-      ob += q.out_blocks;
     }
-    build_grid_ = bb;
-    probe_grid_ = pb;
-    out_grid_ = ob;
     slot_total_ = slot_total;
     acc_total_ = acc_total;
-    KDB_CUDA(cudaMalloc(&d_qs_, sizeof(QueryDesc) * nq));
     KDB_CUDA(cudaMemcpy(d_qs_, host_qs_.data(), sizeof(QueryDesc) * nq, cudaMemcpyHostToDevice));
-    KDB_CUDA(cudaMalloc(&slots_, sizeof(uint64_t) * std::max<int64_t>(slot_total, 1)));
-    KDB_CUDA(cudaMalloc(&sum_, sizeof(double) * acc_total));
-    KDB_CUDA(cudaMalloc(&cnt_, sizeof(unsigned long long) * acc_total));
-    KDB_CUDA(cudaMalloc(&first_, sizeof(unsigned long long) * acc_total));
+    KDB_CUDA(cudaMalloc(&slots_, sizeof(unsigned long long) * std::max<int64_t>(slot_total, 1)));
+    KDB_CUDA(cudaMalloc(&acc_, sizeof(Acc) * acc_total));
     KDB_CUDA(cudaMalloc(&out_key_, sizeof(int32_t) * acc_total));
     KDB_CUDA(cudaMalloc(&out_sum_, sizeof(double) * acc_total));
     KDB_CUDA(cudaMalloc(&out_first_, sizeof(unsigned long long) * acc_total));
@@ -255,7 +341,7 @@ class Batch {
   // Replays the batch (all phases of all queries).
   void Run() {
     KDB_CUDA(cudaGraphLaunch(exec_, ctx_.stream));
-    ctx_.kernel_launches += 6;
+    ctx_.kernel_launches += 3;
   }
 
   float RunTimed(int reps) {
@@ -325,18 +411,13 @@ class Batch {
     const int nq = static_cast<int>(host_qs_.size());
     cudaStream_t s = ctx_.stream;
     KDB_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
-    int fill_grid = std::max(1, std::min(ctx_.num_sms * 8, static_cast<int>((acc_total_ + 255) / 256)));
-    FillU64<<<std::max(1, std::min(ctx_.num_sms * 8, static_cast<int>((slot_total_ + 255) / 256))), 256, 0, s>>>(
-        reinterpret_cast<unsigned long long*>(slots_), slot_total_, 0ULL);
-    FillU64<<<fill_grid, 256, 0, s>>>(reinterpret_cast<unsigned long long*>(sum_), acc_total_, 0ULL);
-    FillU64<<<fill_grid, 256, 0, s>>>(cnt_, acc_total_, 0ULL);
-    FillU64<<<fill_grid, 256, 0, s>>>(first_, acc_total_, ~0ULL);
+    cudaMemsetAsync(slots_, 0, sizeof(unsigned long long) * std::max<int64_t>(slot_total_, 1), s);
+    cudaMemsetAsync(acc_, 0, sizeof(Acc) * acc_total_, s);
     cudaMemsetAsync(out_count_, 0, sizeof(unsigned long long) * nq, s);
     cudaMemsetAsync(err_, 0, sizeof(int), s);
     BatchBuild<<<build_grid_, cfg_.block, 0, s>>>(d_qs_, nq, slots_, fanout_bits_, err_);
-    BatchProbe<<<probe_grid_, cfg_.block, 0, s>>>(d_qs_, nq, slots_, fanout_bits_, sum_, cnt_, first_);
-    BatchOutput<<<out_grid_, cfg_.block, 0, s>>>(d_qs_, nq, sum_, cnt_, first_, out_key_, out_sum_, out_first_,
-                                                 out_count_);
+    BatchProbe<<<probe_grid_, cfg_.block, 0, s>>>(d_qs_, nq, slots_, fanout_bits_, acc_);
+    BatchOutput<<<out_grid_, cfg_.block, 0, s>>>(d_qs_, nq, acc_, out_key_, out_sum_, out_first_, out_count_);
     cudaGraph_t g;
     KDB_CUDA(cudaStreamEndCapture(s, &g));
     KDB_CUDA(cudaGraphInstantiate(&exec_, g, 0));
@@ -346,15 +427,14 @@ class Batch {
   void Release() {
     if (exec_) cudaGraphExecDestroy(exec_);
     exec_ = nullptr;
-    for (void* p : {static_cast<void*>(d_qs_), static_cast<void*>(slots_), static_cast<void*>(sum_),
-                    static_cast<void*>(cnt_), static_cast<void*>(first_), static_cast<void*>(out_key_),
-                    static_cast<void*>(out_sum_), static_cast<void*>(out_first_),
+    for (void* p : {static_cast<void*>(d_qs_), static_cast<void*>(slots_), static_cast<void*>(acc_),
+                    static_cast<void*>(out_key_), static_cast<void*>(out_sum_), static_cast<void*>(out_first_),
                     static_cast<void*>(out_count_), static_cast<void*>(err_)})
       if (p) cudaFree(p);
     d_qs_ = nullptr;
     slots_ = nullptr;
-    sum_ = nullptr;
-    cnt_ = first_ = out_first_ = out_count_ = nullptr;
+    acc_ = nullptr;
+    out_first_ = out_count_ = nullptr;
     out_key_ = nullptr;
     out_sum_ = nullptr;
     err_ = nullptr;
@@ -367,10 +447,8 @@ class Batch {
   int build_grid_ = 0, probe_grid_ = 0, out_grid_ = 0;
   int64_t slot_total_ = 0, acc_total_ = 0;
   QueryDesc* d_qs_ = nullptr;
-  uint64_t* slots_ = nullptr;
-  double* sum_ = nullptr;
-  unsigned long long* cnt_ = nullptr;
-  unsigned long long* first_ = nullptr;
+  unsigned long long* slots_ = nullptr;
+  Acc* acc_ = nullptr;
   int32_t* out_key_ = nullptr;
   double* out_sum_ = nullptr;
   unsigned long long* out_first_ = nullptr;
@@ -385,10 +463,6 @@ struct kdb_batch {
   kdb_ctx* owner;
   std::unique_ptr<kdb::Batch> b;
 };
-
-// the kdb_ctx layout lives in capi.cc; reach the Context through this hook
-kdb::Context* kdb_ctx_context(kdb_ctx* ctx);
-void kdb_ctx_set_error(kdb_ctx* ctx, const std::string& msg);
 
 namespace {
 
@@ -504,6 +578,7 @@ int kdb_batch_run(kdb_batch* b) {
     KDB_CUDA(cudaStreamSynchronize(kdb_ctx_context(b->owner)->stream));
     int e = b->b->CheckError();
     if (e == 3) throw kdb::Error(KDB_ERR_UNSUPPORTED, "batch dimension key is not unique");
+    if (e == 4) throw kdb::Error(KDB_ERR_CAPACITY, "batch join table overflow");
   });
 }
 

@@ -4,17 +4,12 @@
 #include <sstream>
 #include <unordered_map>
 
-#include "../../include/kdb_b200.h"
-#include "engine.h"
+#include "capi_internal.h"
 
 struct kdb_ctx {
   std::unique_ptr<kdb::Context> c;
   std::string err;
   std::unordered_map<std::string, std::unique_ptr<kdb::plan::Operator>> plans;
-};
-
-struct kdb_result {
-  kdb::HostResult r;
 };
 
 namespace {

@@ -157,6 +157,20 @@ Context::Context(int dev) : device(dev) {
   g_drv.Load();
 }
 
+Context::Context(Context& parent)
+    : device(parent.device), dry(parent.dry), num_sms(parent.num_sms), tables(parent.tables),
+      enums(parent.enums), skinner_budget(parent.skinner_budget), skinner_seed(parent.skinner_seed),
+      cache_(parent.cache_), owns_catalog_(false) {
+  if (dry) {
+    d_err = static_cast<int*>(DevAlloc(16));
+    return;
+  }
+  KDB_CUDA(cudaSetDevice(device));
+  KDB_CUDA(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
+  KDB_CUDA(cudaMalloc(&d_err, sizeof(int) * 4));
+  KDB_CUDA(cudaMemset(d_err, 0, sizeof(int) * 4));
+}
+
 Context::~Context() {
   if (dry) {
     std::free(stage_);
@@ -165,15 +179,18 @@ Context::~Context() {
   if (stage_) cudaFreeHost(stage_);
   cudaSetDevice(device);
   cudaStreamSynchronize(stream);
-  for (auto& [n, t] : tables)
-    for (auto& [cn, c] : t.cols) FreeColumn(c);
-  for (auto& [id, e] : enums) {
-    cudaFree(e.d_off);
-    cudaFree(e.d_chars);
-    cudaFree(e.d_rank);
+  if (owns_catalog_) {
+    for (auto& [n, t] : tables)
+      for (auto& [cn, c] : t.cols) FreeColumn(c);
+    for (auto& [id, e] : enums) {
+      cudaFree(e.d_off);
+      cudaFree(e.d_chars);
+      cudaFree(e.d_rank);
+    }
   }
-  for (auto& [k, p] : programs_)
-    if (p->module) g_drv.ModuleUnload(p->module);
+  if (cache_.use_count() == 1)
+    for (auto& [k, p] : cache_->programs)
+      if (p->module) g_drv.ModuleUnload(p->module);
   cudaFree(d_err);
   cudaStreamDestroy(stream);
 }
@@ -328,6 +345,8 @@ EnumDicts Context::HostEnums() const {
 }
 
 CUfunction Context::Kernel(const std::string& source, const std::string& name) {
+  std::lock_guard<std::mutex> lock(cache_->mu);
+  auto& programs_ = cache_->programs;
   auto it = programs_.find(source);
   if (it == programs_.end()) {
     auto prog = std::make_unique<Program>();

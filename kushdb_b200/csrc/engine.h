@@ -13,6 +13,7 @@
 #include <cstdint>
 #include <map>
 #include <memory>
+#include <mutex>
 #include <stdexcept>
 #include <string>
 #include <unordered_map>
@@ -92,6 +93,12 @@ struct Program {
   std::string log;
 };
 
+// Compiled pipelines shared by a context and its serving slots.
+struct ProgramCache {
+  std::mutex mu;
+  std::unordered_map<std::string, std::unique_ptr<Program>> programs;
+};
+
 // Host mirror of the device KArgs struct (passed by value).
 struct KArgs {
   uint64_t w[384];
@@ -121,6 +128,10 @@ class Context {
   // generated and compiled by NVRTC, nothing is allocated, copied or run,
   // and device reads return zeros.
   explicit Context(int device);
+  // A serving slot: its own stream, sharing `parent`'s resident tables, enum
+  // dictionaries and compiled pipelines (the parent must outlive it and must
+  // not change its tables while slots run).
+  explicit Context(Context& parent);
   ~Context();
 
   int device = 0;
@@ -186,7 +197,8 @@ class Context {
   EnumDicts HostEnums() const;
 
  private:
-  std::unordered_map<std::string, std::unique_ptr<Program>> programs_;
+  std::shared_ptr<ProgramCache> cache_ = std::make_shared<ProgramCache>();
+  bool owns_catalog_ = true;
   void* stage_ = nullptr;
   size_t stage_bytes_ = 0;
   void FreeColumn(DevColumn& c);

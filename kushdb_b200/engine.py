@@ -32,6 +32,7 @@ EXPORTS = [
     "kdb_result_free", "kdb_sort_pairs", "kdb_ctx_set_skinner", "kdb_last_skinner_episodes",
     "kdb_batch_create", "kdb_batch_configure", "kdb_batch_tune", "kdb_batch_config", "kdb_batch_run",
     "kdb_batch_run_timed", "kdb_batch_result", "kdb_batch_free", "kdb_sort_pairs_noalloc",
+    "kdb_server_start", "kdb_server_submit", "kdb_server_poll", "kdb_server_stats", "kdb_server_stop",
 ]
 
 _lib = None
@@ -92,6 +93,13 @@ def load_library(path: str = LIB_PATH):
     L.kdb_last_skinner_episodes.restype = I64
     L.kdb_last_skinner_episodes.argtypes = [P]
     L.kdb_sort_pairs_noalloc.argtypes = [P, P, I64, I32, P]
+    L.kdb_server_start.argtypes = [P, I32, I64, ctypes.POINTER(P)]
+    L.kdb_server_submit.restype = I64
+    L.kdb_server_submit.argtypes = [P, ctypes.c_char_p]
+    L.kdb_server_poll.argtypes = [P, I64, I64, ctypes.POINTER(P)]
+    L.kdb_server_stats.restype = I64
+    L.kdb_server_stats.argtypes = [P, ctypes.c_char_p, I64]
+    L.kdb_server_stop.argtypes = [P]
     declare_result_api(L, "kdb_")
     _lib = L
     return L
@@ -290,3 +298,70 @@ class Batch:
             self.close()
         except Exception:
             pass
+
+
+class Server:
+    """Request loop over an engine's resident tables (kdb_server_*): `slots`
+    worker threads with their own CUDA streams run queued plans concurrently
+    as slots and the device-memory budget allow."""
+
+    def __init__(self, engine: Engine, slots: int = 4, hbm_budget_bytes: int = 8 << 30):
+        self.engine = engine
+        self.lib = engine.lib
+        engine.register_enums()
+        h = ctypes.c_void_p()
+        engine._check(self.lib.kdb_server_start(engine.ctx, slots, hbm_budget_bytes, ctypes.byref(h)))
+        self.h = h
+
+    def submit(self, plan) -> int:
+        text = plan.to_json() if isinstance(plan, Operator) else plan
+        if isinstance(text, str):
+            text = text.encode()
+        self.engine.register_enums()
+        t = self.lib.kdb_server_submit(self.h, text)
+        if t < 0:
+            raise KdbError(int(t), self.lib.kdb_last_error(self.engine.ctx).decode())
+        return int(t)
+
+    def poll(self, ticket: int, wait_ms: int = 0):
+        """The ticket's Result once done, else None; raises if it failed."""
+        h = ctypes.c_void_p()
+        rc = self.lib.kdb_server_poll(self.h, ticket, wait_ms, ctypes.byref(h))
+        if rc == 1:
+            return None
+        self.engine._check(rc)
+        return Result.from_handle(self.lib, "kdb_", self.engine.ctx, h)
+
+    def wait(self, ticket: int, timeout_s: float = 600.0):
+        import time
+        end = time.monotonic() + timeout_s
+        while True:
+            r = self.poll(ticket, 100)
+            if r is not None:
+                return r
+            if time.monotonic() > end:
+                raise TimeoutError(f"request {ticket} not done after {timeout_s} s")
+
+    def stats(self):
+        import json
+        n = self.lib.kdb_server_stats(self.h, None, 0)
+        buf = ctypes.create_string_buffer(int(n))
+        self.lib.kdb_server_stats(self.h, buf, n)
+        return json.loads(buf.value.decode())
+
+    def close(self):
+        if self.h:
+            self.lib.kdb_server_stop(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()

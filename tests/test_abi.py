@@ -68,3 +68,14 @@ def test_errors_cross_the_abi_as_codes():
     with pytest.raises(RuntimeError):
         e.execute("{not json")
     e.close()
+
+
+def test_serving_needs_a_device_context():
+    from kushdb_b200.engine import KdbError, Server
+    e = Engine(-1)
+    with pytest.raises(KdbError, match="GPU"):
+        Server(e, slots=2)
+    lib = load_library()
+    assert lib.kdb_server_submit(None, b"{}") < 0
+    assert lib.kdb_server_poll(None, 1, 0, None) < 0
+    e.close()
