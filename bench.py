@@ -7,7 +7,7 @@ available).  Metric: rows/s (whole job), with the roofline of the dominant
 kernel against the measured HBM copy bandwidth.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--workload group_by|scan_agg|join_group|batched|serving]
+                    [--workload group_by|scan_agg|join_group|batched|serving|skinner]
 
 A step is one execution of the query over the resident table.  The timed
 region covers exactly K steps on the engine's CUDA stream (events), bracketed
@@ -240,6 +240,102 @@ def run_batched(args):
     print(json.dumps(line))
 
 
+def skinner_queries(seed0: int, count: int, min_rows: int = 10_000, max_rows: int = 3_000_000):
+    """JOB-style multiway joins: star and chain shapes of 6-8 tables with
+    log-uniform sizes, Zipf 0 / 1.5 foreign keys and LIKE '%tok%' filters."""
+    out = []
+    for i in range(count):
+        shape = "star" if i % 2 == 0 else "chain"
+        n_tables = 6 + i % 3
+        zipf = 1.5 if i % 4 >= 2 else 0.0
+        tables, tokens = wl.skinner_tables(shape, n_tables, min_rows=min_rows, max_rows=max_rows, zipf_s=zipf,
+                                           seed=seed0 + 31 * i, prefix=f"sk{seed0}_{i}_")
+        out.append((f"{shape}{n_tables}{'z' if zipf else ''}", tables, wl.skinner_plan(tables, tokens, shape)))
+    return out
+
+
+def train_join_prior(eng, budget: int, count: int = 16, max_rows: int = 300_000):
+    """Trains the learned join-order prior on queries disjoint from the
+    measured ones (random-order episodes of smaller instances)."""
+    from kushdb_b200.join_prior import fit_prior
+    train_q = skinner_queries(7000, count, max_rows=max_rows)
+    for _, tables, _ in train_q:
+        for t in tables:
+            eng.register_table(t)
+    t0 = time.perf_counter()
+    model, info = fit_prior(eng, [p for _, _, p in train_q], budget, seeds=(0, 1), steps=1500)
+    info["seconds"] = time.perf_counter() - t0
+    for _, tables, _ in train_q:
+        for t in tables:
+            eng.drop_table(t.name)
+    return model, info
+
+
+def run_skinner(args):
+    """Skinner multiway joins (C5 shapes) one at a time: device time,
+    episodes and tuples examined per query under plain UCT and under UCT
+    seeded by the learned prior, on the same resident tables."""
+    import torch
+    from kushdb_b200.engine import Engine
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    eng = Engine(local)
+    budget = args.skinner_budget
+    model, info = train_join_prior(eng, budget)
+    queries = skinner_queries(100, args.skinner_queries)
+    for _, tables, _ in queries:
+        for t in tables:
+            eng.register_table(t)
+    stream = torch.cuda.ExternalStream(eng.stream_handle())
+    per = {}
+    launches0 = eng.kernel_launches()
+    with ClockSampler(local) as clocks:
+        for policy in ("uct", "prior"):
+            eng.set_skinner_policy(policy, prior=model if policy == "prior" else None)
+            rows = []
+            for name, tables, plan in queries:
+                p = plan.to_json().encode()
+                eng.set_skinner(budget, 0)
+                for _ in range(args.warmup):
+                    eng.execute(p, fetch=False)
+                ms, eps, work = [], [], []
+                for s in range(args.steps):
+                    eng.set_skinner(budget, s)
+                    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                    e0.record(stream)
+                    n = eng.execute(p, fetch=False)
+                    e1.record(stream)
+                    e1.synchronize()
+                    ms.append(e0.elapsed_time(e1))
+                    eps.append(eng.last_skinner_episodes())
+                    work.append(eng.last_skinner_work())
+                rows.append({"query": name, "tables": len(tables), "rows": sum(t.rows for t in tables),
+                             "result_rows": int(n), "ms": statistics.median(ms),
+                             "episodes": statistics.median(eps), "work": statistics.median(work)})
+            per[policy] = rows
+    eng.set_skinner_policy("uct")
+    total = {k: sum(r["ms"] for r in v) for k, v in per.items()}
+    best = min(total, key=total.get)
+    nq = len(queries)
+    line = {
+        "metric": "queries_per_second", "value": nq / (total[best] / 1e3), "unit": "queries/s",
+        "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": total[best] / nq,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int32",
+        "data": "synthetic",
+        "config": {"workload": "skinner multiway joins (star/chain, 6-8 tables, rows log-uniform "
+                               "[1e4, 3e6], zipf 0/1.5, LIKE '%tok%' filters), one at a time",
+                   "queries": nq, "budget_per_episode": budget, "policy": best,
+                   "l2": "inputs larger than L2 (126 MB)"},
+        "policies": {k: {"ms_total": total[k], "episodes_total": sum(r["episodes"] for r in v),
+                         "work_total": sum(r["work"] for r in v)} for k, v in per.items()},
+        "prior_training": info,
+        "per_query": per,
+        "gpu_launches": eng.kernel_launches() - launches0,
+        "clocks": clocks.summary(),
+    }
+    print(json.dumps(line))
+
+
 def run_serving(args):
     """Serving form: a stream of requests mixing four query shapes (scan +
     aggregate, group-by, join + group-by + ORDER BY, Skinner multiway join)
@@ -335,9 +431,11 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="group_by",
-                    choices=["group_by", "scan_agg", "join_group", "batched", "serving"])
+                    choices=["group_by", "scan_agg", "join_group", "batched", "serving", "skinner"])
     ap.add_argument("--batch-queries", type=int, default=256)
     ap.add_argument("--batch-max-fact", type=int, default=6_000_000)
+    ap.add_argument("--skinner-budget", type=int, default=100_000)
+    ap.add_argument("--skinner-queries", type=int, default=8)
     ap.add_argument("--serving-requests", type=int, default=2000)
     ap.add_argument("--serving-slots", type=int, default=4)
     ap.add_argument("--serving-rate", type=float, default=1000.0)
@@ -355,6 +453,9 @@ def main():
         return
     if args.workload == "serving":
         run_serving(args)
+        return
+    if args.workload == "skinner":
+        run_skinner(args)
         return
 
     import torch
@@ -380,9 +481,19 @@ def main():
         res = eng.execute(plan)
     torch.cuda.synchronize()
 
+    # L2 flush between steps: write a 256 MiB buffer, then read another one,
+    # so the timed kernels start with none of their inputs in L2 and with no
+    # dirty flush lines left to write back while they run
     flush = None
     if algo_bytes < 2 * L2_BYTES:
-        flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device=f"cuda:{local}")
+        flush = (torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device=f"cuda:{local}"),
+                 torch.ones(64 * 1024 * 1024, dtype=torch.int32, device=f"cuda:{local}"))
+
+    def flush_l2():
+        if flush is not None:
+            with torch.cuda.stream(stream):
+                flush[0].fill_(1)
+                flush[1].sum()
 
     # timed region: K steps on the engine stream
     if dist:
@@ -392,9 +503,7 @@ def main():
     step_ms = []
     with ClockSampler(local) as clocks:
         for _ in range(args.steps):
-            if flush is not None:
-                with torch.cuda.stream(stream):
-                    flush.fill_(1)
+            flush_l2()
             e0 = torch.cuda.Event(enable_timing=True)
             e1 = torch.cuda.Event(enable_timing=True)
             e0.record(stream)
@@ -416,6 +525,7 @@ def main():
     eng.set_profiling(True)
     kern = []
     for _ in range(5):
+        flush_l2()
         eng.execute(plan)
         kern.append(eng.last_kernels())
     eng.set_profiling(False)
@@ -475,7 +585,7 @@ def main():
             cpu = {"value": None, "unit": "rows/s", "cores": 1, "kind": "port", "sample": f"failed: {ex}"}
 
     cfg = dict(cfg)
-    cfg["l2"] = "flushed between steps (256 MiB write)" if flush is not None else \
+    cfg["l2"] = "flushed between steps (256 MiB write, then 256 MiB read)" if flush is not None else \
         "inputs larger than L2 (126 MB)"
     line = {
         "metric": "rows_per_second", "value": value, "unit": "rows/s", "n_gpus": world,

@@ -113,6 +113,13 @@ int kdb_query_execute(kdb_ctx* ctx, const char* plan_json, kdb_result** out);
  * excluding result download, and the bytes read from table columns. */
 double kdb_last_query_device_ms(kdb_ctx* ctx);
 
+/* Prepared queries (on by default): the first run of a plan text records
+ * its launches; later runs of the same text over unchanged tables replay
+ * them as one CUDA graph (no code generation or per-kernel launches) and
+ * keep that plan's device buffers between runs.  Any table or enum change
+ * invalidates them; Skinner joins and profiling runs are never replayed. */
+int kdb_ctx_set_prepared_queries(kdb_ctx* ctx, int32_t on);
+
 /* ---- Skinner join options (runtime/skinner_join_executor.cc:20-22) ------
  * Work budget per episode (tuples examined, the reference's
  * --budget_per_episode) and the UCT random seed (--join_seed).  Join order
@@ -120,6 +127,40 @@ double kdb_last_query_device_ms(kdb_ctx* ctx);
 int kdb_ctx_set_skinner(kdb_ctx* ctx, int64_t budget_per_episode, uint32_t seed);
 /* Episodes the last SKINNER_JOIN of the last query ran. */
 int64_t kdb_last_skinner_episodes(kdb_ctx* ctx);
+/* Tuples examined by all episodes of the last Skinner join. */
+int64_t kdb_last_skinner_work(kdb_ctx* ctx);
+
+/* ---- learned join-order prior (no reference counterpart) ----------------
+ * A 64 -> 128 -> 128 -> 128 -> 1 ReLU MLP (fp32) predicting the episode
+ * reward of appending a table to a join-order prefix, with hand-written
+ * CUDA forward / backward / Adam kernels.  Policies of the Skinner join:
+ *   0 UCT as the reference (runtime/skinner_join_executor.cc:779-838);
+ *   1 UCT seeded by the prior: every action starts as tried once with the
+ *     predicted reward and playouts follow the prior, observed rewards
+ *     overrule it; joins of more than 8 tables fall back to 0;
+ *   2 uniformly random connected orders (collects training data).
+ * The policy never changes a result, only the order search.  With
+ * log_samples set, every (prefix, next table) step of every episode is
+ * recorded as a feature row and the episode's reward. */
+typedef struct kdb_mlp kdb_mlp;
+int32_t kdb_mlp_num_features(void);
+int64_t kdb_mlp_num_params(void);
+int kdb_mlp_create(kdb_ctx* ctx, uint32_t seed, kdb_mlp** out);
+const char* kdb_mlp_last_error(kdb_mlp* m);
+int kdb_mlp_set_params(kdb_mlp* m, const float* params, int64_t n);
+int kdb_mlp_get_params(kdb_mlp* m, float* params, int64_t n);
+/* n <= 4096 rows of kdb_mlp_num_features() floats -> n predictions */
+int kdb_mlp_forward(kdb_mlp* m, const float* x, int64_t n, float* y);
+/* gradient of mean((y - t)^2) w.r.t. every parameter, without an update */
+int kdb_mlp_gradient(kdb_mlp* m, const float* x, const float* t, int64_t n, float* grad, double* loss);
+/* one Adam step (beta 0.9 / 0.999); loss before the step */
+int kdb_mlp_train_step(kdb_mlp* m, const float* x, const float* t, int64_t n, float lr, double* loss);
+void kdb_mlp_free(kdb_mlp* m);
+/* The model must outlive its use by the context. */
+int kdb_ctx_set_skinner_policy(kdb_ctx* ctx, int32_t policy, kdb_mlp* prior, int32_t log_samples);
+/* Samples of the last Skinner join with logging on: copies min(n, cap) rows
+ * of features (row-major) and rewards; returns n. */
+int64_t kdb_last_skinner_samples(kdb_ctx* ctx, float* features, float* rewards, int64_t cap);
 
 /* ---- device sort (runtime/vector.cc:45-110) ------------------------------
  * Stable sort of n (key, value) pairs already in device memory by the low

@@ -7,10 +7,21 @@
 #include "capi_internal.h"
 
 struct kdb_ctx {
+  // parsed plans by their JSON text, each with its prepared (recorded)
+  // execution once it has run
+  struct Entry {
+    std::unique_ptr<kdb::plan::Operator> plan;
+    std::unique_ptr<kdb::PreparedQuery> prepared;
+  };
   std::unique_ptr<kdb::Context> c;
   std::string err;
-  std::unordered_map<std::string, std::unique_ptr<kdb::plan::Operator>> plans;
+  std::unordered_map<std::string, Entry> plans;
+  bool prepare = true;
 };
+
+namespace {
+constexpr size_t kMaxPreparedTotal = size_t(4) << 30;  // device memory held by all prepared queries
+}
 
 namespace {
 
@@ -202,11 +213,31 @@ int kdb_query_execute(kdb_ctx* ctx, const char* plan_json, kdb_result** out) {
     auto it = cache.find(plan_json);
     if (it == cache.end()) {
       if (cache.size() >= 256) cache.clear();
-      it = cache.emplace(plan_json, kdb::plan::ParsePlan(plan_json)).first;
+      kdb_ctx::Entry e;
+      e.plan = kdb::plan::ParsePlan(plan_json);
+      it = cache.emplace(plan_json, std::move(e)).first;
     }
     auto res = std::make_unique<kdb_result>();
-    res->r = kdb::ExecutePlan(*ctx->c, *it->second);
+    kdb_ctx::Entry& entry = it->second;
+    res->r = kdb::ExecutePlan(*ctx->c, *entry.plan, ctx->prepare ? &entry.prepared : nullptr);
+    if (entry.prepared) {
+      // keep the device memory held by prepared queries bounded
+      size_t total = 0;
+      for (auto& [k, e] : cache)
+        if (e.prepared) total += e.prepared->arena->bytes();
+      if (total > kMaxPreparedTotal)
+        for (auto& [k, e] : cache)
+          if (&e != &entry) e.prepared.reset();
+    }
     *out = res.release();
+  });
+}
+
+int kdb_ctx_set_prepared_queries(kdb_ctx* ctx, int32_t on) {
+  return Guard(ctx, [&] {
+    ctx->prepare = on != 0;
+    if (!ctx->prepare)
+      for (auto& [k, e] : ctx->plans) e.prepared.reset();
   });
 }
 
@@ -220,13 +251,31 @@ int kdb_ctx_set_skinner(kdb_ctx* ctx, int64_t budget_per_episode, uint32_t seed)
 
 int64_t kdb_last_skinner_episodes(kdb_ctx* ctx) { return ctx ? ctx->c->last_skinner_episodes : -1; }
 
+int64_t kdb_last_skinner_work(kdb_ctx* ctx) { return ctx ? ctx->c->last_skinner_work : -1; }
+
+int64_t kdb_last_skinner_samples(kdb_ctx* ctx, float* features, float* rewards, int64_t cap) {
+  if (!ctx) return KDB_ERR_INVALID;
+  const auto& f = ctx->c->skinner_features;
+  const auto& r = ctx->c->skinner_rewards;
+  const int64_t n = static_cast<int64_t>(r.size());
+  const int64_t k = std::min<int64_t>(n, std::max<int64_t>(cap, 0));
+  const size_t width = r.empty() ? 0 : f.size() / r.size();
+  if (features && k) std::memcpy(features, f.data(), sizeof(float) * width * k);
+  if (rewards && k) std::memcpy(rewards, r.data(), sizeof(float) * k);
+  return n;
+}
+
 int kdb_sort_pairs(kdb_ctx* ctx, uint64_t* d_keys, uint32_t* d_vals, int64_t n, int32_t key_bits) {
   return Guard(ctx, [&] {
     if (n < 0 || (n > 0 && (!d_keys || !d_vals))) throw kdb::Error(KDB_ERR_INVALID, "bad sort arguments");
     if (key_bits < 1 || key_bits > 64) throw kdb::Error(KDB_ERR_INVALID, "key_bits must be in [1, 64]");
-    kdb::Arena arena(*ctx->c);
-    ctx->c->RadixSortPairs(d_keys, d_vals, n, arena, key_bits);
+    ctx->c->BeginQueryProfile();
+    {
+      kdb::Arena arena(*ctx->c);
+      ctx->c->RadixSortPairs(d_keys, d_vals, n, arena, key_bits);
+    }
     if (!ctx->c->dry) KDB_CUDA(cudaStreamSynchronize(ctx->c->stream));
+    ctx->c->EndQueryProfile();
   });
 }
 

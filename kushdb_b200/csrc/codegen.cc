@@ -20,11 +20,13 @@
 #include <cstdio>
 #include <cstring>
 #include <functional>
+#include <map>
 #include <random>
 #include <set>
 #include <sstream>
 
 #include "engine.h"
+#include "join_prior.h"
 
 namespace kdb {
 namespace {
@@ -531,6 +533,13 @@ struct JoinTable {
   MatBuffer build;
   uint64_t* slots = nullptr;
   uint64_t mask = 0;
+  // grouped form (Skinner indexes): rows sorted by key hash (`srow`, with
+  // their hashes `sh`), and `slots` holding one entry per distinct hash
+  // (hash << 32 | first sorted index + 1) with the group's length in `lens`
+  uint32_t* lens = nullptr;
+  uint64_t* sh = nullptr;
+  uint32_t* srow = nullptr;
+  int64_t n = 0;
 };
 
 class Executor {
@@ -538,6 +547,9 @@ class Executor {
   Executor(Context& ctx, Arena& arena) : ctx_(ctx), arena_(arena) {}
 
   HostResult Run(const Operator& root);
+  MatBuffer MaterializeRoot(const Operator& root) { return Materialize(root); }
+  // the root's rows from the device into a host result
+  HostResult Download(const MatBuffer& m, const Operator& root, bool check_error = false);
   int64_t bytes_scanned = 0;
 
  private:
@@ -635,6 +647,7 @@ class Executor {
   MatBuffer RunGroupByDense(const Operator& op, const std::vector<AggPlan>& plans, const KeyLayout& kl);
   void BuildJoin(const Operator& op);
   JoinTable BuildIndex(const MatBuffer& m, const std::vector<int>& key_cols);
+  JoinTable BuildGroupedIndex(const MatBuffer& m, int key_col);
   void EmitProbe(KernelSource& ks, ExprGen& eg, const JoinTable& jt,
                  const std::vector<int>& build_key_cols, const std::vector<CVal>& probe_keys,
                  const std::function<void(const std::vector<CVal>&, const std::string&)>& on_match);
@@ -941,6 +954,75 @@ JoinTable Executor::BuildIndex(const MatBuffer& m, const std::vector<int>& key_c
   return jt;
 }
 
+// Index for the Skinner join's lookups (the role of the reference's column
+// indexes, runtime/column_index.cc / memory_column_index.cc: key -> rows):
+// rows sorted by key hash, and a table of distinct hashes pointing at each
+// run.  A lookup costs one probe of the distinct table plus its matches, so
+// heavily repeated keys (Zipf) neither form long probe clusters nor slow
+// the lookups of other keys.  Rows with a NULL key are left out.
+JoinTable Executor::BuildGroupedIndex(const MatBuffer& m, int key_col) {
+  JoinTable jt;
+  jt.build = m;
+  const int64_t n = m.rows;
+  jt.n = n;
+  uint64_t cap = 1024;
+  while (cap < static_cast<uint64_t>(n) * 2) cap <<= 1;
+  jt.mask = cap - 1;
+  jt.slots = arena_.AllocT<uint64_t>(cap);
+  jt.lens = arena_.AllocT<uint32_t>(cap);
+  jt.sh = arena_.AllocT<uint64_t>(std::max<int64_t>(n, 1));
+  jt.srow = arena_.AllocT<uint32_t>(std::max<int64_t>(n, 1));
+  ctx_.Memset(jt.slots, 0, cap * sizeof(uint64_t));
+  ctx_.Memset(jt.lens, 0, cap * sizeof(uint32_t));
+  if (n == 0) return jt;
+  const uint64_t kNullHash = 1ULL << 32;  // sorts after every real hash
+  {
+    KernelSource ks;
+    ExprGen eg(ctx_, ks);
+    std::string N = ks.Word(static_cast<uint64_t>(n));
+    std::string SH = ks.Ptr(jt.sh, "uint64_t"), SR = ks.Ptr(jt.srow, "uint32_t");
+    ks.Open("for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < (int64_t)" + N +
+            "; r += (int64_t)gridDim.x * blockDim.x)");
+    auto vals = LoadMatRow(ks, eg, m, "r", nullptr);
+    const CVal& key = vals.at(key_col);
+    ks.L(SH + "[r] = (" + key.n + ") ? " + std::to_string(kNullHash) + "ULL : (uint64_t)" + JoinHash(eg, {key}) + ";");
+    ks.L(SR + "[r] = (uint32_t)r;");
+    ks.Close();
+    LaunchPipeline(ks, n, "index keys");
+  }
+  ctx_.RadixSortPairs(jt.sh, jt.srow, n, arena_, 33);
+  for (int pass = 0; pass < 2; pass++) {
+    // pass 0: the first row of every run claims a slot; pass 1: the last row
+    // of every run writes the run's length into that slot
+    KernelSource ks;
+    std::string N = ks.Word(static_cast<uint64_t>(n));
+    std::string SH = ks.Ptr(jt.sh, "uint64_t", true), SL = ks.Ptr(jt.slots, "uint64_t");
+    std::string LN = ks.Ptr(jt.lens, "uint32_t"), M = ks.Word(jt.mask);
+    ks.Open("for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < (int64_t)" + N +
+            "; i += (int64_t)gridDim.x * blockDim.x)");
+    ks.L("const uint64_t h = " + SH + "[i];");
+    ks.L("if (h >= " + std::to_string(kNullHash) + "ULL) continue;");
+    if (pass == 0) {
+      ks.L("if (i > 0 && " + SH + "[i - 1] == h) continue;");
+      ks.L("kdb_join_insert(" + SL + ", " + M + ", (uint32_t)h, (uint32_t)i);");
+    } else {
+      ks.L("if (i + 1 < (int64_t)" + N + " && " + SH + "[i + 1] == h) continue;");
+      ks.L("uint64_t s = kdb_mix64((uint32_t)h) & " + M + ";");
+      ks.Open("for (uint64_t k = 0; k <= " + M + "; k++, s = (s + 1) & " + M + ")");
+      ks.L("const uint64_t e = " + SL + "[s];");
+      ks.L("if (e == 0) break;");
+      ks.Open("if ((uint32_t)(e >> 32) == (uint32_t)h)");
+      ks.L(LN + "[s] = (uint32_t)(i + 1 - ((int64_t)(uint32_t)e - 1));");
+      ks.L("break;");
+      ks.Close();
+      ks.Close();
+    }
+    ks.Close();
+    LaunchPipeline(ks, n, pass == 0 ? "index runs" : "index lengths");
+  }
+  return jt;
+}
+
 void Executor::BuildJoin(const Operator& op) {
   if (joins_.count(&op)) return;
   MatBuffer left = Materialize(op.child(0));
@@ -962,6 +1044,7 @@ MatBuffer Executor::MaterializeStream(const Operator& op, const uint32_t* order,
   if (!ordered_src) Prepare(op);
   int64_t cap = ordered_src ? ordered_src->rows : RowBound(op);
   for (int attempt = 0; attempt < 3; attempt++) {
+    const auto mark = ctx_.RecordMark();
     KernelSource ks;
     ExprGen eg(ctx_, ks);
     const auto& schema = op.output;
@@ -1022,6 +1105,7 @@ MatBuffer Executor::MaterializeStream(const Operator& op, const uint32_t* order,
     }
     if (ordered_src) throw Error(-4, "ordered materialisation overflow");
     cap = produced;
+    ctx_.RecordTruncate(mark);
   }
   throw Error(-4, "materialisation did not converge");
 }
@@ -1394,9 +1478,15 @@ MatBuffer Executor::RunGroupByDense(const Operator& op, const std::vector<AggPla
   const int W = static_cast<int>(words.size());
   const int64_t K = D * W;
   // block size and the launch-bounds occupancy hint (env overrides for tuning)
-  const int block = std::getenv("KDB_DENSE_BLOCK") ? std::atoi(std::getenv("KDB_DENSE_BLOCK")) : 256;
-  const int min_blocks = std::getenv("KDB_DENSE_MINB") ? std::atoi(std::getenv("KDB_DENSE_MINB")) : 1;
-  const int grid_per_sm = std::getenv("KDB_DENSE_GRID") ? std::atoi(std::getenv("KDB_DENSE_GRID")) : 2;
+  const int block = std::getenv("KDB_DENSE_BLOCK") ? std::atoi(std::getenv("KDB_DENSE_BLOCK")) : 128;
+  const int min_blocks = std::getenv("KDB_DENSE_MINB") ? std::atoi(std::getenv("KDB_DENSE_MINB")) : 2;
+  const int grid_per_sm = std::getenv("KDB_DENSE_GRID") ? std::atoi(std::getenv("KDB_DENSE_GRID")) : 4;
+  // Accumulators in registers (every row updates every group's words under a
+  // predicate) or, for larger groups x words, in per-thread shared-memory
+  // slots indexed by the group id (a row touches only its own group's words).
+  const char* smem_env = std::getenv("KDB_DENSE_SMEM");
+  const bool smem_fits = K * block * 8 <= 48 * 1024;  // static shared memory limit
+  const bool in_smem = smem_fits && (smem_env ? std::atoi(smem_env) != 0 : K > 16);
 
   auto reg = [&](int64_t g, int w) { return "a" + std::to_string(g) + "_" + std::to_string(w); };
   auto combine = [&](WordKind k, const std::string& a, const std::string& b) -> std::string {
@@ -1417,8 +1507,17 @@ MatBuffer Executor::RunGroupByDense(const Operator& op, const std::vector<AggPla
 
   KernelSource ks;
   ExprGen eg(ctx_, ks);
-  for (int64_t g = 0; g < D; g++)
-    for (int w = 0; w < W; w++) ks.L(words[w].ctype + " " + reg(g, w) + " = " + words[w].init + ";");
+  auto slot = [&](int w) { return "s" + std::to_string(w); };
+  const std::string DB = std::to_string(D * block);
+  if (in_smem) {
+    for (int w = 0; w < W; w++) {
+      ks.L("__shared__ " + words[w].ctype + " " + slot(w) + "[" + DB + "];");
+      ks.L("for (int i = threadIdx.x; i < " + DB + "; i += blockDim.x) " + slot(w) + "[i] = " + words[w].init + ";");
+    }
+  } else {
+    for (int64_t g = 0; g < D; g++)
+      for (int w = 0; w < W; w++) ks.L(words[w].ctype + " " + reg(g, w) + " = " + words[w].init + ";");
+  }
   int64_t src_rows = 0;
   auto consume = [&](const std::vector<CVal>& in, const std::string& pos) {
     Scope s;
@@ -1463,6 +1562,18 @@ MatBuffer Executor::RunGroupByDense(const Operator& op, const std::vector<AggPla
       cv[w] = ks.Fresh("c");
       ks.L(words[w].ctype + " " + cv[w] + " = " + contrib[w] + ";");
     }
+    if (in_smem) {
+      // a key outside the domain matches no group (as in the register form)
+      ks.Open("if ((uint64_t)" + G + " < " + std::to_string(D) + "ULL)");
+      std::string I = ks.Fresh("si");
+      ks.L("const int " + I + " = (int)" + G + " * " + std::to_string(block) + " + threadIdx.x;");
+      for (int w = 0; w < W; w++) {
+        std::string upd = slot(w) + "[" + I + "] = " + combine(words[w].kind, slot(w) + "[" + I + "]", cv[w]) + ";";
+        ks.L(active[w] == "true" ? upd : "if (" + active[w] + ") " + upd);
+      }
+      ks.Close();
+      return;
+    }
     for (int64_t g = 0; g < D; g++) {
       std::string h = ks.Fresh("h");
       ks.L("bool " + h + " = " + G + " == " + std::to_string(g) + ";");
@@ -1479,6 +1590,27 @@ MatBuffer Executor::RunGroupByDense(const Operator& op, const std::vector<AggPla
                                                 static_cast<int64_t>(ctx_.num_sms) * grid_per_sm));
   uint64_t* part = arena_.AllocT<uint64_t>(static_cast<size_t>(grid) * K);
   std::string PP = ks.Ptr(part, "uint64_t");
+  if (in_smem) {
+    // per (group, word): fold the block's thread slots in thread order
+    ks.L("__syncthreads();");
+    ks.Open("for (int k = threadIdx.x; k < " + std::to_string(K) + "; k += blockDim.x)");
+    ks.L("const int g = k / " + std::to_string(W) + ", w = k % " + std::to_string(W) + ";");
+    ks.L("uint64_t acc = 0;");
+    ks.Open("switch (w)");
+    for (int w = 0; w < W; w++) {
+      const std::string base = "g * " + std::to_string(block);
+      ks.Open("case " + std::to_string(w) + ":");
+      ks.L(words[w].ctype + " v = " + slot(w) + "[" + base + "];");
+      ks.L("for (int i = 1; i < " + std::to_string(block) + "; i++) v = " +
+           combine(words[w].kind, "v", slot(w) + "[" + base + " + i]") + ";");
+      ks.L("acc = " + to_bits(words[w], "v") + ";");
+      ks.L("break;");
+      ks.Close();
+    }
+    ks.Close();
+    ks.L(PP + "[(int64_t)blockIdx.x * " + std::to_string(K) + " + k] = acc;");
+    ks.Close();
+  } else {
   ks.L("__shared__ uint64_t red[" + std::to_string(block / 32) + "][" + std::to_string(K) + "];");
   ks.L("const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;");
   for (int64_t g = 0; g < D; g++)
@@ -1503,6 +1635,7 @@ MatBuffer Executor::RunGroupByDense(const Operator& op, const std::vector<AggPla
   ks.Close();
   ks.L(PP + "[(int64_t)blockIdx.x * " + std::to_string(K) + " + k] = acc;");
   ks.Close();
+  }
   {
     std::string src = ks.Kernel("kdb_group_by_dense", block, min_blocks);
     CUfunction f = ctx_.Kernel(src, "kdb_group_by_dense");
@@ -1637,6 +1770,7 @@ MatBuffer Executor::RunGroupBy(const Operator& op) {
     while (cap < want) cap <<= 1;
   }
   for (int attempt = 0; attempt < 8; attempt++) {
+    const auto mark = ctx_.RecordMark();
     uint64_t mask = cap - 1;
     uint64_t* slots = arena_.AllocT<uint64_t>(cap);
     uint64_t* first = arena_.AllocT<uint64_t>(cap);
@@ -1768,6 +1902,7 @@ MatBuffer Executor::RunGroupBy(const Operator& op) {
     } catch (const Error& e) {
       if (e.code == -4 && !kl.small_domain) {
         cap <<= 3;
+        ctx_.RecordTruncate(mark);
         continue;
       }
       throw;
@@ -2093,6 +2228,12 @@ class JoinEnv {
   virtual bool IsConnected(const std::set<int>& joined, int table) = 0;
   virtual bool IsComplete() = 0;
   virtual double Execute(const std::vector<int>& order) = 0;
+  // Learned prior: predicted episode reward of appending each of `cands`
+  // to the tables in `joined` (a bit mask).
+  virtual bool HasPrior() const { return false; }
+  virtual void PriorValues(uint64_t joined, const std::vector<int>& cands, std::vector<double>& out) {
+    out.assign(cands.size(), 0.0);
+  }
 };
 
 class UctNode {
@@ -2112,6 +2253,7 @@ class UctNode {
         unjoined_.push_back(t);
         table_of_action_[a++] = t;
       }
+    InitPrior();
   }
 
   UctNode(int round, UctNode& parent, int joined_table, uint32_t seed)
@@ -2129,6 +2271,7 @@ class UctNode {
       for (int a = 0; a < num_actions_; a++) recommended_.insert(a);
     for (int a = 0; a < num_actions_; a++)
       if (recommended_.count(a)) priority_.push_back(a);
+    InitPrior();
   }
 
   double Sample(int round, std::vector<int>& order) {
@@ -2147,6 +2290,27 @@ class UctNode {
   }
 
  private:
+  // With a learned prior every action starts as tried once with the
+  // predicted reward: the search begins at the prior's choice and the
+  // observed rewards overrule it (UCT stays the judge).
+  void InitPrior() {
+    if (!env_.HasPrior() || num_actions_ == 0) return;
+    std::vector<double> v;
+    env_.PriorValues(Mask(joined_), table_of_action_, v);
+    priority_.clear();
+    for (int a = 0; a < num_actions_; a++) {
+      tries_[a] = 1;
+      reward_[a] = v[a];
+    }
+    visits_ = num_actions_;
+  }
+
+  static uint64_t Mask(const std::set<int>& s) {
+    uint64_t m = 0;
+    for (int t : s) m |= 1ULL << t;
+    return m;
+  }
+
   double Playout(std::vector<int>& order) {
     int last = order[joined_.size()];
     std::set<int> cur(joined_.begin(), joined_.end());
@@ -2154,6 +2318,26 @@ class UctNode {
     std::vector<int> rest;
     for (int t = 0; t < num_tables_; t++)
       if (!joined_.count(t) && t != last) rest.push_back(t);
+    if (env_.HasPrior()) {  // greedy continuation by the prior among connected tables
+      for (int pos = static_cast<int>(joined_.size()) + 1; pos < num_tables_; pos++) {
+        std::vector<int> cands;
+        for (int t : rest)
+          if (!cur.count(t)) cands.push_back(t);
+        std::vector<double> v;
+        env_.PriorValues(Mask(cur), cands, v);
+        int pick = -1;
+        double best = -1e300;
+        for (int pass = 0; pass < 2 && pick < 0; pass++)
+          for (size_t i = 0; i < cands.size(); i++)
+            if ((pass == 1 || env_.IsConnected(cur, cands[i])) && v[i] > best) {
+              best = v[i];
+              pick = cands[i];
+            }
+        order[pos] = pick;
+        cur.insert(pick);
+      }
+      return env_.Execute(order);
+    }
     std::shuffle(rest.begin(), rest.end(), rng_);
     for (int pos = static_cast<int>(joined_.size()) + 1; pos < num_tables_; pos++) {
       int pick = -1;
@@ -2239,12 +2423,92 @@ class SkinnerEngine : public JoinEnv {
       collect(*c, m);
       cond_tables_.push_back(m);
     }
+    adj_.assign(T_, 0);
     for (const auto& pr : preds_) {
       connected_.insert({pr.ta, pr.tb});
       connected_.insert({pr.tb, pr.ta});
+      adj_[pr.ta] |= 1ULL << pr.tb;
+      adj_[pr.tb] |= 1ULL << pr.ta;
     }
     index_for_ = std::move(index_for);
   }
+
+  bool HasPrior() const override {
+    return ctx_.skinner_policy == 1 && ctx_.join_prior != nullptr && T_ <= kPriorTables;
+  }
+
+  void PriorValues(uint64_t joined, const std::vector<int>& cands, std::vector<double>& out) override {
+    auto it = prior_cache_.find(joined);
+    if (it == prior_cache_.end()) {
+      // one forward pass for every table not yet joined
+      std::vector<int> all;
+      for (int t = 0; t < T_; t++)
+        if (!(joined >> t & 1ULL)) all.push_back(t);
+      std::vector<float> x(all.size() * JoinPrior::kIn), y(all.size());
+      for (size_t i = 0; i < all.size(); i++) Features(joined, all[i], &x[i * JoinPrior::kIn]);
+      if (!all.empty() && !ctx_.dry) ctx_.join_prior->Forward(x.data(), static_cast<int64_t>(all.size()), y.data());
+      std::vector<double> v(T_, 0.0);
+      for (size_t i = 0; i < all.size(); i++) v[all[i]] = y[i];
+      it = prior_cache_.emplace(joined, std::move(v)).first;
+    }
+    out.resize(cands.size());
+    for (size_t i = 0; i < cands.size(); i++) out[i] = it->second[cands[i]];
+  }
+
+  // Features of appending table `cand` to the tables in `joined`: per table
+  // slot (6 each, 8 slots) presence, log cardinality after the table's
+  // filters, joined, candidate, linked to the joined set, linked to the
+  // candidate; then candidate-centred summaries.  Only the join graph and
+  // the cardinalities enter, so a (joined set, candidate) pair always maps
+  // to the same vector.
+  void Features(uint64_t joined, int cand, float* f) const {
+    std::fill(f, f + JoinPrior::kIn, 0.f);
+    auto lrows = [&](int t) { return static_cast<float>(std::log2(1.0 + static_cast<double>(cards_[t])) / 24.0); };
+    auto linked = [&](int t, uint64_t set) { return (adj_[t] & set) != 0; };
+    const uint64_t cand_bit = 1ULL << cand;
+    int njoined = 0;
+    for (int t = 0; t < T_ && t < kPriorTables; t++) {
+      float* g = f + 6 * t;
+      const bool in = joined >> t & 1ULL;
+      njoined += in;
+      g[0] = 1.f;
+      g[1] = lrows(t);
+      g[2] = in ? 1.f : 0.f;
+      g[3] = t == cand ? 1.f : 0.f;
+      g[4] = linked(t, joined) ? 1.f : 0.f;
+      g[5] = linked(t, cand_bit) ? 1.f : 0.f;
+    }
+    float min_other = 0.f, max_other = 0.f, min_joined = 0.f;
+    int smaller = 0, nb_unjoined = 0, nb_joined = 0;
+    bool any_other = false, any_joined = false;
+    for (int t = 0; t < T_; t++) {
+      if (t == cand) continue;
+      const float l = lrows(t);
+      if (joined >> t & 1ULL) {
+        min_joined = any_joined ? std::min(min_joined, l) : l;
+        any_joined = true;
+        nb_joined += (adj_[cand] >> t) & 1ULL;
+      } else {
+        min_other = any_other ? std::min(min_other, l) : l;
+        max_other = any_other ? std::max(max_other, l) : l;
+        any_other = true;
+        smaller += cards_[t] < cards_[cand];
+        nb_unjoined += (adj_[cand] >> t) & 1ULL;
+      }
+    }
+    f[48] = njoined / 8.f;
+    f[49] = T_ / 8.f;
+    f[50] = lrows(cand);
+    f[51] = linked(cand, joined) ? 1.f : 0.f;
+    f[52] = min_other;
+    f[53] = smaller / 8.f;
+    f[54] = nb_unjoined / 8.f;
+    f[55] = nb_joined / 8.f;
+    f[56] = max_other;
+    f[57] = min_joined;
+  }
+
+  int64_t work() const { return total_work_; }
 
   bool IsConnected(const std::set<int>& joined, int table) override {
     for (int t : joined)
@@ -2267,18 +2531,64 @@ class SkinnerEngine : public JoinEnv {
     bool empty = false;
     for (int64_t c : cards_) empty |= c == 0;
     if (!empty) {
+      beg_ = arena_.AllocT<uint64_t>(kMaxSlice);
+      offs_ = arena_.AllocT<uint64_t>(kMaxSlice + 1);
       Generate();
       std::vector<int> order(T_);
       for (size_t i = 0; i < prefix.size(); i++) order[i] = prefix[i];
-      UctNode root(0, T_, *this, prefix, seed_);
-      int round = 0;
-      while (!IsComplete() && episodes_ < (ctx_.dry ? 1 : (1 << 24))) {
-        round++;
-        root.Sample(round, order);
+      const int64_t max_episodes = ctx_.dry ? 1 : (1 << 24);
+      if (ctx_.skinner_policy == 2) {
+        // uniformly random connected orders (training data for the prior)
+        std::mt19937_64 rng(seed_);
+        while (!IsComplete() && episodes_ < max_episodes) {
+          uint64_t in = 0;
+          for (size_t i = 0; i < prefix.size(); i++) in |= 1ULL << prefix[i];
+          for (int pos = static_cast<int>(prefix.size()); pos < T_; pos++) {
+            std::vector<int> linked, any;
+            for (int t = 0; t < T_; t++)
+              if (!(in >> t & 1ULL)) {
+                any.push_back(t);
+                if (adj_[t] & in) linked.push_back(t);
+              }
+            const std::vector<int>& from = linked.empty() ? any : linked;
+            order[pos] = from[rng() % from.size()];
+            in |= 1ULL << order[pos];
+          }
+          Execute(order);
+        }
+      } else {
+        UctNode root(0, T_, *this, prefix, seed_);
+        int round = 0;
+        while (!IsComplete() && episodes_ < max_episodes) {
+          round++;
+          root.Sample(round, order);
+        }
       }
+      LogSamples(prefix.size());
     }
     out_.rows = produced_;
     return out_;
+  }
+
+  // (features, reward) of every choice of every episode, for training the
+  // prior
+  void LogSamples(size_t prefix_len) {
+    ctx_.skinner_features.clear();
+    ctx_.skinner_rewards.clear();
+    if (!ctx_.skinner_log || T_ > kPriorTables) return;
+    constexpr size_t kMaxSamples = 1 << 16;
+    for (const auto& [order, reward] : log_) {
+      uint64_t in = 0;
+      for (size_t d = 0; d < prefix_len; d++) in |= 1ULL << order[d];
+      for (int d = static_cast<int>(prefix_len); d + 1 < T_; d++) {
+        if (ctx_.skinner_rewards.size() >= kMaxSamples) return;
+        const size_t base = ctx_.skinner_features.size();
+        ctx_.skinner_features.resize(base + JoinPrior::kIn);
+        Features(in, order[d], &ctx_.skinner_features[base]);
+        ctx_.skinner_rewards.push_back(static_cast<float>(reward));
+        in |= 1ULL << order[d];
+      }
+    }
   }
 
   int64_t episodes() const { return episodes_; }
@@ -2287,7 +2597,7 @@ class SkinnerEngine : public JoinEnv {
     episodes_++;
     int L = order[0];
     int64_t remaining = cards_[L] - offsets_[L];
-    int64_t len = std::max<int64_t>(1, std::min<int64_t>(slice_est_[L], remaining));
+    int64_t len = std::max<int64_t>(1, std::min<int64_t>({slice_est_[L], remaining, kMaxSlice}));
     int64_t s0 = offsets_[L], s1 = s0 + len;
     KArgs a = args_;
     // order, lookup plan and condition schedule of this order
@@ -2329,7 +2639,13 @@ class SkinnerEngine : public JoinEnv {
     for (int attempt = 0; attempt < 8; attempt++) {
       a.w[w_cap_] = static_cast<uint64_t>(out_.cap);
       PatchOut(a);
-      ctx_.Launch(fn_, ctx_.GridFor(len, 128), 128, a, 0, "skinner episode");
+      a.w[w_phase_] = 0;
+      ctx_.Launch(fn_, ctx_.GridFor(len, 128), 128, a, 0, T_ > 1 ? "skinner expand" : "skinner episode");
+      if (T_ > 1) {
+        ctx_.ScanU64(offs_, len);
+        a.w[w_phase_] = 1;
+        ctx_.Launch(fn_, ctx_.num_sms * 8, 128, a, 0, "skinner episode");
+      }
       uint64_t cw[2] = {0, 0};
       ctx_.D2H(&cw[0], count_, sizeof(uint64_t));
       ctx_.D2H(&cw[1], work_, sizeof(uint64_t));
@@ -2352,7 +2668,10 @@ class SkinnerEngine : public JoinEnv {
     double per_row = static_cast<double>(std::max<int64_t>(work, 1)) / len;
     slice_est_[L] = std::max<int64_t>(1, std::min<int64_t>(int64_t(budget_ / per_row), 1LL << 26));
     double progress = static_cast<double>(len) / static_cast<double>(remaining);
-    return 0.5 * progress + 0.5 * static_cast<double>(results) / static_cast<double>(budget_);
+    const double reward = 0.5 * progress + 0.5 * static_cast<double>(results) / static_cast<double>(budget_);
+    total_work_ += work;
+    if (ctx_.skinner_log && log_.size() < (1u << 16)) log_.emplace_back(order, reward);
+    return reward;
   }
 
  private:
@@ -2381,7 +2700,8 @@ class SkinnerEngine : public JoinEnv {
     ks.L("int64_t card[" + TS + "];");
     for (int t = 0; t < T; t++) ks.L("card[" + std::to_string(t) + "] = (int64_t)" + ks.Word(static_cast<uint64_t>(cards_[t])) + ";");
     ks.L("const int64_t s0 = (int64_t)a.w[" + std::to_string(w_s0_) + "], s1 = (int64_t)a.w[" + std::to_string(w_s1_) + "];");
-    ks.L("int64_t rows[" + TS + "]; uint64_t iti[" + TS + "]; uint32_t ith[" + TS + "]; int64_t itk[" + TS + "];");
+    w_phase_ = ks.Arg(0);
+    ks.L("int64_t rows[" + TS + "]; int64_t iti[" + TS + "]; int64_t ite[" + TS + "];");
     ks.L("unsigned long long work = 0;");
     std::vector<std::vector<std::string>> cache(T);
     auto load = [&](int t, std::vector<CVal>& out) {
@@ -2405,10 +2725,12 @@ class SkinnerEngine : public JoinEnv {
     ks.indent--;
     ks.L("};");
     ks.L("auto conds_ok = [&](uint64_t m) -> bool { while (m) { int c = __ffsll((long long)m) - 1; m &= m - 1; if (!cond(c)) return false; } return true; };");
-    // lookups: case 2j probes table tb with the key of ta; 2j+1 the reverse
+    // lookups: case 2j probes table tb with the key of ta; 2j+1 the reverse.
+    // init(p) sets [iti, ite) to the candidate run of position p: the whole
+    // table for a scan, the run of the probe key's hash in the grouped index
     ks.Open("auto init = [&](int p)");
     ks.Open("switch (lk[p])");
-    ks.L("case -1: iti[p] = 0; itk[p] = 0; break;");
+    ks.L("case -1: iti[p] = 0; ite[p] = card[ord[p]]; break;");
     for (size_t j = 0; j < preds_.size(); j++)
       for (int side = 0; side < 2; side++) {
         const SkinnerPred& pr = preds_[j];
@@ -2419,12 +2741,20 @@ class SkinnerEngine : public JoinEnv {
         std::vector<CVal> fv;
         load(from, fv);
         const CVal& key = fv.at(fcol);
-        ks.Open("if (" + key.n + ")");
-        ks.L("itk[p] = -1;");
+        ks.L("iti[p] = 0; ite[p] = 0;");
+        ks.Open("if (!(" + key.n + "))");
+        std::string SL = ks.Ptr(jt.slots, "uint64_t", true), LN = ks.Ptr(jt.lens, "uint32_t", true);
+        std::string M = ks.Word(jt.mask);
+        ks.L("const uint32_t h = " + JoinHash(eg, {key}) + ";");
+        ks.L("uint64_t s = kdb_mix64(h) & " + M + ";");
+        ks.Open("for (uint64_t k = 0; k <= " + M + "; k++, s = (s + 1) & " + M + ")");
+        ks.L("const uint64_t e = " + SL + "[s];");
+        ks.L("if (e == 0) break;");
+        ks.Open("if ((uint32_t)(e >> 32) == h)");
+        ks.L("iti[p] = (int64_t)(uint32_t)e - 1; ite[p] = iti[p] + (int64_t)" + LN + "[s];");
+        ks.L("break;");
         ks.Close();
-        ks.Open("else");
-        ks.L("uint32_t h = " + JoinHash(eg, {key}) + ";");
-        ks.L("ith[p] = h; iti[p] = kdb_mix64(h) & " + ks.Word(jt.mask) + "; itk[p] = 0;");
+        ks.Close();
         ks.Close();
         ks.L("break;");
         ks.Close();
@@ -2432,9 +2762,11 @@ class SkinnerEngine : public JoinEnv {
     ks.Close();
     ks.indent--;
     ks.L("};");
-    ks.Open("auto next = [&](int p) -> int64_t");
+    // cand(p, c): the row of candidate c of position p's run, or -1 when its
+    // key differs from the probe key (another key with the same hash)
+    ks.Open("auto cand = [&](int p, int64_t c) -> int64_t");
     ks.Open("switch (lk[p])");
-    ks.L("case -1: { int t = ord[p]; if (iti[p] < (uint64_t)card[t]) return (int64_t)(iti[p]++); return -1; }");
+    ks.L("case -1: return c;");
     for (size_t j = 0; j < preds_.size(); j++)
       for (int side = 0; side < 2; side++) {
         const SkinnerPred& pr = preds_[j];
@@ -2442,27 +2774,22 @@ class SkinnerEngine : public JoinEnv {
         int to = side == 0 ? pr.tb : pr.ta, tcol = side == 0 ? pr.cb : pr.ca;
         const JoinTable& jt = index_for_[to][tcol];
         ks.Open("case " + std::to_string(j * 2 + side) + ":");
-        std::string slots = ks.Ptr(jt.slots, "uint64_t", true);
-        std::string mask = ks.Word(jt.mask);
-        ks.Open("while (itk[p] >= 0 && (uint64_t)itk[p] <= " + mask + ")");
-        ks.L("uint64_t e = " + slots + "[iti[p]];");
-        ks.Open("if (e == 0)");
-        ks.L("itk[p] = -1;");
-        ks.L("break;");
-        ks.Close();
-        ks.L("iti[p] = (iti[p] + 1) & " + mask + "; itk[p]++;");
-        ks.Open("if ((uint32_t)(e >> 32) == ith[p])");
-        ks.L("int64_t br = (int64_t)(uint32_t)e - 1;");
+        std::string SR = ks.Ptr(jt.srow, "uint32_t", true);
+        ks.L("int64_t br = (int64_t)" + SR + "[c];");
         std::vector<CVal> fv;
         load(from, fv);
-        std::vector<std::string> tcache;
         auto tv = LoadMat(ks, eg, *mats_[to], "br", &cache[to]);
-        ks.L("if (" + eg.EqOf(tv.at(tcol), fv.at(fcol)) + ") return br;");
-        ks.Close();
-        ks.Close();
-        ks.L("return -1;");
+        ks.L("return (" + eg.EqOf(tv.at(tcol), fv.at(fcol)) + ") ? br : (int64_t)-1;");
         ks.Close();
       }
+    ks.Close();
+    ks.L("return -1;");
+    ks.indent--;
+    ks.L("};");
+    ks.Open("auto next = [&](int p) -> int64_t");
+    ks.Open("while (iti[p] < ite[p])");
+    ks.L("const int64_t r = cand(p, iti[p]++);");
+    ks.L("if (r >= 0) return r;");
     ks.Close();
     ks.L("return -1;");
     ks.indent--;
@@ -2496,34 +2823,71 @@ class SkinnerEngine : public JoinEnv {
     }
     ks.indent--;
     ks.L("};");
-    // the episode: DFS over positions for each leftmost tuple of the slice
+    // Phase 0 (expand): each leftmost tuple of the slice that passes its
+    // conditions records its position-1 candidate run [beg, beg + len).
+    // Phase 1 (episode), after an exclusive scan of the lengths: every
+    // (leftmost tuple, position-1 candidate) pair is a work item spread over
+    // all threads, so a tuple with a huge fan-out (skewed keys) is shared by
+    // the whole grid; each item continues depth-first from position 2.
+    std::string BG = ks.Ptr(beg_, "uint64_t"), OF = ks.Ptr(offs_, "uint64_t");
+    ks.L("const int phase = (int)a.w[" + std::to_string(w_phase_) + "];");
+    ks.Open("if (phase == 0)");
     ks.Open("for (int64_t x = s0 + blockIdx.x * (int64_t)blockDim.x + threadIdx.x; x < s1; x += (int64_t)gridDim.x * blockDim.x)");
     ks.L("rows[ord[0]] = x; work++;");
-    ks.L("if (!conds_ok(sched[0])) continue;");
     if (T == 1) {
-      ks.L("emit();");
+      ks.L("if (conds_ok(sched[0])) emit();");
     } else {
-      ks.L("int p = 1; init(1);");
-      ks.Open("while (p >= 1)");
-      ks.L("int64_t c = next(p);");
-      ks.Open("if (c < 0)");
-      ks.L("p--;");
-      ks.L("continue;");
+      ks.L("uint64_t len = 0;");
+      ks.Open("if (conds_ok(sched[0]))");
+      ks.L("init(1);");
+      ks.L(BG + "[x - s0] = (uint64_t)iti[1];");
+      ks.L("len = (uint64_t)(ite[1] - iti[1]);");
       ks.Close();
-      ks.L("int t = ord[p];");
-      ks.L("if (c < off[t]) continue;");
-      ks.L("rows[t] = c; work++;");
-      ks.L("if (!conds_ok(sched[p])) continue;");
-      ks.Open("if (p == " + std::to_string(T - 1) + ")");
-      ks.L("emit();");
-      ks.Close();
+      ks.L(OF + "[x - s0] = len;");
+    }
+    ks.Close();
+    ks.Close();
+    if (T > 1) {
       ks.Open("else");
-      ks.L("p++;");
-      ks.L("init(p);");
+      ks.L("const int64_t m = s1 - s0;");
+      ks.L("const uint64_t total = " + OF + "[m];");
+      ks.Open("for (uint64_t w = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; w < total; w += (uint64_t)gridDim.x * blockDim.x)");
+      ks.L("int64_t lo = 0, hi = m - 1;");
+      ks.Open("while (lo < hi)");
+      ks.L("const int64_t mid = (lo + hi + 1) >> 1;");
+      ks.L("if (" + OF + "[mid] <= w) lo = mid; else hi = mid - 1;");
+      ks.Close();
+      ks.L("rows[ord[0]] = s0 + lo;");
+      ks.L("const int64_t c1 = cand(1, (int64_t)(" + BG + "[lo] + (w - " + OF + "[lo])));");
+      ks.L("if (c1 < 0 || c1 < off[ord[1]]) continue;");
+      ks.L("rows[ord[1]] = c1; work++;");
+      ks.L("if (!conds_ok(sched[1])) continue;");
+      if (T == 2) {
+        ks.L("emit();");
+      } else {
+        ks.L("int p = 2; init(2);");
+        ks.Open("while (p >= 2)");
+        ks.L("int64_t c = next(p);");
+        ks.Open("if (c < 0)");
+        ks.L("p--;");
+        ks.L("continue;");
+        ks.Close();
+        ks.L("int t = ord[p];");
+        ks.L("if (c < off[t]) continue;");
+        ks.L("rows[t] = c; work++;");
+        ks.L("if (!conds_ok(sched[p])) continue;");
+        ks.Open("if (p == " + std::to_string(T - 1) + ")");
+        ks.L("emit();");
+        ks.Close();
+        ks.Open("else");
+        ks.L("p++;");
+        ks.L("init(p);");
+        ks.Close();
+        ks.Close();
+      }
       ks.Close();
       ks.Close();
     }
-    ks.Close();
     std::string wk = ks.Ptr(work_, "unsigned long long");
     ks.L("if (work) atomicAdd(" + wk + ", work);");
     std::string src = ks.Kernel("kdb_skinner_episode", 128);
@@ -2592,6 +2956,11 @@ class SkinnerEngine : public JoinEnv {
   std::vector<int64_t> cards_, offsets_, slice_est_;
   std::vector<uint64_t> cond_tables_;
   std::set<std::pair<int, int>> connected_;
+  std::vector<uint64_t> adj_;  // join-graph neighbours of each table
+  static constexpr int kPriorTables = 8;
+  std::map<uint64_t, std::vector<double>> prior_cache_;  // joined set -> value per table
+  std::vector<std::pair<std::vector<int>, double>> log_;   // (order, reward) per episode
+  int64_t total_work_ = 0;
   std::vector<std::vector<JoinTable>> index_for_;
   MatBuffer out_;
   uint64_t* count_ = nullptr;
@@ -2601,11 +2970,15 @@ class SkinnerEngine : public JoinEnv {
   CUfunction fn_ = nullptr;
   KArgs args_;
   int w_order_ = 0, w_lookup_ = 0, w_sched_ = 0, w_off_ = 0, w_s0_ = 0, w_s1_ = 0, w_cap_ = 0, w_count_ = 0,
-      w_pos_ = 0;
+      w_pos_ = 0, w_phase_ = 0;
+  static constexpr int64_t kMaxSlice = 1 << 20;  // leftmost tuples per episode
+  uint64_t* beg_ = nullptr;   // per slice tuple: first position-1 candidate
+  uint64_t* offs_ = nullptr;  // per slice tuple: candidate count, then its exclusive prefix
   std::vector<int> out_ptr_words_;
 };
 
 MatBuffer Executor::RunSkinner(const Operator& op) {
+  ctx_.NotReplayable();  // episode decisions follow the host's UCT search
   const int T = static_cast<int>(op.children.size());
   if (T > 16) throw Error(-5, "Skinner join of more than 16 tables");
   if (op.conditions.size() > 64) throw Error(-5, "Skinner join with more than 64 conditions");
@@ -2626,23 +2999,29 @@ MatBuffer Executor::RunSkinner(const Operator& op) {
   std::vector<std::vector<JoinTable>> index_for(T);
   for (int t = 0; t < T; t++) index_for[t].resize(mats[t]->cols.size());
   for (const auto& pr : preds) {
-    if (!index_for[pr.tb][pr.cb].slots) index_for[pr.tb][pr.cb] = BuildIndex(*mats[pr.tb], {pr.cb});
-    if (!index_for[pr.ta][pr.ca].slots) index_for[pr.ta][pr.ca] = BuildIndex(*mats[pr.ta], {pr.ca});
+    if (!index_for[pr.tb][pr.cb].slots) index_for[pr.tb][pr.cb] = BuildGroupedIndex(*mats[pr.tb], pr.cb);
+    if (!index_for[pr.ta][pr.ca].slots) index_for[pr.ta][pr.ca] = BuildGroupedIndex(*mats[pr.ta], pr.ca);
   }
   auto alloc = [&](int64_t cap) { return AllocMat(op.output, cap); };
   SkinnerEngine eng(ctx_, arena_, op, mats, index_for, preds, alloc, ctx_.skinner_budget, ctx_.skinner_seed);
   MatBuffer out = eng.Run(op.prefix_order);
   ctx_.last_skinner_episodes = eng.episodes();
+  ctx_.last_skinner_work = eng.work();
   return out;
 }
 
 HostResult Executor::Run(const Operator& root) {
   MatBuffer m = Materialize(root);
+  return Download(m, root);
+}
+
+HostResult Executor::Download(const MatBuffer& m, const Operator& root, bool check_error) {
   const auto& schema = SchemaOf(root);
   HostResult res;
   res.rows = m.rows;
   // one batch of device->host copies into the context's pinned staging
-  // buffer and a single synchronisation (not one per column)
+  // buffer and a single synchronisation (not one per column); with
+  // `check_error` the device error word travels in the same batch
   std::vector<size_t> data_off(m.cols.size()), null_off(m.cols.size());
   size_t total = 0;
   for (size_t c = 0; c < m.cols.size(); c++) {
@@ -2651,16 +3030,29 @@ HostResult Executor::Run(const Operator& root) {
     null_off[c] = total;
     if (m.cols[c].nulls) total += (static_cast<size_t>(m.rows) + 15) & ~size_t(15);
   }
-  char* stage = static_cast<char*>(ctx_.HostStage(total));
-  if (m.rows > 0 && !ctx_.dry) {
-    for (size_t c = 0; c < m.cols.size(); c++) {
-      const MatCol& mc = m.cols[c];
-      KDB_CUDA(cudaMemcpyAsync(stage + data_off[c], mc.data, StoreWidth(mc.type.id) * m.rows,
-                               cudaMemcpyDeviceToHost, ctx_.stream));
-      if (mc.nulls)
-        KDB_CUDA(cudaMemcpyAsync(stage + null_off[c], mc.nulls, m.rows, cudaMemcpyDeviceToHost, ctx_.stream));
-    }
+  const size_t err_off = total;
+  char* stage = static_cast<char*>(ctx_.HostStage(total + 16));
+  if (!ctx_.dry && (m.rows > 0 || check_error)) {
+    if (m.rows > 0)
+      for (size_t c = 0; c < m.cols.size(); c++) {
+        const MatCol& mc = m.cols[c];
+        KDB_CUDA(cudaMemcpyAsync(stage + data_off[c], mc.data, StoreWidth(mc.type.id) * m.rows,
+                                 cudaMemcpyDeviceToHost, ctx_.stream));
+        if (mc.nulls)
+          KDB_CUDA(cudaMemcpyAsync(stage + null_off[c], mc.nulls, m.rows, cudaMemcpyDeviceToHost, ctx_.stream));
+      }
+    if (check_error)
+      KDB_CUDA(cudaMemcpyAsync(stage + err_off, ctx_.d_err, 16, cudaMemcpyDeviceToHost, ctx_.stream));
     KDB_CUDA(cudaStreamSynchronize(ctx_.stream));
+    if (check_error) {
+      int err[4];
+      std::memcpy(err, stage + err_off, sizeof(err));
+      if (err[0]) {
+        KDB_CUDA(cudaMemsetAsync(ctx_.d_err, 0, sizeof(int) * 4, ctx_.stream));
+        throw Error(-4, "replayed query raised a device error");
+      }
+    }
+    if (m.rows == 0 && total) std::memset(stage, 0, total);
   } else if (total) {
     std::memset(stage, 0, total);
   }
@@ -2726,32 +3118,108 @@ HostResult Executor::Run(const Operator& root) {
 
 }  // namespace
 
-HostResult ExecutePlan(Context& ctx, const plan::Operator& root) {
-  Arena arena(ctx);
-  Executor ex(ctx, arena);
-  if (ctx.dry) return ex.Run(root);
-  ctx.BeginQueryProfile();
-  cudaEvent_t e0, e1;
-  KDB_CUDA(cudaEventCreate(&e0));
-  KDB_CUDA(cudaEventCreate(&e1));
-  KDB_CUDA(cudaEventRecord(e0, ctx.stream));
+PreparedQuery::~PreparedQuery() {
+  if (exec) cudaGraphExecDestroy(exec);
+}
+
+namespace {
+
+constexpr size_t kMaxPreparedBytes = size_t(1) << 30;  // device memory a prepared query may keep
+
+// CUDA-event timing of one query on the context's stream.
+class QueryTimer {
+ public:
+  explicit QueryTimer(Context& ctx) : ctx_(ctx) {
+    ctx.BeginQueryProfile();
+    KDB_CUDA(cudaEventCreate(&e0_));
+    KDB_CUDA(cudaEventCreate(&e1_));
+    KDB_CUDA(cudaEventRecord(e0_, ctx.stream));
+  }
+  ~QueryTimer() {
+    cudaEventDestroy(e0_);
+    cudaEventDestroy(e1_);
+  }
+  void Done() {
+    KDB_CUDA(cudaEventRecord(e1_, ctx_.stream));
+    KDB_CUDA(cudaEventSynchronize(e1_));
+    float ms = 0;
+    KDB_CUDA(cudaEventElapsedTime(&ms, e0_, e1_));
+    ctx_.last_device_ms = ms;
+    ctx_.EndQueryProfile();
+  }
+
+ private:
+  Context& ctx_;
+  cudaEvent_t e0_ = nullptr, e1_ = nullptr;
+};
+
+}  // namespace
+
+HostResult ExecutePlan(Context& ctx, const plan::Operator& root, std::unique_ptr<PreparedQuery>* prepared) {
+  if (ctx.dry) {
+    Arena arena(ctx);
+    Executor ex(ctx, arena);
+    return ex.Run(root);
+  }
+  const bool prepare = prepared != nullptr && !ctx.profile;
+  if (prepare && *prepared) {
+    PreparedQuery& pq = **prepared;
+    if (pq.catalog_version == ctx.catalog_version) {
+      // replay: one graph launch, then the result download
+      QueryTimer timer(ctx);
+      KDB_CUDA(cudaGraphLaunch(pq.exec, ctx.stream));
+      ctx.kernel_launches += pq.launches;
+      bool ok = true;
+      HostResult r;
+      try {
+        Arena arena(ctx);
+        Executor ex(ctx, arena);
+        r = ex.Download(pq.result, root, true);
+      } catch (const Error&) {
+        ok = false;  // run it afresh below
+      }
+      if (ok) {
+        timer.Done();
+        return r;
+      }
+    }
+    prepared->reset();
+  }
+  QueryTimer timer(ctx);
+  auto pq = std::make_unique<PreparedQuery>();
+  pq->arena = std::make_unique<Arena>(ctx);
+  Recorder rec;
+  if (prepare) ctx.rec = &rec;
   HostResult r;
+  MatBuffer m;
   try {
-    r = ex.Run(root);
+    Executor ex(ctx, *pq->arena);
+    m = ex.MaterializeRoot(root);
+    ctx.rec = nullptr;
+    r = ex.Download(m, root);
   } catch (...) {
-    cudaEventDestroy(e0);
-    cudaEventDestroy(e1);
+    ctx.rec = nullptr;
     cudaStreamSynchronize(ctx.stream);
     throw;
   }
-  KDB_CUDA(cudaEventRecord(e1, ctx.stream));
-  KDB_CUDA(cudaEventSynchronize(e1));
-  float ms = 0;
-  KDB_CUDA(cudaEventElapsedTime(&ms, e0, e1));
-  ctx.last_device_ms = ms;
-  cudaEventDestroy(e0);
-  cudaEventDestroy(e1);
-  ctx.EndQueryProfile();
+  timer.Done();
+  if (prepare && rec.replayable && pq->arena->bytes() <= kMaxPreparedBytes) {
+    cudaGraph_t g = nullptr;
+    KDB_CUDA(cudaStreamBeginCapture(ctx.stream, cudaStreamCaptureModeThreadLocal));
+    for (auto& op : rec.ops) op(ctx.stream);
+    KDB_CUDA(cudaStreamEndCapture(ctx.stream, &g));
+    cudaError_t ie = cudaGraphInstantiate(&pq->exec, g, 0);
+    cudaGraphDestroy(g);
+    if (ie == cudaSuccess) {
+      pq->result = m;
+      pq->catalog_version = ctx.catalog_version;
+      pq->launches = rec.launches;
+      *prepared = std::move(pq);
+    } else {
+      cudaGetLastError();
+      pq->exec = nullptr;
+    }
+  }
   return r;
 }
 

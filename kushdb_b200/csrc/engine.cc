@@ -80,6 +80,7 @@ void* Arena::Alloc(size_t bytes) {
   void* p = nullptr;
   KDB_CUDA(cudaMallocAsync(&p, bytes, ctx_.stream));
   ptrs_.push_back(p);
+  bytes_ += bytes;
   return p;
 }
 
@@ -103,10 +104,13 @@ void Context::DevFree(void* p) {
 }
 
 void Context::Memset(void* d, int v, size_t bytes) {
-  if (!dry && bytes) KDB_CUDA(cudaMemsetAsync(d, v, bytes, stream));
+  if (dry || !bytes) return;
+  KDB_CUDA(cudaMemsetAsync(d, v, bytes, stream));
+  if (rec) rec->ops.push_back([d, v, bytes](cudaStream_t s) { cudaMemsetAsync(d, v, bytes, s); });
 }
 
 void Context::H2D(void* d, const void* h, size_t bytes) {
+  NotReplayable();
   if (!dry && bytes) KDB_CUDA(cudaMemcpyAsync(d, h, bytes, cudaMemcpyHostToDevice, stream));
 }
 
@@ -160,7 +164,8 @@ Context::Context(int dev) : device(dev) {
 Context::Context(Context& parent)
     : device(parent.device), dry(parent.dry), num_sms(parent.num_sms), tables(parent.tables),
       enums(parent.enums), skinner_budget(parent.skinner_budget), skinner_seed(parent.skinner_seed),
-      cache_(parent.cache_), owns_catalog_(false) {
+      skinner_policy(parent.skinner_policy), join_prior(parent.join_prior), cache_(parent.cache_),
+      owns_catalog_(false) {
   if (dry) {
     d_err = static_cast<int*>(DevAlloc(16));
     return;
@@ -212,6 +217,7 @@ static void CheckRows(DevTable& t, int64_t n, const std::string& name) {
 
 void Context::AddColumn(const std::string& table, const std::string& column, const plan::Type& type,
                         const void* data, int64_t n, const int8_t* nulls) {
+  catalog_version++;
   if (type.id == plan::TypeId::TEXT) throw Error(-1, "TEXT columns use kdb_table_add_text_column");
   if (n < 0) throw Error(-1, "negative row count");
   DevTable& t = tables[table];
@@ -247,6 +253,7 @@ void Context::AddColumn(const std::string& table, const std::string& column, con
 void Context::AddTextColumn(const std::string& table, const std::string& column,
                             const int64_t* offsets, const char* chars, int64_t n,
                             const int8_t* nulls) {
+  catalog_version++;
   if (n < 0) throw Error(-1, "negative row count");
   DevTable& t = tables[table];
   CheckRows(t, n, column);
@@ -276,6 +283,7 @@ void Context::AddTextColumn(const std::string& table, const std::string& column,
 }
 
 void Context::DropTable(const std::string& table) {
+  catalog_version++;
   auto it = tables.find(table);
   if (it == tables.end()) return;
   if (!dry) KDB_CUDA(cudaStreamSynchronize(stream));
@@ -284,6 +292,7 @@ void Context::DropTable(const std::string& table) {
 }
 
 void Context::RegisterEnum(int32_t id, std::vector<std::string> values) {
+  catalog_version++;
   auto it = enums.find(id);
   if (it != enums.end()) {
     if (it->second.values == values) return;
@@ -412,6 +421,15 @@ void Context::Launch(CUfunction f, int grid, int block, const KArgs& args, size_
                              reinterpret_cast<CUstream>(stream), params, nullptr),
           "cuLaunchKernel");
   TimedStop();
+  if (rec) {
+    rec->launches++;
+    auto held = std::make_shared<KArgs>(args);
+    rec->ops.push_back([f, grid, block, smem, held](cudaStream_t s) {
+      void* p[] = {held.get()};
+      g_drv.LaunchKernel(f, grid, 1, 1, block, 1, 1, static_cast<unsigned>(smem), reinterpret_cast<CUstream>(s),
+                         p, nullptr);
+    });
+  }
 }
 
 void Context::TimedStart(const char* tag) {

@@ -11,6 +11,7 @@
 #include <cuda_runtime.h>
 
 #include <cstdint>
+#include <functional>
 #include <map>
 #include <memory>
 #include <mutex>
@@ -105,6 +106,15 @@ struct KArgs {
 };
 
 class Context;
+class JoinPrior;
+
+// The device work of one query execution, kept to be replayed as a CUDA
+// graph when the same plan runs again over unchanged tables.
+struct Recorder {
+  std::vector<std::function<void(cudaStream_t)>> ops;
+  int64_t launches = 0;
+  bool replayable = true;
+};
 
 // Stream-ordered device allocations owned by one query execution.
 class Arena {
@@ -116,10 +126,12 @@ class Arena {
   T* AllocT(size_t count) {
     return static_cast<T*>(Alloc(count * sizeof(T) + 16));
   }
+  size_t bytes() const { return bytes_; }
 
  private:
   Context& ctx_;
   std::vector<void*> ptrs_;
+  size_t bytes_ = 0;
 };
 
 class Context {
@@ -148,9 +160,49 @@ class Context {
   int64_t skinner_budget = 1 << 20;
   uint32_t skinner_seed = 0;
   int64_t last_skinner_episodes = 0;
+  int64_t last_skinner_work = 0;  // tuples examined by all episodes
+  // Join-order policy: 0 = UCT as the reference, 1 = UCT seeded by the
+  // learned prior (falls back to 0 without a model or above 8 tables),
+  // 2 = uniformly random connected orders (training-data collection).
+  int skinner_policy = 0;
+  JoinPrior* join_prior = nullptr;
+  // (features, reward) of every (prefix, next table) step of every episode
+  // of the last Skinner join, when logging is on
+  bool skinner_log = false;
+  std::vector<float> skinner_features;
+  std::vector<float> skinner_rewards;
 
   // device error word shared by all launches of a query
   int* d_err = nullptr;
+
+  // Recording (prepared-query replay): while `rec` is set, every launch and
+  // memset of the query is also kept; a host-to-device copy or a Skinner
+  // join makes the query not replayable.  `catalog_version` changes with
+  // every table or enum change and invalidates prepared queries.
+  Recorder* rec = nullptr;
+  uint64_t catalog_version = 0;
+  void Issue(std::function<void(cudaStream_t)> op, bool is_kernel = true) {
+    kernel_launches += is_kernel;
+    if (dry) return;
+    op(stream);
+    if (rec) {
+      rec->launches += is_kernel;
+      rec->ops.push_back(std::move(op));
+    }
+  }
+  // a retried step drops what its failed attempt recorded
+  std::pair<size_t, int64_t> RecordMark() const {
+    return rec ? std::make_pair(rec->ops.size(), rec->launches) : std::make_pair(size_t(0), int64_t(0));
+  }
+  void RecordTruncate(const std::pair<size_t, int64_t>& mark) {
+    if (rec && rec->ops.size() > mark.first) {
+      rec->ops.resize(mark.first);
+      rec->launches = mark.second;
+    }
+  }
+  void NotReplayable() {
+    if (rec) rec->replayable = false;
+  }
 
   void AddColumn(const std::string& table, const std::string& column, const plan::Type& type,
                  const void* data, int64_t n, const int8_t* nulls);
@@ -192,6 +244,8 @@ class Context {
 
   // Static kernels (kernels.cu).
   void RadixSortPairs(uint64_t* keys, uint32_t* vals, int64_t n, Arena& arena, int key_bits = 64);
+  // exclusive prefix sum of a[0..n) in place, the total into a[n]
+  void ScanU64(uint64_t* a, int64_t n);
   void CheckDeviceError(const char* what);
 
   EnumDicts HostEnums() const;
@@ -204,7 +258,21 @@ class Context {
   void FreeColumn(DevColumn& c);
 };
 
-// Runs a plan on the device and returns the host result.
-HostResult ExecutePlan(Context& ctx, const plan::Operator& root);
+// A plan executed once and kept for replay: its device buffers, the CUDA
+// graph of its launches, and the location of its result.
+struct PreparedQuery {
+  std::unique_ptr<Arena> arena;
+  cudaGraphExec_t exec = nullptr;
+  MatBuffer result;
+  uint64_t catalog_version = 0;
+  int64_t launches = 0;
+  ~PreparedQuery();
+};
+
+// Runs a plan on the device and returns the host result.  With `prepared`,
+// the first run of a plan records it, and later runs over unchanged tables
+// replay the recorded graph (no code generation, one graph launch).
+HostResult ExecutePlan(Context& ctx, const plan::Operator& root,
+                       std::unique_ptr<PreparedQuery>* prepared = nullptr);
 
 }  // namespace kdb

@@ -10,6 +10,7 @@
 // key from the least to the most significant.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cstdint>
 #include <mutex>
 #include <vector>
@@ -23,65 +24,188 @@ namespace {
 constexpr int kSortBlock = 256;
 constexpr int kSortTile = 4096;  // items per block per pass
 constexpr int kSortWarps = kSortBlock / 32;
+static_assert(kSortBlock == 256, "one thread per radix digit");
+constexpr int64_t kPlanMinRows = 1 << 15;  // below this a counting read costs more than it saves
 
 __global__ void __launch_bounds__(kSortBlock) RadixHistogram(const uint64_t* __restrict__ keys,
-                                                             int64_t n, int shift,
+                                                             int64_t n, int shift, int tile,
                                                              uint32_t* __restrict__ hist,
                                                              int nblocks) {
   __shared__ uint32_t h[256];
   for (int i = threadIdx.x; i < 256; i += blockDim.x) h[i] = 0;
   __syncthreads();
-  int64_t base = static_cast<int64_t>(blockIdx.x) * kSortTile;
-  int64_t end = min(base + kSortTile, n);
+  int64_t base = static_cast<int64_t>(blockIdx.x) * tile;
+  int64_t end = min(base + tile, n);
   for (int64_t i = base + threadIdx.x; i < end; i += blockDim.x)
     atomicAdd(&h[(keys[i] >> shift) & 0xff], 1u);
   __syncthreads();
   for (int d = threadIdx.x; d < 256; d += blockDim.x) hist[d * nblocks + blockIdx.x] = h[d];
 }
 
-// Exclusive scan of `count` uint32 in place (one block of 1024 threads).
-__global__ void __launch_bounds__(1024) ExclusiveScanSmall(uint32_t* __restrict__ a,
-                                                           int64_t count) {
-  __shared__ uint32_t partial[1024];
-  int t = threadIdx.x;
-  int64_t per = (count + blockDim.x - 1) / blockDim.x;
-  int64_t b = t * per, e = min(b + per, count);
-  uint32_t s = 0;
-  for (int64_t i = b; i < e; i++) s += a[i];
-  partial[t] = s;
+// Digit counts of every 8-bit pass at once (order independent), so passes
+// whose digit is the same for every key can be skipped.
+__global__ void __launch_bounds__(kSortBlock) RadixDigitCounts(const uint64_t* __restrict__ keys, int64_t n,
+                                                               int passes, uint32_t* __restrict__ counts) {
+  __shared__ uint32_t h[8][256];
+  for (int i = threadIdx.x; i < 8 * 256; i += blockDim.x) (&h[0][0])[i] = 0;
   __syncthreads();
-  if (t == 0) {
-    uint32_t run = 0;
-    for (int i = 0; i < static_cast<int>(blockDim.x); i++) {
-      uint32_t x = partial[i];
-      partial[i] = run;
-      run += x;
+  for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < n;
+       i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const uint64_t k = keys[i];
+    for (int p = 0; p < passes; p++) atomicAdd(&h[p][(k >> (8 * p)) & 0xff], 1u);
+  }
+  __syncthreads();
+  for (int i = threadIdx.x; i < passes * 256; i += blockDim.x) {
+    const uint32_t c = (&h[0][0])[i];
+    if (c) atomicAdd(counts + i, c);
+  }
+}
+
+// Exclusive scan in place by one block of 1024 threads: each thread owns
+// kPer contiguous elements of a tile (moved with 16-byte vector loads and
+// stores), scans them in registers, the thread sums are scanned with warp
+// shuffles, and a carry runs from tile to tile.  With `total`, the sum of all
+// elements is also written to total[0].  `a` must be 16-byte aligned.
+template <typename T, int kPer>
+__device__ __forceinline__ void BlockScanTiles(T* __restrict__ a, int64_t count, T* __restrict__ total) {
+  static_assert((kPer * sizeof(T)) % 16 == 0, "whole vectors per thread");
+  constexpr int kVec = static_cast<int>(kPer * sizeof(T) / 16);
+  constexpr int64_t kTile = 1024LL * kPer;
+  __shared__ T warp_sum[32];
+  __shared__ T carry;
+  const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
+  if (t == 0) carry = 0;
+  for (int64_t base = 0; base < count; base += kTile) {
+    const int64_t i0 = base + static_cast<int64_t>(t) * kPer;
+    const bool full = i0 + kPer <= count;
+    T v[kPer];
+    if (full) {
+      const uint4* src = reinterpret_cast<const uint4*>(a + i0);
+      uint4 q[kVec];
+#pragma unroll
+      for (int k = 0; k < kVec; k++) q[k] = src[k];
+      memcpy(v, q, sizeof(v));
+    } else {
+#pragma unroll
+      for (int j = 0; j < kPer; j++) v[j] = i0 + j < count ? a[i0 + j] : T(0);
     }
+    T s = 0;
+#pragma unroll
+    for (int j = 0; j < kPer; j++) s += v[j];
+    T incl = s;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const T y = __shfl_up_sync(0xffffffffu, incl, o);
+      if (lane >= o) incl += y;
+    }
+    if (lane == 31) warp_sum[warp] = incl;
+    __syncthreads();
+    if (warp == 0) {
+      const T w = warp_sum[lane];
+      T wi = w;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const T y = __shfl_up_sync(0xffffffffu, wi, o);
+        if (lane >= o) wi += y;
+      }
+      warp_sum[lane] = wi - w;
+    }
+    __syncthreads();
+    T run = carry + warp_sum[warp] + incl - s;
+    T out[kPer];
+#pragma unroll
+    for (int j = 0; j < kPer; j++) {
+      out[j] = run;
+      run += v[j];
+    }
+    if (full) {
+      uint4 q[kVec];
+      memcpy(q, out, sizeof(out));
+      uint4* dst = reinterpret_cast<uint4*>(a + i0);
+#pragma unroll
+      for (int k = 0; k < kVec; k++) dst[k] = q[k];
+    } else {
+#pragma unroll
+      for (int j = 0; j < kPer; j++)
+        if (i0 + j < count) a[i0 + j] = out[j];
+    }
+    __syncthreads();
+    if (t == 1023) carry = run;
   }
   __syncthreads();
-  uint32_t run = partial[t];
-  for (int64_t i = b; i < e; i++) {
-    uint32_t x = a[i];
-    a[i] = run;
-    run += x;
-  }
+  if (total && t == 0) total[0] = carry;
+}
+
+__global__ void __launch_bounds__(1024) ExclusiveScanSmall(uint32_t* __restrict__ a, int64_t count) {
+  BlockScanTiles<uint32_t, 16>(a, count, nullptr);
+}
+
+// Exclusive scan of n uint64 in place, total written to a[n].
+__global__ void __launch_bounds__(1024) ExclusiveScanU64(uint64_t* __restrict__ a, int64_t n) {
+  BlockScanTiles<unsigned long long, 8>(reinterpret_cast<unsigned long long*>(a), n,
+                                           reinterpret_cast<unsigned long long*>(a) + n);
 }
 
 // Stable scatter: each block walks its tile in chunks of blockDim items in
 // order; ranks inside a chunk come from a warp match plus per-warp digit
 // counts prefixed in warp order.
+// Exclusive prefix of the 256 values v (one per thread of a 256-thread
+// block) through warp shuffles; `ws` is 8 words of shared scratch.
+__device__ __forceinline__ uint32_t BlockExclusive256(uint32_t v, uint32_t* ws) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  uint32_t incl = v;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const uint32_t y = __shfl_up_sync(0xffffffffu, incl, o);
+    if (lane >= o) incl += y;
+  }
+  if (lane == 31) ws[warp] = incl;
+  __syncthreads();
+  uint32_t before = 0;
+  for (int w = 0; w < warp; w++) before += ws[w];
+  __syncthreads();
+  return before + incl - v;
+}
+
+// Per digit (one block each): exclusive scan of the digit's per-block counts
+// hist[d][0..nblocks) in place, the digit's total into totals[d].
+__global__ void __launch_bounds__(kSortBlock) RadixRowScan(uint32_t* __restrict__ hist, int nblocks,
+                                                           uint32_t* __restrict__ totals) {
+  __shared__ uint32_t ws[kSortWarps];
+  uint32_t* row = hist + static_cast<int64_t>(blockIdx.x) * nblocks;
+  const int per = (nblocks + kSortBlock - 1) / kSortBlock;
+  const int b0 = min(static_cast<int>(threadIdx.x) * per, nblocks), e = min(b0 + per, nblocks);
+  uint32_t s = 0;
+  for (int i = b0; i < e; i++) s += row[i];
+  uint32_t run = BlockExclusive256(s, ws);
+  if (threadIdx.x == kSortBlock - 1) totals[blockIdx.x] = run + s;
+  for (int i = b0; i < e; i++) {
+    const uint32_t x = row[i];
+    row[i] = run;
+    run += x;
+  }
+}
+
+// `offsets` holds each (digit, block) start: global when `totals` is null
+// (one scan over all counts), else relative to the digit, whose start is the
+// exclusive prefix of `totals`.
 __global__ void __launch_bounds__(kSortBlock) RadixScatter(
     const uint64_t* __restrict__ kin, const uint32_t* __restrict__ vin, uint64_t* __restrict__ kout,
-    uint32_t* __restrict__ vout, int64_t n, int shift, const uint32_t* __restrict__ offsets,
-    int nblocks) {
+    uint32_t* __restrict__ vout, int64_t n, int shift, int tile, const uint32_t* __restrict__ offsets,
+    int nblocks, const uint32_t* __restrict__ totals) {
   __shared__ uint32_t base[256];
   __shared__ uint32_t total[256];
   __shared__ uint32_t wcnt[kSortWarps][256];
+  __shared__ uint32_t ws[kSortWarps];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  for (int d = threadIdx.x; d < 256; d += blockDim.x) base[d] = offsets[d * nblocks + blockIdx.x];
-  int64_t tile = static_cast<int64_t>(blockIdx.x) * kSortTile;
-  int64_t end = min(tile + kSortTile, n);
-  for (int64_t c = tile; c < end; c += blockDim.x) {
+  {
+    const int d = threadIdx.x;  // kSortBlock == 256: one digit per thread
+    const uint32_t digit_start = totals ? BlockExclusive256(totals[d], ws) : 0u;
+    base[d] = offsets[d * nblocks + blockIdx.x] + digit_start;
+  }
+  const int64_t first = static_cast<int64_t>(blockIdx.x) * tile;
+  const int64_t end = min(first + tile, n);
+  for (int64_t c = first; c < end; c += blockDim.x) {
     for (int i = threadIdx.x; i < kSortWarps * 256; i += blockDim.x) (&wcnt[0][0])[i] = 0;
     __syncthreads();
     int64_t i = c + threadIdx.x;
@@ -150,6 +274,14 @@ __global__ void CopyPairs(const uint64_t* __restrict__ ks, const uint32_t* __res
 
 }  // namespace
 
+void Context::ScanU64(uint64_t* a, int64_t n) {
+  if (dry) return;
+  TimedStart("skinner scan");
+  Issue([=](cudaStream_t s) { ExclusiveScanU64<<<1, 1024, 0, s>>>(a, n); });
+  TimedStop();
+  KDB_CUDA(cudaGetLastError());
+}
+
 // Sorts (keys, vals) by the low `key_bits` bits of keys, stably.
 void Context::RadixSortPairs(uint64_t* keys, uint32_t* vals, int64_t n, Arena& arena,
                              int key_bits) {
@@ -158,42 +290,64 @@ void Context::RadixSortPairs(uint64_t* keys, uint32_t* vals, int64_t n, Arena& a
   if (n <= kSmallSort) {
     uint64_t mask = key_bits >= 64 ? ~0ULL : ((1ULL << key_bits) - 1);
     TimedStart("sort small");
-    SmallRankSort<<<1, 1024, 0, stream>>>(keys, vals, static_cast<int>(n), mask);
+    Issue([=](cudaStream_t s) { SmallRankSort<<<1, 1024, 0, s>>>(keys, vals, static_cast<int>(n), mask); });
     TimedStop();
-    kernel_launches++;
     KDB_CUDA(cudaGetLastError());
     return;
   }
-  int nblocks = static_cast<int>((n + kSortTile - 1) / kSortTile);
+  // tiles small enough that every SM gets about two blocks, at most 4096
+  // items (a multiple of the block size)
+  int64_t tile = (n + 2 * num_sms - 1) / (2 * num_sms);
+  tile = std::min<int64_t>(kSortTile, std::max<int64_t>(kSortBlock, (tile + kSortBlock - 1) / kSortBlock * kSortBlock));
+  const int nblocks = static_cast<int>((n + tile - 1) / tile);
+  const int itile = static_cast<int>(tile);
   uint64_t* k2 = arena.AllocT<uint64_t>(n);
   uint32_t* v2 = arena.AllocT<uint32_t>(n);
   uint32_t* hist = arena.AllocT<uint32_t>(static_cast<size_t>(nblocks) * 256);
+  uint32_t* totals = arena.AllocT<uint32_t>(256);
   uint64_t* ka = keys;
   uint32_t* va = vals;
   uint64_t* kb = k2;
   uint32_t* vb = v2;
-  int passes = (key_bits + 7) / 8;
+  const int passes = (key_bits + 7) / 8;
+  // skip passes whose digit is constant (one counting read of the keys)
+  std::vector<bool> needed(passes, true);
+  if (passes > 1 && n >= kPlanMinRows) {
+    uint32_t* counts = arena.AllocT<uint32_t>(8 * 256);
+    Memset(counts, 0, sizeof(uint32_t) * 8 * 256);
+    TimedStart("sort digit counts");
+    const int grid = GridFor(n, kSortBlock);
+    Issue([=](cudaStream_t s) { RadixDigitCounts<<<grid, kSortBlock, 0, s>>>(ka, n, passes, counts); });
+    TimedStop();
+    std::vector<uint32_t> h(static_cast<size_t>(passes) * 256);
+    D2H(h.data(), counts, sizeof(uint32_t) * h.size());
+    for (int p = 0; p < passes; p++)
+      for (int d = 0; d < 256; d++)
+        if (h[p * 256 + d] == static_cast<uint64_t>(n)) needed[p] = false;
+  }
   for (int p = 0; p < passes; p++) {
-    int shift = 8 * p;
+    if (!needed[p]) continue;
+    const int shift = 8 * p;
     TimedStart("sort histogram");
-    RadixHistogram<<<nblocks, kSortBlock, 0, stream>>>(ka, n, shift, hist, nblocks);
+    Issue([=](cudaStream_t s) { RadixHistogram<<<nblocks, kSortBlock, 0, s>>>(ka, n, shift, itile, hist, nblocks); });
     TimedStop();
     TimedStart("sort scan");
-    ExclusiveScanSmall<<<1, 1024, 0, stream>>>(hist, static_cast<int64_t>(nblocks) * 256);
+    Issue([=](cudaStream_t s) { RadixRowScan<<<256, kSortBlock, 0, s>>>(hist, nblocks, totals); });
     TimedStop();
     TimedStart("sort scatter");
-    RadixScatter<<<nblocks, kSortBlock, 0, stream>>>(ka, va, kb, vb, n, shift, hist, nblocks);
+    Issue([=](cudaStream_t s) {
+      RadixScatter<<<nblocks, kSortBlock, 0, s>>>(ka, va, kb, vb, n, shift, itile, hist, nblocks, totals);
+    });
     TimedStop();
-    kernel_launches += 3;
     std::swap(ka, kb);
     std::swap(va, vb);
   }
   KDB_CUDA(cudaGetLastError());
   if (ka != keys) {
     TimedStart("sort copy");
-    CopyPairs<<<GridFor(n, 256), 256, 0, stream>>>(ka, va, keys, vals, n);
+    const int grid = GridFor(n, 256);
+    Issue([=](cudaStream_t s) { CopyPairs<<<grid, 256, 0, s>>>(ka, va, keys, vals, n); });
     TimedStop();
-    kernel_launches++;
     KDB_CUDA(cudaGetLastError());
   }
 }
@@ -278,9 +432,9 @@ extern "C" int kdb_sort_pairs_noalloc(uint64_t* d_keys, uint32_t* d_vals, int64_
     int shift = 8 * p;
     // every histogram entry is rewritten by each pass, so nothing left in the
     // shared scratch by an earlier call is read
-    RadixHistogram<<<nblocks, kSortBlock, 0, s>>>(ka, n, shift, hist, nblocks);
+    RadixHistogram<<<nblocks, kSortBlock, 0, s>>>(ka, n, shift, kSortTile, hist, nblocks);
     ExclusiveScanSmall<<<1, 1024, 0, s>>>(hist, static_cast<int64_t>(nblocks) * 256);
-    RadixScatter<<<nblocks, kSortBlock, 0, s>>>(ka, va, kb, vb, n, shift, hist, nblocks);
+    RadixScatter<<<nblocks, kSortBlock, 0, s>>>(ka, va, kb, vb, n, shift, kSortTile, hist, nblocks, nullptr);
     std::swap(ka, kb);
     std::swap(va, vb);
   }

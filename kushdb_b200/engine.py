@@ -33,6 +33,10 @@ EXPORTS = [
     "kdb_batch_create", "kdb_batch_configure", "kdb_batch_tune", "kdb_batch_config", "kdb_batch_run",
     "kdb_batch_run_timed", "kdb_batch_result", "kdb_batch_free", "kdb_sort_pairs_noalloc",
     "kdb_server_start", "kdb_server_submit", "kdb_server_poll", "kdb_server_stats", "kdb_server_stop",
+    "kdb_last_skinner_work", "kdb_mlp_num_features", "kdb_mlp_num_params", "kdb_mlp_create",
+    "kdb_mlp_last_error", "kdb_mlp_set_params", "kdb_mlp_get_params", "kdb_mlp_forward", "kdb_mlp_gradient",
+    "kdb_mlp_train_step", "kdb_mlp_free", "kdb_ctx_set_skinner_policy", "kdb_last_skinner_samples",
+    "kdb_ctx_set_prepared_queries",
 ]
 
 _lib = None
@@ -100,6 +104,25 @@ def load_library(path: str = LIB_PATH):
     L.kdb_server_stats.restype = I64
     L.kdb_server_stats.argtypes = [P, ctypes.c_char_p, I64]
     L.kdb_server_stop.argtypes = [P]
+    L.kdb_ctx_set_prepared_queries.argtypes = [P, I32]
+    L.kdb_last_skinner_work.restype = I64
+    L.kdb_last_skinner_work.argtypes = [P]
+    L.kdb_mlp_num_features.restype = I32
+    L.kdb_mlp_num_features.argtypes = []
+    L.kdb_mlp_num_params.restype = I64
+    L.kdb_mlp_num_params.argtypes = []
+    L.kdb_mlp_create.argtypes = [P, ctypes.c_uint32, ctypes.POINTER(P)]
+    L.kdb_mlp_last_error.restype = ctypes.c_char_p
+    L.kdb_mlp_last_error.argtypes = [P]
+    L.kdb_mlp_set_params.argtypes = [P, P, I64]
+    L.kdb_mlp_get_params.argtypes = [P, P, I64]
+    L.kdb_mlp_forward.argtypes = [P, P, I64, P]
+    L.kdb_mlp_gradient.argtypes = [P, P, P, I64, P, ctypes.POINTER(ctypes.c_double)]
+    L.kdb_mlp_train_step.argtypes = [P, P, P, I64, ctypes.c_float, ctypes.POINTER(ctypes.c_double)]
+    L.kdb_mlp_free.argtypes = [P]
+    L.kdb_ctx_set_skinner_policy.argtypes = [P, I32, P, I32]
+    L.kdb_last_skinner_samples.restype = I64
+    L.kdb_last_skinner_samples.argtypes = [P, P, P, I64]
     declare_result_api(L, "kdb_")
     _lib = L
     return L
@@ -191,6 +214,10 @@ class Engine:
             return n
         return Result.from_handle(self.lib, "kdb_", self.ctx, h)
 
+    def set_prepared_queries(self, on: bool) -> None:
+        """Replay repeated plans as recorded CUDA graphs (default on)."""
+        self._check(self.lib.kdb_ctx_set_prepared_queries(self.ctx, 1 if on else 0))
+
     def last_device_ms(self) -> float:
         return self.lib.kdb_last_query_device_ms(self.ctx)
 
@@ -207,6 +234,31 @@ class Engine:
 
     def last_skinner_episodes(self) -> int:
         return self.lib.kdb_last_skinner_episodes(self.ctx)
+
+    def last_skinner_work(self) -> int:
+        """Tuples examined by all episodes of the last Skinner join."""
+        return self.lib.kdb_last_skinner_work(self.ctx)
+
+    def set_skinner_policy(self, policy: str = "uct", prior: "JoinPriorModel" = None, log: bool = False) -> None:
+        """Join-order search: "uct" (the reference's), "prior" (UCT seeded by
+        a learned JoinPriorModel), "random" (random connected orders, for
+        collecting training samples); `log` records (features, reward) of
+        every episode step."""
+        code = {"uct": 0, "prior": 1, "random": 2}[policy]
+        self._check(self.lib.kdb_ctx_set_skinner_policy(self.ctx, code, prior.h if prior else None,
+                                                         1 if log else 0))
+        self._prior = prior
+
+    def last_skinner_samples(self):
+        """(features [n, 64] float32, rewards [n] float32) of the last Skinner
+        join run with logging on."""
+        n = self.lib.kdb_last_skinner_samples(self.ctx, None, None, 0)
+        d = self.lib.kdb_mlp_num_features()
+        x = np.zeros((n, d), np.float32)
+        r = np.zeros(n, np.float32)
+        if n:
+            self.lib.kdb_last_skinner_samples(self.ctx, _ptr(x), _ptr(r), n)
+        return x, r
 
     def stream_handle(self) -> int:
         return self.lib.kdb_ctx_stream(self.ctx) or 0
@@ -365,3 +417,68 @@ class Server:
 
     def __exit__(self, *a):
         self.close()
+
+
+class JoinPriorModel:
+    """The learned join-order prior (kdb_mlp_*): a 64-128-128-128-1 ReLU MLP
+    whose forward, backward and Adam kernels run on the engine's GPU."""
+
+    MAX_ROWS = 4096
+
+    def __init__(self, engine: Engine, seed: int = 0):
+        self.engine = engine
+        self.lib = engine.lib
+        h = ctypes.c_void_p()
+        engine._check(self.lib.kdb_mlp_create(engine.ctx, seed, ctypes.byref(h)))
+        self.h = h
+        self.num_features = int(self.lib.kdb_mlp_num_features())
+        self.num_params = int(self.lib.kdb_mlp_num_params())
+
+    def _check(self, rc):
+        if rc != 0:
+            raise KdbError(rc, self.lib.kdb_mlp_last_error(self.h).decode())
+
+    def params(self) -> np.ndarray:
+        p = np.zeros(self.num_params, np.float32)
+        self._check(self.lib.kdb_mlp_get_params(self.h, _ptr(p), self.num_params))
+        return p
+
+    def set_params(self, p) -> None:
+        p = np.ascontiguousarray(p, np.float32)
+        self._check(self.lib.kdb_mlp_set_params(self.h, _ptr(p), p.size))
+
+    def forward(self, x) -> np.ndarray:
+        x = np.ascontiguousarray(x, np.float32)
+        out = []
+        for i in range(0, len(x), self.MAX_ROWS):
+            xb = np.ascontiguousarray(x[i:i + self.MAX_ROWS])
+            y = np.zeros(len(xb), np.float32)
+            self._check(self.lib.kdb_mlp_forward(self.h, _ptr(xb), len(xb), _ptr(y)))
+            out.append(y)
+        return np.concatenate(out) if out else np.zeros(0, np.float32)
+
+    def gradient(self, x, t):
+        x = np.ascontiguousarray(x, np.float32)
+        t = np.ascontiguousarray(t, np.float32)
+        g = np.zeros(self.num_params, np.float32)
+        loss = ctypes.c_double()
+        self._check(self.lib.kdb_mlp_gradient(self.h, _ptr(x), _ptr(t), len(x), _ptr(g), ctypes.byref(loss)))
+        return g, loss.value
+
+    def train_step(self, x, t, lr: float = 1e-3) -> float:
+        x = np.ascontiguousarray(x, np.float32)
+        t = np.ascontiguousarray(t, np.float32)
+        loss = ctypes.c_double()
+        self._check(self.lib.kdb_mlp_train_step(self.h, _ptr(x), _ptr(t), len(x), lr, ctypes.byref(loss)))
+        return loss.value
+
+    def close(self):
+        if self.h:
+            self.lib.kdb_mlp_free(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -79,3 +79,17 @@ def test_serving_needs_a_device_context():
     assert lib.kdb_server_submit(None, b"{}") < 0
     assert lib.kdb_server_poll(None, 1, 0, None) < 0
     e.close()
+
+
+def test_join_prior_needs_a_device_context():
+    from kushdb_b200.engine import JoinPriorModel, KdbError
+    e = Engine(-1)
+    with pytest.raises(KdbError, match="GPU"):
+        JoinPriorModel(e)
+    with pytest.raises(KdbError):
+        e.set_skinner_policy("prior")  # no model
+    e.set_skinner_policy("random", log=True)
+    e.set_skinner_policy("uct")
+    lib = load_library()
+    assert lib.kdb_mlp_num_params() == 41473 and lib.kdb_mlp_num_features() == 64
+    e.close()

@@ -16,7 +16,8 @@ def engine():
 
 
 @pytest.mark.parametrize("n,bits,hi", [(1, 64, 10), (7, 64, 3), (2048, 64, 1 << 40), (2049, 64, 100),
-                                       (100_000, 64, 1 << 62), (300_000, 20, 1 << 20), (1 << 20, 64, 7)])
+                                       (5000, 64, 1 << 63), (40_000, 64, 1 << 40), (100_000, 64, 1 << 62),
+                                       (300_000, 20, 1 << 20), (1 << 20, 64, 7)])
 def test_sort_pairs_matches_stable_argsort(engine, n, bits, hi):
     import torch
     rng = np.random.default_rng(n + bits)
