@@ -67,10 +67,12 @@ def make_workload(name: str, scale: float = 1.0):
         b, p = wl.join_tables(build_rows=b_rows, probe_rows=p_rows)
         cfg = {"workload": "hash_join+group_by+order_by (Q3 shape)", "build_rows": b_rows,
                "probe_rows": p_rows, "fk": "uniform"}
-        # groups ~ build rows passing the filters (45.7% x 20%)
+        # groups ~ build rows passing the filters (45.7% x 20%); the dominant
+        # kernel is the probe pipeline that aggregates into the groups: it
+        # reads the probe columns (20 B/row) and writes 16 B per group
         groups = int(b_rows * 0.457 * 0.2)
-        return [b, p], wl.join_plan(b, p), b_rows + p_rows, wl.join_bytes(b_rows, p_rows, groups), \
-            "materialize", cfg
+        cfg["query_algorithmic_bytes"] = wl.join_bytes(b_rows, p_rows, groups)
+        return [b, p], wl.join_plan(b, p), b_rows + p_rows, p_rows * 20 + groups * 16, "group by", cfg
     raise SystemExit(f"unknown workload {name}")
 
 
@@ -133,48 +135,60 @@ def _ranks(values):
     return r
 
 
-def run_cpu_baseline(name: str, tables):
+def run_cpu_baseline(name: str, tables, threads: int = 1):
     """One execution of the compiled CPU baseline loop for the workload
     (oracle/baseline.cc: the reference's generated-code loop + runtime
-    structures, restated, one thread).  Returns seconds."""
+    structures, restated; one thread like the reference executor, or the rows
+    split over `threads` host threads with partial tables merged).  Returns
+    seconds."""
     import oracle
     from kushdb_b200.plan import EPOCH_JDN
     if name == "scan_agg":
-        return oracle.baseline_scan_agg(tables[0], 9300 + EPOCH_JDN, 0.05, 0.07)[0]
+        return oracle.baseline_scan_agg(tables[0], 9300 + EPOCH_JDN, 0.05, 0.07, threads=threads)[0]
     if name == "group_by":
         return oracle.baseline_group_by(tables[0], 10471 + EPOCH_JDN, _ranks(wl.RF_VALUES),
-                                        _ranks(wl.LS_VALUES))[0]
+                                        _ranks(wl.LS_VALUES), threads=threads)[0]
     return oracle.baseline_join_group(tables[0], tables[1], 9204 + EPOCH_JDN,
-                                      wl.SEG_VALUES.index("BUILDING"))[0]
+                                      wl.SEG_VALUES.index("BUILDING"), threads=threads)[0]
 
 
 def cpu_baseline(name: str, tables, rows: int, repeats: int = 3):
     """Times the compiled CPU baseline on the full workload (a few seconds of
-    CPU work at most); rows/s from the best of `repeats`."""
-    secs = min(run_cpu_baseline(name, tables) for _ in range(repeats))
-    return rows / secs, {"rows": rows, "seconds": secs, "repeats": repeats}
+    CPU work at most), on every host core and on one; rows/s from the best
+    of `repeats`."""
+    import oracle
+    threads = oracle.host_threads()
+    secs = min(run_cpu_baseline(name, tables, threads) for _ in range(repeats))
+    secs1 = min(run_cpu_baseline(name, tables, 1) for _ in range(repeats))
+    return rows / secs, {"rows": rows, "seconds": secs, "repeats": repeats, "threads": threads,
+                         "single_thread_rows_per_second": rows / secs1}
 
 
 def run_reference(args):
+    """The CPU arm: the reference's path restated (no build of the reference
+    is possible here), on all host cores, on the same workload and metric."""
+    import oracle
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
+    threads = oracle.host_threads()
     tables, plan, rows, _, _, cfg = make_workload(args.workload)
     for _ in range(args.warmup):
-        run_cpu_baseline(args.workload, tables)
+        run_cpu_baseline(args.workload, tables, threads)
     total = 0.0
     for _ in range(args.steps):
-        total += run_cpu_baseline(args.workload, tables)
+        total += run_cpu_baseline(args.workload, tables, threads)
     value = rows * args.steps / total
     line = {
         "impl": "reference", "metric": "rows_per_second", "value": value, "unit": "rows/s",
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": total / args.steps * 1e3, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": cfg,
-        "cpu_baseline": {"value": value, "unit": "rows/s", "cores": 1, "kind": "port",
+        "cpu_baseline": {"value": value, "unit": "rows/s", "cores": threads, "kind": "port",
                          "sample": f"the full {args.workload} workload ({rows} rows) per step: "
                                    "compiled restatement of the reference's generated loop and "
-                                   "runtime tables, one thread like the reference executor"},
+                                   f"runtime tables, rows split over {threads} host threads "
+                                   "(partial tables merged)"},
         "e2e": {"value": value, "unit": "rows/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line))
@@ -337,88 +351,100 @@ def run_skinner(args):
 
 
 def run_serving(args):
-    """Serving form: a stream of requests mixing four query shapes (scan +
-    aggregate, group-by, join + group-by + ORDER BY, Skinner multiway join)
-    arrives as a Poisson process; the server's slots run them concurrently.
-    Reports throughput and submission-to-completion latency (p50/p99), beside
-    the same request sequence run one at a time through the plain API."""
+    """Serving form (C5): requests arrive (all at once, then as a Poisson
+    process) and the server's slots run them concurrently.  The default mix
+    is Skinner multiway joins (star/chain, 6-8 tables, 1e4-3e6 rows, Zipf
+    0/1.5, LIKE filters) under plain UCT and under UCT seeded by the learned
+    prior; `--serving-mix mixed` adds scan + aggregate, group-by and join +
+    group-by shapes.  Reports queries/s and submission-to-completion
+    latency p50/p99, beside the same requests run one at a time."""
     import random
     import torch
     from kushdb_b200.engine import Engine, Server
     local = int(os.environ.get("LOCAL_RANK", "0"))
     torch.cuda.set_device(local)
     eng = Engine(local)
-    sa = wl.scan_agg_table(1_000_000, name="srv_sales")
-    gb = wl.group_by_table(6_000_000, name="srv_lineitem")
-    build, probe = wl.join_tables(1_500_000, 6_000_000)
-    sk, tokens = wl.skinner_tables("star", 6, min_rows=10_000, max_rows=1_000_000, seed=5, prefix="srv_sk")
-    for t in [sa, gb, build, probe] + sk:
-        eng.register_table(t)
-    shapes = {
-        "scan_agg": [wl.scan_agg_plan(sa, date_lt=d) for d in (9000, 9300, 9800)],
-        "group_by": [wl.group_by_plan(gb, date_leq=d) for d in (10000, 10471)],
-        "join_group": [wl.join_plan(build, probe, date_lt=d) for d in (9000, 9204)],
-        "skinner": [wl.skinner_plan(sk, tokens, "star")],
-    }
-    plans = [(k, p.to_json().encode()) for k, ps in shapes.items() for p in ps]
-    alone_ms = {}
-    for k, p in plans:  # compile and warm every pipeline
-        for _ in range(args.warmup):
-            eng.execute(p, fetch=False)
-    stream = torch.cuda.ExternalStream(eng.stream_handle())
+    budget = args.skinner_budget
+    model, info = train_join_prior(eng, budget)
+    plans = []
+    for name, tables, plan in skinner_queries(100, args.skinner_queries):
+        for t in tables:
+            eng.register_table(t)
+        plans.append((name, plan.to_json().encode()))
+    if args.serving_mix == "mixed":
+        sa = wl.scan_agg_table(1_000_000, name="srv_sales")
+        gb = wl.group_by_table(6_000_000, name="srv_lineitem")
+        build, probe = wl.join_tables(1_500_000, 6_000_000)
+        for t in (sa, gb, build, probe):
+            eng.register_table(t)
+        plans += [("scan_agg", wl.scan_agg_plan(sa, date_lt=d).to_json().encode()) for d in (9000, 9800)]
+        plans += [("group_by", wl.group_by_plan(gb, date_leq=d).to_json().encode()) for d in (10000, 10471)]
+        plans += [("join_group", wl.join_plan(build, probe, date_lt=d).to_json().encode()) for d in (9000, 9204)]
+    eng.set_skinner(budget, 0)
     rnd = random.Random(1234)
     n = args.serving_requests
     seq = [plans[rnd.randrange(len(plans))] for _ in range(n)]
-    # one at a time through the plain API (device time per request)
-    t0 = time.perf_counter()
-    for k, p in seq:
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record(stream)
-        eng.execute(p, fetch=False)
-        e1.record(stream)
-        e1.synchronize()
-        alone_ms.setdefault(k, []).append(e0.elapsed_time(e1))
-    seq_s = time.perf_counter() - t0
+    stream = torch.cuda.ExternalStream(eng.stream_handle())
     out = {}
-    for mode in ("saturated", "poisson"):
-        with ClockSampler(local) as clocks, Server(eng, slots=args.serving_slots,
-                                                   hbm_budget_bytes=args.serving_budget_gb << 30) as srv:
-            tickets = []
-            t0 = time.perf_counter()
-            if mode == "saturated":
-                for _, p in seq:
-                    tickets.append(srv.submit(p))
-            else:
-                gaps = np.random.default_rng(7).exponential(1.0 / args.serving_rate, n)
-                t_next = t0
-                for (_, p), g in zip(seq, gaps):
-                    t_next += g
-                    while time.perf_counter() < t_next:
-                        pass
-                    tickets.append(srv.submit(p))
-            for t in tickets:
-                r = srv.wait(t)
-                r.close()
-            wall = time.perf_counter() - t0
-            st = srv.stats()
-        st["wall_s"] = wall
-        st["clocks"] = clocks.summary()
-        out[mode] = st
-    sat = out["saturated"]
+    for policy in ("uct", "prior"):
+        eng.set_skinner_policy(policy, prior=model if policy == "prior" else None)
+        for _ in range(args.warmup):  # compile and warm every pipeline
+            for _, p in plans:
+                eng.execute(p, fetch=False)
+        # one at a time through the plain API (device time per request)
+        alone = {}
+        t0 = time.perf_counter()
+        for k, p in seq:
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            eng.execute(p, fetch=False)
+            e1.record(stream)
+            e1.synchronize()
+            alone.setdefault(k, []).append(e0.elapsed_time(e1))
+        seq_s = time.perf_counter() - t0
+        res = {"one_at_a_time": {"queries_per_second": n / seq_s,
+                                 "device_ms_p50_by_query": {k: statistics.median(v) for k, v in alone.items()}}}
+        for mode in ("saturated", "poisson"):
+            with ClockSampler(local) as clocks, Server(eng, slots=args.serving_slots,
+                                                       hbm_budget_bytes=args.serving_budget_gb << 30) as srv:
+                tickets = []
+                t0 = time.perf_counter()
+                if mode == "saturated":
+                    for _, p in seq:
+                        tickets.append(srv.submit(p))
+                else:
+                    gaps = np.random.default_rng(7).exponential(1.0 / args.serving_rate, n)
+                    t_next = t0
+                    for (_, p), g in zip(seq, gaps):
+                        t_next += g
+                        while time.perf_counter() < t_next:
+                            pass
+                        tickets.append(srv.submit(p))
+                for t in tickets:
+                    srv.wait(t).close()
+                st = srv.stats()
+                st["wall_s"] = time.perf_counter() - t0
+            st["clocks"] = clocks.summary()
+            res[mode] = st
+        out[policy] = res
+    eng.set_skinner_policy("uct")
+    best = max(out, key=lambda k: out[k]["saturated"]["queries_per_second"])
+    sat = out[best]["saturated"]
     line = {
         "metric": "queries_per_second", "value": sat["queries_per_second"], "unit": "queries/s",
         "n_gpus": 1, "steps": n, "warmup": args.warmup, "ms_per_step": 1e3 / sat["queries_per_second"],
-        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": "serving mix (scan_agg 1M rows, group_by 6M, join_group 1.5M x 6M, "
-                               "skinner star of 6 tables 10k-1M rows)", "requests": n,
-                   "slots": args.serving_slots, "hbm_budget_gb": args.serving_budget_gb,
-                   "poisson_rate_qps": args.serving_rate, "l2": "inputs larger than L2 (126 MB)"},
-        "saturated": sat,
-        "poisson": out["poisson"],
-        "one_at_a_time": {"queries_per_second": n / seq_s,
-                          "device_ms_p50_by_shape": {k: statistics.median(v) for k, v in alone_ms.items()}},
-        "speedup_vs_one_at_a_time": sat["queries_per_second"] / (n / seq_s),
-        "gpu_launches": sat["kernel_launches"] + out["poisson"]["kernel_launches"],
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int32", "data": "synthetic",
+        "config": {"workload": "served Skinner multiway joins (star/chain, 6-8 tables, rows log-uniform "
+                               "[1e4, 3e6], zipf 0/1.5, LIKE '%tok%' filters)"
+                               + (" + scan_agg/group_by/join_group" if args.serving_mix == "mixed" else ""),
+                   "requests": n, "distinct_queries": len(plans), "slots": args.serving_slots,
+                   "hbm_budget_gb": args.serving_budget_gb, "poisson_rate_qps": args.serving_rate,
+                   "budget_per_episode": budget, "policy": best, "l2": "inputs larger than L2 (126 MB)"},
+        "p50_ms": out[best]["poisson"]["p50_ms"], "p99_ms": out[best]["poisson"]["p99_ms"],
+        "policies": out,
+        "speedup_vs_one_at_a_time": sat["queries_per_second"] / out[best]["one_at_a_time"]["queries_per_second"],
+        "prior_training": info,
+        "gpu_launches": sum(out[k][m]["kernel_launches"] for k in out for m in ("saturated", "poisson")),
         "clocks": sat["clocks"],
     }
     print(json.dumps(line))
@@ -434,11 +460,15 @@ def main():
                     choices=["group_by", "scan_agg", "join_group", "batched", "serving", "skinner"])
     ap.add_argument("--batch-queries", type=int, default=256)
     ap.add_argument("--batch-max-fact", type=int, default=6_000_000)
+    ap.add_argument("--rows", type=int, default=0,
+                    help="rows per step for scan_agg / group_by / join_group (size sweeps); default: the "
+                         "configuration's own size")
     ap.add_argument("--skinner-budget", type=int, default=100_000)
     ap.add_argument("--skinner-queries", type=int, default=8)
-    ap.add_argument("--serving-requests", type=int, default=2000)
+    ap.add_argument("--serving-requests", type=int, default=400)
+    ap.add_argument("--serving-mix", default="skinner", choices=["skinner", "mixed"])
     ap.add_argument("--serving-slots", type=int, default=4)
-    ap.add_argument("--serving-rate", type=float, default=1000.0)
+    ap.add_argument("--serving-rate", type=float, default=50.0)
     ap.add_argument("--serving-budget-gb", type=int, default=32)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
@@ -470,7 +500,10 @@ def main():
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
 
     from kushdb_b200.engine import Engine
-    tables, plan, rows, algo_bytes, dom_tag, cfg = make_workload(args.workload)
+    scale = 1.0
+    if args.rows:
+        scale = args.rows / {"scan_agg": 1_000_000, "group_by": 6_000_000, "join_group": 7_500_000}[args.workload]
+    tables, plan, rows, algo_bytes, dom_tag, cfg = make_workload(args.workload, scale)
     eng = Engine(local)
     for t in tables:
         eng.register_table(t)
@@ -577,12 +610,14 @@ def main():
     if not args.no_cpu_baseline:
         try:
             v, info = cpu_baseline(args.workload, tables, rows)
-            cpu = {"value": v, "unit": "rows/s", "cores": 1, "kind": "port",
+            cpu = {"value": v, "unit": "rows/s", "cores": info["threads"], "kind": "port",
+                   "single_thread_value": info["single_thread_rows_per_second"],
                    "sample": f"full workload ({info['rows']} rows), best of {info['repeats']}: "
-                             f"{info['seconds']:.4f} s; compiled restatement of the reference's "
-                             "generated loop + runtime tables (oracle/baseline.cc), one thread"}
+                             f"{info['seconds']:.4f} s on {info['threads']} host threads; compiled "
+                             "restatement of the reference's generated loop + runtime tables "
+                             "(oracle/baseline.cc), rows split over the threads"}
         except Exception as ex:  # the oracle is a reported baseline, not the product
-            cpu = {"value": None, "unit": "rows/s", "cores": 1, "kind": "port", "sample": f"failed: {ex}"}
+            cpu = {"value": None, "unit": "rows/s", "cores": 0, "kind": "port", "sample": f"failed: {ex}"}
 
     cfg = dict(cfg)
     cfg["l2"] = "flushed between steps (256 MiB write, then 256 MiB read)" if flush is not None else \

@@ -20,6 +20,7 @@
 #include <cstdio>
 #include <cstring>
 #include <functional>
+#include <limits>
 #include <map>
 #include <random>
 #include <set>
@@ -422,14 +423,19 @@ void EmitPartialReduce(KernelSource& ks, const std::string& part, const std::str
     ks.Open("case " + std::to_string(w) + ":");
     switch (kinds[w]) {
       case WordKind::AddF64:
-        ks.L("{ double x = 0.0; for (int64_t b = lane; b < (int64_t)" + G + "; b += 32) x = __dadd_rn(x, __longlong_as_double((long long)" +
-             part + "[b * " + std::to_string(nw) + " + k]));");
+        ks.L("{ double x = 0.0; for (int64_t b0 = lane; b0 < (int64_t)" + G + "; b0 += 256) { uint64_t v[8]; "
+             "_Pragma(\"unroll\") for (int u = 0; u < 8; u++) { const int64_t b = b0 + 32 * u; v[u] = b < (int64_t)" + G +
+             " ? " + part + "[b * " + std::to_string(nw) + " + k] : 0ULL; } "
+             "_Pragma(\"unroll\") for (int u = 0; u < 8; u++) if (b0 + 32 * u < (int64_t)" + G +
+             ") x = __dadd_rn(x, __longlong_as_double((long long)v[u])); }");
         ks.L("for (int o = 16; o > 0; o >>= 1) x = __dadd_rn(x, __shfl_down_sync(0xffffffffu, x, o));");
         ks.L("acc = (uint64_t)__double_as_longlong(x); }");
         break;
       case WordKind::AddI64:
-        ks.L("{ uint64_t x = 0; for (int64_t b = lane; b < (int64_t)" + G + "; b += 32) x += " + part + "[b * " +
-             std::to_string(nw) + " + k];");
+        ks.L("{ uint64_t x = 0; for (int64_t b0 = lane; b0 < (int64_t)" + G + "; b0 += 256) { uint64_t v[8]; "
+             "_Pragma(\"unroll\") for (int u = 0; u < 8; u++) { const int64_t b = b0 + 32 * u; v[u] = b < (int64_t)" + G +
+             " ? " + part + "[b * " + std::to_string(nw) + " + k] : 0ULL; } "
+             "_Pragma(\"unroll\") for (int u = 0; u < 8; u++) x += v[u]; }");
         ks.L("for (int o = 16; o > 0; o >>= 1) x += __shfl_down_sync(0xffffffffu, x, o);");
         ks.L("acc = x; }");
         break;
@@ -437,8 +443,10 @@ void EmitPartialReduce(KernelSource& ks, const std::string& part, const std::str
       case WordKind::MaxU64: {
         bool mn = kinds[w] == WordKind::MinU64;
         std::string cmp = mn ? "<" : ">";
-        ks.L(std::string("{ uint64_t x = ") + (mn ? "~0ULL" : "0ULL") + "; for (int64_t b = lane; b < (int64_t)" + G +
-             "; b += 32) { uint64_t y = " + part + "[b * " + std::to_string(nw) + " + k]; x = y " + cmp + " x ? y : x; }");
+        ks.L(std::string("{ uint64_t x = ") + (mn ? "~0ULL" : "0ULL") + "; for (int64_t b0 = lane; b0 < (int64_t)" + G +
+             "; b0 += 256) { uint64_t v[8]; _Pragma(\"unroll\") for (int u = 0; u < 8; u++) { const int64_t b = b0 + 32 * u; "
+             "v[u] = b < (int64_t)" + G + " ? " + part + "[b * " + std::to_string(nw) + " + k] : x; } "
+             "_Pragma(\"unroll\") for (int u = 0; u < 8; u++) x = v[u] " + cmp + " x ? v[u] : x; }");
         ks.L("for (int o = 16; o > 0; o >>= 1) { uint64_t y = __shfl_down_sync(0xffffffffu, x, o); x = y " + cmp +
              " x ? y : x; }");
         ks.L("acc = x; }");
@@ -542,6 +550,16 @@ struct JoinTable {
   int64_t n = 0;
 };
 
+// An ungrouped aggregate over a Skinner join evaluated inside the episode
+// kernel: no result row is materialised.  `state` holds, per aggregate, a
+// value word and a count word, then the row count and the first position
+// (the layout of the aggregate's per-CTA partials).
+struct SkinnerAgg {
+  const std::vector<AggPlan>* plans = nullptr;
+  uint64_t* state = nullptr;
+  int nw = 0;
+};
+
 class Executor {
  public:
   Executor(Context& ctx, Arena& arena) : ctx_(ctx), arena_(arena) {}
@@ -641,13 +659,17 @@ class Executor {
   MatBuffer RunAggregate(const Operator& op);
   MatBuffer RunGroupBy(const Operator& op);
   MatBuffer RunOrderBy(const Operator& op);
-  MatBuffer RunSkinner(const Operator& op);
+  MatBuffer RunSkinner(const Operator& op, const SkinnerAgg* agg = nullptr);
   MatBuffer SmallOrderBy(const Operator& op, MatBuffer& m);
   MatBuffer LargeOrderBy(const Operator& op, MatBuffer& m);
   MatBuffer RunGroupByDense(const Operator& op, const std::vector<AggPlan>& plans, const KeyLayout& kl);
+  bool BuildRowGroups(const Operator& op, std::vector<int>* key_cols);
+  MatBuffer RunGroupByBuildRows(const Operator& op, const std::vector<AggPlan>& plans,
+                                const std::vector<int>& key_cols);
   void BuildJoin(const Operator& op);
   JoinTable BuildIndex(const MatBuffer& m, const std::vector<int>& key_cols);
   JoinTable BuildGroupedIndex(const MatBuffer& m, int key_col);
+  std::string probe_br_;  // inside an on_match callback: the matched build row's index
   void EmitProbe(KernelSource& ks, ExprGen& eg, const JoinTable& jt,
                  const std::vector<int>& build_key_cols, const std::vector<CVal>& probe_keys,
                  const std::function<void(const std::vector<CVal>&, const std::string&)>& on_match);
@@ -765,24 +787,64 @@ void Executor::EmitStream(KernelSource& ks, ExprGen& eg, const Operator& op, con
       if (vec) {
         // 4 consecutive rows per thread, every column loaded with vector
         // loads up front (all loads of an iteration in flight together)
+        // With prefetch (default), the next iteration's vectors are loaded
+        // before this iteration's rows are processed, so a warp keeps two
+        // iterations of loads in flight.
+        const bool prefetch = !std::getenv("KDB_NO_SCAN_PREFETCH");
         ks.L("const int64_t nrows = (int64_t)" + n + ";");
-        ks.Open("for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q * 4 < nrows; q += (int64_t)gridDim.x * blockDim.x)");
+        ks.L("const int64_t qstride = (int64_t)gridDim.x * blockDim.x;");
+        std::vector<std::string> arr(cols.size()), narr(cols.size()), parr(cols.size()), pnarr(cols.size());
+        // loads of the 4 rows at `qv` into the arrays `dst` / `ndst`
+        auto fetch = [&](const std::string& qv, const std::vector<std::string>& dst,
+                         const std::vector<std::string>& ndst) {
+          ks.Open("");
+          ks.L("const int64_t fb = (" + qv + ") * 4;");
+          ks.L("const bool ffull = fb + 4 <= nrows;");
+          for (size_t k = 0; k < cols.size(); k++) {
+            const DevColumn& c = *cols[k];
+            std::string st = StoreType(c.type.id);
+            ks.L("if (ffull) kdb_ld4(" + dp[k] + ", fb, " + dst[k] + "); else for (int u = 0; u < 4; u++) " + dst[k] +
+                 "[u] = fb + u < nrows ? " + dp[k] + "[fb + u] : (" + st + ")0;");
+            if (!np[k].empty())
+              ks.L("if (ffull) kdb_ld4(" + np[k] + ", fb, " + ndst[k] + "); else for (int u = 0; u < 4; u++) " +
+                   ndst[k] + "[u] = fb + u < nrows ? " + np[k] + "[fb + u] : (int8_t)0;");
+          }
+          ks.Close();
+        };
+        if (prefetch) {
+          for (size_t k = 0; k < cols.size(); k++) {
+            parr[k] = ks.Fresh("P");
+            ks.L(StoreType(cols[k]->type.id) + " " + parr[k] + "[4];");
+            if (!np[k].empty()) {
+              pnarr[k] = ks.Fresh("PN");
+              ks.L("int8_t " + pnarr[k] + "[4];");
+            }
+          }
+          ks.L("const int64_t q0 = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;");
+          ks.Open("if (q0 * 4 < nrows)");
+          fetch("q0", parr, pnarr);
+          ks.Close();
+        }
+        ks.Open("for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q * 4 < nrows; q += qstride)");
         ks.L("const int64_t base = q * 4;");
-        ks.L("const bool full = base + 4 <= nrows;");
-        std::vector<std::string> arr(cols.size()), narr(cols.size());
         for (size_t k = 0; k < cols.size(); k++) {
-          const DevColumn& c = *cols[k];
-          std::string st = StoreType(c.type.id);
           arr[k] = ks.Fresh("L");
-          ks.L(st + " " + arr[k] + "[4];");
-          ks.L("if (full) kdb_ld4(" + dp[k] + ", base, " + arr[k] + "); else for (int u = 0; u < 4; u++) " + arr[k] +
-               "[u] = base + u < nrows ? " + dp[k] + "[base + u] : (" + st + ")0;");
+          ks.L(StoreType(cols[k]->type.id) + " " + arr[k] + "[4];");
           if (!np[k].empty()) {
             narr[k] = ks.Fresh("N");
             ks.L("int8_t " + narr[k] + "[4];");
-            ks.L("if (full) kdb_ld4(" + np[k] + ", base, " + narr[k] + "); else for (int u = 0; u < 4; u++) " +
-                 narr[k] + "[u] = base + u < nrows ? " + np[k] + "[base + u] : (int8_t)0;");
           }
+        }
+        if (prefetch) {
+          for (size_t k = 0; k < cols.size(); k++) {
+            ks.L("for (int u = 0; u < 4; u++) " + arr[k] + "[u] = " + parr[k] + "[u];");
+            if (!np[k].empty()) ks.L("for (int u = 0; u < 4; u++) " + narr[k] + "[u] = " + pnarr[k] + "[u];");
+          }
+          ks.Open("if ((q + qstride) * 4 < nrows)");
+          fetch("q + qstride", parr, pnarr);
+          ks.Close();
+        } else {
+          fetch("q", arr, narr);
         }
         ks.L("#pragma unroll");
         ks.Open("for (int u = 0; u < 4; u++)");
@@ -913,6 +975,7 @@ void Executor::EmitProbe(KernelSource& ks, ExprGen& eg, const JoinTable& jt,
   for (size_t j = 0; j < bkeys.size(); j++) eq += " && " + eg.EqOf(left.at(bkeys[j]), pk[j]);
   ks.Open("if (" + eq + ")");
   std::string bpos = ks.Ptr(jt.build.pos, "uint64_t", true) + "[" + br + "]";
+  probe_br_ = br;
   on_match(left, bpos);
   ks.Close();
   ks.Close();
@@ -1173,12 +1236,37 @@ CVal GroupResult(ExprGen& eg, const AggPlan& p, const std::string& sv, const std
 // ---------------------------------------------------------------------------
 
 MatBuffer Executor::RunAggregate(const Operator& op) {
-  PrepareInput(op.child());
   int flags = 0;
   std::vector<AggPlan> plans;
   for (const auto& a : op.aggs) plans.push_back(PlanAgg(*a, flags));
   const int nw = static_cast<int>(plans.size()) * 2 + 2;  // per agg: value, count; + rows, first
   const int block = 256;
+  // An aggregate of exact, order-free states (COUNT, MIN/MAX of keys,
+  // integer SUM) over non-NULL inputs directly above a Skinner join is
+  // evaluated inside the join's episode kernel, without materialising the
+  // join's result (JOB-style MIN(...) queries).
+  bool fuse = op.child().kind == OpKind::SKINNER_JOIN && !std::getenv("KDB_NO_SKINNER_AGG");
+  for (const auto& p : plans)
+    fuse = fuse && !p.child_nullable && p.count_flag < 0 &&
+           (p.kind == StateKind::Count || p.kind == StateKind::MinMaxKey || p.kind == StateKind::SumI64);
+  int grid = 1;
+  uint64_t* part = nullptr;
+  uint64_t* text_state = arena_.AllocT<uint64_t>(plans.size() + 1);
+  ctx_.Memset(text_state, 0, sizeof(uint64_t) * (plans.size() + 1));
+  if (fuse) {
+    part = arena_.AllocT<uint64_t>(nw);
+    std::vector<uint64_t> init(nw, 0);
+    for (size_t j = 0; j < plans.size(); j++)
+      if (plans[j].kind == StateKind::MinMaxKey && plans[j].is_min) init[2 * j] = ~0ULL;
+    init[nw - 1] = ~0ULL;
+    ctx_.H2D(part, init.data(), sizeof(uint64_t) * nw);
+    SkinnerAgg sa;
+    sa.plans = &plans;
+    sa.state = part;
+    sa.nw = nw;
+    RunSkinner(op.child(), &sa);
+  } else {
+  PrepareInput(op.child());
 
   KernelSource ks;
   ExprGen eg(ctx_, ks);
@@ -1196,8 +1284,6 @@ MatBuffer Executor::RunAggregate(const Operator& op) {
   }
   ks.L("int64_t rows = 0;");
   ks.L("uint64_t first = ~0ULL;");
-  uint64_t* text_state = arena_.AllocT<uint64_t>(plans.size() + 1);
-  ctx_.Memset(text_state, 0, sizeof(uint64_t) * (plans.size() + 1));
   std::string tsp = ks.Ptr(text_state, "uint64_t");
   auto consume = [&](const std::vector<CVal>& in, const std::string& pos) {
     Scope s;
@@ -1233,8 +1319,8 @@ MatBuffer Executor::RunAggregate(const Operator& op) {
   if (Streamable(op.child())) EmitStream(ks, eg, op.child(), consume, src_rows);
   else EmitMatScan(ks, mats_.at(&op.child()), nullptr, consume, src_rows);
 
-  int grid = ctx_.GridFor(std::max<int64_t>(src_rows, 1), block);
-  uint64_t* part = arena_.AllocT<uint64_t>(static_cast<size_t>(grid) * nw);
+  grid = ctx_.GridFor(std::max<int64_t>(src_rows, 1), block);
+  part = arena_.AllocT<uint64_t>(static_cast<size_t>(grid) * nw);
   std::string pp = ks.Ptr(part, "uint64_t");
   ks.L("__shared__ uint64_t red_u[32];");
   ks.L("__shared__ double red_d[32];");
@@ -1288,6 +1374,7 @@ MatBuffer Executor::RunAggregate(const Operator& op) {
     CUfunction f = ctx_.Kernel(src, "kdb_aggregate");
     ctx_.Launch(f, grid, block, ks.Args(), 0, "aggregate");
   }
+  }  // not fused
 
   // Finalize.  Every output column gets a NULL array: an empty input emits a
   // single all-NULL row even for COUNT (aggregate_translator.cc:82-89).
@@ -1724,12 +1811,196 @@ MatBuffer Executor::RunGroupByDense(const Operator& op, const std::vector<AggPla
   fk.Close();
   fk.Close();
   {
-    std::string src = fk.Kernel("kdb_group_by_finalize", 256);
+    std::string src = fk.Kernel("kdb_group_by_finalize", 1024);
     CUfunction f = ctx_.Kernel(src, "kdb_group_by_finalize");
-    ctx_.Launch(f, 1, 256, fk.Args(), 0, "group by finalize");
+    ctx_.Launch(f, 1, 1024, fk.Args(), 0, "group by finalize");
   }
   out.rows = ReadU64(ngroups);
   ctx_.CheckDeviceError("group by");
+  out.pos_is_index = true;
+  return out;
+}
+
+// GROUP BY over a hash join whose keys are all build-side columns and
+// include the build key, with that key unique among the build rows (checked
+// on the device): each build row then is its own group, so the matched build
+// row's index is the group id and no group table is probed.  (The reference
+// still hashes every joined row into its AggregateHashTable,
+// compile/proxy/aggregate_hash_table.cc:187-243; the groups, their values
+// and their first-insertion order are the same.)
+bool Executor::BuildRowGroups(const Operator& op, std::vector<int>* key_cols) {
+  const Operator& join = op.child();
+  if (join.kind != OpKind::HASH_JOIN || op.group_by.empty() || !joins_.count(&join)) return false;
+  const JoinTable& jt = joins_.at(&join);
+  if (jt.build.rows <= 0 || jt.build.rows >= (int64_t(1) << 31)) return false;
+  key_cols->clear();
+  for (const auto& g : op.group_by) {
+    if (g->kind != ExprKind::ColRef || g->child_idx != 0) return false;
+    const Expr& src = *join.output.at(g->column_idx).expr;
+    if (src.kind != ExprKind::ColRef || src.child_idx != 0) return false;
+    key_cols->push_back(src.column_idx);
+  }
+  std::vector<int> bkeys;
+  for (const auto& k : join.left_keys) {
+    if (std::find(key_cols->begin(), key_cols->end(), k->column_idx) == key_cols->end()) return false;
+    bkeys.push_back(k->column_idx);
+  }
+  // uniqueness of the build key: every non-NULL build row must find itself
+  // only (rows with a NULL key never join)
+  uint64_t* dup = arena_.AllocT<uint64_t>(1);
+  ctx_.Memset(dup, 0, sizeof(uint64_t));
+  {
+    KernelSource ks;
+    ExprGen eg(ctx_, ks);
+    std::string N = ks.Word(static_cast<uint64_t>(jt.build.rows)), D = ks.Ptr(dup, "unsigned long long");
+    ks.Open("for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < (int64_t)" + N +
+            "; r += (int64_t)gridDim.x * blockDim.x)");
+    auto vals = LoadMatRow(ks, eg, jt.build, "r", nullptr);
+    std::vector<CVal> keys;
+    for (int c : bkeys) keys.push_back(vals.at(c));
+    ks.L("int matches = 0;");
+    EmitProbe(ks, eg, jt, bkeys, keys, [&](const std::vector<CVal>&, const std::string&) { ks.L("matches++;"); });
+    ks.L("if (matches > 1) atomicOr(" + D + ", 1ULL);");
+    ks.Close();
+    LaunchPipeline(ks, jt.build.rows, "join key check");
+  }
+  return ReadU64(dup) == 0 || ctx_.dry;
+}
+
+MatBuffer Executor::RunGroupByBuildRows(const Operator& op, const std::vector<AggPlan>& plans,
+                                        const std::vector<int>& key_cols) {
+  const Operator& join = op.child();
+  const JoinTable& jt = joins_.at(&join);
+  const int64_t nb = jt.build.rows;
+  const size_t nk = op.group_by.size();
+  uint64_t* first = arena_.AllocT<uint64_t>(nb);
+  std::vector<uint64_t*> sv(plans.size()), sc(plans.size());
+  for (size_t j = 0; j < plans.size(); j++) {
+    sv[j] = arena_.AllocT<uint64_t>(nb);
+    sc[j] = arena_.AllocT<uint64_t>(nb);
+  }
+  {
+    KernelSource ks;
+    std::string F = ks.Ptr(first, "uint64_t"), C = ks.Word(static_cast<uint64_t>(nb));
+    ks.Open("for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < (int64_t)" + C +
+            "; i += (int64_t)gridDim.x * blockDim.x)");
+    ks.L(F + "[i] = ~0ULL;");
+    for (size_t j = 0; j < plans.size(); j++) {
+      std::string V = ks.Ptr(sv[j], "uint64_t"), N = ks.Ptr(sc[j], "uint64_t");
+      bool min_init = plans[j].kind == StateKind::MinMaxKey && plans[j].is_min;
+      ks.L(V + "[i] = " + (min_init ? "~0ULL" : "0ULL") + "; " + N + "[i] = 0;");
+    }
+    ks.Close();
+    LaunchPipeline(ks, nb, "group init");
+  }
+  // probe pipeline: aggregate into the matched build row
+  {
+    KernelSource ks;
+    ExprGen eg(ctx_, ks);
+    std::string F = ks.Ptr(first, "uint64_t");
+    std::vector<std::string> SV(plans.size()), SC(plans.size());
+    for (size_t j = 0; j < plans.size(); j++) {
+      SV[j] = ks.Ptr(sv[j], "uint64_t");
+      SC[j] = ks.Ptr(sc[j], "uint64_t");
+    }
+    std::vector<int> bkeys;
+    for (const auto& k : join.left_keys) bkeys.push_back(k->column_idx);
+    int64_t src_rows = 0;
+    auto body = [&](const std::vector<CVal>& right, const std::string& pos) {
+      Scope s;
+      s.child.resize(2);
+      s.child[1] = right;
+      std::vector<CVal> pk;
+      for (const auto& k : join.right_keys) pk.push_back(eg.Emit(*k, s));
+      EmitProbe(ks, eg, jt, bkeys, pk, [&](const std::vector<CVal>& left, const std::string& bpos) {
+        const std::string g = probe_br_;
+        Scope s2;
+        s2.child.push_back(left);
+        s2.child.push_back(right);
+        std::vector<CVal> joined;
+        for (const auto& c : join.output) joined.push_back(eg.Emit(*c.expr, s2));
+        Scope s3;
+        s3.child.push_back(joined);
+        std::string fl = "0ULL";
+        for (size_t j = 0; j < plans.size(); j++) {
+          CVal c = eg.Emit(plans[j].agg->kid(0), s3);
+          if (plans[j].count_flag >= 0)
+            fl += " | ((" + c.n + ") ? " + std::to_string(1 << plans[j].count_flag) + "ULL : 0ULL)";
+          EmitGroupUpdate(ks, eg, plans[j], c, SV[j], SC[j], g);
+        }
+        const std::string jpos = "(((uint64_t)(" + pos + ") << 32) | ((" + bpos + ") & 0xffffffffULL))";
+        ks.L("kdb_atomic_min_u64(&" + F + "[" + g + "], (" + jpos + " << 8) | (" + fl + "));");
+      });
+    };
+    if (Streamable(join.child(1))) EmitStream(ks, eg, join.child(1), body, src_rows);
+    else EmitMatScan(ks, mats_.at(&join.child(1)), nullptr, body, src_rows);
+    LaunchPipeline(ks, src_rows, "group by");
+  }
+  ctx_.CheckDeviceError("group by");
+  // groups = touched build rows, in first-insertion order
+  uint64_t* keys = arena_.AllocT<uint64_t>(nb);
+  uint32_t* vals = arena_.AllocT<uint32_t>(nb);
+  uint64_t* ngroups = arena_.AllocT<uint64_t>(1);
+  ctx_.Memset(ngroups, 0, sizeof(uint64_t));
+  {
+    KernelSource ks;
+    std::string F = ks.Ptr(first, "uint64_t", true);
+    std::string K = ks.Ptr(keys, "uint64_t"), V = ks.Ptr(vals, "uint32_t");
+    std::string NG = ks.Ptr(ngroups, "unsigned long long");
+    std::string C = ks.Word(static_cast<uint64_t>(nb));
+    ks.Open("for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < (int64_t)" + C +
+            "; i += (int64_t)gridDim.x * blockDim.x)");
+    ks.L("const uint64_t f = " + F + "[i];");
+    ks.Open("if (f != ~0ULL)");
+    ks.L("uint64_t o = kdb_alloc_slot(" + NG + ");");
+    ks.L(K + "[o] = f; " + V + "[o] = (uint32_t)i;");
+    ks.Close();
+    ks.Close();
+    LaunchPipeline(ks, nb, "group compact");
+  }
+  int64_t ng = ReadU64(ngroups);
+  ctx_.RadixSortPairs(keys, vals, ng, arena_, 64);
+  MatBuffer out = AllocMat(op.output, ng);
+  if (ng > 0) {
+    KernelSource ks;
+    ExprGen eg(ctx_, ks);
+    std::string F = ks.Ptr(first, "uint64_t", true), V = ks.Ptr(vals, "uint32_t", true);
+    std::string NGW = ks.Word(static_cast<uint64_t>(ng));
+    std::vector<std::string> SV(plans.size()), SC(plans.size());
+    for (size_t j = 0; j < plans.size(); j++) {
+      SV[j] = ks.Ptr(sv[j], "uint64_t", true);
+      SC[j] = ks.Ptr(sc[j], "uint64_t", true);
+    }
+    std::vector<std::string> optr, onull;
+    for (const auto& c : out.cols) {
+      optr.push_back(ks.Ptr(c.data, StoreType(c.type.id)));
+      onull.push_back(c.nullable ? ks.Ptr(c.nulls, "int8_t") : "");
+    }
+    std::string posp = ks.Ptr(out.pos, "uint64_t");
+    ks.Open("for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < (int64_t)" + NGW +
+            "; r += (int64_t)gridDim.x * blockDim.x)");
+    ks.L("uint64_t i = " + V + "[r];");
+    ks.L("uint64_t fst = " + F + "[i];");
+    auto bv = LoadMatRow(ks, eg, jt.build, "i", nullptr);
+    std::vector<CVal> virt;
+    for (size_t k = 0; k < nk; k++) {
+      const CVal& c = bv.at(key_cols[k]);
+      virt.push_back(eg.Bind(op.group_by[k]->type, c.v, c.n));
+    }
+    for (size_t j = 0; j < plans.size(); j++) virt.push_back(GroupResult(eg, plans[j], SV[j], SC[j], "i", "fst"));
+    Scope sc;
+    sc.virt = virt;
+    for (size_t c = 0; c < op.output.size(); c++) {
+      CVal v = eg.Emit(*op.output[c].expr, sc);
+      std::string val = v.type.id == TypeId::BOOLEAN ? "(int8_t)(" + v.v + " ? 1 : 0)" : v.v;
+      ks.L(optr[c] + "[r] = " + val + ";");
+      if (!onull[c].empty()) ks.L(onull[c] + "[r] = (" + v.n + ") ? 1 : 0;");
+    }
+    ks.L(posp + "[r] = (uint64_t)r;");
+    ks.Close();
+    LaunchPipeline(ks, ng, "group output");
+  }
+  out.rows = ng;
   out.pos_is_index = true;
   return out;
 }
@@ -1757,6 +2028,12 @@ MatBuffer Executor::RunGroupBy(const Operator& op) {
     int64_t words = static_cast<int64_t>(distinct.size()) + 2;
     if (dense && static_cast<int64_t>(kl.domain) * words <= 64 && !std::getenv("KDB_NO_DENSE_GROUPBY"))
       return RunGroupByDense(op, plans, kl);
+  }
+
+  {
+    std::vector<int> key_cols;
+    if (!std::getenv("KDB_NO_BUILD_ROW_GROUPS") && BuildRowGroups(op, &key_cols))
+      return RunGroupByBuildRows(op, plans, key_cols);
   }
 
   // capacity: exact for small key domains; otherwise twice the input-row
@@ -2404,9 +2681,10 @@ class SkinnerEngine : public JoinEnv {
  public:
   SkinnerEngine(Context& ctx, Arena& arena, const Operator& op, std::vector<const MatBuffer*> mats,
                 std::vector<std::vector<JoinTable>> index_for, const std::vector<SkinnerPred>& preds,
-                std::function<MatBuffer(int64_t)> alloc_out, int64_t budget, uint32_t seed)
+                std::function<MatBuffer(int64_t)> alloc_out, int64_t budget, uint32_t seed,
+                const SkinnerAgg* agg = nullptr)
       : ctx_(ctx), arena_(arena), op_(op), mats_(std::move(mats)), preds_(preds),
-        alloc_out_(std::move(alloc_out)), budget_(budget), seed_(seed) {
+        alloc_out_(std::move(alloc_out)), budget_(budget), seed_(seed), agg_(agg) {
     T_ = static_cast<int>(mats_.size());
     for (const MatBuffer* m : mats_) cards_.push_back(m->rows);
     offsets_.assign(T_, 0);
@@ -2522,7 +2800,12 @@ class SkinnerEngine : public JoinEnv {
   }
 
   MatBuffer Run(const std::vector<int>& prefix) {
-    out_ = alloc_out_(1 << 12);
+    if (agg_) {
+      out_ = MatBuffer();
+      out_.cap = std::numeric_limits<int64_t>::max();
+    } else {
+      out_ = alloc_out_(1 << 12);
+    }
     count_ = arena_.AllocT<uint64_t>(1);
     work_ = arena_.AllocT<uint64_t>(1);
     ctx_.Memset(count_, 0, sizeof(uint64_t));
@@ -2703,6 +2986,15 @@ class SkinnerEngine : public JoinEnv {
     w_phase_ = ks.Arg(0);
     ks.L("int64_t rows[" + TS + "]; int64_t iti[" + TS + "]; int64_t ite[" + TS + "];");
     ks.L("unsigned long long work = 0;");
+    if (agg_) {
+      ks.L("unsigned long long fa_nres = 0; int64_t fa_rows = 0;");
+      for (size_t j = 0; j < agg_->plans->size(); j++) {
+        const AggPlan& p = (*agg_->plans)[j];
+        const std::string J = std::to_string(j);
+        const bool mn = p.kind == StateKind::MinMaxKey && p.is_min;
+        ks.L("uint64_t fa_v" + J + " = " + (mn ? "~0ULL" : "0ULL") + "; int64_t fa_c" + J + " = 0;");
+      }
+    }
     std::vector<std::vector<std::string>> cache(T);
     auto load = [&](int t, std::vector<CVal>& out) {
       out = LoadMat(ks, eg, *mats_[t], "rows[" + std::to_string(t) + "]", &cache[t]);
@@ -2797,7 +3089,31 @@ class SkinnerEngine : public JoinEnv {
     // emission of one result row (output schema over the bound children)
     out_ptr_words_.clear();
     ks.Open("auto emit = [&]()");
-    {
+    if (agg_) {
+      Scope sc;
+      sc.child.resize(T);
+      for (int t = 0; t < T; t++) load(t, sc.child[t]);
+      std::vector<CVal> vals;
+      for (const auto& c : op_.output) vals.push_back(eg.Emit(*c.expr, sc));
+      Scope s2;
+      s2.child.push_back(vals);
+      for (size_t j = 0; j < agg_->plans->size(); j++) {
+        const AggPlan& p = (*agg_->plans)[j];
+        const std::string J = std::to_string(j);
+        CVal c = eg.Emit(p.agg->kid(0), s2);
+        switch (p.kind) {
+          case StateKind::MinMaxKey:
+            ks.L("{ uint64_t k = " + OKey(eg, c) + "; fa_v" + J + " = (k " + (p.is_min ? "<" : ">") + " fa_v" + J +
+                 ") ? k : fa_v" + J + "; }");
+            break;
+          case StateKind::SumI64: ks.L("fa_v" + J + " += (uint64_t)(int64_t)" + c.v + ";"); break;
+          default: break;
+        }
+        ks.L("fa_c" + J + "++;");
+      }
+      ks.L("fa_rows++; fa_nres++;");
+      w_count_ = ks.Arg(0);
+    } else {
       Scope sc;
       sc.child.resize(T);
       for (int t = 0; t < T; t++) load(t, sc.child[t]);
@@ -2890,6 +3206,23 @@ class SkinnerEngine : public JoinEnv {
     }
     std::string wk = ks.Ptr(work_, "unsigned long long");
     ks.L("if (work) atomicAdd(" + wk + ", work);");
+    if (agg_) {
+      std::string ST = ks.Ptr(agg_->state, "unsigned long long");
+      ks.Open("if (fa_rows)");
+      for (size_t j = 0; j < agg_->plans->size(); j++) {
+        const AggPlan& p = (*agg_->plans)[j];
+        const std::string J = std::to_string(j), V = std::to_string(2 * j), C = std::to_string(2 * j + 1);
+        if (p.kind == StateKind::MinMaxKey)
+          ks.L(std::string(p.is_min ? "atomicMin" : "atomicMax") + "(&" + ST + "[" + V + "], (unsigned long long)fa_v" +
+               J + ");");
+        else if (p.kind == StateKind::SumI64)
+          ks.L("atomicAdd(&" + ST + "[" + V + "], (unsigned long long)fa_v" + J + ");");
+        ks.L("atomicAdd(&" + ST + "[" + C + "], (unsigned long long)fa_c" + J + ");");
+      }
+      ks.L("atomicAdd(&" + ST + "[" + std::to_string(agg_->nw - 2) + "], (unsigned long long)fa_rows);");
+      ks.L("atomicAdd((unsigned long long*)a.w[" + std::to_string(w_count_) + "], fa_nres);");
+      ks.Close();
+    }
     std::string src = ks.Kernel("kdb_skinner_episode", 128);
     fn_ = ctx_.Kernel(src, "kdb_skinner_episode");
     args_ = ks.Args();
@@ -2897,6 +3230,7 @@ class SkinnerEngine : public JoinEnv {
 
   void PatchOut(KArgs& a) {
     a.w[w_count_] = reinterpret_cast<uint64_t>(count_);
+    if (agg_) return;
     for (size_t c = 0; c < out_.cols.size(); c++) {
       a.w[out_ptr_words_[2 * c]] = reinterpret_cast<uint64_t>(out_.cols[c].data);
       a.w[out_ptr_words_[2 * c + 1]] = reinterpret_cast<uint64_t>(out_.cols[c].nulls);
@@ -2956,6 +3290,7 @@ class SkinnerEngine : public JoinEnv {
   std::vector<int64_t> cards_, offsets_, slice_est_;
   std::vector<uint64_t> cond_tables_;
   std::set<std::pair<int, int>> connected_;
+  const SkinnerAgg* agg_ = nullptr;  // fused aggregate, or null: materialise the results
   std::vector<uint64_t> adj_;  // join-graph neighbours of each table
   static constexpr int kPriorTables = 8;
   std::map<uint64_t, std::vector<double>> prior_cache_;  // joined set -> value per table
@@ -2977,7 +3312,7 @@ class SkinnerEngine : public JoinEnv {
   std::vector<int> out_ptr_words_;
 };
 
-MatBuffer Executor::RunSkinner(const Operator& op) {
+MatBuffer Executor::RunSkinner(const Operator& op, const SkinnerAgg* agg) {
   ctx_.NotReplayable();  // episode decisions follow the host's UCT search
   const int T = static_cast<int>(op.children.size());
   if (T > 16) throw Error(-5, "Skinner join of more than 16 tables");
@@ -3003,7 +3338,7 @@ MatBuffer Executor::RunSkinner(const Operator& op) {
     if (!index_for[pr.ta][pr.ca].slots) index_for[pr.ta][pr.ca] = BuildGroupedIndex(*mats[pr.ta], pr.ca);
   }
   auto alloc = [&](int64_t cap) { return AllocMat(op.output, cap); };
-  SkinnerEngine eng(ctx_, arena_, op, mats, index_for, preds, alloc, ctx_.skinner_budget, ctx_.skinner_seed);
+  SkinnerEngine eng(ctx_, arena_, op, mats, index_for, preds, alloc, ctx_.skinner_budget, ctx_.skinner_seed, agg);
   MatBuffer out = eng.Run(op.prefix_order);
   ctx_.last_skinner_episodes = eng.episodes();
   ctx_.last_skinner_work = eng.work();

@@ -57,6 +57,12 @@ def lib():
         L.kdbo_baseline_group_by.argtypes = [P, P, P, P, P, P, P, I64, I32, P, P, P, I32, P]
         L.kdbo_baseline_join_group.restype = D
         L.kdbo_baseline_join_group.argtypes = [P, P, P, I64, I32, I32, P, P, P, I64, I32, P, P, P]
+        L.kdbo_baseline_scan_agg_mt.restype = D
+        L.kdbo_baseline_scan_agg_mt.argtypes = [P, P, P, I64, I32, D, D, P, P, P, I32]
+        L.kdbo_baseline_group_by_mt.restype = D
+        L.kdbo_baseline_group_by_mt.argtypes = [P, P, P, P, P, P, P, I64, I32, P, P, P, I32, P, I32]
+        L.kdbo_baseline_join_group_mt.restype = D
+        L.kdbo_baseline_join_group_mt.argtypes = [P, P, P, I64, I32, I32, P, P, P, I64, I32, P, P, P, I32]
         _lib = L
     return _lib
 
@@ -142,19 +148,28 @@ def oracle_for(tables: Dict[str, HostTable]) -> Oracle:
 # ---------------------------------------------------------------------------
 
 
-def baseline_scan_agg(table, date_lt_jdn: int, lo: float, hi: float):
+def host_threads() -> int:
+    """Host cores this process may run on."""
+    try:
+        return len(os.sched_getaffinity(0))
+    except AttributeError:
+        return os.cpu_count() or 1
+
+
+def baseline_scan_agg(table, date_lt_jdn: int, lo: float, hi: float, threads: int = 1):
     L = lib()
     c = table.columns
     date = np.ascontiguousarray(c["s_date"].values)
     disc = np.ascontiguousarray(c["s_discount"].values)
     price = np.ascontiguousarray(c["s_price"].values)
     s, n, e = ctypes.c_double(), ctypes.c_int64(), ctypes.c_int8()
-    secs = L.kdbo_baseline_scan_agg(_ptr(date), _ptr(disc), _ptr(price), len(date), date_lt_jdn, lo, hi,
-                                    ctypes.byref(s), ctypes.byref(n), ctypes.byref(e))
+    args = [_ptr(date), _ptr(disc), _ptr(price), len(date), date_lt_jdn, lo, hi,
+            ctypes.byref(s), ctypes.byref(n), ctypes.byref(e)]
+    secs = L.kdbo_baseline_scan_agg(*args) if threads <= 1 else L.kdbo_baseline_scan_agg_mt(*args, threads)
     return secs, (None if e.value else s.value, None if e.value else n.value)
 
 
-def baseline_group_by(table, date_leq_jdn: int, rank_rf, rank_ls):
+def baseline_group_by(table, date_leq_jdn: int, rank_rf, rank_ls, threads: int = 1):
     L = lib()
     c = table.columns
     arrs = [np.ascontiguousarray(c[k].values) for k in
@@ -163,12 +178,13 @@ def baseline_group_by(table, date_leq_jdn: int, rank_rf, rank_ls):
     rl = np.ascontiguousarray(rank_ls, np.int32)
     out = np.zeros((64, 10), np.float64)
     ng = ctypes.c_int32()
-    secs = L.kdbo_baseline_group_by(*[_ptr(a) for a in arrs], len(arrs[0]), date_leq_jdn, _ptr(rr), _ptr(rl),
-                                    _ptr(out), 64, ctypes.byref(ng))
+    args = [*[_ptr(a) for a in arrs], len(arrs[0]), date_leq_jdn, _ptr(rr), _ptr(rl), _ptr(out), 64,
+            ctypes.byref(ng)]
+    secs = L.kdbo_baseline_group_by(*args) if threads <= 1 else L.kdbo_baseline_group_by_mt(*args, threads)
     return secs, out[:min(ng.value, 64)]
 
 
-def baseline_join_group(build, probe, date_lt_jdn: int, seg: int, top: int = 10):
+def baseline_join_group(build, probe, date_lt_jdn: int, seg: int, top: int = 10, threads: int = 1):
     L = lib()
     b, p = build.columns, probe.columns
     ck, cd, cs = (np.ascontiguousarray(b[k].values) for k in ["c_custkey", "c_date", "c_segment"])
@@ -176,7 +192,7 @@ def baseline_join_group(build, probe, date_lt_jdn: int, seg: int, top: int = 10)
     keys = np.zeros(top, np.int32)
     sums = np.zeros(top, np.float64)
     ng = ctypes.c_int32()
-    secs = L.kdbo_baseline_join_group(_ptr(ck), _ptr(cd), _ptr(cs), len(ck), date_lt_jdn, seg, _ptr(ok),
-                                      _ptr(op), _ptr(od), len(ok), top, _ptr(keys), _ptr(sums),
-                                      ctypes.byref(ng))
+    args = [_ptr(ck), _ptr(cd), _ptr(cs), len(ck), date_lt_jdn, seg, _ptr(ok), _ptr(op), _ptr(od), len(ok), top,
+            _ptr(keys), _ptr(sums), ctypes.byref(ng)]
+    secs = L.kdbo_baseline_join_group(*args) if threads <= 1 else L.kdbo_baseline_join_group_mt(*args, threads)
     return secs, (ng.value, keys, sums)

@@ -38,3 +38,25 @@ def test_skinner_multiway_matches_oracle(engine, shape, n_tables, zipf, budget):
     ref = o.execute(plan)
     assert compare(g, ref) == ""
     assert engine.last_skinner_episodes() >= 1
+
+
+def test_aggregate_fused_into_episodes_matches_materialised(engine):
+    """COUNT/MIN over the join evaluated inside the episode kernel equals the
+    same aggregate over the materialised join result."""
+    import os
+    tables, tokens = wl.skinner_tables("chain", 6, min_rows=1000, max_rows=30_000, zipf_s=1.5, seed=77,
+                                       prefix="fuse_")
+    for t in tables:
+        engine.register_table(t)
+    plan = wl.skinner_plan(tables, tokens, "chain").to_json()
+    engine.set_skinner(5000, seed=3)
+    try:
+        fused = engine.execute(plan)
+        os.environ["KDB_NO_SKINNER_AGG"] = "1"
+        try:
+            plain = engine.execute(plan)
+        finally:
+            del os.environ["KDB_NO_SKINNER_AGG"]
+    finally:
+        engine.set_skinner()
+    assert compare(fused, plain) == ""

@@ -46,3 +46,25 @@ def test_join_group_baseline_matches_oracle():
     assert ng == ref.num_rows
     assert np.array_equal(sums, ref.columns[1].values[:10])
     assert np.array_equal(keys, ref.columns[0].values[:10])
+
+
+def test_threaded_baselines_match_single_thread():
+    """The all-cores CPU arm splits rows over threads and merges partial
+    tables: same groups and counts, float sums within 1e-12 relative."""
+    t = wl.scan_agg_table(rows=200_000)
+    _, (s1, n1) = oracle.baseline_scan_agg(t, 9300 + EPOCH_JDN, 0.05, 0.07)
+    _, (s4, n4) = oracle.baseline_scan_agg(t, 9300 + EPOCH_JDN, 0.05, 0.07, threads=4)
+    assert n1 == n4 and abs(s1 - s4) <= 1e-12 * abs(s1)
+    g = wl.group_by_table(rows=200_000)
+    args = (10471 + EPOCH_JDN, _ranks(wl.RF_VALUES), _ranks(wl.LS_VALUES))
+    _, r1 = oracle.baseline_group_by(g, *args)
+    _, r4 = oracle.baseline_group_by(g, *args, threads=4)
+    assert r1.shape == r4.shape
+    assert np.array_equal(r1[:, [0, 1, 9]], r4[:, [0, 1, 9]])
+    assert np.all(np.abs(r1 - r4) <= 1e-12 * np.maximum(np.abs(r1), 1e-300))
+    b, p = wl.join_tables(build_rows=20_000, probe_rows=80_000)
+    seg = wl.SEG_VALUES.index("BUILDING")
+    ng1, k1, x1 = oracle.baseline_join_group(b, p, 9204 + EPOCH_JDN, seg)[1]
+    ng4, k4, x4 = oracle.baseline_join_group(b, p, 9204 + EPOCH_JDN, seg, threads=4)[1]
+    assert ng1 == ng4 and np.array_equal(k1, k4)
+    assert np.all(np.abs(x1 - x4) <= 1e-12 * np.abs(x1))
