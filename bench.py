@@ -13,8 +13,9 @@ A step is one execution of the query over the resident table.  The timed
 region covers exactly K steps on the engine's CUDA stream (events), bracketed
 by a barrier and device synchronisation; multi-GPU runs are independent
 replicas (weak scaling, max time over ranks).  `--impl reference` times the
-CPU implementation of the path (the oracle restatement of the reference's
-generated code, single thread like the reference) on the same workload.
+CPU implementation of the path (the compiled restatement of the reference's
+generated loops and runtime tables, rows split over every host core) on the
+same workload.
 """
 
 from __future__ import annotations
@@ -503,7 +504,8 @@ def main():
     scale = 1.0
     if args.rows:
         scale = args.rows / {"scan_agg": 1_000_000, "group_by": 6_000_000, "join_group": 7_500_000}[args.workload]
-    tables, plan, rows, algo_bytes, dom_tag, cfg = make_workload(args.workload, scale)
+    tables, plan_tree, rows, algo_bytes, dom_tag, cfg = make_workload(args.workload, scale)
+    plan = plan_tree.to_json().encode()  # the statement text, prepared once like a client would
     eng = Engine(local)
     for t in tables:
         eng.register_table(t)

@@ -210,7 +210,10 @@ __global__ void BatchProbe(const QueryDesc* __restrict__ qs, int nq, const unsig
           // plain per-row IEEE arithmetic, like the reference's generated code
           const double v = __dmul_rn(__ldcs(q.f_price + r), __dsub_rn(1.0, __ldcs(q.f_disc + r)));
           atomicAdd(&a->sum, v);
-          atomicMax(&a->first_inv, ~static_cast<unsigned long long>(r));
+          // the first fact row only moves down: skip the atomic once an
+          // earlier row is already recorded (a stale read costs one atomic)
+          const unsigned long long fi = ~static_cast<unsigned long long>(r);
+          if (__ldcg(&a->first_inv) < fi) atomicMax(&a->first_inv, fi);
           break;  // keys are unique on the build side
         }
         if (++i == q.sub_cap) i = 0;

@@ -1833,6 +1833,8 @@ bool Executor::BuildRowGroups(const Operator& op, std::vector<int>* key_cols) {
   if (join.kind != OpKind::HASH_JOIN || op.group_by.empty() || !joins_.count(&join)) return false;
   const JoinTable& jt = joins_.at(&join);
   if (jt.build.rows <= 0 || jt.build.rows >= (int64_t(1) << 31)) return false;
+  // first positions keep the probe row in 24 bits (see the group ordering)
+  if (RowBound(join.child(1)) >= (int64_t(1) << 24)) return false;
   key_cols->clear();
   for (const auto& g : op.group_by) {
     if (g->kind != ExprKind::ColRef || g->child_idx != 0) return false;
@@ -1953,13 +1955,15 @@ MatBuffer Executor::RunGroupByBuildRows(const Operator& op, const std::vector<Ag
     ks.L("const uint64_t f = " + F + "[i];");
     ks.Open("if (f != ~0ULL)");
     ks.L("uint64_t o = kdb_alloc_slot(" + NG + ");");
-    ks.L(K + "[o] = f; " + V + "[o] = (uint32_t)i;");
+    // a probe row matches at most one (unique) build row, so groups'
+    // first positions differ in their probe part: sort on it alone
+    ks.L(K + "[o] = f >> 40; " + V + "[o] = (uint32_t)i;");
     ks.Close();
     ks.Close();
     LaunchPipeline(ks, nb, "group compact");
   }
   int64_t ng = ReadU64(ngroups);
-  ctx_.RadixSortPairs(keys, vals, ng, arena_, 64);
+  ctx_.RadixSortPairs(keys, vals, ng, arena_, 24);
   MatBuffer out = AllocMat(op.output, ng);
   if (ng > 0) {
     KernelSource ks;
@@ -2401,68 +2405,133 @@ MatBuffer Executor::LargeOrderBy(const Operator& op, MatBuffer& m) {
     // the tie key uses at most depth = ceil(log2 n) + 1 leading bits
     int depth = 1;
     while ((1LL << (depth - 1)) < n) depth++;
-    keygen([&](KernelSource&, ExprGen&, const std::string&) {
-      return "(kdb_tie_path((uint64_t)i, " + std::to_string(n) + "ULL) >> " + std::to_string(64 - depth) + ")";
-    });
-    ctx_.RadixSortPairs(keys, idx, n, arena_, depth);
-    const auto& child_schema = SchemaOf(op.child());
-    for (int k = static_cast<int>(op.sort_keys.size()) - 1; k >= 0; k--) {
-      int col = op.sort_keys[k]->column_idx;
-      const MatCol& mc = m.cols.at(col);
-      bool asc = op.asc[k];
-      (void)child_schema;
-      const std::string inv = asc ? "" : "~";
-      auto load = [&](KernelSource& ks, ExprGen& eg, const std::string& I) {
-        std::string D = ks.Ptr(mc.data, StoreType(mc.type.id), true);
-        return std::make_pair(D + "[" + I + "[i]]", std::string());
-      };
-      if (mc.type.id == TypeId::BOOLEAN) throw Error(-1, "Can't be less than.");
-      if (mc.type.id == TypeId::TEXT) {
-        // max length over the rows decides the number of 8-byte chunks
-        uint64_t* mx = arena_.AllocT<uint64_t>(1);
-        ctx_.Memset(mx, 0, sizeof(uint64_t));
-        {
-          KernelSource ks;
-          std::string D = ks.Ptr(mc.data, "kdb_str", true), MX = ks.Ptr(mx, "unsigned long long");
-          std::string N = ks.Word(static_cast<uint64_t>(n));
-          ks.Open("for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < (int64_t)" + N +
-                  "; i += (int64_t)gridDim.x * blockDim.x)");
-          ks.L("atomicMax(" + MX + ", (unsigned long long)" + D + "[i].len);");
-          ks.Close();
-          LaunchPipeline(ks, n, "text max len");
-        }
-        int64_t maxlen = ReadU64(mx);
-        keygen([&](KernelSource& ks, ExprGen& eg, const std::string& I) {
-          return inv + "(uint64_t)" + load(ks, eg, I).first + ".len";
-        });
-        ctx_.RadixSortPairs(keys, idx, n, arena_, 64);
-        for (int64_t c = (maxlen + 7) / 8 - 1; c >= 0; c--) {
+    auto tie_sort = [&]() {
+      keygen([&](KernelSource&, ExprGen&, const std::string&) {
+        return "(kdb_tie_path((uint64_t)i, " + std::to_string(n) + "ULL) >> " + std::to_string(64 - depth) + ")";
+      });
+      ctx_.RadixSortPairs(keys, idx, n, arena_, depth);
+    };
+    auto key_sorts = [&]() {
+      const auto& child_schema = SchemaOf(op.child());
+      for (int k = static_cast<int>(op.sort_keys.size()) - 1; k >= 0; k--) {
+        int col = op.sort_keys[k]->column_idx;
+        const MatCol& mc = m.cols.at(col);
+        bool asc = op.asc[k];
+        (void)child_schema;
+        const std::string inv = asc ? "" : "~";
+        auto load = [&](KernelSource& ks, ExprGen& eg, const std::string& I) {
+          std::string D = ks.Ptr(mc.data, StoreType(mc.type.id), true);
+          return std::make_pair(D + "[" + I + "[i]]", std::string());
+        };
+        if (mc.type.id == TypeId::BOOLEAN) throw Error(-1, "Can't be less than.");
+        if (mc.type.id == TypeId::TEXT) {
+          // max length over the rows decides the number of 8-byte chunks
+          uint64_t* mx = arena_.AllocT<uint64_t>(1);
+          ctx_.Memset(mx, 0, sizeof(uint64_t));
+          {
+            KernelSource ks;
+            std::string D = ks.Ptr(mc.data, "kdb_str", true), MX = ks.Ptr(mx, "unsigned long long");
+            std::string N = ks.Word(static_cast<uint64_t>(n));
+            ks.Open("for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < (int64_t)" + N +
+                    "; i += (int64_t)gridDim.x * blockDim.x)");
+            ks.L("atomicMax(" + MX + ", (unsigned long long)" + D + "[i].len);");
+            ks.Close();
+            LaunchPipeline(ks, n, "text max len");
+          }
+          int64_t maxlen = ReadU64(mx);
           keygen([&](KernelSource& ks, ExprGen& eg, const std::string& I) {
-            return inv + "kdb_str_chunk(" + load(ks, eg, I).first + ", " + std::to_string(c) + ")";
+            return inv + "(uint64_t)" + load(ks, eg, I).first + ".len";
+          });
+          ctx_.RadixSortPairs(keys, idx, n, arena_, 64);
+          for (int64_t c = (maxlen + 7) / 8 - 1; c >= 0; c--) {
+            keygen([&](KernelSource& ks, ExprGen& eg, const std::string& I) {
+              return inv + "kdb_str_chunk(" + load(ks, eg, I).first + ", " + std::to_string(c) + ")";
+            });
+            ctx_.RadixSortPairs(keys, idx, n, arena_, 64);
+          }
+        } else {
+          keygen([&](KernelSource& ks, ExprGen& eg, const std::string& I) {
+            std::string v = load(ks, eg, I).first;
+            std::string norm;
+            switch (mc.type.id) {
+              case TypeId::REAL: norm = "kdb_dord(" + v + ")"; break;
+              case TypeId::ENUM: norm = "(uint64_t)(uint32_t)" + eg.EnumRank(mc.type, v); break;
+              default: norm = "((uint64_t)(int64_t)" + v + " ^ 0x8000000000000000ULL)"; break;
+            }
+            return inv + "(" + norm + ")";
           });
           ctx_.RadixSortPairs(keys, idx, n, arena_, 64);
         }
-      } else {
-        keygen([&](KernelSource& ks, ExprGen& eg, const std::string& I) {
-          std::string v = load(ks, eg, I).first;
-          std::string norm;
-          switch (mc.type.id) {
-            case TypeId::REAL: norm = "kdb_dord(" + v + ")"; break;
-            case TypeId::ENUM: norm = "(uint64_t)(uint32_t)" + eg.EnumRank(mc.type, v); break;
-            default: norm = "((uint64_t)(int64_t)" + v + " ^ 0x8000000000000000ULL)"; break;
+        if (mc.nullable) {
+          keygen([&](KernelSource& ks, ExprGen&, const std::string& I) {
+            std::string NP = ks.Ptr(mc.nulls, "int8_t", true);
+            std::string isnull = "(uint64_t)(" + NP + "[" + I + "[i]] != 0)";
+            return asc ? isnull : "(1ULL - " + isnull + ")";
+          });
+          ctx_.RadixSortPairs(keys, idx, n, arena_, 8);
+        }
+      }
+    };
+    // Float sort keys rarely tie: sort the stream-ordered rows by the keys
+    // alone and check adjacent rows for ties; only if two rows tie is the
+    // merge sort's tie order (the tie-path key) needed, and the sort is
+    // redone with it from the stream order.
+    bool floats_only = !std::getenv("KDB_ORDER_TIE_SORT");
+    for (const auto& sk : op.sort_keys)
+      if (m.cols.at(sk->column_idx).type.id != TypeId::REAL) floats_only = false;
+    bool done = false;
+    if (floats_only) {
+      uint32_t* stream_rows = nullptr;  // the stream order, when it is not the identity
+      if (!m.pos_is_index) {
+        stream_rows = arena_.AllocT<uint32_t>(n);
+        KernelSource ks;
+        std::string I = ks.Ptr(idx, "uint32_t", true), SR = ks.Ptr(stream_rows, "uint32_t");
+        std::string N = ks.Word(static_cast<uint64_t>(n));
+        ks.Open("for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < (int64_t)" + N +
+                "; i += (int64_t)gridDim.x * blockDim.x)");
+        ks.L(SR + "[i] = " + I + "[i];");
+        ks.Close();
+        LaunchPipeline(ks, n, "order stream copy");
+      }
+      key_sorts();
+      uint64_t* ties = arena_.AllocT<uint64_t>(1);
+      ctx_.Memset(ties, 0, sizeof(uint64_t));
+      {
+        KernelSource ks;
+        std::string I = ks.Ptr(idx, "uint32_t", true), T = ks.Ptr(ties, "unsigned long long");
+        std::string N = ks.Word(static_cast<uint64_t>(n));
+        ks.Open("for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i + 1 < (int64_t)" + N +
+                "; i += (int64_t)gridDim.x * blockDim.x)");
+        ks.L("const uint32_t ra = " + I + "[i], rb = " + I + "[i + 1];");
+        ks.L("bool eq = true;");
+        for (const auto& sk : op.sort_keys) {
+          const MatCol& mc = m.cols.at(sk->column_idx);
+          std::string D = ks.Ptr(mc.data, "double", true);
+          if (mc.nullable) {
+            std::string NP = ks.Ptr(mc.nulls, "int8_t", true);
+            ks.L("{ const bool na = " + NP + "[ra] != 0, nb = " + NP + "[rb] != 0; eq = eq && na == nb && (na || kdb_dord(" +
+                 D + "[ra]) == kdb_dord(" + D + "[rb])); }");
+          } else {
+            ks.L("eq = eq && kdb_dord(" + D + "[ra]) == kdb_dord(" + D + "[rb]);");
           }
-          return inv + "(" + norm + ")";
-        });
-        ctx_.RadixSortPairs(keys, idx, n, arena_, 64);
+        }
+        ks.L("if (eq) atomicAdd(" + T + ", 1ULL);");
+        ks.Close();
+        LaunchPipeline(ks, n, "order ties");
       }
-      if (mc.nullable) {
-        keygen([&](KernelSource& ks, ExprGen&, const std::string& I) {
-          std::string NP = ks.Ptr(mc.nulls, "int8_t", true);
-          std::string isnull = "(uint64_t)(" + NP + "[" + I + "[i]] != 0)";
-          return asc ? isnull : "(1ULL - " + isnull + ")";
+      if (ReadU64(ties) == 0 && !ctx_.dry) {
+        done = true;
+      } else {
+        keygen([&](KernelSource& ks, ExprGen&, const std::string& I) {  // back to stream order
+          if (stream_rows) ks.L(I + "[i] = " + ks.Ptr(stream_rows, "uint32_t", true) + "[i];");
+          else ks.L(I + "[i] = (uint32_t)i;");
+          return std::string("0ULL");
         });
-        ctx_.RadixSortPairs(keys, idx, n, arena_, 8);
       }
+    }
+    if (!done) {
+      tie_sort();
+      key_sorts();
     }
   } else if (n == 1) {
     ctx_.Memset(idx, 0, sizeof(uint32_t));

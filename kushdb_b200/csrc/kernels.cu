@@ -169,10 +169,15 @@ __device__ __forceinline__ uint32_t BlockExclusive256(uint32_t v, uint32_t* ws) 
 
 // Per digit (one block each): exclusive scan of the digit's per-block counts
 // hist[d][0..nblocks) in place, the digit's total into totals[d].
+// With `zero_next`, also clears the same digit's row of the next pass's
+// counts (which the scatter then fills).
 __global__ void __launch_bounds__(kSortBlock) RadixRowScan(uint32_t* __restrict__ hist, int nblocks,
-                                                           uint32_t* __restrict__ totals) {
+                                                           uint32_t* __restrict__ totals,
+                                                           uint32_t* __restrict__ zero_next) {
   __shared__ uint32_t ws[kSortWarps];
   uint32_t* row = hist + static_cast<int64_t>(blockIdx.x) * nblocks;
+  if (zero_next)
+    for (int i = threadIdx.x; i < nblocks; i += kSortBlock) zero_next[static_cast<int64_t>(blockIdx.x) * nblocks + i] = 0;
   const int per = (nblocks + kSortBlock - 1) / kSortBlock;
   const int b0 = min(static_cast<int>(threadIdx.x) * per, nblocks), e = min(b0 + per, nblocks);
   uint32_t s = 0;
@@ -188,11 +193,13 @@ __global__ void __launch_bounds__(kSortBlock) RadixRowScan(uint32_t* __restrict_
 
 // `offsets` holds each (digit, block) start: global when `totals` is null
 // (one scan over all counts), else relative to the digit, whose start is the
-// exclusive prefix of `totals`.
+// exclusive prefix of `totals`.  With `next_hist`, every element also counts
+// itself in the next pass's per-tile histogram at its destination (the next
+// pass needs no histogram launch).
 __global__ void __launch_bounds__(kSortBlock) RadixScatter(
     const uint64_t* __restrict__ kin, const uint32_t* __restrict__ vin, uint64_t* __restrict__ kout,
     uint32_t* __restrict__ vout, int64_t n, int shift, int tile, const uint32_t* __restrict__ offsets,
-    int nblocks, const uint32_t* __restrict__ totals) {
+    int nblocks, const uint32_t* __restrict__ totals, uint32_t* __restrict__ next_hist, int next_shift) {
   __shared__ uint32_t base[256];
   __shared__ uint32_t total[256];
   __shared__ uint32_t wcnt[kSortWarps][256];
@@ -231,6 +238,8 @@ __global__ void __launch_bounds__(kSortBlock) RadixScatter(
       uint32_t dst = base[digit] + wcnt[warp][digit] + rank;
       kout[dst] = k;
       vout[dst] = v;
+      if (next_hist)
+        atomicAdd(&next_hist[static_cast<int64_t>((k >> next_shift) & 0xff) * nblocks + dst / tile], 1u);
     }
     __syncthreads();
     for (int d = threadIdx.x; d < 256; d += blockDim.x) base[d] += total[d];
@@ -304,6 +313,7 @@ void Context::RadixSortPairs(uint64_t* keys, uint32_t* vals, int64_t n, Arena& a
   uint64_t* k2 = arena.AllocT<uint64_t>(n);
   uint32_t* v2 = arena.AllocT<uint32_t>(n);
   uint32_t* hist = arena.AllocT<uint32_t>(static_cast<size_t>(nblocks) * 256);
+  uint32_t* hist2 = arena.AllocT<uint32_t>(static_cast<size_t>(nblocks) * 256);
   uint32_t* totals = arena.AllocT<uint32_t>(256);
   uint64_t* ka = keys;
   uint32_t* va = vals;
@@ -325,20 +335,34 @@ void Context::RadixSortPairs(uint64_t* keys, uint32_t* vals, int64_t n, Arena& a
       for (int d = 0; d < 256; d++)
         if (h[p * 256 + d] == static_cast<uint64_t>(n)) needed[p] = false;
   }
-  for (int p = 0; p < passes; p++) {
-    if (!needed[p]) continue;
-    const int shift = 8 * p;
+  // Passes: one histogram launch for the first; each scatter counts the
+  // next pass's histogram as it writes.
+  std::vector<int> plist;
+  for (int p = 0; p < passes; p++)
+    if (needed[p]) plist.push_back(p);
+  if (!plist.empty()) {
+    const int shift0 = 8 * plist[0];
     TimedStart("sort histogram");
-    Issue([=](cudaStream_t s) { RadixHistogram<<<nblocks, kSortBlock, 0, s>>>(ka, n, shift, itile, hist, nblocks); });
+    Issue([=](cudaStream_t s) { RadixHistogram<<<nblocks, kSortBlock, 0, s>>>(ka, n, shift0, itile, hist, nblocks); });
     TimedStop();
+  }
+  uint32_t* cur = hist;
+  uint32_t* other = hist2;
+  for (size_t q = 0; q < plist.size(); q++) {
+    const int shift = 8 * plist[q];
+    const bool more = q + 1 < plist.size();
+    const int next_shift = more ? 8 * plist[q + 1] : 0;
+    uint32_t* next = more ? other : nullptr;
     TimedStart("sort scan");
-    Issue([=](cudaStream_t s) { RadixRowScan<<<256, kSortBlock, 0, s>>>(hist, nblocks, totals); });
+    Issue([=](cudaStream_t s) { RadixRowScan<<<256, kSortBlock, 0, s>>>(cur, nblocks, totals, next); });
     TimedStop();
     TimedStart("sort scatter");
     Issue([=](cudaStream_t s) {
-      RadixScatter<<<nblocks, kSortBlock, 0, s>>>(ka, va, kb, vb, n, shift, itile, hist, nblocks, totals);
+      RadixScatter<<<nblocks, kSortBlock, 0, s>>>(ka, va, kb, vb, n, shift, itile, cur, nblocks, totals, next,
+                                                  next_shift);
     });
     TimedStop();
+    std::swap(cur, other);
     std::swap(ka, kb);
     std::swap(va, vb);
   }
@@ -434,7 +458,8 @@ extern "C" int kdb_sort_pairs_noalloc(uint64_t* d_keys, uint32_t* d_vals, int64_
     // shared scratch by an earlier call is read
     RadixHistogram<<<nblocks, kSortBlock, 0, s>>>(ka, n, shift, kSortTile, hist, nblocks);
     ExclusiveScanSmall<<<1, 1024, 0, s>>>(hist, static_cast<int64_t>(nblocks) * 256);
-    RadixScatter<<<nblocks, kSortBlock, 0, s>>>(ka, va, kb, vb, n, shift, kSortTile, hist, nblocks, nullptr);
+    RadixScatter<<<nblocks, kSortBlock, 0, s>>>(ka, va, kb, vb, n, shift, kSortTile, hist, nblocks, nullptr,
+                                                nullptr, 0);
     std::swap(ka, kb);
     std::swap(va, vb);
   }
