@@ -2423,6 +2423,12 @@ MatBuffer Executor::LargeOrderBy(const Operator& op, MatBuffer& m) {
           std::string D = ks.Ptr(mc.data, StoreType(mc.type.id), true);
           return std::make_pair(D + "[" + I + "[i]]", std::string());
         };
+        // NULLs compare equal among themselves: their key is a constant (the
+        // NULL pass below then moves them last), so they keep tie order
+        auto guard = [&](KernelSource& ks, const std::string& I, const std::string& key) {
+          if (!mc.nullable) return key;
+          return "((" + ks.Ptr(mc.nulls, "int8_t", true) + "[" + I + "[i]] != 0) ? 0ULL : (uint64_t)(" + key + "))";
+        };
         if (mc.type.id == TypeId::BOOLEAN) throw Error(-1, "Can't be less than.");
         if (mc.type.id == TypeId::TEXT) {
           // max length over the rows decides the number of 8-byte chunks
@@ -2440,12 +2446,12 @@ MatBuffer Executor::LargeOrderBy(const Operator& op, MatBuffer& m) {
           }
           int64_t maxlen = ReadU64(mx);
           keygen([&](KernelSource& ks, ExprGen& eg, const std::string& I) {
-            return inv + "(uint64_t)" + load(ks, eg, I).first + ".len";
+            return guard(ks, I, inv + "(uint64_t)" + load(ks, eg, I).first + ".len");
           });
           ctx_.RadixSortPairs(keys, idx, n, arena_, 64);
           for (int64_t c = (maxlen + 7) / 8 - 1; c >= 0; c--) {
             keygen([&](KernelSource& ks, ExprGen& eg, const std::string& I) {
-              return inv + "kdb_str_chunk(" + load(ks, eg, I).first + ", " + std::to_string(c) + ")";
+              return guard(ks, I, inv + "kdb_str_chunk(" + load(ks, eg, I).first + ", " + std::to_string(c) + ")");
             });
             ctx_.RadixSortPairs(keys, idx, n, arena_, 64);
           }
@@ -2458,7 +2464,7 @@ MatBuffer Executor::LargeOrderBy(const Operator& op, MatBuffer& m) {
               case TypeId::ENUM: norm = "(uint64_t)(uint32_t)" + eg.EnumRank(mc.type, v); break;
               default: norm = "((uint64_t)(int64_t)" + v + " ^ 0x8000000000000000ULL)"; break;
             }
-            return inv + "(" + norm + ")";
+            return guard(ks, I, inv + "(" + norm + ")");
           });
           ctx_.RadixSortPairs(keys, idx, n, arena_, 64);
         }
