@@ -490,15 +490,10 @@ def main():
         return
 
     import torch
-    rank = int(os.environ.get("RANK", "0"))
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
+    from kushdb_b200 import replicas
+    rank, world, local = replicas.rank_info()
     torch.cuda.set_device(local)
-    dist = None
-    if world > 1:
-        import datetime
-        import torch.distributed as dist
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    dist = replicas.init("nccl", timeout_s=300)
 
     from kushdb_b200.engine import Engine
     scale = 1.0
@@ -531,8 +526,7 @@ def main():
                 flush[1].sum()
 
     # timed region: K steps on the engine stream
-    if dist:
-        dist.barrier()
+    replicas.barrier(dist)
     torch.cuda.synchronize()
     launches0 = eng.kernel_launches()
     step_ms = []
@@ -548,13 +542,9 @@ def main():
             step_ms.append(e0.elapsed_time(e1))
     torch.cuda.synchronize()
     launches = eng.kernel_launches() - launches0
-    total_ms = sum(step_ms)
-    if dist:
-        t = torch.tensor([total_ms], device=f"cuda:{local}")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        total_ms = float(t.item())
-        dist.barrier()
-    value = rows * args.steps * world / (total_ms / 1e3)
+    total_ms = replicas.max_over_ranks(sum(step_ms), dist, f"cuda:{local}")
+    replicas.barrier(dist)
+    value = replicas.whole_job_rate(rows, args.steps, world, total_ms)
 
     # roofline of the dominant kernel: per-launch CUDA events (profiling mode)
     eng.set_profiling(True)
@@ -599,13 +589,13 @@ def main():
             if i > 0:
                 e2e_ms.append(e0.elapsed_time(e1))
             d2h = sum(8 * r.num_rows + r.num_rows for _ in r.columns)
-        e2e = {"value": rows * world / (statistics.median(e2e_ms) / 1e3), "unit": "rows/s",
+        e2e_med = replicas.max_over_ranks(statistics.median(e2e_ms), dist, f"cuda:{local}")
+        e2e = {"value": replicas.whole_job_rate(rows, 1, world, e2e_med), "unit": "rows/s",
                "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
-               "ms_per_step": statistics.median(e2e_ms)}
+               "ms_per_step": e2e_med}
 
     if rank != 0:
-        if dist:
-            dist.destroy_process_group()
+        replicas.finish(dist)
         return
 
     cpu = None
@@ -640,8 +630,7 @@ def main():
         "clocks": clocks.summary(),
     }
     print(json.dumps(line))
-    if dist:
-        dist.destroy_process_group()
+    replicas.finish(dist)
 
 
 if __name__ == "__main__":
