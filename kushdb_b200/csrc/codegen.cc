@@ -647,8 +647,12 @@ class Executor {
   // --- stream emission ---------------------------------------------------
   void EmitStream(KernelSource& ks, ExprGen& eg, const Operator& op, const Consume& consume,
                   int64_t& src_rows);
+  // `ind_array` names an order array already declared in the kernel (e.g.
+  // in shared memory), used instead of `indirection`
   void EmitMatScan(KernelSource& ks, const MatBuffer& m, const uint32_t* indirection,
-                   const Consume& consume, int64_t& src_rows);
+                   const Consume& consume, int64_t& src_rows, const std::string& ind_array = "");
+  MatBuffer EmitOrderedMaterialize(KernelSource& ks, ExprGen& eg, const Operator& op, const uint32_t* order,
+                                   const std::string& ind_array, const MatBuffer& src, int64_t& src_rows);
   std::vector<CVal> LoadMatRow(KernelSource& ks, ExprGen& eg, const MatBuffer& m,
                                const std::string& row, std::vector<std::string>* col_ptrs_cache);
 
@@ -723,11 +727,12 @@ std::vector<CVal> Executor::LoadMatRow(KernelSource& ks, ExprGen& eg, const MatB
 }
 
 void Executor::EmitMatScan(KernelSource& ks, const MatBuffer& m, const uint32_t* indirection,
-                           const Consume& consume, int64_t& src_rows) {
+                           const Consume& consume, int64_t& src_rows, const std::string& ind_array) {
   ExprGen eg(ctx_, ks);
   src_rows = m.rows;
   std::string n = ks.Word(static_cast<uint64_t>(m.rows));
-  std::string ind = indirection ? ks.Ptr(indirection, "uint32_t", true) : "";
+  std::string ind = !ind_array.empty() ? ind_array : indirection ? ks.Ptr(indirection, "uint32_t", true) : "";
+  if (!ind_array.empty()) indirection = reinterpret_cast<const uint32_t*>(1);  // an order is given
   std::string pos = ks.Ptr(m.pos, "uint64_t", true);
   ks.Open("for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < (int64_t)" + n +
           "; r += (int64_t)gridDim.x * blockDim.x)");
@@ -1102,9 +1107,53 @@ void Executor::BuildJoin(const Operator& op) {
 // `ordered_src` is given, project `op.output` over that buffer read in
 // `order`.  Capacity: exact bound for scans; join outputs are counted and the
 // pipeline reruns once at the counted size if the first guess was short.
+// Projection of `op.output` over `src` read in sorted order (row r of the
+// result is src row order[r]), emitted into `ks`; returns the output buffer.
+MatBuffer Executor::EmitOrderedMaterialize(KernelSource& ks, ExprGen& eg, const Operator& op, const uint32_t* order,
+                                           const std::string& ind_array, const MatBuffer& src, int64_t& src_rows) {
+  const auto& schema = op.output;
+  MatBuffer out = AllocMat(schema, src.rows);
+  std::vector<std::string> optr, onull;
+  for (const auto& c : out.cols) {
+    optr.push_back(ks.Ptr(c.data, StoreType(c.type.id)));
+    onull.push_back(c.nullable ? ks.Ptr(c.nulls, "int8_t") : "");
+  }
+  std::string posp = ks.Ptr(out.pos, "uint64_t");
+  auto body = [&](const std::vector<CVal>& in, const std::string& pos) {
+    Scope s;
+    s.child.push_back(in);
+    std::vector<CVal> vals;
+    for (const auto& c : schema) vals.push_back(eg.Emit(*c.expr, s));
+    ks.Open("");
+    ks.L("const uint64_t slot = (uint64_t)r;");
+    for (size_t c = 0; c < vals.size(); c++) {
+      const CVal& v = vals[c];
+      std::string val = v.type.id == TypeId::BOOLEAN ? "(int8_t)(" + v.v + " ? 1 : 0)" : v.v;
+      ks.L(optr[c] + "[slot] = " + val + ";");
+      if (!onull[c].empty()) ks.L(onull[c] + "[slot] = (" + v.n + ") ? 1 : 0;");
+    }
+    ks.L(posp + "[slot] = " + pos + ";");
+    ks.Close();
+  };
+  EmitMatScan(ks, src, order, body, src_rows, ind_array);
+  out.rows = src.rows;
+  out.pos_is_index = true;
+  return out;
+}
+
 MatBuffer Executor::MaterializeStream(const Operator& op, const uint32_t* order,
                                       const MatBuffer* ordered_src) {
-  if (!ordered_src) Prepare(op);
+  if (ordered_src) {
+    // every row r is written at index r: the count is known without a
+    // read-back (device errors surface at the next synchronisation)
+    KernelSource ks;
+    ExprGen eg(ctx_, ks);
+    int64_t src_rows = 0;
+    MatBuffer out = EmitOrderedMaterialize(ks, eg, op, order, "", *ordered_src, src_rows);
+    LaunchPipeline(ks, src_rows, "materialize");
+    return out;
+  }
+  Prepare(op);
   int64_t cap = ordered_src ? ordered_src->rows : RowBound(op);
   for (int attempt = 0; attempt < 3; attempt++) {
     const auto mark = ctx_.RecordMark();
@@ -2358,14 +2407,20 @@ MatBuffer Executor::SmallOrderBy(const Operator& op, MatBuffer& m) {
     }
     less += "    return kdb_tie_path(sidx[ra], " + N + ") < kdb_tie_path(sidx[rb], " + N + ");\n  };";
     ks.L(less);
+    ks.L("__shared__ uint32_t sord[" + std::to_string(kSmallOrder) + "];");
     ks.Open("for (int64_t i = threadIdx.x; i < " + N + "; i += blockDim.x)");
     ks.L("uint32_t r = 0;");
     ks.L("for (int64_t j = 0; j < " + N + "; j++) r += (j != i) && less(j, i);");
-    ks.L(I + "[r] = (uint32_t)i;");
+    ks.L("sord[r] = (uint32_t)i;");
     ks.Close();
+    ks.L("__syncthreads();");
+    // the ORDER BY output, projected in the same block
+    int64_t src_rows = 0;
+    MatBuffer out = EmitOrderedMaterialize(ks, eg, op, nullptr, "sord", m, src_rows);
     std::string src = ks.Kernel("kdb_order_by_small", 1024);
     CUfunction f = ctx_.Kernel(src, "kdb_order_by_small");
     ctx_.Launch(f, 1, 1024, ks.Args(), 0, "order by small");
+    return out;
   }
   return MaterializeStream(op, idx, &m);
 }
@@ -3443,16 +3498,42 @@ HostResult Executor::Download(const MatBuffer& m, const Operator& root, bool che
   const size_t err_off = total;
   char* stage = static_cast<char*>(ctx_.HostStage(total + 16));
   if (!ctx_.dry && (m.rows > 0 || check_error)) {
+    // several small segments: gather on the device, one copy to the host
+    PackSegs segs;
+    auto add = [&](const void* src, size_t bytes, size_t off) {
+      if (segs.n < kMaxPackSegs) segs.seg[segs.n] = PackSeg{static_cast<const char*>(src), bytes, off};
+      segs.n++;
+    };
     if (m.rows > 0)
       for (size_t c = 0; c < m.cols.size(); c++) {
         const MatCol& mc = m.cols[c];
-        KDB_CUDA(cudaMemcpyAsync(stage + data_off[c], mc.data, StoreWidth(mc.type.id) * m.rows,
-                                 cudaMemcpyDeviceToHost, ctx_.stream));
-        if (mc.nulls)
-          KDB_CUDA(cudaMemcpyAsync(stage + null_off[c], mc.nulls, m.rows, cudaMemcpyDeviceToHost, ctx_.stream));
+        add(mc.data, StoreWidth(mc.type.id) * m.rows, data_off[c]);
+        if (mc.nulls) add(mc.nulls, m.rows, null_off[c]);
       }
-    if (check_error)
-      KDB_CUDA(cudaMemcpyAsync(stage + err_off, ctx_.d_err, 16, cudaMemcpyDeviceToHost, ctx_.stream));
+    if (check_error) add(ctx_.d_err, 16, err_off);
+    if (segs.n > 2 && segs.n <= kMaxPackSegs && total + 16 <= (size_t(64) << 20)) {
+      ctx_.PackToHost(segs, err_off + (check_error ? 16 : 0), stage);
+    } else {
+      for (int i = 0; i < std::min(segs.n, kMaxPackSegs); i++)
+        KDB_CUDA(cudaMemcpyAsync(stage + segs.seg[i].off, segs.seg[i].src, segs.seg[i].bytes, cudaMemcpyDeviceToHost,
+                                 ctx_.stream));
+      if (segs.n > kMaxPackSegs) {  // wide results: the remaining segments one by one
+        int i = 0;
+        for (size_t c = 0; c < m.cols.size() && m.rows > 0; c++) {
+          const MatCol& mc = m.cols[c];
+          for (int part = 0; part < (mc.nulls ? 2 : 1); part++, i++) {
+            if (i < kMaxPackSegs) continue;
+            if (part == 0)
+              KDB_CUDA(cudaMemcpyAsync(stage + data_off[c], mc.data, StoreWidth(mc.type.id) * m.rows,
+                                       cudaMemcpyDeviceToHost, ctx_.stream));
+            else
+              KDB_CUDA(cudaMemcpyAsync(stage + null_off[c], mc.nulls, m.rows, cudaMemcpyDeviceToHost, ctx_.stream));
+          }
+        }
+        if (check_error && i >= kMaxPackSegs)
+          KDB_CUDA(cudaMemcpyAsync(stage + err_off, ctx_.d_err, 16, cudaMemcpyDeviceToHost, ctx_.stream));
+      }
+    }
     KDB_CUDA(cudaStreamSynchronize(ctx_.stream));
     if (check_error) {
       int err[4];

@@ -183,6 +183,7 @@ Context::~Context() {
   }
   if (stage_) cudaFreeHost(stage_);
   cudaSetDevice(device);
+  if (dev_stage_) cudaFreeAsync(dev_stage_, stream);
   cudaStreamSynchronize(stream);
   if (owns_catalog_) {
     for (auto& [n, t] : tables)

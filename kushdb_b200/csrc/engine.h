@@ -108,6 +108,18 @@ struct KArgs {
 class Context;
 class JoinPrior;
 
+// Segments gathered into one buffer for a single device-to-host copy.
+constexpr int kMaxPackSegs = 32;
+struct PackSeg {
+  const char* src;
+  uint64_t bytes;
+  uint64_t off;
+};
+struct PackSegs {
+  PackSeg seg[kMaxPackSegs];
+  int n = 0;
+};
+
 // The device work of one query execution, kept to be replayed as a CUDA
 // graph when the same plan runs again over unchanged tables.
 struct Recorder {
@@ -246,6 +258,9 @@ class Context {
   void RadixSortPairs(uint64_t* keys, uint32_t* vals, int64_t n, Arena& arena, int key_bits = 64);
   // exclusive prefix sum of a[0..n) in place, the total into a[n]
   void ScanU64(uint64_t* a, int64_t n);
+  // gathers the segments into the device staging buffer and queues one copy
+  // of `total` bytes to `host` (pinned); the caller synchronises
+  void PackToHost(const PackSegs& segs, size_t total, void* host);
   void CheckDeviceError(const char* what);
 
   EnumDicts HostEnums() const;
@@ -255,6 +270,8 @@ class Context {
   bool owns_catalog_ = true;
   void* stage_ = nullptr;
   size_t stage_bytes_ = 0;
+  void* dev_stage_ = nullptr;  // device side of PackToHost
+  size_t dev_stage_bytes_ = 0;
   void FreeColumn(DevColumn& c);
 };
 

@@ -272,6 +272,23 @@ __global__ void __launch_bounds__(1024) SmallRankSort(uint64_t* __restrict__ key
   }
 }
 
+// Result download: copies up to kMaxPackSegs device segments into one
+// contiguous staging buffer (16-byte aligned offsets), so the host reads the
+// whole result with a single copy instead of one per column.
+__global__ void PackSegments(PackSegs a, char* __restrict__ dst) {
+  const PackSeg& g = a.seg[blockIdx.y];
+  const uint64_t nvec = g.bytes / 16;
+  const bool aligned = (reinterpret_cast<uintptr_t>(g.src) & 15) == 0;
+  for (uint64_t i = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x; i * 16 < g.bytes;
+       i += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
+    if (aligned && i < nvec) {
+      reinterpret_cast<uint4*>(dst + g.off)[i] = reinterpret_cast<const uint4*>(g.src)[i];
+    } else {
+      for (uint64_t b = i * 16; b < g.bytes && b < i * 16 + 16; b++) dst[g.off + b] = g.src[b];
+    }
+  }
+}
+
 __global__ void CopyPairs(const uint64_t* __restrict__ ks, const uint32_t* __restrict__ vs,
                           uint64_t* __restrict__ kd, uint32_t* __restrict__ vd, int64_t n) {
   for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < n;
@@ -282,6 +299,23 @@ __global__ void CopyPairs(const uint64_t* __restrict__ ks, const uint32_t* __res
 }
 
 }  // namespace
+
+void Context::PackToHost(const PackSegs& segs, size_t total, void* host) {
+  if (dry || segs.n == 0) return;
+  if (total > dev_stage_bytes_) {
+    if (dev_stage_) cudaFreeAsync(dev_stage_, stream);
+    dev_stage_bytes_ = std::max<size_t>(total, 1 << 20);
+    KDB_CUDA(cudaMallocAsync(&dev_stage_, dev_stage_bytes_, stream));
+  }
+  uint64_t most = 0;
+  for (int i = 0; i < segs.n; i++) most = std::max<uint64_t>(most, segs.seg[i].bytes);
+  const int gx = static_cast<int>(std::max<uint64_t>(1, std::min<uint64_t>((most / 16 + 255) / 256, 64)));
+  char* dst = static_cast<char*>(dev_stage_);
+  PackSegments<<<dim3(gx, segs.n), 256, 0, stream>>>(segs, dst);
+  kernel_launches++;
+  KDB_CUDA(cudaGetLastError());
+  KDB_CUDA(cudaMemcpyAsync(host, dst, total, cudaMemcpyDeviceToHost, stream));
+}
 
 void Context::ScanU64(uint64_t* a, int64_t n) {
   if (dry) return;
