@@ -647,12 +647,10 @@ class Executor {
   // --- stream emission ---------------------------------------------------
   void EmitStream(KernelSource& ks, ExprGen& eg, const Operator& op, const Consume& consume,
                   int64_t& src_rows);
-  // `ind_array` names an order array already declared in the kernel (e.g.
-  // in shared memory), used instead of `indirection`
   void EmitMatScan(KernelSource& ks, const MatBuffer& m, const uint32_t* indirection,
-                   const Consume& consume, int64_t& src_rows, const std::string& ind_array = "");
+                   const Consume& consume, int64_t& src_rows);
   MatBuffer EmitOrderedMaterialize(KernelSource& ks, ExprGen& eg, const Operator& op, const uint32_t* order,
-                                   const std::string& ind_array, const MatBuffer& src, int64_t& src_rows);
+                                   const MatBuffer& src, int64_t& src_rows);
   std::vector<CVal> LoadMatRow(KernelSource& ks, ExprGen& eg, const MatBuffer& m,
                                const std::string& row, std::vector<std::string>* col_ptrs_cache);
 
@@ -727,12 +725,11 @@ std::vector<CVal> Executor::LoadMatRow(KernelSource& ks, ExprGen& eg, const MatB
 }
 
 void Executor::EmitMatScan(KernelSource& ks, const MatBuffer& m, const uint32_t* indirection,
-                           const Consume& consume, int64_t& src_rows, const std::string& ind_array) {
+                           const Consume& consume, int64_t& src_rows) {
   ExprGen eg(ctx_, ks);
   src_rows = m.rows;
   std::string n = ks.Word(static_cast<uint64_t>(m.rows));
-  std::string ind = !ind_array.empty() ? ind_array : indirection ? ks.Ptr(indirection, "uint32_t", true) : "";
-  if (!ind_array.empty()) indirection = reinterpret_cast<const uint32_t*>(1);  // an order is given
+  std::string ind = indirection ? ks.Ptr(indirection, "uint32_t", true) : "";
   std::string pos = ks.Ptr(m.pos, "uint64_t", true);
   ks.Open("for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < (int64_t)" + n +
           "; r += (int64_t)gridDim.x * blockDim.x)");
@@ -1110,7 +1107,7 @@ void Executor::BuildJoin(const Operator& op) {
 // Projection of `op.output` over `src` read in sorted order (row r of the
 // result is src row order[r]), emitted into `ks`; returns the output buffer.
 MatBuffer Executor::EmitOrderedMaterialize(KernelSource& ks, ExprGen& eg, const Operator& op, const uint32_t* order,
-                                           const std::string& ind_array, const MatBuffer& src, int64_t& src_rows) {
+                                           const MatBuffer& src, int64_t& src_rows) {
   const auto& schema = op.output;
   MatBuffer out = AllocMat(schema, src.rows);
   std::vector<std::string> optr, onull;
@@ -1135,7 +1132,7 @@ MatBuffer Executor::EmitOrderedMaterialize(KernelSource& ks, ExprGen& eg, const 
     ks.L(posp + "[slot] = " + pos + ";");
     ks.Close();
   };
-  EmitMatScan(ks, src, order, body, src_rows, ind_array);
+  EmitMatScan(ks, src, order, body, src_rows);
   out.rows = src.rows;
   out.pos_is_index = true;
   return out;
@@ -1149,12 +1146,12 @@ MatBuffer Executor::MaterializeStream(const Operator& op, const uint32_t* order,
     KernelSource ks;
     ExprGen eg(ctx_, ks);
     int64_t src_rows = 0;
-    MatBuffer out = EmitOrderedMaterialize(ks, eg, op, order, "", *ordered_src, src_rows);
+    MatBuffer out = EmitOrderedMaterialize(ks, eg, op, order, *ordered_src, src_rows);
     LaunchPipeline(ks, src_rows, "materialize");
     return out;
   }
   Prepare(op);
-  int64_t cap = ordered_src ? ordered_src->rows : RowBound(op);
+  int64_t cap = RowBound(op);
   for (int attempt = 0; attempt < 3; attempt++) {
     const auto mark = ctx_.RecordMark();
     KernelSource ks;
@@ -1173,10 +1170,8 @@ MatBuffer Executor::MaterializeStream(const Operator& op, const uint32_t* order,
     std::string capw = "(uint64_t)" + ks.Word(static_cast<uint64_t>(out.cap));
     auto sink = [&](const std::vector<CVal>& vals, const std::string& pos) {
       ks.Open("");
-      // an ordered source (ORDER BY output) writes row r at index r; other
-      // streams append through the warp-aggregated counter
-      if (ordered_src) ks.L("uint64_t slot = (uint64_t)r; if (r == 0) *(unsigned long long*)" + cnt + " = " + capw + ";");
-      else ks.L("uint64_t slot = kdb_alloc_slot((unsigned long long*)" + cnt + ");");
+      // rows append through the warp-aggregated counter
+      ks.L("uint64_t slot = kdb_alloc_slot((unsigned long long*)" + cnt + ");");
       ks.Open("if (slot < " + capw + ")");
       for (size_t c = 0; c < vals.size(); c++) {
         const CVal& v = vals[c];
@@ -1189,33 +1184,14 @@ MatBuffer Executor::MaterializeStream(const Operator& op, const uint32_t* order,
       ks.Close();
     };
     int64_t src_rows = 0;
-    if (ordered_src) {
-      auto body = [&](const std::vector<CVal>& in, const std::string& pos) {
-        Scope s;
-        s.child.push_back(in);
-        std::vector<CVal> vals;
-        for (const auto& c : schema) vals.push_back(eg.Emit(*c.expr, s));
-        sink(vals, pos);
-      };
-      EmitMatScan(ks, *ordered_src, order, body, src_rows);
-    } else {
-      EmitStream(ks, eg, op, sink, src_rows);
-    }
+    EmitStream(ks, eg, op, sink, src_rows);
     LaunchPipeline(ks, src_rows, "materialize");
-    if (ordered_src) {
-      // every row r is written at index r: the count is known without a
-      // read-back (device errors surface at the next synchronisation)
-      out.rows = ordered_src->rows;
-      out.pos_is_index = true;
-      return out;
-    }
     int64_t produced = ReadU64(counter);
     ctx_.CheckDeviceError("materialize");
     if (produced <= out.cap) {
       out.rows = produced;
       return out;
     }
-    if (ordered_src) throw Error(-4, "ordered materialisation overflow");
     cap = produced;
     ctx_.RecordTruncate(mark);
   }
@@ -2407,20 +2383,14 @@ MatBuffer Executor::SmallOrderBy(const Operator& op, MatBuffer& m) {
     }
     less += "    return kdb_tie_path(sidx[ra], " + N + ") < kdb_tie_path(sidx[rb], " + N + ");\n  };";
     ks.L(less);
-    ks.L("__shared__ uint32_t sord[" + std::to_string(kSmallOrder) + "];");
     ks.Open("for (int64_t i = threadIdx.x; i < " + N + "; i += blockDim.x)");
     ks.L("uint32_t r = 0;");
     ks.L("for (int64_t j = 0; j < " + N + "; j++) r += (j != i) && less(j, i);");
-    ks.L("sord[r] = (uint32_t)i;");
+    ks.L(I + "[r] = (uint32_t)i;");
     ks.Close();
-    ks.L("__syncthreads();");
-    // the ORDER BY output, projected in the same block
-    int64_t src_rows = 0;
-    MatBuffer out = EmitOrderedMaterialize(ks, eg, op, nullptr, "sord", m, src_rows);
     std::string src = ks.Kernel("kdb_order_by_small", 1024);
     CUfunction f = ctx_.Kernel(src, "kdb_order_by_small");
     ctx_.Launch(f, 1, 1024, ks.Args(), 0, "order by small");
-    return out;
   }
   return MaterializeStream(op, idx, &m);
 }
