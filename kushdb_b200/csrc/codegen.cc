@@ -2430,6 +2430,64 @@ MatBuffer Executor::LargeOrderBy(const Operator& op, MatBuffer& m) {
     // the tie key uses at most depth = ceil(log2 n) + 1 leading bits
     int depth = 1;
     while ((1LL << (depth - 1)) < n) depth++;
+    // One numeric non-NULL key: (key, tie rank) pairs are unique, so a block
+    // sort plus merge-path passes over 16-byte items orders them in a few
+    // launches (the radix path needs two launches per 8-bit digit).
+    if (op.sort_keys.size() == 1 && depth <= 32 && !std::getenv("KDB_ORDER_RADIX")) {
+      const MatCol& mc = m.cols.at(op.sort_keys[0]->column_idx);
+      const TypeId t = mc.type.id;
+      // a nullable key folds its NULL flag in as the most significant bit:
+      // the key's low bit moves to the top of the tie word, which then holds
+      // the tie rank in 31 bits
+      if (t != TypeId::TEXT && t != TypeId::BOOLEAN && (!mc.nullable || depth <= 31)) {
+        uint64_t* items = arena_.AllocT<uint64_t>(2 * n);
+        {
+          KernelSource ks;
+          ExprGen eg(ctx_, ks);
+          std::string IT = ks.Ptr(items, "uint64_t"), I = ks.Ptr(idx, "uint32_t", true);
+          std::string D = ks.Ptr(mc.data, StoreType(t), true);
+          std::string N = ks.Word(static_cast<uint64_t>(n));
+          ks.Open("for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < (int64_t)" + N +
+                  "; i += (int64_t)gridDim.x * blockDim.x)");
+          ks.L(std::string("const uint32_t row = ") + (m.pos_is_index ? "(uint32_t)i" : I + "[i]") + ";");
+          std::string v = D + "[row]", norm;
+          switch (t) {
+            case TypeId::REAL: norm = "kdb_dord(" + v + ")"; break;
+            case TypeId::ENUM: norm = "(uint64_t)(uint32_t)" + eg.EnumRank(mc.type, v); break;
+            default: norm = "((uint64_t)(int64_t)" + v + " ^ 0x8000000000000000ULL)"; break;
+          }
+          const std::string tie = "(kdb_tie_path((uint64_t)i, " + std::to_string(n) + "ULL) >> " +
+                                  std::to_string(64 - depth) + ")";
+          if (!mc.nullable) {
+            ks.L(IT + "[2 * i] = " + (op.asc[0] ? "" : "~") + "(" + norm + ");");
+            ks.L(IT + "[2 * i + 1] = " + tie + " | ((uint64_t)row << 32);");
+          } else {
+            // NULLs sort after every value ascending, before them descending
+            // (proxy::LessThan), and tie among themselves
+            std::string NP = ks.Ptr(mc.nulls, "int8_t", true);
+            ks.L("const bool isnull = " + NP + "[row] != 0;");
+            ks.L("const uint64_t k = isnull ? 0ULL : " + std::string(op.asc[0] ? "" : "~") + "(" + norm + ");");
+            ks.L(std::string("const uint64_t flag = ") + (op.asc[0] ? "isnull" : "!isnull") + " ? 1ULL : 0ULL;");
+            ks.L(IT + "[2 * i] = (flag << 63) | (k >> 1);");
+            ks.L(IT + "[2 * i + 1] = ((k & 1ULL) << 31) | " + tie + " | ((uint64_t)row << 32);");
+          }
+          ks.Close();
+          LaunchPipeline(ks, n, "order key");
+        }
+        ctx_.MergeSortItems(items, n, arena_);
+        {
+          KernelSource ks;
+          std::string IT = ks.Ptr(items, "uint64_t", true), I = ks.Ptr(idx, "uint32_t");
+          std::string N = ks.Word(static_cast<uint64_t>(n));
+          ks.Open("for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < (int64_t)" + N +
+                  "; i += (int64_t)gridDim.x * blockDim.x)");
+          ks.L(I + "[i] = (uint32_t)(" + IT + "[2 * i + 1] >> 32);");
+          ks.Close();
+          LaunchPipeline(ks, n, "order rows");
+        }
+        return MaterializeStream(op, idx, &m);
+      }
+    }
     auto tie_sort = [&]() {
       keygen([&](KernelSource&, ExprGen&, const std::string&) {
         return "(kdb_tie_path((uint64_t)i, " + std::to_string(n) + "ULL) >> " + std::to_string(64 - depth) + ")";
@@ -3560,14 +3618,20 @@ HostResult Executor::Download(const MatBuffer& m, const Operator& root, bool che
       }
       default: {
         hc.i.resize(m.rows);
-        for (int64_t r = 0; r < m.rows; r++) {
-          const char* p = raw + w * r;
-          switch (mc.type.id) {
-            case TypeId::BOOLEAN: hc.i[r] = *reinterpret_cast<const int8_t*>(p); break;
-            case TypeId::SMALLINT: hc.i[r] = *reinterpret_cast<const int16_t*>(p); break;
-            case TypeId::BIGINT: hc.i[r] = *reinterpret_cast<const int64_t*>(p); break;
-            default: hc.i[r] = *reinterpret_cast<const int32_t*>(p); break;
-          }
+        (void)w;
+        auto widen = [&](auto tag) {  // one tight loop per stored width
+          using T = decltype(tag);
+          std::vector<T> tmp(m.rows);
+          if (m.rows) std::memcpy(tmp.data(), raw, sizeof(T) * m.rows);
+          for (int64_t r = 0; r < m.rows; r++) hc.i[r] = tmp[r];
+        };
+        switch (mc.type.id) {
+          case TypeId::BOOLEAN: widen(int8_t{}); break;
+          case TypeId::SMALLINT: widen(int16_t{}); break;
+          case TypeId::BIGINT:
+            if (m.rows) std::memcpy(hc.i.data(), raw, sizeof(int64_t) * m.rows);
+            break;
+          default: widen(int32_t{}); break;
         }
         break;
       }

@@ -256,6 +256,9 @@ class Context {
 
   // Static kernels (kernels.cu).
   void RadixSortPairs(uint64_t* keys, uint32_t* vals, int64_t n, Arena& arena, int key_bits = 64);
+  // sorts n 16-byte items {uint64 key, uint32 tie, uint32 value} by
+  // (key, tie), which must be unique (block sort + merge-path passes)
+  void MergeSortItems(void* items, int64_t n, Arena& arena);
   // exclusive prefix sum of a[0..n) in place, the total into a[n]
   void ScanU64(uint64_t* a, int64_t n);
   // gathers the segments into the device staging buffer and queues one copy

@@ -289,6 +289,85 @@ __global__ void PackSegments(PackSegs a, char* __restrict__ dst) {
   }
 }
 
+// ---- merge sort of unique (key, tie) pairs ---------------------------------
+// ORDER BY on one numeric key: the key and the reference merge sort's tie
+// rank together are unique, so any correct sort gives the reference order;
+// for mid-size inputs a block sort plus log2(n / tile) merge-path passes
+// take far fewer launches than 8-bit radix passes.
+struct SortItem {
+  uint64_t key;
+  uint32_t tie;
+  uint32_t val;
+};
+static_assert(sizeof(SortItem) == 16, "SortItem layout");
+
+__device__ __forceinline__ bool ItemLess(const SortItem& a, const SortItem& b) {
+  return a.key < b.key || (a.key == b.key && a.tie < b.tie);
+}
+
+constexpr int kMergeTile = 2048;  // items per block sort
+constexpr int kMergeItems = 8;    // outputs per thread per merge pass
+
+// Bitonic sort of each tile of kMergeTile items in shared memory (padding
+// with maximal items).
+__global__ void __launch_bounds__(1024) BlockSortItems(SortItem* __restrict__ items, int64_t n) {
+  __shared__ SortItem t[kMergeTile];
+  const int64_t base = static_cast<int64_t>(blockIdx.x) * kMergeTile;
+  for (int i = threadIdx.x; i < kMergeTile; i += blockDim.x)
+    t[i] = base + i < n ? items[base + i] : SortItem{~0ULL, ~0u, ~0u};
+  __syncthreads();
+  for (int size = 2; size <= kMergeTile; size <<= 1)
+    for (int stride = size >> 1; stride > 0; stride >>= 1) {
+      for (int i = threadIdx.x; i < kMergeTile / 2; i += blockDim.x) {
+        const int lo = 2 * i - (i & (stride - 1));
+        const int hi = lo + stride;
+        const bool up = (lo & size) == 0;
+        const SortItem a = t[lo], b = t[hi];
+        if (ItemLess(b, a) == up) {
+          t[lo] = b;
+          t[hi] = a;
+        }
+      }
+      __syncthreads();
+    }
+  for (int i = threadIdx.x; i < kMergeTile; i += blockDim.x)
+    if (base + i < n) items[base + i] = t[i];
+}
+
+// One merge pass: sorted runs of `w` items merge pairwise into runs of 2w;
+// each thread finds its output diagonal by binary search (merge path) and
+// writes kMergeItems outputs.
+__global__ void __launch_bounds__(256) MergeItems(const SortItem* __restrict__ in, SortItem* __restrict__ out,
+                                                  int64_t n, int64_t w) {
+  const int64_t o = (blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x) * kMergeItems;
+  if (o >= n) return;
+  const int64_t base = o / (2 * w) * (2 * w);
+  const int64_t a_len = min(w, n - base);
+  const int64_t b0 = base + w;
+  const int64_t b_len = b0 < n ? min(w, n - b0) : 0;
+  const SortItem* A = in + base;
+  const SortItem* B = in + b0;
+  const int64_t diag = o - base;
+  int64_t lo = diag - b_len > 0 ? diag - b_len : 0, hi = diag < a_len ? diag : a_len;
+  while (lo < hi) {  // first i with A[i] > B[diag - i - 1]
+    const int64_t mid = (lo + hi) >> 1;
+    if (ItemLess(B[diag - mid - 1], A[mid])) hi = mid;
+    else lo = mid + 1;
+  }
+  int64_t i = lo, j = diag - lo;
+  const int64_t end = min(o + static_cast<int64_t>(kMergeItems), base + a_len + b_len);
+  for (int64_t k = o; k < end; k++) {
+    const bool take_a = j >= b_len || (i < a_len && ItemLess(A[i], B[j]));
+    out[k] = take_a ? A[i++] : B[j++];
+  }
+}
+
+__global__ void CopyItems(const SortItem* __restrict__ src, SortItem* __restrict__ dst, int64_t n) {
+  for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < n;
+       i += static_cast<int64_t>(gridDim.x) * blockDim.x)
+    dst[i] = src[i];
+}
+
 __global__ void CopyPairs(const uint64_t* __restrict__ ks, const uint32_t* __restrict__ vs,
                           uint64_t* __restrict__ kd, uint32_t* __restrict__ vd, int64_t n) {
   for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < n;
@@ -315,6 +394,32 @@ void Context::PackToHost(const PackSegs& segs, size_t total, void* host) {
   kernel_launches++;
   KDB_CUDA(cudaGetLastError());
   KDB_CUDA(cudaMemcpyAsync(host, dst, total, cudaMemcpyDeviceToHost, stream));
+}
+
+void Context::MergeSortItems(void* items, int64_t n, Arena& arena) {
+  if (n <= 1 || dry) return;
+  SortItem* a = static_cast<SortItem*>(items);
+  SortItem* b = reinterpret_cast<SortItem*>(arena.Alloc(sizeof(SortItem) * n));
+  const int tiles = static_cast<int>((n + kMergeTile - 1) / kMergeTile);
+  TimedStart("sort block");
+  Issue([=](cudaStream_t s) { BlockSortItems<<<tiles, 1024, 0, s>>>(a, n); });
+  TimedStop();
+  for (int64_t w = kMergeTile; w < n; w <<= 1) {
+    const int grid = static_cast<int>(((n + kMergeItems - 1) / kMergeItems + 255) / 256);
+    TimedStart("sort merge");
+    Issue([=](cudaStream_t s) { MergeItems<<<grid, 256, 0, s>>>(a, b, n, w); });
+    TimedStop();
+    std::swap(a, b);
+  }
+  if (a != items) {
+    const int grid = GridFor(n, 256);
+    SortItem* dst = static_cast<SortItem*>(items);
+    const SortItem* src = a;
+    TimedStart("sort copy");
+    Issue([=](cudaStream_t s) { CopyItems<<<grid, 256, 0, s>>>(src, dst, n); });
+    TimedStop();
+  }
+  KDB_CUDA(cudaGetLastError());
 }
 
 void Context::ScanU64(uint64_t* a, int64_t n) {

@@ -1,6 +1,7 @@
-"""ORDER BY above the one-block size (radix path) against the oracle's merge
-sort, line by line: float keys with and without ties (ties must come out in
-the reference merge sort's order), NULLs, descending, and a second key."""
+"""ORDER BY above the one-block size against the oracle's merge sort, line
+by line: single numeric keys (block sort + merge path), NULLs and several
+keys (radix passes); float and integer keys with and without ties (ties must
+come out in the reference merge sort's order), ascending and descending."""
 
 import numpy as np
 import pytest
@@ -25,6 +26,7 @@ def setup():
     t.add(HostColumn("tied_r", Type.Real(), values=rng.integers(0, 50, N).astype(np.float64) / 4.0))
     nulls = (rng.random(N) < 0.1).astype(np.int8)
     t.add(HostColumn("null_r", Type.Real(), values=rng.integers(0, 20, N).astype(np.float64), nulls=nulls))
+    t.add(HostColumn("tied_i", Type.Int(), values=rng.integers(-5, 5, N).astype(np.int32)))
     e = Engine(0)
     e.register_table(t)
     o = Oracle()
@@ -36,7 +38,7 @@ def setup():
 def _plan(t, keys, asc):
     rel = catalog_of([t])[t.name]
     s = OperatorSchema()
-    s.AddGeneratedColumns(rel, ["id", "distinct_r", "tied_r", "null_r"])
+    s.AddGeneratedColumns(rel, ["id", "distinct_r", "tied_r", "null_r", "tied_i"])
     base = ScanOperator(s, rel)
     out = OperatorSchema()
     out.AddPassthroughColumns(base)
@@ -46,7 +48,8 @@ def _plan(t, keys, asc):
 @pytest.mark.parametrize("keys,asc", [(["distinct_r"], [True]), (["distinct_r"], [False]),
                                       (["tied_r"], [True]), (["tied_r"], [False]),
                                       (["null_r"], [True]), (["null_r"], [False]),
-                                      (["tied_r", "null_r"], [False, True])])
+                                      (["tied_r", "null_r"], [False, True]),
+                                      (["tied_i"], [True]), (["tied_i"], [False]), (["id"], [False])])
 def test_order_matches_reference_merge_sort(setup, keys, asc):
     e, o, t = setup
     plan = _plan(t, keys, asc).to_json()
