@@ -295,24 +295,17 @@ int kdb_result_col_type(const kdb_result* r, int32_t col, char* buf, int32_t cap
 
 int kdb_result_get_i64(const kdb_result* r, int32_t col, int64_t* out) {
   if (!r || col < 0 || col >= static_cast<int32_t>(r->r.cols.size())) return KDB_ERR_INVALID;
-  const auto& c = r->r.cols[col];
-  if (c.i.size() != static_cast<size_t>(r->r.rows)) return KDB_ERR_INVALID;
-  std::memcpy(out, c.i.data(), sizeof(int64_t) * c.i.size());
-  return KDB_OK;
+  return r->r.cols[col].CopyInts(r->r.rows, out) ? KDB_OK : KDB_ERR_INVALID;
 }
 
 int kdb_result_get_f64(const kdb_result* r, int32_t col, double* out) {
   if (!r || col < 0 || col >= static_cast<int32_t>(r->r.cols.size())) return KDB_ERR_INVALID;
-  const auto& c = r->r.cols[col];
-  if (c.f.size() != static_cast<size_t>(r->r.rows)) return KDB_ERR_INVALID;
-  std::memcpy(out, c.f.data(), sizeof(double) * c.f.size());
-  return KDB_OK;
+  return r->r.cols[col].CopyReals(r->r.rows, out) ? KDB_OK : KDB_ERR_INVALID;
 }
 
 int kdb_result_get_nulls(const kdb_result* r, int32_t col, int8_t* out) {
   if (!r || col < 0 || col >= static_cast<int32_t>(r->r.cols.size())) return KDB_ERR_INVALID;
-  const auto& c = r->r.cols[col];
-  std::memcpy(out, c.null.data(), c.null.size());
+  r->r.cols[col].CopyNulls(r->r.rows, out);
   return KDB_OK;
 }
 

@@ -658,8 +658,16 @@ class Executor {
   MatBuffer Materialize(const Operator& op);
   MatBuffer MaterializeStream(const Operator& op, const uint32_t* order = nullptr,
                               const MatBuffer* ordered_src = nullptr);
+  MatBuffer MaterializeCounted(const Operator& op);
+  static bool StreamHasJoin(const Operator& op) {
+    if (op.kind == OpKind::HASH_JOIN) return true;
+    return op.kind == OpKind::SELECT && Streamable(op.child()) && StreamHasJoin(op.child());
+  }
   MatBuffer RunAggregate(const Operator& op);
-  MatBuffer RunGroupBy(const Operator& op);
+  // any_order: the consumer (an ORDER BY) orders the rows itself, so the
+  // groups may come out in any order with their first-appearance key as the
+  // stream position (pos_is_index false) instead of being sorted by it
+  MatBuffer RunGroupBy(const Operator& op, bool any_order = false);
   MatBuffer RunOrderBy(const Operator& op);
   MatBuffer RunSkinner(const Operator& op, const SkinnerAgg* agg = nullptr);
   MatBuffer SmallOrderBy(const Operator& op, MatBuffer& m);
@@ -667,7 +675,7 @@ class Executor {
   MatBuffer RunGroupByDense(const Operator& op, const std::vector<AggPlan>& plans, const KeyLayout& kl);
   bool BuildRowGroups(const Operator& op, std::vector<int>* key_cols);
   MatBuffer RunGroupByBuildRows(const Operator& op, const std::vector<AggPlan>& plans,
-                                const std::vector<int>& key_cols);
+                                const std::vector<int>& key_cols, bool any_order);
   void BuildJoin(const Operator& op);
   JoinTable BuildIndex(const MatBuffer& m, const std::vector<int>& key_cols);
   JoinTable BuildGroupedIndex(const MatBuffer& m, int key_col);
@@ -1151,6 +1159,7 @@ MatBuffer Executor::MaterializeStream(const Operator& op, const uint32_t* order,
     return out;
   }
   Prepare(op);
+  if (!StreamHasJoin(op) && !std::getenv("KDB_MATERIALIZE_ATOMIC")) return MaterializeCounted(op);
   int64_t cap = RowBound(op);
   for (int attempt = 0; attempt < 3; attempt++) {
     const auto mark = ctx_.RecordMark();
@@ -1196,6 +1205,72 @@ MatBuffer Executor::MaterializeStream(const Operator& op, const uint32_t* order,
     ctx_.RecordTruncate(mark);
   }
   throw Error(-4, "materialisation did not converge");
+}
+
+// Join-free streams (scans and filters) materialise in two passes over the
+// same grid: the first counts each block's rows, an exclusive scan turns the
+// counts into block offsets, and the second writes each block's rows at its
+// offset through a shared-memory slot counter.  One global atomic per
+// produced warp-row would serialise on the counter's L2 line (tens of
+// microseconds for a filtered scan of a few million rows); the count pass
+// reads only the filter columns.
+MatBuffer Executor::MaterializeCounted(const Operator& op) {
+  const int block = 256;
+  const auto& schema = op.output;
+  const std::string shared_init =
+      "  __shared__ unsigned kdb_block_rows;\n"
+      "  if (threadIdx.x == 0) kdb_block_rows = 0;\n"
+      "  __syncthreads();\n";
+  int64_t src_rows = 0;
+  KernelSource kc;
+  ExprGen egc(ctx_, kc);
+  kc.pre << shared_init;
+  auto count_sink = [&](const std::vector<CVal>&, const std::string&) {
+    kc.L("kdb_alloc_block_slot(&kdb_block_rows);");
+  };
+  EmitStream(kc, egc, op, count_sink, src_rows);
+  const int grid = ctx_.GridFor(std::max<int64_t>(src_rows, 1), block);
+  uint64_t* offsets = arena_.AllocT<uint64_t>(grid + 1);
+  const std::string offp = kc.Ptr(offsets, "uint64_t");
+  kc.L("__syncthreads();");
+  kc.L("if (threadIdx.x == 0) " + offp + "[blockIdx.x] = kdb_block_rows;");
+  LaunchPipeline(kc, src_rows, "materialize count", block);
+  ctx_.ScanU64(offsets, grid, "materialize offsets");
+  const int64_t produced = ReadU64(offsets + grid);
+  ctx_.CheckDeviceError("materialize");
+
+  KernelSource ks;
+  ExprGen eg(ctx_, ks);
+  MatBuffer out = AllocMat(schema, std::max<int64_t>(produced, 1));
+  std::vector<std::string> optr, onull;
+  for (const auto& c : out.cols) {
+    optr.push_back(ks.Ptr(c.data, StoreType(c.type.id)));
+    onull.push_back(c.nullable ? ks.Ptr(c.nulls, "int8_t") : "");
+  }
+  const std::string posp = ks.Ptr(out.pos, "uint64_t");
+  const std::string offr = ks.Ptr(offsets, "uint64_t", true);
+  const std::string capw = "(uint64_t)" + ks.Word(static_cast<uint64_t>(out.cap));
+  ks.pre << shared_init;
+  ks.pre << "  const uint64_t kdb_block_base = " << offr << "[blockIdx.x];\n";
+  auto sink = [&](const std::vector<CVal>& vals, const std::string& pos) {
+    ks.Open("");
+    ks.L("const uint64_t slot = kdb_block_base + kdb_alloc_block_slot(&kdb_block_rows);");
+    ks.Open("if (slot < " + capw + ")");
+    for (size_t c = 0; c < vals.size(); c++) {
+      const CVal& v = vals[c];
+      std::string val = v.type.id == TypeId::BOOLEAN ? "(int8_t)(" + v.v + " ? 1 : 0)" : v.v;
+      ks.L(optr[c] + "[slot] = " + val + ";");
+      if (!onull[c].empty()) ks.L(onull[c] + "[slot] = (" + v.n + ") ? 1 : 0;");
+    }
+    ks.L(posp + "[slot] = " + pos + ";");
+    ks.Close();
+    ks.Close();
+  };
+  int64_t src_rows2 = 0;
+  EmitStream(ks, eg, op, sink, src_rows2);
+  LaunchPipeline(ks, src_rows2, "materialize", block);
+  out.rows = produced;
+  return out;
 }
 
 MatBuffer Executor::Materialize(const Operator& op) {
@@ -1895,7 +1970,7 @@ bool Executor::BuildRowGroups(const Operator& op, std::vector<int>* key_cols) {
 }
 
 MatBuffer Executor::RunGroupByBuildRows(const Operator& op, const std::vector<AggPlan>& plans,
-                                        const std::vector<int>& key_cols) {
+                                        const std::vector<int>& key_cols, bool any_order) {
   const Operator& join = op.child();
   const JoinTable& jt = joins_.at(&join);
   const int64_t nb = jt.build.rows;
@@ -1988,12 +2063,13 @@ MatBuffer Executor::RunGroupByBuildRows(const Operator& op, const std::vector<Ag
     LaunchPipeline(ks, nb, "group compact");
   }
   int64_t ng = ReadU64(ngroups);
-  ctx_.RadixSortPairs(keys, vals, ng, arena_, 24);
+  if (!any_order) ctx_.RadixSortPairs(keys, vals, ng, arena_, 24);
   MatBuffer out = AllocMat(op.output, ng);
   if (ng > 0) {
     KernelSource ks;
     ExprGen eg(ctx_, ks);
     std::string F = ks.Ptr(first, "uint64_t", true), V = ks.Ptr(vals, "uint32_t", true);
+    std::string FK = any_order ? ks.Ptr(keys, "uint64_t", true) : "";
     std::string NGW = ks.Word(static_cast<uint64_t>(ng));
     std::vector<std::string> SV(plans.size()), SC(plans.size());
     for (size_t j = 0; j < plans.size(); j++) {
@@ -2025,16 +2101,16 @@ MatBuffer Executor::RunGroupByBuildRows(const Operator& op, const std::vector<Ag
       ks.L(optr[c] + "[r] = " + val + ";");
       if (!onull[c].empty()) ks.L(onull[c] + "[r] = (" + v.n + ") ? 1 : 0;");
     }
-    ks.L(posp + "[r] = (uint64_t)r;");
+    ks.L(posp + "[r] = " + (any_order ? FK + "[r]" : std::string("(uint64_t)r")) + ";");
     ks.Close();
     LaunchPipeline(ks, ng, "group output");
   }
   out.rows = ng;
-  out.pos_is_index = true;
+  out.pos_is_index = !any_order;
   return out;
 }
 
-MatBuffer Executor::RunGroupBy(const Operator& op) {
+MatBuffer Executor::RunGroupBy(const Operator& op, bool any_order) {
   PrepareInput(op.child());
   int flags = 0;
   std::vector<AggPlan> plans;
@@ -2062,7 +2138,7 @@ MatBuffer Executor::RunGroupBy(const Operator& op) {
   {
     std::vector<int> key_cols;
     if (!std::getenv("KDB_NO_BUILD_ROW_GROUPS") && BuildRowGroups(op, &key_cols))
-      return RunGroupByBuildRows(op, plans, key_cols);
+      return RunGroupByBuildRows(op, plans, key_cols, any_order);
   }
 
   // capacity: exact for small key domains; otherwise twice the input-row
@@ -2234,7 +2310,7 @@ MatBuffer Executor::RunGroupBy(const Operator& op) {
       LaunchPipeline(ks, static_cast<int64_t>(cap), "group compact");
     }
     int64_t ng = ReadU64(ngroups);
-    ctx_.RadixSortPairs(keys, vals, ng, arena_, 64);
+    if (!any_order) ctx_.RadixSortPairs(keys, vals, ng, arena_, 64);
     // output kernel
     MatBuffer out = AllocMat(op.output, ng);
     if (ng > 0) {
@@ -2242,6 +2318,7 @@ MatBuffer Executor::RunGroupBy(const Operator& op) {
       ExprGen eg(ctx_, ks);
       std::string S = ks.Ptr(slots, "uint64_t", true), F = ks.Ptr(first, "uint64_t", true);
       std::string V = ks.Ptr(vals, "uint32_t", true);
+      std::string FK = any_order ? ks.Ptr(keys, "uint64_t", true) : "";
       std::string NGW = ks.Word(static_cast<uint64_t>(ng));
       std::vector<std::string> KW(nk), KL(nk), KN(nk), SV(plans.size()), SC(plans.size());
       if (!kl.packed)
@@ -2303,13 +2380,13 @@ MatBuffer Executor::RunGroupBy(const Operator& op) {
         ks.L(optr[c] + "[r] = " + val + ";");
         if (!onull[c].empty()) ks.L(onull[c] + "[r] = (" + v.n + ") ? 1 : 0;");
       }
-      ks.L(posp + "[r] = (uint64_t)r;");
+      ks.L(posp + "[r] = " + (any_order ? FK + "[r]" : std::string("(uint64_t)r")) + ";");
       ks.Close();
       LaunchPipeline(ks, ng, "group output");
     }
     ctx_.CheckDeviceError("group output");
     out.rows = ng;
-    out.pos_is_index = true;
+    out.pos_is_index = !any_order;
     return out;
   }
   throw Error(-4, "group table did not fit");
@@ -2323,7 +2400,11 @@ MatBuffer Executor::RunGroupBy(const Operator& op) {
 // ---------------------------------------------------------------------------
 
 MatBuffer Executor::RunOrderBy(const Operator& op) {
-  MatBuffer m = Materialize(op.child());
+  // every ORDER BY path below orders rows that are not in stream order by
+  // their stream position, so a GROUP BY child need not sort its groups
+  MatBuffer m = op.child().kind == OpKind::GROUP_BY_AGGREGATE && !std::getenv("KDB_GROUP_ORDER_SORT")
+                    ? RunGroupBy(op.child(), true)
+                    : Materialize(op.child());
   int64_t n = m.rows;
   if (n <= kSmallOrder) return SmallOrderBy(op, m);
   return LargeOrderBy(op, m);
@@ -2414,80 +2495,117 @@ MatBuffer Executor::LargeOrderBy(const Operator& op, MatBuffer& m) {
   };
   if (n > 1) {
     // stream order (skipped when the rows already are in it)
-    if (m.pos_is_index) {
-      keygen([&](KernelSource& ks, ExprGen&, const std::string& I) {
-        ks.L(I + "[i] = (uint32_t)i;");
-        return std::string("0ULL");
-      });
-    } else {
-      keygen([&](KernelSource& ks, ExprGen&, const std::string& I) {
-        std::string P = ks.Ptr(m.pos, "uint64_t", true);
-        ks.L(I + "[i] = (uint32_t)i;");
-        return P + "[i]";
-      });
-      ctx_.RadixSortPairs(keys, idx, n, arena_, 64);
-    }
+    auto stream_order = [&]() {
+      if (m.pos_is_index) {
+        keygen([&](KernelSource& ks, ExprGen&, const std::string& I) {
+          ks.L(I + "[i] = (uint32_t)i;");
+          return std::string("0ULL");
+        });
+      } else {
+        keygen([&](KernelSource& ks, ExprGen&, const std::string& I) {
+          std::string P = ks.Ptr(m.pos, "uint64_t", true);
+          ks.L(I + "[i] = (uint32_t)i;");
+          return P + "[i]";
+        });
+        ctx_.RadixSortPairs(keys, idx, n, arena_, 64);
+      }
+    };
     // the tie key uses at most depth = ceil(log2 n) + 1 leading bits
     int depth = 1;
     while ((1LL << (depth - 1)) < n) depth++;
-    // One numeric non-NULL key: (key, tie rank) pairs are unique, so a block
-    // sort plus merge-path passes over 16-byte items orders them in a few
-    // launches (the radix path needs two launches per 8-bit digit).
-    if (op.sort_keys.size() == 1 && depth <= 32 && !std::getenv("KDB_ORDER_RADIX")) {
-      const MatCol& mc = m.cols.at(op.sort_keys[0]->column_idx);
+    // One numeric key: (key, tie rank) pairs are unique, so a block sort
+    // plus merge-path passes over 16-byte items orders them in a few
+    // launches (the radix path needs two launches per 8-bit digit).  A
+    // nullable key folds its NULL flag in as the most significant bit: the
+    // key's low bit moves to the top of the tie word, which then holds the
+    // tie rank in 31 bits.
+    const MatCol* mk = op.sort_keys.size() == 1 ? &m.cols.at(op.sort_keys[0]->column_idx) : nullptr;
+    const bool merge_ok = mk && depth <= 32 && !std::getenv("KDB_ORDER_RADIX") && mk->type.id != TypeId::TEXT &&
+                          mk->type.id != TypeId::BOOLEAN && (!mk->nullable || depth <= 31);
+    if (merge_ok) {
+      const MatCol& mc = *mk;
       const TypeId t = mc.type.id;
-      // a nullable key folds its NULL flag in as the most significant bit:
-      // the key's low bit moves to the top of the tie word, which then holds
-      // the tie rank in 31 bits
-      if (t != TypeId::TEXT && t != TypeId::BOOLEAN && (!mc.nullable || depth <= 31)) {
-        uint64_t* items = arena_.AllocT<uint64_t>(2 * n);
-        {
-          KernelSource ks;
-          ExprGen eg(ctx_, ks);
-          std::string IT = ks.Ptr(items, "uint64_t"), I = ks.Ptr(idx, "uint32_t", true);
-          std::string D = ks.Ptr(mc.data, StoreType(t), true);
-          std::string N = ks.Word(static_cast<uint64_t>(n));
-          ks.Open("for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < (int64_t)" + N +
-                  "; i += (int64_t)gridDim.x * blockDim.x)");
-          ks.L(std::string("const uint32_t row = ") + (m.pos_is_index ? "(uint32_t)i" : I + "[i]") + ";");
-          std::string v = D + "[row]", norm;
-          switch (t) {
-            case TypeId::REAL: norm = "kdb_dord(" + v + ")"; break;
-            case TypeId::ENUM: norm = "(uint64_t)(uint32_t)" + eg.EnumRank(mc.type, v); break;
-            default: norm = "((uint64_t)(int64_t)" + v + " ^ 0x8000000000000000ULL)"; break;
-          }
-          const std::string tie = "(kdb_tie_path((uint64_t)i, " + std::to_string(n) + "ULL) >> " +
-                                  std::to_string(64 - depth) + ")";
-          if (!mc.nullable) {
-            ks.L(IT + "[2 * i] = " + (op.asc[0] ? "" : "~") + "(" + norm + ");");
-            ks.L(IT + "[2 * i + 1] = " + tie + " | ((uint64_t)row << 32);");
-          } else {
-            // NULLs sort after every value ascending, before them descending
-            // (proxy::LessThan), and tie among themselves
-            std::string NP = ks.Ptr(mc.nulls, "int8_t", true);
-            ks.L("const bool isnull = " + NP + "[row] != 0;");
-            ks.L("const uint64_t k = isnull ? 0ULL : " + std::string(op.asc[0] ? "" : "~") + "(" + norm + ");");
-            ks.L(std::string("const uint64_t flag = ") + (op.asc[0] ? "isnull" : "!isnull") + " ? 1ULL : 0ULL;");
-            ks.L(IT + "[2 * i] = (flag << 63) | (k >> 1);");
-            ks.L(IT + "[2 * i + 1] = ((k & 1ULL) << 31) | " + tie + " | ((uint64_t)row << 32);");
-          }
-          ks.Close();
-          LaunchPipeline(ks, n, "order key");
+      uint64_t* items = arena_.AllocT<uint64_t>(2 * n);
+      // stream_ties: rows in stream order (idx) with the reference merge
+      // sort's tie rank; otherwise rows in buffer order with the row index
+      // as a provisional (unique) tie
+      auto make_items = [&](bool stream_ties) {
+        KernelSource ks;
+        ExprGen eg(ctx_, ks);
+        std::string IT = ks.Ptr(items, "uint64_t"), I = ks.Ptr(idx, "uint32_t", true);
+        std::string D = ks.Ptr(mc.data, StoreType(t), true);
+        std::string N = ks.Word(static_cast<uint64_t>(n));
+        ks.Open("for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < (int64_t)" + N +
+                "; i += (int64_t)gridDim.x * blockDim.x)");
+        ks.L(std::string("const uint32_t row = ") + (m.pos_is_index || !stream_ties ? "(uint32_t)i" : I + "[i]") +
+             ";");
+        std::string v = D + "[row]", norm;
+        switch (t) {
+          case TypeId::REAL: norm = "kdb_dord(" + v + ")"; break;
+          case TypeId::ENUM: norm = "(uint64_t)(uint32_t)" + eg.EnumRank(mc.type, v); break;
+          default: norm = "((uint64_t)(int64_t)" + v + " ^ 0x8000000000000000ULL)"; break;
         }
+        const std::string tie = stream_ties ? "(kdb_tie_path((uint64_t)i, " + std::to_string(n) + "ULL) >> " +
+                                                  std::to_string(64 - depth) + ")"
+                                            : std::string("(uint64_t)row");
+        if (!mc.nullable) {
+          ks.L(IT + "[2 * i] = " + (op.asc[0] ? "" : "~") + "(" + norm + ");");
+          ks.L(IT + "[2 * i + 1] = " + tie + " | ((uint64_t)row << 32);");
+        } else {
+          // NULLs sort after every value ascending, before them descending
+          // (proxy::LessThan), and tie among themselves
+          std::string NP = ks.Ptr(mc.nulls, "int8_t", true);
+          ks.L("const bool isnull = " + NP + "[row] != 0;");
+          ks.L("const uint64_t k = isnull ? 0ULL : " + std::string(op.asc[0] ? "" : "~") + "(" + norm + ");");
+          ks.L(std::string("const uint64_t flag = ") + (op.asc[0] ? "isnull" : "!isnull") + " ? 1ULL : 0ULL;");
+          ks.L(IT + "[2 * i] = (flag << 63) | (k >> 1);");
+          ks.L(IT + "[2 * i + 1] = ((k & 1ULL) << 31) | " + tie + " | ((uint64_t)row << 32);");
+        }
+        ks.Close();
+        LaunchPipeline(ks, n, "order key");
+      };
+      auto order_rows = [&]() {
+        KernelSource ks;
+        std::string IT = ks.Ptr(items, "uint64_t", true), I = ks.Ptr(idx, "uint32_t");
+        std::string N = ks.Word(static_cast<uint64_t>(n));
+        ks.Open("for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < (int64_t)" + N +
+                "; i += (int64_t)gridDim.x * blockDim.x)");
+        ks.L(I + "[i] = (uint32_t)(" + IT + "[2 * i + 1] >> 32);");
+        ks.Close();
+        LaunchPipeline(ks, n, "order rows");
+      };
+      if (!m.pos_is_index && !std::getenv("KDB_ORDER_TIE_SORT")) {
+        // Rows not in stream order (groups in table order): sort by the key
+        // alone and look for equal neighbours.  Without ties the tie rank
+        // never decides, and the stream-order sort is not needed.
+        make_items(false);
         ctx_.MergeSortItems(items, n, arena_);
+        uint64_t* ties = arena_.AllocT<uint64_t>(1);
+        ctx_.Memset(ties, 0, sizeof(uint64_t));
         {
           KernelSource ks;
-          std::string IT = ks.Ptr(items, "uint64_t", true), I = ks.Ptr(idx, "uint32_t");
+          std::string IT = ks.Ptr(items, "uint64_t", true), T = ks.Ptr(ties, "unsigned long long");
           std::string N = ks.Word(static_cast<uint64_t>(n));
-          ks.Open("for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < (int64_t)" + N +
+          ks.Open("for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i + 1 < (int64_t)" + N +
                   "; i += (int64_t)gridDim.x * blockDim.x)");
-          ks.L(I + "[i] = (uint32_t)(" + IT + "[2 * i + 1] >> 32);");
+          std::string eq = IT + "[2 * i] == " + IT + "[2 * i + 2]";
+          if (mc.nullable) eq += " && ((" + IT + "[2 * i + 1] ^ " + IT + "[2 * i + 3]) & 0x80000000ULL) == 0";
+          ks.L("if (" + eq + ") atomicAdd(" + T + ", 1ULL);");
           ks.Close();
-          LaunchPipeline(ks, n, "order rows");
+          LaunchPipeline(ks, n, "order ties");
         }
-        return MaterializeStream(op, idx, &m);
+        if (ReadU64(ties) == 0 && !ctx_.dry) {
+          order_rows();
+          return MaterializeStream(op, idx, &m);
+        }
       }
+      stream_order();
+      make_items(true);
+      ctx_.MergeSortItems(items, n, arena_);
+      order_rows();
+      return MaterializeStream(op, idx, &m);
     }
+    stream_order();
     auto tie_sort = [&]() {
       keygen([&](KernelSource&, ExprGen&, const std::string&) {
         return "(kdb_tie_path((uint64_t)i, " + std::to_string(n) + "ULL) >> " + std::to_string(64 - depth) + ")";
@@ -3524,7 +3642,8 @@ HostResult Executor::Download(const MatBuffer& m, const Operator& root, bool che
     if (m.cols[c].nulls) total += (static_cast<size_t>(m.rows) + 15) & ~size_t(15);
   }
   const size_t err_off = total;
-  char* stage = static_cast<char*>(ctx_.HostStage(total + 16));
+  res.block = ctx_.AcquireHostBlock(total + 16);
+  char* stage = res.block.get();
   if (!ctx_.dry && (m.rows > 0 || check_error)) {
     // several small segments: gather on the device, one copy to the host
     PackSegs segs;
@@ -3580,61 +3699,41 @@ HostResult Executor::Download(const MatBuffer& m, const Operator& root, bool che
     HostColumn hc;
     hc.name = schema[c].name;
     hc.type = mc.type;
+    const char* raw = stage + data_off[c];
+    if (mc.type.id != TypeId::TEXT) {
+      // the column stays in the result's block as downloaded
+      hc.packed = true;
+      hc.data = raw;
+      hc.nulls = mc.nulls ? reinterpret_cast<const int8_t*>(stage + null_off[c]) : nullptr;
+      hc.width = static_cast<int>(StoreWidth(mc.type.id));
+      res.cols.push_back(std::move(hc));
+      continue;
+    }
     if (mc.nulls) hc.null.assign(stage + null_off[c], stage + null_off[c] + m.rows);
     else hc.null.assign(m.rows, 0);
-    size_t w = StoreWidth(mc.type.id);
-    const char* raw = stage + data_off[c];
-    switch (mc.type.id) {
-      case TypeId::REAL: {
-        hc.f.resize(m.rows);
-        if (m.rows) std::memcpy(hc.f.data(), raw, w * m.rows);
-        break;
-      }
-      case TypeId::TEXT: {
-        const DevStr* ds = reinterpret_cast<const DevStr*>(raw);
-        std::vector<int64_t> off(m.rows + 1, 0);
-        for (int64_t r = 0; r < m.rows; r++) off[r + 1] = off[r] + (hc.null[r] ? 0 : ds[r].len);
-        int64_t nbytes = off[m.rows];
-        hc.s.resize(m.rows);
-        if (nbytes > 0) {
-          int64_t* d_off = arena_.AllocT<int64_t>(m.rows + 1);
-          char* d_chars = arena_.AllocT<char>(nbytes);
-          ctx_.H2D(d_off, off.data(), sizeof(int64_t) * (m.rows + 1));
-          KernelSource ks;
-          std::string D = ks.Ptr(mc.data, "kdb_str", true), O = ks.Ptr(d_off, "int64_t", true);
-          std::string CH = ks.Ptr(d_chars, "char");
-          std::string N = ks.Word(static_cast<uint64_t>(m.rows));
-          ks.Open("for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < (int64_t)" + N +
-                  "; r += (int64_t)gridDim.x * blockDim.x)");
-          ks.L("int64_t len = " + O + "[r + 1] - " + O + "[r];");
-          ks.L("for (int64_t b = 0; b < len; b++) " + CH + "[" + O + "[r] + b] = " + D + "[r].p[b];");
-          ks.Close();
-          LaunchPipeline(ks, m.rows, "text download");
-          std::vector<char> chars(nbytes);
-          ctx_.D2H(chars.data(), d_chars, nbytes);
-          for (int64_t r = 0; r < m.rows; r++) hc.s[r].assign(chars.data() + off[r], off[r + 1] - off[r]);
-        }
-        break;
-      }
-      default: {
-        hc.i.resize(m.rows);
-        (void)w;
-        auto widen = [&](auto tag) {  // one tight loop per stored width
-          using T = decltype(tag);
-          std::vector<T> tmp(m.rows);
-          if (m.rows) std::memcpy(tmp.data(), raw, sizeof(T) * m.rows);
-          for (int64_t r = 0; r < m.rows; r++) hc.i[r] = tmp[r];
-        };
-        switch (mc.type.id) {
-          case TypeId::BOOLEAN: widen(int8_t{}); break;
-          case TypeId::SMALLINT: widen(int16_t{}); break;
-          case TypeId::BIGINT:
-            if (m.rows) std::memcpy(hc.i.data(), raw, sizeof(int64_t) * m.rows);
-            break;
-          default: widen(int32_t{}); break;
-        }
-        break;
-      }
+    // TEXT: the strings' bytes are gathered on the device and copied once
+    const DevStr* ds = reinterpret_cast<const DevStr*>(raw);
+    std::vector<int64_t> off(m.rows + 1, 0);
+    for (int64_t r = 0; r < m.rows; r++) off[r + 1] = off[r] + (hc.null[r] ? 0 : ds[r].len);
+    int64_t nbytes = off[m.rows];
+    hc.s.resize(m.rows);
+    if (nbytes > 0) {
+      int64_t* d_off = arena_.AllocT<int64_t>(m.rows + 1);
+      char* d_chars = arena_.AllocT<char>(nbytes);
+      ctx_.H2D(d_off, off.data(), sizeof(int64_t) * (m.rows + 1));
+      KernelSource ks;
+      std::string D = ks.Ptr(mc.data, "kdb_str", true), O = ks.Ptr(d_off, "int64_t", true);
+      std::string CH = ks.Ptr(d_chars, "char");
+      std::string N = ks.Word(static_cast<uint64_t>(m.rows));
+      ks.Open("for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < (int64_t)" + N +
+              "; r += (int64_t)gridDim.x * blockDim.x)");
+      ks.L("int64_t len = " + O + "[r + 1] - " + O + "[r];");
+      ks.L("for (int64_t b = 0; b < len; b++) " + CH + "[" + O + "[r] + b] = " + D + "[r].p[b];");
+      ks.Close();
+      LaunchPipeline(ks, m.rows, "text download");
+      std::vector<char> chars(nbytes);
+      ctx_.D2H(chars.data(), d_chars, nbytes);
+      for (int64_t r = 0; r < m.rows; r++) hc.s[r].assign(chars.data() + off[r], off[r + 1] - off[r]);
     }
     res.cols.push_back(std::move(hc));
   }

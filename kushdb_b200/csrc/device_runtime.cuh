@@ -195,6 +195,17 @@ KDB_DEV uint64_t kdb_alloc_slot(unsigned long long* counter) {
   return base + __popc(mask & ((1u << lane) - 1));
 }
 
+// The same for a block-local counter in shared memory.
+KDB_DEV uint32_t kdb_alloc_block_slot(unsigned* counter) {
+  unsigned mask = __activemask();
+  int lane = threadIdx.x & 31;
+  int leader = __ffs(mask) - 1;
+  unsigned base = 0;
+  if (lane == leader) base = atomicAdd(counter, (unsigned)__popc(mask));
+  base = __shfl_sync(mask, base, leader);
+  return base + __popc(mask & ((1u << lane) - 1));
+}
+
 KDB_DEV void kdb_set_error(int* err, int code) { atomicCAS(err, 0, code); }
 
 // ---- atomics for aggregate state -------------------------------------------

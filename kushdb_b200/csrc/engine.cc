@@ -137,6 +137,71 @@ void* Context::HostStage(size_t bytes) {
   return stage_;
 }
 
+HostBlockPool::~HostBlockPool() {
+  for (auto& b : free_) FreeBlock(b.second);
+}
+
+void HostBlockPool::FreeBlock(char* p) const {
+  if (pinned_) cudaFreeHost(p);
+  else std::free(p);
+}
+
+std::shared_ptr<char> HostBlockPool::Acquire(size_t bytes) {
+  char* p = nullptr;
+  size_t size = 0;
+  {
+    std::lock_guard<std::mutex> g(mu_);
+    size_t best = free_.size();
+    for (size_t i = 0; i < free_.size(); i++)
+      if (free_[i].first >= bytes && (best == free_.size() || free_[i].first < free_[best].first)) best = i;
+    if (best < free_.size()) {
+      size = free_[best].first;
+      p = free_[best].second;
+      free_.erase(free_.begin() + best);
+    }
+  }
+  if (!p) {
+    size = size_t(1) << 20;
+    while (size < bytes) size <<= 1;
+    if (pinned_) {
+      void* h = nullptr;
+      KDB_CUDA(cudaMallocHost(&h, size));
+      p = static_cast<char*>(h);
+    } else {
+      p = static_cast<char*>(std::malloc(size));
+      if (!p) throw Error(-3, "host allocation failed");
+    }
+  }
+  std::weak_ptr<HostBlockPool> pool = shared_from_this();
+  const bool pinned = pinned_;
+  return std::shared_ptr<char>(p, [pool, size, pinned](char* q) {
+    if (auto live = pool.lock()) live->Release(q, size);
+    else if (pinned) cudaFreeHost(q);
+    else std::free(q);
+  });
+}
+
+void HostBlockPool::Release(char* p, size_t bytes) {
+  {
+    std::lock_guard<std::mutex> g(mu_);
+    if (free_.size() < kKeep) {
+      free_.emplace_back(bytes, p);
+      return;
+    }
+  }
+  FreeBlock(p);
+}
+
+std::shared_ptr<char> Context::AcquireHostBlock(size_t bytes) {
+  if (!host_blocks_) host_blocks_ = std::make_shared<HostBlockPool>(!dry);
+  return host_blocks_->Acquire(bytes);
+}
+
+void Context::ReserveHostBlocks(int count, size_t bytes) {
+  std::vector<std::shared_ptr<char>> held;
+  for (int i = 0; i < count; i++) held.push_back(AcquireHostBlock(bytes));
+}
+
 // ---------------------------------------------------------------------------
 // Context
 // ---------------------------------------------------------------------------

@@ -106,6 +106,24 @@ struct KArgs {
 };
 
 class Context;
+
+// Host blocks that downloaded results own (pinned unless compile-only).  A
+// block comes back to the pool when its last owner lets go; the pool keeps
+// a few for the next results and frees the rest.
+class HostBlockPool : public std::enable_shared_from_this<HostBlockPool> {
+ public:
+  explicit HostBlockPool(bool pinned) : pinned_(pinned) {}
+  ~HostBlockPool();
+  std::shared_ptr<char> Acquire(size_t bytes);
+
+ private:
+  static constexpr size_t kKeep = 8;  // free blocks kept for reuse
+  void Release(char* p, size_t bytes);
+  void FreeBlock(char* p) const;
+  bool pinned_;
+  std::mutex mu_;
+  std::vector<std::pair<size_t, char*>> free_;
+};
 class JoinPrior;
 
 // Segments gathered into one buffer for a single device-to-host copy.
@@ -253,14 +271,22 @@ class Context {
   void D2H(void* h, const void* d, size_t bytes);  // synchronous
   // Pinned host staging buffer of at least `bytes` (reused across queries).
   void* HostStage(size_t bytes);
+  // Pinned host block of at least `bytes` for a downloaded result: the
+  // result keeps it until it is freed, then it returns to the context's pool
+  // (no host copy of the columns, no pinned allocation per query).
+  std::shared_ptr<char> AcquireHostBlock(size_t bytes);
+  // Puts `count` blocks of `bytes` into the pool ahead of use (a pinned
+  // allocation synchronises with the device).
+  void ReserveHostBlocks(int count, size_t bytes);
 
   // Static kernels (kernels.cu).
   void RadixSortPairs(uint64_t* keys, uint32_t* vals, int64_t n, Arena& arena, int key_bits = 64);
-  // sorts n 16-byte items {uint64 key, uint32 tie, uint32 value} by
-  // (key, tie), which must be unique (block sort + merge-path passes)
+  // sorts n < 2^31 16-byte items {uint64 key, uint32 tie, uint32 value} by
+  // (key, tie) (block sort + merge-path passes; items equal in (key, tie)
+  // come out in no particular order)
   void MergeSortItems(void* items, int64_t n, Arena& arena);
   // exclusive prefix sum of a[0..n) in place, the total into a[n]
-  void ScanU64(uint64_t* a, int64_t n);
+  void ScanU64(uint64_t* a, int64_t n, const char* tag = "skinner scan");
   // gathers the segments into the device staging buffer and queues one copy
   // of `total` bytes to `host` (pinned); the caller synchronises
   void PackToHost(const PackSegs& segs, size_t total, void* host);
@@ -273,6 +299,7 @@ class Context {
   bool owns_catalog_ = true;
   void* stage_ = nullptr;
   size_t stage_bytes_ = 0;
+  std::shared_ptr<HostBlockPool> host_blocks_;
   void* dev_stage_ = nullptr;  // device side of PackToHost
   size_t dev_stage_bytes_ = 0;
   void FreeColumn(DevColumn& c);

@@ -9,7 +9,9 @@
 
 #include <cstdint>
 #include <cstdio>
+#include <cstring>
 #include <map>
+#include <memory>
 #include <string>
 #include <vector>
 
@@ -65,38 +67,104 @@ struct HostColumn {
   std::vector<double> f;         // REAL
   std::vector<std::string> s;    // TEXT
   std::vector<int8_t> null;      // 1 = NULL
+  // Packed form of a downloaded non-TEXT column (the vectors above stay
+  // empty): `width`-byte values as stored on the device (signed integers,
+  // REAL as double) at `data`, one NULL byte per row at `nulls` (nullptr:
+  // no NULLs).  The bytes belong to HostResult::block.
+  bool packed = false;
+  const char* data = nullptr;
+  const int8_t* nulls = nullptr;
+  int width = 0;
+
+  bool IsNull(int64_t r) const { return packed ? (nulls != nullptr && nulls[r] != 0) : null[r] != 0; }
+  int64_t IntAt(int64_t r) const {
+    if (!packed) return i[r];
+    switch (width) {
+      case 1: return reinterpret_cast<const int8_t*>(data)[r];
+      case 2: return reinterpret_cast<const int16_t*>(data)[r];
+      case 4: return reinterpret_cast<const int32_t*>(data)[r];
+      default: return reinterpret_cast<const int64_t*>(data)[r];
+    }
+  }
+  double RealAt(int64_t r) const { return packed ? reinterpret_cast<const double*>(data)[r] : f[r]; }
+
+  // Whole-column copies (the C interface); false when the column has no
+  // values of that kind (integers of a REAL or TEXT column, reals of a
+  // non-REAL column).
+  bool CopyInts(int64_t rows, int64_t* out) const {
+    if (!packed) {
+      if (i.size() != static_cast<size_t>(rows)) return false;
+      if (rows) std::memcpy(out, i.data(), sizeof(int64_t) * rows);
+      return true;
+    }
+    if (type.id == plan::TypeId::REAL) return rows == 0;
+    auto widen = [&](auto tag) {  // one tight loop per stored width
+      using T = decltype(tag);
+      const T* v = reinterpret_cast<const T*>(data);
+      for (int64_t r = 0; r < rows; r++) out[r] = v[r];
+    };
+    switch (width) {
+      case 1: widen(int8_t{}); break;
+      case 2: widen(int16_t{}); break;
+      case 4: widen(int32_t{}); break;
+      default:
+        if (rows) std::memcpy(out, data, sizeof(int64_t) * rows);
+        break;
+    }
+    return true;
+  }
+  bool CopyReals(int64_t rows, double* out) const {
+    if (!packed) {
+      if (f.size() != static_cast<size_t>(rows)) return false;
+      if (rows) std::memcpy(out, f.data(), sizeof(double) * rows);
+      return true;
+    }
+    if (type.id != plan::TypeId::REAL) return rows == 0;
+    if (rows) std::memcpy(out, data, sizeof(double) * rows);
+    return true;
+  }
+  void CopyNulls(int64_t rows, int8_t* out) const {
+    if (!packed) {
+      if (!null.empty()) std::memcpy(out, null.data(), null.size());
+    } else if (nulls) {
+      std::memcpy(out, nulls, rows);
+    } else if (rows) {
+      std::memset(out, 0, rows);
+    }
+  }
 };
 
 struct HostResult {
   std::vector<HostColumn> cols;
   int64_t rows = 0;
+  std::shared_ptr<char> block;  // owns the packed columns' bytes
 };
 
 using EnumDicts = std::map<int32_t, std::vector<std::string>>;
 
 inline std::string FormatValue(const HostColumn& c, int64_t r, const EnumDicts& enums) {
-  if (c.null[r]) return "";
+  if (c.IsNull(r)) return "";
   char buf[64];
   switch (c.type.id) {
-    case plan::TypeId::BOOLEAN: return c.i[r] ? "t" : "f";
+    case plan::TypeId::BOOLEAN: return c.IntAt(r) ? "t" : "f";
     case plan::TypeId::SMALLINT:
     case plan::TypeId::INT:
     case plan::TypeId::BIGINT:
-      std::snprintf(buf, sizeof(buf), "%lld", static_cast<long long>(c.i[r]));
+      std::snprintf(buf, sizeof(buf), "%lld", static_cast<long long>(c.IntAt(r)));
       return buf;
     case plan::TypeId::DATE: {
       int32_t y, m, d;
-      SplitDate(static_cast<int32_t>(c.i[r]), &y, &m, &d);
+      SplitDate(static_cast<int32_t>(c.IntAt(r)), &y, &m, &d);
       std::snprintf(buf, sizeof(buf), "%d-%02d-%02d", y, m, d);
       return buf;
     }
     case plan::TypeId::REAL:
-      std::snprintf(buf, sizeof(buf), "%.6f", c.f[r]);
+      std::snprintf(buf, sizeof(buf), "%.6f", c.RealAt(r));
       return buf;
     case plan::TypeId::TEXT: return c.s[r];
     case plan::TypeId::ENUM: {
       auto it = enums.find(c.type.enum_id);
-      int64_t k = c.i[r];
+      int64_t k = c.IntAt(r);
       if (it == enums.end() || k < 0 || k >= static_cast<int64_t>(it->second.size()))
         return "<enum:" + std::to_string(k) + ">";
       return it->second[k];

@@ -305,67 +305,162 @@ __device__ __forceinline__ bool ItemLess(const SortItem& a, const SortItem& b) {
   return a.key < b.key || (a.key == b.key && a.tie < b.tie);
 }
 
-constexpr int kMergeTile = 2048;  // items per block sort
-constexpr int kMergeItems = 8;    // outputs per thread per merge pass
+constexpr int kMergeTile = 2048;    // items per block sort and per merge tile
+constexpr int kMergeThreads = 256;  // threads per block; kMergeTile / kMergeThreads items each
+constexpr int kMergeItems = kMergeTile / kMergeThreads;
+static_assert(kMergeItems == 8, "the register sort network is written for 8 items");
 
-// Bitonic sort of each tile of kMergeTile items in shared memory (padding
-// with maximal items).
-__global__ void __launch_bounds__(1024) BlockSortItems(SortItem* __restrict__ items, int64_t n) {
-  __shared__ SortItem t[kMergeTile];
-  const int64_t base = static_cast<int64_t>(blockIdx.x) * kMergeTile;
-  for (int i = threadIdx.x; i < kMergeTile; i += blockDim.x)
-    t[i] = base + i < n ? items[base + i] : SortItem{~0ULL, ~0u, ~0u};
-  __syncthreads();
-  for (int size = 2; size <= kMergeTile; size <<= 1)
-    for (int stride = size >> 1; stride > 0; stride >>= 1) {
-      for (int i = threadIdx.x; i < kMergeTile / 2; i += blockDim.x) {
-        const int lo = 2 * i - (i & (stride - 1));
-        const int hi = lo + stride;
-        const bool up = (lo & size) == 0;
-        const SortItem a = t[lo], b = t[hi];
-        if (ItemLess(b, a) == up) {
-          t[lo] = b;
-          t[hi] = a;
-        }
-      }
-      __syncthreads();
-    }
-  for (int i = threadIdx.x; i < kMergeTile; i += blockDim.x)
-    if (base + i < n) items[base + i] = t[i];
+// Shared-memory tiles hold one pad item after every 8, so that the 8
+// consecutive items of consecutive threads fall in different banks.
+__device__ __forceinline__ int Padded(int i) { return i + (i >> 3); }
+constexpr int kPaddedTile = kMergeTile + kMergeTile / 8;
+
+// Number of items of A among the first `diag` outputs of merging A and B,
+// where B's item goes first on equal items.  `at`/`bt` read A[i] and B[j].
+template <typename AT, typename BT>
+__device__ __forceinline__ int MergePathSplit(AT at, int a_len, BT bt, int b_len, int diag) {
+  int lo = diag - b_len > 0 ? diag - b_len : 0, hi = diag < a_len ? diag : a_len;
+  while (lo < hi) {
+    const int mid = (lo + hi) >> 1;
+    if (ItemLess(at(mid), bt(diag - 1 - mid))) lo = mid + 1;
+    else hi = mid;
+  }
+  return lo;
 }
 
-// One merge pass: sorted runs of `w` items merge pairwise into runs of 2w;
-// each thread finds its output diagonal by binary search (merge path) and
-// writes kMergeItems outputs.
-__global__ void __launch_bounds__(256) MergeItems(const SortItem* __restrict__ in, SortItem* __restrict__ out,
-                                                  int64_t n, int64_t w) {
-  const int64_t o = (blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x) * kMergeItems;
-  if (o >= n) return;
-  const int64_t base = o / (2 * w) * (2 * w);
-  const int64_t a_len = min(w, n - base);
+// The same split for runs in global memory, searched by a whole warp: each
+// step tests 32 evenly spaced candidates, so a run of 2^20 items takes four
+// dependent rounds of loads instead of twenty.  Every lane returns the split.
+__device__ int64_t WarpMergePathSplit(const SortItem* __restrict__ A, int64_t a_len,
+                                      const SortItem* __restrict__ B, int64_t b_len, int64_t diag) {
+  const int lane = threadIdx.x & 31;
+  int64_t lo = diag - b_len > 0 ? diag - b_len : 0, hi = diag < a_len ? diag : a_len;
+  // A[i] is among the first `diag` outputs exactly for i < split, i.e. where
+  // A[i] < B[diag - 1 - i]; that test is true on a prefix of [lo, hi)
+  while (hi - lo > 32) {
+    const int64_t step = (hi - lo + 31) / 32;
+    const int64_t p = lo + lane * step;
+    const bool before = p < hi && ItemLess(A[p], B[diag - 1 - p]);
+    const int k = __popc(__ballot_sync(0xffffffffu, before));
+    if (k == 0) return lo;
+    const int64_t next_hi = lo + k * step;
+    lo = lo + (k - 1) * step + 1;
+    hi = next_hi < hi ? next_hi : hi;
+  }
+  const int64_t p = lo + lane;
+  const bool before = p < hi && ItemLess(A[p], B[diag - 1 - p]);
+  return lo + __popc(__ballot_sync(0xffffffffu, before));
+}
+
+__device__ __forceinline__ void CompareSwap(SortItem& a, SortItem& b) {
+  if (ItemLess(b, a)) {
+    const SortItem t = a;
+    a = b;
+    b = t;
+  }
+}
+
+// Batcher's odd-even merge sort network for 8 items (19 comparators).
+__device__ __forceinline__ void SortNetwork8(SortItem (&x)[8]) {
+  CompareSwap(x[0], x[1]); CompareSwap(x[2], x[3]); CompareSwap(x[4], x[5]); CompareSwap(x[6], x[7]);
+  CompareSwap(x[0], x[2]); CompareSwap(x[1], x[3]); CompareSwap(x[4], x[6]); CompareSwap(x[5], x[7]);
+  CompareSwap(x[1], x[2]); CompareSwap(x[5], x[6]);
+  CompareSwap(x[0], x[4]); CompareSwap(x[1], x[5]); CompareSwap(x[2], x[6]); CompareSwap(x[3], x[7]);
+  CompareSwap(x[2], x[4]); CompareSwap(x[3], x[5]);
+  CompareSwap(x[1], x[2]); CompareSwap(x[3], x[4]); CompareSwap(x[5], x[6]);
+}
+
+// Sorts each tile of kMergeTile items of `in` into `out` (which may be `in`):
+// every thread sorts 8 items in registers, then eight rounds of merge path in
+// shared memory double the sorted runs from 8 to kMergeTile items.  Missing
+// items of the last tile are maximal padding and never written.
+__global__ void __launch_bounds__(kMergeThreads) BlockSortItems(const SortItem* in, SortItem* out, int64_t n) {
+  __shared__ SortItem s[kPaddedTile];
+  const int64_t base = static_cast<int64_t>(blockIdx.x) * kMergeTile;
+  const int cnt = static_cast<int>(n - base < kMergeTile ? n - base : kMergeTile);
+  for (int i = threadIdx.x; i < kMergeTile; i += kMergeThreads)
+    s[Padded(i)] = i < cnt ? in[base + i] : SortItem{~0ULL, ~0u, ~0u};
+  __syncthreads();
+  const int d = threadIdx.x * kMergeItems;
+  SortItem x[kMergeItems];
+#pragma unroll
+  for (int k = 0; k < kMergeItems; k++) x[k] = s[Padded(d + k)];
+  SortNetwork8(x);
+  for (int run = kMergeItems; run < kMergeTile; run <<= 1) {
+    __syncthreads();
+#pragma unroll
+    for (int k = 0; k < kMergeItems; k++) s[Padded(d + k)] = x[k];
+    __syncthreads();
+    const int pb = d & ~(2 * run - 1);
+    auto at = [&](int i) -> const SortItem& { return s[Padded(pb + i)]; };
+    auto bt = [&](int j) -> const SortItem& { return s[Padded(pb + run + j)]; };
+    int i = MergePathSplit(at, run, bt, run, d - pb);
+    int j = d - pb - i;
+#pragma unroll
+    for (int k = 0; k < kMergeItems; k++) {
+      const bool take_a = j >= run || (i < run && ItemLess(at(i), bt(j)));
+      x[k] = take_a ? at(i++) : bt(j++);
+    }
+  }
+  __syncthreads();
+#pragma unroll
+  for (int k = 0; k < kMergeItems; k++) s[Padded(d + k)] = x[k];
+  __syncthreads();
+  for (int i = threadIdx.x; i < cnt; i += kMergeThreads) out[base + i] = s[Padded(i)];
+}
+
+// One merge pass: sorted runs of `w` (a multiple of kMergeTile) items merge
+// pairwise into runs of 2w.  Each block makes one tile of kMergeTile
+// outputs: two warps find the tile's first and last merge-path splits in
+// global memory, the block stages the tile's inputs in shared memory with
+// coalesced loads, and every thread merges 8 outputs from there.
+__global__ void __launch_bounds__(kMergeThreads) MergeItems(const SortItem* __restrict__ in,
+                                                            SortItem* __restrict__ out, int64_t n, int64_t w) {
+  __shared__ SortItem s[kPaddedTile];
+  __shared__ int64_t split[2];
+  const int64_t o0 = static_cast<int64_t>(blockIdx.x) * kMergeTile;
+  const int64_t base = o0 / (2 * w) * (2 * w);
+  const int64_t a_len = w < n - base ? w : n - base;
   const int64_t b0 = base + w;
-  const int64_t b_len = b0 < n ? min(w, n - b0) : 0;
+  const int64_t b_len = b0 < n ? (w < n - b0 ? w : n - b0) : 0;
+  const int64_t pair_end = base + a_len + b_len;
+  const int64_t o1 = o0 + kMergeTile < pair_end ? o0 + kMergeTile : pair_end;
   const SortItem* A = in + base;
   const SortItem* B = in + b0;
-  const int64_t diag = o - base;
-  int64_t lo = diag - b_len > 0 ? diag - b_len : 0, hi = diag < a_len ? diag : a_len;
-  while (lo < hi) {  // first i with A[i] > B[diag - i - 1]
-    const int64_t mid = (lo + hi) >> 1;
-    if (ItemLess(B[diag - mid - 1], A[mid])) hi = mid;
-    else lo = mid + 1;
+  const int warp = threadIdx.x >> 5;
+  if (warp < 2) {
+    const int64_t sp = WarpMergePathSplit(A, a_len, B, b_len, (warp == 0 ? o0 : o1) - base);
+    if ((threadIdx.x & 31) == 0) split[warp] = sp;
   }
-  int64_t i = lo, j = diag - lo;
-  const int64_t end = min(o + static_cast<int64_t>(kMergeItems), base + a_len + b_len);
-  for (int64_t k = o; k < end; k++) {
-    const bool take_a = j >= b_len || (i < a_len && ItemLess(A[i], B[j]));
-    out[k] = take_a ? A[i++] : B[j++];
+  __syncthreads();
+  const int64_t ia = split[0], jb = o0 - base - split[0];
+  const int na = static_cast<int>(split[1] - split[0]);
+  const int cnt = static_cast<int>(o1 - o0);
+  const int nb = cnt - na;
+  for (int i = threadIdx.x; i < cnt; i += kMergeThreads)
+    s[Padded(i)] = i < na ? A[ia + i] : B[jb + i - na];
+  __syncthreads();
+  const int d = threadIdx.x * kMergeItems;
+  SortItem x[kMergeItems];
+  if (d < cnt) {
+    auto at = [&](int i) -> const SortItem& { return s[Padded(i)]; };
+    auto bt = [&](int j) -> const SortItem& { return s[Padded(na + j)]; };
+    int i = MergePathSplit(at, na, bt, nb, d);
+    int j = d - i;
+#pragma unroll
+    for (int k = 0; k < kMergeItems; k++) {
+      if (d + k < cnt) {
+        const bool take_a = j >= nb || (i < na && ItemLess(at(i), bt(j)));
+        x[k] = take_a ? at(i++) : bt(j++);
+      }
+    }
   }
-}
-
-__global__ void CopyItems(const SortItem* __restrict__ src, SortItem* __restrict__ dst, int64_t n) {
-  for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < n;
-       i += static_cast<int64_t>(gridDim.x) * blockDim.x)
-    dst[i] = src[i];
+  __syncthreads();
+#pragma unroll
+  for (int k = 0; k < kMergeItems; k++)
+    if (d + k < cnt) s[Padded(d + k)] = x[k];
+  __syncthreads();
+  for (int i = threadIdx.x; i < cnt; i += kMergeThreads) out[o0 + i] = s[Padded(i)];
 }
 
 __global__ void CopyPairs(const uint64_t* __restrict__ ks, const uint32_t* __restrict__ vs,
@@ -398,33 +493,35 @@ void Context::PackToHost(const PackSegs& segs, size_t total, void* host) {
 
 void Context::MergeSortItems(void* items, int64_t n, Arena& arena) {
   if (n <= 1 || dry) return;
+  if (n > 0x7fffffffLL) throw Error(-5, "merge sort of more than 2^31 items");
   SortItem* a = static_cast<SortItem*>(items);
   SortItem* b = reinterpret_cast<SortItem*>(arena.Alloc(sizeof(SortItem) * n));
-  const int tiles = static_cast<int>((n + kMergeTile - 1) / kMergeTile);
+  const int64_t tiles = (n + kMergeTile - 1) / kMergeTile;
+  int passes = 0;
+  for (int64_t w = kMergeTile; w < n; w <<= 1) passes++;
+  // with an odd number of merge passes the block sort writes into the
+  // scratch buffer, so that the last pass ends in `items` (no copy back)
+  SortItem* src = a;
+  SortItem* dst = passes % 2 ? b : a;
   TimedStart("sort block");
-  Issue([=](cudaStream_t s) { BlockSortItems<<<tiles, 1024, 0, s>>>(a, n); });
+  Issue([=](cudaStream_t s) { BlockSortItems<<<static_cast<unsigned>(tiles), kMergeThreads, 0, s>>>(src, dst, n); });
   TimedStop();
+  SortItem* cur = dst;
+  SortItem* other = cur == a ? b : a;
   for (int64_t w = kMergeTile; w < n; w <<= 1) {
-    const int grid = static_cast<int>(((n + kMergeItems - 1) / kMergeItems + 255) / 256);
+    const SortItem* in = cur;
+    SortItem* out = other;
     TimedStart("sort merge");
-    Issue([=](cudaStream_t s) { MergeItems<<<grid, 256, 0, s>>>(a, b, n, w); });
+    Issue([=](cudaStream_t s) { MergeItems<<<static_cast<unsigned>(tiles), kMergeThreads, 0, s>>>(in, out, n, w); });
     TimedStop();
-    std::swap(a, b);
-  }
-  if (a != items) {
-    const int grid = GridFor(n, 256);
-    SortItem* dst = static_cast<SortItem*>(items);
-    const SortItem* src = a;
-    TimedStart("sort copy");
-    Issue([=](cudaStream_t s) { CopyItems<<<grid, 256, 0, s>>>(src, dst, n); });
-    TimedStop();
+    std::swap(cur, other);
   }
   KDB_CUDA(cudaGetLastError());
 }
 
-void Context::ScanU64(uint64_t* a, int64_t n) {
+void Context::ScanU64(uint64_t* a, int64_t n, const char* tag) {
   if (dry) return;
-  TimedStart("skinner scan");
+  TimedStart(tag);
   Issue([=](cudaStream_t s) { ExclusiveScanU64<<<1, 1024, 0, s>>>(a, n); });
   TimedStop();
   KDB_CUDA(cudaGetLastError());

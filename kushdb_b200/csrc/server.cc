@@ -63,7 +63,7 @@ class Server {
   Server(Context& parent, int slots, int64_t hbm_budget) : budget_(hbm_budget) {
     for (int i = 0; i < slots; i++) {
       slots_.push_back(std::make_unique<Context>(parent));
-      slots_.back()->HostStage(16 << 20);  // pinned result staging up front: no host-alloc syncs later
+      slots_.back()->ReserveHostBlocks(4, 16 << 20);  // pinned result blocks up front: no host-alloc syncs later
     }
     for (int i = 0; i < slots; i++) workers_.emplace_back([this, i] { Loop(i); });
   }
