@@ -221,6 +221,16 @@ class ExprGen {
     }
   }
 
+  // 32-bit join key hash; equal values of any integer width hash alike
+  std::string KeyHash32(const CVal& c) {
+    switch (c.type.id) {
+      case TypeId::REAL: return "kdb_hash64to32(kdb_dbits(" + c.v + "))";
+      case TypeId::TEXT: return "(uint32_t)(kdb_hash_str(" + c.v + ") >> 32)";
+      case TypeId::BOOLEAN: return "kdb_hash64to32((uint64_t)(" + c.v + " ? 1 : 0))";
+      default: return "kdb_hash64to32((uint64_t)(int64_t)" + c.v + ")";
+    }
+  }
+
   std::string EqOf(const CVal& a, const CVal& b) {
     switch (a.type.id) {
       case TypeId::TEXT: return "kdb_str_eq(" + a.v + ", " + b.v + ")";
@@ -692,9 +702,9 @@ class Executor {
     return n;
   }
 
-  void LaunchPipeline(KernelSource& ks, int64_t src_rows, const char* what, int block = 256) {
+  void LaunchPipeline(KernelSource& ks, int64_t src_rows, const char* what, int block = 256, int min_blocks = 1) {
     std::string name = KernelName(what);
-    std::string src = ks.Kernel(name, block);
+    std::string src = ks.Kernel(name, block, min_blocks);
     CUfunction f = ctx_.Kernel(src, name);
     int grid = ctx_.GridFor(std::max<int64_t>(src_rows, 1), block);
     ctx_.Launch(f, grid, block, ks.Args(), 0, what);
@@ -702,9 +712,9 @@ class Executor {
 };
 
 std::string Executor::JoinHash(ExprGen& eg, const std::vector<CVal>& keys) {
-  std::string h = "0x51ed270b27f1a0c9ULL";
-  for (const auto& k : keys) h = "kdb_hash_combine(" + h + ", " + eg.HashOf(k) + ")";
-  return "(uint32_t)((" + h + ") >> 32)";
+  std::string h;
+  for (const auto& k : keys) h = h.empty() ? eg.KeyHash32(k) : "kdb_hash_combine32(" + h + ", " + eg.KeyHash32(k) + ")";
+  return h;
 }
 
 std::vector<CVal> Executor::LoadMatRow(KernelSource& ks, ExprGen& eg, const MatBuffer& m,
@@ -856,15 +866,15 @@ void Executor::EmitStream(KernelSource& ks, ExprGen& eg, const Operator& op, con
         } else {
           fetch("q", arr, narr);
         }
-        ks.L("#pragma unroll");
-        ks.Open("for (int u = 0; u < 4; u++)");
-        ks.L("const int64_t r = base + u;");
-        ks.Open("if (r < nrows)");
         load = [&, arr, narr](size_t k) {
           const DevColumn& c = *cols[k];
           std::string v = c.type.id == TypeId::BOOLEAN ? "(" + arr[k] + "[u] != 0)" : arr[k] + "[u]";
           scan[k] = eg.Bind(c.type, v, narr[k].empty() ? "false" : "(" + narr[k] + "[u] != 0)");
         };
+        ks.L("#pragma unroll");
+        ks.Open("for (int u = 0; u < 4; u++)");
+        ks.L("const int64_t r = base + u;");
+        ks.Open("if (r < nrows)");
       } else {
         ks.Open("for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < (int64_t)" + n +
                 "; r += (int64_t)gridDim.x * blockDim.x)");
@@ -970,10 +980,10 @@ void Executor::EmitProbe(KernelSource& ks, ExprGen& eg, const JoinTable& jt,
   std::string h = ks.Fresh("h");
   ks.L("uint32_t " + h + " = " + JoinHash(eg, pk) + ";");
   std::string slots = ks.Ptr(jt.slots, "uint64_t", true);
-  std::string mask = ks.Word(jt.mask);
+  std::string mask = "(uint32_t)" + ks.Word(jt.mask);
   std::string i = ks.Fresh("i"), k = ks.Fresh("k"), e = ks.Fresh("e");
-  ks.L("uint64_t " + i + " = kdb_mix64(" + h + ") & " + mask + ";");
-  ks.Open("for (uint64_t " + k + " = 0; " + k + " <= " + mask + "; " + k + "++, " + i + " = (" + i +
+  ks.L("uint32_t " + i + " = " + h + " & " + mask + ";");
+  ks.Open("for (uint32_t " + k + " = 0; " + k + " <= " + mask + "; " + k + "++, " + i + " = (" + i +
           " + 1) & " + mask + ")");
   ks.L("uint64_t " + e + " = " + slots + "[" + i + "];");
   ks.L("if (" + e + " == 0) break;");
@@ -1001,6 +1011,7 @@ JoinTable Executor::BuildIndex(const MatBuffer& m, const std::vector<int>& key_c
   jt.build = m;
   uint64_t cap = 1024;
   while (cap < static_cast<uint64_t>(m.rows) * 2) cap <<= 1;
+  if (cap > (uint64_t(1) << 31)) throw Error(-5, "join build side of more than 2^30 rows");
   jt.mask = cap - 1;
   jt.slots = arena_.AllocT<uint64_t>(cap);
   ctx_.Memset(jt.slots, 0, cap * sizeof(uint64_t));
@@ -1040,6 +1051,7 @@ JoinTable Executor::BuildGroupedIndex(const MatBuffer& m, int key_col) {
   jt.n = n;
   uint64_t cap = 1024;
   while (cap < static_cast<uint64_t>(n) * 2) cap <<= 1;
+  if (cap > (uint64_t(1) << 31)) throw Error(-5, "join index over more than 2^30 rows");
   jt.mask = cap - 1;
   jt.slots = arena_.AllocT<uint64_t>(cap);
   jt.lens = arena_.AllocT<uint32_t>(cap);
@@ -1080,8 +1092,8 @@ JoinTable Executor::BuildGroupedIndex(const MatBuffer& m, int key_col) {
       ks.L("kdb_join_insert(" + SL + ", " + M + ", (uint32_t)h, (uint32_t)i);");
     } else {
       ks.L("if (i + 1 < (int64_t)" + N + " && " + SH + "[i + 1] == h) continue;");
-      ks.L("uint64_t s = kdb_mix64((uint32_t)h) & " + M + ";");
-      ks.Open("for (uint64_t k = 0; k <= " + M + "; k++, s = (s + 1) & " + M + ")");
+      ks.L("uint32_t s = (uint32_t)h & (uint32_t)" + M + ";");
+      ks.Open("for (uint32_t k = 0; k <= (uint32_t)" + M + "; k++, s = (s + 1) & (uint32_t)" + M + ")");
       ks.L("const uint64_t e = " + SL + "[s];");
       ks.L("if (e == 0) break;");
       ks.Open("if ((uint32_t)(e >> 32) == (uint32_t)h)");
@@ -1285,8 +1297,16 @@ MatBuffer Executor::Materialize(const Operator& op) {
 }
 
 // Emits the per-row update of one aggregate at group slot `g` (atomics).
+// Whether an aggregate needs its per-group count of non-NULL inputs: COUNT
+// and AVG always; SUM, MIN and MAX only to tell an all-NULL group (NULL
+// result), which cannot happen when the input is never NULL.
+bool NeedsCount(const AggPlan& p, const CVal& c) {
+  const bool value_only = p.kind == StateKind::SumF64 || p.kind == StateKind::SumI64 || p.kind == StateKind::MinMaxKey;
+  return !(value_only && c.n == "false");
+}
+
 void EmitGroupUpdate(KernelSource& ks, ExprGen& eg, const AggPlan& p, const CVal& c,
-                     const std::string& sv, const std::string& sc, const std::string& g) {
+                     const std::string& sv, const std::string& sc, const std::string& g, bool count = true) {
   ks.Open("if (!(" + c.n + "))");
   switch (p.kind) {
     case StateKind::SumF64: ks.L("atomicAdd((double*)&" + sv + "[" + g + "], " + c.v + ");"); break;
@@ -1303,19 +1323,22 @@ void EmitGroupUpdate(KernelSource& ks, ExprGen& eg, const AggPlan& p, const CVal
       break;
     case StateKind::Count: break;
   }
-  ks.L("atomicAdd((unsigned long long*)&" + sc + "[" + g + "], 1ULL);");
+  if (count) ks.L("atomicAdd((unsigned long long*)&" + sc + "[" + g + "], 1ULL);");
   ks.Close();
 }
 
 // The aggregate's result value from its state at slot `g`.
+// `counted`: the group's count of non-NULL inputs was kept (NeedsCount);
+// without it a group's SUM / MIN / MAX is never NULL.
 CVal GroupResult(ExprGen& eg, const AggPlan& p, const std::string& sv, const std::string& sc,
-                 const std::string& g, const std::string& first) {
+                 const std::string& g, const std::string& first, bool counted = true) {
   const Type& rt = p.agg->type;
   const Type& ct = p.agg->kid(0).type;
   std::string v = sv + "[" + g + "]", c = "(int64_t)" + sc + "[" + g + "]";
+  const std::string none = counted ? c + " == 0" : "false";
   switch (p.kind) {
-    case StateKind::SumF64: return eg.Bind(rt, "__longlong_as_double((long long)" + v + ")", c + " == 0");
-    case StateKind::SumI64: return eg.Bind(rt, "(" + CType(rt.id) + ")(int64_t)" + v, c + " == 0");
+    case StateKind::SumF64: return eg.Bind(rt, "__longlong_as_double((long long)" + v + ")", none);
+    case StateKind::SumI64: return eg.Bind(rt, "(" + CType(rt.id) + ")(int64_t)" + v, none);
     case StateKind::AvgF64:
       return eg.Bind(rt, "__ddiv_rn(__longlong_as_double((long long)" + v + "), (double)" + c + ")", c + " == 0");
     case StateKind::Count: {
@@ -1323,7 +1346,7 @@ CVal GroupResult(ExprGen& eg, const AggPlan& p, const std::string& sv, const std
       if (p.count_flag >= 0) val = "(" + c + " + (int64_t)((" + first + " >> " + std::to_string(p.count_flag) + ") & 1ULL))";
       return eg.Bind(rt, val, "false");
     }
-    case StateKind::MinMaxKey: return eg.Bind(rt, OKeyInv(ct, v), c + " == 0");
+    case StateKind::MinMaxKey: return eg.Bind(rt, OKeyInv(ct, v), none);
     case StateKind::MinMaxText: return eg.Bind(rt, "kdb_str_from_handle(" + v + ")", c + " == 0");
   }
   throw Error(-1, "bad aggregate");
@@ -1975,6 +1998,7 @@ MatBuffer Executor::RunGroupByBuildRows(const Operator& op, const std::vector<Ag
   const JoinTable& jt = joins_.at(&join);
   const int64_t nb = jt.build.rows;
   const size_t nk = op.group_by.size();
+  std::vector<char> counted(plans.size(), 1);  // per aggregate: NeedsCount, decided at emission
   uint64_t* first = arena_.AllocT<uint64_t>(nb);
   std::vector<uint64_t*> sv(plans.size()), sc(plans.size());
   for (size_t j = 0; j < plans.size(); j++) {
@@ -2028,10 +2052,13 @@ MatBuffer Executor::RunGroupByBuildRows(const Operator& op, const std::vector<Ag
           CVal c = eg.Emit(plans[j].agg->kid(0), s3);
           if (plans[j].count_flag >= 0)
             fl += " | ((" + c.n + ") ? " + std::to_string(1 << plans[j].count_flag) + "ULL : 0ULL)";
-          EmitGroupUpdate(ks, eg, plans[j], c, SV[j], SC[j], g);
+          counted[j] = NeedsCount(plans[j], c);
+          EmitGroupUpdate(ks, eg, plans[j], c, SV[j], SC[j], g, counted[j]);
         }
-        const std::string jpos = "(((uint64_t)(" + pos + ") << 32) | ((" + bpos + ") & 0xffffffffULL))";
-        ks.L("kdb_atomic_min_u64(&" + F + "[" + g + "], (" + jpos + " << 8) | (" + fl + "));");
+        // every row of the group matches the same build row: the first
+        // position is the probe position alone (bits 40 and up)
+        (void)bpos;
+        ks.L("kdb_atomic_min_u64(&" + F + "[" + g + "], ((uint64_t)(" + pos + ") << 40) | (" + fl + "));");
       });
     };
     if (Streamable(join.child(1))) EmitStream(ks, eg, join.child(1), body, src_rows);
@@ -2092,7 +2119,8 @@ MatBuffer Executor::RunGroupByBuildRows(const Operator& op, const std::vector<Ag
       const CVal& c = bv.at(key_cols[k]);
       virt.push_back(eg.Bind(op.group_by[k]->type, c.v, c.n));
     }
-    for (size_t j = 0; j < plans.size(); j++) virt.push_back(GroupResult(eg, plans[j], SV[j], SC[j], "i", "fst"));
+    for (size_t j = 0; j < plans.size(); j++)
+      virt.push_back(GroupResult(eg, plans[j], SV[j], SC[j], "i", "fst", counted[j] != 0));
     Scope sc;
     sc.virt = virt;
     for (size_t c = 0; c < op.output.size(); c++) {
@@ -2117,6 +2145,7 @@ MatBuffer Executor::RunGroupBy(const Operator& op, bool any_order) {
   for (const auto& a : op.aggs) plans.push_back(PlanAgg(*a, flags));
   KeyLayout kl = PlanKeys(ctx_, op.group_by);
   const size_t nk = op.group_by.size();
+  std::vector<char> counted(plans.size(), 1);  // per aggregate: NeedsCount, decided at emission
   {
     // small key domain: register pre-aggregation (no atomics) when the
     // per-thread state (groups x distinct accumulator words) stays small
@@ -2270,7 +2299,8 @@ MatBuffer Executor::RunGroupBy(const Operator& op, bool any_order) {
           CVal c = eg.Emit(plans[j].agg->kid(0), s);
           if (plans[j].count_flag >= 0)
             fl += " | ((" + c.n + ") ? " + std::to_string(1 << plans[j].count_flag) + "ULL : 0ULL)";
-          EmitGroupUpdate(ks, eg, plans[j], c, SV[j], SC[j], g);
+          counted[j] = NeedsCount(plans[j], c);
+          EmitGroupUpdate(ks, eg, plans[j], c, SV[j], SC[j], g, counted[j]);
         }
         ks.L("kdb_atomic_min_u64(&" + F + "[" + g + "], ((uint64_t)(" + pos + ") << 8) | (" + fl + "));");
         ks.Close();
@@ -2371,7 +2401,8 @@ MatBuffer Executor::RunGroupBy(const Operator& op, bool any_order) {
           virt.push_back(eg.Bind(t, v, "(" + KN[k] + "[i] != 0)"));
         }
       }
-      for (size_t j = 0; j < plans.size(); j++) virt.push_back(GroupResult(eg, plans[j], SV[j], SC[j], "i", "fst"));
+      for (size_t j = 0; j < plans.size(); j++)
+        virt.push_back(GroupResult(eg, plans[j], SV[j], SC[j], "i", "fst", counted[j] != 0));
       Scope s;
       s.virt = virt;
       for (size_t c = 0; c < op.output.size(); c++) {
@@ -3314,8 +3345,8 @@ class SkinnerEngine : public JoinEnv {
         std::string SL = ks.Ptr(jt.slots, "uint64_t", true), LN = ks.Ptr(jt.lens, "uint32_t", true);
         std::string M = ks.Word(jt.mask);
         ks.L("const uint32_t h = " + JoinHash(eg, {key}) + ";");
-        ks.L("uint64_t s = kdb_mix64(h) & " + M + ";");
-        ks.Open("for (uint64_t k = 0; k <= " + M + "; k++, s = (s + 1) & " + M + ")");
+        ks.L("uint32_t s = h & (uint32_t)" + M + ";");
+        ks.Open("for (uint32_t k = 0; k <= (uint32_t)" + M + "; k++, s = (s + 1) & (uint32_t)" + M + ")");
         ks.L("const uint64_t e = " + SL + "[s];");
         ks.L("if (e == 0) break;");
         ks.Open("if ((uint32_t)(e >> 32) == h)");
@@ -3549,9 +3580,9 @@ class SkinnerEngine : public JoinEnv {
   }
 
   std::string JoinHash(ExprGen& eg, const std::vector<CVal>& keys) {
-    std::string h = "0x51ed270b27f1a0c9ULL";
-    for (const auto& k : keys) h = "kdb_hash_combine(" + h + ", " + eg.HashOf(k) + ")";
-    return "(uint32_t)((" + h + ") >> 32)";
+    std::string h;
+    for (const auto& k : keys) h = h.empty() ? eg.KeyHash32(k) : "kdb_hash_combine32(" + h + ", " + eg.KeyHash32(k) + ")";
+    return h;
   }
 
   Context& ctx_;

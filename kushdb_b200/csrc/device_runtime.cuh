@@ -158,6 +158,23 @@ KDB_DEV uint64_t kdb_mix64(uint64_t x) {
 KDB_DEV uint64_t kdb_hash_combine(uint64_t h, uint64_t v) {
   return kdb_mix64(h ^ (v + 0x9e3779b97f4a7c15ULL + (h << 6) + (h >> 2)));
 }
+// Join keys hash to 32 bits with murmur3's 32-bit finaliser; a 64-bit value
+// is folded first (low + high * golden ratio), so equal values of any
+// integer width hash alike.  The low bits of the hash index the table.
+KDB_DEV uint32_t kdb_fmix32(uint32_t x) {
+  x ^= x >> 16;
+  x *= 0x85ebca6bu;
+  x ^= x >> 13;
+  x *= 0xc2b2ae35u;
+  x ^= x >> 16;
+  return x;
+}
+KDB_DEV uint32_t kdb_hash64to32(uint64_t v) {
+  return kdb_fmix32((uint32_t)v + (uint32_t)(v >> 32) * 0x9e3779b9u);
+}
+KDB_DEV uint32_t kdb_hash_combine32(uint32_t h, uint32_t v) {
+  return kdb_fmix32(h ^ (v + 0x9e3779b9u + (h << 6) + (h >> 2)));
+}
 KDB_DEV uint64_t kdb_hash_str(kdb_str s) {
   uint64_t h = 0xcbf29ce484222325ULL;  // FNV-1a
   for (int32_t i = 0; i < s.len; i++) {
@@ -253,10 +270,11 @@ KDB_DEV void kdb_atomic_str_minmax(uint64_t* p, kdb_str v, bool is_min) {
 // of two at least twice the build rows, so the table never fills.
 KDB_DEV void kdb_join_insert(uint64_t* slots, uint64_t mask, uint32_t h, uint32_t row) {
   uint64_t e = ((uint64_t)h << 32) | (uint64_t)(row + 1);
-  uint64_t i = kdb_mix64(h) & mask;
-  for (uint64_t k = 0; k <= mask; k++) {
+  const uint32_t m = (uint32_t)mask;  // tables hold at most 2^32 slots
+  uint32_t i = h & m;
+  for (uint32_t k = 0; k <= m; k++) {
     if (atomicCAS((unsigned long long*)&slots[i], 0ULL, (unsigned long long)e) == 0ULL) return;
-    i = (i + 1) & mask;
+    i = (i + 1) & m;
   }
 }
 

@@ -305,10 +305,11 @@ __device__ __forceinline__ bool ItemLess(const SortItem& a, const SortItem& b) {
   return a.key < b.key || (a.key == b.key && a.tie < b.tie);
 }
 
-constexpr int kMergeTile = 2048;    // items per block sort and per merge tile
-constexpr int kMergeThreads = 256;  // threads per block; kMergeTile / kMergeThreads items each
-constexpr int kMergeItems = kMergeTile / kMergeThreads;
-static_assert(kMergeItems == 8, "the register sort network is written for 8 items");
+constexpr int kMergeTile = 2048;  // items per block sort and per merge tile
+// items per thread: the block sort runs 1024 threads of 2 (latency-bound
+// merge rounds want many warps), a merge pass 256 threads of 8
+constexpr int kSortItems = 2;
+constexpr int kPassItems = 8;
 
 // Shared-memory tiles hold one pad item after every 8, so that the 8
 // consecutive items of consecutive threads fall in different banks.
@@ -360,36 +361,49 @@ __device__ __forceinline__ void CompareSwap(SortItem& a, SortItem& b) {
   }
 }
 
-// Batcher's odd-even merge sort network for 8 items (19 comparators).
-__device__ __forceinline__ void SortNetwork8(SortItem (&x)[8]) {
-  CompareSwap(x[0], x[1]); CompareSwap(x[2], x[3]); CompareSwap(x[4], x[5]); CompareSwap(x[6], x[7]);
-  CompareSwap(x[0], x[2]); CompareSwap(x[1], x[3]); CompareSwap(x[4], x[6]); CompareSwap(x[5], x[7]);
-  CompareSwap(x[1], x[2]); CompareSwap(x[5], x[6]);
-  CompareSwap(x[0], x[4]); CompareSwap(x[1], x[5]); CompareSwap(x[2], x[6]); CompareSwap(x[3], x[7]);
-  CompareSwap(x[2], x[4]); CompareSwap(x[3], x[5]);
-  CompareSwap(x[1], x[2]); CompareSwap(x[3], x[4]); CompareSwap(x[5], x[6]);
+// Batcher's odd-even merge sort networks for 2, 4 and 8 items (1, 5 and 19
+// comparators).
+template <int N>
+__device__ __forceinline__ void SortNetwork(SortItem (&x)[N]) {
+  static_assert(N == 2 || N == 4 || N == 8, "sort network size");
+  if constexpr (N == 2) {
+    CompareSwap(x[0], x[1]);
+  } else if constexpr (N == 4) {
+    CompareSwap(x[0], x[1]); CompareSwap(x[2], x[3]);
+    CompareSwap(x[0], x[2]); CompareSwap(x[1], x[3]);
+    CompareSwap(x[1], x[2]);
+  } else {
+    CompareSwap(x[0], x[1]); CompareSwap(x[2], x[3]); CompareSwap(x[4], x[5]); CompareSwap(x[6], x[7]);
+    CompareSwap(x[0], x[2]); CompareSwap(x[1], x[3]); CompareSwap(x[4], x[6]); CompareSwap(x[5], x[7]);
+    CompareSwap(x[1], x[2]); CompareSwap(x[5], x[6]);
+    CompareSwap(x[0], x[4]); CompareSwap(x[1], x[5]); CompareSwap(x[2], x[6]); CompareSwap(x[3], x[7]);
+    CompareSwap(x[2], x[4]); CompareSwap(x[3], x[5]);
+    CompareSwap(x[1], x[2]); CompareSwap(x[3], x[4]); CompareSwap(x[5], x[6]);
+  }
 }
 
 // Sorts each tile of kMergeTile items of `in` into `out` (which may be `in`):
-// every thread sorts 8 items in registers, then eight rounds of merge path in
-// shared memory double the sorted runs from 8 to kMergeTile items.  Missing
-// items of the last tile are maximal padding and never written.
-__global__ void __launch_bounds__(kMergeThreads) BlockSortItems(const SortItem* in, SortItem* out, int64_t n) {
+// every thread sorts ITEMS items in registers, then rounds of merge path in
+// shared memory double the sorted runs from ITEMS to kMergeTile items.
+// Missing items of the last tile are maximal padding and never written.
+template <int ITEMS>
+__global__ void __launch_bounds__(kMergeTile / ITEMS) BlockSortItems(const SortItem* in, SortItem* out, int64_t n) {
+  constexpr int kThreads = kMergeTile / ITEMS;
   __shared__ SortItem s[kPaddedTile];
   const int64_t base = static_cast<int64_t>(blockIdx.x) * kMergeTile;
   const int cnt = static_cast<int>(n - base < kMergeTile ? n - base : kMergeTile);
-  for (int i = threadIdx.x; i < kMergeTile; i += kMergeThreads)
+  for (int i = threadIdx.x; i < kMergeTile; i += kThreads)
     s[Padded(i)] = i < cnt ? in[base + i] : SortItem{~0ULL, ~0u, ~0u};
   __syncthreads();
-  const int d = threadIdx.x * kMergeItems;
-  SortItem x[kMergeItems];
+  const int d = threadIdx.x * ITEMS;
+  SortItem x[ITEMS];
 #pragma unroll
-  for (int k = 0; k < kMergeItems; k++) x[k] = s[Padded(d + k)];
-  SortNetwork8(x);
-  for (int run = kMergeItems; run < kMergeTile; run <<= 1) {
+  for (int k = 0; k < ITEMS; k++) x[k] = s[Padded(d + k)];
+  SortNetwork<ITEMS>(x);
+  for (int run = ITEMS; run < kMergeTile; run <<= 1) {
     __syncthreads();
 #pragma unroll
-    for (int k = 0; k < kMergeItems; k++) s[Padded(d + k)] = x[k];
+    for (int k = 0; k < ITEMS; k++) s[Padded(d + k)] = x[k];
     __syncthreads();
     const int pb = d & ~(2 * run - 1);
     auto at = [&](int i) -> const SortItem& { return s[Padded(pb + i)]; };
@@ -397,25 +411,27 @@ __global__ void __launch_bounds__(kMergeThreads) BlockSortItems(const SortItem* 
     int i = MergePathSplit(at, run, bt, run, d - pb);
     int j = d - pb - i;
 #pragma unroll
-    for (int k = 0; k < kMergeItems; k++) {
+    for (int k = 0; k < ITEMS; k++) {
       const bool take_a = j >= run || (i < run && ItemLess(at(i), bt(j)));
       x[k] = take_a ? at(i++) : bt(j++);
     }
   }
   __syncthreads();
 #pragma unroll
-  for (int k = 0; k < kMergeItems; k++) s[Padded(d + k)] = x[k];
+  for (int k = 0; k < ITEMS; k++) s[Padded(d + k)] = x[k];
   __syncthreads();
-  for (int i = threadIdx.x; i < cnt; i += kMergeThreads) out[base + i] = s[Padded(i)];
+  for (int i = threadIdx.x; i < cnt; i += kThreads) out[base + i] = s[Padded(i)];
 }
 
 // One merge pass: sorted runs of `w` (a multiple of kMergeTile) items merge
 // pairwise into runs of 2w.  Each block makes one tile of kMergeTile
 // outputs: two warps find the tile's first and last merge-path splits in
 // global memory, the block stages the tile's inputs in shared memory with
-// coalesced loads, and every thread merges 8 outputs from there.
-__global__ void __launch_bounds__(kMergeThreads) MergeItems(const SortItem* __restrict__ in,
-                                                            SortItem* __restrict__ out, int64_t n, int64_t w) {
+// coalesced loads, and every thread merges ITEMS outputs from there.
+template <int ITEMS>
+__global__ void __launch_bounds__(kMergeTile / ITEMS) MergeItems(const SortItem* __restrict__ in,
+                                                                 SortItem* __restrict__ out, int64_t n, int64_t w) {
+  constexpr int kThreads = kMergeTile / ITEMS;
   __shared__ SortItem s[kPaddedTile];
   __shared__ int64_t split[2];
   const int64_t o0 = static_cast<int64_t>(blockIdx.x) * kMergeTile;
@@ -437,18 +453,18 @@ __global__ void __launch_bounds__(kMergeThreads) MergeItems(const SortItem* __re
   const int na = static_cast<int>(split[1] - split[0]);
   const int cnt = static_cast<int>(o1 - o0);
   const int nb = cnt - na;
-  for (int i = threadIdx.x; i < cnt; i += kMergeThreads)
+  for (int i = threadIdx.x; i < cnt; i += kThreads)
     s[Padded(i)] = i < na ? A[ia + i] : B[jb + i - na];
   __syncthreads();
-  const int d = threadIdx.x * kMergeItems;
-  SortItem x[kMergeItems];
+  const int d = threadIdx.x * ITEMS;
+  SortItem x[ITEMS];
   if (d < cnt) {
     auto at = [&](int i) -> const SortItem& { return s[Padded(i)]; };
     auto bt = [&](int j) -> const SortItem& { return s[Padded(na + j)]; };
     int i = MergePathSplit(at, na, bt, nb, d);
     int j = d - i;
 #pragma unroll
-    for (int k = 0; k < kMergeItems; k++) {
+    for (int k = 0; k < ITEMS; k++) {
       if (d + k < cnt) {
         const bool take_a = j >= nb || (i < na && ItemLess(at(i), bt(j)));
         x[k] = take_a ? at(i++) : bt(j++);
@@ -457,10 +473,10 @@ __global__ void __launch_bounds__(kMergeThreads) MergeItems(const SortItem* __re
   }
   __syncthreads();
 #pragma unroll
-  for (int k = 0; k < kMergeItems; k++)
+  for (int k = 0; k < ITEMS; k++)
     if (d + k < cnt) s[Padded(d + k)] = x[k];
   __syncthreads();
-  for (int i = threadIdx.x; i < cnt; i += kMergeThreads) out[o0 + i] = s[Padded(i)];
+  for (int i = threadIdx.x; i < cnt; i += kThreads) out[o0 + i] = s[Padded(i)];
 }
 
 __global__ void CopyPairs(const uint64_t* __restrict__ ks, const uint32_t* __restrict__ vs,
@@ -504,7 +520,9 @@ void Context::MergeSortItems(void* items, int64_t n, Arena& arena) {
   SortItem* src = a;
   SortItem* dst = passes % 2 ? b : a;
   TimedStart("sort block");
-  Issue([=](cudaStream_t s) { BlockSortItems<<<static_cast<unsigned>(tiles), kMergeThreads, 0, s>>>(src, dst, n); });
+  Issue([=](cudaStream_t s) {
+    BlockSortItems<kSortItems><<<static_cast<unsigned>(tiles), kMergeTile / kSortItems, 0, s>>>(src, dst, n);
+  });
   TimedStop();
   SortItem* cur = dst;
   SortItem* other = cur == a ? b : a;
@@ -512,7 +530,9 @@ void Context::MergeSortItems(void* items, int64_t n, Arena& arena) {
     const SortItem* in = cur;
     SortItem* out = other;
     TimedStart("sort merge");
-    Issue([=](cudaStream_t s) { MergeItems<<<static_cast<unsigned>(tiles), kMergeThreads, 0, s>>>(in, out, n, w); });
+    Issue([=](cudaStream_t s) {
+      MergeItems<kPassItems><<<static_cast<unsigned>(tiles), kMergeTile / kPassItems, 0, s>>>(in, out, n, w);
+    });
     TimedStop();
     std::swap(cur, other);
   }
