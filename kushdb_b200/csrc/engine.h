@@ -310,9 +310,15 @@ class Context {
 struct PreparedQuery {
   std::unique_ptr<Arena> arena;
   cudaGraphExec_t exec = nullptr;
+  // the recorded launches and memsets: a replay issues them one by one
+  // instead of launching the graph when that measured faster at prepare
+  // time (a short query pays the graph launch's fixed latency)
+  std::vector<std::function<void(cudaStream_t)>> ops;
+  bool direct = false;
   MatBuffer result;
   uint64_t catalog_version = 0;
   int64_t launches = 0;
+  void Replay(cudaStream_t s) const;
   ~PreparedQuery();
 };
 

@@ -12,6 +12,8 @@
 
 #include <algorithm>
 #include <cstdint>
+#include <cstdio>
+#include <cstdlib>
 #include <mutex>
 #include <vector>
 
@@ -305,16 +307,13 @@ __device__ __forceinline__ bool ItemLess(const SortItem& a, const SortItem& b) {
   return a.key < b.key || (a.key == b.key && a.tie < b.tie);
 }
 
-constexpr int kMergeTile = 2048;  // items per block sort and per merge tile
-// items per thread: the block sort runs 1024 threads of 2 (latency-bound
-// merge rounds want many warps), a merge pass 256 threads of 8
-constexpr int kSortItems = 2;
-constexpr int kPassItems = 8;
+constexpr int kMergeTile = 2048;  // largest tile of a block sort or a merge pass
 
 // Shared-memory tiles hold one pad item after every 8, so that the 8
 // consecutive items of consecutive threads fall in different banks.
 __device__ __forceinline__ int Padded(int i) { return i + (i >> 3); }
-constexpr int kPaddedTile = kMergeTile + kMergeTile / 8;
+template <int TILE>
+__host__ __device__ constexpr int PaddedTile() { return TILE + TILE / 8; }
 
 // Number of items of A among the first `diag` outputs of merging A and B,
 // where B's item goes first on equal items.  `at`/`bt` read A[i] and B[j].
@@ -382,17 +381,17 @@ __device__ __forceinline__ void SortNetwork(SortItem (&x)[N]) {
   }
 }
 
-// Sorts each tile of kMergeTile items of `in` into `out` (which may be `in`):
+// Sorts each tile of TILE items of `in` into `out` (which may be `in`):
 // every thread sorts ITEMS items in registers, then rounds of merge path in
-// shared memory double the sorted runs from ITEMS to kMergeTile items.
-// Missing items of the last tile are maximal padding and never written.
-template <int ITEMS>
-__global__ void __launch_bounds__(kMergeTile / ITEMS) BlockSortItems(const SortItem* in, SortItem* out, int64_t n) {
-  constexpr int kThreads = kMergeTile / ITEMS;
-  __shared__ SortItem s[kPaddedTile];
-  const int64_t base = static_cast<int64_t>(blockIdx.x) * kMergeTile;
-  const int cnt = static_cast<int>(n - base < kMergeTile ? n - base : kMergeTile);
-  for (int i = threadIdx.x; i < kMergeTile; i += kThreads)
+// shared memory double the sorted runs from ITEMS to TILE items.  Missing
+// items of the last tile are maximal padding and never written.
+template <int TILE, int ITEMS>
+__global__ void __launch_bounds__(TILE / ITEMS) BlockSortItems(const SortItem* in, SortItem* out, int64_t n) {
+  constexpr int kThreads = TILE / ITEMS;
+  __shared__ SortItem s[PaddedTile<TILE>()];
+  const int64_t base = static_cast<int64_t>(blockIdx.x) * TILE;
+  const int cnt = static_cast<int>(n - base < TILE ? n - base : TILE);
+  for (int i = threadIdx.x; i < TILE; i += kThreads)
     s[Padded(i)] = i < cnt ? in[base + i] : SortItem{~0ULL, ~0u, ~0u};
   __syncthreads();
   const int d = threadIdx.x * ITEMS;
@@ -400,7 +399,7 @@ __global__ void __launch_bounds__(kMergeTile / ITEMS) BlockSortItems(const SortI
 #pragma unroll
   for (int k = 0; k < ITEMS; k++) x[k] = s[Padded(d + k)];
   SortNetwork<ITEMS>(x);
-  for (int run = ITEMS; run < kMergeTile; run <<= 1) {
+  for (int run = ITEMS; run < TILE; run <<= 1) {
     __syncthreads();
 #pragma unroll
     for (int k = 0; k < ITEMS; k++) s[Padded(d + k)] = x[k];
@@ -423,24 +422,24 @@ __global__ void __launch_bounds__(kMergeTile / ITEMS) BlockSortItems(const SortI
   for (int i = threadIdx.x; i < cnt; i += kThreads) out[base + i] = s[Padded(i)];
 }
 
-// One merge pass: sorted runs of `w` (a multiple of kMergeTile) items merge
-// pairwise into runs of 2w.  Each block makes one tile of kMergeTile
+// One merge pass: sorted runs of `w` (a multiple of TILE) items merge
+// pairwise into runs of 2w.  Each block makes one tile of TILE
 // outputs: two warps find the tile's first and last merge-path splits in
 // global memory, the block stages the tile's inputs in shared memory with
 // coalesced loads, and every thread merges ITEMS outputs from there.
-template <int ITEMS>
-__global__ void __launch_bounds__(kMergeTile / ITEMS) MergeItems(const SortItem* __restrict__ in,
-                                                                 SortItem* __restrict__ out, int64_t n, int64_t w) {
-  constexpr int kThreads = kMergeTile / ITEMS;
-  __shared__ SortItem s[kPaddedTile];
+template <int TILE, int ITEMS>
+__global__ void __launch_bounds__(TILE / ITEMS) MergeItems(const SortItem* __restrict__ in,
+                                                           SortItem* __restrict__ out, int64_t n, int64_t w) {
+  constexpr int kThreads = TILE / ITEMS;
+  __shared__ SortItem s[PaddedTile<TILE>()];
   __shared__ int64_t split[2];
-  const int64_t o0 = static_cast<int64_t>(blockIdx.x) * kMergeTile;
+  const int64_t o0 = static_cast<int64_t>(blockIdx.x) * TILE;
   const int64_t base = o0 / (2 * w) * (2 * w);
   const int64_t a_len = w < n - base ? w : n - base;
   const int64_t b0 = base + w;
   const int64_t b_len = b0 < n ? (w < n - b0 ? w : n - b0) : 0;
   const int64_t pair_end = base + a_len + b_len;
-  const int64_t o1 = o0 + kMergeTile < pair_end ? o0 + kMergeTile : pair_end;
+  const int64_t o1 = o0 + TILE < pair_end ? o0 + TILE : pair_end;
   const SortItem* A = in + base;
   const SortItem* B = in + b0;
   const int warp = threadIdx.x >> 5;
@@ -507,32 +506,84 @@ void Context::PackToHost(const PackSegs& segs, size_t total, void* host) {
   KDB_CUDA(cudaMemcpyAsync(host, dst, total, cudaMemcpyDeviceToHost, stream));
 }
 
+// Launch shapes of the two sort kernels: tile size and items per thread.
+struct SortShape {
+  int tile, items;
+};
+
+template <int TILE, int ITEMS>
+void LaunchBlockSort(const SortItem* in, SortItem* out, int64_t n, cudaStream_t s) {
+  BlockSortItems<TILE, ITEMS><<<static_cast<unsigned>((n + TILE - 1) / TILE), TILE / ITEMS, 0, s>>>(in, out, n);
+}
+template <int TILE, int ITEMS>
+void LaunchMerge(const SortItem* in, SortItem* out, int64_t n, int64_t w, cudaStream_t s) {
+  MergeItems<TILE, ITEMS><<<static_cast<unsigned>((n + TILE - 1) / TILE), TILE / ITEMS, 0, s>>>(in, out, n, w);
+}
+
+// KDB_SORT_SHAPE="bt,bi,mt,mi" overrides the shapes (tuning)
+void SortShapes(SortShape* block, SortShape* merge) {
+  // measured on the 134k-item ORDER BY of the Q3-shape query: smaller
+  // tiles give a pass more blocks (latency-bound searches and staging)
+  *block = {1024, 2};
+  *merge = {512, 2};
+  if (const char* e = std::getenv("KDB_SORT_SHAPE")) {
+    int v[4];
+    if (std::sscanf(e, "%d,%d,%d,%d", &v[0], &v[1], &v[2], &v[3]) == 4) {
+      *block = {v[0], v[1]};
+      *merge = {v[2], v[3]};
+    }
+  }
+}
+
 void Context::MergeSortItems(void* items, int64_t n, Arena& arena) {
   if (n <= 1 || dry) return;
   if (n > 0x7fffffffLL) throw Error(-5, "merge sort of more than 2^31 items");
+  SortShape bs, ms;
+  SortShapes(&bs, &ms);
+  auto block_sort = [&]() -> void (*)(const SortItem*, SortItem*, int64_t, cudaStream_t) {
+    switch (bs.tile * 16 + bs.items) {
+      case 2048 * 16 + 2: return LaunchBlockSort<2048, 2>;
+      case 2048 * 16 + 4: return LaunchBlockSort<2048, 4>;
+      case 2048 * 16 + 8: return LaunchBlockSort<2048, 8>;
+      case 1024 * 16 + 2: return LaunchBlockSort<1024, 2>;
+      case 1024 * 16 + 4: return LaunchBlockSort<1024, 4>;
+      case 512 * 16 + 2: return LaunchBlockSort<512, 2>;
+      default: throw Error(-5, "unsupported block sort shape");
+    }
+  }();
+  auto merge = [&]() -> void (*)(const SortItem*, SortItem*, int64_t, int64_t, cudaStream_t) {
+    switch (ms.tile * 16 + ms.items) {
+      case 2048 * 16 + 8: return LaunchMerge<2048, 8>;
+      case 2048 * 16 + 4: return LaunchMerge<2048, 4>;
+      case 2048 * 16 + 2: return LaunchMerge<2048, 2>;
+      case 1024 * 16 + 4: return LaunchMerge<1024, 4>;
+      case 1024 * 16 + 8: return LaunchMerge<1024, 8>;
+      case 512 * 16 + 4: return LaunchMerge<512, 4>;
+      case 512 * 16 + 2: return LaunchMerge<512, 2>;
+      case 256 * 16 + 2: return LaunchMerge<256, 2>;
+      default: throw Error(-5, "unsupported merge shape");
+    }
+  }();
+  // a merge tile must divide every run width
+  if (ms.tile > bs.tile) throw Error(-5, "merge tile larger than the block sort tile");
   SortItem* a = static_cast<SortItem*>(items);
   SortItem* b = reinterpret_cast<SortItem*>(arena.Alloc(sizeof(SortItem) * n));
-  const int64_t tiles = (n + kMergeTile - 1) / kMergeTile;
   int passes = 0;
-  for (int64_t w = kMergeTile; w < n; w <<= 1) passes++;
+  for (int64_t w = bs.tile; w < n; w <<= 1) passes++;
   // with an odd number of merge passes the block sort writes into the
   // scratch buffer, so that the last pass ends in `items` (no copy back)
   SortItem* src = a;
   SortItem* dst = passes % 2 ? b : a;
   TimedStart("sort block");
-  Issue([=](cudaStream_t s) {
-    BlockSortItems<kSortItems><<<static_cast<unsigned>(tiles), kMergeTile / kSortItems, 0, s>>>(src, dst, n);
-  });
+  Issue([=](cudaStream_t s) { block_sort(src, dst, n, s); });
   TimedStop();
   SortItem* cur = dst;
   SortItem* other = cur == a ? b : a;
-  for (int64_t w = kMergeTile; w < n; w <<= 1) {
+  for (int64_t w = bs.tile; w < n; w <<= 1) {
     const SortItem* in = cur;
     SortItem* out = other;
     TimedStart("sort merge");
-    Issue([=](cudaStream_t s) {
-      MergeItems<kPassItems><<<static_cast<unsigned>(tiles), kMergeTile / kPassItems, 0, s>>>(in, out, n, w);
-    });
+    Issue([=](cudaStream_t s) { merge(in, out, n, w, s); });
     TimedStop();
     std::swap(cur, other);
   }
