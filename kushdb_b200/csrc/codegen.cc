@@ -3868,6 +3868,23 @@ HostResult ExecutePlan(Context& ctx, const plan::Operator& root, std::unique_ptr
   const bool prepare = prepared != nullptr && !ctx.profile;
   if (prepare && *prepared) {
     PreparedQuery& pq = **prepared;
+    if (pq.catalog_version == ctx.catalog_version && !pq.exec && !pq.direct) {
+      // first replay: capture the recorded launches as a graph and choose
+      // between the graph and the launches themselves
+      cudaGraph_t g = nullptr;
+      KDB_CUDA(cudaStreamBeginCapture(ctx.stream, cudaStreamCaptureModeThreadLocal));
+      for (auto& op : pq.ops) op(ctx.stream);
+      KDB_CUDA(cudaStreamEndCapture(ctx.stream, &g));
+      cudaError_t ie = cudaGraphInstantiate(&pq.exec, g, 0);
+      cudaGraphDestroy(g);
+      if (ie != cudaSuccess) {
+        cudaGetLastError();
+        pq.exec = nullptr;
+        pq.direct = true;
+      } else {
+        ChooseReplay(ctx, pq);
+      }
+    }
     if (pq.catalog_version == ctx.catalog_version) {
       // replay: one graph launch (or the recorded launches), then the
       // result download
@@ -3909,23 +3926,14 @@ HostResult ExecutePlan(Context& ctx, const plan::Operator& root, std::unique_ptr
   }
   timer.Done();
   if (prepare && rec.replayable && pq->arena->bytes() <= kMaxPreparedBytes) {
-    cudaGraph_t g = nullptr;
-    KDB_CUDA(cudaStreamBeginCapture(ctx.stream, cudaStreamCaptureModeThreadLocal));
-    for (auto& op : rec.ops) op(ctx.stream);
-    KDB_CUDA(cudaStreamEndCapture(ctx.stream, &g));
-    cudaError_t ie = cudaGraphInstantiate(&pq->exec, g, 0);
-    cudaGraphDestroy(g);
-    if (ie == cudaSuccess) {
-      pq->result = m;
-      pq->catalog_version = ctx.catalog_version;
-      pq->launches = rec.launches;
-      pq->ops = std::move(rec.ops);
-      ChooseReplay(ctx, *pq);
-      *prepared = std::move(pq);
-    } else {
-      cudaGetLastError();
-      pq->exec = nullptr;
-    }
+    // the graph is built on the first replay: a plan that never repeats
+    // over the same tables (tables re-uploaded before every run) pays only
+    // for recording the launches
+    pq->result = m;
+    pq->catalog_version = ctx.catalog_version;
+    pq->launches = rec.launches;
+    pq->ops = std::move(rec.ops);
+    *prepared = std::move(pq);
   }
   return r;
 }
