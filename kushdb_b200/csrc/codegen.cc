@@ -157,9 +157,12 @@ class KernelSource {
   }
 
   std::string Kernel(const std::string& name, int block, int min_blocks = 1) const {
+    int words = 16;
+    while (words < static_cast<int>(args.size())) words *= 2;
+    if (words > 384) words = 384;
     std::ostringstream o;
     o << globals.str() << "\nextern \"C\" __global__ void __launch_bounds__(" << block << ", " << min_blocks
-      << ") " << name << "(KArgs a) {\n"
+      << ") " << name << "(KArgsN<" << words << "> a) {\n"
       << pre.str() << body.str() << "}\n";
     return o.str();
   }

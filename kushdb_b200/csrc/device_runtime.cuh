@@ -33,6 +33,12 @@ typedef unsigned long long uint64_t;
 struct KArgs {
   uint64_t w[384];
 };
+// A kernel's parameter block holds only the words it uses (rounded up): the
+// launch copies sizeof(parameter) bytes, and a 3 KB block costs launch time.
+template <int N>
+struct KArgsN {
+  uint64_t w[N];
+};
 
 // A TEXT value: pointer into device column data (or a kernel literal) + length.
 struct kdb_str {
