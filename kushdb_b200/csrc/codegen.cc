@@ -555,6 +555,17 @@ struct JoinTable {
   MatBuffer build;
   uint64_t* slots = nullptr;
   uint64_t mask = 0;
+  // one-bit-per-position filter of the build keys' hashes (about 8 bits per
+  // build row, 2^bloom_log2 bits): a probe whose bit is clear skips the
+  // table; the filter is small enough to stay in L1 / L2 where the table
+  // does not
+  uint32_t* bloom = nullptr;
+  int bloom_log2 = 0;
+  // one 32-bit-or-narrower build key: the slot holds the key itself in its
+  // high word (instead of the hash), so a probe compares it there and never
+  // loads the build row's key; `key_col` is that column
+  bool key_in_slot = false;
+  int key_col = -1;
   // grouped form (Skinner indexes): rows sorted by key hash (`srow`, with
   // their hashes `sh`), and `slots` holding one entry per distinct hash
   // (hash << 32 | first sorted index + 1) with the group's length in `lens`
@@ -985,25 +996,42 @@ void Executor::EmitProbe(KernelSource& ks, ExprGen& eg, const JoinTable& jt,
   ks.L("uint32_t " + h + " = " + JoinHash(eg, pk) + ";");
   std::string slots = ks.Ptr(jt.slots, "uint64_t", true);
   std::string mask = "(uint32_t)" + ks.Word(jt.mask);
+  if (jt.bloom)
+    ks.Open("if (kdb_bloom_test(" + ks.Ptr(jt.bloom, "uint32_t", true) + ", " + h + ", " +
+            std::to_string(jt.bloom_log2) + "))");
   std::string i = ks.Fresh("i"), k = ks.Fresh("k"), e = ks.Fresh("e");
   ks.L("uint32_t " + i + " = " + h + " & " + mask + ";");
   ks.Open("for (uint32_t " + k + " = 0; " + k + " <= " + mask + "; " + k + "++, " + i + " = (" + i +
           " + 1) & " + mask + ")");
   ks.L("uint64_t " + e + " = " + slots + "[" + i + "];");
   ks.L("if (" + e + " == 0) break;");
-  ks.Open("if ((uint32_t)(" + e + " >> 32) == " + h + ")");
   std::string br = ks.Fresh("br");
-  ks.L("int64_t " + br + " = (int64_t)(uint32_t)" + e + " - 1;");
-  auto left = LoadMatRow(ks, eg, jt.build, br, nullptr);
-  std::string eq = "true";
-  for (size_t j = 0; j < bkeys.size(); j++) eq += " && " + eg.EqOf(left.at(bkeys[j]), pk[j]);
-  ks.Open("if (" + eq + ")");
+  std::vector<CVal> left;
+  if (jt.key_in_slot && bkeys.size() == 1 && bkeys[0] == jt.key_col && pk[0].type.id != TypeId::REAL &&
+      pk[0].type.id != TypeId::TEXT && pk[0].type.id != TypeId::BOOLEAN) {
+    // the stored key, sign-extended, against the probe value in 64 bits
+    ks.Open("if ((int64_t)(int32_t)(uint32_t)(" + e + " >> 32) == (int64_t)(" + pk[0].v + "))");
+    ks.L("int64_t " + br + " = (int64_t)(uint32_t)" + e + " - 1;");
+    left = LoadMatRow(ks, eg, jt.build, br, nullptr);
+    const MatCol& kc = jt.build.cols.at(jt.key_col);
+    left.at(jt.key_col) = eg.Bind(kc.type, "(" + CType(kc.type.id) + ")(" + pk[0].v + ")", "false");
+    ks.Open("");
+  } else {
+    if (jt.key_in_slot) throw Error(-5, "join probe does not match its key-in-slot table");
+    ks.Open("if ((uint32_t)(" + e + " >> 32) == " + h + ")");
+    ks.L("int64_t " + br + " = (int64_t)(uint32_t)" + e + " - 1;");
+    left = LoadMatRow(ks, eg, jt.build, br, nullptr);
+    std::string eq = "true";
+    for (size_t j = 0; j < bkeys.size(); j++) eq += " && " + eg.EqOf(left.at(bkeys[j]), pk[j]);
+    ks.Open("if (" + eq + ")");
+  }
   std::string bpos = ks.Ptr(jt.build.pos, "uint64_t", true) + "[" + br + "]";
   probe_br_ = br;
   on_match(left, bpos);
   ks.Close();
   ks.Close();
   ks.Close();
+  if (jt.bloom) ks.Close();
   ks.Close();
 }
 
@@ -1019,12 +1047,25 @@ JoinTable Executor::BuildIndex(const MatBuffer& m, const std::vector<int>& key_c
   jt.mask = cap - 1;
   jt.slots = arena_.AllocT<uint64_t>(cap);
   ctx_.Memset(jt.slots, 0, cap * sizeof(uint64_t));
+  if (!std::getenv("KDB_NO_JOIN_FILTER")) {
+    jt.bloom_log2 = 14;
+    while (jt.bloom_log2 < 26 && (int64_t(1) << jt.bloom_log2) < m.rows * 8) jt.bloom_log2++;
+    const size_t words = (size_t(1) << jt.bloom_log2) / 32;
+    jt.bloom = arena_.AllocT<uint32_t>(words);
+    ctx_.Memset(jt.bloom, 0, words * sizeof(uint32_t));
+  }
+  if (key_cols.size() == 1 && !std::getenv("KDB_NO_KEY_IN_SLOT")) {
+    const TypeId t = m.cols.at(key_cols[0]).type.id;
+    jt.key_in_slot = t == TypeId::INT || t == TypeId::DATE || t == TypeId::ENUM || t == TypeId::SMALLINT;
+    jt.key_col = key_cols[0];
+  }
   if (m.rows == 0) return jt;
   KernelSource ks;
   ExprGen eg(ctx_, ks);
   std::string n = ks.Word(static_cast<uint64_t>(m.rows));
   std::string slots = ks.Ptr(jt.slots, "uint64_t");
   std::string mask = ks.Word(jt.mask);
+  std::string bloom = jt.bloom ? ks.Ptr(jt.bloom, "uint32_t") : "";
   ks.Open("for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < (int64_t)" + n +
           "; r += (int64_t)gridDim.x * blockDim.x)");
   auto vals = LoadMatRow(ks, eg, m, "r", nullptr);
@@ -1035,7 +1076,12 @@ JoinTable Executor::BuildIndex(const MatBuffer& m, const std::vector<int>& key_c
     nn += " && !(" + vals.at(c).n + ")";
   }
   ks.Open("if (" + nn + ")");
-  ks.L("kdb_join_insert(" + slots + ", " + mask + ", " + JoinHash(eg, keys) + ", (uint32_t)r);");
+  ks.L("const uint32_t h = " + JoinHash(eg, keys) + ";");
+  if (jt.key_in_slot)
+    ks.L("kdb_join_insert_keyed(" + slots + ", " + mask + ", h, (uint32_t)(int32_t)" + keys[0].v + ", (uint32_t)r);");
+  else
+    ks.L("kdb_join_insert(" + slots + ", " + mask + ", h, (uint32_t)r);");
+  if (jt.bloom) ks.L("kdb_bloom_set(" + bloom + ", h, " + std::to_string(jt.bloom_log2) + ");");
   ks.Close();
   ks.Close();
   LaunchPipeline(ks, m.rows, "join build");

@@ -274,6 +274,29 @@ KDB_DEV void kdb_atomic_str_minmax(uint64_t* p, kdb_str v, bool is_min) {
 // Entry = (hash32 << 32) | (row + 1); 0 = empty.  Duplicate keys are separate
 // entries (a probe walks the run until an empty slot).  Capacity is a power
 // of two at least twice the build rows, so the table never fills.
+// Join filter: one bit per 32-bit hash, placed by the hash's multiplicative
+// remix (top bits), independent of the table index (its low bits).
+KDB_DEV uint32_t kdb_bloom_bit(uint32_t h, int log2_bits) { return (h * 0x9e3779b1u) >> (32 - log2_bits); }
+KDB_DEV void kdb_bloom_set(uint32_t* bits, uint32_t h, int log2_bits) {
+  const uint32_t b = kdb_bloom_bit(h, log2_bits);
+  atomicOr(&bits[b >> 5], 1u << (b & 31));
+}
+KDB_DEV bool kdb_bloom_test(const uint32_t* __restrict__ bits, uint32_t h, int log2_bits) {
+  const uint32_t b = kdb_bloom_bit(h, log2_bits);
+  return (__ldg(&bits[b >> 5]) >> (b & 31)) & 1u;
+}
+
+// Same, storing the (32-bit) key in the slot's high word instead of the hash.
+KDB_DEV void kdb_join_insert_keyed(uint64_t* slots, uint64_t mask, uint32_t h, uint32_t key, uint32_t row) {
+  uint64_t e = ((uint64_t)key << 32) | (uint64_t)(row + 1);
+  const uint32_t m = (uint32_t)mask;
+  uint32_t i = h & m;
+  for (uint32_t k = 0; k <= m; k++) {
+    if (atomicCAS((unsigned long long*)&slots[i], 0ULL, (unsigned long long)e) == 0ULL) return;
+    i = (i + 1) & m;
+  }
+}
+
 KDB_DEV void kdb_join_insert(uint64_t* slots, uint64_t mask, uint32_t h, uint32_t row) {
   uint64_t e = ((uint64_t)h << 32) | (uint64_t)(row + 1);
   const uint32_t m = (uint32_t)mask;  // tables hold at most 2^32 slots
