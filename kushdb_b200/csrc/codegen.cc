@@ -705,6 +705,11 @@ class Executor {
   JoinTable BuildIndex(const MatBuffer& m, const std::vector<int>& key_cols);
   JoinTable BuildGroupedIndex(const MatBuffer& m, int key_col);
   std::string probe_br_;  // inside an on_match callback: the matched build row's index
+  // set while emitting a join's probe side: its scan takes one row per
+  // thread per iteration (the probe's dependent table accesses, not the
+  // column loads, bound such a pipeline, and the 4-row vector's registers
+  // cost occupancy)
+  bool probe_side_scan_ = false;
   void EmitProbe(KernelSource& ks, ExprGen& eg, const JoinTable& jt,
                  const std::vector<int>& build_key_cols, const std::vector<CVal>& probe_keys,
                  const std::function<void(const std::vector<CVal>&, const std::string&)>& on_match);
@@ -816,7 +821,9 @@ void Executor::EmitStream(KernelSource& ks, ExprGen& eg, const Operator& op, con
       }
       bool any_text = false;
       for (const DevColumn* c : cols) any_text |= c->type.id == TypeId::TEXT;
-      const bool vec = !any_text && !std::getenv("KDB_NO_VECTOR_SCAN");
+      const bool probe_side = probe_side_scan_;
+      probe_side_scan_ = false;
+      const bool vec = !any_text && !probe_side && !std::getenv("KDB_NO_VECTOR_SCAN");
       std::vector<CVal> scan(cols.size());
       std::function<void(size_t)> load;
       if (vec) {
@@ -974,8 +981,10 @@ void Executor::EmitStream(KernelSource& ks, ExprGen& eg, const Operator& op, con
           consume(out, "((" + pos + ") << 32) | ((" + bpos + ") & 0xffffffffULL)");
         });
       };
+      probe_side_scan_ = !std::getenv("KDB_VECTOR_PROBE_SCAN");
       if (Streamable(op.child(1))) EmitStream(ks, eg, op.child(1), body, src_rows);
       else EmitMatScan(ks, mats_.at(&op.child(1)), nullptr, body, src_rows);
+      probe_side_scan_ = false;
       return;
     }
     default: {
@@ -1738,9 +1747,11 @@ MatBuffer Executor::RunGroupByDense(const Operator& op, const std::vector<AggPla
   const int W = static_cast<int>(words.size());
   const int64_t K = D * W;
   // block size and the launch-bounds occupancy hint (env overrides for tuning)
-  const int block = std::getenv("KDB_DENSE_BLOCK") ? std::atoi(std::getenv("KDB_DENSE_BLOCK")) : 128;
-  const int min_blocks = std::getenv("KDB_DENSE_MINB") ? std::atoi(std::getenv("KDB_DENSE_MINB")) : 2;
-  const int grid_per_sm = std::getenv("KDB_DENSE_GRID") ? std::atoi(std::getenv("KDB_DENSE_GRID")) : 4;
+  // (64 threads, 6 CTAs per SM: measured best on the Q1 shape among 64/128
+  // threads and 2-8 CTAs per SM)
+  const int block = std::getenv("KDB_DENSE_BLOCK") ? std::atoi(std::getenv("KDB_DENSE_BLOCK")) : 64;
+  const int min_blocks = std::getenv("KDB_DENSE_MINB") ? std::atoi(std::getenv("KDB_DENSE_MINB")) : 6;
+  const int grid_per_sm = std::getenv("KDB_DENSE_GRID") ? std::atoi(std::getenv("KDB_DENSE_GRID")) : 6;
   // Accumulators in registers (every row updates every group's words under a
   // predicate) or, for larger groups x words, in per-thread shared-memory
   // slots indexed by the group id (a row touches only its own group's words).
@@ -2111,8 +2122,10 @@ MatBuffer Executor::RunGroupByBuildRows(const Operator& op, const std::vector<Ag
         ks.L("kdb_atomic_min_u64(&" + F + "[" + g + "], ((uint64_t)(" + pos + ") << 40) | (" + fl + "));");
       });
     };
+    probe_side_scan_ = !std::getenv("KDB_VECTOR_PROBE_SCAN");
     if (Streamable(join.child(1))) EmitStream(ks, eg, join.child(1), body, src_rows);
     else EmitMatScan(ks, mats_.at(&join.child(1)), nullptr, body, src_rows);
+    probe_side_scan_ = false;
     LaunchPipeline(ks, src_rows, "group by");
   }
   ctx_.CheckDeviceError("group by");

@@ -523,9 +523,9 @@ void LaunchMerge(const SortItem* in, SortItem* out, int64_t n, int64_t w, cudaSt
 // KDB_SORT_SHAPE="bt,bi,mt,mi" overrides the shapes (tuning)
 void SortShapes(SortShape* block, SortShape* merge) {
   // measured on the 134k-item ORDER BY of the Q3-shape query: smaller
-  // tiles give a pass more blocks (latency-bound searches and staging)
+  // merge tiles give a pass more blocks (latency-bound searches and staging)
   *block = {1024, 2};
-  *merge = {512, 2};
+  *merge = {256, 2};
   if (const char* e = std::getenv("KDB_SORT_SHAPE")) {
     int v[4];
     if (std::sscanf(e, "%d,%d,%d,%d", &v[0], &v[1], &v[2], &v[3]) == 4) {
