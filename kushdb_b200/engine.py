@@ -212,7 +212,7 @@ class Engine:
             n = self.lib.kdb_result_num_rows(h)
             self.lib.kdb_result_free(h)
             return n
-        return Result.from_handle(self.lib, "kdb_", self.ctx, h)
+        return Result.from_handle(self.lib, "kdb_", self.ctx, h, owner=self)
 
     def set_prepared_queries(self, on: bool) -> None:
         """Replay repeated plans as recorded CUDA graphs (default on)."""
@@ -382,7 +382,7 @@ class Server:
         if rc == 1:
             return None
         self.engine._check(rc)
-        return Result.from_handle(self.lib, "kdb_", self.engine.ctx, h)
+        return Result.from_handle(self.lib, "kdb_", self.engine.ctx, h, owner=self.engine)
 
     def wait(self, ticket: int, timeout_s: float = 600.0):
         import time

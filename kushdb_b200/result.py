@@ -56,9 +56,12 @@ class Result:
         return [None if c.nulls[r] else c.values[r] for c in self.columns]
 
     @staticmethod
-    def from_handle(lib, prefix: str, ctx, handle) -> "Result":
-        """Takes ownership of `handle`."""
+    def from_handle(lib, prefix: str, ctx, handle, owner=None) -> "Result":
+        """Takes ownership of `handle`.  `owner` is the engine that made it:
+        the printer-format lines need its enum dictionaries, so they are read
+        only while it is open (the columns stay readable after it closed)."""
         res = Result()
+        res._owner = owner
         res._src = (lib, prefix, ctx, ctypes.c_void_p(handle.value if hasattr(handle, "value") else handle))
         return res
 
@@ -109,6 +112,10 @@ class Result:
 
     def _read_lines(self) -> List[str]:
         lib, prefix, ctx, handle = self._src
+        owner = getattr(self, "_owner", None)
+        if owner is not None and getattr(owner, "ctx", None) is None:
+            raise RuntimeError("result lines are formatted with the engine's enum dictionaries: "
+                               "read them before closing the engine")
         f = lambda n: getattr(lib, prefix + n)  # noqa: E731
         need = f("result_format")(ctx, handle, None, 0)
         tbuf = ctypes.create_string_buffer(int(need))
