@@ -3186,6 +3186,11 @@ class SkinnerEngine : public JoinEnv {
     if (!empty) {
       beg_ = arena_.AllocT<uint64_t>(kMaxSlice);
       offs_ = arena_.AllocT<uint64_t>(kMaxSlice + 1);
+      deep_ = T_ > 2 && !std::getenv("KDB_SKINNER_DEPTH1");
+      if (deep_) {
+        beg2_ = arena_.AllocT<uint64_t>(kMaxItems2);
+        offs2_ = arena_.AllocT<uint64_t>(kMaxItems2 + 1);
+      }
       Generate();
       std::vector<int> order(T_);
       for (size_t i = 0; i < prefix.size(); i++) order[i] = prefix[i];
@@ -3296,8 +3301,19 @@ class SkinnerEngine : public JoinEnv {
       ctx_.Launch(fn_, ctx_.GridFor(len, 128), 128, a, 0, T_ > 1 ? "skinner expand" : "skinner episode");
       if (T_ > 1) {
         ctx_.ScanU64(offs_, len);
-        a.w[w_phase_] = 1;
-        ctx_.Launch(fn_, ctx_.num_sms * 8, 128, a, 0, "skinner episode");
+        if (deep_) {
+          // position-1 items expand their position-2 runs (or, past
+          // kMaxItems2 items, run depth-first as below); then every
+          // position-2 candidate is an item of its own
+          a.w[w_phase_] = 2;
+          ctx_.Launch(fn_, ctx_.num_sms * 8, 128, a, 0, "skinner expand2");
+          ctx_.ScanU64Bounded(offs2_, offs_ + len, kMaxItems2);
+          a.w[w_phase_] = 3;
+          ctx_.Launch(fn_, ctx_.num_sms * 8, 128, a, 0, "skinner episode");
+        } else {
+          a.w[w_phase_] = 1;
+          ctx_.Launch(fn_, ctx_.num_sms * 8, 128, a, 0, "skinner episode");
+        }
       }
       uint64_t cw[2] = {0, 0};
       ctx_.D2H(&cw[0], count_, sizeof(uint64_t));
@@ -3534,7 +3550,7 @@ class SkinnerEngine : public JoinEnv {
     ks.Close();
     ks.Close();
     if (T > 1) {
-      ks.Open("else");
+      ks.Open("else if (phase == 1)");
       ks.L("const int64_t m = s1 - s0;");
       ks.L("const uint64_t total = " + OF + "[m];");
       ks.Open("for (uint64_t w = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; w < total; w += (uint64_t)gridDim.x * blockDim.x)");
@@ -3548,11 +3564,11 @@ class SkinnerEngine : public JoinEnv {
       ks.L("if (c1 < 0 || c1 < off[ord[1]]) continue;");
       ks.L("rows[ord[1]] = c1; work++;");
       ks.L("if (!conds_ok(sched[1])) continue;");
-      if (T == 2) {
-        ks.L("emit();");
-      } else {
-        ks.L("int p = 2; init(2);");
-        ks.Open("while (p >= 2)");
+      // depth-first over positions from..T-1, the earlier ones bound
+      auto depth_first = [&](int from) {
+        const std::string F = std::to_string(from);
+        ks.L("int p = " + F + "; init(" + F + ");");
+        ks.Open("while (p >= " + F + ")");
         ks.L("int64_t c = next(p);");
         ks.Open("if (c < 0)");
         ks.L("p--;");
@@ -3570,9 +3586,83 @@ class SkinnerEngine : public JoinEnv {
         ks.L("init(p);");
         ks.Close();
         ks.Close();
+      };
+      if (T == 2) {
+        ks.L("emit();");
+      } else {
+        depth_first(2);
       }
       ks.Close();
       ks.Close();
+      if (T > 2 && deep_) {
+        // Phase 2: every position-1 item records its position-2 run (when
+        // the items fit kMaxItems2; otherwise it finishes depth-first here).
+        // Phase 3, after a scan of those lengths: every position-2
+        // candidate is a work item, so a position-1 item whose key is hot
+        // at position 2 is shared by the grid instead of one thread.
+        std::string B2 = ks.Ptr(beg2_, "uint64_t"), O2 = ks.Ptr(offs2_, "uint64_t");
+        std::string CAP2 = "(uint64_t)" + ks.Word(static_cast<uint64_t>(kMaxItems2));
+        ks.Open("else if (phase == 2)");
+        ks.L("const int64_t m = s1 - s0;");
+        ks.L("const uint64_t total = " + OF + "[m];");
+        ks.L("const bool fits = total <= " + CAP2 + ";");
+        ks.Open("for (uint64_t w = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; w < total; w += (uint64_t)gridDim.x * blockDim.x)");
+        ks.L("uint64_t len2 = 0;");
+        ks.Open("");
+        ks.L("int64_t lo = 0, hi = m - 1;");
+        ks.Open("while (lo < hi)");
+        ks.L("const int64_t mid = (lo + hi + 1) >> 1;");
+        ks.L("if (" + OF + "[mid] <= w) lo = mid; else hi = mid - 1;");
+        ks.Close();
+        ks.L("rows[ord[0]] = s0 + lo;");
+        ks.L("const int64_t c1 = cand(1, (int64_t)(" + BG + "[lo] + (w - " + OF + "[lo])));");
+        ks.Open("if (c1 >= 0 && c1 >= off[ord[1]])");
+        ks.L("rows[ord[1]] = c1; work++;");
+        ks.Open("if (conds_ok(sched[1]))");
+        ks.Open("if (fits)");
+        ks.L("init(2);");
+        ks.L(B2 + "[w] = (uint64_t)iti[2];");
+        ks.L("len2 = (uint64_t)(ite[2] - iti[2]);");
+        ks.Close();
+        ks.Open("else");
+        depth_first(2);
+        ks.Close();
+        ks.Close();
+        ks.Close();
+        ks.Close();
+        ks.L("if (fits) " + O2 + "[w] = len2;");
+        ks.Close();
+        ks.Close();
+        ks.Open("else if (phase == 3)");
+        ks.L("const int64_t m = s1 - s0;");
+        ks.L("const uint64_t total = " + OF + "[m];");
+        ks.Open("if (total <= " + CAP2 + " && total > 0)");
+        ks.L("const uint64_t total2 = " + O2 + "[total];");
+        ks.Open("for (uint64_t w2 = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; w2 < total2; w2 += (uint64_t)gridDim.x * blockDim.x)");
+        ks.L("int64_t lo1 = 0, hi1 = (int64_t)total - 1;");
+        ks.Open("while (lo1 < hi1)");
+        ks.L("const int64_t mid = (lo1 + hi1 + 1) >> 1;");
+        ks.L("if (" + O2 + "[mid] <= w2) lo1 = mid; else hi1 = mid - 1;");
+        ks.Close();
+        ks.L("const uint64_t w = (uint64_t)lo1;");
+        ks.L("int64_t lo = 0, hi = m - 1;");
+        ks.Open("while (lo < hi)");
+        ks.L("const int64_t mid = (lo + hi + 1) >> 1;");
+        ks.L("if (" + OF + "[mid] <= w) lo = mid; else hi = mid - 1;");
+        ks.Close();
+        ks.L("rows[ord[0]] = s0 + lo;");
+        // the item had a non-empty run: its position-1 candidate is valid
+        ks.L("rows[ord[1]] = cand(1, (int64_t)(" + BG + "[lo] + (w - " + OF + "[lo])));");
+        ks.L("const int64_t c2 = cand(2, (int64_t)(" + B2 + "[w] + (w2 - " + O2 + "[w])));");
+        ks.L("if (c2 < 0 || c2 < off[ord[2]]) continue;");
+        ks.L("rows[ord[2]] = c2; work++;");
+        ks.L("if (!conds_ok(sched[2])) continue;");
+        if (T == 3) ks.L("emit();");
+        else depth_first(3);
+        ks.Close();
+        ks.Close();
+        ks.Close();
+      }
     }
     std::string wk = ks.Ptr(work_, "unsigned long long");
     ks.L("if (work) atomicAdd(" + wk + ", work);");
@@ -3677,6 +3767,11 @@ class SkinnerEngine : public JoinEnv {
   int w_order_ = 0, w_lookup_ = 0, w_sched_ = 0, w_off_ = 0, w_s0_ = 0, w_s1_ = 0, w_cap_ = 0, w_count_ = 0,
       w_pos_ = 0, w_phase_ = 0;
   static constexpr int64_t kMaxSlice = 1 << 20;  // leftmost tuples per episode
+  // position-1 items of an episode that can be expanded to position 2
+  static constexpr int64_t kMaxItems2 = 1 << 20;
+  bool deep_ = false;
+  uint64_t* beg2_ = nullptr;   // per position-1 item: first position-2 candidate
+  uint64_t* offs2_ = nullptr;  // per position-1 item: candidate count, then its exclusive prefix
   uint64_t* beg_ = nullptr;   // per slice tuple: first position-1 candidate
   uint64_t* offs_ = nullptr;  // per slice tuple: candidate count, then its exclusive prefix
   std::vector<int> out_ptr_words_;

@@ -287,6 +287,8 @@ class Context {
   void MergeSortItems(void* items, int64_t n, Arena& arena);
   // exclusive prefix sum of a[0..n) in place, the total into a[n]
   void ScanU64(uint64_t* a, int64_t n, const char* tag = "skinner scan");
+  // the same over *n_ptr elements (a device word), skipped when *n_ptr > cap
+  void ScanU64Bounded(uint64_t* a, const uint64_t* n_ptr, int64_t cap, const char* tag = "skinner scan");
   // gathers the segments into the device staging buffer and queues one copy
   // of `total` bytes to `host` (pinned); the caller synchronises
   void PackToHost(const PackSegs& segs, size_t total, void* host);

@@ -148,6 +148,16 @@ __global__ void __launch_bounds__(1024) ExclusiveScanU64(uint64_t* __restrict__ 
                                            reinterpret_cast<unsigned long long*>(a) + n);
 }
 
+// The same with the count read on the device (*n_ptr); nothing is done when
+// it exceeds `cap` (the array's capacity).
+__global__ void __launch_bounds__(1024) ExclusiveScanU64Bounded(uint64_t* __restrict__ a,
+                                                                const uint64_t* __restrict__ n_ptr, int64_t cap) {
+  const int64_t n = static_cast<int64_t>(*n_ptr);
+  if (n > cap) return;
+  BlockScanTiles<unsigned long long, 8>(reinterpret_cast<unsigned long long*>(a), n,
+                                           reinterpret_cast<unsigned long long*>(a) + n);
+}
+
 // Stable scatter: each block walks its tile in chunks of blockDim items in
 // order; ranks inside a chunk come from a warp match plus per-warp digit
 // counts prefixed in warp order.
@@ -587,6 +597,14 @@ void Context::MergeSortItems(void* items, int64_t n, Arena& arena) {
     TimedStop();
     std::swap(cur, other);
   }
+  KDB_CUDA(cudaGetLastError());
+}
+
+void Context::ScanU64Bounded(uint64_t* a, const uint64_t* n_ptr, int64_t cap, const char* tag) {
+  if (dry) return;
+  TimedStart(tag);
+  Issue([=](cudaStream_t s) { ExclusiveScanU64Bounded<<<1, 1024, 0, s>>>(a, n_ptr, cap); });
+  TimedStop();
   KDB_CUDA(cudaGetLastError());
 }
 
