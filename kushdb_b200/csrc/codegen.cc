@@ -3176,10 +3176,12 @@ class SkinnerEngine : public JoinEnv {
     } else {
       out_ = alloc_out_(1 << 12);
     }
-    count_ = arena_.AllocT<uint64_t>(1);
-    work_ = arena_.AllocT<uint64_t>(1);
-    ctx_.Memset(count_, 0, sizeof(uint64_t));
-    ctx_.Memset(work_, 0, sizeof(uint64_t));
+    // result count, work, then the two task queues' counts (read together)
+    stats_ = arena_.AllocT<uint64_t>(4);
+    ctx_.Memset(stats_, 0, 4 * sizeof(uint64_t));
+    count_ = stats_;
+    work_ = stats_ + 1;
+    tcount_ = stats_ + 2;
     produced_ = 0;
     bool empty = false;
     for (int64_t c : cards_) empty |= c == 0;
@@ -3191,6 +3193,11 @@ class SkinnerEngine : public JoinEnv {
         beg2_ = arena_.AllocT<uint64_t>(kMaxItems2);
         offs2_ = arena_.AllocT<uint64_t>(kMaxItems2 + 1);
       }
+      split_ = T_ > 2 && !std::getenv("KDB_SKINNER_NO_SPLIT");
+      if (const char* r = std::getenv("KDB_SKINNER_SPLIT")) split_run_ = std::max<int64_t>(1, std::atoll(r));
+      if (const char* c = std::getenv("KDB_SKINNER_TASKS")) task_cap_ = std::max<int64_t>(1, std::atoll(c));
+      if (split_)
+        for (int q = 0; q < 2; q++) tasks_[q] = arena_.AllocT<uint64_t>(task_cap_ * (3 + T_));
       Generate();
       std::vector<int> order(T_);
       for (size_t i = 0; i < prefix.size(); i++) order[i] = prefix[i];
@@ -3315,9 +3322,24 @@ class SkinnerEngine : public JoinEnv {
           ctx_.Launch(fn_, ctx_.num_sms * 8, 128, a, 0, "skinner episode");
         }
       }
-      uint64_t cw[2] = {0, 0};
-      ctx_.D2H(&cw[0], count_, sizeof(uint64_t));
-      ctx_.D2H(&cw[1], work_, sizeof(uint64_t));
+      uint64_t cw[3] = {0, 0, 0};
+      ctx_.D2H(cw, stats_, 3 * sizeof(uint64_t));
+      if (split_ && cw[2] > 0 && !ctx_.dry) {
+        // queued hot runs: each round's tasks sit one position deeper than
+        // the previous round's, so at most T rounds
+        int qi = 0;
+        uint64_t pending = cw[2];
+        for (int round = 0; pending > 0; round++) {
+          if (round > T_) throw Error(-5, "skinner task rounds did not converge");
+          a.w[w_phase_] = 4;
+          a.w[w_qin_] = static_cast<uint64_t>(qi);
+          ctx_.Launch(fn_, ctx_.num_sms * 8, 128, a, 0, "skinner tasks");
+          ctx_.Memset(tcount_ + qi, 0, sizeof(uint64_t));
+          qi = 1 - qi;
+          ctx_.D2H(&pending, tcount_ + qi, sizeof(uint64_t));
+        }
+        ctx_.D2H(cw, stats_, 2 * sizeof(uint64_t));
+      }
       ctx_.CheckDeviceError("skinner episode");
       int64_t total = static_cast<int64_t>(cw[0]);
       if (total <= out_.cap || ctx_.dry) {
@@ -3370,6 +3392,7 @@ class SkinnerEngine : public JoinEnv {
     for (int t = 0; t < T; t++) ks.L("card[" + std::to_string(t) + "] = (int64_t)" + ks.Word(static_cast<uint64_t>(cards_[t])) + ";");
     ks.L("const int64_t s0 = (int64_t)a.w[" + std::to_string(w_s0_) + "], s1 = (int64_t)a.w[" + std::to_string(w_s1_) + "];");
     w_phase_ = ks.Arg(0);
+    w_qin_ = ks.Arg(0);
     ks.L("int64_t rows[" + TS + "]; int64_t iti[" + TS + "]; int64_t ite[" + TS + "];");
     ks.L("unsigned long long work = 0;");
     if (agg_) {
@@ -3525,6 +3548,36 @@ class SkinnerEngine : public JoinEnv {
     }
     ks.indent--;
     ks.L("};");
+    // push(p, q): queue the candidate run of position p (rows of the earlier
+    // positions bound) as tasks of split_run_ candidates on queue q; false
+    // when the queue is full (the caller walks the run itself; the slots it
+    // reserved past the capacity that are in range hold empty tasks)
+    std::string TQ0, TQ1, TC, RUN, TCAP;
+    const std::string TW = std::to_string(3 + T);
+    if (split_) {
+      TQ0 = ks.Ptr(tasks_[0], "uint64_t");
+      TQ1 = ks.Ptr(tasks_[1], "uint64_t");
+      TC = ks.Ptr(tcount_, "unsigned long long");
+      RUN = "(int64_t)" + ks.Word(static_cast<uint64_t>(split_run_));
+      TCAP = "(uint64_t)" + ks.Word(static_cast<uint64_t>(task_cap_));
+      ks.Open("auto push = [&](int p, int q) -> bool");
+      ks.L("const int64_t len = ite[p] - iti[p];");
+      ks.L("const uint64_t n = (uint64_t)((len + " + RUN + " - 1) / " + RUN + ");");
+      ks.L("const uint64_t base = atomicAdd(&" + TC + "[q], (unsigned long long)n);");
+      ks.L("uint64_t* tq = q ? " + TQ1 + " : " + TQ0 + ";");
+      ks.L("const bool ok = base + n <= " + TCAP + ";");
+      ks.L("const uint64_t lim = ok ? base + n : (base < " + TCAP + " ? " + TCAP + " : base);");
+      ks.Open("for (uint64_t i = base; i < lim; i++)");
+      ks.L("uint64_t* t = tq + i * " + TW + ";");
+      ks.L("const int64_t b = ok ? iti[p] + (int64_t)(i - base) * " + RUN + " : 0;");
+      ks.L("const int64_t e = ok ? (b + " + RUN + " < ite[p] ? b + " + RUN + " : ite[p]) : 0;");
+      ks.L("t[0] = (uint64_t)p; t[1] = (uint64_t)b; t[2] = (uint64_t)e;");
+      ks.L("for (int k = 0; k < " + TS + "; k++) t[3 + k] = (uint64_t)rows[k];");
+      ks.Close();
+      ks.L("return ok;");
+      ks.indent--;
+      ks.L("};");
+    }
     // Phase 0 (expand): each leftmost tuple of the slice that passes its
     // conditions records its position-1 candidate run [beg, beg + len).
     // Phase 1 (episode), after an exclusive scan of the lengths: every
@@ -3564,11 +3617,21 @@ class SkinnerEngine : public JoinEnv {
       ks.L("if (c1 < 0 || c1 < off[ord[1]]) continue;");
       ks.L("rows[ord[1]] = c1; work++;");
       ks.L("if (!conds_ok(sched[1])) continue;");
-      // depth-first over positions from..T-1, the earlier ones bound
-      auto depth_first = [&](int from) {
-        const std::string F = std::to_string(from);
-        ks.L("int p = " + F + "; init(" + F + ");");
-        ks.Open("while (p >= " + F + ")");
+      // depth-first over positions from..T-1, the earlier ones bound; with
+      // `preset` position `from`'s run is already in [iti, ite) (a task);
+      // hot runs at position 3 and deeper go to queue `q`
+      auto depth_first = [&](const std::string& from, bool preset, const std::string& q) {
+        auto split = [&]() {
+          if (split_)
+            ks.L("if (p >= 3 && ite[p] - iti[p] > " + RUN + " && push(p, " + q + ")) iti[p] = ite[p];");
+        };
+        ks.L("int p = " + from + ";");
+        ks.L("const int pmin = p;");
+        if (!preset) {
+          ks.L("init(p);");
+          split();
+        }
+        ks.Open("while (p >= pmin)");
         ks.L("int64_t c = next(p);");
         ks.Open("if (c < 0)");
         ks.L("p--;");
@@ -3584,13 +3647,14 @@ class SkinnerEngine : public JoinEnv {
         ks.Open("else");
         ks.L("p++;");
         ks.L("init(p);");
+        split();
         ks.Close();
         ks.Close();
       };
       if (T == 2) {
         ks.L("emit();");
       } else {
-        depth_first(2);
+        depth_first("2", false, "0");
       }
       ks.Close();
       ks.Close();
@@ -3625,7 +3689,7 @@ class SkinnerEngine : public JoinEnv {
         ks.L("len2 = (uint64_t)(ite[2] - iti[2]);");
         ks.Close();
         ks.Open("else");
-        depth_first(2);
+        depth_first("2", false, "0");
         ks.Close();
         ks.Close();
         ks.Close();
@@ -3658,8 +3722,26 @@ class SkinnerEngine : public JoinEnv {
         ks.L("rows[ord[2]] = c2; work++;");
         ks.L("if (!conds_ok(sched[2])) continue;");
         if (T == 3) ks.L("emit();");
-        else depth_first(3);
+        else depth_first("3", false, "0");
         ks.Close();
+        ks.Close();
+        ks.Close();
+      }
+      if (split_) {
+        // Phase 4: the queued tasks of queue qin, one per thread, each
+        // continuing depth-first from its position; their hot runs go to
+        // the other queue
+        ks.Open("else if (phase == 4)");
+        ks.L("const int qi = (int)a.w[" + std::to_string(w_qin_) + "];");
+        ks.L("const uint64_t nq = " + TC + "[qi];");
+        ks.L("const uint64_t nt = nq < " + TCAP + " ? nq : " + TCAP + ";");
+        ks.L("const uint64_t* tq = qi ? " + TQ1 + " : " + TQ0 + ";");
+        ks.Open("for (uint64_t w = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; w < nt; w += (uint64_t)gridDim.x * blockDim.x)");
+        ks.L("const uint64_t* t = tq + w * " + TW + ";");
+        ks.L("const int tp = (int)t[0];");
+        ks.L("iti[tp] = (int64_t)t[1]; ite[tp] = (int64_t)t[2];");
+        ks.L("for (int k = 0; k < " + TS + "; k++) rows[k] = (int64_t)t[3 + k];");
+        depth_first("tp", true, "1 - qi");
         ks.Close();
         ks.Close();
       }
@@ -3758,8 +3840,21 @@ class SkinnerEngine : public JoinEnv {
   int64_t total_work_ = 0;
   std::vector<std::vector<JoinTable>> index_for_;
   MatBuffer out_;
+  uint64_t* stats_ = nullptr;
   uint64_t* count_ = nullptr;
   uint64_t* work_ = nullptr;
+  // Hot runs: a depth-first walk that meets a candidate run longer than
+  // split_run_ at position 3 or deeper pushes it, in chunks of split_run_,
+  // as tasks {position, begin, end, bound rows} to a queue instead of
+  // walking it alone; the host then runs the queued tasks grid-wide (their
+  // own hot runs go to the other queue) until both are empty.  A full queue
+  // leaves the run to the thread that met it.
+  bool split_ = false;
+  int64_t split_run_ = 1024;
+  int64_t task_cap_ = 1 << 16;
+  uint64_t* tasks_[2] = {nullptr, nullptr};
+  uint64_t* tcount_ = nullptr;
+  int w_qin_ = 0;
   int64_t produced_ = 0;
   int64_t episodes_ = 0;
   CUfunction fn_ = nullptr;

@@ -60,3 +60,33 @@ def test_aggregate_fused_into_episodes_matches_materialised(engine):
     finally:
         engine.set_skinner()
     assert compare(fused, plain) == ""
+
+
+@pytest.mark.parametrize("split,tasks", [(8, 1 << 16), (8, 16), (64, 1 << 16)])
+@pytest.mark.parametrize("shape,n_tables", [("chain", 7), ("star", 8)])
+@pytest.mark.parametrize("fused", [True, False])
+def test_hot_runs_as_tasks_match_oracle(engine, split, tasks, shape, n_tables, fused):
+    """Runs longer than `split` candidates at position 3 and deeper go to the
+    task queues (a queue of `tasks` entries: with 16 it fills, and the rest
+    is walked in place); the result stays exactly the join's."""
+    import os
+    from oracle import Oracle
+    tables, tokens = wl.skinner_tables(shape, n_tables, min_rows=1000, max_rows=20_000, zipf_s=1.5,
+                                       seed=31 + n_tables, prefix=f"hot{shape}{n_tables}_")
+    plan = wl.skinner_plan(tables, tokens, shape)
+    o = Oracle()
+    for t in tables:
+        engine.register_table(t)
+        o.register_table(t)
+    os.environ["KDB_SKINNER_SPLIT"] = str(split)
+    os.environ["KDB_SKINNER_TASKS"] = str(tasks)
+    if not fused:  # results materialised (slot allocation, regrowth) instead of folded
+        os.environ["KDB_NO_SKINNER_AGG"] = "1"
+    engine.set_skinner(3000, seed=2)
+    try:
+        g = engine.execute(plan)
+    finally:
+        for k in ("KDB_SKINNER_SPLIT", "KDB_SKINNER_TASKS", "KDB_NO_SKINNER_AGG"):
+            os.environ.pop(k, None)
+        engine.set_skinner()
+    assert compare(g, o.execute(plan)) == ""
