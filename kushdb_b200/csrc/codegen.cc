@@ -3926,8 +3926,8 @@ HostResult Executor::Download(const MatBuffer& m, const Operator& root, bool che
     if (m.cols[c].nulls) total += (static_cast<size_t>(m.rows) + 15) & ~size_t(15);
   }
   const size_t err_off = total;
-  res.block = ctx_.AcquireHostBlock(total + 16);
-  char* stage = res.block.get();
+  std::shared_ptr<char> pinned = ctx_.AcquireHostBlock(total + 16);
+  char* stage = pinned.get();
   if (!ctx_.dry && (m.rows > 0 || check_error)) {
     // several small segments: gather on the device, one copy to the host
     PackSegs segs;
@@ -3977,6 +3977,18 @@ HostResult Executor::Download(const MatBuffer& m, const Operator& root, bool che
     if (m.rows == 0 && total) std::memset(stage, 0, total);
   } else if (total) {
     std::memset(stage, 0, total);
+  }
+  // A small result is copied out of the pinned block, which goes straight
+  // back to the pool: callers that hold many results (a server's finished
+  // tickets) would otherwise make every further result allocate pinned
+  // memory, and pinned allocation and release stall the whole device.
+  constexpr size_t kSmallResult = size_t(64) << 10;
+  if (total + 16 <= kSmallResult) {
+    res.block = std::shared_ptr<char>(new char[total + 16], std::default_delete<char[]>());
+    std::memcpy(res.block.get(), stage, total + 16);
+    stage = res.block.get();
+  } else {
+    res.block = pinned;
   }
   for (size_t c = 0; c < m.cols.size(); c++) {
     const MatCol& mc = m.cols[c];
