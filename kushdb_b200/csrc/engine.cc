@@ -165,7 +165,8 @@ std::shared_ptr<char> HostBlockPool::Acquire(size_t bytes) {
     while (size < bytes) size <<= 1;
     if (pinned_) {
       void* h = nullptr;
-      KDB_CUDA(cudaMallocHost(&h, size));
+      // mapped: small results are written into the block by a kernel
+      KDB_CUDA(cudaHostAlloc(&h, size, cudaHostAllocMapped));
       p = static_cast<char*>(h);
     } else {
       p = static_cast<char*>(std::malloc(size));

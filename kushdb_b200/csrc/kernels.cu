@@ -501,14 +501,31 @@ __global__ void CopyPairs(const uint64_t* __restrict__ ks, const uint32_t* __res
 
 void Context::PackToHost(const PackSegs& segs, size_t total, void* host) {
   if (dry || segs.n == 0) return;
+  uint64_t most = 0;
+  for (int i = 0; i < segs.n; i++) most = std::max<uint64_t>(most, segs.seg[i].bytes);
+  const int gx = static_cast<int>(std::max<uint64_t>(1, std::min<uint64_t>((most / 16 + 255) / 256, 64)));
+  // A small result is gathered by the kernel straight into the pinned host
+  // block (mapped into the device's address space): no device stage and no
+  // copy to launch and wait for after the kernel.
+  constexpr size_t kDirect = size_t(64) << 10;
+  void* mapped = nullptr;
+  if (total <= kDirect && !std::getenv("KDB_NO_MAPPED_RESULT")) {
+    if (cudaHostGetDevicePointer(&mapped, host, 0) != cudaSuccess) {
+      cudaGetLastError();
+      mapped = nullptr;
+    }
+  }
+  if (mapped) {
+    PackSegments<<<dim3(gx, segs.n), 256, 0, stream>>>(segs, static_cast<char*>(mapped));
+    kernel_launches++;
+    KDB_CUDA(cudaGetLastError());
+    return;
+  }
   if (total > dev_stage_bytes_) {
     if (dev_stage_) cudaFreeAsync(dev_stage_, stream);
     dev_stage_bytes_ = std::max<size_t>(total, 1 << 20);
     KDB_CUDA(cudaMallocAsync(&dev_stage_, dev_stage_bytes_, stream));
   }
-  uint64_t most = 0;
-  for (int i = 0; i < segs.n; i++) most = std::max<uint64_t>(most, segs.seg[i].bytes);
-  const int gx = static_cast<int>(std::max<uint64_t>(1, std::min<uint64_t>((most / 16 + 255) / 256, 64)));
   char* dst = static_cast<char*>(dev_stage_);
   PackSegments<<<dim3(gx, segs.n), 256, 0, stream>>>(segs, dst);
   kernel_launches++;
