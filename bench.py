@@ -47,6 +47,15 @@ def _peaks():
     return 6650.0, "fallback"
 
 
+# DRAM bytes (read + write) of one launch of each workload's dominant kernel
+# at the default size, from one ncu capture of the current kernels
+# (profiles/dram_traffic_dominant_kernels.md); other sizes scale it by the
+# rows processed, the traffic being proportional to them.
+MEASURED_TRAFFIC = {"group_by": 264_034_304 + 3_061_760,
+                    "join_group": 119_308_288 + 3_159_808,
+                    "scan_agg": 20_026_112}
+
+
 def make_workload(name: str, scale: float = 1.0):
     """Returns (tables, plan, rows per step, algorithmic bytes per step,
     dominant kernel tag, config dict)."""
@@ -620,7 +629,9 @@ def main():
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic", "config": cfg,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                     "frac": (achieved / peak) if achieved else None, "traffic": None,
+                     "frac": (achieved / peak) if achieved else None,
+                     "traffic": (round(MEASURED_TRAFFIC[args.workload] * scale)
+                                 if args.workload in MEASURED_TRAFFIC else None),
                      "kernel": dom_tag, "kernel_ms": dom_ms, "algorithmic_bytes": algo_bytes,
                      "peak_source": f"{peak_kind} hbm_gbs"},
         "cpu_baseline": cpu,
