@@ -47,10 +47,10 @@ def _peaks():
     return 6650.0, "fallback"
 
 
-# DRAM bytes (read + write) of one launch of each workload's dominant kernel
-# at the default size, from one ncu capture of the current kernels
-# (profiles/dram_traffic_dominant_kernels.md); other sizes scale it by the
-# rows processed, the traffic being proportional to them.
+# DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of one launch of
+# each workload's dominant kernel at the default size, from one ncu capture
+# of the current kernels; other sizes scale it by the rows processed, the
+# traffic being proportional to them.
 MEASURED_TRAFFIC = {"group_by": 264_034_304 + 3_061_760,
                     "join_group": 119_308_288 + 3_159_808,
                     "scan_agg": 20_026_112}
