@@ -2939,7 +2939,7 @@ class UctNode {
  private:
   // With a learned prior every action starts as tried once with the
   // predicted reward: the search begins at the prior's choice and the
-  // observed rewards overrule it (UCT stays the judge).
+  // observed rewards overrule it (UCT has the last word).
   void InitPrior() {
     if (!env_.HasPrior() || num_actions_ == 0) return;
     std::vector<double> v;
