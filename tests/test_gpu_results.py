@@ -79,3 +79,36 @@ def test_result_read_after_engine_close():
     assert len(cols[0].nulls) == want.num_rows
     assert np.array_equal(np.asarray(cols[0].values), np.asarray(want.columns[0].values))
     r.close()
+
+
+def test_large_results_held_beyond_the_pool():
+    """Results above the small-result size keep their pinned blocks: more of
+    them held at once than the pool keeps, freed out of order, each still
+    holds its own rows."""
+    from kushdb_b200.engine import Engine
+    from kushdb_b200.data import HostColumn, HostTable, catalog_of
+    from kushdb_b200.plan import ColRef, OperatorSchema, OrderByOperator, OutputOperator, ScanOperator, Type
+    n = 20_000  # 20k rows x 12 bytes downloaded: well above 64 KB
+    rng = np.random.default_rng(3)
+    t = HostTable("held_rows")
+    t.add(HostColumn("id", Type.Int(), values=np.arange(n, dtype=np.int32)))
+    t.add(HostColumn("x", Type.Real(), values=rng.permutation(n).astype(np.float64)))
+    rel = catalog_of([t])[t.name]
+    s = OperatorSchema()
+    s.AddGeneratedColumns(rel, ["id", "x"])
+    scan = ScanOperator(s, rel)
+    out = OperatorSchema()
+    out.AddPassthroughColumns(scan)
+    q = OutputOperator(OrderByOperator(out, scan, [ColRef(scan, "x")], [True])).to_json()
+    want = _oracle(t).execute(q)
+    e = Engine(0)
+    try:
+        e.register_table(t)
+        held = [e.execute(q) for _ in range(20)]
+        for r in held[1::2]:
+            r.close()
+        more = [e.execute(q) for _ in range(4)]
+        for r in held[0::2] + more:
+            assert compare(r, want) == ""
+    finally:
+        e.close()
