@@ -1,0 +1,39 @@
+"""Every A/B switch's alternative code path still generates and compiles
+(NVRTC, sm_100a) for the workload plans, in a compile-only context (no GPU):
+the switches reproduce the measured comparisons, so their paths must not rot."""
+
+import os
+
+import pytest
+
+from kushdb_b200 import workloads as wl
+from kushdb_b200.engine import Engine
+
+SWITCHES = ["KDB_NO_SCAN_PREFETCH", "KDB_NO_VECTOR_SCAN", "KDB_VECTOR_PROBE_SCAN", "KDB_NO_JOIN_FILTER",
+            "KDB_NO_KEY_IN_SLOT", "KDB_NO_BUILD_ROW_GROUPS", "KDB_NO_DENSE_GROUPBY", "KDB_MATERIALIZE_ATOMIC",
+            "KDB_GROUP_ORDER_SORT", "KDB_ORDER_RADIX", "KDB_ORDER_TIE_SORT", "KDB_SKINNER_DEPTH1",
+            "KDB_SKINNER_NO_SPLIT", "KDB_NO_SKINNER_AGG", "KDB_DENSE_SMEM=0"]
+
+
+@pytest.mark.parametrize("switch", SWITCHES)
+def test_switch_path_compiles(switch):
+    name, _, value = switch.partition("=")
+    os.environ[name] = value or "1"
+    try:
+        e = Engine(-1)
+        t1 = wl.scan_agg_table(rows=1000)
+        t2 = wl.group_by_table(rows=1000)
+        b, p = wl.join_tables(build_rows=1000, probe_rows=4000)
+        for t in (t1, t2, b, p):
+            e.register_table(t)
+        e.execute(wl.scan_agg_plan(t1))
+        e.execute(wl.group_by_plan(t2))
+        e.execute(wl.join_plan(b, p))
+        tables, tokens = wl.skinner_tables("chain", 6, min_rows=100, max_rows=1000, prefix="sw")
+        for t in tables:
+            e.register_table(t)
+        e.execute(wl.skinner_plan(tables, tokens, "chain"))
+        assert e.kernel_launches() > 0
+        e.close()
+    finally:
+        del os.environ[name]
