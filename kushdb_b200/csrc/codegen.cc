@@ -1434,7 +1434,9 @@ MatBuffer Executor::RunAggregate(const Operator& op) {
   int grid = 1;
   uint64_t* part = nullptr;
   uint64_t* text_state = arena_.AllocT<uint64_t>(plans.size() + 1);
-  ctx_.Memset(text_state, 0, sizeof(uint64_t) * (plans.size() + 1));
+  bool any_text = false;  // only TEXT MIN/MAX read the text state
+  for (const auto& p : plans) any_text |= p.kind == StateKind::MinMaxText;
+  if (any_text) ctx_.Memset(text_state, 0, sizeof(uint64_t) * (plans.size() + 1));
   if (fuse) {
     part = arena_.AllocT<uint64_t>(nw);
     std::vector<uint64_t> init(nw, 0);
