@@ -170,11 +170,11 @@ int64_t kdb_last_skinner_samples(kdb_ctx* ctx, float* features, float* rewards, 
 int kdb_sort_pairs(kdb_ctx* ctx, uint64_t* d_keys, uint32_t* d_vals, int64_t n, int32_t key_bits);
 
 /* The same sort without any device allocation, for callers that cannot
- * allocate when they sort: code recording a CUDA graph (cudaMalloc is not a
- * stream operation and breaks the capture), host callbacks and other
- * contexts where CUDA allocation calls are not allowed, and host engines that
- * hand out every byte of HBM through their own allocator.  This entry point
- * has no counterpart in the reference.
+ * allocate when they sort: code running inside a CUDA host callback or
+ * another context where CUDA allocation calls are not allowed, and host
+ * engines that hand out every byte of HBM through their own allocator and
+ * forbid a library's hidden allocations.  This entry point has no
+ * counterpart in the reference.
  *
  * Scratch is one static device array sized for KDB_SORT_NOALLOC_MAX_PAIRS
  * pairs (12.25 MiB), held by every GPU that loads this library until the
@@ -183,12 +183,120 @@ int kdb_sort_pairs(kdb_ctx* ctx, uint64_t* d_keys, uint32_t* d_vals, int64_t n, 
  * legacy default stream) on the current device and the call returns without
  * waiting.  The first call on each device looks up the array's device address
  * once (cudaGetSymbolAddress): make that first call before any stream
- * capture.  Every call shares the one array, so calls whose work overlaps on
- * the GPU (different streams, or different host threads) race and must be
- * ordered by the caller. */
+ * capture; resetting the device (cudaDeviceReset) after that first call is
+ * not supported, because the looked-up address is kept.  An error already
+ * pending on the calling thread (cudaPeekAtLastError) is left in place and
+ * the call returns KDB_ERR_CUDA without launching.  Every call shares the one
+ * array, so calls whose work overlaps on the GPU (different streams, or
+ * different host threads) race and must be ordered by the caller. */
 #define KDB_SORT_NOALLOC_MAX_PAIRS (1 << 20)
 int kdb_sort_pairs_noalloc(uint64_t* d_keys, uint32_t* d_vals, int64_t n, int32_t key_bits,
                            void* stream);
+
+/* ---- per-operator boundary ------------------------------------------------
+ * One operator per call over HBM-resident tables, for hosts that drive the
+ * operators themselves the way the reference's generated code calls one
+ * runtime structure at a time.  Objects belong to the context that made them
+ * and must be freed before it is destroyed.
+ *
+ * Selection vectors: ascending row ids of one table.  kdb_scan_select
+ * replaces ScanSelectTranslator::Produce (compile/translators/
+ * scan_select_translator.cc:92-156): `filter_json` is one BOOLEAN expression
+ * in the plan JSON shape over `columns` (bound by position: VIRTUAL_COLUMN_REF
+ * or COLUMN_REF of child 0 with column_idx = position), with the reference's
+ * three-valued logic; a row qualifies when the filter is TRUE. */
+typedef struct kdb_selvec kdb_selvec;
+int kdb_scan_select(kdb_ctx* ctx, const char* table, const char* const* columns, int32_t ncols,
+                    const char* filter_json, kdb_selvec** out);
+int64_t kdb_selvec_size(const kdb_selvec* s);
+/* copies min(cap, size) row ids to host memory; returns the size */
+int64_t kdb_selvec_get(const kdb_selvec* s, int32_t* rows, int64_t cap);
+/* device array of the row ids (valid until the vector is freed) */
+const int32_t* kdb_selvec_device_rows(const kdb_selvec* s);
+void kdb_selvec_free(kdb_selvec* s);
+
+/* Hash join build / probe: runtime::HashTable::{Create,Insert,GetBucket}
+ * (runtime/hash_table.h:22-38) as hash_join_translator.cc:79-139 drives it.
+ * The key is one SMALLINT/INT/BIGINT/DATE/ENUM/BOOLEAN column; rows with a
+ * NULL key are not inserted (and never match), duplicates are all kept.
+ * sel NULL = every row.  load_factor in (0.05, 0.95].  fanout: 1 = one
+ * open-addressing table; a power of two up to 8192 = that many sub-tables
+ * chosen by the key hash's top bits (radix partitioned: both sides are
+ * scattered by partition and each partition joins in shared memory, its
+ * sub-table and probe tiles brought in by TMA bulk copies); 0 = one table
+ * while it fits well inside L2, partitioned above. */
+typedef struct kdb_hash kdb_hash;
+typedef struct kdb_pairs kdb_pairs;
+int kdb_hash_build(kdb_ctx* ctx, const char* table, const char* key_column, const kdb_selvec* sel,
+                   double load_factor, int32_t fanout, kdb_hash** out);
+int kdb_hash_info(const kdb_hash* h, int32_t* fanout, int64_t* slots, int64_t* bytes);
+/* Every (probe row, build row) pair with equal keys.  ordered != 0: sorted
+ * by probe row, then build row -- the reference's order, in which a probe
+ * row meets its bucket's rows in insertion order; 0: in no particular order.
+ * The probe key must have the build key's width class (BIGINT with BIGINT,
+ * the narrower types among themselves). */
+int kdb_hash_probe(kdb_ctx* ctx, const kdb_hash* h, const char* table, const char* key_column,
+                   const kdb_selvec* sel, int32_t ordered, kdb_pairs** out);
+void kdb_hash_free(kdb_hash* h);
+int64_t kdb_pairs_size(const kdb_pairs* p);
+int64_t kdb_pairs_get(const kdb_pairs* p, int32_t* probe_rows, int32_t* build_rows, int64_t cap);
+void kdb_pairs_free(kdb_pairs* p);
+
+/* Group-by aggregation: runtime::AggregateHashTable with the proxy
+ * aggregators (runtime/aggregate_hash_table.h:28-49, compile/proxy/
+ * aggregate_hash_table.cc:187-333, compile/proxy/aggregator.cc:28-296).
+ * 1-4 integer/date/enum/boolean key columns (NULL is a key value of its
+ * own) and 1-8 aggregates over numeric columns of the same table:
+ * SUM/MIN/MAX keep the input type (integer sums wrap at its width), AVG is
+ * REAL, COUNT is BIGINT (column NULL = rows; COUNT(col) counts the non-NULL
+ * values plus the group's first row when that one is NULL, as the reference
+ * does); a SUM/MIN/MAX/AVG of only NULLs is NULL.  max_groups bounds the
+ * groups (<= 0: the table's row count); more return KDB_ERR_CAPACITY and the
+ * table is then unusable.  Updates accumulate (one per morsel/selection);
+ * the result lists the groups in first-insertion order, keys first, then
+ * the aggregates.  Float sums differ from sequential ones only in summation
+ * order.  Pre-aggregation in shared memory is on by default. */
+#define KDB_AGG_SUM 0
+#define KDB_AGG_MIN 1
+#define KDB_AGG_MAX 2
+#define KDB_AGG_AVG 3
+#define KDB_AGG_COUNT 4
+typedef struct {
+  int32_t agg;
+  const char* column;
+} kdb_agg_spec;
+typedef struct kdb_agg kdb_agg;
+int kdb_agg_create(kdb_ctx* ctx, const char* table, const char* const* key_columns, int32_t nkeys,
+                   const kdb_agg_spec* aggs, int32_t naggs, int64_t max_groups, kdb_agg** out);
+int kdb_agg_set_pre_aggregation(kdb_agg* a, int32_t on);
+int kdb_agg_update(kdb_ctx* ctx, kdb_agg* a, const kdb_selvec* sel);
+int kdb_agg_finalize(kdb_ctx* ctx, kdb_agg* a, kdb_result** out);
+void kdb_agg_free(kdb_agg* a);
+
+/* Column indexes: key -> ascending row ids.  kdb_index_build replaces
+ * runtime::MemoryColumnIndex (runtime/memory_column_index.cc:17-121) over a
+ * resident column; kdb_index_open_kdbindex reads a reference .kdbindex file
+ * (runtime/column_index.h:21-41, runtime/column_index.cc:67-144; integer,
+ * date, enum and boolean keys).  NULL keys are not indexed. */
+typedef struct kdb_index kdb_index;
+int kdb_index_build(kdb_ctx* ctx, const char* table, const char* column, kdb_index** out);
+int kdb_index_open_kdbindex(kdb_ctx* ctx, const char* path, const char* type, kdb_index** out);
+int64_t kdb_index_num_keys(const kdb_index* i);
+int64_t kdb_index_num_rows(const kdb_index* i);
+/* distinct keys in ascending order (copies min(cap, n)); returns n */
+int64_t kdb_index_keys(const kdb_index* i, int64_t* keys, int64_t cap);
+/* rows of `key` (copies min(cap, n)); returns n (0 for an absent key) */
+int64_t kdb_index_get(const kdb_index* i, int64_t key, int32_t* rows, int64_t cap);
+void kdb_index_free(kdb_index* i);
+
+/* The Skinner join operator on its own: runtime::ExecutePermutableSkinnerJoin
+ * (runtime/skinner_join_executor.h:16-25).  skinner_json is one SKINNER_JOIN
+ * operator in the plan JSON shape whose children are scans; policy as in
+ * kdb_ctx_set_skinner_policy (0 UCT, 1 learned prior, 2 random), the budget
+ * and seed as in kdb_ctx_set_skinner, for this call only.  The result rows
+ * are the operator's output schema. */
+int kdb_skinner_execute(kdb_ctx* ctx, const char* skinner_json, int32_t policy, int64_t budget_per_episode,
+                        uint32_t seed, kdb_result** out);
 
 /* ---- batched form ----------------------------------------------------------
  * Many queries of one template, run together as a captured CUDA graph of

@@ -12,8 +12,10 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libkdb_b200.so")
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
-SOURCES = ["kernels.cu", "batch.cu", "engine.cc", "codegen.cc", "capi.cc", "server.cc", "join_prior.cu"]
-HEADERS = ["engine.h", "plan.h", "json.h", "host_result.h", "capi_internal.h", "join_prior.h", "device_runtime.cuh"]
+SOURCES = ["kernels.cu", "batch.cu", "engine.cc", "codegen.cc", "capi.cc", "server.cc", "join_prior.cu",
+           "operators.cu", "capi_ops.cc"]
+HEADERS = ["engine.h", "plan.h", "json.h", "host_result.h", "capi_internal.h", "join_prior.h", "device_runtime.cuh",
+           "operators.h"]
 
 
 def _embed_runtime():

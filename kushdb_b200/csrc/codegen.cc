@@ -28,6 +28,7 @@
 
 #include "engine.h"
 #include "join_prior.h"
+#include "operators.h"
 
 namespace kdb {
 namespace {
@@ -4202,6 +4203,129 @@ HostResult ExecutePlan(Context& ctx, const plan::Operator& root, std::unique_ptr
     *prepared = std::move(pq);
   }
   return r;
+}
+
+
+// ---------------------------------------------------------------------------
+// Per-operator scan-select (kernel a; scan_select_translator.cc:92-156 with
+// the filter semantics of expression_translator.cc): the filter is compiled
+// into a kernel that evaluates 4 consecutive rows per thread from 128-bit
+// loads and compacts the qualifying row ids of each 1024-row tile in row
+// order (per-thread counts, warp shuffle scan, block scan of the warp
+// totals) into a tile-sized region of a scratch buffer; a scan of the tile
+// counts and one gather then produce the selection vector in ascending row
+// order.
+// ---------------------------------------------------------------------------
+std::unique_ptr<ops::SelVec> ScanSelectRows(Context& ctx, const std::string& table,
+                                            const std::vector<std::string>& colnames, const plan::Expr& filter) {
+  auto it = ctx.tables.find(table);
+  if (it == ctx.tables.end()) throw Error(-1, "unknown table " + table);
+  if (ctx.dry) throw Error(-5, "operators need a device context");
+  const int64_t n = std::max<int64_t>(it->second.rows, 0);
+  if (n >= (int64_t(1) << 31)) throw Error(-4, "selection vectors hold row ids below 2^31");
+  auto sv = std::make_unique<ops::SelVec>();
+  sv->table = table;
+  KernelSource ks;
+  ExprGen eg(ctx, ks);
+  std::vector<const DevColumn*> cols;
+  std::vector<std::string> dp, np, tp;
+  for (const auto& name : colnames) {
+    const DevColumn& c = ctx.Column(table, name);
+    cols.push_back(&c);
+    if (c.type.id == TypeId::TEXT) {
+      dp.push_back(ks.Ptr(c.toff, "int64_t", true));
+      tp.push_back(ks.Ptr(c.tchars, "char", true));
+    } else {
+      dp.push_back(ks.Ptr(c.data, StoreType(c.type.id), true));
+      tp.push_back("");
+    }
+    np.push_back(c.nulls ? ks.Ptr(c.nulls, "int8_t", true) : "");
+  }
+  const int64_t ntiles = (n + 1023) / 1024;
+  Arena arena(ctx);
+  int32_t* scratch = arena.AllocT<int32_t>(std::max<int64_t>(ntiles * 1024, 1));
+  uint64_t* counts = arena.AllocT<uint64_t>(ntiles + 1);
+  const std::string sp = ks.Ptr(scratch, "int32_t");
+  const std::string cp = ks.Ptr(counts, "uint64_t");
+  ks.pre << "  __shared__ unsigned kdb_wsum[8];\n";
+  ks.L("const int64_t nrows = (int64_t)" + ks.Word(static_cast<uint64_t>(n)) + ";");
+  ks.L("const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;");
+  ks.Open("for (int64_t tile = blockIdx.x; tile * 1024 < nrows; tile += gridDim.x)");
+  ks.L("const int64_t base = tile * 1024 + threadIdx.x * 4;");
+  ks.L("const bool full = base + 4 <= nrows;");
+  std::vector<std::string> arr(cols.size()), narr(cols.size());
+  for (size_t k = 0; k < cols.size(); k++) {
+    if (cols[k]->type.id == TypeId::TEXT) continue;
+    const std::string st = StoreType(cols[k]->type.id);
+    arr[k] = ks.Fresh("L");
+    ks.L(st + " " + arr[k] + "[4];");
+    ks.L("if (full) kdb_ld4(" + dp[k] + ", base, " + arr[k] + "); else for (int u = 0; u < 4; u++) " + arr[k] +
+         "[u] = base + u < nrows ? " + dp[k] + "[base + u] : (" + st + ")0;");
+    if (!np[k].empty()) {
+      narr[k] = ks.Fresh("N");
+      ks.L("int8_t " + narr[k] + "[4];");
+      ks.L("if (full) kdb_ld4(" + np[k] + ", base, " + narr[k] + "); else for (int u = 0; u < 4; u++) " + narr[k] +
+           "[u] = base + u < nrows ? " + np[k] + "[base + u] : (int8_t)0;");
+    }
+  }
+  ks.L("bool f[4];");
+  ks.L("#pragma unroll");
+  ks.Open("for (int u = 0; u < 4; u++)");
+  ks.L("const int64_t r = base + u;");
+  ks.L("f[u] = false;");
+  ks.Open("if (r < nrows)");
+  std::vector<CVal> bound;
+  for (size_t k = 0; k < cols.size(); k++) {
+    const DevColumn& c = *cols[k];
+    std::string v;
+    std::string nul = "false";
+    if (c.type.id == TypeId::TEXT) {
+      v = "kdb_text_at(" + dp[k] + ", " + tp[k] + ", r)";
+      if (!np[k].empty()) nul = "(" + np[k] + "[r] != 0)";
+    } else {
+      v = c.type.id == TypeId::BOOLEAN ? "(" + arr[k] + "[u] != 0)" : arr[k] + "[u]";
+      if (!narr[k].empty()) nul = "(" + narr[k] + "[u] != 0)";
+    }
+    bound.push_back(eg.Bind(c.type, v, nul));
+  }
+  Scope sc;
+  sc.virt = bound;
+  sc.child.push_back(bound);
+  CVal fv = eg.Emit(filter, sc);
+  ks.L("f[u] = !(" + fv.n + ") && (" + fv.v + ");");
+  ks.Close();
+  ks.Close();
+  // ordered compaction of the tile: thread t holds rows 4t..4t+3
+  ks.L("const unsigned mine = (unsigned)f[0] + (unsigned)f[1] + (unsigned)f[2] + (unsigned)f[3];");
+  ks.L("unsigned incl = mine;");
+  ks.L("for (int d = 1; d < 32; d <<= 1) { unsigned y = __shfl_up_sync(0xffffffffu, incl, d); if (lane >= d) incl += y; }");
+  ks.L("if (lane == 31) kdb_wsum[warp] = incl;");
+  ks.L("__syncthreads();");
+  ks.L("unsigned before = 0, total = 0;");
+  ks.L("for (int w = 0; w < (int)(blockDim.x >> 5); w++) { unsigned x = kdb_wsum[w]; if (w < warp) before += x; total += x; }");
+  ks.L("unsigned at = before + incl - mine;");
+  ks.L("int32_t* dst = " + sp + " + tile * 1024;");
+  ks.L("for (int u = 0; u < 4; u++) if (f[u]) dst[at++] = (int32_t)(base + u);");
+  ks.L("if (threadIdx.x == 0) " + cp + "[tile] = total;");
+  ks.L("__syncthreads();");
+  ks.Close();
+  const std::string name = "kdb_scan_select_rows";
+  CUfunction fn = ctx.Kernel(ks.Kernel(name, 256), name);
+  const int grid = static_cast<int>(std::max<int64_t>(1, std::min<int64_t>(ntiles, ctx.num_sms * 8)));
+  if (ntiles > 0) ctx.Launch(fn, grid, 256, ks.Args(), 0, "scan select");
+  ctx.ScanU64(counts, ntiles, "scan select offsets");
+  uint64_t total = 0;
+  ctx.D2H(&total, counts + ntiles, sizeof(total));
+  ctx.CheckDeviceError("scan select");
+  sv->n = static_cast<int64_t>(total);
+  sv->rows = static_cast<int32_t*>(nullptr);
+  void* out = nullptr;
+  KDB_CUDA(cudaMallocAsync(&out, sizeof(int32_t) * std::max<uint64_t>(total, 1), ctx.stream));
+  sv->rows = static_cast<int32_t*>(out);
+  sv->ctx = &ctx;
+  ops::GatherTiles(ctx, scratch, counts, ntiles, sv->rows);
+  KDB_CUDA(cudaStreamSynchronize(ctx.stream));
+  return sv;
 }
 
 }  // namespace kdb

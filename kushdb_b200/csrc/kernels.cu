@@ -509,7 +509,10 @@ void Context::PackToHost(const PackSegs& segs, size_t total, void* host) {
   // copy to launch and wait for after the kernel.
   constexpr size_t kDirect = size_t(64) << 10;
   void* mapped = nullptr;
-  if (total <= kDirect && !std::getenv("KDB_NO_MAPPED_RESULT")) {
+  // The lookup is skipped while an earlier error is pending, so that clearing
+  // the lookup's own failure below can never swallow someone else's error.
+  if (total <= kDirect && !std::getenv("KDB_NO_MAPPED_RESULT") &&
+      cudaPeekAtLastError() == cudaSuccess) {
     if (cudaHostGetDevicePointer(&mapped, host, 0) != cudaSuccess) {
       cudaGetLastError();
       mapped = nullptr;
@@ -724,9 +727,8 @@ void Context::RadixSortPairs(uint64_t* keys, uint32_t* vals, int64_t n, Arena& a
 // Allocation-free sort entry point.
 //
 // Some callers cannot allocate device memory at the moment they need a sort:
-// code recording a CUDA graph (cudaMalloc is not a stream operation and breaks
-// the capture), host callbacks and driver-owned threads where CUDA
-// allocation calls are not allowed, and host engines that budget every byte
+// host callbacks and driver-owned threads where CUDA allocation calls are
+// not allowed, and host engines that budget every byte
 // of HBM through their own allocator and forbid hidden allocations from a
 // library.  kdb_sort_pairs_noalloc serves them: the radix passes' scratch (a
 // second key/value buffer and the per-block digit histograms) lives in one
@@ -747,7 +749,11 @@ static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratch
 
 // Device address of g_noalloc_scratch per device.  In host code the array's
 // name is only a host-side stand-in, so its device address is looked up once
-// per device, with that device current, through cudaGetSymbolAddress.
+// per device, with that device current, through cudaGetSymbolAddress.  The
+// cached address belongs to the device's primary context as it was at the
+// first call: after cudaDeviceReset the module is loaded again and the cache
+// would be stale, so resetting a device after this entry point has run on it
+// is not supported.
 constexpr int kMaxDevices = 64;
 std::mutex g_noalloc_mu;
 void* g_noalloc_addr[kMaxDevices] = {};
@@ -775,6 +781,10 @@ extern "C" int kdb_sort_pairs_noalloc(uint64_t* d_keys, uint32_t* d_vals, int64_
   if (n < 0 || (n > 0 && (!d_keys || !d_vals)) || key_bits < 1 || key_bits > 64)
     return KDB_ERR_INVALID;
   if (n > kNoAllocMaxPairs) return KDB_ERR_CAPACITY;  // scratch holds at most this many pairs
+  // An error already pending on this thread belongs to the caller's earlier
+  // work: leave it in place and launch nothing, so the final check below
+  // only ever reports (and clears) this call's own launch errors.
+  if (cudaPeekAtLastError() != cudaSuccess) return KDB_ERR_CUDA;
   unsigned char* scratch = nullptr;
   int rc = NoAllocScratch(&scratch);
   if (rc != KDB_OK) return rc;

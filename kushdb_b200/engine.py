@@ -37,6 +37,11 @@ EXPORTS = [
     "kdb_mlp_last_error", "kdb_mlp_set_params", "kdb_mlp_get_params", "kdb_mlp_forward", "kdb_mlp_gradient",
     "kdb_mlp_train_step", "kdb_mlp_free", "kdb_ctx_set_skinner_policy", "kdb_last_skinner_samples",
     "kdb_ctx_set_prepared_queries",
+    "kdb_scan_select", "kdb_selvec_size", "kdb_selvec_get", "kdb_selvec_device_rows", "kdb_selvec_free",
+    "kdb_hash_build", "kdb_hash_info", "kdb_hash_probe", "kdb_hash_free", "kdb_pairs_size", "kdb_pairs_get",
+    "kdb_pairs_free", "kdb_agg_create", "kdb_agg_set_pre_aggregation", "kdb_agg_update", "kdb_agg_finalize",
+    "kdb_agg_free", "kdb_index_build", "kdb_index_open_kdbindex", "kdb_index_num_keys", "kdb_index_num_rows",
+    "kdb_index_keys", "kdb_index_get", "kdb_index_free", "kdb_skinner_execute",
 ]
 
 _lib = None
@@ -123,6 +128,42 @@ def load_library(path: str = LIB_PATH):
     L.kdb_ctx_set_skinner_policy.argtypes = [P, I32, P, I32]
     L.kdb_last_skinner_samples.restype = I64
     L.kdb_last_skinner_samples.argtypes = [P, P, P, I64]
+    # per-operator boundary
+    CP = ctypes.c_char_p
+    L.kdb_scan_select.argtypes = [P, CP, P, I32, CP, ctypes.POINTER(P)]
+    L.kdb_selvec_size.restype = I64
+    L.kdb_selvec_size.argtypes = [P]
+    L.kdb_selvec_get.restype = I64
+    L.kdb_selvec_get.argtypes = [P, P, I64]
+    L.kdb_selvec_device_rows.restype = P
+    L.kdb_selvec_device_rows.argtypes = [P]
+    L.kdb_selvec_free.argtypes = [P]
+    L.kdb_hash_build.argtypes = [P, CP, CP, P, ctypes.c_double, I32, ctypes.POINTER(P)]
+    L.kdb_hash_info.argtypes = [P, P, P, P]
+    L.kdb_hash_probe.argtypes = [P, P, CP, CP, P, I32, ctypes.POINTER(P)]
+    L.kdb_hash_free.argtypes = [P]
+    L.kdb_pairs_size.restype = I64
+    L.kdb_pairs_size.argtypes = [P]
+    L.kdb_pairs_get.restype = I64
+    L.kdb_pairs_get.argtypes = [P, P, P, I64]
+    L.kdb_pairs_free.argtypes = [P]
+    L.kdb_agg_create.argtypes = [P, CP, P, I32, P, I32, I64, ctypes.POINTER(P)]
+    L.kdb_agg_set_pre_aggregation.argtypes = [P, I32]
+    L.kdb_agg_update.argtypes = [P, P, P]
+    L.kdb_agg_finalize.argtypes = [P, P, ctypes.POINTER(P)]
+    L.kdb_agg_free.argtypes = [P]
+    L.kdb_index_build.argtypes = [P, CP, CP, ctypes.POINTER(P)]
+    L.kdb_index_open_kdbindex.argtypes = [P, CP, CP, ctypes.POINTER(P)]
+    L.kdb_index_num_keys.restype = I64
+    L.kdb_index_num_keys.argtypes = [P]
+    L.kdb_index_num_rows.restype = I64
+    L.kdb_index_num_rows.argtypes = [P]
+    L.kdb_index_keys.restype = I64
+    L.kdb_index_keys.argtypes = [P, P, I64]
+    L.kdb_index_get.restype = I64
+    L.kdb_index_get.argtypes = [P, I64, P, I64]
+    L.kdb_index_free.argtypes = [P]
+    L.kdb_skinner_execute.argtypes = [P, CP, I32, I64, ctypes.c_uint32, ctypes.POINTER(P)]
     declare_result_api(L, "kdb_")
     _lib = L
     return L

@@ -1,8 +1,8 @@
 """The allocation-free sort entry point (kdb_sort_pairs_noalloc).
 
-Callers that cannot allocate device memory while they sort -- code recording
-a CUDA graph, host callbacks where CUDA allocation calls are not allowed,
-engines that budget all HBM through their own allocator -- use this entry
+Callers that cannot allocate device memory while they sort -- host callbacks
+where CUDA allocation calls are not allowed, engines that budget all HBM
+through their own allocator -- use this entry
 point: its scratch is a static device array, so it never calls cudaMalloc.
 This test runs it through the C ABI and checks it against the allocating
 entry point (kdb_sort_pairs) on the same inputs, twice in a row, so stale
