@@ -72,11 +72,12 @@ def make_workload(name: str, scale: float = 1.0):
         cfg = {"workload": "scan_select+group_by_aggregate+order_by (Q1 shape)", "rows": rows,
                "groups": 4, "aggregates": 8, "predicate": "date<=10471"}
         return [t], wl.group_by_plan(t), rows, rows * wl.GROUP_BY_BYTES_PER_ROW, "group by", cfg
-    if name == "join_group":
+    if name in ("join_group", "join_group_zipf"):
         b_rows, p_rows = int(1_500_000 * scale), int(6_000_000 * scale)
-        b, p = wl.join_tables(build_rows=b_rows, probe_rows=p_rows)
+        zipf = name == "join_group_zipf"
+        b, p = wl.join_tables(build_rows=b_rows, probe_rows=p_rows, zipf=zipf)
         cfg = {"workload": "hash_join+group_by+order_by (Q3 shape)", "build_rows": b_rows,
-               "probe_rows": p_rows, "fk": "uniform"}
+               "probe_rows": p_rows, "fk": "zipf s=1.0" if zipf else "uniform"}
         # groups ~ build rows passing the filters (45.7% x 20%); the dominant
         # kernel is the probe pipeline that aggregates into the groups: it
         # reads the probe columns (20 B/row) and writes 16 B per group
@@ -467,7 +468,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="group_by",
-                    choices=["group_by", "scan_agg", "join_group", "batched", "serving", "skinner"])
+                    choices=["group_by", "scan_agg", "join_group", "join_group_zipf", "batched", "serving",
+                             "skinner"])
     ap.add_argument("--batch-queries", type=int, default=256)
     ap.add_argument("--batch-max-fact", type=int, default=6_000_000)
     ap.add_argument("--rows", type=int, default=0,
@@ -482,6 +484,8 @@ def main():
     ap.add_argument("--serving-budget-gb", type=int, default=32)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-sub", action="store_true",
+                    help="only the headline workload (no scan_agg / join_group lines beside group_by)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
@@ -505,19 +509,117 @@ def main():
     dist = replicas.init("nccl", timeout_s=300)
 
     from kushdb_b200.engine import Engine
+    eng = Engine(local)
+    stream = torch.cuda.ExternalStream(eng.stream_handle())
     scale = 1.0
     if args.rows:
-        scale = args.rows / {"scan_agg": 1_000_000, "group_by": 6_000_000, "join_group": 7_500_000}[args.workload]
-    tables, plan_tree, rows, algo_bytes, dom_tag, cfg = make_workload(args.workload, scale)
+        scale = args.rows / BASE_ROWS[args.workload]
+    with ClockSampler(local) as clocks:
+        line = measure(args.workload, args, eng, stream, local, world, dist, scale, args.steps, args.warmup,
+                       rank == 0)
+    line["clocks"] = clocks.summary()
+    # the other plain configurations under the same clock: scan + ungrouped
+    # aggregate (1M rows) and hash join + group-by (1.5M x 6M, uniform and
+    # Zipf s=1.0 foreign keys)
+    subs = {}
+    if not args.no_sub and args.workload == "group_by" and not args.rows:
+        for sub in ("scan_agg", "join_group", "join_group_zipf"):
+            subs[sub] = measure(sub, args, eng, stream, local, world, dist, 1.0, args.steps, args.warmup, rank == 0)
+    if rank != 0:
+        replicas.finish(dist)
+        return
+    if subs:
+        line["sub"] = subs
+    print(json.dumps(line))
+    replicas.finish(dist)
+
+
+BASE_ROWS = {"scan_agg": 1_000_000, "group_by": 6_000_000, "join_group": 7_500_000, "join_group_zipf": 7_500_000}
+
+
+def _gpu_local_cpus(local: int):
+    """The host CPUs attached to GPU `local`'s NUMA node (empty when unknown)."""
+    try:
+        out = subprocess.run(["nvidia-smi", "-i", str(local), "--query-gpu=pci.bus_id", "--format=csv,noheader"],
+                             capture_output=True, text=True, timeout=20).stdout.strip().lower()
+        bus = out[4:] if out.startswith("0000") and len(out) > 12 else out
+        with open(f"/sys/bus/pci/devices/{bus}/local_cpulist") as f:
+            spec = f.read().strip()
+    except (OSError, subprocess.SubprocessError, ValueError):
+        return set()
+    cpus = set()
+    for part in spec.split(","):
+        if "-" in part:
+            a, b = part.split("-")
+            cpus.update(range(int(a), int(b) + 1))
+        elif part:
+            cpus.add(int(part))
+    return cpus & os.sched_getaffinity(0)
+
+
+def pin_tables(tables, local: int):
+    """Moves every fixed-width column of `tables` into pinned host memory,
+    allocated and first touched from the CPUs next to the GPU so that the
+    pages sit on the GPU's NUMA node.  Returns the pinned tensors (kept
+    alive by the caller) and the bytes per step."""
+    import torch
+    keep, nbytes = [], 0
+    old = os.sched_getaffinity(0)
+    near = _gpu_local_cpus(local)
+    if near:
+        os.sched_setaffinity(0, near)
+    try:
+        for t in tables:
+            for c in t.columns.values():
+                for attr in ("values", "nulls"):
+                    a = getattr(c, attr)
+                    if a is None:
+                        continue
+                    pt = torch.empty(a.nbytes, dtype=torch.uint8, pin_memory=True)
+                    pt.numpy()[:] = np.frombuffer(np.ascontiguousarray(a).tobytes(), np.uint8)
+                    setattr(c, attr, pt.numpy().view(a.dtype))
+                    keep.append(pt)
+                    nbytes += a.nbytes
+    finally:
+        if near:
+            os.sched_setaffinity(0, old)
+    return keep, nbytes, len(near)
+
+
+def pinned_copy_gbs(keep, local: int, stream) -> float:
+    """The host link's rate in this run: the same pinned buffers copied to
+    the device with plain cudaMemcpyAsync, one copy per buffer on one stream
+    (median of 5)."""
+    import torch
+    dev = [torch.empty(k.numel(), dtype=torch.uint8, device=f"cuda:{local}") for k in keep]
+    total = sum(k.numel() for k in keep)
+    ms = []
+    for _ in range(6):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        with torch.cuda.stream(stream):
+            e0.record(stream)
+            for d, h in zip(dev, keep):
+                d.copy_(h, non_blocking=True)
+            e1.record(stream)
+        e1.synchronize()
+        ms.append(e0.elapsed_time(e1))
+    del dev
+    return total / (statistics.median(ms[1:]) / 1e3) / 1e9
+
+
+def measure(name, args, eng, stream, local, world, dist, scale, steps, warmup, with_cpu):
+    """One plain workload: device-resident throughput (CUDA events over
+    exactly `steps` steps, L2 flushed between steps when the inputs fit in
+    it), the dominant kernel's roofline, end to end from pinned host memory
+    through kdb_query_execute_host, and the CPU arm."""
+    import torch
+    from kushdb_b200 import replicas
+    tables, plan_tree, rows, algo_bytes, dom_tag, cfg = make_workload(name, scale)
     plan = plan_tree.to_json().encode()  # the statement text, prepared once like a client would
-    eng = Engine(local)
     for t in tables:
         eng.register_table(t)
-    stream = torch.cuda.ExternalStream(eng.stream_handle())
-
-    # warm-up: compiles the pipelines (cached) and checks the result once
-    for _ in range(args.warmup):
-        res = eng.execute(plan)
+    for _ in range(warmup):  # compiles the pipelines (cached) and records the prepared query
+        eng.execute(plan)
     torch.cuda.synchronize()
 
     # L2 flush between steps: write a 256 MiB buffer, then read another one,
@@ -534,26 +636,24 @@ def main():
                 flush[0].fill_(1)
                 flush[1].sum()
 
-    # timed region: K steps on the engine stream
     replicas.barrier(dist)
     torch.cuda.synchronize()
     launches0 = eng.kernel_launches()
     step_ms = []
-    with ClockSampler(local) as clocks:
-        for _ in range(args.steps):
-            flush_l2()
-            e0 = torch.cuda.Event(enable_timing=True)
-            e1 = torch.cuda.Event(enable_timing=True)
-            e0.record(stream)
-            eng.execute(plan)
-            e1.record(stream)
-            e1.synchronize()
-            step_ms.append(e0.elapsed_time(e1))
+    for _ in range(steps):
+        flush_l2()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        eng.execute(plan)
+        e1.record(stream)
+        e1.synchronize()
+        step_ms.append(e0.elapsed_time(e1))
     torch.cuda.synchronize()
     launches = eng.kernel_launches() - launches0
     total_ms = replicas.max_over_ranks(sum(step_ms), dist, f"cuda:{local}")
     replicas.barrier(dist)
-    value = replicas.whole_job_rate(rows, args.steps, world, total_ms)
+    value = replicas.whole_job_rate(rows, steps, world, total_ms)
 
     # roofline of the dominant kernel: per-launch CUDA events (profiling mode)
     eng.set_profiling(True)
@@ -570,47 +670,41 @@ def main():
     kernels_per_query = {}
     for k in kern[-1]:
         kernels_per_query[k["tag"]] = round(kernels_per_query.get(k["tag"], 0) + k["ms"], 5)
+    del flush
 
-    # end to end through the public API from pinned host memory
+    # end to end through the public API: every step brings the tables from
+    # pinned host memory (chunked copies on several streams) and runs the
+    # query (kdb_query_execute_host); the result comes back to the host
     e2e = None
     if not args.no_e2e:
-        pinned = []
-        h2d = 0
-        for t in tables:
-            for c in t.columns.values():
-                if c.values is not None:
-                    pt = torch.from_numpy(c.values).pin_memory()
-                    c.values = pt.numpy()
-                    pinned.append(pt)
-                    h2d += c.values.nbytes
+        keep, h2d, near = pin_tables(tables, local)
+        link = pinned_copy_gbs(keep, local, stream)
         torch.cuda.synchronize()
         e2e_ms = []
         d2h = 0
-        for i in range(max(3, args.steps // 2) + 1):
+        for i in range(max(3, steps // 2) + 2):
             e0 = torch.cuda.Event(enable_timing=True)
             e1 = torch.cuda.Event(enable_timing=True)
             e0.record(stream)
-            for t in tables:
-                eng.register_table(t)
-            r = eng.execute(plan)
+            r = eng.execute_host(plan, tables)
             e1.record(stream)
             e1.synchronize()
-            if i > 0:
+            if i >= 2:
                 e2e_ms.append(e0.elapsed_time(e1))
             d2h = sum(8 * r.num_rows + r.num_rows for _ in r.columns)
         e2e_med = replicas.max_over_ranks(statistics.median(e2e_ms), dist, f"cuda:{local}")
+        h2d_gbs = h2d / (e2e_med / 1e3) / 1e9
         e2e = {"value": replicas.whole_job_rate(rows, 1, world, e2e_med), "unit": "rows/s",
-               "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
-               "ms_per_step": e2e_med}
-
-    if rank != 0:
-        replicas.finish(dist)
-        return
+               "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h, "ms_per_step": e2e_med,
+               "h2d_gbs": h2d_gbs, "pinned_copy_gbs": link, "link_frac": h2d_gbs / link,
+               "pinned_numa_local_cpus": near,
+               "path": "kdb_query_execute_host: chunked H2D on copy streams, then the query"}
+        del keep
 
     cpu = None
-    if not args.no_cpu_baseline:
+    if with_cpu and not args.no_cpu_baseline:
         try:
-            v, info = cpu_baseline(args.workload, tables, rows)
+            v, info = cpu_baseline(name, tables, rows)
             cpu = {"value": v, "unit": "rows/s", "cores": info["threads"], "kind": "port",
                    "single_thread_value": info["single_thread_rows_per_second"],
                    "sample": f"full workload ({info['rows']} rows), best of {info['repeats']}: "
@@ -619,29 +713,27 @@ def main():
                              "(oracle/baseline.cc), rows split over the threads"}
         except Exception as ex:  # the oracle is a reported baseline, not the product
             cpu = {"value": None, "unit": "rows/s", "cores": 0, "kind": "port", "sample": f"failed: {ex}"}
+    for t in tables:
+        eng.drop_table(t.name)
 
     cfg = dict(cfg)
-    cfg["l2"] = "flushed between steps (256 MiB write, then 256 MiB read)" if flush is not None else \
+    cfg["l2"] = "flushed between steps (256 MiB write, then 256 MiB read)" if algo_bytes < 2 * L2_BYTES else \
         "inputs larger than L2 (126 MB)"
-    line = {
+    return {
         "metric": "rows_per_second", "value": value, "unit": "rows/s", "n_gpus": world,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": total_ms / args.steps,
+        "steps": steps, "warmup": warmup, "ms_per_step": total_ms / steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic", "config": cfg,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": (achieved / peak) if achieved else None,
-                     "traffic": (round(MEASURED_TRAFFIC[args.workload] * scale)
-                                 if args.workload in MEASURED_TRAFFIC else None),
+                     "traffic": (round(MEASURED_TRAFFIC[name] * scale) if name in MEASURED_TRAFFIC else None),
                      "kernel": dom_tag, "kernel_ms": dom_ms, "algorithmic_bytes": algo_bytes,
                      "peak_source": f"{peak_kind} hbm_gbs"},
         "cpu_baseline": cpu,
         "e2e": e2e,
         "gpu_launches": launches,
         "kernels_ms_per_query": kernels_per_query,
-        "clocks": clocks.summary(),
     }
-    print(json.dumps(line))
-    replicas.finish(dist)
 
 
 if __name__ == "__main__":

@@ -109,6 +109,27 @@ int kdb_enum_open_kdbenum(kdb_ctx* ctx, int32_t enum_id, const char* path);
  * NVRTC and cached by plan shape) and runs them; the result stays on the
  * host in `out`. */
 int kdb_query_execute(kdb_ctx* ctx, const char* plan_json, kdb_result** out);
+/* End to end from host memory: brings the listed fixed-width columns into
+ * HBM (added, or refreshed in place when the table already holds a column of
+ * that name, type and row count) and runs the plan over them, returning
+ * when the result is on the host.  The copies are split into chunks spread
+ * over several copy streams, all in flight together with no
+ * synchronisation between columns (kdb_ctx_set_ingest); pinned host memory
+ * copies at the full host-link rate.  Like kdb_table_add_column this changes
+ * the tables, so prepared recordings of plans over them are dropped. */
+typedef struct {
+  const char* table;
+  const char* column;
+  const char* type;     /* as kdb_table_add_column */
+  const void* data;     /* n values in the type's physical width */
+  int64_t n;
+  const int8_t* nulls;  /* optional, one byte per row, 1 = NULL */
+} kdb_host_column;
+int kdb_query_execute_host(kdb_ctx* ctx, const char* plan_json, const kdb_host_column* cols, int32_t ncols,
+                           kdb_result** out);
+/* Chunk size (>= 64 KiB) and copy streams (1-8) of host-to-device column
+ * copies (kdb_query_execute_host); defaults 8 MiB and 2. */
+int kdb_ctx_set_ingest(kdb_ctx* ctx, int64_t chunk_bytes, int32_t streams);
 /* Device time (ms, CUDA events) of the last kdb_query_execute's pipelines,
  * excluding result download, and the bytes read from table columns. */
 double kdb_last_query_device_ms(kdb_ctx* ctx);

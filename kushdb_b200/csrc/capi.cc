@@ -48,6 +48,10 @@ std::vector<char> ReadFile(const std::string& path) {
 
 }  // namespace
 
+namespace {
+void RunPlan(kdb_ctx* ctx, const char* plan_json, kdb_result** out);
+}  // namespace
+
 kdb::Context* kdb_ctx_context(kdb_ctx* ctx) { return ctx->c.get(); }
 void kdb_ctx_set_error(kdb_ctx* ctx, const std::string& msg) {
   if (ctx) ctx->err = msg;
@@ -135,23 +139,11 @@ int kdb_column_open_kdb(kdb_ctx* ctx, const char* table, const char* column, con
     if (null_path && *null_path) nulls = ReadFile(null_path);
     const int8_t* np = nulls.empty() ? nullptr : reinterpret_cast<const int8_t*>(nulls.data());
     if (t.id == kdb::plan::TypeId::TEXT) {
-      if (raw.size() < 8) throw kdb::Error(KDB_ERR_INVALID, "short TEXT file");
-      int32_t card;
-      std::memcpy(&card, raw.data(), 4);
-      std::vector<int64_t> off(card + 1, 0);
-      std::string chars;
-      for (int32_t r = 0; r < card; r++) {
-        int32_t len;
-        uint64_t o;
-        std::memcpy(&len, raw.data() + 8 + 16 * r, 4);
-        std::memcpy(&o, raw.data() + 8 + 16 * r + 8, 8);
-        if (o + len > raw.size()) throw kdb::Error(KDB_ERR_INVALID, "corrupt TEXT file");
-        chars.append(raw.data() + o, len);
-        off[r + 1] = static_cast<int64_t>(chars.size());
-      }
-      ctx->c->AddTextColumn(table, column, off.data(), chars.data(), card, np);
+      ctx->c->AddTextColumnFromKdb(table, column, raw.data(), raw.size(), np,
+                                   static_cast<int64_t>(nulls.size()));
     } else {
       int w = kdb::plan::TypeWidth(t.id);
+      if (raw.size() % w) throw kdb::Error(KDB_ERR_INVALID, "file length is not a multiple of the type's width");
       int64_t n = static_cast<int64_t>(raw.size()) / w;
       if (np && static_cast<int64_t>(nulls.size()) != n)
         throw kdb::Error(KDB_ERR_INVALID, "null file length differs from column length");
@@ -184,21 +176,32 @@ int kdb_enum_register(kdb_ctx* ctx, int32_t enum_id, const int64_t* offsets, con
 int kdb_enum_open_kdbenum(kdb_ctx* ctx, int32_t enum_id, const char* path) {
   return Guard(ctx, [&] {
     std::vector<char> raw = ReadFile(path);
-    if (raw.size() < 16) throw kdb::Error(KDB_ERR_INVALID, "short .kdbenum file");
+    const uint64_t size = raw.size();
+    if (size < 16) throw kdb::Error(KDB_ERR_INVALID, "short .kdbenum file");
     uint64_t entry_offset;
     std::memcpy(&entry_offset, raw.data(), 8);
-    std::vector<std::string> values;
-    uint64_t first_str = UINT64_MAX;
-    for (uint64_t pos = entry_offset; pos + 16 <= raw.size() && pos < first_str; pos += 16) {
+    if (entry_offset < 16 || entry_offset > size) throw kdb::Error(KDB_ERR_INVALID, "corrupt .kdbenum file (header)");
+    // entries are dense in key order; the first string follows the last entry
+    uint64_t n = 0;
+    if (entry_offset + 16 <= size) {
+      uint64_t first_str;
+      std::memcpy(&first_str, raw.data() + entry_offset, 8);
+      if (first_str < entry_offset + 16 || first_str > size || (first_str - entry_offset) % 16)
+        throw kdb::Error(KDB_ERR_INVALID, "corrupt .kdbenum file (entries)");
+      n = (first_str - entry_offset) / 16;
+    }
+    if (n > static_cast<uint64_t>(INT32_MAX)) throw kdb::Error(KDB_ERR_INVALID, "corrupt .kdbenum file (size)");
+    std::vector<std::string> values(n);
+    for (uint64_t k = 0; k < n; k++) {
+      const uint64_t pos = entry_offset + 16 * k;
       uint64_t so;
       uint32_t sl, v;
       std::memcpy(&so, raw.data() + pos, 8);
       std::memcpy(&sl, raw.data() + pos + 8, 4);
       std::memcpy(&v, raw.data() + pos + 12, 4);
-      if (first_str == UINT64_MAX) first_str = so;
-      if (so + sl > raw.size()) throw kdb::Error(KDB_ERR_INVALID, "corrupt .kdbenum file");
-      if (v >= values.size()) values.resize(v + 1);
-      values[v] = std::string(raw.data() + so, sl);
+      if (v != k || so > size || sl > size - so)
+        throw kdb::Error(KDB_ERR_INVALID, "corrupt .kdbenum file (entry " + std::to_string(k) + ")");
+      values[k] = std::string(raw.data() + so, sl);
     }
     ctx->c->RegisterEnum(enum_id, std::move(values));
   });
@@ -206,7 +209,40 @@ int kdb_enum_open_kdbenum(kdb_ctx* ctx, int32_t enum_id, const char* path) {
 
 int kdb_query_execute(kdb_ctx* ctx, const char* plan_json, kdb_result** out) {
   if (out) *out = nullptr;
+  return Guard(ctx, [&] { RunPlan(ctx, plan_json, out); });
+}
+
+int kdb_query_execute_host(kdb_ctx* ctx, const char* plan_json, const kdb_host_column* cols, int32_t ncols,
+                           kdb_result** out) {
+  if (out) *out = nullptr;
   return Guard(ctx, [&] {
+    if (ncols < 0 || (ncols > 0 && !cols)) throw kdb::Error(KDB_ERR_INVALID, "bad column list");
+    std::vector<kdb::Context::HostColumnSpec> specs;
+    for (int32_t i = 0; i < ncols; i++) {
+      const kdb_host_column& c = cols[i];
+      if (!c.table || !c.column || !c.type) throw kdb::Error(KDB_ERR_INVALID, "null column field");
+      specs.push_back({c.table, c.column, kdb::plan::ParseType(c.type), c.data, c.n, c.nulls});
+    }
+    ctx->c->StreamColumns(specs);
+    RunPlan(ctx, plan_json, out);
+  });
+}
+
+int kdb_ctx_set_ingest(kdb_ctx* ctx, int64_t chunk_bytes, int32_t streams) {
+  return Guard(ctx, [&] {
+    if (chunk_bytes < (1 << 16) || streams < 1 || streams > 8)
+      throw kdb::Error(KDB_ERR_INVALID, "chunk of at least 64 KiB, 1 to 8 streams");
+    ctx->c->ingest_chunk_bytes = chunk_bytes;
+    ctx->c->ingest_streams = streams;
+  });
+}
+
+}  // extern "C"
+
+namespace {
+
+void RunPlan(kdb_ctx* ctx, const char* plan_json, kdb_result** out) {
+  {
     if (!plan_json || !out) throw kdb::Error(KDB_ERR_INVALID, "null argument");
     // parsed plans are cached by their text (a prepared statement's tree)
     auto& cache = ctx->plans;
@@ -230,8 +266,12 @@ int kdb_query_execute(kdb_ctx* ctx, const char* plan_json, kdb_result** out) {
           if (&e != &entry) e.prepared.reset();
     }
     *out = res.release();
-  });
+  }
 }
+
+}  // namespace
+
+extern "C" {
 
 int kdb_ctx_set_prepared_queries(kdb_ctx* ctx, int32_t on) {
   return Guard(ctx, [&] {

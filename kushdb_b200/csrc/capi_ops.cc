@@ -256,7 +256,6 @@ int kdb_index_open_kdbindex(kdb_ctx* ctx, const char* path, const char* type, kd
       case kdb::plan::TypeId::BIGINT: w = 8; break;
       default: throw kdb::Error(KDB_ERR_UNSUPPORTED, "indexes over integer, date, enum or boolean keys");
     }
-    if (c.dry) throw kdb::Error(KDB_ERR_UNSUPPORTED, "operators need a device context");
     *out = new kdb_index{kdb::ops::IndexFromPostings(c, t, ReadKdbIndex(ReadAll(path), w))};
   });
 }
@@ -267,7 +266,7 @@ int64_t kdb_index_num_rows(const kdb_index* i) { return i ? i->i->n : -1; }
 int64_t kdb_index_get(const kdb_index* i, int64_t key, int32_t* rows, int64_t cap) {
   if (!i) return KDB_ERR_INVALID;
   try {
-    cudaSetDevice(i->i->ctx->device);
+    if (!i->i->ctx->dry) cudaSetDevice(i->i->ctx->device);
     return i->i->Get(key, rows, cap);
   } catch (const std::exception&) {
     return KDB_ERR_CUDA;

@@ -901,13 +901,20 @@ void Executor::EmitStream(KernelSource& ks, ExprGen& eg, const Operator& op, con
       } else {
         ks.Open("for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < (int64_t)" + n +
                 "; r += (int64_t)gridDim.x * blockDim.x)");
-        load = [&](size_t k) {
+        // The probe side of a join reads its columns where the consumer uses
+        // them: the probe key at once, every other column only inside the
+        // match branch, so rows without a match never load them (about a
+        // third of the sectors of a 9%-selective probe).
+        const bool lazy = probe_side && !std::getenv("KDB_EAGER_PROBE_COLUMNS");
+        load = [&, lazy](size_t k) {
           const DevColumn& c = *cols[k];
           std::string v;
           if (c.type.id == TypeId::TEXT) v = "kdb_text_at(" + dp[k] + ", " + tp[k] + ", r)";
           else if (c.type.id == TypeId::BOOLEAN) v = "(" + dp[k] + "[r] != 0)";
           else v = dp[k] + "[r]";
-          scan[k] = eg.Bind(c.type, v, np[k].empty() ? "false" : "(" + np[k] + "[r] != 0)");
+          const std::string nul = np[k].empty() ? "false" : "(" + np[k] + "[r] != 0)";
+          if (lazy) scan[k] = CVal{c.type, "(" + v + ")", nul};
+          else scan[k] = eg.Bind(c.type, v, nul);
         };
       }
       auto close_loop = [&]() {

@@ -247,6 +247,10 @@ Context::~Context() {
     std::free(stage_);
     return;
   }
+  for (cudaStream_t cs : copy_streams_) cudaStreamSynchronize(cs);
+  for (cudaStream_t cs : copy_streams_) cudaStreamDestroy(cs);
+  for (cudaEvent_t e : copy_events_) cudaEventDestroy(e);
+  if (copy_start_) cudaEventDestroy(copy_start_);
   if (stage_) cudaFreeHost(stage_);
   cudaSetDevice(device);
   if (dev_stage_) cudaFreeAsync(dev_stage_, stream);
@@ -317,6 +321,80 @@ void Context::AddColumn(const std::string& table, const std::string& column, con
   t.cols[column] = c;
 }
 
+int64_t Context::StreamColumns(const std::vector<HostColumnSpec>& cols) {
+  catalog_version++;
+  struct Copy {
+    void* dst;
+    const char* src;
+    size_t bytes;
+  };
+  std::vector<Copy> copies;
+  for (const auto& spec : cols) {
+    if (spec.type.id == plan::TypeId::TEXT) throw Error(-1, "TEXT columns use kdb_table_add_text_column");
+    if (spec.n < 0 || (spec.n > 0 && !spec.data)) throw Error(-1, "bad host column " + spec.column);
+    DevTable& t = tables[spec.table];
+    CheckRows(t, spec.n, spec.column);
+    const size_t w = plan::TypeWidth(spec.type.id);
+    auto it = t.cols.find(spec.column);
+    DevColumn* c = nullptr;
+    if (it != t.cols.end() && it->second.type == spec.type && it->second.n == spec.n &&
+        (it->second.nulls != nullptr) == (spec.nulls != nullptr)) {
+      c = &it->second;  // same shape: refreshed in place
+    } else {
+      if (it != t.cols.end()) {
+        if (!dry) KDB_CUDA(cudaStreamSynchronize(stream));
+        FreeColumn(it->second);
+      }
+      DevColumn nc;
+      nc.type = spec.type;
+      nc.n = spec.n;
+      nc.bytes = w * spec.n;
+      nc.data = DevAlloc(std::max<size_t>(nc.bytes, 16));
+      if (spec.nulls) {
+        nc.nulls = static_cast<int8_t*>(DevAlloc(std::max<int64_t>(spec.n, 16)));
+        nc.bytes += spec.n;
+      }
+      t.cols[spec.column] = nc;
+      c = &t.cols[spec.column];
+    }
+    if (w * spec.n) copies.push_back({c->data, static_cast<const char*>(spec.data), w * spec.n});
+    if (spec.nulls && spec.n) copies.push_back({c->nulls, reinterpret_cast<const char*>(spec.nulls),
+                                                static_cast<size_t>(spec.n)});
+  }
+  int64_t total = 0;
+  for (const auto& cp : copies) total += static_cast<int64_t>(cp.bytes);
+  if (dry || copies.empty()) return total;
+  const int ns = std::max(1, std::min(ingest_streams, 8));
+  while (static_cast<int>(copy_streams_.size()) < ns) {
+    cudaStream_t cs;
+    cudaEvent_t ev;
+    KDB_CUDA(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
+    KDB_CUDA(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+    copy_streams_.push_back(cs);
+    copy_events_.push_back(ev);
+  }
+  if (!copy_start_) KDB_CUDA(cudaEventCreateWithFlags(&copy_start_, cudaEventDisableTiming));
+  // the copies start after the work already queued on the context's stream
+  // (which may still read the columns being refreshed)
+  KDB_CUDA(cudaEventRecord(copy_start_, stream));
+  for (int i = 0; i < ns; i++) KDB_CUDA(cudaStreamWaitEvent(copy_streams_[i], copy_start_, 0));
+  const size_t chunk = static_cast<size_t>(std::max<int64_t>(ingest_chunk_bytes, 1 << 16));
+  int next = 0;
+  for (const auto& cp : copies) {
+    for (size_t off = 0; off < cp.bytes; off += chunk) {
+      const size_t b = std::min(chunk, cp.bytes - off);
+      KDB_CUDA(cudaMemcpyAsync(static_cast<char*>(cp.dst) + off, cp.src + off, b, cudaMemcpyHostToDevice,
+                               copy_streams_[next]));
+      next = (next + 1) % ns;
+    }
+  }
+  for (int i = 0; i < ns; i++) {
+    KDB_CUDA(cudaEventRecord(copy_events_[i], copy_streams_[i]));
+    KDB_CUDA(cudaStreamWaitEvent(stream, copy_events_[i], 0));
+  }
+  return total;
+}
+
 void Context::AddTextColumn(const std::string& table, const std::string& column,
                             const int64_t* offsets, const char* chars, int64_t n,
                             const int8_t* nulls) {
@@ -344,6 +422,60 @@ void Context::AddTextColumn(const std::string& table, const std::string& column,
     c.nulls = static_cast<int8_t*>(DevAlloc(std::max<int64_t>(n, 16)));
     H2D(c.nulls, nulls, n);
     c.bytes += n;
+  }
+  if (!dry) KDB_CUDA(cudaStreamSynchronize(stream));
+  t.cols[column] = c;
+}
+
+void Context::AddTextColumnFromKdb(const std::string& table, const std::string& column, const char* raw,
+                                   size_t size, const int8_t* nulls, int64_t null_rows) {
+  if (size < 8) throw Error(-1, "short TEXT file");
+  int32_t card;
+  std::memcpy(&card, raw, 4);
+  if (card < 0) throw Error(-1, "TEXT file with a negative cardinality");
+  const uint64_t meta_end = 8 + 16 * static_cast<uint64_t>(card);
+  if (meta_end > size) throw Error(-1, "TEXT file shorter than its metadata");
+  if (nulls && null_rows != card) throw Error(-1, "null file length differs from column length");
+  int32_t max_len = 0;
+  uint64_t nbytes = 0;
+  for (int32_t r = 0; r < card; r++) {
+    int32_t len;
+    uint64_t o;
+    std::memcpy(&len, raw + 8 + 16 * static_cast<uint64_t>(r), 4);
+    std::memcpy(&o, raw + 8 + 16 * static_cast<uint64_t>(r) + 8, 8);
+    if (len < 0 || o < meta_end || o > size || static_cast<uint64_t>(len) > size - o)
+      throw Error(-1, "corrupt TEXT file (slot " + std::to_string(r) + ")");
+    max_len = std::max(max_len, len);
+    nbytes += static_cast<uint64_t>(len);
+  }
+  catalog_version++;
+  DevTable& t = tables[table];
+  CheckRows(t, card, column);
+  auto it = t.cols.find(column);
+  if (it != t.cols.end()) {
+    if (!dry) KDB_CUDA(cudaStreamSynchronize(stream));
+    FreeColumn(it->second);
+  }
+  DevColumn c;
+  c.type = plan::Type{plan::TypeId::TEXT, 0};
+  c.n = card;
+  c.max_text_len = max_len;
+  c.toff = static_cast<int64_t*>(DevAlloc(sizeof(int64_t) * (card + 1)));
+  c.tchars = static_cast<char*>(DevAlloc(std::max<uint64_t>(nbytes, 16)));
+  c.bytes = sizeof(int64_t) * (card + 1) + nbytes;
+  if (!dry && card > 0) {
+    void* d_raw = nullptr;
+    KDB_CUDA(cudaMallocAsync(&d_raw, size, stream));
+    KDB_CUDA(cudaMemcpyAsync(d_raw, raw, size, cudaMemcpyHostToDevice, stream));
+    DecodeKdbText(static_cast<const char*>(d_raw), card, c.toff, c.tchars);
+    KDB_CUDA(cudaFreeAsync(d_raw, stream));
+  } else if (!dry) {
+    Memset(c.toff, 0, sizeof(int64_t));
+  }
+  if (nulls) {
+    c.nulls = static_cast<int8_t*>(DevAlloc(std::max<int64_t>(card, 16)));
+    H2D(c.nulls, nulls, card);
+    c.bytes += card;
   }
   if (!dry) KDB_CUDA(cudaStreamSynchronize(stream));
   t.cols[column] = c;

@@ -236,8 +236,34 @@ class Context {
 
   void AddColumn(const std::string& table, const std::string& column, const plan::Type& type,
                  const void* data, int64_t n, const int8_t* nulls);
+  // A fixed-width column in host memory to bring into HBM.
+  struct HostColumnSpec {
+    std::string table, column;
+    plan::Type type;
+    const void* data = nullptr;
+    int64_t n = 0;
+    const int8_t* nulls = nullptr;
+  };
+  // Adds or refreshes fixed-width columns from host memory with every copy
+  // split into chunks spread over the copy streams, all in flight together
+  // (no synchronisation between columns); the context's stream waits for
+  // all of them, so work issued on it afterwards sees the new contents.
+  // The host memory must stay unchanged until that work has run (pinned
+  // memory copies asynchronously; pageable memory is copied before the
+  // call returns).  Returns the bytes copied.
+  int64_t StreamColumns(const std::vector<HostColumnSpec>& cols);
+  // Chunk size and number of copy streams used by StreamColumns.
+  int64_t ingest_chunk_bytes = int64_t(8) << 20;
+  int ingest_streams = 2;
   void AddTextColumn(const std::string& table, const std::string& column, const int64_t* offsets,
                      const char* chars, int64_t n, const int8_t* nulls);
+  // A reference TEXT .kdb file's bytes (runtime/column_data.h:45-57:
+  // StringMetadata {int32 cardinality; {int32 length; uint64 offset}[]}, then
+  // the strings): the metadata is checked on the host against the file
+  // size, the file goes to HBM in one copy, and the device decodes it into
+  // the column's offsets and bytes (a scan of the lengths, one gather).
+  void AddTextColumnFromKdb(const std::string& table, const std::string& column, const char* raw,
+                            size_t size, const int8_t* nulls, int64_t null_rows);
   void DropTable(const std::string& table);
   void RegisterEnum(int32_t id, std::vector<std::string> values);
   int64_t ColumnBytes() const;
@@ -292,6 +318,8 @@ class Context {
   // gathers the segments into the device staging buffer and queues one copy
   // of `total` bytes to `host` (pinned); the caller synchronises
   void PackToHost(const PackSegs& segs, size_t total, void* host);
+  // device decode of a TEXT .kdb image at d_raw (kernels.cu)
+  void DecodeKdbText(const char* d_raw, int64_t n, int64_t* toff, char* tchars);
   void CheckDeviceError(const char* what);
 
   EnumDicts HostEnums() const;
@@ -304,6 +332,9 @@ class Context {
   std::shared_ptr<HostBlockPool> host_blocks_;
   void* dev_stage_ = nullptr;  // device side of PackToHost
   size_t dev_stage_bytes_ = 0;
+  std::vector<cudaStream_t> copy_streams_;  // StreamColumns
+  std::vector<cudaEvent_t> copy_events_;
+  cudaEvent_t copy_start_ = nullptr;
   void FreeColumn(DevColumn& c);
 };
 

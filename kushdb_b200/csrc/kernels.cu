@@ -499,6 +499,44 @@ __global__ void CopyPairs(const uint64_t* __restrict__ ks, const uint32_t* __res
 
 }  // namespace
 
+namespace {
+// lengths of a TEXT .kdb image's slots (validated on the host) into toff[r]
+__global__ void KdbTextLengths(const char* __restrict__ raw, int64_t n, int64_t* __restrict__ toff) {
+  for (int64_t r = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; r < n;
+       r += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    int32_t len;
+    memcpy(&len, raw + 8 + 16 * r, 4);
+    toff[r] = len;
+  }
+}
+// one warp per string: its bytes from the image to the column's byte array
+__global__ void KdbTextGather(const char* __restrict__ raw, int64_t n, const int64_t* __restrict__ toff,
+                              char* __restrict__ chars) {
+  const int lane = threadIdx.x & 31;
+  for (int64_t r = (blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x) >> 5; r < n;
+       r += (static_cast<int64_t>(gridDim.x) * blockDim.x) >> 5) {
+    uint64_t o;
+    memcpy(&o, raw + 8 + 16 * r + 8, 8);
+    const int64_t b = toff[r], len = toff[r + 1] - b;
+    for (int64_t i = lane; i < len; i += 32) chars[b + i] = raw[o + i];
+  }
+}
+}  // namespace
+
+void Context::DecodeKdbText(const char* d_raw, int64_t n, int64_t* toff, char* tchars) {
+  if (dry || n <= 0) return;
+  TimedStart("text decode");
+  KdbTextLengths<<<GridFor(n, 256), 256, 0, stream>>>(d_raw, n, toff);
+  kernel_launches++;
+  TimedStop();
+  ScanU64(reinterpret_cast<uint64_t*>(toff), n, "text decode offsets");
+  TimedStart("text decode");
+  KdbTextGather<<<GridFor(n * 32, 256), 256, 0, stream>>>(d_raw, n, toff, tchars);
+  kernel_launches++;
+  TimedStop();
+  KDB_CUDA(cudaGetLastError());
+}
+
 void Context::PackToHost(const PackSegs& segs, size_t total, void* host) {
   if (dry || segs.n == 0) return;
   uint64_t most = 0;

@@ -782,6 +782,7 @@ constexpr int kMaxAggs = 8;
 constexpr int kLocalGroups = 512;   // shared-memory pre-aggregation entries per CTA
 constexpr int kLocalProbes = 16;
 constexpr uint32_t kLocked = 0xffffffffu;  // slot claimed, group not yet published
+constexpr uint32_t kDead = 0xfffffffeu;    // slot claimed when the group arrays were full
 
 struct AggCols {
   const void* kd[kMaxAggKeys];
@@ -854,6 +855,8 @@ __device__ int64_t FindGroup(const AggDev& a, int nkeys, const int64_t* kv, cons
       if (s == 0) {
         const unsigned long long g = atomicAdd(a.ngroups, 1ULL);
         if (static_cast<int64_t>(g) >= a.G) {
+          // no group id left: the slot is marked so that its waiters stop
+          atomicExch(&a.slots[i], (static_cast<unsigned long long>(h32) << 32) | kDead);
           atomicOr(a.err, kErrFull);
           return -1;
         }
@@ -872,6 +875,10 @@ __device__ int64_t FindGroup(const AggDev& a, int nkeys, const int64_t* kv, cons
         s = *reinterpret_cast<volatile unsigned long long*>(&a.slots[i]);
       if (static_cast<uint32_t>(s) == kLocked) {
         atomicOr(a.err, kErrWait);
+        return -1;
+      }
+      if (static_cast<uint32_t>(s) == kDead) {
+        atomicOr(a.err, kErrFull);
         return -1;
       }
       __threadfence();
@@ -1364,7 +1371,7 @@ __global__ void RunHeadWrite(const unsigned long long* __restrict__ keys, int64_
 }  // namespace
 
 ColumnIndex::~ColumnIndex() {
-  if (!ctx) return;
+  if (!ctx || ctx->dry) return;
   cudaSetDevice(ctx->device);
   if (rows) cudaFree(rows);
   if (dkeys) cudaFree(dkeys);
@@ -1378,7 +1385,8 @@ int64_t ColumnIndex::Get(int64_t key, int32_t* out, int64_t cap) const {
   const int64_t b = hstarts[k], e = hstarts[k + 1];
   if (out && cap > 0) {
     const int64_t m = std::min(cap, e - b);
-    KDB_CUDA(cudaMemcpy(out, rows + b, sizeof(int32_t) * m, cudaMemcpyDeviceToHost));
+    if (!rows) std::memcpy(out, hrows.data() + b, sizeof(int32_t) * m);
+    else KDB_CUDA(cudaMemcpy(out, rows + b, sizeof(int32_t) * m, cudaMemcpyDeviceToHost));
   }
   return e - b;
 }
@@ -1470,6 +1478,10 @@ std::unique_ptr<ColumnIndex> IndexFromPostings(Context& c, plan::Type type,
   }
   idx->n = static_cast<int64_t>(rows.size());
   idx->nkeys = static_cast<int64_t>(idx->hkeys.size());
+  if (c.dry) {  // compile-only context: the posting lists stay on the host
+    idx->hrows = std::move(rows);
+    return idx;
+  }
   idx->rows = static_cast<int32_t*>(c.DevAlloc(sizeof(int32_t) * std::max<size_t>(rows.size(), 1)));
   idx->dkeys = static_cast<int64_t*>(c.DevAlloc(sizeof(int64_t) * std::max<size_t>(idx->hkeys.size(), 1)));
   idx->starts = static_cast<int64_t*>(c.DevAlloc(sizeof(int64_t) * idx->hstarts.size()));

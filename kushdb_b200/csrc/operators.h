@@ -100,6 +100,7 @@ struct ColumnIndex {
   int64_t* dkeys = nullptr;  // device, nkeys ascending
   int64_t* starts = nullptr;  // device, nkeys + 1
   std::vector<int64_t> hkeys, hstarts;  // host mirrors
+  std::vector<int32_t> hrows;           // the rows, in a compile-only context
   // rows of `key` (at most cap copied to out); returns how many there are
   int64_t Get(int64_t key, int32_t* out, int64_t cap) const;
   ~ColumnIndex();

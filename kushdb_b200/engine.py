@@ -42,6 +42,7 @@ EXPORTS = [
     "kdb_pairs_free", "kdb_agg_create", "kdb_agg_set_pre_aggregation", "kdb_agg_update", "kdb_agg_finalize",
     "kdb_agg_free", "kdb_index_build", "kdb_index_open_kdbindex", "kdb_index_num_keys", "kdb_index_num_rows",
     "kdb_index_keys", "kdb_index_get", "kdb_index_free", "kdb_skinner_execute",
+    "kdb_query_execute_host", "kdb_ctx_set_ingest",
 ]
 
 _lib = None
@@ -164,6 +165,8 @@ def load_library(path: str = LIB_PATH):
     L.kdb_index_get.argtypes = [P, I64, P, I64]
     L.kdb_index_free.argtypes = [P]
     L.kdb_skinner_execute.argtypes = [P, CP, I32, I64, ctypes.c_uint32, ctypes.POINTER(P)]
+    L.kdb_query_execute_host.argtypes = [P, CP, P, I32, ctypes.POINTER(P)]
+    L.kdb_ctx_set_ingest.argtypes = [P, I64, I32]
     declare_result_api(L, "kdb_")
     _lib = L
     return L
@@ -171,6 +174,12 @@ def load_library(path: str = LIB_PATH):
 
 def _ptr(a):
     return None if a is None else a.ctypes.data_as(ctypes.c_void_p)
+
+
+class HostColumnSpec(ctypes.Structure):
+    """kdb_host_column"""
+    _fields_ = [("table", ctypes.c_char_p), ("column", ctypes.c_char_p), ("type", ctypes.c_char_p),
+                ("data", ctypes.c_void_p), ("n", ctypes.c_int64), ("nulls", ctypes.c_void_p)]
 
 
 class Engine:
@@ -237,6 +246,52 @@ class Engine:
                 self._check(self.lib.kdb_table_add_column(
                     self.ctx, name, c.name.encode(), c.type.to_json().encode(), _ptr(v), len(v),
                     _ptr(nulls)))
+
+    def execute_host(self, plan, tables, fetch: bool = True):
+        """End to end from host memory: brings every fixed-width column of
+        `tables` into HBM (chunked copies on several streams, all in flight
+        together) and runs the plan over them (kdb_query_execute_host)."""
+        text = plan.to_json() if isinstance(plan, Operator) else plan
+        if isinstance(text, str):
+            text = text.encode()
+        self.register_enums()
+        specs, keep = [], []
+        for t in tables:
+            for c in t.columns.values():
+                if c.type.type_id == "TEXT":
+                    raise ValueError("execute_host takes fixed-width columns")
+                v = np.ascontiguousarray(c.values)
+                nl = None if c.nulls is None else np.ascontiguousarray(c.nulls, np.int8)
+                names = (t.name.encode(), c.name.encode(), c.type.to_json().encode())
+                keep.append((v, nl, names))
+                specs.append((names, v, nl))
+        arr = (HostColumnSpec * max(len(specs), 1))()
+        for i, (names, v, nl) in enumerate(specs):
+            arr[i].table, arr[i].column, arr[i].type = names
+            arr[i].data = v.ctypes.data_as(ctypes.c_void_p)
+            arr[i].n = len(v)
+            arr[i].nulls = None if nl is None else nl.ctypes.data_as(ctypes.c_void_p)
+        h = ctypes.c_void_p()
+        self._check(self.lib.kdb_query_execute_host(self.ctx, text, ctypes.cast(arr, ctypes.c_void_p), len(specs),
+                                                    ctypes.byref(h)))
+        del keep
+        if not fetch:
+            n = self.lib.kdb_result_num_rows(h)
+            self.lib.kdb_result_free(h)
+            return n
+        return Result.from_handle(self.lib, "kdb_", self.ctx, h, owner=self)
+
+    def open_kdb(self, table: str, column: str, type_str: str, path: str, null_path: str = "") -> None:
+        """Reads a reference .kdb column file (and its _null.kdb) into HBM."""
+        self._check(self.lib.kdb_column_open_kdb(self.ctx, table.encode(), column.encode(), type_str.encode(),
+                                                 path.encode(), null_path.encode()))
+
+    def open_kdbenum(self, enum_id: int, path: str) -> None:
+        """Reads a reference .kdbenum dictionary."""
+        self._check(self.lib.kdb_enum_open_kdbenum(self.ctx, enum_id, path.encode()))
+
+    def set_ingest(self, chunk_bytes: int = 8 << 20, streams: int = 2) -> None:
+        self._check(self.lib.kdb_ctx_set_ingest(self.ctx, chunk_bytes, streams))
 
     def drop_table(self, name: str) -> None:
         self._check(self.lib.kdb_table_drop(self.ctx, name.encode()))

@@ -7,7 +7,11 @@ Reads the reference's end-to-end test inputs (``end_to_end_test/data/*.kdb``,
 * ``tests/golden/tables/<table>.npz`` -- the columns the parity tests scan
   (text columns as int64 offsets + bytes, null flags as int8);
 * ``tests/golden/enums.json`` -- enum dictionaries (key -> string);
-* ``tests/golden/expected/<operator>/<name>.tbl`` -- the expected tables.
+* ``tests/golden/expected/<operator>/<name>.tbl`` -- the expected tables;
+* ``tests/golden/kdb/`` -- the raw reference files (``.kdb``, ``_null.kdb``,
+  ``.kdbenum``, ``.kdbindex``) of the small tables in RAW_KDB, byte for byte,
+  for the tests of the file readers (kdb_column_open_kdb,
+  kdb_enum_open_kdbenum, kdb_index_open_kdbindex).
 
 File formats read (reference):
 * fixed-width ``.kdb``: raw little-endian values (runtime/column_data.cc:121-172);
@@ -30,6 +34,10 @@ import sys
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
+
+# stems whose raw reference files are copied into tests/golden/kdb/
+RAW_KDB = ["people_id", "people_name", "people_name_enum", "info_id", "info_cheated", "info_date",
+           "info_zscore", "info_num1", "info_num2"]
 
 WIDTH = {"SMALLINT": np.int16, "INT": np.int32, "BIGINT": np.int64, "REAL": np.float64,
          "DATE": np.int32, "BOOLEAN": np.int8, "ENUM": np.int32}
@@ -141,6 +149,13 @@ def main(ref):
         json.dump(schema, f, indent=1)
     with open(os.path.join(HERE, "enums.json"), "w") as f:
         json.dump({str(k): v for k, v in enums.items()}, f)
+    raw = os.path.join(HERE, "kdb")
+    os.makedirs(raw, exist_ok=True)
+    for stem in RAW_KDB:
+        for suffix in (".kdb", "_null.kdb", ".kdbenum", ".kdbindex"):
+            src = os.path.join(data, stem + suffix)
+            if os.path.exists(src):
+                shutil.copyfile(src, os.path.join(raw, stem + suffix))
     for d in EXPECTED_DIRS:
         src = os.path.join(ref, "end_to_end_test", d)
         dst = os.path.join(HERE, "expected", d)
