@@ -128,7 +128,7 @@ typedef struct {
 int kdb_query_execute_host(kdb_ctx* ctx, const char* plan_json, const kdb_host_column* cols, int32_t ncols,
                            kdb_result** out);
 /* Chunk size (>= 64 KiB) and copy streams (1-8) of host-to-device column
- * copies (kdb_query_execute_host); defaults 8 MiB and 2. */
+ * copies (kdb_query_execute_host); defaults 64 MiB and 2. */
 int kdb_ctx_set_ingest(kdb_ctx* ctx, int64_t chunk_bytes, int32_t streams);
 /* Device time (ms, CUDA events) of the last kdb_query_execute's pipelines,
  * excluding result download, and the bytes read from table columns. */

@@ -1445,6 +1445,83 @@ MatBuffer Executor::RunAggregate(const Operator& op) {
   bool any_text = false;  // only TEXT MIN/MAX read the text state
   for (const auto& p : plans) any_text |= p.kind == StateKind::MinMaxText;
   if (any_text) ctx_.Memset(text_state, 0, sizeof(uint64_t) * (plans.size() + 1));
+  // Finalize.  Every output column gets a NULL array: an empty input emits a
+  // single all-NULL row even for COUNT (aggregate_translator.cc:82-89).
+  MatBuffer out = AllocMat(op.output, 1);
+  for (auto& mc : out.cols)
+    if (!mc.nulls) {
+      mc.nullable = true;
+      mc.nulls = arena_.AllocT<int8_t>(1);
+    }
+  bool fused_finalize = false;
+  // (the finalize is emitted into the aggregate kernel's last CTA, or into
+  // a one-block kernel after a fused Skinner join)
+  auto emit_finalize = [&](KernelSource& fk, ExprGen& fg, const std::string& fp, const std::string& G) {
+  std::string ftp = fk.Ptr(text_state, "uint64_t", true);
+  {
+    std::vector<WordKind> kinds(nw, WordKind::AddI64);
+    for (size_t j = 0; j < plans.size(); j++) {
+      const AggPlan& p = plans[j];
+      if (p.kind == StateKind::SumF64 || p.kind == StateKind::AvgF64) kinds[j * 2] = WordKind::AddF64;
+      if (p.kind == StateKind::MinMaxKey) kinds[j * 2] = p.is_min ? WordKind::MinU64 : WordKind::MaxU64;
+    }
+    kinds[nw - 1] = WordKind::MinU64;
+    EmitPartialReduce(fk, fp, G, nw, kinds);
+  }
+  fk.Open("if (threadIdx.x == 0)");
+  for (size_t j = 0; j < plans.size(); j++) {
+    const AggPlan& p = plans[j];
+    std::string J = std::to_string(j), W = std::to_string(j * 2), C = std::to_string(j * 2 + 1);
+    switch (p.kind) {
+      case StateKind::SumF64:
+      case StateKind::AvgF64: fk.L("double s" + J + " = __longlong_as_double((long long)tot[" + W + "]);"); break;
+      case StateKind::MinMaxKey: fk.L("uint64_t s" + J + " = tot[" + W + "];"); break;
+      default: fk.L("int64_t s" + J + " = (int64_t)tot[" + W + "];"); break;
+    }
+    fk.L("int64_t c" + J + " = (int64_t)tot[" + C + "];");
+  }
+  fk.L("int64_t rows = (int64_t)tot[" + std::to_string(nw - 2) + "];");
+  fk.L("uint64_t first = tot[" + std::to_string(nw - 1) + "];");
+  std::vector<CVal> virt;
+  for (size_t j = 0; j < plans.size(); j++) {
+    const AggPlan& p = plans[j];
+    std::string J = std::to_string(j);
+    const Type& rt = p.agg->type;
+    const Type& ct = p.agg->kid(0).type;
+    switch (p.kind) {
+      case StateKind::SumF64: virt.push_back(fg.Bind(rt, "s" + J, "c" + J + " == 0")); break;
+      case StateKind::SumI64: virt.push_back(fg.Bind(rt, "(" + CType(rt.id) + ")s" + J, "c" + J + " == 0")); break;
+      case StateKind::AvgF64:
+        virt.push_back(fg.Bind(rt, "__ddiv_rn(s" + J + ", (double)c" + J + ")", "c" + J + " == 0"));
+        break;
+      case StateKind::Count: {
+        std::string v = "c" + J;
+        if (p.count_flag >= 0) v = "(c" + J + " + (int64_t)((first >> " + std::to_string(p.count_flag) + ") & 1ULL))";
+        virt.push_back(fg.Bind(rt, v, "false"));
+        break;
+      }
+      case StateKind::MinMaxKey: virt.push_back(fg.Bind(rt, OKeyInv(ct, "s" + J), "c" + J + " == 0")); break;
+      case StateKind::MinMaxText:
+        virt.push_back(fg.Bind(rt, "kdb_str_from_handle(" + ftp + "[" + J + "])", "c" + J + " == 0"));
+        break;
+    }
+  }
+  Scope s;
+  s.virt = virt;
+  std::vector<CVal> vals;
+  for (const auto& c : op.output) vals.push_back(fg.Emit(*c.expr, s));
+  for (size_t c = 0; c < out.cols.size(); c++) {
+    const MatCol& mc = out.cols[c];
+    std::string dp = fk.Ptr(mc.data, StoreType(mc.type.id));
+    std::string val = mc.type.id == TypeId::BOOLEAN ? "(int8_t)(" + vals[c].v + " ? 1 : 0)" : vals[c].v;
+    fk.L(dp + "[0] = " + val + ";");
+    std::string np = fk.Ptr(mc.nulls, "int8_t");
+    fk.L(np + "[0] = (rows == 0 || (" + vals[c].n + ")) ? 1 : 0;");
+  }
+  std::string posp = fk.Ptr(out.pos, "uint64_t");
+  fk.L(posp + "[0] = 0;");
+  fk.Close();
+  };
   if (fuse) {
     part = arena_.AllocT<uint64_t>(nw);
     std::vector<uint64_t> init(nw, 0);
@@ -1511,7 +1588,18 @@ MatBuffer Executor::RunAggregate(const Operator& op) {
   if (Streamable(op.child())) EmitStream(ks, eg, op.child(), consume, src_rows);
   else EmitMatScan(ks, mats_.at(&op.child()), nullptr, consume, src_rows);
 
-  grid = ctx_.GridFor(std::max<int64_t>(src_rows, 1), block);
+  // Enough rows per thread that every thread runs a few prefetched
+  // iterations (at 1M rows one row group per thread left most of the
+  // kernel's time to ramp-up and the block reductions), at least one CTA
+  // per SM.
+  {
+    const int64_t rpt = std::getenv("KDB_AGG_ROWS_PER_THREAD") ? std::atoll(std::getenv("KDB_AGG_ROWS_PER_THREAD"))
+                                                               : 16;
+    const int64_t want = (std::max<int64_t>(src_rows, 1) + block * rpt - 1) / (block * rpt);
+    grid = static_cast<int>(std::max<int64_t>(std::min<int64_t>(ctx_.GridFor(std::max<int64_t>(src_rows, 1), block),
+                                                                want),
+                                              std::min<int64_t>(ctx_.num_sms, ctx_.GridFor(std::max<int64_t>(src_rows, 1), block))));
+  }
   part = arena_.AllocT<uint64_t>(static_cast<size_t>(grid) * nw);
   std::string pp = ks.Ptr(part, "uint64_t");
   ks.L("__shared__ uint64_t red_u[32];");
@@ -1561,6 +1649,23 @@ MatBuffer Executor::RunAggregate(const Operator& op) {
   ks.L("uint64_t t = kdb_block_reduce(first, KdbMinU64(), red_u);");
   store(nw - 1, "t");
   ks.Close();
+  fused_finalize = !std::getenv("KDB_AGG_SEPARATE_FINALIZE");
+  if (fused_finalize) {
+    // the last CTA to finish combines the partials (same fixed-order
+    // reduction as the separate finalize) and writes the result row
+    uint32_t* done = arena_.AllocT<uint32_t>(1);
+    ctx_.Memset(done, 0, sizeof(uint32_t));
+    const std::string dn = ks.Ptr(done, "unsigned");
+    ks.L("__shared__ bool kdb_last_block;");
+    ks.L("__threadfence();");
+    ks.L("__syncthreads();");
+    ks.L("if (threadIdx.x == 0) kdb_last_block = atomicAdd(" + dn + ", 1u) == gridDim.x - 1;");
+    ks.L("__syncthreads();");
+    ks.Open("if (kdb_last_block)");
+    ks.L("__threadfence();");
+    emit_finalize(ks, eg, pp, "gridDim.x");
+    ks.Close();
+  }
   {
     std::string src = ks.Kernel("kdb_aggregate", block);
     CUfunction f = ctx_.Kernel(src, "kdb_aggregate");
@@ -1568,83 +1673,11 @@ MatBuffer Executor::RunAggregate(const Operator& op) {
   }
   }  // not fused
 
-  // Finalize.  Every output column gets a NULL array: an empty input emits a
-  // single all-NULL row even for COUNT (aggregate_translator.cc:82-89).
-  MatBuffer out = AllocMat(op.output, 1);
-  for (auto& mc : out.cols)
-    if (!mc.nulls) {
-      mc.nullable = true;
-      mc.nulls = arena_.AllocT<int8_t>(1);
-    }
-  KernelSource fk;
-  ExprGen fg(ctx_, fk);
-  std::string fp = fk.Ptr(part, "uint64_t", true);
-  std::string ftp = fk.Ptr(text_state, "uint64_t", true);
-  std::string G = fk.Word(static_cast<uint64_t>(grid));
-  {
-    std::vector<WordKind> kinds(nw, WordKind::AddI64);
-    for (size_t j = 0; j < plans.size(); j++) {
-      const AggPlan& p = plans[j];
-      if (p.kind == StateKind::SumF64 || p.kind == StateKind::AvgF64) kinds[j * 2] = WordKind::AddF64;
-      if (p.kind == StateKind::MinMaxKey) kinds[j * 2] = p.is_min ? WordKind::MinU64 : WordKind::MaxU64;
-    }
-    kinds[nw - 1] = WordKind::MinU64;
-    EmitPartialReduce(fk, fp, G, nw, kinds);
-  }
-  fk.Open("if (threadIdx.x == 0)");
-  for (size_t j = 0; j < plans.size(); j++) {
-    const AggPlan& p = plans[j];
-    std::string J = std::to_string(j), W = std::to_string(j * 2), C = std::to_string(j * 2 + 1);
-    switch (p.kind) {
-      case StateKind::SumF64:
-      case StateKind::AvgF64: fk.L("double s" + J + " = __longlong_as_double((long long)tot[" + W + "]);"); break;
-      case StateKind::MinMaxKey: fk.L("uint64_t s" + J + " = tot[" + W + "];"); break;
-      default: fk.L("int64_t s" + J + " = (int64_t)tot[" + W + "];"); break;
-    }
-    fk.L("int64_t c" + J + " = (int64_t)tot[" + C + "];");
-  }
-  fk.L("int64_t rows = (int64_t)tot[" + std::to_string(nw - 2) + "];");
-  fk.L("uint64_t first = tot[" + std::to_string(nw - 1) + "];");
-  std::vector<CVal> virt;
-  for (size_t j = 0; j < plans.size(); j++) {
-    const AggPlan& p = plans[j];
-    std::string J = std::to_string(j);
-    const Type& rt = p.agg->type;
-    const Type& ct = p.agg->kid(0).type;
-    switch (p.kind) {
-      case StateKind::SumF64: virt.push_back(fg.Bind(rt, "s" + J, "c" + J + " == 0")); break;
-      case StateKind::SumI64: virt.push_back(fg.Bind(rt, "(" + CType(rt.id) + ")s" + J, "c" + J + " == 0")); break;
-      case StateKind::AvgF64:
-        virt.push_back(fg.Bind(rt, "__ddiv_rn(s" + J + ", (double)c" + J + ")", "c" + J + " == 0"));
-        break;
-      case StateKind::Count: {
-        std::string v = "c" + J;
-        if (p.count_flag >= 0) v = "(c" + J + " + (int64_t)((first >> " + std::to_string(p.count_flag) + ") & 1ULL))";
-        virt.push_back(fg.Bind(rt, v, "false"));
-        break;
-      }
-      case StateKind::MinMaxKey: virt.push_back(fg.Bind(rt, OKeyInv(ct, "s" + J), "c" + J + " == 0")); break;
-      case StateKind::MinMaxText:
-        virt.push_back(fg.Bind(rt, "kdb_str_from_handle(" + ftp + "[" + J + "])", "c" + J + " == 0"));
-        break;
-    }
-  }
-  Scope s;
-  s.virt = virt;
-  std::vector<CVal> vals;
-  for (const auto& c : op.output) vals.push_back(fg.Emit(*c.expr, s));
-  for (size_t c = 0; c < out.cols.size(); c++) {
-    const MatCol& mc = out.cols[c];
-    std::string dp = fk.Ptr(mc.data, StoreType(mc.type.id));
-    std::string val = mc.type.id == TypeId::BOOLEAN ? "(int8_t)(" + vals[c].v + " ? 1 : 0)" : vals[c].v;
-    fk.L(dp + "[0] = " + val + ";");
-    std::string np = fk.Ptr(mc.nulls, "int8_t");
-    fk.L(np + "[0] = (rows == 0 || (" + vals[c].n + ")) ? 1 : 0;");
-  }
-  std::string posp = fk.Ptr(out.pos, "uint64_t");
-  fk.L(posp + "[0] = 0;");
-  fk.Close();
-  {
+  if (!fused_finalize) {
+    KernelSource fk;
+    ExprGen fg(ctx_, fk);
+    const std::string fp = fk.Ptr(part, "uint64_t", true);
+    emit_finalize(fk, fg, fp, fk.Word(static_cast<uint64_t>(grid)));
     std::string src = fk.Kernel("kdb_aggregate_finalize", 256);
     CUfunction f = ctx_.Kernel(src, "kdb_aggregate_finalize");
     ctx_.Launch(f, 1, 256, fk.Args(), 0, "aggregate finalize");

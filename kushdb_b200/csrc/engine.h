@@ -253,7 +253,7 @@ class Context {
   // call returns).  Returns the bytes copied.
   int64_t StreamColumns(const std::vector<HostColumnSpec>& cols);
   // Chunk size and number of copy streams used by StreamColumns.
-  int64_t ingest_chunk_bytes = int64_t(8) << 20;
+  int64_t ingest_chunk_bytes = int64_t(64) << 20;
   int ingest_streams = 2;
   void AddTextColumn(const std::string& table, const std::string& column, const int64_t* offsets,
                      const char* chars, int64_t n, const int8_t* nulls);

@@ -290,7 +290,7 @@ class Engine:
         """Reads a reference .kdbenum dictionary."""
         self._check(self.lib.kdb_enum_open_kdbenum(self.ctx, enum_id, path.encode()))
 
-    def set_ingest(self, chunk_bytes: int = 8 << 20, streams: int = 2) -> None:
+    def set_ingest(self, chunk_bytes: int = 64 << 20, streams: int = 2) -> None:
         self._check(self.lib.kdb_ctx_set_ingest(self.ctx, chunk_bytes, streams))
 
     def drop_table(self, name: str) -> None:
