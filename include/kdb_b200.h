@@ -141,6 +141,17 @@ double kdb_last_query_device_ms(kdb_ctx* ctx);
  * invalidates them; Skinner joins and profiling runs are never replayed. */
 int kdb_ctx_set_prepared_queries(kdb_ctx* ctx, int32_t on);
 
+/* Code-generation switches and tuning values of the context, named KDB_*
+ * (e.g. "KDB_NO_VECTOR_SCAN", "KDB_DENSE_BLOCK" = "128"): every measured
+ * choice of the generated pipelines can be turned off or retuned through
+ * one, for A/B comparisons.  A context starts from the KDB_* environment
+ * variables present when it is created; value NULL removes an option.
+ * Changing an option drops the prepared recordings.  kdb_ctx_get_option
+ * returns 0 when the option is unset, else the size of its value with the
+ * NUL (copied into buf when it fits cap). */
+int kdb_ctx_set_option(kdb_ctx* ctx, const char* name, const char* value);
+int64_t kdb_ctx_get_option(kdb_ctx* ctx, const char* name, char* buf, int64_t cap);
+
 /* ---- Skinner join options (runtime/skinner_join_executor.cc:20-22) ------
  * Work budget per episode (tuples examined, the reference's
  * --budget_per_episode) and the UCT random seed (--join_seed).  Join order

@@ -273,6 +273,28 @@ void RunPlan(kdb_ctx* ctx, const char* plan_json, kdb_result** out) {
 
 extern "C" {
 
+int kdb_ctx_set_option(kdb_ctx* ctx, const char* name, const char* value) {
+  return Guard(ctx, [&] {
+    if (!name || std::strncmp(name, "KDB_", 4) != 0) throw kdb::Error(KDB_ERR_INVALID, "option names start with KDB_");
+    if (value) ctx->c->options[name] = value;
+    else ctx->c->options.erase(name);
+    ctx->c->catalog_version++;  // recordings were generated under the old options
+  });
+}
+
+int64_t kdb_ctx_get_option(kdb_ctx* ctx, const char* name, char* buf, int64_t cap) {
+  if (!ctx || !name) return KDB_ERR_INVALID;
+  const char* v = ctx->c->OptStr(name);
+  if (!v) return 0;
+  const int64_t n = static_cast<int64_t>(std::strlen(v));
+  if (buf && cap > 0) {
+    const int64_t m = std::min<int64_t>(cap - 1, n);
+    std::memcpy(buf, v, m);
+    buf[m] = 0;
+  }
+  return n + 1;
+}
+
 int kdb_ctx_set_prepared_queries(kdb_ctx* ctx, int32_t on) {
   return Guard(ctx, [&] {
     ctx->prepare = on != 0;

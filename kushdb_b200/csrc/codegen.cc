@@ -824,7 +824,7 @@ void Executor::EmitStream(KernelSource& ks, ExprGen& eg, const Operator& op, con
       for (const DevColumn* c : cols) any_text |= c->type.id == TypeId::TEXT;
       const bool probe_side = probe_side_scan_;
       probe_side_scan_ = false;
-      const bool vec = !any_text && !probe_side && !std::getenv("KDB_NO_VECTOR_SCAN");
+      const bool vec = !any_text && !probe_side && !ctx_.OptStr("KDB_NO_VECTOR_SCAN");
       std::vector<CVal> scan(cols.size());
       std::function<void(size_t)> load;
       if (vec) {
@@ -833,7 +833,7 @@ void Executor::EmitStream(KernelSource& ks, ExprGen& eg, const Operator& op, con
         // With prefetch (default), the next iteration's vectors are loaded
         // before this iteration's rows are processed, so a warp keeps two
         // iterations of loads in flight.
-        const bool prefetch = !std::getenv("KDB_NO_SCAN_PREFETCH");
+        const bool prefetch = !ctx_.OptStr("KDB_NO_SCAN_PREFETCH");
         ks.L("const int64_t nrows = (int64_t)" + n + ";");
         ks.L("const int64_t qstride = (int64_t)gridDim.x * blockDim.x;");
         std::vector<std::string> arr(cols.size()), narr(cols.size()), parr(cols.size()), pnarr(cols.size());
@@ -905,7 +905,7 @@ void Executor::EmitStream(KernelSource& ks, ExprGen& eg, const Operator& op, con
         // them: the probe key at once, every other column only inside the
         // match branch, so rows without a match never load them (about a
         // third of the sectors of a 9%-selective probe).
-        const bool lazy = probe_side && !std::getenv("KDB_EAGER_PROBE_COLUMNS");
+        const bool lazy = probe_side && !ctx_.OptStr("KDB_EAGER_PROBE_COLUMNS");
         load = [&, lazy](size_t k) {
           const DevColumn& c = *cols[k];
           std::string v;
@@ -989,7 +989,7 @@ void Executor::EmitStream(KernelSource& ks, ExprGen& eg, const Operator& op, con
           consume(out, "((" + pos + ") << 32) | ((" + bpos + ") & 0xffffffffULL)");
         });
       };
-      probe_side_scan_ = !std::getenv("KDB_VECTOR_PROBE_SCAN");
+      probe_side_scan_ = !ctx_.OptStr("KDB_VECTOR_PROBE_SCAN");
       if (Streamable(op.child(1))) EmitStream(ks, eg, op.child(1), body, src_rows);
       else EmitMatScan(ks, mats_.at(&op.child(1)), nullptr, body, src_rows);
       probe_side_scan_ = false;
@@ -1064,14 +1064,14 @@ JoinTable Executor::BuildIndex(const MatBuffer& m, const std::vector<int>& key_c
   jt.mask = cap - 1;
   jt.slots = arena_.AllocT<uint64_t>(cap);
   ctx_.Memset(jt.slots, 0, cap * sizeof(uint64_t));
-  if (!std::getenv("KDB_NO_JOIN_FILTER")) {
+  if (!ctx_.OptStr("KDB_NO_JOIN_FILTER")) {
     jt.bloom_log2 = 14;
     while (jt.bloom_log2 < 26 && (int64_t(1) << jt.bloom_log2) < m.rows * 8) jt.bloom_log2++;
     const size_t words = (size_t(1) << jt.bloom_log2) / 32;
     jt.bloom = arena_.AllocT<uint32_t>(words);
     ctx_.Memset(jt.bloom, 0, words * sizeof(uint32_t));
   }
-  if (key_cols.size() == 1 && !std::getenv("KDB_NO_KEY_IN_SLOT")) {
+  if (key_cols.size() == 1 && !ctx_.OptStr("KDB_NO_KEY_IN_SLOT")) {
     const TypeId t = m.cols.at(key_cols[0]).type.id;
     jt.key_in_slot = t == TypeId::INT || t == TypeId::DATE || t == TypeId::ENUM || t == TypeId::SMALLINT;
     jt.key_col = key_cols[0];
@@ -1238,7 +1238,7 @@ MatBuffer Executor::MaterializeStream(const Operator& op, const uint32_t* order,
     return out;
   }
   Prepare(op);
-  if (!StreamHasJoin(op) && !std::getenv("KDB_MATERIALIZE_ATOMIC")) return MaterializeCounted(op);
+  if (!StreamHasJoin(op) && !ctx_.OptStr("KDB_MATERIALIZE_ATOMIC")) return MaterializeCounted(op);
   int64_t cap = RowBound(op);
   for (int attempt = 0; attempt < 3; attempt++) {
     const auto mark = ctx_.RecordMark();
@@ -1435,7 +1435,7 @@ MatBuffer Executor::RunAggregate(const Operator& op) {
   // integer SUM) over non-NULL inputs directly above a Skinner join is
   // evaluated inside the join's episode kernel, without materialising the
   // join's result (JOB-style MIN(...) queries).
-  bool fuse = op.child().kind == OpKind::SKINNER_JOIN && !std::getenv("KDB_NO_SKINNER_AGG");
+  bool fuse = op.child().kind == OpKind::SKINNER_JOIN && !ctx_.OptStr("KDB_NO_SKINNER_AGG");
   for (const auto& p : plans)
     fuse = fuse && !p.child_nullable && p.count_flag < 0 &&
            (p.kind == StateKind::Count || p.kind == StateKind::MinMaxKey || p.kind == StateKind::SumI64);
@@ -1593,7 +1593,7 @@ MatBuffer Executor::RunAggregate(const Operator& op) {
   // kernel's time to ramp-up and the block reductions), at least one CTA
   // per SM.
   {
-    const int64_t rpt = std::getenv("KDB_AGG_ROWS_PER_THREAD") ? std::atoll(std::getenv("KDB_AGG_ROWS_PER_THREAD"))
+    const int64_t rpt = ctx_.OptStr("KDB_AGG_ROWS_PER_THREAD") ? std::atoll(ctx_.OptStr("KDB_AGG_ROWS_PER_THREAD"))
                                                                : 16;
     const int64_t want = (std::max<int64_t>(src_rows, 1) + block * rpt - 1) / (block * rpt);
     grid = static_cast<int>(std::max<int64_t>(std::min<int64_t>(ctx_.GridFor(std::max<int64_t>(src_rows, 1), block),
@@ -1649,7 +1649,7 @@ MatBuffer Executor::RunAggregate(const Operator& op) {
   ks.L("uint64_t t = kdb_block_reduce(first, KdbMinU64(), red_u);");
   store(nw - 1, "t");
   ks.Close();
-  fused_finalize = !std::getenv("KDB_AGG_SEPARATE_FINALIZE");
+  fused_finalize = !ctx_.OptStr("KDB_AGG_SEPARATE_FINALIZE");
   if (fused_finalize) {
     // the last CTA to finish combines the partials (same fixed-order
     // reduction as the separate finalize) and writes the result row
@@ -1792,13 +1792,13 @@ MatBuffer Executor::RunGroupByDense(const Operator& op, const std::vector<AggPla
   // block size and the launch-bounds occupancy hint (env overrides for tuning)
   // (64 threads, 6 CTAs per SM: measured best on the Q1 shape among 64/128
   // threads and 2-8 CTAs per SM)
-  const int block = std::getenv("KDB_DENSE_BLOCK") ? std::atoi(std::getenv("KDB_DENSE_BLOCK")) : 64;
-  const int min_blocks = std::getenv("KDB_DENSE_MINB") ? std::atoi(std::getenv("KDB_DENSE_MINB")) : 6;
-  const int grid_per_sm = std::getenv("KDB_DENSE_GRID") ? std::atoi(std::getenv("KDB_DENSE_GRID")) : 6;
+  const int block = ctx_.OptStr("KDB_DENSE_BLOCK") ? std::atoi(ctx_.OptStr("KDB_DENSE_BLOCK")) : 64;
+  const int min_blocks = ctx_.OptStr("KDB_DENSE_MINB") ? std::atoi(ctx_.OptStr("KDB_DENSE_MINB")) : 6;
+  const int grid_per_sm = ctx_.OptStr("KDB_DENSE_GRID") ? std::atoi(ctx_.OptStr("KDB_DENSE_GRID")) : 6;
   // Accumulators in registers (every row updates every group's words under a
   // predicate) or, for larger groups x words, in per-thread shared-memory
   // slots indexed by the group id (a row touches only its own group's words).
-  const char* smem_env = std::getenv("KDB_DENSE_SMEM");
+  const char* smem_env = ctx_.OptStr("KDB_DENSE_SMEM");
   const bool smem_fits = K * block * 8 <= 48 * 1024;  // static shared memory limit
   const bool in_smem = smem_fits && (smem_env ? std::atoi(smem_env) != 0 : K > 16);
 
@@ -2165,7 +2165,7 @@ MatBuffer Executor::RunGroupByBuildRows(const Operator& op, const std::vector<Ag
         ks.L("kdb_atomic_min_u64(&" + F + "[" + g + "], ((uint64_t)(" + pos + ") << 40) | (" + fl + "));");
       });
     };
-    probe_side_scan_ = !std::getenv("KDB_VECTOR_PROBE_SCAN");
+    probe_side_scan_ = !ctx_.OptStr("KDB_VECTOR_PROBE_SCAN");
     if (Streamable(join.child(1))) EmitStream(ks, eg, join.child(1), body, src_rows);
     else EmitMatScan(ks, mats_.at(&join.child(1)), nullptr, body, src_rows);
     probe_side_scan_ = false;
@@ -2266,13 +2266,13 @@ MatBuffer Executor::RunGroupBy(const Operator& op, bool any_order) {
       if (p.child_nullable) distinct.insert("c|" + csig);
     }
     int64_t words = static_cast<int64_t>(distinct.size()) + 2;
-    if (dense && static_cast<int64_t>(kl.domain) * words <= 64 && !std::getenv("KDB_NO_DENSE_GROUPBY"))
+    if (dense && static_cast<int64_t>(kl.domain) * words <= 64 && !ctx_.OptStr("KDB_NO_DENSE_GROUPBY"))
       return RunGroupByDense(op, plans, kl);
   }
 
   {
     std::vector<int> key_cols;
-    if (!std::getenv("KDB_NO_BUILD_ROW_GROUPS") && BuildRowGroups(op, &key_cols))
+    if (!ctx_.OptStr("KDB_NO_BUILD_ROW_GROUPS") && BuildRowGroups(op, &key_cols))
       return RunGroupByBuildRows(op, plans, key_cols, any_order);
   }
 
@@ -2539,7 +2539,7 @@ MatBuffer Executor::RunGroupBy(const Operator& op, bool any_order) {
 MatBuffer Executor::RunOrderBy(const Operator& op) {
   // every ORDER BY path below orders rows that are not in stream order by
   // their stream position, so a GROUP BY child need not sort its groups
-  MatBuffer m = op.child().kind == OpKind::GROUP_BY_AGGREGATE && !std::getenv("KDB_GROUP_ORDER_SORT")
+  MatBuffer m = op.child().kind == OpKind::GROUP_BY_AGGREGATE && !ctx_.OptStr("KDB_GROUP_ORDER_SORT")
                     ? RunGroupBy(op.child(), true)
                     : Materialize(op.child());
   int64_t n = m.rows;
@@ -2657,7 +2657,7 @@ MatBuffer Executor::LargeOrderBy(const Operator& op, MatBuffer& m) {
     // key's low bit moves to the top of the tie word, which then holds the
     // tie rank in 31 bits.
     const MatCol* mk = op.sort_keys.size() == 1 ? &m.cols.at(op.sort_keys[0]->column_idx) : nullptr;
-    const bool merge_ok = mk && depth <= 32 && !std::getenv("KDB_ORDER_RADIX") && mk->type.id != TypeId::TEXT &&
+    const bool merge_ok = mk && depth <= 32 && !ctx_.OptStr("KDB_ORDER_RADIX") && mk->type.id != TypeId::TEXT &&
                           mk->type.id != TypeId::BOOLEAN && (!mk->nullable || depth <= 31);
     if (merge_ok) {
       const MatCol& mc = *mk;
@@ -2711,7 +2711,7 @@ MatBuffer Executor::LargeOrderBy(const Operator& op, MatBuffer& m) {
         ks.Close();
         LaunchPipeline(ks, n, "order rows");
       };
-      if (!m.pos_is_index && !std::getenv("KDB_ORDER_TIE_SORT")) {
+      if (!m.pos_is_index && !ctx_.OptStr("KDB_ORDER_TIE_SORT")) {
         // Rows not in stream order (groups in table order): sort by the key
         // alone and look for equal neighbours.  Without ties the tie rank
         // never decides, and the stream-order sort is not needed.
@@ -2820,7 +2820,7 @@ MatBuffer Executor::LargeOrderBy(const Operator& op, MatBuffer& m) {
     // alone and check adjacent rows for ties; only if two rows tie is the
     // merge sort's tie order (the tie-path key) needed, and the sort is
     // redone with it from the stream order.
-    bool floats_only = !std::getenv("KDB_ORDER_TIE_SORT");
+    bool floats_only = !ctx_.OptStr("KDB_ORDER_TIE_SORT");
     for (const auto& sk : op.sort_keys)
       if (m.cols.at(sk->column_idx).type.id != TypeId::REAL) floats_only = false;
     bool done = false;
@@ -3231,14 +3231,14 @@ class SkinnerEngine : public JoinEnv {
     if (!empty) {
       beg_ = arena_.AllocT<uint64_t>(kMaxSlice);
       offs_ = arena_.AllocT<uint64_t>(kMaxSlice + 1);
-      deep_ = T_ > 2 && !std::getenv("KDB_SKINNER_DEPTH1");
+      deep_ = T_ > 2 && !ctx_.OptStr("KDB_SKINNER_DEPTH1");
       if (deep_) {
         beg2_ = arena_.AllocT<uint64_t>(kMaxItems2);
         offs2_ = arena_.AllocT<uint64_t>(kMaxItems2 + 1);
       }
-      split_ = T_ > 2 && !std::getenv("KDB_SKINNER_NO_SPLIT");
-      if (const char* r = std::getenv("KDB_SKINNER_SPLIT")) split_run_ = std::max<int64_t>(1, std::atoll(r));
-      if (const char* c = std::getenv("KDB_SKINNER_TASKS")) task_cap_ = std::max<int64_t>(1, std::atoll(c));
+      split_ = T_ > 2 && !ctx_.OptStr("KDB_SKINNER_NO_SPLIT");
+      if (const char* r = ctx_.OptStr("KDB_SKINNER_SPLIT")) split_run_ = std::max<int64_t>(1, std::atoll(r));
+      if (const char* c = ctx_.OptStr("KDB_SKINNER_TASKS")) task_cap_ = std::max<int64_t>(1, std::atoll(c));
       if (split_)
         for (int q = 0; q < 2; q++) tasks_[q] = arena_.AllocT<uint64_t>(task_cap_ * (3 + T_));
       Generate();
@@ -4134,7 +4134,7 @@ class QueryTimer {
 // milliseconds; the replays recompute the same result in place.
 void ChooseReplay(Context& ctx, PreparedQuery& pq) {
   constexpr size_t kMaxDirectOps = 48;
-  if (pq.ops.size() > kMaxDirectOps || std::getenv("KDB_REPLAY_GRAPH")) return;
+  if (pq.ops.size() > kMaxDirectOps || ctx.OptStr("KDB_REPLAY_GRAPH")) return;
   cudaEvent_t e0, e1;
   KDB_CUDA(cudaEventCreate(&e0));
   KDB_CUDA(cudaEventCreate(&e1));
@@ -4161,7 +4161,7 @@ void ChooseReplay(Context& ctx, PreparedQuery& pq) {
     std::sort(d.begin(), d.end());
   }
   pq.direct = !d.empty() && d[1] < g[1];
-  if (std::getenv("KDB_REPLAY_DIRECT")) pq.direct = true;
+  if (ctx.OptStr("KDB_REPLAY_DIRECT")) pq.direct = true;
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
 }

@@ -207,7 +207,24 @@ void Context::ReserveHostBlocks(int count, size_t bytes) {
 // Context
 // ---------------------------------------------------------------------------
 
+extern "C" char** environ;
+
+namespace {
+// the KDB_* environment variables, as a context's initial options
+std::map<std::string, std::string> OptionsFromEnvironment() {
+  std::map<std::string, std::string> o;
+  for (char** e = environ; e && *e; e++) {
+    const char* kv = *e;
+    if (std::strncmp(kv, "KDB_", 4) != 0) continue;
+    const char* eq = std::strchr(kv, '=');
+    if (eq) o.emplace(std::string(kv, eq - kv), std::string(eq + 1));
+  }
+  return o;
+}
+}  // namespace
+
 Context::Context(int dev) : device(dev) {
+  options = OptionsFromEnvironment();
   if (dev < 0) {
     dry = true;
     d_err = static_cast<int*>(DevAlloc(16));
@@ -230,8 +247,8 @@ Context::Context(int dev) : device(dev) {
 Context::Context(Context& parent)
     : device(parent.device), dry(parent.dry), num_sms(parent.num_sms), tables(parent.tables),
       enums(parent.enums), skinner_budget(parent.skinner_budget), skinner_seed(parent.skinner_seed),
-      skinner_policy(parent.skinner_policy), join_prior(parent.join_prior), cache_(parent.cache_),
-      owns_catalog_(false) {
+      skinner_policy(parent.skinner_policy), join_prior(parent.join_prior), options(parent.options),
+      cache_(parent.cache_), owns_catalog_(false) {
   if (dry) {
     d_err = static_cast<int*>(DevAlloc(16));
     return;

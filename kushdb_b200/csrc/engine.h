@@ -202,6 +202,17 @@ class Context {
   std::vector<float> skinner_features;
   std::vector<float> skinner_rewards;
 
+  // Code-generation switches and tuning values, named KDB_* (for example
+  // KDB_NO_VECTOR_SCAN, KDB_DENSE_BLOCK=128): set with kdb_ctx_set_option;
+  // a context starts from the KDB_* environment variables present when it
+  // is created.  Changing one drops the prepared recordings (they were
+  // generated under the old values).
+  std::map<std::string, std::string> options;
+  const char* OptStr(const char* name) const {
+    auto it = options.find(name);
+    return it == options.end() ? nullptr : it->second.c_str();
+  }
+
   // device error word shared by all launches of a query
   int* d_err = nullptr;
 

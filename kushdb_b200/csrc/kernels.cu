@@ -549,7 +549,7 @@ void Context::PackToHost(const PackSegs& segs, size_t total, void* host) {
   void* mapped = nullptr;
   // The lookup is skipped while an earlier error is pending, so that clearing
   // the lookup's own failure below can never swallow someone else's error.
-  if (total <= kDirect && !std::getenv("KDB_NO_MAPPED_RESULT") &&
+  if (total <= kDirect && !OptStr("KDB_NO_MAPPED_RESULT") &&
       cudaPeekAtLastError() == cudaSuccess) {
     if (cudaHostGetDevicePointer(&mapped, host, 0) != cudaSuccess) {
       cudaGetLastError();
@@ -588,13 +588,13 @@ void LaunchMerge(const SortItem* in, SortItem* out, int64_t n, int64_t w, cudaSt
   MergeItems<TILE, ITEMS><<<static_cast<unsigned>((n + TILE - 1) / TILE), TILE / ITEMS, 0, s>>>(in, out, n, w);
 }
 
-// KDB_SORT_SHAPE="bt,bi,mt,mi" overrides the shapes (tuning)
-void SortShapes(SortShape* block, SortShape* merge) {
+// option KDB_SORT_SHAPE="bt,bi,mt,mi" overrides the shapes (tuning)
+void SortShapes(const Context& ctx, SortShape* block, SortShape* merge) {
   // measured on the 134k-item ORDER BY of the Q3-shape query: smaller
   // merge tiles give a pass more blocks (latency-bound searches and staging)
   *block = {1024, 2};
   *merge = {256, 2};
-  if (const char* e = std::getenv("KDB_SORT_SHAPE")) {
+  if (const char* e = ctx.OptStr("KDB_SORT_SHAPE")) {
     int v[4];
     if (std::sscanf(e, "%d,%d,%d,%d", &v[0], &v[1], &v[2], &v[3]) == 4) {
       *block = {v[0], v[1]};
@@ -607,7 +607,7 @@ void Context::MergeSortItems(void* items, int64_t n, Arena& arena) {
   if (n <= 1 || dry) return;
   if (n > 0x7fffffffLL) throw Error(-5, "merge sort of more than 2^31 items");
   SortShape bs, ms;
-  SortShapes(&bs, &ms);
+  SortShapes(*this, &bs, &ms);
   auto block_sort = [&]() -> void (*)(const SortItem*, SortItem*, int64_t, cudaStream_t) {
     switch (bs.tile * 16 + bs.items) {
       case 2048 * 16 + 2: return LaunchBlockSort<2048, 2>;

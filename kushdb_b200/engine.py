@@ -42,7 +42,7 @@ EXPORTS = [
     "kdb_pairs_free", "kdb_agg_create", "kdb_agg_set_pre_aggregation", "kdb_agg_update", "kdb_agg_finalize",
     "kdb_agg_free", "kdb_index_build", "kdb_index_open_kdbindex", "kdb_index_num_keys", "kdb_index_num_rows",
     "kdb_index_keys", "kdb_index_get", "kdb_index_free", "kdb_skinner_execute",
-    "kdb_query_execute_host", "kdb_ctx_set_ingest",
+    "kdb_query_execute_host", "kdb_ctx_set_ingest", "kdb_ctx_set_option", "kdb_ctx_get_option",
 ]
 
 _lib = None
@@ -167,6 +167,9 @@ def load_library(path: str = LIB_PATH):
     L.kdb_skinner_execute.argtypes = [P, CP, I32, I64, ctypes.c_uint32, ctypes.POINTER(P)]
     L.kdb_query_execute_host.argtypes = [P, CP, P, I32, ctypes.POINTER(P)]
     L.kdb_ctx_set_ingest.argtypes = [P, I64, I32]
+    L.kdb_ctx_set_option.argtypes = [P, CP, CP]
+    L.kdb_ctx_get_option.restype = I64
+    L.kdb_ctx_get_option.argtypes = [P, CP, ctypes.c_char_p, I64]
     declare_result_api(L, "kdb_")
     _lib = L
     return L
@@ -289,6 +292,19 @@ class Engine:
     def open_kdbenum(self, enum_id: int, path: str) -> None:
         """Reads a reference .kdbenum dictionary."""
         self._check(self.lib.kdb_enum_open_kdbenum(self.ctx, enum_id, path.encode()))
+
+    def set_option(self, name: str, value: Optional[str] = "1") -> None:
+        """Sets (value None: removes) a KDB_* code-generation switch."""
+        self._check(self.lib.kdb_ctx_set_option(self.ctx, name.encode(),
+                                                None if value is None else str(value).encode()))
+
+    def get_option(self, name: str) -> Optional[str]:
+        n = self.lib.kdb_ctx_get_option(self.ctx, name.encode(), None, 0)
+        if n <= 0:
+            return None
+        buf = ctypes.create_string_buffer(n)
+        self.lib.kdb_ctx_get_option(self.ctx, name.encode(), buf, n)
+        return buf.value.decode()
 
     def set_ingest(self, chunk_bytes: int = 64 << 20, streams: int = 2) -> None:
         self._check(self.lib.kdb_ctx_set_ingest(self.ctx, chunk_bytes, streams))

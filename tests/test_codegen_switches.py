@@ -18,9 +18,10 @@ SWITCHES = ["KDB_NO_SCAN_PREFETCH", "KDB_NO_VECTOR_SCAN", "KDB_VECTOR_PROBE_SCAN
 @pytest.mark.parametrize("switch", SWITCHES)
 def test_switch_path_compiles(switch):
     name, _, value = switch.partition("=")
-    os.environ[name] = value or "1"
+    e = Engine(-1)
     try:
-        e = Engine(-1)
+        e.set_option(name, value or "1")
+        assert e.get_option(name) == (value or "1")
         t1 = wl.scan_agg_table(rows=1000)
         t2 = wl.group_by_table(rows=1000)
         b, p = wl.join_tables(build_rows=1000, probe_rows=4000)
@@ -34,6 +35,17 @@ def test_switch_path_compiles(switch):
             e.register_table(t)
         e.execute(wl.skinner_plan(tables, tokens, "chain"))
         assert e.kernel_launches() > 0
-        e.close()
     finally:
-        del os.environ[name]
+        e.close()
+
+
+def test_options_start_from_the_environment_and_can_be_removed():
+    os.environ["KDB_NO_VECTOR_SCAN"] = "1"
+    try:
+        e = Engine(-1)
+    finally:
+        del os.environ["KDB_NO_VECTOR_SCAN"]
+    assert e.get_option("KDB_NO_VECTOR_SCAN") == "1"
+    e.set_option("KDB_NO_VECTOR_SCAN", None)
+    assert e.get_option("KDB_NO_VECTOR_SCAN") is None
+    e.close()

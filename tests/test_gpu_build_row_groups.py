@@ -2,7 +2,6 @@
 row path must give the oracle's result, in the same first-insertion order as
 the general group table, and must not be taken when build keys repeat."""
 
-import os
 
 import numpy as np
 import pytest
@@ -43,11 +42,11 @@ def _register(engine, *tables):
 def _both_paths(engine, plan):
     text = plan.to_json()
     fast = engine.execute(text)
-    os.environ["KDB_NO_BUILD_ROW_GROUPS"] = "1"
+    engine.set_option("KDB_NO_BUILD_ROW_GROUPS", "1")
     try:
         general = engine.execute(text)
     finally:
-        del os.environ["KDB_NO_BUILD_ROW_GROUPS"]
+        engine.set_option("KDB_NO_BUILD_ROW_GROUPS", None)
     return fast, general
 
 

@@ -6,7 +6,6 @@ the group-per-build-row path and the general group table, above and below
 the one-block ORDER BY size, against the oracle and against the path that
 sorts the groups first."""
 
-import os
 
 import numpy as np
 import pytest
@@ -41,18 +40,13 @@ def _register(engine, oracle, *tables):
 
 def _run(engine, plan, env=None):
     text = plan.to_json()
-    saved = {}
     for k, v in (env or {}).items():
-        saved[k] = os.environ.get(k)
-        os.environ[k] = v
+        engine.set_option(k, v)
     try:
         return engine.execute(text)
     finally:
-        for k, v in saved.items():
-            if v is None:
-                del os.environ[k]
-            else:
-                os.environ[k] = v
+        for k in (env or {}):
+            engine.set_option(k, None)
 
 
 def _join_group_plan(b, p, order_col, asc):

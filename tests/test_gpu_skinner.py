@@ -43,7 +43,6 @@ def test_skinner_multiway_matches_oracle(engine, shape, n_tables, zipf, budget):
 def test_aggregate_fused_into_episodes_matches_materialised(engine):
     """COUNT/MIN over the join evaluated inside the episode kernel equals the
     same aggregate over the materialised join result."""
-    import os
     tables, tokens = wl.skinner_tables("chain", 6, min_rows=1000, max_rows=30_000, zipf_s=1.5, seed=77,
                                        prefix="fuse_")
     for t in tables:
@@ -52,11 +51,11 @@ def test_aggregate_fused_into_episodes_matches_materialised(engine):
     engine.set_skinner(5000, seed=3)
     try:
         fused = engine.execute(plan)
-        os.environ["KDB_NO_SKINNER_AGG"] = "1"
+        engine.set_option("KDB_NO_SKINNER_AGG", "1")
         try:
             plain = engine.execute(plan)
         finally:
-            del os.environ["KDB_NO_SKINNER_AGG"]
+            engine.set_option("KDB_NO_SKINNER_AGG", None)
     finally:
         engine.set_skinner()
     assert compare(fused, plain) == ""
@@ -69,7 +68,6 @@ def test_hot_runs_as_tasks_match_oracle(engine, split, tasks, shape, n_tables, f
     """Runs longer than `split` candidates at position 3 and deeper go to the
     task queues (a queue of `tasks` entries: with 16 it fills, and the rest
     is walked in place); the result stays exactly the join's."""
-    import os
     from oracle import Oracle
     tables, tokens = wl.skinner_tables(shape, n_tables, min_rows=1000, max_rows=20_000, zipf_s=1.5,
                                        seed=31 + n_tables, prefix=f"hot{shape}{n_tables}_")
@@ -78,15 +76,15 @@ def test_hot_runs_as_tasks_match_oracle(engine, split, tasks, shape, n_tables, f
     for t in tables:
         engine.register_table(t)
         o.register_table(t)
-    os.environ["KDB_SKINNER_SPLIT"] = str(split)
-    os.environ["KDB_SKINNER_TASKS"] = str(tasks)
+    engine.set_option("KDB_SKINNER_SPLIT", str(split))
+    engine.set_option("KDB_SKINNER_TASKS", str(tasks))
     if not fused:  # results materialised (slot allocation, regrowth) instead of folded
-        os.environ["KDB_NO_SKINNER_AGG"] = "1"
+        engine.set_option("KDB_NO_SKINNER_AGG", "1")
     engine.set_skinner(3000, seed=2)
     try:
         g = engine.execute(plan)
     finally:
         for k in ("KDB_SKINNER_SPLIT", "KDB_SKINNER_TASKS", "KDB_NO_SKINNER_AGG"):
-            os.environ.pop(k, None)
+            engine.set_option(k, None)
         engine.set_skinner()
     assert compare(g, o.execute(plan)) == ""
