@@ -161,6 +161,13 @@ int kdb_ctx_set_skinner(kdb_ctx* ctx, int64_t budget_per_episode, uint32_t seed)
 int64_t kdb_last_skinner_episodes(kdb_ctx* ctx);
 /* Tuples examined by all episodes of the last Skinner join. */
 int64_t kdb_last_skinner_work(kdb_ctx* ctx);
+/* Episode batches of the last Skinner join.  The episodes run in batches
+ * (option KDB_SKINNER_BATCH, 1-16, default 8): the search picks the next
+ * join orders before the running ones report their rewards (the statistics
+ * are corrected when they do), and a batch shares one set of launches and
+ * one read-back.  Each episode's slice and offsets are those a one-at-a-
+ * time run would give it, so results stay exactly-once. */
+int64_t kdb_last_skinner_batches(kdb_ctx* ctx);
 
 /* ---- learned join-order prior (no reference counterpart) ----------------
  * A 64 -> 128 -> 128 -> 128 -> 1 ReLU MLP (fp32) predicting the episode

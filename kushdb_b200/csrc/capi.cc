@@ -315,6 +315,8 @@ int64_t kdb_last_skinner_episodes(kdb_ctx* ctx) { return ctx ? ctx->c->last_skin
 
 int64_t kdb_last_skinner_work(kdb_ctx* ctx) { return ctx ? ctx->c->last_skinner_work : -1; }
 
+int64_t kdb_last_skinner_batches(kdb_ctx* ctx) { return ctx ? ctx->c->last_skinner_batches : -1; }
+
 int64_t kdb_last_skinner_samples(kdb_ctx* ctx, float* features, float* rewards, int64_t cap) {
   if (!ctx) return KDB_ERR_INVALID;
   const auto& f = ctx->c->skinner_features;

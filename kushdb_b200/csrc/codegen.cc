@@ -2964,7 +2964,13 @@ class UctNode {
     InitPrior();
   }
 
-  double Sample(int round, std::vector<int>& order) {
+  // One episode of the search (select, expand, playout, back-propagate).
+  // With `trail`, every (node, action) whose statistics the sample updated
+  // is recorded: an episode that runs later in a batch reports its reward
+  // as a placeholder, and Correct() adds the difference to the true reward
+  // along exactly that path once the batch has run, leaving the statistics
+  // as if the true reward had been back-propagated.
+  double Sample(int round, std::vector<int>& order, std::vector<std::pair<UctNode*, int>>* trail = nullptr) {
     if (num_actions_ == 0) return env_.Execute(order);
     int action = SelectAction();
     int table = table_of_action_[action];
@@ -2972,11 +2978,16 @@ class UctNode {
     if (created_in_ != round && !children_[action])
       children_[action] = std::make_unique<UctNode>(round, *this, table, static_cast<uint32_t>(rng_()));
     UctNode* child = children_[action].get();
-    double reward = child ? child->Sample(round, order) : Playout(order);
+    double reward = child ? child->Sample(round, order, trail) : Playout(order);
     visits_++;
     tries_[action]++;
     reward_[action] += reward;
+    if (trail) trail->emplace_back(this, action);
     return reward;
+  }
+
+  static void Correct(const std::vector<std::pair<UctNode*, int>>& trail, double delta) {
+    for (const auto& [node, action] : trail) node->reward_[action] += delta;
   }
 
  private:
@@ -3219,12 +3230,22 @@ class SkinnerEngine : public JoinEnv {
     } else {
       out_ = alloc_out_(1 << 12);
     }
-    // result count, work, then the two task queues' counts (read together)
-    stats_ = arena_.AllocT<uint64_t>(4);
-    ctx_.Memset(stats_, 0, 4 * sizeof(uint64_t));
+    // result count, work, the two task queues' counts, then per episode of
+    // a batch its results and its work (all read back together)
+    stats_ = arena_.AllocT<uint64_t>(4 + 2 * kMaxBatch);
+    ctx_.Memset(stats_, 0, (4 + 2 * kMaxBatch) * sizeof(uint64_t));
     count_ = stats_;
     work_ = stats_ + 1;
     tcount_ = stats_ + 2;
+    eres_ = stats_ + 4;
+    ework_ = stats_ + 4 + kMaxBatch;
+    ep_ = arena_.AllocT<uint64_t>(static_cast<size_t>(kMaxBatch) * EpWords());
+    // episodes per batch: the next join orders are chosen before the
+    // current ones' rewards are known (their placeholders corrected after),
+    // so a batch's episodes share each launch and host round trip
+    batch_ = 8;
+    if (const char* b = ctx_.OptStr("KDB_SKINNER_BATCH")) batch_ = std::atoi(b);
+    batch_ = std::max(1, std::min(batch_, kMaxBatch));
     produced_ = 0;
     bool empty = false;
     for (int64_t c : cards_) empty |= c == 0;
@@ -3240,15 +3261,23 @@ class SkinnerEngine : public JoinEnv {
       if (const char* r = ctx_.OptStr("KDB_SKINNER_SPLIT")) split_run_ = std::max<int64_t>(1, std::atoll(r));
       if (const char* c = ctx_.OptStr("KDB_SKINNER_TASKS")) task_cap_ = std::max<int64_t>(1, std::atoll(c));
       if (split_)
-        for (int q = 0; q < 2; q++) tasks_[q] = arena_.AllocT<uint64_t>(task_cap_ * (3 + T_));
+        for (int q = 0; q < 2; q++) tasks_[q] = arena_.AllocT<uint64_t>(task_cap_ * (4 + T_));
       Generate();
       std::vector<int> order(T_);
       for (size_t i = 0; i < prefix.size(); i++) order[i] = prefix[i];
       const int64_t max_episodes = ctx_.dry ? 1 : (1 << 24);
+      // a batch fills until it holds batch_ episodes, the join completes
+      // (an offset reaches its table's end) or its slices fill kMaxSlice
+      auto batch_open = [&]() {
+        return static_cast<int>(pending_.size()) < batch_ && !IsComplete() &&
+               episodes_ + static_cast<int64_t>(pending_.size()) < max_episodes && batch_items_ < kMaxSlice;
+      };
       if (ctx_.skinner_policy == 2) {
         // uniformly random connected orders (training data for the prior)
         std::mt19937_64 rng(seed_);
+        batching_ = true;
         while (!IsComplete() && episodes_ < max_episodes) {
+         while (batch_open()) {
           uint64_t in = 0;
           for (size_t i = 0; i < prefix.size(); i++) in |= 1ULL << prefix[i];
           for (int pos = static_cast<int>(prefix.size()); pos < T_; pos++) {
@@ -3263,14 +3292,30 @@ class SkinnerEngine : public JoinEnv {
             in |= 1ULL << order[pos];
           }
           Execute(order);
+         }
+         RunBatch();
         }
+        batching_ = false;
       } else {
         UctNode root(0, T_, *this, prefix, seed_);
         int round = 0;
+        std::vector<std::vector<std::pair<UctNode*, int>>> trails;
+        std::vector<double> placeholders;
+        batching_ = true;
         while (!IsComplete() && episodes_ < max_episodes) {
-          round++;
-          root.Sample(round, order);
+          trails.clear();
+          placeholders.clear();
+          while (batch_open()) {
+            round++;
+            trails.emplace_back();
+            root.Sample(round, order, &trails.back());
+            placeholders.push_back(pending_.back().placeholder);
+          }
+          RunBatch();
+          for (size_t k = 0; k < trails.size(); k++)
+            UctNode::Correct(trails[k], last_rewards_[k] - placeholders[k]);
         }
+        batching_ = false;
       }
       LogSamples(prefix.size());
     }
@@ -3301,63 +3346,109 @@ class SkinnerEngine : public JoinEnv {
 
   int64_t episodes() const { return episodes_; }
 
+  // An episode's join order and slice, decided when it is chosen: its
+  // leftmost table's slice starts at that table's offset, which moves past
+  // the slice at once, so the episodes of one batch take consecutive slices
+  // and each sees the offsets the earlier ones leave -- exactly the state a
+  // one-at-a-time run would give it.  Results therefore stay exactly-once
+  // however many episodes run together.
+  struct Pending {
+    std::vector<int> order;
+    int L = 0;
+    int64_t s0 = 0, s1 = 0, remaining = 0;
+    std::vector<int64_t> off;
+    double placeholder = 0;
+  };
+
   double Execute(const std::vector<int>& order) override {
-    episodes_++;
-    int L = order[0];
-    int64_t remaining = cards_[L] - offsets_[L];
-    int64_t len = std::max<int64_t>(1, std::min<int64_t>({slice_est_[L], remaining, kMaxSlice}));
-    int64_t s0 = offsets_[L], s1 = s0 + len;
-    KArgs a = args_;
-    // order, lookup plan and condition schedule of this order
-    std::vector<int> pos_of(T_);
-    for (int p = 0; p < T_; p++) pos_of[order[p]] = p;
-    uint64_t bound = 0;
-    for (int p = 0; p < T_; p++) {
-      int t = order[p];
-      int lk = -1;
-      int used_pred = -1;
-      if (p > 0)
-        for (size_t j = 0; j < preds_.size() && lk < 0; j++) {
-          const SkinnerPred& pr = preds_[j];
-          if (pr.tb == t && (bound >> pr.ta & 1ULL)) {
-            lk = static_cast<int>(j) * 2;
-            used_pred = pr.cond;
-          } else if (pr.ta == t && (bound >> pr.tb & 1ULL)) {
-            lk = static_cast<int>(j) * 2 + 1;
-            used_pred = pr.cond;
+    Pending p;
+    p.order = order;
+    p.L = order[0];
+    p.remaining = cards_[p.L] - offsets_[p.L];
+    const int64_t room = std::max<int64_t>(1, kMaxSlice - batch_items_);
+    const int64_t len = std::max<int64_t>(1, std::min<int64_t>({slice_est_[p.L], p.remaining, room}));
+    p.s0 = offsets_[p.L];
+    p.s1 = p.s0 + len;
+    p.off = offsets_;
+    offsets_[p.L] = p.s1;
+    batch_items_ += len;
+    p.placeholder = rewards_seen_ ? reward_sum_ / rewards_seen_ : 0.0;
+    pending_.push_back(std::move(p));
+    if (batching_) return pending_.back().placeholder;
+    RunBatch();
+    return last_rewards_[0];
+  }
+
+  // Runs the pending episodes together: one set of launches for the whole
+  // batch, each item finding its episode's parameters in a small block the
+  // host writes first.
+  void RunBatch() {
+    const int nb = static_cast<int>(pending_.size());
+    if (nb == 0) return;
+    const int W = EpWords();
+    std::vector<uint64_t> ep(static_cast<size_t>(nb) * W, 0);
+    int64_t start = 0;
+    for (int e = 0; e < nb; e++) {
+      const Pending& pe = pending_[e];
+      uint64_t* q = ep.data() + static_cast<size_t>(e) * W;
+      std::vector<int> pos_of(T_);
+      for (int p = 0; p < T_; p++) pos_of[pe.order[p]] = p;
+      uint64_t bound = 0;
+      for (int p = 0; p < T_; p++) {
+        int t = pe.order[p];
+        int lk = -1;
+        int used_pred = -1;
+        if (p > 0)
+          for (size_t j = 0; j < preds_.size() && lk < 0; j++) {
+            const SkinnerPred& pr = preds_[j];
+            if (pr.tb == t && (bound >> pr.ta & 1ULL)) {
+              lk = static_cast<int>(j) * 2;
+              used_pred = pr.cond;
+            } else if (pr.ta == t && (bound >> pr.tb & 1ULL)) {
+              lk = static_cast<int>(j) * 2 + 1;
+              used_pred = pr.cond;
+            }
           }
+        uint64_t after = bound | (1ULL << t);
+        uint64_t sched = 0;
+        for (size_t c = 0; c < cond_tables_.size(); c++) {
+          uint64_t m = cond_tables_[c];
+          bool ready_now = (m & ~after) == 0 && (p == 0 ? true : (m & ~bound) != 0);
+          if (p == 0 && m == 0) ready_now = true;  // constant conditions at the first table
+          if (ready_now && static_cast<int>(c) != used_pred) sched |= 1ULL << c;
         }
-      uint64_t after = bound | (1ULL << t);
-      uint64_t sched = 0;
-      for (size_t c = 0; c < cond_tables_.size(); c++) {
-        uint64_t m = cond_tables_[c];
-        bool ready_now = (m & ~after) == 0 && (p == 0 ? true : (m & ~bound) != 0);
-        if (p == 0 && m == 0) ready_now = true;  // constant conditions at the first table
-        if (ready_now && static_cast<int>(c) != used_pred) sched |= 1ULL << c;
+        bound = after;
+        q[p] = static_cast<uint64_t>(t);
+        q[T_ + p] = static_cast<uint64_t>(static_cast<int64_t>(lk));
+        q[2 * T_ + p] = sched;
       }
-      bound = after;
-      a.w[w_order_ + p] = static_cast<uint64_t>(t);
-      a.w[w_lookup_ + p] = static_cast<uint64_t>(static_cast<int64_t>(lk));
-      a.w[w_sched_ + p] = sched;
+      for (int t = 0; t < T_; t++) q[3 * T_ + t] = static_cast<uint64_t>(pe.off[t]);
+      q[4 * T_] = static_cast<uint64_t>(pe.s0);
+      q[4 * T_ + 1] = static_cast<uint64_t>(pe.s1);
+      q[4 * T_ + 2] = static_cast<uint64_t>(start);
+      start += pe.s1 - pe.s0;
     }
-    for (int t = 0; t < T_; t++) a.w[w_off_ + t] = static_cast<uint64_t>(offsets_[t]);
-    a.w[w_s0_] = static_cast<uint64_t>(s0);
-    a.w[w_s1_] = static_cast<uint64_t>(s1);
-    int64_t results = 0, work = 0;
+    const int64_t S = start;
+    ctx_.H2D(ep_, ep.data(), sizeof(uint64_t) * ep.size());
+    KArgs a = args_;
+    a.w[w_nep_] = static_cast<uint64_t>(nb);
+    a.w[w_total_] = static_cast<uint64_t>(S);
+    const int K = kMaxBatch;
+    std::vector<uint64_t> st(4 + 2 * K, 0);
     for (int attempt = 0; attempt < 8; attempt++) {
       a.w[w_cap_] = static_cast<uint64_t>(out_.cap);
       PatchOut(a);
       a.w[w_phase_] = 0;
-      ctx_.Launch(fn_, ctx_.GridFor(len, 128), 128, a, 0, T_ > 1 ? "skinner expand" : "skinner episode");
+      ctx_.Launch(fn_, ctx_.GridFor(S, 128), 128, a, 0, T_ > 1 ? "skinner expand" : "skinner episode");
       if (T_ > 1) {
-        ctx_.ScanU64(offs_, len);
+        ctx_.ScanU64(offs_, S);
         if (deep_) {
           // position-1 items expand their position-2 runs (or, past
           // kMaxItems2 items, run depth-first as below); then every
           // position-2 candidate is an item of its own
           a.w[w_phase_] = 2;
           ctx_.Launch(fn_, ctx_.num_sms * 8, 128, a, 0, "skinner expand2");
-          ctx_.ScanU64Bounded(offs2_, offs_ + len, kMaxItems2);
+          ctx_.ScanU64Bounded(offs2_, offs_ + S, kMaxItems2);
           a.w[w_phase_] = 3;
           ctx_.Launch(fn_, ctx_.num_sms * 8, 128, a, 0, "skinner episode");
         } else {
@@ -3365,13 +3456,12 @@ class SkinnerEngine : public JoinEnv {
           ctx_.Launch(fn_, ctx_.num_sms * 8, 128, a, 0, "skinner episode");
         }
       }
-      uint64_t cw[3] = {0, 0, 0};
-      ctx_.D2H(cw, stats_, 3 * sizeof(uint64_t));
-      if (split_ && cw[2] > 0 && !ctx_.dry) {
+      ctx_.D2H(st.data(), stats_, sizeof(uint64_t) * st.size());
+      if (split_ && st[2] > 0 && !ctx_.dry) {
         // queued hot runs: each round's tasks sit one position deeper than
         // the previous round's, so at most T rounds
         int qi = 0;
-        uint64_t pending = cw[2];
+        uint64_t pending = st[2];
         for (int round = 0; pending > 0; round++) {
           if (round > T_) throw Error(-5, "skinner task rounds did not converge");
           a.w[w_phase_] = 4;
@@ -3381,32 +3471,53 @@ class SkinnerEngine : public JoinEnv {
           qi = 1 - qi;
           ctx_.D2H(&pending, tcount_ + qi, sizeof(uint64_t));
         }
-        ctx_.D2H(cw, stats_, 2 * sizeof(uint64_t));
+        ctx_.D2H(st.data(), stats_, sizeof(uint64_t) * st.size());
       }
       ctx_.CheckDeviceError("skinner episode");
-      int64_t total = static_cast<int64_t>(cw[0]);
+      int64_t total = static_cast<int64_t>(st[0]);
       if (total <= out_.cap || ctx_.dry) {
-        results = total - produced_;
-        work = static_cast<int64_t>(cw[1]);
         produced_ = ctx_.dry ? 0 : total;
         break;
       }
-      Grow(total);  // the slice reruns into the larger buffer
+      Grow(total);  // the batch reruns into the larger buffer
       uint64_t keep = static_cast<uint64_t>(produced_);
       ctx_.H2D(count_, &keep, sizeof(uint64_t));
       ctx_.Memset(work_, 0, sizeof(uint64_t));
+      ctx_.Memset(eres_, 0, sizeof(uint64_t) * 2 * K);
     }
     ctx_.Memset(work_, 0, sizeof(uint64_t));
-    offsets_[L] = s1;
-    // size the next slice of L so its work matches the budget
-    double per_row = static_cast<double>(std::max<int64_t>(work, 1)) / len;
-    slice_est_[L] = std::max<int64_t>(1, std::min<int64_t>(int64_t(budget_ / per_row), 1LL << 26));
-    double progress = static_cast<double>(len) / static_cast<double>(remaining);
-    const double reward = 0.5 * progress + 0.5 * static_cast<double>(results) / static_cast<double>(budget_);
-    total_work_ += work;
-    if (ctx_.skinner_log && log_.size() < (1u << 16)) log_.emplace_back(order, reward);
-    return reward;
+    ctx_.Memset(eres_, 0, sizeof(uint64_t) * 2 * K);
+    // per episode: reward, and the next slice size of its leftmost table
+    // so its work matches the budget
+    last_rewards_.assign(nb, 0.0);
+    std::vector<int64_t> lwork(T_, 0), llen(T_, 0);
+    for (int e = 0; e < nb; e++) {
+      const Pending& pe = pending_[e];
+      const int64_t len = pe.s1 - pe.s0;
+      const int64_t results = static_cast<int64_t>(st[4 + e]);
+      const int64_t work = static_cast<int64_t>(st[4 + K + e]);
+      lwork[pe.L] += work;
+      llen[pe.L] += len;
+      const double progress = static_cast<double>(len) / static_cast<double>(pe.remaining);
+      const double reward = 0.5 * progress + 0.5 * static_cast<double>(results) / static_cast<double>(budget_);
+      last_rewards_[e] = reward;
+      reward_sum_ += reward;
+      rewards_seen_++;
+      total_work_ += work;
+      if (ctx_.skinner_log && log_.size() < (1u << 16)) log_.emplace_back(pe.order, reward);
+    }
+    for (int t = 0; t < T_; t++)
+      if (llen[t]) {
+        const double per_row = static_cast<double>(std::max<int64_t>(lwork[t], 1)) / llen[t];
+        slice_est_[t] = std::max<int64_t>(1, std::min<int64_t>(int64_t(budget_ / per_row), 1LL << 26));
+      }
+    episodes_ += nb;
+    batches_++;
+    pending_.clear();
+    batch_items_ = 0;
   }
+
+  int64_t batches() const { return batches_; }
 
  private:
   // Generates the episode kernel once; per-episode values are patched into
@@ -3415,29 +3526,45 @@ class SkinnerEngine : public JoinEnv {
     KernelSource ks;
     ExprGen eg(ctx_, ks);
     const int T = T_;
-    w_order_ = ks.Arg(0);
-    for (int i = 1; i < T; i++) ks.Arg(0);
-    w_lookup_ = ks.Arg(0);
-    for (int i = 1; i < T; i++) ks.Arg(0);
-    w_sched_ = ks.Arg(0);
-    for (int i = 1; i < T; i++) ks.Arg(0);
-    w_off_ = ks.Arg(0);
-    for (int i = 1; i < T; i++) ks.Arg(0);
-    w_s0_ = ks.Arg(0);
-    w_s1_ = ks.Arg(0);
+    // per-episode parameters of the batch (host-written block, EPW words
+    // per episode): order, lookup, condition schedule, offsets, s0, s1,
+    // first item index
+    const std::string EP = ks.Ptr(ep_, "uint64_t", true);
+    const std::string EPW = std::to_string(EpWords());
+    w_nep_ = ks.Arg(0);
+    w_total_ = ks.Arg(0);
     w_cap_ = ks.Arg(0);
     std::string TS = std::to_string(T);
+    const std::string KB = std::to_string(kMaxBatch);
     ks.L("int32_t ord[" + TS + "]; int32_t lk[" + TS + "]; uint64_t sched[" + TS + "]; int64_t off[" + TS + "];");
-    ks.L("for (int p = 0; p < " + TS + "; p++) { ord[p] = (int32_t)a.w[" + std::to_string(w_order_) +
-         " + p]; lk[p] = (int32_t)(int64_t)a.w[" + std::to_string(w_lookup_) + " + p]; sched[p] = a.w[" +
-         std::to_string(w_sched_) + " + p]; off[p] = (int64_t)a.w[" + std::to_string(w_off_) + " + p]; }");
     ks.L("int64_t card[" + TS + "];");
     for (int t = 0; t < T; t++) ks.L("card[" + std::to_string(t) + "] = (int64_t)" + ks.Word(static_cast<uint64_t>(cards_[t])) + ";");
-    ks.L("const int64_t s0 = (int64_t)a.w[" + std::to_string(w_s0_) + "], s1 = (int64_t)a.w[" + std::to_string(w_s1_) + "];");
+    ks.L("const int nep = (int)a.w[" + std::to_string(w_nep_) + "];");
+    ks.L("const int64_t S = (int64_t)a.w[" + std::to_string(w_total_) + "];");
+    ks.L("int cur_e = -1; int64_t s0 = 0, e_start = 0;");
+    ks.Open("auto use_ep = [&](int e)");
+    ks.L("if (e == cur_e) return;");
+    ks.L("cur_e = e;");
+    ks.L("const uint64_t* q = " + EP + " + (int64_t)e * " + EPW + ";");
+    ks.L("for (int p = 0; p < " + TS + "; p++) { ord[p] = (int32_t)q[p]; lk[p] = (int32_t)(int64_t)q[" + TS +
+         " + p]; sched[p] = q[2 * " + TS + " + p]; off[p] = (int64_t)q[3 * " + TS + " + p]; }");
+    ks.L("s0 = (int64_t)q[4 * " + TS + "]; e_start = (int64_t)q[4 * " + TS + " + 2];");
+    ks.indent--;
+    ks.L("};");
+    // the episode whose slice holds batch item x (items numbered episode
+    // after episode)
+    ks.Open("auto ep_of = [&](int64_t x) -> int");
+    ks.L("int e = 0;");
+    ks.L("while (e + 1 < nep && (int64_t)" + EP + "[(int64_t)(e + 1) * " + EPW + " + 4 * " + TS + " + 2] <= x) e++;");
+    ks.L("return e;");
+    ks.indent--;
+    ks.L("};");
+    // tuples examined and results, per episode of the batch
+    ks.L("unsigned long long wk[" + KB + "]; unsigned long long nres[" + KB + "];");
+    ks.L("for (int e = 0; e < " + KB + "; e++) { wk[e] = 0; nres[e] = 0; }");
     w_phase_ = ks.Arg(0);
     w_qin_ = ks.Arg(0);
     ks.L("int64_t rows[" + TS + "]; int64_t iti[" + TS + "]; int64_t ite[" + TS + "];");
-    ks.L("unsigned long long work = 0;");
     if (agg_) {
       ks.L("unsigned long long fa_nres = 0; int64_t fa_rows = 0;");
       for (size_t j = 0; j < agg_->plans->size(); j++) {
@@ -3563,7 +3690,7 @@ class SkinnerEngine : public JoinEnv {
         }
         ks.L("fa_c" + J + "++;");
       }
-      ks.L("fa_rows++; fa_nres++;");
+      ks.L("fa_rows++; fa_nres++; nres[cur_e]++;");
       w_count_ = ks.Arg(0);
     } else {
       Scope sc;
@@ -3573,6 +3700,7 @@ class SkinnerEngine : public JoinEnv {
       for (const auto& c : op_.output) vals.push_back(eg.Emit(*c.expr, sc));
       int wc = ks.Arg(0);
       w_count_ = wc;
+      ks.L("nres[cur_e]++;");
       ks.L("uint64_t slot = kdb_alloc_slot((unsigned long long*)a.w[" + std::to_string(wc) + "]);");
       ks.Open("if (slot < a.w[" + std::to_string(w_cap_) + "])");
       for (size_t c = 0; c < vals.size(); c++) {
@@ -3596,7 +3724,7 @@ class SkinnerEngine : public JoinEnv {
     // when the queue is full (the caller walks the run itself; the slots it
     // reserved past the capacity that are in range hold empty tasks)
     std::string TQ0, TQ1, TC, RUN, TCAP;
-    const std::string TW = std::to_string(3 + T);
+    const std::string TW = std::to_string(4 + T);  // position, begin, end, rows, episode
     if (split_) {
       TQ0 = ks.Ptr(tasks_[0], "uint64_t");
       TQ1 = ks.Ptr(tasks_[1], "uint64_t");
@@ -3616,6 +3744,7 @@ class SkinnerEngine : public JoinEnv {
       ks.L("const int64_t e = ok ? (b + " + RUN + " < ite[p] ? b + " + RUN + " : ite[p]) : 0;");
       ks.L("t[0] = (uint64_t)p; t[1] = (uint64_t)b; t[2] = (uint64_t)e;");
       ks.L("for (int k = 0; k < " + TS + "; k++) t[3 + k] = (uint64_t)rows[k];");
+      ks.L("t[3 + " + TS + "] = (uint64_t)cur_e;");
       ks.Close();
       ks.L("return ok;");
       ks.indent--;
@@ -3630,24 +3759,24 @@ class SkinnerEngine : public JoinEnv {
     std::string BG = ks.Ptr(beg_, "uint64_t"), OF = ks.Ptr(offs_, "uint64_t");
     ks.L("const int phase = (int)a.w[" + std::to_string(w_phase_) + "];");
     ks.Open("if (phase == 0)");
-    ks.Open("for (int64_t x = s0 + blockIdx.x * (int64_t)blockDim.x + threadIdx.x; x < s1; x += (int64_t)gridDim.x * blockDim.x)");
-    ks.L("rows[ord[0]] = x; work++;");
+    ks.Open("for (int64_t x = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; x < S; x += (int64_t)gridDim.x * blockDim.x)");
+    ks.L("use_ep(ep_of(x)); rows[ord[0]] = s0 + (x - e_start); wk[cur_e]++;");
     if (T == 1) {
       ks.L("if (conds_ok(sched[0])) emit();");
     } else {
       ks.L("uint64_t len = 0;");
       ks.Open("if (conds_ok(sched[0]))");
       ks.L("init(1);");
-      ks.L(BG + "[x - s0] = (uint64_t)iti[1];");
+      ks.L(BG + "[x] = (uint64_t)iti[1];");
       ks.L("len = (uint64_t)(ite[1] - iti[1]);");
       ks.Close();
-      ks.L(OF + "[x - s0] = len;");
+      ks.L(OF + "[x] = len;");
     }
     ks.Close();
     ks.Close();
     if (T > 1) {
       ks.Open("else if (phase == 1)");
-      ks.L("const int64_t m = s1 - s0;");
+      ks.L("const int64_t m = S;");
       ks.L("const uint64_t total = " + OF + "[m];");
       ks.Open("for (uint64_t w = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; w < total; w += (uint64_t)gridDim.x * blockDim.x)");
       ks.L("int64_t lo = 0, hi = m - 1;");
@@ -3655,10 +3784,10 @@ class SkinnerEngine : public JoinEnv {
       ks.L("const int64_t mid = (lo + hi + 1) >> 1;");
       ks.L("if (" + OF + "[mid] <= w) lo = mid; else hi = mid - 1;");
       ks.Close();
-      ks.L("rows[ord[0]] = s0 + lo;");
+      ks.L("use_ep(ep_of(lo)); rows[ord[0]] = s0 + (lo - e_start);");
       ks.L("const int64_t c1 = cand(1, (int64_t)(" + BG + "[lo] + (w - " + OF + "[lo])));");
       ks.L("if (c1 < 0 || c1 < off[ord[1]]) continue;");
-      ks.L("rows[ord[1]] = c1; work++;");
+      ks.L("rows[ord[1]] = c1; wk[cur_e]++;");
       ks.L("if (!conds_ok(sched[1])) continue;");
       // depth-first over positions from..T-1, the earlier ones bound; with
       // `preset` position `from`'s run is already in [iti, ite) (a task);
@@ -3682,7 +3811,7 @@ class SkinnerEngine : public JoinEnv {
         ks.Close();
         ks.L("int t = ord[p];");
         ks.L("if (c < off[t]) continue;");
-        ks.L("rows[t] = c; work++;");
+        ks.L("rows[t] = c; wk[cur_e]++;");
         ks.L("if (!conds_ok(sched[p])) continue;");
         ks.Open("if (p == " + std::to_string(T - 1) + ")");
         ks.L("emit();");
@@ -3710,7 +3839,7 @@ class SkinnerEngine : public JoinEnv {
         std::string B2 = ks.Ptr(beg2_, "uint64_t"), O2 = ks.Ptr(offs2_, "uint64_t");
         std::string CAP2 = "(uint64_t)" + ks.Word(static_cast<uint64_t>(kMaxItems2));
         ks.Open("else if (phase == 2)");
-        ks.L("const int64_t m = s1 - s0;");
+        ks.L("const int64_t m = S;");
         ks.L("const uint64_t total = " + OF + "[m];");
         ks.L("const bool fits = total <= " + CAP2 + ";");
         ks.Open("for (uint64_t w = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; w < total; w += (uint64_t)gridDim.x * blockDim.x)");
@@ -3721,10 +3850,10 @@ class SkinnerEngine : public JoinEnv {
         ks.L("const int64_t mid = (lo + hi + 1) >> 1;");
         ks.L("if (" + OF + "[mid] <= w) lo = mid; else hi = mid - 1;");
         ks.Close();
-        ks.L("rows[ord[0]] = s0 + lo;");
+        ks.L("use_ep(ep_of(lo)); rows[ord[0]] = s0 + (lo - e_start);");
         ks.L("const int64_t c1 = cand(1, (int64_t)(" + BG + "[lo] + (w - " + OF + "[lo])));");
         ks.Open("if (c1 >= 0 && c1 >= off[ord[1]])");
-        ks.L("rows[ord[1]] = c1; work++;");
+        ks.L("rows[ord[1]] = c1; wk[cur_e]++;");
         ks.Open("if (conds_ok(sched[1]))");
         ks.Open("if (fits)");
         ks.L("init(2);");
@@ -3741,7 +3870,7 @@ class SkinnerEngine : public JoinEnv {
         ks.Close();
         ks.Close();
         ks.Open("else if (phase == 3)");
-        ks.L("const int64_t m = s1 - s0;");
+        ks.L("const int64_t m = S;");
         ks.L("const uint64_t total = " + OF + "[m];");
         ks.Open("if (total <= " + CAP2 + " && total > 0)");
         ks.L("const uint64_t total2 = " + O2 + "[total];");
@@ -3757,12 +3886,12 @@ class SkinnerEngine : public JoinEnv {
         ks.L("const int64_t mid = (lo + hi + 1) >> 1;");
         ks.L("if (" + OF + "[mid] <= w) lo = mid; else hi = mid - 1;");
         ks.Close();
-        ks.L("rows[ord[0]] = s0 + lo;");
+        ks.L("use_ep(ep_of(lo)); rows[ord[0]] = s0 + (lo - e_start);");
         // the item had a non-empty run: its position-1 candidate is valid
         ks.L("rows[ord[1]] = cand(1, (int64_t)(" + BG + "[lo] + (w - " + OF + "[lo])));");
         ks.L("const int64_t c2 = cand(2, (int64_t)(" + B2 + "[w] + (w2 - " + O2 + "[w])));");
         ks.L("if (c2 < 0 || c2 < off[ord[2]]) continue;");
-        ks.L("rows[ord[2]] = c2; work++;");
+        ks.L("rows[ord[2]] = c2; wk[cur_e]++;");
         ks.L("if (!conds_ok(sched[2])) continue;");
         if (T == 3) ks.L("emit();");
         else depth_first("3", false, "0");
@@ -3781,6 +3910,7 @@ class SkinnerEngine : public JoinEnv {
         ks.L("const uint64_t* tq = qi ? " + TQ1 + " : " + TQ0 + ";");
         ks.Open("for (uint64_t w = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; w < nt; w += (uint64_t)gridDim.x * blockDim.x)");
         ks.L("const uint64_t* t = tq + w * " + TW + ";");
+        ks.L("use_ep((int)t[3 + " + TS + "]);");
         ks.L("const int tp = (int)t[0];");
         ks.L("iti[tp] = (int64_t)t[1]; ite[tp] = (int64_t)t[2];");
         ks.L("for (int k = 0; k < " + TS + "; k++) rows[k] = (int64_t)t[3 + k];");
@@ -3789,8 +3919,14 @@ class SkinnerEngine : public JoinEnv {
         ks.Close();
       }
     }
-    std::string wk = ks.Ptr(work_, "unsigned long long");
-    ks.L("if (work) atomicAdd(" + wk + ", work);");
+    {
+      const std::string WT = ks.Ptr(work_, "unsigned long long");
+      const std::string ER = ks.Ptr(eres_, "unsigned long long"), EW = ks.Ptr(ework_, "unsigned long long");
+      ks.Open("for (int e = 0; e < nep; e++)");
+      ks.L("if (wk[e]) { atomicAdd(&" + EW + "[e], wk[e]); atomicAdd(" + WT + ", wk[e]); }");
+      ks.L("if (nres[e]) atomicAdd(&" + ER + "[e], nres[e]);");
+      ks.Close();
+    }
     if (agg_) {
       std::string ST = ks.Ptr(agg_->state, "unsigned long long");
       ks.Open("if (fa_rows)");
@@ -3902,8 +4038,21 @@ class SkinnerEngine : public JoinEnv {
   int64_t episodes_ = 0;
   CUfunction fn_ = nullptr;
   KArgs args_;
-  int w_order_ = 0, w_lookup_ = 0, w_sched_ = 0, w_off_ = 0, w_s0_ = 0, w_s1_ = 0, w_cap_ = 0, w_count_ = 0,
-      w_pos_ = 0, w_phase_ = 0;
+  int w_nep_ = 0, w_total_ = 0, w_cap_ = 0, w_count_ = 0, w_pos_ = 0, w_phase_ = 0;
+  // batched episodes
+  static constexpr int kMaxBatch = 16;
+  int EpWords() const { return 4 * T_ + 4; }  // order, lookup, schedule, offsets (T each), s0, s1, start, pad
+  int batch_ = 8;
+  bool batching_ = false;  // Execute queues the episode instead of running it
+  std::vector<Pending> pending_;
+  int64_t batch_items_ = 0;  // leftmost tuples of the pending episodes
+  std::vector<double> last_rewards_;
+  double reward_sum_ = 0;
+  int64_t rewards_seen_ = 0;
+  int64_t batches_ = 0;
+  uint64_t* ep_ = nullptr;     // device: per-episode parameters
+  uint64_t* eres_ = nullptr;   // device: per-episode results (in stats_)
+  uint64_t* ework_ = nullptr;  // device: per-episode work (in stats_)
   static constexpr int64_t kMaxSlice = 1 << 20;  // leftmost tuples per episode
   // position-1 items of an episode that can be expanded to position 2
   static constexpr int64_t kMaxItems2 = 1 << 20;
@@ -3944,6 +4093,7 @@ MatBuffer Executor::RunSkinner(const Operator& op, const SkinnerAgg* agg) {
   SkinnerEngine eng(ctx_, arena_, op, mats, index_for, preds, alloc, ctx_.skinner_budget, ctx_.skinner_seed, agg);
   MatBuffer out = eng.Run(op.prefix_order);
   ctx_.last_skinner_episodes = eng.episodes();
+  ctx_.last_skinner_batches = eng.batches();
   ctx_.last_skinner_work = eng.work();
   return out;
 }

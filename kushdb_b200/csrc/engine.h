@@ -191,6 +191,7 @@ class Context {
   uint32_t skinner_seed = 0;
   int64_t last_skinner_episodes = 0;
   int64_t last_skinner_work = 0;  // tuples examined by all episodes
+  int64_t last_skinner_batches = 0;  // launches of episode batches
   // Join-order policy: 0 = UCT as the reference, 1 = UCT seeded by the
   // learned prior (falls back to 0 without a model or above 8 tables),
   // 2 = uniformly random connected orders (training-data collection).

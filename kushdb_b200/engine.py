@@ -33,7 +33,7 @@ EXPORTS = [
     "kdb_batch_create", "kdb_batch_configure", "kdb_batch_tune", "kdb_batch_config", "kdb_batch_run",
     "kdb_batch_run_timed", "kdb_batch_result", "kdb_batch_free", "kdb_sort_pairs_noalloc",
     "kdb_server_start", "kdb_server_submit", "kdb_server_poll", "kdb_server_stats", "kdb_server_stop",
-    "kdb_last_skinner_work", "kdb_mlp_num_features", "kdb_mlp_num_params", "kdb_mlp_create",
+    "kdb_last_skinner_work", "kdb_last_skinner_batches", "kdb_mlp_num_features", "kdb_mlp_num_params", "kdb_mlp_create",
     "kdb_mlp_last_error", "kdb_mlp_set_params", "kdb_mlp_get_params", "kdb_mlp_forward", "kdb_mlp_gradient",
     "kdb_mlp_train_step", "kdb_mlp_free", "kdb_ctx_set_skinner_policy", "kdb_last_skinner_samples",
     "kdb_ctx_set_prepared_queries",
@@ -113,6 +113,8 @@ def load_library(path: str = LIB_PATH):
     L.kdb_ctx_set_prepared_queries.argtypes = [P, I32]
     L.kdb_last_skinner_work.restype = I64
     L.kdb_last_skinner_work.argtypes = [P]
+    L.kdb_last_skinner_batches.restype = I64
+    L.kdb_last_skinner_batches.argtypes = [P]
     L.kdb_mlp_num_features.restype = I32
     L.kdb_mlp_num_features.argtypes = []
     L.kdb_mlp_num_params.restype = I64
@@ -346,6 +348,9 @@ class Engine:
 
     def last_skinner_episodes(self) -> int:
         return self.lib.kdb_last_skinner_episodes(self.ctx)
+
+    def last_skinner_batches(self) -> int:
+        return int(self.lib.kdb_last_skinner_batches(self.ctx))
 
     def last_skinner_work(self) -> int:
         """Tuples examined by all episodes of the last Skinner join."""

@@ -88,3 +88,36 @@ def test_hot_runs_as_tasks_match_oracle(engine, split, tasks, shape, n_tables, f
             engine.set_option(k, None)
         engine.set_skinner()
     assert compare(g, o.execute(plan)) == ""
+
+
+@pytest.mark.parametrize("batch", [1, 4, 16])
+@pytest.mark.parametrize("policy", ["uct", "random"])
+def test_episode_batches_keep_the_result(engine, batch, policy):
+    """Episodes run in batches (several join orders per launch, rewards
+    corrected after the batch): the result is the join's for every batch
+    size, and with more than one episode per batch there are fewer batches
+    than episodes."""
+    from oracle import Oracle
+    tables, tokens = wl.skinner_tables("chain", 7, min_rows=2000, max_rows=40_000, zipf_s=1.5, seed=91,
+                                       prefix=f"batch{batch}{policy}_")
+    plan = wl.skinner_plan(tables, tokens, "chain", like_tables=(2,))
+    o = Oracle()
+    for t in tables:
+        engine.register_table(t)
+        o.register_table(t)
+    engine.set_option("KDB_SKINNER_BATCH", str(batch))
+    engine.set_skinner_policy(policy)
+    engine.set_skinner(2000, seed=4)
+    try:
+        g = engine.execute(plan)
+        episodes, batches = engine.last_skinner_episodes(), engine.last_skinner_batches()
+    finally:
+        engine.set_option("KDB_SKINNER_BATCH", None)
+        engine.set_skinner_policy("uct")
+        engine.set_skinner()
+    assert compare(g, o.execute(plan)) == ""
+    assert episodes >= batches >= 1
+    if batch == 1:
+        assert batches == episodes
+    elif episodes > 4 * batch:
+        assert batches < episodes
