@@ -693,12 +693,15 @@ class Executor {
   // any_order: the consumer (an ORDER BY) orders the rows itself, so the
   // groups may come out in any order with their first-appearance key as the
   // stream position (pos_is_index false) instead of being sorted by it
-  MatBuffer RunGroupBy(const Operator& op, bool any_order = false);
+  MatBuffer RunGroupBy(const Operator& op, bool any_order = false, const Operator* order_by = nullptr);
   MatBuffer RunOrderBy(const Operator& op);
   MatBuffer RunSkinner(const Operator& op, const SkinnerAgg* agg = nullptr);
   MatBuffer SmallOrderBy(const Operator& op, MatBuffer& m);
   MatBuffer LargeOrderBy(const Operator& op, MatBuffer& m);
-  MatBuffer RunGroupByDense(const Operator& op, const std::vector<AggPlan>& plans, const KeyLayout& kl);
+  MatBuffer RunGroupByDense(const Operator& op, const std::vector<AggPlan>& plans, const KeyLayout& kl,
+                            const Operator* order_by = nullptr);
+  // the ORDER BY was done by its GROUP BY child (dense path)
+  bool group_sorted_ = false;
   bool BuildRowGroups(const Operator& op, std::vector<int>* key_cols);
   MatBuffer RunGroupByBuildRows(const Operator& op, const std::vector<AggPlan>& plans,
                                 const std::vector<int>& key_cols, bool any_order);
@@ -1754,7 +1757,7 @@ std::string ExprSig(const Expr& e) {
 // (compile/proxy/aggregate_hash_table.cc:187-243) turns into on a GPU when the
 // group count is tiny.
 MatBuffer Executor::RunGroupByDense(const Operator& op, const std::vector<AggPlan>& plans,
-                                    const KeyLayout& kl) {
+                                    const KeyLayout& kl, const Operator* order_by) {
   const int64_t D = static_cast<int64_t>(kl.domain);
   // words per group: per-agg value / count words (shared when identical),
   // then rows and first position
@@ -1984,6 +1987,62 @@ MatBuffer Executor::RunGroupByDense(const Operator& op, const std::vector<AggPla
   fk.Close();
   fk.Close();
   fk.L("*" + NG + " = (uint64_t)ng;");
+  // A parent ORDER BY whose keys are all enum GROUP BY keys is done here:
+  // the groups, in stream order, are re-ranked by the ORDER BY comparator
+  // (enum string order, NULLs after values, ascending or descending) with
+  // ties broken by the reference merge sort's tie path of the stream rank --
+  // the order the separate ORDER BY would produce.
+  std::vector<int> sort_key, sort_asc;
+  if (order_by) {
+    for (size_t k = 0; k < order_by->sort_keys.size(); k++) {
+      const Expr& sk = *order_by->sort_keys[k];
+      int key = -1;
+      if (sk.kind == ExprKind::ColRef && sk.child_idx == 0 && sk.column_idx < static_cast<int>(op.output.size())) {
+        const Expr& oe = *op.output[sk.column_idx].expr;
+        if (oe.kind == ExprKind::VirtColRef && oe.column_idx < static_cast<int>(op.group_by.size()) &&
+            op.group_by[oe.column_idx]->type.id == TypeId::ENUM)
+          key = oe.column_idx;
+      }
+      if (key < 0) {
+        sort_key.clear();
+        break;
+      }
+      sort_key.push_back(key);
+      sort_asc.push_back(order_by->asc[k] ? 1 : 0);
+    }
+  }
+  const bool fuse_order = !sort_key.empty();
+  if (fuse_order) {
+    // digit of key k of group g, and its enum string rank (NULL: -1)
+    auto key_rank = [&](int k, const std::string& g) {
+      int64_t stride = 1;
+      for (int j = 0; j < k; j++) stride *= static_cast<int64_t>(kl.card[j] + (kl.nullable[j] ? 1 : 0));
+      const int64_t base = static_cast<int64_t>(kl.card[k] + (kl.nullable[k] ? 1 : 0));
+      const std::string digit = "((" + g + " / " + std::to_string(stride) + ") % " + std::to_string(base) + ")";
+      const std::string rank = "(int64_t)" + fg.EnumRank(op.group_by[k]->type, "(int32_t)" + digit);
+      if (!kl.nullable[k]) return rank;
+      return "(" + digit + " == " + std::to_string(kl.card[k]) + " ? (int64_t)-1 : " + rank + ")";
+    };
+    fk.Open("auto kless = [&](int32_t ra, int32_t rb) -> bool");
+    fk.L("const int64_t ga = order[ra], gb = order[rb];");
+    for (size_t k = 0; k < sort_key.size(); k++) {
+      const std::string K = std::to_string(k);
+      fk.L("{ const int64_t xa = " + key_rank(sort_key[k], "ga") + ", xb = " + key_rank(sort_key[k], "gb") + ";");
+      // proxy::LessThan: a NULL (-1) sorts after every value
+      fk.L("  const bool ab = xa >= 0 && (xb < 0 || xa < xb), ba = xb >= 0 && (xa < 0 || xb < xa);");
+      fk.L(std::string("  if (ab) return ") + (sort_asc[k] ? "true" : "false") + "; if (ba) return " +
+           (sort_asc[k] ? "false" : "true") + "; }");
+    }
+    fk.L("return kdb_tie_path((uint64_t)ra, (uint64_t)ng) < kdb_tie_path((uint64_t)rb, (uint64_t)ng);");
+    fk.indent--;
+    fk.L("};");
+    fk.L("int32_t fin[" + std::to_string(D) + "];");
+    fk.Open("for (int32_t r = 0; r < ng; r++)");
+    fk.L("int32_t j = r;");
+    fk.L("while (j > 0 && kless(r, fin[j - 1])) { fin[j] = fin[j - 1]; j--; }");
+    fk.L("fin[j] = r;");
+    fk.Close();
+  }
   std::vector<std::string> optr, onull;
   for (const auto& c : out.cols) {
     optr.push_back(fk.Ptr(c.data, StoreType(c.type.id)));
@@ -1991,7 +2050,7 @@ MatBuffer Executor::RunGroupByDense(const Operator& op, const std::vector<AggPla
   }
   std::string posp = fk.Ptr(out.pos, "uint64_t");
   fk.Open("for (int32_t r = 0; r < ng; r++)");
-  fk.L("int64_t g = order[r];");
+  fk.L(fuse_order ? "int64_t g = order[fin[r]];" : "int64_t g = order[r];");
   fk.L("const uint64_t* t = tot + g * " + std::to_string(W) + ";");
   fk.L("int64_t rows = (int64_t)t[" + std::to_string(rows_w) + "];");
   fk.L("uint64_t fst = t[" + std::to_string(first_w) + "];");
@@ -2045,6 +2104,7 @@ MatBuffer Executor::RunGroupByDense(const Operator& op, const std::vector<AggPla
   out.rows = ReadU64(ngroups);
   ctx_.CheckDeviceError("group by");
   out.pos_is_index = true;
+  group_sorted_ = fuse_order;
   return out;
 }
 
@@ -2244,7 +2304,7 @@ MatBuffer Executor::RunGroupByBuildRows(const Operator& op, const std::vector<Ag
   return out;
 }
 
-MatBuffer Executor::RunGroupBy(const Operator& op, bool any_order) {
+MatBuffer Executor::RunGroupBy(const Operator& op, bool any_order, const Operator* order_by) {
   PrepareInput(op.child());
   int flags = 0;
   std::vector<AggPlan> plans;
@@ -2267,7 +2327,7 @@ MatBuffer Executor::RunGroupBy(const Operator& op, bool any_order) {
     }
     int64_t words = static_cast<int64_t>(distinct.size()) + 2;
     if (dense && static_cast<int64_t>(kl.domain) * words <= 64 && !ctx_.OptStr("KDB_NO_DENSE_GROUPBY"))
-      return RunGroupByDense(op, plans, kl);
+      return RunGroupByDense(op, plans, kl, order_by);
   }
 
   {
@@ -2539,9 +2599,34 @@ MatBuffer Executor::RunGroupBy(const Operator& op, bool any_order) {
 MatBuffer Executor::RunOrderBy(const Operator& op) {
   // every ORDER BY path below orders rows that are not in stream order by
   // their stream position, so a GROUP BY child need not sort its groups
+  group_sorted_ = false;
   MatBuffer m = op.child().kind == OpKind::GROUP_BY_AGGREGATE && !ctx_.OptStr("KDB_GROUP_ORDER_SORT")
-                    ? RunGroupBy(op.child(), true)
+                    ? RunGroupBy(op.child(), true, ctx_.OptStr("KDB_NO_GROUP_ORDER_FUSE") ? nullptr : &op)
                     : Materialize(op.child());
+  if (group_sorted_) {
+    // the dense GROUP BY wrote its groups in this ORDER BY's order; an
+    // output schema that passes every column through in place needs no
+    // further work
+    group_sorted_ = false;
+    bool identity = op.output.size() == m.cols.size();
+    for (size_t c = 0; identity && c < op.output.size(); c++) {
+      const Expr& e = *op.output[c].expr;
+      identity = e.kind == ExprKind::ColRef && e.child_idx == 0 && e.column_idx == static_cast<int>(c);
+    }
+    if (identity) return m;
+    uint32_t* idx = arena_.AllocT<uint32_t>(std::max<int64_t>(m.rows, 1));
+    if (m.rows > 0) {
+      KernelSource ks;
+      std::string I = ks.Ptr(idx, "uint32_t");
+      std::string N = ks.Word(static_cast<uint64_t>(m.rows));
+      ks.Open("for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < (int64_t)" + N +
+              "; i += (int64_t)gridDim.x * blockDim.x)");
+      ks.L(I + "[i] = (uint32_t)i;");
+      ks.Close();
+      LaunchPipeline(ks, m.rows, "order rows");
+    }
+    return MaterializeStream(op, idx, &m);
+  }
   int64_t n = m.rows;
   if (n <= kSmallOrder) return SmallOrderBy(op, m);
   return LargeOrderBy(op, m);

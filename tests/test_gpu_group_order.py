@@ -124,3 +124,45 @@ def test_table_group_order(engine, groups, order_col, asc):
     plan = _table_group_plan(t, order_col, asc)
     got = _run(engine, plan)
     assert compare(got, o.execute(plan.to_json()), ordered=True) == ""
+
+
+@pytest.mark.parametrize("keys_asc", [((0, True), (1, True)), ((0, False), (1, True)), ((1, False),),
+                                      ((1, True), (0, False))])
+@pytest.mark.parametrize("rows", [500, 200_000])
+def test_dense_group_order_fused(engine, keys_asc, rows):
+    """An ORDER BY over enum GROUP BY keys (one of them nullable) is done by
+    the dense group-by itself: same rows and order as the oracle and as the
+    separate one-block ORDER BY."""
+    from oracle import Oracle
+    from kushdb_b200.plan import EnumRegistry
+    EnumRegistry.register(61, ["zeta", "alpha", "mu"])
+    EnumRegistry.register(62, ["b", "a"])
+    o = Oracle()
+    rng = np.random.default_rng(rows)
+    t = HostTable("dense_order")
+    t.add(HostColumn("k1", Type.Enum(61), values=rng.integers(0, 3, rows).astype(np.int32)))
+    t.add(HostColumn("k2", Type.Enum(62), values=rng.integers(0, 2, rows).astype(np.int32),
+                     nulls=(rng.random(rows) < 0.2).astype(np.int8)))
+    t.add(HostColumn("v", Type.Real(), values=rng.random(rows)))
+    _register(engine, o, t)
+    rel = catalog_of([t])[t.name]
+    ss = OperatorSchema()
+    ss.AddGeneratedColumns(rel, ["k1", "k2", "v"])
+    scan = ScanOperator(ss, rel)
+    k1, k2 = ColRef(scan, "k1"), ColRef(scan, "k2")
+    aggs = [Sum(ColRef(scan, "v")), Count()]
+    g = OperatorSchema()
+    g.AddDerivedColumn("k1", VirtColRef(k1, 0))
+    g.AddDerivedColumn("k2", VirtColRef(k2, 1))
+    g.AddDerivedColumn("s", VirtColRef(aggs[0], 2))
+    g.AddDerivedColumn("n", VirtColRef(aggs[1], 3))
+    agg = GroupByAggregateOperator(g, scan, [k1, k2], aggs)
+    out = OperatorSchema()
+    out.AddPassthroughColumns(agg)
+    names = ["k1", "k2"]
+    plan = OutputOperator(OrderByOperator(out, agg, [ColRef(agg, names[k]) for k, _ in keys_asc],
+                                          [a for _, a in keys_asc]))
+    fused = _run(engine, plan)
+    assert compare(fused, o.execute(plan.to_json()), ordered=True) == ""
+    separate = _run(engine, plan, {"KDB_NO_GROUP_ORDER_FUSE": "1"})
+    assert compare(fused, separate, ordered=True) == ""
