@@ -19,7 +19,7 @@
  *   kdb_query_execute(ctx, json.c_str(), &result);
  *
  * Not supported by the backend (throws std::runtime_error):
- * CrossProductOperator and RegexpMatchingExpression (general LIKE).
+ * RegexpMatchingExpression (general LIKE with a regular expression).
  */
 #ifndef KDB_PLAN_JSON_H_
 #define KDB_PLAN_JSON_H_
@@ -299,8 +299,11 @@ class OpWriter : public kush::plan::ImmutableOperatorVisitor {
     out = "{\"op\":\"ORDER_BY\",\"child\":" + Of(op.Child()) + ",\"keys\":" + ExprList(op.KeyExprs()) +
           ",\"asc\":[" + asc + "],\"output\":" + Schema(op.Schema()) + "}";
   }
-  void Visit(const kush::plan::CrossProductOperator&) override {
-    throw std::runtime_error("CrossProduct is not supported by the B200 backend");
+  void Visit(const kush::plan::CrossProductOperator& op) override {
+    const auto ch = op.Children();
+    if (ch.size() != 2) throw std::runtime_error("CrossProduct takes two children");
+    out = "{\"op\":\"CROSS_PRODUCT\",\"left\":" + Of(ch[0].get()) + ",\"right\":" + Of(ch[1].get()) +
+          ",\"output\":" + Schema(op.Schema()) + "}";
   }
 
  private:

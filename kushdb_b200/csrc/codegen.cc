@@ -614,6 +614,8 @@ class Executor {
       case OpKind::SELECT: return RowBound(o.child());
       case OpKind::HASH_JOIN:
         return 2 * std::max<int64_t>(RowBound(o.child(1)), joins_.count(&o) ? joins_.at(&o).build.rows : 0);
+      case OpKind::CROSS_PRODUCT:
+        return std::max<int64_t>(1, RowBound(o.child(1)) * (mats_.count(&o.child(0)) ? mats_.at(&o.child(0)).rows : 1));
       default: {
         auto it = mats_.find(&o);
         return it == mats_.end() ? 1024 : it->second.rows;
@@ -622,7 +624,7 @@ class Executor {
   }
   static bool Streamable(const Operator& op) {
     return op.kind == OpKind::SCAN || op.kind == OpKind::SCAN_SELECT || op.kind == OpKind::SELECT ||
-           op.kind == OpKind::HASH_JOIN;
+           op.kind == OpKind::HASH_JOIN || op.kind == OpKind::CROSS_PRODUCT;
   }
 
   // Reads a device counter.  In a compile-only context it reports 2 rows so
@@ -662,6 +664,12 @@ class Executor {
         BuildJoin(op);
         PrepareInput(op.child(1));
         return;
+      case OpKind::CROSS_PRODUCT:
+        // the left child is buffered (cross_product_translator.cc:19-40)
+        if (!mats_.count(&op.child(0))) mats_[&op.child(0)] = Materialize(op.child(0));
+        PrepareCrossLeft(op);
+        PrepareInput(op.child(1));
+        return;
       default: return;
     }
   }
@@ -685,8 +693,12 @@ class Executor {
   MatBuffer MaterializeStream(const Operator& op, const uint32_t* order = nullptr,
                               const MatBuffer* ordered_src = nullptr);
   MatBuffer MaterializeCounted(const Operator& op);
+  // left rows of a CROSS_PRODUCT in the left child's stream order (null:
+  // the buffer already is in that order)
+  std::map<const Operator*, uint32_t*> cross_order_;
+  void PrepareCrossLeft(const Operator& op);
   static bool StreamHasJoin(const Operator& op) {
-    if (op.kind == OpKind::HASH_JOIN) return true;
+    if (op.kind == OpKind::HASH_JOIN || op.kind == OpKind::CROSS_PRODUCT) return true;
     return op.kind == OpKind::SELECT && Streamable(op.child()) && StreamHasJoin(op.child());
   }
   MatBuffer RunAggregate(const Operator& op);
@@ -904,11 +916,13 @@ void Executor::EmitStream(KernelSource& ks, ExprGen& eg, const Operator& op, con
       } else {
         ks.Open("for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < (int64_t)" + n +
                 "; r += (int64_t)gridDim.x * blockDim.x)");
-        // The probe side of a join reads its columns where the consumer uses
-        // them: the probe key at once, every other column only inside the
-        // match branch, so rows without a match never load them (about a
-        // third of the sectors of a 9%-selective probe).
-        const bool lazy = probe_side && !ctx_.OptStr("KDB_EAGER_PROBE_COLUMNS");
+        // With KDB_LAZY_PROBE_COLUMNS the probe side of a join reads its
+        // columns where the consumer uses them (non-key columns only inside
+        // the match branch).  Measured on the Q3 shape it is slower (61 vs
+        // 55 us for the probe + group-by kernel): the loads then wait behind
+        // the probe's dependent accesses instead of overlapping them, which
+        // costs more than the sectors saved, so all columns load up front.
+        const bool lazy = probe_side && ctx_.OptStr("KDB_LAZY_PROBE_COLUMNS");
         load = [&, lazy](size_t k) {
           const DevColumn& c = *cols[k];
           std::string v;
@@ -998,11 +1012,55 @@ void Executor::EmitStream(KernelSource& ks, ExprGen& eg, const Operator& op, con
       probe_side_scan_ = false;
       return;
     }
+    case OpKind::CROSS_PRODUCT: {
+      // cross_product_translator.cc:43-74: every right row meets the
+      // buffered left rows in their stream order; the pair's position is
+      // (right position, left stream rank)
+      const MatBuffer& lm = mats_.at(&op.child(0));
+      const uint32_t* lorder = cross_order_.count(&op) ? cross_order_.at(&op) : nullptr;
+      const std::string NL = "(int64_t)" + ks.Word(static_cast<uint64_t>(lm.rows));
+      const std::string LO = lorder ? ks.Ptr(lorder, "uint32_t", true) : "";
+      auto body = [&](const std::vector<CVal>& right, const std::string& pos) {
+        const std::string li = ks.Fresh("li"), lr = ks.Fresh("lr");
+        ks.Open("for (int64_t " + li + " = 0; " + li + " < " + NL + "; " + li + "++)");
+        ks.L("const int64_t " + lr + " = " + (lorder ? "(int64_t)" + LO + "[" + li + "]" : li) + ";");
+        std::vector<CVal> left = LoadMatRow(ks, eg, lm, lr, nullptr);
+        Scope s2;
+        s2.child.push_back(left);
+        s2.child.push_back(right);
+        std::vector<CVal> out;
+        for (const auto& c : op.output) out.push_back(eg.Emit(*c.expr, s2));
+        consume(out, "((" + pos + ") << 32) | (uint64_t)" + li);
+        ks.Close();
+      };
+      if (Streamable(op.child(1))) EmitStream(ks, eg, op.child(1), body, src_rows);
+      else EmitMatScan(ks, mats_.at(&op.child(1)), nullptr, body, src_rows);
+      return;
+    }
     default: {
       EmitMatScan(ks, mats_.at(&op), nullptr, consume, src_rows);
       return;
     }
   }
+}
+
+void Executor::PrepareCrossLeft(const Operator& op) {
+  const MatBuffer& lm = mats_.at(&op.child(0));
+  if (lm.rows >= (int64_t(1) << 32)) throw Error(-5, "CrossProduct left side of 2^32 rows or more");
+  if (lm.pos_is_index || lm.rows <= 1 || cross_order_.count(&op)) return;
+  // buffer rows not in stream order: sort their positions once
+  uint64_t* keys = arena_.AllocT<uint64_t>(lm.rows);
+  uint32_t* idx = arena_.AllocT<uint32_t>(lm.rows);
+  KernelSource ks;
+  const std::string K = ks.Ptr(keys, "uint64_t"), I = ks.Ptr(idx, "uint32_t");
+  const std::string P = ks.Ptr(lm.pos, "uint64_t", true), N = ks.Word(static_cast<uint64_t>(lm.rows));
+  ks.Open("for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < (int64_t)" + N +
+          "; i += (int64_t)gridDim.x * blockDim.x)");
+  ks.L(K + "[i] = " + P + "[i]; " + I + "[i] = (uint32_t)i;");
+  ks.Close();
+  LaunchPipeline(ks, lm.rows, "cross order");
+  ctx_.RadixSortPairs(keys, idx, lm.rows, arena_, 64);
+  cross_order_[&op] = idx;
 }
 
 void Executor::EmitProbe(KernelSource& ks, ExprGen& eg, const JoinTable& jt,
@@ -1652,7 +1710,10 @@ MatBuffer Executor::RunAggregate(const Operator& op) {
   ks.L("uint64_t t = kdb_block_reduce(first, KdbMinU64(), red_u);");
   store(nw - 1, "t");
   ks.Close();
-  fused_finalize = !ctx_.OptStr("KDB_AGG_SEPARATE_FINALIZE");
+  // The last CTA can combine the partials itself (KDB_AGG_FUSED_FINALIZE),
+  // but measured at 1M rows that kernel's serial tail costs more than the
+  // second one-block launch (13.1 us vs 10.6 + 6.6 us; step 50.2 vs 49.1 us)
+  fused_finalize = ctx_.OptStr("KDB_AGG_FUSED_FINALIZE") != nullptr;
   if (fused_finalize) {
     // the last CTA to finish combines the partials (same fixed-order
     // reduction as the separate finalize) and writes the result row

@@ -101,7 +101,7 @@ struct Expr {
 
 // plan::Operator kinds (plan/operator/operator_visitor.h:5-15)
 enum class OpKind { SCAN, SCAN_SELECT, SELECT, HASH_JOIN, GROUP_BY_AGGREGATE, AGGREGATE, ORDER_BY,
-                    SKINNER_JOIN, OUTPUT };
+                    SKINNER_JOIN, OUTPUT, CROSS_PRODUCT };
 
 struct SchemaCol {
   std::string name;
@@ -273,6 +273,12 @@ inline std::unique_ptr<Operator> ParseOperator(const json::Value& j) {
     op->children.push_back(ParseOperator(j.at("right")));
     op->left_keys = ParseExprList(j.at("left_keys"));
     op->right_keys = ParseExprList(j.at("right_keys"));
+    op->output = ParseSchema(j.at("output"));
+  } else if (k == "CROSS_PRODUCT") {
+    // plan/operator/cross_product_operator.h: exactly two children
+    op->kind = OpKind::CROSS_PRODUCT;
+    op->children.push_back(ParseOperator(j.at("left")));
+    op->children.push_back(ParseOperator(j.at("right")));
     op->output = ParseSchema(j.at("output"));
   } else if (k == "GROUP_BY_AGGREGATE") {
     op->kind = OpKind::GROUP_BY_AGGREGATE;

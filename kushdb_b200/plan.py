@@ -627,6 +627,20 @@ class HashJoinOperator(Operator):
                 "output": self.schema.to_list()}
 
 
+class CrossProductOperator(Operator):
+    """plan/operator/cross_product_operator.h: left x right (two children),
+    every right row paired with every left row."""
+
+    def __init__(self, schema: OperatorSchema, children: Sequence[Operator]):
+        if len(children) != 2:
+            raise ValueError("CrossProduct takes two children")
+        super().__init__(schema, list(children))
+
+    def to_dict(self):
+        return {"op": "CROSS_PRODUCT", "left": self.children[0].to_dict(),
+                "right": self.children[1].to_dict(), "output": self.schema.to_list()}
+
+
 class GroupByAggregateOperator(Operator):
     def __init__(self, schema: OperatorSchema, child: Operator,
                  group_by: Sequence[Expression], aggs: Sequence[AggregateExpression]):

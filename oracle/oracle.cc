@@ -424,6 +424,7 @@ class Executor {
       case OpKind::SCAN_SELECT: return ProduceScanSelect(op, consume);
       case OpKind::SELECT: return ProduceSelect(op, consume);
       case OpKind::HASH_JOIN: return ProduceHashJoin(op, consume);
+      case OpKind::CROSS_PRODUCT: return ProduceCrossProduct(op, consume);
       case OpKind::GROUP_BY_AGGREGATE: return ProduceGroupBy(op, consume);
       case OpKind::AGGREGATE: return ProduceAggregate(op, consume);
       case OpKind::ORDER_BY: return ProduceOrderBy(op, consume);
@@ -511,6 +512,23 @@ class Executor {
       default: k.i = v.i; break;
     }
     return k;
+  }
+
+  // cross_product_translator.cc:19-74: the left child is buffered in its
+  // stream order; every right row then meets every buffered left row.
+  void ProduceCrossProduct(const Operator& op, const Consumer& consume) {
+    std::vector<Row> left;
+    Produce(op.child(0), [&](const Row& in) { left.push_back(in); });
+    Row out(op.output.size());
+    Produce(op.child(1), [&](const Row& in) {
+      EvalEnv env;
+      env.child[1] = &in;
+      for (const Row& l : left) {
+        env.child[0] = &l;
+        for (size_t k = 0; k < op.output.size(); k++) out[k] = Eval(*op.output[k].expr, env);
+        consume(out);
+      }
+    });
   }
 
   // hash_join_translator.cc:34-139.  Build = left child, rows with a NULL key

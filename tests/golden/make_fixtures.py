@@ -44,6 +44,7 @@ WIDTH = {"SMALLINT": np.int16, "INT": np.int32, "BIGINT": np.int64, "REAL": np.f
 
 # table -> list of (column, type, data file stem, has null file)
 TABLES = {
+    "region": [("r_regionkey", "INT", "r_regionkey", False), ("r_name", "TEXT", "r_name", False)],
     "people": [("id", "INT", "people_id", True), ("name", "TEXT", "people_name", True)],
     "people_enum": [("id", "INT", "people_id", True),
                     ("name", "ENUM:people_name_enum", "people_name_enum", True)],
@@ -80,7 +81,7 @@ TABLES = {
 }
 
 EXPECTED_DIRS = ["tpch", "hash_join", "group_by_aggregate", "aggregate", "scan_select",
-                 "select", "order_by", "skinner_join", "simd_scan_select"]
+                 "select", "order_by", "skinner_join", "simd_scan_select", "cross_product"]
 TPCH_KEEP = {"q01_expected.tbl", "q03_expected.tbl", "q06_expected.tbl"}
 
 

@@ -24,7 +24,7 @@ from kushdb_b200.plan import (INT_MIN, INT_MAX, And, Avg, BigIntLiteral, Case, C
                               Leq, Literal, Lt, Max, Min, Mul, OperatorSchema, OrderByOperator,
                               OutputOperator, ScanOperator, ScanSelectOperator, SelectOperator,
                               SkinnerJoinOperator, SmallIntLiteral, Sub, Add, Sum, VirtColRef,
-                              AggregateOperator, SimdScanSelectOperator)
+                              AggregateOperator, SimdScanSelectOperator, CrossProductOperator)
 
 GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
 
@@ -274,6 +274,18 @@ for _t, _rel, _col in [("bigint", "info", "num2"), ("boolean", "info", "cheated"
     _add(f"hash_join/{_t}", (lambda r=_rel, c=_col: _hash_join(r, r, c)), f"hash_join/{_t}_expected.tbl", "sorted")
     _add(f"skinner_join/{_t}", (lambda r=_rel, c=_col: _skinner(r, c)), f"skinner_join/{_t}_expected.tbl", "sorted")
 _add("hash_join/int", lambda: _hash_join("people", "info", "id"), "hash_join/int_expected.tbl", "sorted")
+
+
+def _cross_product():
+    # end_to_end_test/cross_product/cross_product_test.cc: region x region on r_name
+    a, b = _two_scans("region", "r_name", "region", "r_name")
+    schema = OperatorSchema()
+    schema.AddPassthroughColumns(a, 0)
+    schema.AddPassthroughColumns(b, 1)
+    return OutputOperator(CrossProductOperator(schema, [a, b]))
+
+
+_add("cross_product/text", _cross_product, "cross_product/cross_product_expected.tbl", "sorted")
 _add("skinner_join/int", lambda: _skinner("info", "id"), "skinner_join/int_expected.tbl", "sorted")
 
 
