@@ -710,6 +710,7 @@ class Executor {
   MatBuffer RunSkinner(const Operator& op, const SkinnerAgg* agg = nullptr);
   MatBuffer SmallOrderBy(const Operator& op, MatBuffer& m);
   MatBuffer LargeOrderBy(const Operator& op, MatBuffer& m);
+  void SortItems(uint64_t* items, int64_t n);
   MatBuffer RunGroupByDense(const Operator& op, const std::vector<AggPlan>& plans, const KeyLayout& kl,
                             const Operator* order_by = nullptr);
   // the ORDER BY was done by its GROUP BY child (dense path)
@@ -2759,6 +2760,14 @@ MatBuffer Executor::SmallOrderBy(const Operator& op, MatBuffer& m) {
   return MaterializeStream(op, idx, &m);
 }
 
+// (key, tie) order of 16-byte items: a sample sort, or the block sort plus
+// merge passes (KDB_ORDER_MERGE, or when the sample sort's buckets came out
+// too large)
+void Executor::SortItems(uint64_t* items, int64_t n) {
+  if (!ctx_.OptStr("KDB_ORDER_MERGE") && ctx_.SampleSortItems(items, n, arena_)) return;
+  ctx_.MergeSortItems(items, n, arena_);
+}
+
 MatBuffer Executor::LargeOrderBy(const Operator& op, MatBuffer& m) {
   int64_t n = m.rows;
   uint64_t* keys = arena_.AllocT<uint64_t>(std::max<int64_t>(n, 1));
@@ -2862,7 +2871,7 @@ MatBuffer Executor::LargeOrderBy(const Operator& op, MatBuffer& m) {
         // alone and look for equal neighbours.  Without ties the tie rank
         // never decides, and the stream-order sort is not needed.
         make_items(false);
-        ctx_.MergeSortItems(items, n, arena_);
+        SortItems(items, n);
         uint64_t* ties = arena_.AllocT<uint64_t>(1);
         ctx_.Memset(ties, 0, sizeof(uint64_t));
         {
@@ -2884,7 +2893,7 @@ MatBuffer Executor::LargeOrderBy(const Operator& op, MatBuffer& m) {
       }
       stream_order();
       make_items(true);
-      ctx_.MergeSortItems(items, n, arena_);
+      SortItems(items, n);
       order_rows();
       return MaterializeStream(op, idx, &m);
     }

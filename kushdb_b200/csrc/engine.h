@@ -323,6 +323,10 @@ class Context {
   // (key, tie) (block sort + merge-path passes; items equal in (key, tie)
   // come out in no particular order)
   void MergeSortItems(void* items, int64_t n, Arena& arena);
+  // the same order by a sample sort (splitters, one bucketing pass, one
+  // shared-memory sort per bucket); false, with the items untouched, when a
+  // bucket came out too large (the caller then merge sorts)
+  bool SampleSortItems(void* items, int64_t n, Arena& arena);
   // exclusive prefix sum of a[0..n) in place, the total into a[n]
   void ScanU64(uint64_t* a, int64_t n, const char* tag = "skinner scan");
   // the same over *n_ptr elements (a device word), skipped when *n_ptr > cap

@@ -603,6 +603,192 @@ void SortShapes(const Context& ctx, SortShape* block, SortShape* merge) {
   }
 }
 
+// ---------------------------------------------------------------------------
+// Sample sort of 16-byte items by (key, tie): splitters are quantiles of a
+// strided sample (sorted in one block), one pass sends every item to its
+// bucket, and one CTA per bucket sorts it in shared memory (bitonic) and
+// writes it at the bucket's offset.  (key, tie) pairs are unique, so the
+// buckets stay balanced whatever the key distribution; a bucket larger than
+// kBucketCap makes the caller fall back to the merge sort.
+// ---------------------------------------------------------------------------
+namespace {
+
+constexpr int kSampleOver = 8;       // samples per bucket
+constexpr int kMaxBuckets = 1024;
+constexpr int kBucketCap = 8192;     // items a bucket may hold (128 KiB of shared memory)
+
+// (key, tie, val): the order of ItemLess, refined by the value so that the
+// padding items (all ones; real values are rows below 2^31) sort last
+__device__ __forceinline__ bool ItemLess3(const SortItem& a, const SortItem& b) {
+  if (a.key != b.key) return a.key < b.key;
+  if (a.tie != b.tie) return a.tie < b.tie;
+  return a.val < b.val;
+}
+
+__device__ __forceinline__ void CmpSwap(SortItem* s, int i, int j, bool up) {
+  SortItem a = s[i], b = s[j];
+  if (ItemLess3(b, a) == up) {
+    s[i] = b;
+    s[j] = a;
+  }
+}
+
+// bitonic sort of s[0..m) in shared memory, m a power of two
+__device__ void BitonicSort(SortItem* s, int m) {
+  for (int k = 2; k <= m; k <<= 1)
+    for (int j = k >> 1; j > 0; j >>= 1) {
+      for (int i = threadIdx.x; i < m; i += blockDim.x) {
+        const int l = i ^ j;
+        if (l > i) CmpSwap(s, i, l, (i & k) == 0);
+      }
+      __syncthreads();
+    }
+}
+
+__device__ __forceinline__ SortItem MaxItem() {
+  SortItem m;
+  m.key = ~0ULL;
+  m.tie = 0xffffffffu;
+  m.val = 0xffffffffu;
+  return m;
+}
+
+// one block: the strided sample, sorted; splitter j = sample[(j + 1) * over]
+__global__ void SampleSplitters(const SortItem* __restrict__ items, int64_t n, int buckets,
+                                SortItem* __restrict__ splitters) {
+  extern __shared__ SortItem smp[];
+  const int m = buckets * kSampleOver;  // a power of two
+  for (int i = threadIdx.x; i < m; i += blockDim.x) {
+    const int64_t at = (static_cast<int64_t>(i) * n) / m;
+    smp[i] = items[at];
+  }
+  __syncthreads();
+  BitonicSort(smp, m);
+  for (int j = threadIdx.x; j + 1 < buckets; j += blockDim.x) splitters[j] = smp[(j + 1) * kSampleOver];
+}
+
+__device__ __forceinline__ int BucketOf(const SortItem& x, const SortItem* spl, int buckets) {
+  int lo = 0, hi = buckets - 1;  // first splitter greater than x, in [0, buckets - 1]
+  while (lo < hi) {
+    const int mid = (lo + hi) >> 1;
+    if (ItemLess(x, spl[mid])) hi = mid;
+    else lo = mid + 1;
+  }
+  return lo;
+}
+
+__global__ void SampleBucketCount(const SortItem* __restrict__ items, int64_t n, int buckets,
+                                  const SortItem* __restrict__ splitters, uint16_t* __restrict__ bucket_of,
+                                  unsigned* __restrict__ counts) {
+  __shared__ SortItem spl[kMaxBuckets];
+  __shared__ unsigned cnt[kMaxBuckets];
+  for (int j = threadIdx.x; j < buckets; j += blockDim.x) {
+    if (j + 1 < buckets) spl[j] = splitters[j];
+    cnt[j] = 0;
+  }
+  __syncthreads();
+  for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < n;
+       i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const int b = BucketOf(items[i], spl, buckets);
+    bucket_of[i] = static_cast<uint16_t>(b);
+    atomicAdd(&cnt[b], 1u);
+  }
+  __syncthreads();
+  for (int j = threadIdx.x; j < buckets; j += blockDim.x)
+    if (cnt[j]) atomicAdd(&counts[j], cnt[j]);
+}
+
+// one block: exclusive offsets of the bucket counts (offs[buckets] = n),
+// cursors zeroed, the largest bucket into *largest
+__global__ void SampleBucketOffsets(const unsigned* __restrict__ counts, int buckets, unsigned* __restrict__ offs,
+                                    unsigned* __restrict__ cursor, unsigned* __restrict__ largest) {
+  __shared__ unsigned s[kMaxBuckets];
+  for (int j = threadIdx.x; j < buckets; j += blockDim.x) s[j] = counts[j];
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    unsigned run = 0, big = 0;
+    for (int j = 0; j < buckets; j++) {
+      const unsigned c = s[j];
+      offs[j] = run;
+      run += c;
+      big = c > big ? c : big;
+    }
+    offs[buckets] = run;
+    *largest = big;
+  }
+  for (int j = threadIdx.x; j < buckets; j += blockDim.x) cursor[j] = 0;
+}
+
+__global__ void SampleScatter(const SortItem* __restrict__ items, int64_t n, const uint16_t* __restrict__ bucket_of,
+                              const unsigned* __restrict__ offs, unsigned* __restrict__ cursor,
+                              SortItem* __restrict__ out) {
+  for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < n;
+       i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const int b = bucket_of[i];
+    out[offs[b] + atomicAdd(&cursor[b], 1u)] = items[i];
+  }
+}
+
+// one block per bucket: sort it in shared memory, write it in place in dst
+__global__ void SampleBucketSort(const SortItem* __restrict__ src, const unsigned* __restrict__ offs,
+                                 SortItem* __restrict__ dst) {
+  extern __shared__ SortItem sb[];
+  const unsigned b0 = offs[blockIdx.x], cnt = offs[blockIdx.x + 1] - b0;
+  if (cnt == 0) return;
+  int m = 1;
+  while (m < static_cast<int>(cnt)) m <<= 1;
+  for (int i = threadIdx.x; i < m; i += blockDim.x) sb[i] = i < static_cast<int>(cnt) ? src[b0 + i] : MaxItem();
+  __syncthreads();
+  BitonicSort(sb, m);
+  for (int i = threadIdx.x; i < static_cast<int>(cnt); i += blockDim.x) dst[b0 + i] = sb[i];
+}
+
+}  // namespace
+
+bool Context::SampleSortItems(void* items_v, int64_t n, Arena& arena) {
+  if (n <= 1 || dry) return true;
+  if (n > 0x7fffffffLL) return false;
+  // buckets: a power of two near n / 512, at most kMaxBuckets
+  int buckets = 2;
+  while (buckets < kMaxBuckets && static_cast<int64_t>(buckets) * 512 < n) buckets <<= 1;
+  SortItem* items = static_cast<SortItem*>(items_v);
+  SortItem* spl = reinterpret_cast<SortItem*>(arena.Alloc(sizeof(SortItem) * buckets));
+  SortItem* tmp = reinterpret_cast<SortItem*>(arena.Alloc(sizeof(SortItem) * n));
+  uint16_t* bof = reinterpret_cast<uint16_t*>(arena.Alloc(sizeof(uint16_t) * n));
+  unsigned* counts = arena.AllocT<unsigned>(buckets);
+  unsigned* offs = arena.AllocT<unsigned>(buckets + 1);
+  unsigned* cursor = arena.AllocT<unsigned>(buckets);
+  unsigned* largest = arena.AllocT<unsigned>(1);
+  Memset(counts, 0, sizeof(unsigned) * buckets);
+  const size_t smem_sample = sizeof(SortItem) * buckets * kSampleOver;
+  const int grid = GridFor(n, 256);
+  TimedStart("sort sample");
+  if (smem_sample > 48 * 1024)
+    KDB_CUDA(cudaFuncSetAttribute(SampleSplitters, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  static_cast<int>(smem_sample)));
+  const int b = buckets;
+  Issue([=](cudaStream_t s) { SampleSplitters<<<1, 1024, smem_sample, s>>>(items, n, b, spl); });
+  Issue([=](cudaStream_t s) { SampleBucketCount<<<grid, 256, 0, s>>>(items, n, b, spl, bof, counts); });
+  Issue([=](cudaStream_t s) { SampleBucketOffsets<<<1, 256, 0, s>>>(counts, b, offs, cursor, largest); });
+  TimedStop();
+  KDB_CUDA(cudaGetLastError());
+  unsigned big = 0;
+  D2H(&big, largest, sizeof(big));
+  if (big > static_cast<unsigned>(kBucketCap)) return false;  // skewed sample: the merge sort takes it
+  int m = 1;
+  while (m < static_cast<int>(big)) m <<= 1;
+  const size_t smem_bucket = sizeof(SortItem) * std::max(m, 1);
+  TimedStart("sort buckets");
+  Issue([=](cudaStream_t s) { SampleScatter<<<grid, 256, 0, s>>>(items, n, bof, offs, cursor, tmp); });
+  if (smem_bucket > 48 * 1024)
+    KDB_CUDA(cudaFuncSetAttribute(SampleBucketSort, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  static_cast<int>(smem_bucket)));
+  Issue([=](cudaStream_t s) { SampleBucketSort<<<b, 512, smem_bucket, s>>>(tmp, offs, items); });
+  TimedStop();
+  KDB_CUDA(cudaGetLastError());
+  return true;
+}
+
 void Context::MergeSortItems(void* items, int64_t n, Arena& arena) {
   if (n <= 1 || dry) return;
   if (n > 0x7fffffffLL) throw Error(-5, "merge sort of more than 2^31 items");
