@@ -915,8 +915,48 @@ void Executor::EmitStream(KernelSource& ks, ExprGen& eg, const Operator& op, con
         ks.L("const int64_t r = base + u;");
         ks.Open("if (r < nrows)");
       } else {
+        // On a join's probe side (one row per thread and iteration) the next
+        // iteration's values of every fixed-width column are loaded before
+        // this iteration's row is probed, so their HBM latency overlaps the
+        // probe's dependent L2 accesses (KDB_NO_PROBE_PREFETCH: off).
+        const bool pf = probe_side && !ctx_.OptStr("KDB_NO_PROBE_PREFETCH") && !ctx_.OptStr("KDB_LAZY_PROBE_COLUMNS");
+        std::vector<std::string> nxt(cols.size()), nnx(cols.size());
+        if (pf) {
+          ks.L("const int64_t kdb_pstride = (int64_t)gridDim.x * blockDim.x;");
+          ks.L("const int64_t kdb_p0 = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;");
+          for (size_t k = 0; k < cols.size(); k++) {
+            if (cols[k]->type.id == TypeId::TEXT) continue;
+            const std::string st = StoreType(cols[k]->type.id);
+            nxt[k] = ks.Fresh("X");
+            ks.L(st + " " + nxt[k] + " = kdb_p0 < (int64_t)" + n + " ? " + dp[k] + "[kdb_p0] : (" + st + ")0;");
+            if (!np[k].empty()) {
+              nnx[k] = ks.Fresh("XN");
+              ks.L("int8_t " + nnx[k] + " = kdb_p0 < (int64_t)" + n + " ? " + np[k] + "[kdb_p0] : (int8_t)0;");
+            }
+          }
+        }
         ks.Open("for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < (int64_t)" + n +
                 "; r += (int64_t)gridDim.x * blockDim.x)");
+        std::vector<std::string> cur(cols.size()), ncur(cols.size());
+        if (pf) {
+          for (size_t k = 0; k < cols.size(); k++) {
+            if (nxt[k].empty()) continue;
+            const std::string st = StoreType(cols[k]->type.id);
+            cur[k] = ks.Fresh("C");
+            ks.L("const " + st + " " + cur[k] + " = " + nxt[k] + ";");
+            if (!nnx[k].empty()) {
+              ncur[k] = ks.Fresh("CN");
+              ks.L("const int8_t " + ncur[k] + " = " + nnx[k] + ";");
+            }
+          }
+          ks.Open("if (r + kdb_pstride < (int64_t)" + n + ")");
+          for (size_t k = 0; k < cols.size(); k++) {
+            if (nxt[k].empty()) continue;
+            ks.L(nxt[k] + " = " + dp[k] + "[r + kdb_pstride];");
+            if (!nnx[k].empty()) ks.L(nnx[k] + " = " + np[k] + "[r + kdb_pstride];");
+          }
+          ks.Close();
+        }
         // With KDB_LAZY_PROBE_COLUMNS the probe side of a join reads its
         // columns where the consumer uses them (non-key columns only inside
         // the match branch).  Measured on the Q3 shape it is slower (61 vs
@@ -924,13 +964,15 @@ void Executor::EmitStream(KernelSource& ks, ExprGen& eg, const Operator& op, con
         // the probe's dependent accesses instead of overlapping them, which
         // costs more than the sectors saved, so all columns load up front.
         const bool lazy = probe_side && ctx_.OptStr("KDB_LAZY_PROBE_COLUMNS");
-        load = [&, lazy](size_t k) {
+        load = [&, lazy, cur, ncur](size_t k) {
           const DevColumn& c = *cols[k];
           std::string v;
+          const std::string raw = cur[k].empty() ? dp[k] + "[r]" : cur[k];
           if (c.type.id == TypeId::TEXT) v = "kdb_text_at(" + dp[k] + ", " + tp[k] + ", r)";
-          else if (c.type.id == TypeId::BOOLEAN) v = "(" + dp[k] + "[r] != 0)";
-          else v = dp[k] + "[r]";
-          const std::string nul = np[k].empty() ? "false" : "(" + np[k] + "[r] != 0)";
+          else if (c.type.id == TypeId::BOOLEAN) v = "(" + raw + " != 0)";
+          else v = raw;
+          const std::string nul = np[k].empty() ? "false"
+                                  : ncur[k].empty() ? "(" + np[k] + "[r] != 0)" : "(" + ncur[k] + " != 0)";
           if (lazy) scan[k] = CVal{c.type, "(" + v + ")", nul};
           else scan[k] = eg.Bind(c.type, v, nul);
         };
