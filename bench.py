@@ -415,7 +415,11 @@ def run_serving(args):
         seq_s = time.perf_counter() - t0
         res = {"one_at_a_time": {"queries_per_second": n / seq_s,
                                  "device_ms_p50_by_query": {k: statistics.median(v) for k, v in alone.items()}}}
-        for mode in ("saturated", "poisson"):
+        # all requests at once (saturated), then Poisson arrivals at the fixed
+        # rate and at 80% of the saturated throughput (near saturation)
+        for mode in ("saturated", "poisson", "poisson_near_saturation"):
+            rate = args.serving_rate if mode == "poisson" else \
+                0.8 * res.get("saturated", {}).get("queries_per_second", args.serving_rate)
             with ClockSampler(local) as clocks, Server(eng, slots=args.serving_slots,
                                                        hbm_budget_bytes=args.serving_budget_gb << 30) as srv:
                 tickets = []
@@ -424,7 +428,7 @@ def run_serving(args):
                     for _, p in seq:
                         tickets.append(srv.submit(p))
                 else:
-                    gaps = np.random.default_rng(7).exponential(1.0 / args.serving_rate, n)
+                    gaps = np.random.default_rng(7).exponential(1.0 / rate, n)
                     t_next = t0
                     for (_, p), g in zip(seq, gaps):
                         t_next += g
@@ -435,6 +439,8 @@ def run_serving(args):
                     srv.wait(t).close()
                 st = srv.stats()
                 st["wall_s"] = time.perf_counter() - t0
+                if mode != "saturated":
+                    st["arrival_rate_qps"] = rate
             st["clocks"] = clocks.summary()
             res[mode] = st
         out[policy] = res
@@ -452,10 +458,13 @@ def run_serving(args):
                    "hbm_budget_gb": args.serving_budget_gb, "poisson_rate_qps": args.serving_rate,
                    "budget_per_episode": budget, "policy": best, "l2": "inputs larger than L2 (126 MB)"},
         "p50_ms": out[best]["poisson"]["p50_ms"], "p99_ms": out[best]["poisson"]["p99_ms"],
+        "near_saturation": {k: out[best]["poisson_near_saturation"].get(k)
+                            for k in ("arrival_rate_qps", "queries_per_second", "p50_ms", "p99_ms")},
         "policies": out,
         "speedup_vs_one_at_a_time": sat["queries_per_second"] / out[best]["one_at_a_time"]["queries_per_second"],
         "prior_training": info,
-        "gpu_launches": sum(out[k][m]["kernel_launches"] for k in out for m in ("saturated", "poisson")),
+        "gpu_launches": sum(out[k][m]["kernel_launches"] for k in out
+                            for m in ("saturated", "poisson", "poisson_near_saturation")),
         "clocks": sat["clocks"],
     }
     print(json.dumps(line))
@@ -479,7 +488,7 @@ def main():
     ap.add_argument("--skinner-queries", type=int, default=8)
     ap.add_argument("--serving-requests", type=int, default=400)
     ap.add_argument("--serving-mix", default="skinner", choices=["skinner", "mixed"])
-    ap.add_argument("--serving-slots", type=int, default=4)
+    ap.add_argument("--serving-slots", type=int, default=16)
     ap.add_argument("--serving-rate", type=float, default=50.0)
     ap.add_argument("--serving-budget-gb", type=int, default=32)
     ap.add_argument("--no-cpu-baseline", action="store_true")
