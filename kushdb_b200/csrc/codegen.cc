@@ -3336,6 +3336,34 @@ class SkinnerEngine : public JoinEnv {
     return ctx_.skinner_policy == 1 && ctx_.join_prior != nullptr && T_ <= kPriorTables;
   }
 
+  // The prior's value of every (joined set, next table) pair of the join,
+  // in one forward pass (at most 8 tables: 2^7 * 8 = 1024 rows), so the
+  // search never waits on a forward pass of its own.
+  void PrecomputePrior() {
+    if (!HasPrior() || ctx_.dry) return;
+    std::vector<uint64_t> masks;
+    std::vector<int> cand;
+    const uint64_t full = (T_ >= 64) ? ~0ULL : ((1ULL << T_) - 1);
+    for (uint64_t m = 0; m < full; m++)
+      for (int t = 0; t < T_; t++)
+        if (!(m >> t & 1ULL)) {
+          masks.push_back(m);
+          cand.push_back(t);
+        }
+    std::vector<float> x(masks.size() * JoinPrior::kIn), y(masks.size());
+    for (size_t i = 0; i < masks.size(); i++) Features(masks[i], cand[i], &x[i * JoinPrior::kIn]);
+    constexpr int64_t kChunk = 4096;  // rows per forward call
+    for (size_t b = 0; b < masks.size(); b += kChunk) {
+      const int64_t rows = std::min<int64_t>(kChunk, static_cast<int64_t>(masks.size() - b));
+      ctx_.join_prior->Forward(x.data() + b * JoinPrior::kIn, rows, y.data() + b);
+    }
+    for (size_t i = 0; i < masks.size(); i++) {
+      auto& v = prior_cache_[masks[i]];
+      if (v.empty()) v.assign(T_, 0.0);
+      v[cand[i]] = y[i];
+    }
+  }
+
   void PriorValues(uint64_t joined, const std::vector<int>& cands, std::vector<double>& out) override {
     auto it = prior_cache_.find(joined);
     if (it == prior_cache_.end()) {
@@ -3494,6 +3522,7 @@ class SkinnerEngine : public JoinEnv {
         }
         batching_ = false;
       } else {
+        PrecomputePrior();
         UctNode root(0, T_, *this, prefix, seed_);
         int round = 0;
         std::vector<std::vector<std::pair<UctNode*, int>>> trails;

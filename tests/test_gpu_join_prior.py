@@ -111,7 +111,7 @@ def test_prior_needs_fewer_episodes_than_uct(engine):
     model, info = fit_prior(engine, [p for _, p in train_q], budget, seeds=(0, 1), steps=1500)
     assert info["samples"] > 1000
     assert info["last_loss"] < info["first_loss"]
-    totals = {"uct": [0, 0], "prior": [0, 0]}
+    totals = {"uct": [0, 0, 0, 0.0], "prior": [0, 0, 0, 0.0]}
     for _, plan in test_q:
         for seed in (0, 1, 2):
             for policy in ("uct", "prior"):
@@ -120,8 +120,14 @@ def test_prior_needs_fewer_episodes_than_uct(engine):
                 engine.execute(plan, fetch=False)
                 totals[policy][0] += engine.last_skinner_episodes()
                 totals[policy][1] += engine.last_skinner_work()
+                totals[policy][2] += engine.last_skinner_batches()
+                totals[policy][3] += engine.last_device_ms()
     engine.set_skinner_policy("uct")
     engine.set_skinner()
-    print("episodes / work (uct, prior):", totals)
+    print("episodes / work / batches / device ms (uct, prior):", totals)
     assert totals["prior"][0] < totals["uct"][0]
+    # the gain reaches the clock: fewer episode batches, less device time
+    # (the prior's values come from one forward pass per join)
+    assert totals["prior"][2] < totals["uct"][2]
+    assert totals["prior"][3] < totals["uct"][3]
     model.close()
