@@ -176,13 +176,16 @@ __global__ void BatchBuild(const QueryDesc* __restrict__ qs, int nq, unsigned lo
 
 // sum and first fact row per build row; kProbeUnroll rows per thread are
 // loaded and hashed together so their table reads overlap.
+// eager: the measures of the unrolled rows load with their keys, so their
+// HBM latency overlaps the probes (otherwise only matching rows load them)
 __global__ void BatchProbe(const QueryDesc* __restrict__ qs, int nq, const unsigned long long* __restrict__ slots,
-                           int fanout_bits, Acc* __restrict__ acc) {
+                           int fanout_bits, Acc* __restrict__ acc, int eager) {
   int64_t r0, r1;
   const QueryDesc& q = Chunk<1>(qs, nq, r0, r1);
   const int64_t step = blockDim.x;
   for (int64_t base = r0 + threadIdx.x; base < r1; base += kProbeUnroll * step) {
     int32_t k[kProbeUnroll];
+    double mp[kProbeUnroll], md[kProbeUnroll];
     uint32_t pos[kProbeUnroll];
     const unsigned long long* sub[kProbeUnroll];
     unsigned long long e[kProbeUnroll];
@@ -190,6 +193,8 @@ __global__ void BatchProbe(const QueryDesc* __restrict__ qs, int nq, const unsig
     for (int j = 0; j < kProbeUnroll; j++) {
       const int64_t r = base + j * step;
       k[j] = r < r1 ? __ldcs(q.f_fk + r) : 0;
+      mp[j] = eager && r < r1 ? __ldcs(q.f_price + r) : 0.0;
+      md[j] = eager && r < r1 ? __ldcs(q.f_disc + r) : 0.0;
     }
 #pragma unroll
     for (int j = 0; j < kProbeUnroll; j++) {
@@ -208,7 +213,8 @@ __global__ void BatchProbe(const QueryDesc* __restrict__ qs, int nq, const unsig
         if (static_cast<uint32_t>(s >> 32) == static_cast<uint32_t>(k[j])) {
           Acc* a = acc + q.acc_base + (static_cast<int64_t>(static_cast<uint32_t>(s)) - 1);
           // plain per-row IEEE arithmetic, like the reference's generated code
-          const double v = __dmul_rn(__ldcs(q.f_price + r), __dsub_rn(1.0, __ldcs(q.f_disc + r)));
+          const double pr = eager ? mp[j] : __ldcs(q.f_price + r), di = eager ? md[j] : __ldcs(q.f_disc + r);
+          const double v = __dmul_rn(pr, __dsub_rn(1.0, di));
           atomicAdd(&a->sum, v);
           // the first fact row only moves down: skip the atomic once an
           // earlier row is already recorded (a stale read costs one atomic)
@@ -419,7 +425,8 @@ class Batch {
     cudaMemsetAsync(out_count_, 0, sizeof(unsigned long long) * nq, s);
     cudaMemsetAsync(err_, 0, sizeof(int), s);
     BatchBuild<<<build_grid_, cfg_.block, 0, s>>>(d_qs_, nq, slots_, fanout_bits_, err_);
-    BatchProbe<<<probe_grid_, cfg_.block, 0, s>>>(d_qs_, nq, slots_, fanout_bits_, acc_);
+    BatchProbe<<<probe_grid_, cfg_.block, 0, s>>>(d_qs_, nq, slots_, fanout_bits_, acc_,
+                                                   ctx_.OptStr("KDB_BATCH_LAZY_MEASURES") ? 0 : 1);
     BatchOutput<<<out_grid_, cfg_.block, 0, s>>>(d_qs_, nq, acc_, out_key_, out_sum_, out_first_, out_count_);
     cudaGraph_t g;
     KDB_CUDA(cudaStreamEndCapture(s, &g));
