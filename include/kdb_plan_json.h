@@ -18,8 +18,10 @@
  *   std::string json = kdb_b200::ToBackendJson(root);   // root: plan::Operator
  *   kdb_query_execute(ctx, json.c_str(), &result);
  *
- * Not supported by the backend (throws std::runtime_error):
- * RegexpMatchingExpression (general LIKE with a regular expression).
+ * RegexpMatchingExpression is written with its RE2 pattern text; the
+ * backend runs the patterns the planner makes from SQL LIKE
+ * (plan/planner.cc:283-321: ^...$ over escaped bytes, "." and ".*") and
+ * rejects any other regular expression with KDB_ERR_UNSUPPORTED.
  */
 #ifndef KDB_PLAN_JSON_H_
 #define KDB_PLAN_JSON_H_
@@ -196,8 +198,9 @@ class ExprWriter : public kush::plan::ImmutableExpressionVisitor {
   void Visit(const kush::plan::ExtractExpression& e) override {
     out = "{\"e\":\"extract\",\"what\":\"YEAR\"," + Head(e) + ",\"c\":" + Of(e.Child()) + "}";
   }
-  void Visit(const kush::plan::RegexpMatchingExpression&) override {
-    throw std::runtime_error("general LIKE (regular expressions) is not supported by the B200 backend");
+  void Visit(const kush::plan::RegexpMatchingExpression& e) override {
+    out = "{\"e\":\"regex\"," + Head(e) + ",\"c\":" + Of(e.Child()) + ",\"pattern\":" +
+          Quote(e.Regex()->pattern()) + "}";
   }
   void Visit(const kush::plan::EnumInExpression& e) override {
     std::string vals;

@@ -292,6 +292,31 @@ class ExprGen {
         for (int32_t x : e.in_values) cond += " || " + c.v + " == " + std::to_string(x);
         return Bind(e.type, "!(" + c.n + ") && (" + cond + ")", "false");
       }
+      case ExprKind::Regexp: {
+        // expression_translator.cc:277-297: NULL -> false; an ENUM matches
+        // through its string
+        CVal c = Emit(e.kid(0), s);
+        const auto tok = LikeTokens(e.regex);
+        if (tok.size() > 63) throw Error(-5, "LIKE pattern of more than 63 tokens");
+        uint64_t tr[256] = {0}, star = 0;
+        for (size_t i = 0; i < tok.size(); i++) {
+          if (tok[i].first == 0) tr[tok[i].second] |= 1ULL << i;
+          else if (tok[i].first == 1) {
+            for (int b = 0; b < 256; b++)
+              if (b != '\n') tr[b] |= 1ULL << i;
+          } else {
+            star |= 1ULL << i;
+          }
+        }
+        const std::string name = "kdb_like_tr" + std::to_string(ks_.lits++);
+        ks_.globals << "__device__ const unsigned long long " << name << "[256] = {";
+        for (int b = 0; b < 256; b++) ks_.globals << tr[b] << "ULL,";
+        ks_.globals << "};\n";
+        const std::string str = c.type.id == TypeId::ENUM ? EnumString(c.type, c.v) : c.v;
+        return Bind(e.type, "!(" + c.n + ") && kdb_like(" + str + ", " + name + ", " + std::to_string(star) + "ULL, " +
+                                std::to_string(tok.size()) + ")",
+                    "false");
+      }
       case ExprKind::Agg: throw Error(-1, "Aggregate expression can't be derived");
       case ExprKind::Binary: break;
     }
@@ -1846,7 +1871,7 @@ std::string ExprSig(const Expr& e) {
     << e.sval.size() << "'" << e.sval << "'(";
   for (const auto& k : e.kids) o << ExprSig(*k) << ";";
   for (int32_t v : e.in_values) o << v << ",";
-  o << ")";
+  o << ")" << e.regex.size() << "'" << e.regex << "'";
   return o.str();
 }
 

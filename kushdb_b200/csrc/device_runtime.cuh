@@ -90,6 +90,30 @@ KDB_DEV bool kdb_str_ends_with(kdb_str a, kdb_str b) {
 // Substring search (string_view::find != npos).  Checks the first byte
 // before comparing the rest; the LIKE '%tok%' predicates it serves use
 // short needles.
+// Full match of a LIKE pattern as a bit-parallel NFA: state i = the first i
+// pattern tokens matched (at most 63 tokens).  tr[c] has bit i when token i
+// consumes byte c (a literal c, or '_' for any byte but '\n'); star has the
+// bits of the '%' tokens, which consume any run of bytes but '\n' and may
+// also match nothing.
+KDB_DEV uint64_t kdb_like_close(uint64_t d, uint64_t star) {
+  for (int k = 0; k < 64; k++) {
+    const uint64_t nd = d | ((d & star) << 1);
+    if (nd == d) break;
+    d = nd;
+  }
+  return d;
+}
+KDB_DEV bool kdb_like(kdb_str s, const unsigned long long* tr, unsigned long long star, int n) {
+  uint64_t d = kdb_like_close(1ULL, star);
+  for (int32_t i = 0; i < s.len && d; i++) {
+    const unsigned char c = (unsigned char)s.p[i];
+    uint64_t nd = (d & tr[c]) << 1;
+    if (c != '\n') nd |= d & star;
+    d = kdb_like_close(nd, star);
+  }
+  return (d >> n) & 1ULL;
+}
+
 KDB_DEV bool kdb_str_contains(kdb_str a, kdb_str b) {
   if (b.len == 0) return true;
   if (b.len > a.len) return false;

@@ -10,6 +10,7 @@
 #include <memory>
 #include <stdexcept>
 #include <string>
+#include <utility>
 #include <vector>
 
 #include "json.h"
@@ -76,7 +77,7 @@ enum class UnOp { NOT, IS_NULL };
 // plan::AggregateType (plan/expression/aggregate_expression.h)
 enum class AggType { SUM, MIN, MAX, AVG, COUNT };
 
-enum class ExprKind { ColRef, VirtColRef, Literal, Binary, Unary, Agg, Case, IntToFloat, Extract, EnumIn };
+enum class ExprKind { ColRef, VirtColRef, Literal, Binary, Unary, Agg, Case, IntToFloat, Extract, EnumIn, Regexp };
 
 struct Expr {
   ExprKind kind = ExprKind::Literal;
@@ -95,6 +96,7 @@ struct Expr {
   AggType agg = AggType::SUM;
   std::vector<std::unique_ptr<Expr>> kids;  // binary: l, r; unary/agg/i2f/extract/in: c; case: c, t, f
   std::vector<int32_t> in_values;           // EnumInExpression
+  std::string regex;                        // RegexpMatchingExpression (a LIKE pattern's regex)
 
   const Expr& kid(size_t i) const { return *kids.at(i); }
 };
@@ -159,6 +161,36 @@ inline AggType ParseAgg(const std::string& s) {
   throw std::runtime_error("unknown aggregate " + s);
 }
 
+// The regex the reference's planner makes of a general LIKE pattern
+// (plan/planner.cc:283-323): '^', then per pattern byte an escaped literal,
+// '.' for '_' or ".*" for '%', then '$'.  Tokens: {0, byte} a literal,
+// {1, 0} any one byte but '\n', {2, 0} any run of such bytes (RE2's '.'
+// does not match a newline).  Anything else is not a LIKE regex.
+inline std::vector<std::pair<int, unsigned char>> LikeTokens(const std::string& re) {
+  if (re.size() < 2 || re.front() != '^' || re.back() != '$')
+    throw std::runtime_error("unsupported regex (not a LIKE pattern): " + re);
+  std::vector<std::pair<int, unsigned char>> t;
+  for (size_t i = 1; i + 1 < re.size(); i++) {
+    const char c = re[i];
+    if (c == '\\') {
+      if (i + 2 >= re.size()) throw std::runtime_error("dangling escape in regex " + re);
+      t.emplace_back(0, static_cast<unsigned char>(re[++i]));
+    } else if (c == '.') {
+      if (i + 2 < re.size() && re[i + 1] == '*') {
+        t.emplace_back(2, 0);
+        i++;
+      } else {
+        t.emplace_back(1, 0);
+      }
+    } else if (std::string(".+*?^$()[]{}|").find(c) != std::string::npos) {
+      throw std::runtime_error("unsupported regex (not a LIKE pattern): " + re);
+    } else {
+      t.emplace_back(0, static_cast<unsigned char>(c));
+    }
+  }
+  return t;
+}
+
 inline std::unique_ptr<Expr> ParseExpr(const json::Value& j) {
   auto e = std::make_unique<Expr>();
   const std::string& k = j.at("e").str();
@@ -209,6 +241,12 @@ inline std::unique_ptr<Expr> ParseExpr(const json::Value& j) {
   } else if (k == "extract") {
     e->kind = ExprKind::Extract;
     if (j.at("what").str() != "YEAR") throw std::runtime_error("only EXTRACT(YEAR)");
+    e->kids.push_back(ParseExpr(j.at("c")));
+  } else if (k == "regex") {
+    // RegexpMatchingExpression: the planner's regex of a general LIKE
+    // pattern (plan/planner.cc:283-323), fully matched
+    e->kind = ExprKind::Regexp;
+    e->regex = j.at("pattern").str();
     e->kids.push_back(ParseExpr(j.at("c")));
   } else if (k == "enum_in") {
     e->kind = ExprKind::EnumIn;

@@ -13,7 +13,7 @@ reference's own tests:
   ``LiteralExpression``, ``BinaryArithmeticExpression``,
   ``UnaryArithmeticExpression``, ``AggregateExpression``, ``CaseExpression``,
   ``IntToFloatConversionExpression``, ``ExtractExpression``,
-  ``EnumInExpression``                                (plan/expression/*.h)
+  ``EnumInExpression``, ``RegexpMatchingExpression`` (plan/expression/*.h)
 * the builder DSL ``ColRef``, ``VirtColRef``, ``Literal``, ``Eq`` ... ``Count``
                                                        (util/builder.h:33-300)
 
@@ -442,6 +442,25 @@ class EnumInExpression(Expression):
                 "c": self.child.to_dict(), "values": self.values}
 
 
+class RegexpMatchingExpression(Expression):
+    """SQL LIKE as the planner hands it over: an RE2 full-match pattern
+    ``^...$`` (plan/expression/arithmetic_expression.h:69-83; the pattern
+    text is ``RE2::pattern()``).  Only the planner's LIKE translation is
+    accepted: escaped bytes, ``.`` (any byte but newline) and ``.*``.
+    Never NULL; a NULL child is false (expression_translator.cc:277-297)."""
+
+    def __init__(self, child: Expression, regex: str):
+        if child.type.type_id not in ("TEXT", "ENUM"):
+            raise TypeError("Invalid child type for LIKE. Expected text/enum.")
+        super().__init__(Type.Boolean(), False)
+        self.child = child
+        self.regex = regex
+
+    def to_dict(self):
+        return {"e": "regex", "type": "BOOLEAN", "nullable": False,
+                "c": self.child.to_dict(), "pattern": self.regex}
+
+
 # ----------------------------------------------------------------------------
 # OperatorSchema (plan/operator/operator_schema.cc)
 # ----------------------------------------------------------------------------
@@ -803,6 +822,32 @@ def EndsWith(e1, e2):
 
 def Contains(e1, e2):
     return BinaryArithmeticExpression("CONTAINS", e1, e2)
+
+
+_REGEX_SPECIAL = set(".+*?^$()[]{}|\\")
+
+
+def LikeRegex(pattern: str) -> str:
+    """The planner's LIKE -> RE2 translation (plan/planner.cc:283-318):
+    ``_`` -> ``.``, ``%`` -> ``.*``, regex metacharacters escaped, anchored
+    with ``^...$``."""
+    out = ["^"]
+    for c in pattern:
+        if c in _REGEX_SPECIAL:
+            out.append("\\" + c)
+        elif c == "_":
+            out.append(".")
+        elif c == "%":
+            out.append(".*")
+        else:
+            out.append(c)
+    out.append("$")
+    return "".join(out)
+
+
+def Like(e, pattern: str):
+    """``e LIKE pattern`` in its general (regex) form."""
+    return RegexpMatchingExpression(e, LikeRegex(pattern))
 
 
 def And(exprs: Sequence[Expression]):

@@ -125,6 +125,29 @@ class Executor {
     }
   }
 
+  // Full match of LIKE tokens (literal byte / any byte but '\n' / any run of
+  // bytes without '\n') by dynamic programming over (token, position).
+  static bool LikeMatch(const std::vector<std::pair<int, unsigned char>>& tok, std::string_view s) {
+    const size_t n = tok.size(), m = s.size();
+    // ok[j] = tokens [i, n) match s[j, m)
+    std::vector<char> ok(m + 1, 0), next(m + 1, 0);
+    ok[m] = 1;
+    for (size_t i = n; i-- > 0;) {
+      std::fill(next.begin(), next.end(), 0);
+      for (size_t j = m + 1; j-- > 0;) {
+        const int kind = tok[i].first;
+        if (kind == 2) {
+          next[j] = ok[j] || (j < m && s[j] != '\n' && next[j + 1]);
+        } else if (j < m) {
+          const bool hit = kind == 1 ? s[j] != '\n' : (unsigned char)s[j] == tok[i].second;
+          next[j] = hit && ok[j + 1];
+        }
+      }
+      ok.swap(next);
+    }
+    return ok[0];
+  }
+
   Val Eval(const Expr& e, const EvalEnv& env) const {
     switch (e.kind) {
       case ExprKind::ColRef: {
@@ -176,6 +199,16 @@ class Executor {
         for (int32_t x : e.in_values)
           if (x == c.i) return Bool(true);
         return Bool(false);
+      }
+      case ExprKind::Regexp: {
+        // RE2::FullMatch of the planner's ^...$ pattern
+        // (expression_translator.cc:277-297, planner.cc:283-321): NULL ->
+        // false; an ENUM matches through its string
+        Val c = Eval(e.kid(0), env);
+        if (c.null) return Bool(false);
+        const Type& ct = e.kid(0).type;
+        std::string_view s = ct.id == TypeId::ENUM ? EnumStr(ct.enum_id, c.i) : std::string_view(c.s);
+        return Bool(LikeMatch(LikeTokens(e.regex), s));
       }
       case ExprKind::Agg:
         throw std::runtime_error("Aggregate expression can't be derived");

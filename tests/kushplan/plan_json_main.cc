@@ -216,7 +216,7 @@ std::string Skinner(const catalog::Database& db) {
   return kdb_b200::ToBackendJson(root);
 }
 
-// SELECT over a scan with CASE, EXTRACT, enum IN, IS NULL and NOT
+// SELECT over a scan with CASE, EXTRACT, enum IN, IS NULL, NOT and LIKE
 std::string Misc(const catalog::Database& db) {
   const auto& rel = db["misc"];
   OperatorSchema ss;
@@ -233,6 +233,9 @@ std::string Misc(const catalog::Database& db) {
                                                              std::make_unique<IntToFloatConversionExpression>(
                                                                  ColRef(*scan, "n")),
                                                              Lit(-1.25)));
+  // LIKE '%(B)%_N%' on an enum, as the planner writes it
+  out.AddDerivedColumn("m", std::make_unique<RegexpMatchingExpression>(
+                                ColRef(*scan, "c"), std::make_unique<re2::RE2>("^.*\\(B\\).*.N.*$")));
   OutputOperator root(std::make_unique<SelectOperator>(std::move(out), std::move(scan), std::move(cond)));
   return kdb_b200::ToBackendJson(root);
 }

@@ -19,6 +19,18 @@
 #include <variant>
 #include <vector>
 
+namespace re2 {
+// Stand-in for re2::RE2: only the pattern text the serialiser reads.
+class RE2 {
+ public:
+  explicit RE2(std::string pattern) : pattern_(std::move(pattern)) {}
+  const std::string& pattern() const { return pattern_; }
+
+ private:
+  std::string pattern_;
+};
+}  // namespace re2
+
 namespace kush::catalog {
 
 enum class TypeId { SMALLINT, INT, BIGINT, REAL, DATE, TEXT, BOOLEAN, ENUM };
@@ -370,11 +382,13 @@ class ExtractExpression : public UnaryExpression {
 
 class RegexpMatchingExpression : public UnaryExpression {
  public:
-  explicit RegexpMatchingExpression(std::unique_ptr<Expression> child)
-      : UnaryExpression(catalog::Type::Boolean(), false, std::move(child)) {
-    SetType(catalog::Type::Boolean(), Child().Nullable());
-  }
+  RegexpMatchingExpression(std::unique_ptr<Expression> child, std::unique_ptr<re2::RE2> regexp)
+      : UnaryExpression(catalog::Type::Boolean(), false, std::move(child)), regexp_(std::move(regexp)) {}
   void Accept(ImmutableExpressionVisitor& v) const override { v.Visit(*this); }
+  re2::RE2* Regex() const { return regexp_.get(); }
+
+ private:
+  std::unique_ptr<re2::RE2> regexp_;
 };
 
 class EnumInExpression : public UnaryExpression {

@@ -1,15 +1,16 @@
 """GPU parity, against the CPU oracle, of the expression forms beyond the
 benchmark shapes: EXTRACT(YEAR FROM date) (runtime/date.cc:46-50) as a
 projection and as a group key, enum IN lists (plan/expression/
-enum_in_expression.h), and STARTS_WITH / ENDS_WITH / CONTAINS on TEXT
-(runtime/string.cc:14-40), with NULL inputs."""
+enum_in_expression.h), STARTS_WITH / ENDS_WITH / CONTAINS on TEXT
+(runtime/string.cc:14-40) and general LIKE (RegexpMatchingExpression, the
+planner's ^...$ pattern) on TEXT and ENUM, with NULL inputs."""
 
 import numpy as np
 import pytest
 
 from kushdb_b200.data import HostColumn, HostTable, catalog_of
 from kushdb_b200.plan import (ColRef, Contains, Count, EndsWith, EnumRegistry, Extract, GroupByAggregateOperator,
-                              In, Literal, Max, Min, Not, OperatorSchema, Or, OutputOperator, ScanOperator,
+                              In, Like, Literal, Max, Min, Not, OperatorSchema, Or, OutputOperator, ScanOperator,
                               ScanSelectOperator, StartsWith, Sum, Type, VirtColRef, EPOCH_JDN)
 from parity import compare
 
@@ -61,6 +62,11 @@ def _select(t, filters, out_cols):
     ("not_starts_with", lambda s: Not(StartsWith(VirtColRef(s, "s"), Literal("p")))),
     ("enum_in", lambda s: In(VirtColRef(s, "c"), ["red", "cyan", "black"])),
     ("enum_in_or_text", lambda s: Or([In(VirtColRef(s, "c"), ["green"]), EndsWith(VirtColRef(s, "s"), Literal("on"))])),
+    ("like_inner", lambda s: Like(VirtColRef(s, "s"), "%p_e%")),
+    ("like_anchored", lambda s: Like(VirtColRef(s, "s"), "a%e")),
+    ("like_repeat", lambda s: Like(VirtColRef(s, "s"), "%a%a%a%")),
+    ("like_enum", lambda s: Like(VirtColRef(s, "c"), "%e_")),
+    ("not_like", lambda s: Not(Like(VirtColRef(s, "s"), "%l%m%"))),
 ])
 def test_text_and_enum_filters_match_oracle(setup, name, make):
     t, e, o = setup
@@ -153,3 +159,31 @@ def test_cross_product_under_select_and_group_by(setup):
     # the pairs themselves, as a multiset
     flat = OutputOperator(CrossProductOperator(cs, [lsel, rscan]))
     assert compare(e.execute(flat), o.execute(flat), ordered=False) == ""
+
+
+@pytest.mark.parametrize("pattern", ["%", "", "a%", "%a%b%", "a_b", "%.%", "%(%", "%\n%", "_%_", "ab.c",
+                                     "%xy%xy%", "_" * 6, "%" + "_%" * 30])
+def test_like_random_strings(setup, pattern):
+    """Short random strings over the pattern's own metacharacters and '\n'
+    (which '_' and '%' do not match), 10% NULL."""
+    import zlib
+    from oracle import Oracle
+    _, e, _ = setup
+    o = Oracle()
+    rng = np.random.default_rng(len(pattern))
+    alphabet = list("ab.c%_(\n") + ["xy"]
+    n = 50_000
+    strings = ["".join(alphabet[int(i)] for i in rng.integers(0, len(alphabet), int(k)))
+               for k in rng.integers(0, 8, n)]
+    t = HostTable(f"like_rand_{zlib.crc32(pattern.encode())}")
+    t.add(HostColumn.from_strings("s", strings, nulls=(rng.random(n) < 0.1).astype(np.int8)))
+    e.register_table(t)
+    o.register_table(t)
+    rel = catalog_of([t])[t.name]
+    scan = OperatorSchema()
+    scan.AddGeneratedColumns(rel, ["s"])
+    out = OperatorSchema()
+    out.AddVirtualPassthroughColumns(scan, ["s"])
+    plan = OutputOperator(ScanSelectOperator(out, scan, rel, [Like(VirtColRef(scan, "s"), pattern)]))
+    assert compare(e.execute(plan), o.execute(plan), ordered=False) == ""
+    o.close()

@@ -16,7 +16,7 @@ import pytest
 
 from kushdb_b200 import workloads as wl
 from kushdb_b200.data import HostColumn, HostTable, catalog_of
-from kushdb_b200.plan import (CaseExpression, ColRef, EnumInExpression, ExtractExpression, Float, Gt,
+from kushdb_b200.plan import (CaseExpression, ColRef, EnumInExpression, ExtractExpression, Float, Gt, Like,
                               IntToFloatConversionExpression, Literal, OperatorSchema, OutputOperator, Or,
                               ScanOperator, SelectOperator, Type, UnaryArithmeticExpression)
 
@@ -86,6 +86,7 @@ def _misc_plan(misc):
     out.AddDerivedColumn("y", ExtractExpression(ColRef(scan, "d")))
     out.AddDerivedColumn("w", CaseExpression(Gt(ColRef(scan, "v"), Literal(0.5)),
                                              IntToFloatConversionExpression(ColRef(scan, "n")), Literal(-1.25)))
+    out.AddDerivedColumn("m", Like(ColRef(scan, "c"), "%(B)%_N%"))
     return OutputOperator(SelectOperator(out, scan, cond))
 
 
