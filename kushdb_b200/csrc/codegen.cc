@@ -752,6 +752,28 @@ class Executor {
   // column loads, bound such a pipeline, and the 4-row vector's registers
   // cost occupancy)
   bool probe_side_scan_ = false;
+  // Probe-ahead: set by a join whose probe side is a plain scan of its key
+  // column; that scan then loads the key two rows ahead and, one row ahead,
+  // the row's join-filter word and first table slot, so the probe of a row
+  // starts with its dependent table reads already done (KDB_NO_PROBE_AHEAD:
+  // off).  ahead_jt_/ahead_out_col_ go from the join to its scan; the
+  // ahead_* names come back from the scan to EmitProbe.
+  const JoinTable* ahead_jt_ = nullptr;
+  int ahead_out_col_ = -1;
+  const JoinTable* ahead_probe_jt_ = nullptr;
+  std::string ahead_key_var_, ahead_word_, ahead_slot_;
+  void SetProbeAhead(const Operator& join, const JoinTable& jt) {
+    ahead_jt_ = nullptr;
+    ahead_out_col_ = -1;
+    if (ctx_.OptStr("KDB_NO_PROBE_AHEAD") || ctx_.OptStr("KDB_NO_PROBE_PREFETCH") ||
+        ctx_.OptStr("KDB_LAZY_PROBE_COLUMNS") || join.right_keys.size() != 1)
+      return;
+    const Expr& k = *join.right_keys[0];
+    const OpKind ck = join.child(1).kind;
+    if (k.kind != ExprKind::ColRef || k.child_idx != 1 || (ck != OpKind::SCAN && ck != OpKind::SCAN_SELECT)) return;
+    ahead_jt_ = &jt;
+    ahead_out_col_ = k.column_idx;
+  }
   void EmitProbe(KernelSource& ks, ExprGen& eg, const JoinTable& jt,
                  const std::vector<int>& build_key_cols, const std::vector<CVal>& probe_keys,
                  const std::function<void(const std::vector<CVal>&, const std::string&)>& on_match);
@@ -946,6 +968,31 @@ void Executor::EmitStream(KernelSource& ks, ExprGen& eg, const Operator& op, con
         // probe's dependent L2 accesses (KDB_NO_PROBE_PREFETCH: off).
         const bool pf = probe_side && !ctx_.OptStr("KDB_NO_PROBE_PREFETCH") && !ctx_.OptStr("KDB_LAZY_PROBE_COLUMNS");
         std::vector<std::string> nxt(cols.size()), nnx(cols.size());
+        // probe-ahead: the scan column that is the join's probe key
+        const JoinTable* ajt = ahead_jt_;
+        ahead_jt_ = nullptr;
+        int ak = -1;
+        if (pf && ajt && ahead_out_col_ >= 0 && ahead_out_col_ < static_cast<int>(op.output.size())) {
+          const Expr& oe = *op.output[ahead_out_col_].expr;
+          const bool direct = (oe.kind == ExprKind::ColRef && oe.child_idx == 0) || oe.kind == ExprKind::VirtColRef;
+          if (direct && oe.column_idx >= 0 && oe.column_idx < static_cast<int>(cols.size())) {
+            const TypeId t = cols[oe.column_idx]->type.id;
+            if (t == TypeId::INT || t == TypeId::DATE || t == TypeId::ENUM || t == TypeId::SMALLINT ||
+                t == TypeId::BIGINT)
+              ak = oe.column_idx;
+          }
+        }
+        std::string a_key2, a_word, a_slot, a_slots, a_bloom;
+        auto ahead_loads = [&](const std::string& key) {
+          // the join-filter word and the first table slot of the row whose
+          // probe key is `key` (indexes masked: always in bounds)
+          const std::string h = ks.Fresh("AH");
+          ks.L("const uint32_t " + h + " = " + JoinHash(eg, {CVal{cols[ak]->type, key, "false"}}) + ";");
+          if (ajt->bloom)
+            ks.L(a_word + " = __ldg(&" + a_bloom + "[kdb_bloom_bit(" + h + ", " + std::to_string(ajt->bloom_log2) +
+                 ") >> 5]);");
+          ks.L(a_slot + " = " + a_slots + "[" + h + " & (uint32_t)" + ks.Word(ajt->mask) + "];");
+        };
         if (pf) {
           ks.L("const int64_t kdb_pstride = (int64_t)gridDim.x * blockDim.x;");
           ks.L("const int64_t kdb_p0 = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;");
@@ -958,6 +1005,21 @@ void Executor::EmitStream(KernelSource& ks, ExprGen& eg, const Operator& op, con
               nnx[k] = ks.Fresh("XN");
               ks.L("int8_t " + nnx[k] + " = kdb_p0 < (int64_t)" + n + " ? " + np[k] + "[kdb_p0] : (int8_t)0;");
             }
+          }
+          if (ak >= 0) {
+            const std::string st = StoreType(cols[ak]->type.id);
+            a_key2 = ks.Fresh("XA");
+            ks.L(st + " " + a_key2 + " = kdb_p0 + kdb_pstride < (int64_t)" + n + " ? " + dp[ak] +
+                 "[kdb_p0 + kdb_pstride] : (" + st + ")0;");
+            a_slots = ks.Ptr(ajt->slots, "uint64_t", true);
+            if (ajt->bloom) a_bloom = ks.Ptr(ajt->bloom, "uint32_t", true);
+            a_word = ks.Fresh("AW");
+            a_slot = ks.Fresh("AS");
+            ks.L("uint32_t " + a_word + " = 0;");
+            ks.L("uint64_t " + a_slot + " = 0;");
+            ks.Open("if (kdb_p0 < (int64_t)" + n + ")");
+            ahead_loads(nxt[ak]);
+            ks.Close();
           }
         }
         ks.Open("for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < (int64_t)" + n +
@@ -974,13 +1036,30 @@ void Executor::EmitStream(KernelSource& ks, ExprGen& eg, const Operator& op, con
               ks.L("const int8_t " + ncur[k] + " = " + nnx[k] + ";");
             }
           }
+          std::string cword, cslot;
+          if (ak >= 0) {
+            cword = ks.Fresh("CW");
+            cslot = ks.Fresh("CS");
+            ks.L("const uint32_t " + cword + " = " + a_word + ";");
+            ks.L("const uint64_t " + cslot + " = " + a_slot + ";");
+          }
           ks.Open("if (r + kdb_pstride < (int64_t)" + n + ")");
           for (size_t k = 0; k < cols.size(); k++) {
             if (nxt[k].empty()) continue;
-            ks.L(nxt[k] + " = " + dp[k] + "[r + kdb_pstride];");
+            if (static_cast<int>(k) == ak) ks.L(nxt[k] + " = " + a_key2 + ";");
+            else ks.L(nxt[k] + " = " + dp[k] + "[r + kdb_pstride];");
             if (!nnx[k].empty()) ks.L(nnx[k] + " = " + np[k] + "[r + kdb_pstride];");
           }
+          if (ak >= 0) {
+            ahead_loads(nxt[ak]);
+            ks.L("if (r + 2 * kdb_pstride < (int64_t)" + n + ") " + a_key2 + " = " + dp[ak] + "[r + 2 * kdb_pstride];");
+          }
           ks.Close();
+          if (ak >= 0) {
+            ahead_probe_jt_ = ajt;
+            ahead_word_ = cword;
+            ahead_slot_ = cslot;
+          }
         }
         // With KDB_LAZY_PROBE_COLUMNS the probe side of a join reads its
         // columns where the consumer uses them (non-key columns only inside
@@ -989,7 +1068,7 @@ void Executor::EmitStream(KernelSource& ks, ExprGen& eg, const Operator& op, con
         // the probe's dependent accesses instead of overlapping them, which
         // costs more than the sectors saved, so all columns load up front.
         const bool lazy = probe_side && ctx_.OptStr("KDB_LAZY_PROBE_COLUMNS");
-        load = [&, lazy, cur, ncur](size_t k) {
+        load = [&, lazy, cur, ncur, ak](size_t k) {
           const DevColumn& c = *cols[k];
           std::string v;
           const std::string raw = cur[k].empty() ? dp[k] + "[r]" : cur[k];
@@ -1000,6 +1079,7 @@ void Executor::EmitStream(KernelSource& ks, ExprGen& eg, const Operator& op, con
                                   : ncur[k].empty() ? "(" + np[k] + "[r] != 0)" : "(" + ncur[k] + " != 0)";
           if (lazy) scan[k] = CVal{c.type, "(" + v + ")", nul};
           else scan[k] = eg.Bind(c.type, v, nul);
+          if (static_cast<int>(k) == ak) ahead_key_var_ = scan[k].v;
         };
       }
       auto close_loop = [&]() {
@@ -1075,9 +1155,12 @@ void Executor::EmitStream(KernelSource& ks, ExprGen& eg, const Operator& op, con
         });
       };
       probe_side_scan_ = !ctx_.OptStr("KDB_VECTOR_PROBE_SCAN");
+      if (probe_side_scan_) SetProbeAhead(op, jt);
       if (Streamable(op.child(1))) EmitStream(ks, eg, op.child(1), body, src_rows);
       else EmitMatScan(ks, mats_.at(&op.child(1)), nullptr, body, src_rows);
       probe_side_scan_ = false;
+      ahead_jt_ = nullptr;
+      ahead_probe_jt_ = nullptr;
       return;
     }
     case OpKind::CROSS_PRODUCT: {
@@ -1142,14 +1225,23 @@ void Executor::EmitProbe(KernelSource& ks, ExprGen& eg, const JoinTable& jt,
   ks.L("uint32_t " + h + " = " + JoinHash(eg, pk) + ";");
   std::string slots = ks.Ptr(jt.slots, "uint64_t", true);
   std::string mask = "(uint32_t)" + ks.Word(jt.mask);
-  if (jt.bloom)
-    ks.Open("if (kdb_bloom_test(" + ks.Ptr(jt.bloom, "uint32_t", true) + ", " + h + ", " +
-            std::to_string(jt.bloom_log2) + "))");
+  // the probe-side scan loaded this row's filter word and first slot ahead
+  const bool ahead = ahead_probe_jt_ == &jt && pk.size() == 1 && pk[0].v == ahead_key_var_;
+  if (ahead) ahead_probe_jt_ = nullptr;
+  if (jt.bloom) {
+    if (ahead)
+      ks.Open("if ((" + ahead_word_ + " >> (kdb_bloom_bit(" + h + ", " + std::to_string(jt.bloom_log2) +
+              ") & 31)) & 1u)");
+    else
+      ks.Open("if (kdb_bloom_test(" + ks.Ptr(jt.bloom, "uint32_t", true) + ", " + h + ", " +
+              std::to_string(jt.bloom_log2) + "))");
+  }
   std::string i = ks.Fresh("i"), k = ks.Fresh("k"), e = ks.Fresh("e");
   ks.L("uint32_t " + i + " = " + h + " & " + mask + ";");
   ks.Open("for (uint32_t " + k + " = 0; " + k + " <= " + mask + "; " + k + "++, " + i + " = (" + i +
           " + 1) & " + mask + ")");
-  ks.L("uint64_t " + e + " = " + slots + "[" + i + "];");
+  if (ahead) ks.L("uint64_t " + e + " = " + k + " == 0 ? " + ahead_slot_ + " : " + slots + "[" + i + "];");
+  else ks.L("uint64_t " + e + " = " + slots + "[" + i + "];");
   ks.L("if (" + e + " == 0) break;");
   std::string br = ks.Fresh("br");
   std::vector<CVal> left;
@@ -2355,9 +2447,12 @@ MatBuffer Executor::RunGroupByBuildRows(const Operator& op, const std::vector<Ag
       });
     };
     probe_side_scan_ = !ctx_.OptStr("KDB_VECTOR_PROBE_SCAN");
+    if (probe_side_scan_) SetProbeAhead(join, jt);
     if (Streamable(join.child(1))) EmitStream(ks, eg, join.child(1), body, src_rows);
     else EmitMatScan(ks, mats_.at(&join.child(1)), nullptr, body, src_rows);
     probe_side_scan_ = false;
+    ahead_jt_ = nullptr;
+    ahead_probe_jt_ = nullptr;
     LaunchPipeline(ks, src_rows, "group by");
   }
   ctx_.CheckDeviceError("group by");
@@ -2827,11 +2922,14 @@ MatBuffer Executor::SmallOrderBy(const Operator& op, MatBuffer& m) {
   return MaterializeStream(op, idx, &m);
 }
 
-// (key, tie) order of 16-byte items: a sample sort, or the block sort plus
-// merge passes (KDB_ORDER_MERGE, or when the sample sort's buckets came out
-// too large)
+// (key, tie) order of 16-byte items: the block sort plus merge passes, or
+// with KDB_ORDER_SAMPLE a sample sort (splitters from a sorted sample,
+// bucket scatter, one shared-memory sort per bucket; it falls back to the
+// merge passes when a bucket comes out too large).  On the 134k-item ORDER
+// BY of the Q3-shape query the merge passes take 0.10 ms and the sample
+// sort 0.14 ms, so the merge passes are the default.
 void Executor::SortItems(uint64_t* items, int64_t n) {
-  if (!ctx_.OptStr("KDB_ORDER_MERGE") && ctx_.SampleSortItems(items, n, arena_)) return;
+  if (ctx_.OptStr("KDB_ORDER_SAMPLE") && ctx_.SampleSortItems(items, n, arena_)) return;
   ctx_.MergeSortItems(items, n, arena_);
 }
 

@@ -51,6 +51,7 @@ constexpr int kProbeTile = 2048;                 // probe tuples per bulk-copied
 constexpr uint32_t kWaitLimit = 1u << 24;        // bounded mbarrier waits
 constexpr int kErrWait = 1;                      // device error word: a wait gave up
 constexpr int kErrFull = 2;                      // a table ran out of empty slots
+constexpr unsigned kOutStage = 2048;             // pairs a CTA stages before one global append
 
 // ---- keys --------------------------------------------------------------------
 struct KeyCol {
@@ -358,43 +359,93 @@ __global__ void __launch_bounds__(kBlock) BuildParts(const typename Slot<WIDE>::
 }
 
 // ---- probe -------------------------------------------------------------------
-// Appends one (probe row, build row) pair through a warp-aggregated counter.
+// Output pairs go through a per-CTA shared-memory stage: a match takes a
+// stage position (one shared-memory atomic per coalesced group) and the CTA
+// appends the whole stage to the output with one global atomic.  A match
+// that finds the stage full is appended on its own.
+struct OutStage {
+  unsigned long long buf[kOutStage];
+  unsigned count;  // may pass kOutStage; positions from kOutStage on went direct
+  unsigned long long base;
+};
+
+__device__ __forceinline__ unsigned long long PackPair(int64_t probe_row, int64_t build_row) {
+  return (static_cast<unsigned long long>(probe_row) << 32) | static_cast<uint32_t>(build_row);
+}
+
+// Appends one pair straight to the output through a warp-aggregated counter.
 __device__ __forceinline__ void EmitPair(unsigned long long* out, unsigned long long cap,
-                                         unsigned long long* counter, int64_t probe_row, int64_t build_row) {
+                                         unsigned long long* counter, unsigned long long v) {
   cg::coalesced_group g = cg::coalesced_threads();
   unsigned long long base = 0;
   if (g.thread_rank() == 0) base = atomicAdd(counter, static_cast<unsigned long long>(g.size()));
   base = g.shfl(base, 0) + g.thread_rank();
-  if (base < cap)
-    out[base] = (static_cast<unsigned long long>(probe_row) << 32) | static_cast<uint32_t>(build_row);
+  if (base < cap) out[base] = v;
+}
+
+__device__ __forceinline__ void StagePair(OutStage& st, unsigned long long* out, unsigned long long cap,
+                                          unsigned long long* counter, unsigned long long v) {
+  cg::coalesced_group g = cg::coalesced_threads();
+  unsigned at = 0;
+  if (g.thread_rank() == 0) at = atomicAdd(&st.count, g.size());
+  at = g.shfl(at, 0) + g.thread_rank();
+  if (at < kOutStage) st.buf[at] = v;
+  else EmitPair(out, cap, counter, v);
+}
+
+// Every thread of the CTA calls it: the staged pairs are appended with one
+// global atomic and the stage is emptied.
+__device__ __forceinline__ void FlushPairs(OutStage& st, unsigned long long* out, unsigned long long cap,
+                                           unsigned long long* counter) {
+  __syncthreads();
+  const unsigned n = st.count < kOutStage ? st.count : kOutStage;
+  if (n > 0) {
+    if (threadIdx.x == 0) st.base = atomicAdd(counter, static_cast<unsigned long long>(n));
+    __syncthreads();
+    const unsigned long long base = st.base;
+    for (unsigned i = threadIdx.x; i < n; i += blockDim.x)
+      if (base + i < cap) out[base + i] = st.buf[i];
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) st.count = 0;
+  __syncthreads();
 }
 
 template <bool WIDE>
 __device__ __forceinline__ void ProbeOne(const typename Slot<WIDE>::T* tab, uint64_t cap, int64_t k,
-                                         int64_t probe_row, unsigned long long* out, unsigned long long out_cap,
-                                         unsigned long long* counter) {
+                                         int64_t probe_row, OutStage& st, unsigned long long* out,
+                                         unsigned long long out_cap, unsigned long long* counter) {
   using S = Slot<WIDE>;
   uint64_t i = Hash32(static_cast<uint64_t>(k)) & (cap - 1);
   for (uint64_t step = 0; step < cap; step++) {
     const typename S::T s = tab[i];
     if (S::Empty(s)) return;
-    if (S::Key(s) == k) EmitPair(out, out_cap, counter, probe_row, S::Row(s));
+    if (S::Key(s) == k) StagePair(st, out, out_cap, counter, PackPair(probe_row, S::Row(s)));
     i = (i + 1) & (cap - 1);
   }
 }
 
-// One table: every selected probe row looks its key up directly.
+// One table: every selected probe row looks its key up directly; the CTA
+// appends its staged pairs whenever the stage is half full.
 template <bool WIDE>
-__global__ void ProbeFlat(KeyCol key, const int32_t* __restrict__ sel, int64_t n,
-                          const typename Slot<WIDE>::T* __restrict__ tab, uint64_t cap,
-                          unsigned long long* __restrict__ out, unsigned long long out_cap,
-                          unsigned long long* counter) {
-  for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < n;
-       i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
-    const int64_t r = RowAt(sel, i);
-    if (KeyNull(key, r)) continue;
-    ProbeOne<WIDE>(tab, cap, LoadKey(key, r), r, out, out_cap, counter);
+__global__ void __launch_bounds__(kBlock) ProbeFlat(KeyCol key, const int32_t* __restrict__ sel, int64_t n,
+                                                    const typename Slot<WIDE>::T* __restrict__ tab, uint64_t cap,
+                                                    unsigned long long* __restrict__ out,
+                                                    unsigned long long out_cap, unsigned long long* counter) {
+  __shared__ OutStage st;
+  if (threadIdx.x == 0) st.count = 0;
+  __syncthreads();
+  const int64_t stride = static_cast<int64_t>(gridDim.x) * blockDim.x;
+  for (int64_t b0 = blockIdx.x * static_cast<int64_t>(blockDim.x); b0 < n; b0 += stride) {
+    const int64_t i = b0 + threadIdx.x;
+    if (i < n) {
+      const int64_t r = RowAt(sel, i);
+      if (!KeyNull(key, r)) ProbeOne<WIDE>(tab, cap, LoadKey(key, r), r, st, out, out_cap, counter);
+    }
+    // every thread's matches of this round are staged before thread 0 looks
+    if (__syncthreads_or(threadIdx.x == 0 && st.count >= kOutStage / 2)) FlushPairs(st, out, out_cap, counter);
   }
+  FlushPairs(st, out, out_cap, counter);
 }
 
 // One CTA per partition: the sub-table is bulk-copied into shared memory
@@ -414,10 +465,12 @@ __global__ void __launch_bounds__(kBlock) ProbeParts(const typename Slot<WIDE>::
   using T = typename S::T;
   extern __shared__ __align__(128) unsigned char smem[];
   __shared__ __align__(8) uint64_t bar[3];  // tiles 0 and 1, the sub-table
+  __shared__ OutStage st;
   T* tiles[2] = {reinterpret_cast<T*>(smem), reinterpret_cast<T*>(smem + kProbeTile * sizeof(T))};
   T* stab = reinterpret_cast<T*>(smem + 2 * kProbeTile * sizeof(T));
   if (threadIdx.x == 0) {
     for (int b = 0; b < 3; b++) BarInit(&bar[b]);
+    st.count = 0;
     FenceProxyAsync();
   }
   __syncthreads();
@@ -467,11 +520,14 @@ __global__ void __launch_bounds__(kBlock) ProbeParts(const typename Slot<WIDE>::
       const uint32_t nt = static_cast<uint32_t>(umin64(kProbeTile, count - t * kProbeTile));
       for (uint32_t i = threadIdx.x; i < nt; i += blockDim.x) {
         const T v = tiles[b][i];
-        ProbeOne<WIDE>(tab, cap, S::Key(v), S::Row(v), out, out_cap, counter);
+        ProbeOne<WIDE>(tab, cap, S::Key(v), S::Row(v), st, out, out_cap, counter);
       }
-      __syncthreads();
+      // begins with a barrier: the tile's reads are done before its buffer
+      // is reused
+      FlushPairs(st, out, out_cap, counter);
     }
   }
+  FlushPairs(st, out, out_cap, counter);
 }
 
 __global__ void SplitPairs(const unsigned long long* __restrict__ pairs, int64_t n, int32_t* __restrict__ probe,

@@ -12,7 +12,8 @@ from kushdb_b200.engine import Engine
 SWITCHES = ["KDB_NO_SCAN_PREFETCH", "KDB_NO_VECTOR_SCAN", "KDB_VECTOR_PROBE_SCAN", "KDB_NO_JOIN_FILTER",
             "KDB_NO_KEY_IN_SLOT", "KDB_NO_BUILD_ROW_GROUPS", "KDB_NO_DENSE_GROUPBY", "KDB_MATERIALIZE_ATOMIC",
             "KDB_GROUP_ORDER_SORT", "KDB_ORDER_RADIX", "KDB_ORDER_TIE_SORT", "KDB_SKINNER_DEPTH1",
-            "KDB_SKINNER_NO_SPLIT", "KDB_NO_SKINNER_AGG", "KDB_DENSE_SMEM=0"]
+            "KDB_SKINNER_NO_SPLIT", "KDB_NO_SKINNER_AGG", "KDB_DENSE_SMEM=0", "KDB_ORDER_SAMPLE",
+            "KDB_NO_PROBE_PREFETCH", "KDB_LAZY_PROBE_COLUMNS", "KDB_NO_GROUP_ORDER_FUSE", "KDB_AGG_FUSED_FINALIZE"]
 
 
 @pytest.mark.parametrize("switch", SWITCHES)

@@ -50,7 +50,17 @@ def _plan(t, keys, asc):
                                       (["null_r"], [True]), (["null_r"], [False]),
                                       (["tied_r", "null_r"], [False, True]),
                                       (["tied_i"], [True]), (["tied_i"], [False]), (["id"], [False])])
-def test_order_matches_reference_merge_sort(setup, keys, asc):
+@pytest.mark.parametrize("sort", [None, "KDB_ORDER_SAMPLE", "KDB_ORDER_RADIX"])
+def test_order_matches_reference_merge_sort(setup, keys, asc, sort):
+    """Each device sort (merge passes, sample sort, radix passes) gives the
+    reference merge sort's order."""
     e, o, t = setup
     plan = _plan(t, keys, asc).to_json()
-    assert compare(e.execute(plan), o.execute(plan), ordered=True) == ""
+    if sort:
+        e.set_option(sort, "1")
+    try:
+        got = e.execute(plan)
+    finally:
+        if sort:
+            e.set_option(sort, None)
+    assert compare(got, o.execute(plan), ordered=True) == ""

@@ -40,22 +40,26 @@ def engine():
 
 
 def test_text_decoded_on_device_matches_fixture(engine):
-    from kushdb_b200.data import HostColumn  # noqa: F401
-    t = rp.golden_tables()["people"]
-    want = t.columns["name"].strings()
-    from kushdb_b200.plan import ColRef, OperatorSchema, OutputOperator, ScanOperator  # noqa: F401
+    """Every row's name, decoded on the device from the .kdb image, against
+    the fixture, matched by id (a scan's rows come out in no particular
+    order)."""
     from kushdb_b200.data import catalog_of
+    from kushdb_b200.plan import OperatorSchema, OutputOperator, ScanOperator
+    t = rp.golden_tables()["people"]
+    ids = t.columns["id"].values
+    names = t.columns["name"].strings()
+    nulls = t.columns["name"].nulls
+    want = {int(i): (None if z else n) for i, n, z in zip(ids, names, nulls)}
     rel = catalog_of([t])["people"]
     s = OperatorSchema()
-    s.AddGeneratedColumns(rel, ["name"])
+    s.AddGeneratedColumns(rel, ["id", "name"])
     res = engine.execute(OutputOperator(ScanOperator(s, rel)))
-    nulls = t.columns["name"].nulls
-    got = [res.row(r)[0] for r in range(res.num_rows)]
-    assert len(got) == len(want)
-    for r, (g, w) in enumerate(zip(got, want)):
-        assert (g is None) == bool(nulls[r])
-        if g is not None:
-            assert g == w
+    got = {}
+    for r in range(res.num_rows):
+        i, n = res.row(r)
+        got[int(i)] = n
+    assert res.num_rows == len(want) == len(got)
+    assert got == want
 
 
 @pytest.mark.parametrize("case", [c for c in rp.CASES if not c.name.startswith("tpch/")],
