@@ -451,53 +451,27 @@ std::string CombineBits(WordKind k, const std::string& a, const std::string& b) 
 // fixed order, then a shuffle tree (deterministic).
 void EmitPartialReduce(KernelSource& ks, const std::string& part, const std::string& G, int nw,
                        const std::vector<WordKind>& kinds) {
+  // the words' kinds as a table (one compact loop for every word, instead
+  // of a loop body per word: the latter overflowed the instruction cache)
+  const std::string kt = "kdb_kinds" + std::to_string(ks.lits++);
+  ks.globals << "__device__ const unsigned char " << kt << "[" << nw << "] = {";
+  for (int w = 0; w < nw; w++) ks.globals << static_cast<int>(kinds[w]) << ",";
+  ks.globals << "};\n";
   ks.L("__shared__ uint64_t tot[" + std::to_string(nw) + "];");
   ks.Open("");
   ks.L("const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;");
   ks.Open("for (int k = warp; k < " + std::to_string(nw) + "; k += blockDim.x / 32)");
-  ks.L("uint64_t acc = 0;");
-  // the word's kind is warp-uniform: one tight loop per kind, identity
-  // elements for lanes past the last block
-  ks.Open("switch (k)");
-  for (int w = 0; w < nw; w++) {
-    ks.Open("case " + std::to_string(w) + ":");
-    switch (kinds[w]) {
-      case WordKind::AddF64:
-        ks.L("{ double x = 0.0; for (int64_t b0 = lane; b0 < (int64_t)" + G + "; b0 += 256) { uint64_t v[8]; "
-             "_Pragma(\"unroll\") for (int u = 0; u < 8; u++) { const int64_t b = b0 + 32 * u; v[u] = b < (int64_t)" + G +
-             " ? " + part + "[(int64_t)k * (int64_t)" + G + " + b] : 0ULL; } "
-             "_Pragma(\"unroll\") for (int u = 0; u < 8; u++) if (b0 + 32 * u < (int64_t)" + G +
-             ") x = __dadd_rn(x, __longlong_as_double((long long)v[u])); }");
-        ks.L("for (int o = 16; o > 0; o >>= 1) x = __dadd_rn(x, __shfl_down_sync(0xffffffffu, x, o));");
-        ks.L("acc = (uint64_t)__double_as_longlong(x); }");
-        break;
-      case WordKind::AddI64:
-        ks.L("{ uint64_t x = 0; for (int64_t b0 = lane; b0 < (int64_t)" + G + "; b0 += 256) { uint64_t v[8]; "
-             "_Pragma(\"unroll\") for (int u = 0; u < 8; u++) { const int64_t b = b0 + 32 * u; v[u] = b < (int64_t)" + G +
-             " ? " + part + "[(int64_t)k * (int64_t)" + G + " + b] : 0ULL; } "
-             "_Pragma(\"unroll\") for (int u = 0; u < 8; u++) x += v[u]; }");
-        ks.L("for (int o = 16; o > 0; o >>= 1) x += __shfl_down_sync(0xffffffffu, x, o);");
-        ks.L("acc = x; }");
-        break;
-      case WordKind::MinU64:
-      case WordKind::MaxU64: {
-        bool mn = kinds[w] == WordKind::MinU64;
-        std::string cmp = mn ? "<" : ">";
-        ks.L(std::string("{ uint64_t x = ") + (mn ? "~0ULL" : "0ULL") + "; for (int64_t b0 = lane; b0 < (int64_t)" + G +
-             "; b0 += 256) { uint64_t v[8]; _Pragma(\"unroll\") for (int u = 0; u < 8; u++) { const int64_t b = b0 + 32 * u; "
-             "v[u] = b < (int64_t)" + G + " ? " + part + "[(int64_t)k * (int64_t)" + G + " + b] : x; } "
-             "_Pragma(\"unroll\") for (int u = 0; u < 8; u++) x = v[u] " + cmp + " x ? v[u] : x; }");
-        ks.L("for (int o = 16; o > 0; o >>= 1) { uint64_t y = __shfl_down_sync(0xffffffffu, x, o); x = y " + cmp +
-             " x ? y : x; }");
-        ks.L("acc = x; }");
-        break;
-      }
-    }
-    ks.L("break;");
-    ks.Close();
-  }
+  ks.L("const int kind = " + kt + "[k];");
+  ks.L("uint64_t x = kdb_word_identity(kind);");
+  ks.Open("for (int64_t b0 = lane; b0 < (int64_t)" + G + "; b0 += 256)");
+  ks.L("uint64_t v[8];");
+  ks.L("_Pragma(\"unroll\") for (int u = 0; u < 8; u++) { const int64_t b = b0 + 32 * u; v[u] = b < (int64_t)" + G +
+       " ? " + part + "[(int64_t)k * (int64_t)" + G + " + b] : 0ULL; }");
+  ks.L("_Pragma(\"unroll\") for (int u = 0; u < 8; u++) if (b0 + 32 * u < (int64_t)" + G +
+       ") x = kdb_word_combine(kind, x, v[u]);");
   ks.Close();
-  ks.L("if (lane == 0) tot[k] = acc;");
+  ks.L("for (int o = 16; o > 0; o >>= 1) x = kdb_word_combine(kind, x, __shfl_down_sync(0xffffffffu, x, o));");
+  ks.L("if (lane == 0) tot[k] = x;");
   ks.Close();
   ks.Close();
   ks.L("__syncthreads();");
@@ -752,20 +726,29 @@ class Executor {
   // column loads, bound such a pipeline, and the 4-row vector's registers
   // cost occupancy)
   bool probe_side_scan_ = false;
-  // Probe-ahead: set by a join whose probe side is a plain scan of its key
-  // column; that scan then loads the key two rows ahead and, one row ahead,
-  // the row's join-filter word and first table slot, so the probe of a row
-  // starts with its dependent table reads already done (KDB_NO_PROBE_AHEAD:
-  // off).  ahead_jt_/ahead_out_col_ go from the join to its scan; the
+  // TMA-staged scan: set by a consumer before emitting its scan (rows per
+  // tile, stages); the scan reports the dynamic shared memory it needs in
+  // tma_smem_ (0 when it fell back to register loads).
+  int tma_tile_ = 0, tma_stages_ = 0;
+  size_t tma_smem_ = 0;
+  // Probe-ahead (KDB_PROBE_AHEAD=1, or =word for the filter word alone): a
+  // join whose probe side is a plain scan of its key column has that scan
+  // load the key two rows ahead and, one row ahead, the row's join-filter
+  // word and first table slot, so the probe of a row starts with its
+  // dependent table reads done.  Measured on the Q3 shape it is slower (69
+  // vs 52 us for the probe + group-by kernel: the speculative loads of the
+  // rows the filter rejects crowd the load queues), so it is off by
+  // default.  ahead_jt_/ahead_out_col_ go from the join to its scan; the
   // ahead_* names come back from the scan to EmitProbe.
   const JoinTable* ahead_jt_ = nullptr;
   int ahead_out_col_ = -1;
   const JoinTable* ahead_probe_jt_ = nullptr;
+  bool ahead_slot_on_ = true;
   std::string ahead_key_var_, ahead_word_, ahead_slot_;
   void SetProbeAhead(const Operator& join, const JoinTable& jt) {
     ahead_jt_ = nullptr;
     ahead_out_col_ = -1;
-    if (ctx_.OptStr("KDB_NO_PROBE_AHEAD") || ctx_.OptStr("KDB_NO_PROBE_PREFETCH") ||
+    if (!ctx_.OptStr("KDB_PROBE_AHEAD") || ctx_.OptStr("KDB_NO_PROBE_PREFETCH") ||
         ctx_.OptStr("KDB_LAZY_PROBE_COLUMNS") || join.right_keys.size() != 1)
       return;
     const Expr& k = *join.right_keys[0];
@@ -773,6 +756,7 @@ class Executor {
     if (k.kind != ExprKind::ColRef || k.child_idx != 1 || (ck != OpKind::SCAN && ck != OpKind::SCAN_SELECT)) return;
     ahead_jt_ = &jt;
     ahead_out_col_ = k.column_idx;
+    ahead_slot_on_ = std::string(ctx_.OptStr("KDB_PROBE_AHEAD")) != "word";
   }
   void EmitProbe(KernelSource& ks, ExprGen& eg, const JoinTable& jt,
                  const std::vector<int>& build_key_cols, const std::vector<CVal>& probe_keys,
@@ -890,7 +874,150 @@ void Executor::EmitStream(KernelSource& ks, ExprGen& eg, const Operator& op, con
       const bool vec = !any_text && !probe_side && !ctx_.OptStr("KDB_NO_VECTOR_SCAN");
       std::vector<CVal> scan(cols.size());
       std::function<void(size_t)> load;
-      if (vec) {
+      // TMA staging needs every column (and null array) 16-byte aligned
+      const int TT = tma_tile_, TS = tma_stages_;
+      tma_tile_ = tma_stages_ = 0;
+      tma_smem_ = 0;
+      bool tma = vec && TT > 0 && TS > 0 && TT % 16 == 0;
+      for (size_t k = 0; k < cols.size() && tma; k++) {
+        tma = reinterpret_cast<uintptr_t>(cols[k]->data) % 16 == 0 &&
+              (!cols[k]->nulls || reinterpret_cast<uintptr_t>(cols[k]->nulls) % 16 == 0);
+      }
+      if (tma) {
+        // Persistent CTAs walk tiles of TT rows (tile t = blockIdx.x + i *
+        // gridDim.x).  Thread 0 keeps TS tiles in flight: per tile one
+        // 1-D bulk copy per column into that stage's shared memory, all
+        // completing on the stage's mbarrier; the threads read 4 rows at a
+        // time from shared memory.  The last tile's bytes past its last whole
+        // 16-byte unit are loaded by the threads themselves.
+        std::vector<size_t> off(cols.size(), 0), noff(cols.size(), 0);
+        std::vector<int> width(cols.size());
+        size_t sb = 0;
+        auto place = [&](size_t bytes) {
+          const size_t o = sb;
+          sb += (bytes + 127) / 128 * 128;
+          return o;
+        };
+        for (size_t k = 0; k < cols.size(); k++) {
+          width[k] = static_cast<int>(StoreWidth(cols[k]->type.id));
+          off[k] = place(static_cast<size_t>(TT) * width[k]);
+          if (!np[k].empty()) noff[k] = place(static_cast<size_t>(TT));
+        }
+        const size_t stage_bytes = sb;
+        tma_smem_ = stage_bytes * TS;
+        if (tma_smem_ > (size_t(160) << 10)) {
+          // too wide a row for the stages beside the consumer's own shared
+          // memory: register loads instead
+          tma = false;
+          tma_smem_ = 0;
+        }
+      }
+      if (tma) {
+        std::vector<size_t> off(cols.size(), 0), noff(cols.size(), 0);
+        std::vector<int> width(cols.size());
+        size_t sb = 0;
+        auto place = [&](size_t bytes) {
+          const size_t o = sb;
+          sb += (bytes + 127) / 128 * 128;
+          return o;
+        };
+        for (size_t k = 0; k < cols.size(); k++) {
+          width[k] = static_cast<int>(StoreWidth(cols[k]->type.id));
+          off[k] = place(static_cast<size_t>(TT) * width[k]);
+          if (!np[k].empty()) noff[k] = place(static_cast<size_t>(TT));
+        }
+        const size_t stage_bytes = sb;
+        const std::string ERR = ks.Ptr(ctx_.d_err, "int");
+        const std::string sT = std::to_string(TT), sS = std::to_string(TS), sB = std::to_string(stage_bytes);
+        ks.L("extern __shared__ __align__(128) unsigned char kdb_dsm[];");
+        ks.L("__shared__ __align__(8) uint64_t kdb_tbar[" + sS + "];");
+        ks.L("const int64_t nrows = (int64_t)" + n + ";");
+        ks.L("const int64_t kdb_nt = (nrows + " + sT + " - 1) / " + sT + ";");
+        ks.L("auto kdb_issue = [&](int64_t t, int st) {");
+        ks.indent++;
+        ks.L("const int64_t tb = t * " + sT + ";");
+        ks.L("const int64_t tn = nrows - tb < " + sT + " ? nrows - tb : " + sT + ";");
+        ks.L("unsigned char* sb = kdb_dsm + (size_t)st * " + sB + ";");
+        std::vector<std::string> bn(cols.size()), nbn(cols.size());
+        std::string tot = "0u";
+        for (size_t k = 0; k < cols.size(); k++) {
+          bn[k] = ks.Fresh("tb");
+          ks.L("const uint32_t " + bn[k] + " = (uint32_t)((tn * " + std::to_string(width[k]) + ") & ~15LL);");
+          tot += " + " + bn[k];
+          if (!np[k].empty()) {
+            nbn[k] = ks.Fresh("tnb");
+            ks.L("const uint32_t " + nbn[k] + " = (uint32_t)(tn & ~15LL);");
+            tot += " + " + nbn[k];
+          }
+        }
+        ks.L("kdb_bar_expect(&kdb_tbar[st], " + tot + ");");
+        for (size_t k = 0; k < cols.size(); k++) {
+          ks.L("if (" + bn[k] + ") kdb_bulk_copy(sb + " + std::to_string(off[k]) + ", (const unsigned char*)" + dp[k] +
+               " + tb * " + std::to_string(width[k]) + ", " + bn[k] + ", &kdb_tbar[st]);");
+          if (!np[k].empty())
+            ks.L("if (" + nbn[k] + ") kdb_bulk_copy(sb + " + std::to_string(noff[k]) + ", (const unsigned char*)" +
+                 np[k] + " + tb, " + nbn[k] + ", &kdb_tbar[st]);");
+        }
+        ks.indent--;
+        ks.L("};");
+        ks.L("if (threadIdx.x == 0) { for (int s = 0; s < " + sS +
+             "; s++) kdb_bar_init(&kdb_tbar[s]); kdb_fence_proxy_async(); }");
+        ks.L("__syncthreads();");
+        ks.L("if (threadIdx.x == 0) for (int s = 0; s < " + sS +
+             "; s++) { const int64_t t = blockIdx.x + (int64_t)s * gridDim.x; if (t < kdb_nt) kdb_issue(t, s); }");
+        ks.Open("for (int64_t kdb_it = 0;; kdb_it++)");
+        ks.L("const int64_t kdb_t = blockIdx.x + kdb_it * (int64_t)gridDim.x;");
+        ks.L("if (kdb_t >= kdb_nt) break;");
+        ks.L("const int kdb_st = (int)(kdb_it % " + sS + ");");
+        ks.Open("if (!kdb_bar_wait_all(&kdb_tbar[kdb_st], (uint32_t)((kdb_it / " + sS + ") & 1), " + ERR + "))");
+        // give up: wait (bounded) for every copy this block still has in
+        // flight into its shared memory, then leave
+        ks.Open("if (threadIdx.x == 0)");
+        ks.L("for (int64_t j = kdb_it; j < kdb_it + " + sS + "; j++) if (blockIdx.x + j * (int64_t)gridDim.x < kdb_nt) "
+             "kdb_bar_wait(&kdb_tbar[j % " + sS + "], (uint32_t)((j / " + sS + ") & 1));");
+        ks.Close();
+        ks.L("break;");
+        ks.Close();
+        ks.L("const int64_t kdb_tb = kdb_t * " + sT + ";");
+        ks.L("const int kdb_tn = (int)(nrows - kdb_tb < " + sT + " ? nrows - kdb_tb : " + sT + ");");
+        ks.L("unsigned char* kdb_sb = kdb_dsm + (size_t)kdb_st * " + sB + ";");
+        ks.Open("if (kdb_tn < " + sT + ")");
+        for (size_t k = 0; k < cols.size(); k++) {
+          const std::string st = StoreType(cols[k]->type.id), w = std::to_string(width[k]);
+          ks.L("for (int i = (int)(((kdb_tn * " + w + ") & ~15) / " + w + ") + threadIdx.x; i < kdb_tn; i += blockDim.x) ((" +
+               st + "*)(kdb_sb + " + std::to_string(off[k]) + "))[i] = " + dp[k] + "[kdb_tb + i];");
+          if (!np[k].empty())
+            ks.L("for (int i = (kdb_tn & ~15) + threadIdx.x; i < kdb_tn; i += blockDim.x) ((int8_t*)(kdb_sb + " +
+                 std::to_string(noff[k]) + "))[i] = " + np[k] + "[kdb_tb + i];");
+        }
+        // these generic writes precede later bulk copies into the stage
+        ks.L("kdb_fence_proxy_async();");
+        ks.L("__syncthreads();");
+        ks.Close();
+        std::vector<std::string> arr(cols.size()), narr(cols.size());
+        ks.Open("for (int q = threadIdx.x; q * 4 < kdb_tn; q += blockDim.x)");
+        ks.L("const int64_t base = kdb_tb + (int64_t)q * 4;");
+        for (size_t k = 0; k < cols.size(); k++) {
+          const std::string st = StoreType(cols[k]->type.id);
+          arr[k] = ks.Fresh("L");
+          ks.L(st + " " + arr[k] + "[4];");
+          ks.L("kdb_lds4((const " + st + "*)(kdb_sb + " + std::to_string(off[k]) + "), q * 4, " + arr[k] + ");");
+          if (!np[k].empty()) {
+            narr[k] = ks.Fresh("N");
+            ks.L("int8_t " + narr[k] + "[4];");
+            ks.L("kdb_lds4((const int8_t*)(kdb_sb + " + std::to_string(noff[k]) + "), q * 4, " + narr[k] + ");");
+          }
+        }
+        load = [&, arr, narr](size_t k) {
+          const DevColumn& c = *cols[k];
+          std::string v = c.type.id == TypeId::BOOLEAN ? "(" + arr[k] + "[u] != 0)" : arr[k] + "[u]";
+          scan[k] = eg.Bind(c.type, v, narr[k].empty() ? "false" : "(" + narr[k] + "[u] != 0)");
+        };
+        ks.L("#pragma unroll");
+        ks.Open("for (int u = 0; u < 4; u++)");
+        ks.L("const int64_t r = base + u;");
+        ks.Open("if (r < nrows)");
+      } else if (vec) {
         // 4 consecutive rows per thread, every column loaded with vector
         // loads up front (all loads of an iteration in flight together)
         // With prefetch (default), the next iteration's vectors are loaded
@@ -991,7 +1118,7 @@ void Executor::EmitStream(KernelSource& ks, ExprGen& eg, const Operator& op, con
           if (ajt->bloom)
             ks.L(a_word + " = __ldg(&" + a_bloom + "[kdb_bloom_bit(" + h + ", " + std::to_string(ajt->bloom_log2) +
                  ") >> 5]);");
-          ks.L(a_slot + " = " + a_slots + "[" + h + " & (uint32_t)" + ks.Word(ajt->mask) + "];");
+          if (ahead_slot_on_) ks.L(a_slot + " = " + a_slots + "[" + h + " & (uint32_t)" + ks.Word(ajt->mask) + "];");
         };
         if (pf) {
           ks.L("const int64_t kdb_pstride = (int64_t)gridDim.x * blockDim.x;");
@@ -1088,6 +1215,14 @@ void Executor::EmitStream(KernelSource& ks, ExprGen& eg, const Operator& op, con
           ks.Close();
         }
         ks.Close();
+        if (tma) {
+          // the stage is free once every thread has read it: refill it with
+          // the tile TS iterations ahead
+          ks.L("__syncthreads();");
+          ks.L("if (threadIdx.x == 0) { const int64_t kdb_nx = kdb_t + (int64_t)" + std::to_string(TS) +
+               " * gridDim.x; if (kdb_nx < kdb_nt) { kdb_fence_proxy_async(); kdb_issue(kdb_nx, kdb_st); } }");
+          ks.Close();
+        }
       };
       Scope s;
       if (op.kind == OpKind::SCAN) {
@@ -1240,7 +1375,8 @@ void Executor::EmitProbe(KernelSource& ks, ExprGen& eg, const JoinTable& jt,
   ks.L("uint32_t " + i + " = " + h + " & " + mask + ";");
   ks.Open("for (uint32_t " + k + " = 0; " + k + " <= " + mask + "; " + k + "++, " + i + " = (" + i +
           " + 1) & " + mask + ")");
-  if (ahead) ks.L("uint64_t " + e + " = " + k + " == 0 ? " + ahead_slot_ + " : " + slots + "[" + i + "];");
+  if (ahead && ahead_slot_on_)
+    ks.L("uint64_t " + e + " = " + k + " == 0 ? " + ahead_slot_ + " : " + slots + "[" + i + "];");
   else ks.L("uint64_t " + e + " = " + slots + "[" + i + "];");
   ks.L("if (" + e + " == 0) break;");
   std::string br = ks.Fresh("br");
@@ -1891,7 +2027,10 @@ MatBuffer Executor::RunAggregate(const Operator& op) {
     ks.Close();
   }
   {
-    std::string src = ks.Kernel("kdb_aggregate", block);
+    // KDB_AGG_MINB: CTAs per SM the register budget must allow (launch
+    // bounds); more resident CTAs keep more rows' loads in flight
+    const char* mb = ctx_.OptStr("KDB_AGG_MINB");
+    std::string src = ks.Kernel("kdb_aggregate", block, mb ? std::max(1, std::atoi(mb)) : 1);
     CUfunction f = ctx_.Kernel(src, "kdb_aggregate");
     ctx_.Launch(f, grid, block, ks.Args(), 0, "aggregate");
   }
@@ -2016,9 +2155,17 @@ MatBuffer Executor::RunGroupByDense(const Operator& op, const std::vector<AggPla
   // block size and the launch-bounds occupancy hint (env overrides for tuning)
   // (64 threads, 6 CTAs per SM: measured best on the Q1 shape among 64/128
   // threads and 2-8 CTAs per SM)
-  const int block = ctx_.OptStr("KDB_DENSE_BLOCK") ? std::atoi(ctx_.OptStr("KDB_DENSE_BLOCK")) : 64;
-  const int min_blocks = ctx_.OptStr("KDB_DENSE_MINB") ? std::atoi(ctx_.OptStr("KDB_DENSE_MINB")) : 6;
-  const int grid_per_sm = ctx_.OptStr("KDB_DENSE_GRID") ? std::atoi(ctx_.OptStr("KDB_DENSE_GRID")) : 6;
+  auto opt_int = [&](const char* name, int dflt) {
+    const char* v = ctx_.OptStr(name);
+    return v ? std::atoi(v) : dflt;
+  };
+  // KDB_DENSE_TMA: the scan's tiles come into shared memory by TMA bulk
+  // copies (persistent CTAs, KDB_TMA_CTAS per SM of KDB_TMA_BLOCK threads,
+  // KDB_TMA_STAGES tiles of KDB_TMA_TILE rows in flight)
+  const bool want_tma = ctx_.OptStr("KDB_DENSE_TMA") != nullptr && Streamable(op.child());
+  const int block = want_tma ? opt_int("KDB_TMA_BLOCK", 128) : opt_int("KDB_DENSE_BLOCK", 64);
+  const int min_blocks = want_tma ? opt_int("KDB_TMA_CTAS", 2) : opt_int("KDB_DENSE_MINB", 6);
+  const int grid_per_sm = want_tma ? opt_int("KDB_TMA_CTAS", 2) : opt_int("KDB_DENSE_GRID", 6);
   // Accumulators in registers (every row updates every group's words under a
   // predicate) or, for larger groups x words, in per-thread shared-memory
   // slots indexed by the group id (a row touches only its own group's words).
@@ -2057,6 +2204,11 @@ MatBuffer Executor::RunGroupByDense(const Operator& op, const std::vector<AggPla
       for (int w = 0; w < W; w++) ks.L(words[w].ctype + " " + reg(g, w) + " = " + words[w].init + ";");
   }
   int64_t src_rows = 0;
+  // a streamed child without a join hands each thread its rows in ascending
+  // position (grid-stride rows or tiles); a join's matches of one probe row
+  // come in table order, and a materialised child's positions in any order
+  const bool ascending_rows = Streamable(op.child()) && !StreamHasJoin(op.child()) &&
+                              !ctx_.OptStr("KDB_DENSE_FIRST_MIN");
   auto consume = [&](const std::vector<CVal>& in, const std::string& pos) {
     Scope s;
     s.child.push_back(in);
@@ -2106,6 +2258,16 @@ MatBuffer Executor::RunGroupByDense(const Operator& op, const std::vector<AggPla
       std::string I = ks.Fresh("si");
       ks.L("const int " + I + " = (int)" + G + " * " + std::to_string(block) + " + threadIdx.x;");
       for (int w = 0; w < W; w++) {
+        if (w == first_w && ascending_rows) continue;
+        if (w == rows_w && ascending_rows) {
+          // a thread meets its rows in ascending position: the group's
+          // first row for this thread is the one that finds its count at 0
+          const std::string old = ks.Fresh("nr");
+          ks.L("const int64_t " + old + " = " + slot(w) + "[" + I + "];");
+          ks.L(slot(w) + "[" + I + "] = " + old + " + 1;");
+          ks.L("if (" + old + " == 0) " + slot(first_w) + "[" + I + "] = " + cv[first_w] + ";");
+          continue;
+        }
         std::string upd = slot(w) + "[" + I + "] = " + combine(words[w].kind, slot(w) + "[" + I + "]", cv[w]) + ";";
         ks.L(active[w] == "true" ? upd : "if (" + active[w] + ") " + upd);
       }
@@ -2121,8 +2283,15 @@ MatBuffer Executor::RunGroupByDense(const Operator& op, const std::vector<AggPla
       }
     }
   };
+  if (want_tma && in_smem) {
+    tma_tile_ = opt_int("KDB_TMA_TILE", 512);
+    tma_stages_ = opt_int("KDB_TMA_STAGES", 3);
+  }
   if (Streamable(op.child())) EmitStream(ks, eg, op.child(), consume, src_rows);
   else EmitMatScan(ks, mats_.at(&op.child()), nullptr, consume, src_rows);
+  const size_t dsmem = tma_smem_;
+  tma_tile_ = tma_stages_ = 0;
+  tma_smem_ = 0;
 
   int grid = static_cast<int>(std::min<int64_t>(ctx_.GridFor(std::max<int64_t>(src_rows, 1), block),
                                                 static_cast<int64_t>(ctx_.num_sms) * grid_per_sm));
@@ -2177,7 +2346,7 @@ MatBuffer Executor::RunGroupByDense(const Operator& op, const std::vector<AggPla
   {
     std::string src = ks.Kernel("kdb_group_by_dense", block, min_blocks);
     CUfunction f = ctx_.Kernel(src, "kdb_group_by_dense");
-    ctx_.Launch(f, grid, block, ks.Args(), 0, "group by");
+    ctx_.Launch(f, grid, block, ks.Args(), dsmem, "group by");
   }
 
   // finalize: one block combines the per-CTA partials (warp per word, fixed

@@ -175,6 +175,88 @@ KDB_DEV void kdb_ld4(const int8_t* p, int64_t base, int8_t* o) {
   o[0] = v.x; o[1] = v.y; o[2] = v.z; o[3] = v.w;
 }
 
+// Four consecutive values from a shared-memory stage (`i` a multiple of 4,
+// the column's stage region 16-byte aligned).
+KDB_DEV void kdb_lds4(const int32_t* p, int i, int32_t* o) {
+  int4 v = *reinterpret_cast<const int4*>(p + i);
+  o[0] = v.x; o[1] = v.y; o[2] = v.z; o[3] = v.w;
+}
+KDB_DEV void kdb_lds4(const double* p, int i, double* o) {
+  double2 a = *reinterpret_cast<const double2*>(p + i);
+  double2 b = *reinterpret_cast<const double2*>(p + i + 2);
+  o[0] = a.x; o[1] = a.y; o[2] = b.x; o[3] = b.y;
+}
+KDB_DEV void kdb_lds4(const int64_t* p, int i, int64_t* o) {
+  longlong2 a = *reinterpret_cast<const longlong2*>(p + i);
+  longlong2 b = *reinterpret_cast<const longlong2*>(p + i + 2);
+  o[0] = a.x; o[1] = a.y; o[2] = b.x; o[3] = b.y;
+}
+KDB_DEV void kdb_lds4(const int16_t* p, int i, int16_t* o) {
+  short4 v = *reinterpret_cast<const short4*>(p + i);
+  o[0] = v.x; o[1] = v.y; o[2] = v.z; o[3] = v.w;
+}
+KDB_DEV void kdb_lds4(const int8_t* p, int i, int8_t* o) {
+  char4 v = *reinterpret_cast<const char4*>(p + i);
+  o[0] = v.x; o[1] = v.y; o[2] = v.z; o[3] = v.w;
+}
+
+// ---- partial-word combining (finalize kernels) ---------------------------------
+// Word kinds: 0 = FP64 sum (bits of a double), 1 = 64-bit integer sum,
+// 2 = unsigned minimum, 3 = unsigned maximum.
+KDB_DEV uint64_t kdb_word_identity(int kind) { return kind == 2 ? ~0ULL : 0ULL; }
+KDB_DEV uint64_t kdb_word_combine(int kind, uint64_t a, uint64_t b) {
+  switch (kind) {
+    case 0: return (uint64_t)__double_as_longlong(__dadd_rn(__longlong_as_double((long long)a),
+                                                           __longlong_as_double((long long)b)));
+    case 1: return a + b;
+    case 2: return b < a ? b : a;
+    default: return b > a ? b : a;
+  }
+}
+
+// ---- TMA bulk copies into shared-memory stages -------------------------------
+// One mbarrier per stage (arrival count 1): the issuing thread announces the
+// stage's total bytes, then starts one 1-D bulk copy per column; the phase
+// completes when every byte has landed.  Waits are bounded.
+KDB_DEV uint32_t kdb_smem_addr(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+KDB_DEV void kdb_bar_init(uint64_t* bar) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(kdb_smem_addr(bar)) : "memory");
+}
+// orders this thread's generic shared-memory accesses (and barrier inits)
+// before its later bulk copies
+KDB_DEV void kdb_fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+KDB_DEV void kdb_bar_expect(uint64_t* bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(kdb_smem_addr(bar)), "r"(bytes)
+               : "memory");
+}
+// dst, src and bytes are multiples of 16
+KDB_DEV void kdb_bulk_copy(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                   kdb_smem_addr(dst)),
+               "l"(src), "r"(bytes), "r"(kdb_smem_addr(bar))
+               : "memory");
+}
+KDB_DEV bool kdb_bar_wait(uint64_t* bar, uint32_t parity) {
+  for (int it = 0; it < KDB_SPIN_LIMIT; it++) {
+    uint32_t done;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
+        : "=r"(done)
+        : "r"(kdb_smem_addr(bar)), "r"(parity)
+        : "memory");
+    if (done) return true;
+  }
+  return false;
+}
+// Every thread waits; the outcome is block-uniform.  A wait that gave up
+// records KDB_DEV_ERR_TIMEOUT.
+KDB_DEV bool kdb_bar_wait_all(uint64_t* bar, uint32_t parity, int* err) {
+  const bool ok = kdb_bar_wait(bar, parity);
+  if (!__syncthreads_or(!ok)) return true;
+  if (threadIdx.x == 0) atomicCAS(err, 0, KDB_DEV_ERR_TIMEOUT);
+  return false;
+}
+
 // ---- hashing ----------------------------------------------------------------
 KDB_DEV uint64_t kdb_mix64(uint64_t x) {
   // splitmix64 finaliser

@@ -13,7 +13,9 @@ SWITCHES = ["KDB_NO_SCAN_PREFETCH", "KDB_NO_VECTOR_SCAN", "KDB_VECTOR_PROBE_SCAN
             "KDB_NO_KEY_IN_SLOT", "KDB_NO_BUILD_ROW_GROUPS", "KDB_NO_DENSE_GROUPBY", "KDB_MATERIALIZE_ATOMIC",
             "KDB_GROUP_ORDER_SORT", "KDB_ORDER_RADIX", "KDB_ORDER_TIE_SORT", "KDB_SKINNER_DEPTH1",
             "KDB_SKINNER_NO_SPLIT", "KDB_NO_SKINNER_AGG", "KDB_DENSE_SMEM=0", "KDB_ORDER_SAMPLE",
-            "KDB_NO_PROBE_PREFETCH", "KDB_LAZY_PROBE_COLUMNS", "KDB_NO_GROUP_ORDER_FUSE", "KDB_AGG_FUSED_FINALIZE"]
+            "KDB_NO_PROBE_PREFETCH", "KDB_LAZY_PROBE_COLUMNS", "KDB_NO_GROUP_ORDER_FUSE", "KDB_AGG_FUSED_FINALIZE",
+            "KDB_DENSE_TMA", "KDB_DENSE_FIRST_MIN", "KDB_PROBE_AHEAD", "KDB_PROBE_AHEAD=word",
+            "KDB_AGG_MINB=4"]
 
 
 @pytest.mark.parametrize("switch", SWITCHES)

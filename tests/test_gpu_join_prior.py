@@ -112,6 +112,10 @@ def test_prior_needs_fewer_episodes_than_uct(engine):
     assert info["samples"] > 1000
     assert info["last_loss"] < info["first_loss"]
     totals = {"uct": [0, 0, 0, 0.0], "prior": [0, 0, 0, 0.0]}
+    # one join order per episode batch: every decision is the policy's own
+    # (with 16 orders per batch these small joins finish inside the first
+    # batch whichever policy picks the orders)
+    engine.set_option("KDB_SKINNER_BATCH", "1")
     for _, plan in test_q:  # compile every plan's kernels before timing
         engine.set_skinner_policy("uct")
         engine.set_skinner(budget, seed=0)
@@ -128,13 +132,11 @@ def test_prior_needs_fewer_episodes_than_uct(engine):
                 totals[policy][3] += engine.last_device_ms()
     engine.set_skinner_policy("uct")
     engine.set_skinner()
+    engine.set_option("KDB_SKINNER_BATCH", None)
     print("episodes / work / batches / device ms (uct, prior):", totals)
-    # episodes run 16 join orders per batch, so the episode and batch counts
-    # move in steps; the prior's gain shows in the tuples the episodes
-    # process and reaches the clock: less device time (the prior's values
-    # come from one forward pass per join)
-    assert totals["prior"][0] <= totals["uct"][0]
-    assert totals["prior"][2] <= totals["uct"][2]
-    assert totals["prior"][1] < 0.9 * totals["uct"][1]
+    # fewer episodes and tuples, and the gain reaches the clock: less device
+    # time (the prior's values come from one forward pass per join)
+    assert totals["prior"][0] < totals["uct"][0]
+    assert totals["prior"][1] < totals["uct"][1]
     assert totals["prior"][3] < totals["uct"][3]
     model.close()
