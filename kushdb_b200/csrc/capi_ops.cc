@@ -30,11 +30,17 @@ struct kdb_index {
 
 namespace {
 
+// Runs one operator call; with profiling on, its kernels' CUDA-event times
+// become the context's last-query kernel list (as for a whole plan).
 template <typename F>
 int OpGuard(kdb_ctx* ctx, F&& f) {
   if (!ctx) return KDB_ERR_INVALID;
   try {
-    f(*kdb_ctx_context(ctx));
+    kdb::Context& c = *kdb_ctx_context(ctx);
+    c.BeginQueryProfile();
+    f(c);
+    // (a call that ran a whole plan has collected its own kernels already)
+    if (!c.timings.empty()) c.EndQueryProfile();
     return KDB_OK;
   } catch (const kdb::Error& e) {
     kdb_ctx_set_error(ctx, e.what());

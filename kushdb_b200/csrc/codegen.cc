@@ -748,15 +748,16 @@ class Executor {
   void SetProbeAhead(const Operator& join, const JoinTable& jt) {
     ahead_jt_ = nullptr;
     ahead_out_col_ = -1;
-    if (!ctx_.OptStr("KDB_PROBE_AHEAD") || ctx_.OptStr("KDB_NO_PROBE_PREFETCH") ||
-        ctx_.OptStr("KDB_LAZY_PROBE_COLUMNS") || join.right_keys.size() != 1)
+    const char* mode = ctx_.OptStr("KDB_PROBE_AHEAD");
+    if ((!mode && !ctx_.OptStr("KDB_PROBE_VEC")) || ctx_.OptStr("KDB_LAZY_PROBE_COLUMNS") ||
+        join.right_keys.size() != 1)
       return;
     const Expr& k = *join.right_keys[0];
     const OpKind ck = join.child(1).kind;
     if (k.kind != ExprKind::ColRef || k.child_idx != 1 || (ck != OpKind::SCAN && ck != OpKind::SCAN_SELECT)) return;
     ahead_jt_ = &jt;
     ahead_out_col_ = k.column_idx;
-    ahead_slot_on_ = std::string(ctx_.OptStr("KDB_PROBE_AHEAD")) != "word";
+    ahead_slot_on_ = !mode || std::string(mode) != "word";
   }
   void EmitProbe(KernelSource& ks, ExprGen& eg, const JoinTable& jt,
                  const std::vector<int>& build_key_cols, const std::vector<CVal>& probe_keys,
@@ -871,7 +872,25 @@ void Executor::EmitStream(KernelSource& ks, ExprGen& eg, const Operator& op, con
       for (const DevColumn* c : cols) any_text |= c->type.id == TypeId::TEXT;
       const bool probe_side = probe_side_scan_;
       probe_side_scan_ = false;
-      const bool vec = !any_text && !probe_side && !ctx_.OptStr("KDB_NO_VECTOR_SCAN");
+      // probe-ahead: the scan column that is the join's probe key
+      const JoinTable* ajt = ahead_jt_;
+      ahead_jt_ = nullptr;
+      int ak = -1;
+      if (probe_side && ajt && ahead_out_col_ >= 0 && ahead_out_col_ < static_cast<int>(op.output.size())) {
+        const Expr& oe = *op.output[ahead_out_col_].expr;
+        const bool direct = (oe.kind == ExprKind::ColRef && oe.child_idx == 0) || oe.kind == ExprKind::VirtColRef;
+        if (direct && oe.column_idx >= 0 && oe.column_idx < static_cast<int>(cols.size())) {
+          const TypeId t = cols[oe.column_idx]->type.id;
+          if (t == TypeId::INT || t == TypeId::DATE || t == TypeId::ENUM || t == TypeId::SMALLINT ||
+              t == TypeId::BIGINT)
+            ak = oe.column_idx;
+        }
+      }
+      // KDB_PROBE_VEC: the probe side too takes 4-row vectors, and each
+      // vector's join-filter words, then (for the rows that pass) first
+      // table slots, load together before its rows are probed
+      const bool vec_probe = probe_side && ak >= 0 && ctx_.OptStr("KDB_PROBE_VEC") != nullptr;
+      const bool vec = !any_text && (!probe_side || vec_probe) && !ctx_.OptStr("KDB_NO_VECTOR_SCAN");
       std::vector<CVal> scan(cols.size());
       std::function<void(size_t)> load;
       // TMA staging needs every column (and null array) 16-byte aligned
@@ -1079,10 +1098,38 @@ void Executor::EmitStream(KernelSource& ks, ExprGen& eg, const Operator& op, con
         } else {
           fetch("q", arr, narr);
         }
-        load = [&, arr, narr](size_t k) {
+        if (vec_probe) {
+          // the vector's 4 join-filter words, then the first table slots of
+          // the rows that pass, all in flight together (indexes masked:
+          // always in bounds; rows past the end carry key 0)
+          const std::string vs = ks.Ptr(ajt->slots, "uint64_t", true), vm = ks.Word(ajt->mask);
+          const std::string vb = ajt->bloom ? ks.Ptr(ajt->bloom, "uint32_t", true) : "";
+          const std::string lg = std::to_string(ajt->bloom_log2);
+          const std::string h = JoinHash(eg, {CVal{cols[ak]->type, arr[ak] + "[u]", "false"}});
+          ks.L("uint32_t VW[4];");
+          ks.L("uint64_t VS[4];");
+          ks.L("#pragma unroll");
+          ks.L("for (int u = 0; u < 4; u++) VW[u] = " +
+               (vb.empty() ? std::string("~0u") : "__ldg(&" + vb + "[kdb_bloom_bit(" + h + ", " + lg + ") >> 5])") + ";");
+          ks.L("#pragma unroll");
+          ks.Open("for (int u = 0; u < 4; u++)");
+          ks.L("const uint32_t vh = " + h + ";");
+          if (vb.empty())
+            ks.L("VS[u] = " + vs + "[vh & (uint32_t)" + vm + "];");
+          else
+            ks.L("VS[u] = ((VW[u] >> (kdb_bloom_bit(vh, " + lg + ") & 31)) & 1u) ? " + vs + "[vh & (uint32_t)" + vm +
+                 "] : 0ULL;");
+          ks.Close();
+          ahead_probe_jt_ = ajt;
+          ahead_word_ = "VW[u]";
+          ahead_slot_ = "VS[u]";
+          ahead_slot_on_ = true;
+        }
+        load = [&, arr, narr, ak](size_t k) {
           const DevColumn& c = *cols[k];
           std::string v = c.type.id == TypeId::BOOLEAN ? "(" + arr[k] + "[u] != 0)" : arr[k] + "[u]";
           scan[k] = eg.Bind(c.type, v, narr[k].empty() ? "false" : "(" + narr[k] + "[u] != 0)");
+          if (static_cast<int>(k) == ak) ahead_key_var_ = scan[k].v;
         };
         ks.L("#pragma unroll");
         ks.Open("for (int u = 0; u < 4; u++)");
@@ -1095,20 +1142,7 @@ void Executor::EmitStream(KernelSource& ks, ExprGen& eg, const Operator& op, con
         // probe's dependent L2 accesses (KDB_NO_PROBE_PREFETCH: off).
         const bool pf = probe_side && !ctx_.OptStr("KDB_NO_PROBE_PREFETCH") && !ctx_.OptStr("KDB_LAZY_PROBE_COLUMNS");
         std::vector<std::string> nxt(cols.size()), nnx(cols.size());
-        // probe-ahead: the scan column that is the join's probe key
-        const JoinTable* ajt = ahead_jt_;
-        ahead_jt_ = nullptr;
-        int ak = -1;
-        if (pf && ajt && ahead_out_col_ >= 0 && ahead_out_col_ < static_cast<int>(op.output.size())) {
-          const Expr& oe = *op.output[ahead_out_col_].expr;
-          const bool direct = (oe.kind == ExprKind::ColRef && oe.child_idx == 0) || oe.kind == ExprKind::VirtColRef;
-          if (direct && oe.column_idx >= 0 && oe.column_idx < static_cast<int>(cols.size())) {
-            const TypeId t = cols[oe.column_idx]->type.id;
-            if (t == TypeId::INT || t == TypeId::DATE || t == TypeId::ENUM || t == TypeId::SMALLINT ||
-                t == TypeId::BIGINT)
-              ak = oe.column_idx;
-          }
-        }
+        if (!pf || !ctx_.OptStr("KDB_PROBE_AHEAD")) ak = -1;
         std::string a_key2, a_word, a_slot, a_slots, a_bloom;
         auto ahead_loads = [&](const std::string& key) {
           // the join-filter word and the first table slot of the row whose

@@ -46,7 +46,8 @@ namespace {
 
 constexpr int kBlock = 256;
 constexpr int kMaxPartBits = 13;                 // at most 8192 sub-tables
-constexpr size_t kSmemTableMax = 128 << 10;      // a sub-table copied into shared memory
+constexpr size_t kSmemTableMax = 128 << 10;      // a sub-table built in shared memory
+constexpr size_t kTableBuf = 64 << 10;           // a probe-side sub-table buffer (two of them)
 constexpr int kProbeTile = 2048;                 // probe tuples per bulk-copied tile
 constexpr uint32_t kWaitLimit = 1u << 24;        // bounded mbarrier waits
 constexpr int kErrWait = 1;                      // device error word: a wait gave up
@@ -297,10 +298,12 @@ __global__ void BuildFlat(KeyCol key, const int32_t* __restrict__ sel, int64_t n
   }
 }
 
-// One CTA per partition (grid-stride over partitions): the partition's
-// staged tuples come into shared memory in bulk-copied tiles; a sub-table
-// that fits shared memory is built there with shared-memory CAS and written
-// out with coalesced stores, a larger one is built in place in HBM.
+// Persistent CTAs, partitions p = blockIdx.x + i * gridDim.x (empty ones
+// skipped: their slots are already zero).  A partition's staged tuples come
+// into shared memory in bulk-copied tiles through a two-buffer ring that
+// runs one tile ahead, across partition boundaries too; a sub-table that
+// fits shared memory is built there with shared-memory CAS and written out
+// with coalesced stores, a larger one is built in place in HBM.
 template <bool WIDE>
 __global__ void __launch_bounds__(kBlock) BuildParts(const typename Slot<WIDE>::T* __restrict__ staged,
                                                      const unsigned long long* __restrict__ stage_off,
@@ -310,51 +313,76 @@ __global__ void __launch_bounds__(kBlock) BuildParts(const typename Slot<WIDE>::
   using S = Slot<WIDE>;
   using T = typename S::T;
   extern __shared__ __align__(128) unsigned char smem[];
-  __shared__ __align__(8) uint64_t bar;
-  T* tile = reinterpret_cast<T*>(smem);
-  T* stab = reinterpret_cast<T*>(smem + kProbeTile * sizeof(T));
+  __shared__ __align__(8) uint64_t bar[2];
+  T* tiles[2] = {reinterpret_cast<T*>(smem), reinterpret_cast<T*>(smem + kProbeTile * sizeof(T))};
+  T* stab = reinterpret_cast<T*>(smem + 2 * kProbeTile * sizeof(T));
   if (threadIdx.x == 0) {
-    BarInit(&bar);
+    for (int b = 0; b < 2; b++) BarInit(&bar[b]);
     FenceProxyAsync();
   }
   __syncthreads();
-  uint32_t phase = 0;
+  uint32_t issued[2] = {0, 0}, waited[2] = {0, 0};
+  auto next_part = [&](int q) {
+    for (q += gridDim.x; q < parts && hist[q] == 0; q += gridDim.x) {
+    }
+    return q;
+  };
+  auto issue_tile = [&](int q, uint64_t t, int b) {
+    const uint64_t count = hist[q], t0 = t * kProbeTile;
+    const uint32_t n = static_cast<uint32_t>(umin64(kProbeTile, count - t0));
+    FenceProxyAsync();
+    BulkLoad(tiles[b], staged + stage_off[q] + t0, (n * sizeof(T) + 15) & ~15u, &bar[b]);
+    issued[b]++;
+  };
+  int p = blockIdx.x;
+  if (p < parts && hist[p] == 0) p = next_part(p);
+  if (threadIdx.x == 0 && p < parts) issue_tile(p, 0, 0);
   bool failed = false;
-  for (int p = blockIdx.x; p < parts && !failed; p += gridDim.x) {
+  uint64_t j = 0;
+  while (p < parts && !failed) {
     const uint64_t cap = slot_off[p + 1] - slot_off[p];
     T* gtab = slots + slot_off[p];
     const bool in_smem = cap * sizeof(T) <= kSmemTableMax;
     T* tab = in_smem ? stab : gtab;
+    const uint64_t count = hist[p];
+    const uint64_t ntiles = (count + kProbeTile - 1) / kProbeTile;
+    const int np = next_part(p);
     if (in_smem) {
+      // the previous partition's table was written out before the barrier
+      // that ended it
       for (uint64_t i = threadIdx.x; i < cap; i += blockDim.x) tab[i] = T{};
       __syncthreads();
     }
-    const uint64_t count = hist[p];
-    const T* src = staged + stage_off[p];
-    for (uint64_t t0 = 0; t0 < count; t0 += kProbeTile) {
-      const uint32_t nt = static_cast<uint32_t>(umin64(kProbeTile, count - t0));
-      // the previous tile's reads (generic proxy) are done before the copy
-      // (async proxy) overwrites it
-      __syncthreads();
+    for (uint64_t t = 0; t < ntiles; t++) {
+      const int b = static_cast<int>(j & 1);
+      // tile j + 1 into the other buffer, whose reads ended at the barrier
+      // that closed item j - 1
       if (threadIdx.x == 0) {
-        FenceProxyAsync();
-        BulkLoad(tile, src + t0, ((nt * sizeof(T)) + 15) & ~15u, &bar);
+        if (t + 1 < ntiles) issue_tile(p, t + 1, b ^ 1);
+        else if (np < parts) issue_tile(np, 0, b ^ 1);
       }
-      if (!BarWaitAll(&bar, phase, err)) {
+      if (!BarWaitAll(&bar[b], waited[b] & 1, err)) {
         failed = true;
         break;
       }
-      phase ^= 1;
+      waited[b]++;
+      const uint32_t nt = static_cast<uint32_t>(umin64(kProbeTile, count - t * kProbeTile));
       for (uint32_t i = threadIdx.x; i < nt; i += blockDim.x) {
-        const T v = tile[i];
+        const T v = tiles[b][i];
         const int64_t k = S::Key(v);
         if (!Insert<WIDE>(tab, cap, Hash32(static_cast<uint64_t>(k)), v)) atomicOr(err, kErrFull);
       }
+      __syncthreads();
+      j++;
     }
-    __syncthreads();
     if (in_smem && !failed)
       for (uint64_t i = threadIdx.x; i < cap; i += blockDim.x) gtab[i] = tab[i];
     __syncthreads();
+    p = np;
+  }
+  if (failed && threadIdx.x == 0) {
+    for (int b = 0; b < 2; b++)
+      for (; waited[b] < issued[b]; waited[b]++) BarWait(&bar[b], waited[b] & 1);
   }
 }
 
@@ -448,10 +476,12 @@ __global__ void __launch_bounds__(kBlock) ProbeFlat(KeyCol key, const int32_t* _
   FlushPairs(st, out, out_cap, counter);
 }
 
-// One CTA per partition: the sub-table is bulk-copied into shared memory
-// (when it fits) and the partition's staged probe tuples stream through two
-// shared-memory tiles, the copy of the next tile in flight while this one is
-// probed.
+// Persistent CTAs, partitions p = blockIdx.x + i * gridDim.x.  A CTA's work
+// is the sequence of its partitions' probe tiles (kProbeTile staged tuples
+// each); thread 0 keeps one tile ahead in a two-buffer ring and, as a
+// partition starts, the NEXT partition's sub-table loading into the other of
+// two table buffers, so a partition's table copy overlaps the probing of the
+// one before.  Sub-tables larger than a table buffer are probed in HBM.
 template <bool WIDE>
 __global__ void __launch_bounds__(kBlock) ProbeParts(const typename Slot<WIDE>::T* __restrict__ staged,
                                                      const unsigned long long* __restrict__ stage_off,
@@ -464,68 +494,95 @@ __global__ void __launch_bounds__(kBlock) ProbeParts(const typename Slot<WIDE>::
   using S = Slot<WIDE>;
   using T = typename S::T;
   extern __shared__ __align__(128) unsigned char smem[];
-  __shared__ __align__(8) uint64_t bar[3];  // tiles 0 and 1, the sub-table
+  // barriers 0-1: tile ring; 2-3: table buffers
+  __shared__ __align__(8) uint64_t bar[4];
   __shared__ OutStage st;
   T* tiles[2] = {reinterpret_cast<T*>(smem), reinterpret_cast<T*>(smem + kProbeTile * sizeof(T))};
-  T* stab = reinterpret_cast<T*>(smem + 2 * kProbeTile * sizeof(T));
+  T* tabs[2] = {reinterpret_cast<T*>(smem + 2 * kProbeTile * sizeof(T)),
+                reinterpret_cast<T*>(smem + 2 * kProbeTile * sizeof(T) + kTableBuf)};
   if (threadIdx.x == 0) {
-    for (int b = 0; b < 3; b++) BarInit(&bar[b]);
+    for (int b = 0; b < 4; b++) BarInit(&bar[b]);
     st.count = 0;
     FenceProxyAsync();
   }
   __syncthreads();
-  uint32_t phase[3] = {0, 0, 0};
+  // copies issued / waited per barrier (thread 0 issues, every thread waits
+  // in the same order, so `waited` is block-uniform)
+  uint32_t issued[4] = {0, 0, 0, 0}, waited[4] = {0, 0, 0, 0};
+  auto next_part = [&](int q) {
+    for (q += gridDim.x; q < parts && hist[q] == 0; q += gridDim.x) {
+    }
+    return q;
+  };
+  auto tab_fits = [&](int q) { return (slot_off[q + 1] - slot_off[q]) * sizeof(T) <= kTableBuf; };
+  auto issue_tile = [&](int q, uint64_t t, int b) {
+    const uint64_t count = hist[q], t0 = t * kProbeTile;
+    const uint32_t n = static_cast<uint32_t>(umin64(kProbeTile, count - t0));
+    FenceProxyAsync();
+    BulkLoad(tiles[b], staged + stage_off[q] + t0, (n * sizeof(T) + 15) & ~15u, &bar[b]);
+    issued[b]++;
+  };
+  auto issue_tab = [&](int q, int b) {
+    FenceProxyAsync();
+    BulkLoad(tabs[b], slots + slot_off[q], static_cast<uint32_t>((slot_off[q + 1] - slot_off[q]) * sizeof(T)),
+             &bar[2 + b]);
+    issued[2 + b]++;
+  };
+  int p = blockIdx.x;
+  if (p < parts && hist[p] == 0) p = next_part(p);
+  if (threadIdx.x == 0 && p < parts) {
+    if (tab_fits(p)) issue_tab(p, 0);
+    issue_tile(p, 0, 0);
+  }
   bool failed = false;
-  for (int p = blockIdx.x; p < parts && !failed; p += gridDim.x) {
+  uint64_t j = 0;  // items (tiles) so far
+  int tb = 0;      // table buffer of the current partition
+  while (p < parts && !failed) {
     const uint64_t cap = slot_off[p + 1] - slot_off[p];
-    const T* gtab = slots + slot_off[p];
-    const bool in_smem = cap * sizeof(T) <= kSmemTableMax;
     const uint64_t count = hist[p];
-    const T* src = staged + stage_off[p];
     const uint64_t ntiles = (count + kProbeTile - 1) / kProbeTile;
-    __syncthreads();  // the previous partition's reads are done
-    if (threadIdx.x == 0 && count > 0) {
-      FenceProxyAsync();
-      if (in_smem) BulkLoad(stab, gtab, static_cast<uint32_t>(cap * sizeof(T)), &bar[2]);
-      const uint32_t n0 = static_cast<uint32_t>(umin64(kProbeTile, count));
-      BulkLoad(tiles[0], src, (n0 * sizeof(T) + 15) & ~15u, &bar[0]);
-    }
-    if (count == 0) continue;
-    if (in_smem) {
-      if (!BarWaitAll(&bar[2], phase[2], err)) {
-        if (threadIdx.x == 0) BarWait(&bar[0], phase[0]);  // the first tile's copy
-        failed = true;
-        break;
-      }
-      phase[2] ^= 1;
-    }
-    const T* tab = in_smem ? stab : gtab;
+    const bool fits = tab_fits(p);
+    const int np = next_part(p);
     for (uint64_t t = 0; t < ntiles; t++) {
-      const int b = static_cast<int>(t & 1);
-      // start the next tile into the other buffer, whose reads finished at
-      // the barrier that ended the previous iteration
-      if (threadIdx.x == 0 && t + 1 < ntiles) {
-        FenceProxyAsync();
-        const uint64_t t1 = (t + 1) * kProbeTile;
-        const uint32_t n1 = static_cast<uint32_t>(umin64(kProbeTile, count - t1));
-        BulkLoad(tiles[b ^ 1], src + t1, (n1 * sizeof(T) + 15) & ~15u, &bar[b ^ 1]);
+      const int b = static_cast<int>(j & 1);
+      if (threadIdx.x == 0) {
+        if (t + 1 < ntiles) issue_tile(p, t + 1, b ^ 1);
+        else if (np < parts) issue_tile(np, 0, b ^ 1);
+        // the next fitting partition's buffer: the other one when this
+        // partition holds one, else the free current one
+        if (t == 0 && np < parts && tab_fits(np)) issue_tab(np, fits ? tb ^ 1 : tb);
       }
-      if (!BarWaitAll(&bar[b], phase[b], err)) {
-        // the next tile's copy, when one was started, is waited for (bounded)
-        if (threadIdx.x == 0 && t + 1 < ntiles) BarWait(&bar[b ^ 1], phase[b ^ 1]);
+      if (t == 0 && fits) {
+        if (!BarWaitAll(&bar[2 + tb], waited[2 + tb] & 1, err)) {
+          failed = true;
+          break;
+        }
+        waited[2 + tb]++;
+      }
+      if (!BarWaitAll(&bar[b], waited[b] & 1, err)) {
         failed = true;
         break;
       }
-      phase[b] ^= 1;
+      waited[b]++;
+      const T* tab = fits ? tabs[tb] : slots + slot_off[p];
       const uint32_t nt = static_cast<uint32_t>(umin64(kProbeTile, count - t * kProbeTile));
       for (uint32_t i = threadIdx.x; i < nt; i += blockDim.x) {
         const T v = tiles[b][i];
         ProbeOne<WIDE>(tab, cap, S::Key(v), S::Row(v), st, out, out_cap, counter);
       }
-      // begins with a barrier: the tile's reads are done before its buffer
-      // is reused
+      // begins with a barrier: this tile's (and at the partition's end its
+      // table's) reads are done before those buffers are refilled
       FlushPairs(st, out, out_cap, counter);
+      j++;
     }
+    if (fits) tb ^= 1;
+    p = np;
+  }
+  if (failed && threadIdx.x == 0) {
+    // every copy still in flight into this CTA's shared memory lands (or
+    // its bounded wait gives up) before the CTA leaves
+    for (int b = 0; b < 4; b++)
+      for (; waited[b] < issued[b]; waited[b]++) BarWait(&bar[b], waited[b] & 1);
   }
   FlushPairs(st, out, out_cap, counter);
 }
@@ -680,7 +737,7 @@ std::unique_ptr<HashTable> HashBuild(Context& c, const std::string& table, const
     c.kernel_launches++;
     c.TimedStop();
     c.TimedStart("hash build");
-    const size_t smem = kProbeTile * slot_bytes + kSmemTableMax;
+    const size_t smem = 2 * kProbeTile * slot_bytes + kSmemTableMax;
     const int pgrid = std::min(parts, c.num_sms * 1);
     if (ht->wide) {
       KDB_CUDA(cudaFuncSetAttribute(BuildParts<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
@@ -758,7 +815,7 @@ std::unique_ptr<Pairs> HashProbe(Context& c, const HashTable& ht, const std::str
                                                           static_cast<const unsigned long long*>(ht.slots), tcap, out,
                                                           cap, counter);
       } else {
-        const size_t smem = 2 * kProbeTile * slot_bytes + kSmemTableMax;
+        const size_t smem = 2 * kProbeTile * slot_bytes + 2 * kTableBuf;
         const int pgrid = std::min(parts, c.num_sms);
         if (ht.wide) {
           KDB_CUDA(cudaFuncSetAttribute(ProbeParts<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,

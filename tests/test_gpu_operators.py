@@ -132,8 +132,12 @@ def _key_table(name, keys, nulls=None, dtype=np.int32, tname="INT"):
     return t
 
 
-@pytest.mark.parametrize("fanout", [1, 64, 1024, 0])
-@pytest.mark.parametrize("nb,np_,dup", [(1, 1, 1), (1000, 5000, 1), (150_000, 600_000, 1), (40_000, 200_000, 4)])
+# (262,000 build rows over 64 partitions straddle the size at which a
+# probe-side sub-table still fits a shared-memory table buffer; with 16
+# partitions none fits and they are probed in HBM)
+@pytest.mark.parametrize("fanout", [1, 16, 64, 1024, 0])
+@pytest.mark.parametrize("nb,np_,dup", [(1, 1, 1), (1000, 5000, 1), (150_000, 600_000, 1), (40_000, 200_000, 4),
+                                        (262_000, 600_000, 1)])
 def test_hash_join_matches_numpy(engine, fanout, nb, np_, dup):
     from kushdb_b200.operators import HashTable
     rng = np.random.default_rng(nb + np_)
