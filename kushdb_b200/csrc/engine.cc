@@ -628,7 +628,9 @@ void Context::Launch(CUfunction f, int grid, int block, const KArgs& args, size_
   kernel_launches++;
   if (dry) return;
   void* params[] = {const_cast<KArgs*>(&args)};
-  if (smem > 48 * 1024)
+  // static plus dynamic shared memory above 48 KB needs the opt-in, also
+  // when the dynamic part alone is smaller
+  if (smem > 0)
     CuCheck(g_drv.FuncSetAttribute(f, CU_FUNC_ATTRIBUTE_MAX_DYNAMIC_SHARED_SIZE_BYTES,
                                    static_cast<int>(smem)),
             "cuFuncSetAttribute");
