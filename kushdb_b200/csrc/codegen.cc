@@ -1042,24 +1042,33 @@ void Executor::EmitStream(KernelSource& ks, ExprGen& eg, const Operator& op, con
         // With prefetch (default), the next iteration's vectors are loaded
         // before this iteration's rows are processed, so a warp keeps two
         // iterations of loads in flight.
-        const bool prefetch = !ctx_.OptStr("KDB_NO_SCAN_PREFETCH");
+        // KDB_SCAN_BATCH=B (B > 1, not on a probe side): B vectors per
+        // thread and iteration (vectors q, q + stride, ..., so each load
+        // instruction stays coalesced), all loaded before any is processed,
+        // instead of the one-vector prefetch
+        const char* batch_opt = ctx_.OptStr("KDB_SCAN_BATCH");
+        const int VB = (batch_opt && !probe_side) ? std::max(1, std::min(8, std::atoi(batch_opt))) : 1;
+        const std::string R = std::to_string(4 * VB);
+        const bool prefetch = VB == 1 && !ctx_.OptStr("KDB_NO_SCAN_PREFETCH");
         ks.L("const int64_t nrows = (int64_t)" + n + ";");
         ks.L("const int64_t qstride = (int64_t)gridDim.x * blockDim.x;");
         std::vector<std::string> arr(cols.size()), narr(cols.size()), parr(cols.size()), pnarr(cols.size());
-        // loads of the 4 rows at `qv` into the arrays `dst` / `ndst`
+        // loads of the 4 rows of vector `qv` into the arrays `dst` / `ndst`
+        // from element `off` on
         auto fetch = [&](const std::string& qv, const std::vector<std::string>& dst,
-                         const std::vector<std::string>& ndst) {
+                         const std::vector<std::string>& ndst, int off = 0) {
           ks.Open("");
           ks.L("const int64_t fb = (" + qv + ") * 4;");
           ks.L("const bool ffull = fb + 4 <= nrows;");
+          const std::string o = off ? " + " + std::to_string(off) : "";
           for (size_t k = 0; k < cols.size(); k++) {
             const DevColumn& c = *cols[k];
             std::string st = StoreType(c.type.id);
-            ks.L("if (ffull) kdb_ld4(" + dp[k] + ", fb, " + dst[k] + "); else for (int u = 0; u < 4; u++) " + dst[k] +
-                 "[u] = fb + u < nrows ? " + dp[k] + "[fb + u] : (" + st + ")0;");
+            ks.L("if (ffull) kdb_ld4(" + dp[k] + ", fb, " + dst[k] + o + "); else for (int u = 0; u < 4; u++) (" +
+                 dst[k] + o + ")[u] = fb + u < nrows ? " + dp[k] + "[fb + u] : (" + st + ")0;");
             if (!np[k].empty())
-              ks.L("if (ffull) kdb_ld4(" + np[k] + ", fb, " + ndst[k] + "); else for (int u = 0; u < 4; u++) " +
-                   ndst[k] + "[u] = fb + u < nrows ? " + np[k] + "[fb + u] : (int8_t)0;");
+              ks.L("if (ffull) kdb_ld4(" + np[k] + ", fb, " + ndst[k] + o + "); else for (int u = 0; u < 4; u++) (" +
+                   ndst[k] + o + ")[u] = fb + u < nrows ? " + np[k] + "[fb + u] : (int8_t)0;");
           }
           ks.Close();
         };
@@ -1077,14 +1086,15 @@ void Executor::EmitStream(KernelSource& ks, ExprGen& eg, const Operator& op, con
           fetch("q0", parr, pnarr);
           ks.Close();
         }
-        ks.Open("for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q * 4 < nrows; q += qstride)");
+        ks.Open("for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q * 4 < nrows; q += qstride * " +
+                std::to_string(VB) + ")");
         ks.L("const int64_t base = q * 4;");
         for (size_t k = 0; k < cols.size(); k++) {
           arr[k] = ks.Fresh("L");
-          ks.L(StoreType(cols[k]->type.id) + " " + arr[k] + "[4];");
+          ks.L(StoreType(cols[k]->type.id) + " " + arr[k] + "[" + R + "];");
           if (!np[k].empty()) {
             narr[k] = ks.Fresh("N");
-            ks.L("int8_t " + narr[k] + "[4];");
+            ks.L("int8_t " + narr[k] + "[" + R + "];");
           }
         }
         if (prefetch) {
@@ -1096,7 +1106,7 @@ void Executor::EmitStream(KernelSource& ks, ExprGen& eg, const Operator& op, con
           fetch("q + qstride", parr, pnarr);
           ks.Close();
         } else {
-          fetch("q", arr, narr);
+          for (int b = 0; b < VB; b++) fetch("q + qstride * " + std::to_string(b), arr, narr, 4 * b);
         }
         if (vec_probe) {
           // the vector's 4 join-filter words, then the first table slots of
@@ -1132,8 +1142,8 @@ void Executor::EmitStream(KernelSource& ks, ExprGen& eg, const Operator& op, con
           if (static_cast<int>(k) == ak) ahead_key_var_ = scan[k].v;
         };
         ks.L("#pragma unroll");
-        ks.Open("for (int u = 0; u < 4; u++)");
-        ks.L("const int64_t r = base + u;");
+        ks.Open("for (int u = 0; u < " + R + "; u++)");
+        ks.L(VB == 1 ? "const int64_t r = base + u;" : "const int64_t r = base + (int64_t)(u >> 2) * qstride * 4 + (u & 3);");
         ks.Open("if (r < nrows)");
       } else {
         // On a join's probe side (one row per thread and iteration) the next
@@ -2186,26 +2196,33 @@ MatBuffer Executor::RunGroupByDense(const Operator& op, const std::vector<AggPla
   words.push_back({WordKind::MinU64, "~0ULL", "uint64_t"});
   const int W = static_cast<int>(words.size());
   const int64_t K = D * W;
-  // block size and the launch-bounds occupancy hint (env overrides for tuning)
-  // (64 threads, 6 CTAs per SM: measured best on the Q1 shape among 64/128
-  // threads and 2-8 CTAs per SM)
   auto opt_int = [&](const char* name, int dflt) {
     const char* v = ctx_.OptStr(name);
     return v ? std::atoi(v) : dflt;
   };
+  // Accumulators in registers (every row updates every group's words under a
+  // predicate) while groups x words <= 64: 256-thread CTAs, one per SM, so
+  // a thread may hold them all plus two iterations of loads (measured on
+  // the Q1 shape, 42 words: 51.7 us against 53.8 us for the shared-memory
+  // form).  Beyond that, per-thread shared-memory slots indexed by the group
+  // id (a row touches only its own group's words) in 64-thread CTAs, 6 per
+  // SM.  KDB_DENSE_SMEM=0/1 forces either; KDB_DENSE_BLOCK/MINB/GRID set
+  // the shape.
   // KDB_DENSE_TMA: the scan's tiles come into shared memory by TMA bulk
   // copies (persistent CTAs, KDB_TMA_CTAS per SM of KDB_TMA_BLOCK threads,
-  // KDB_TMA_STAGES tiles of KDB_TMA_TILE rows in flight)
+  // KDB_TMA_STAGES tiles of KDB_TMA_TILE rows in flight), with either kind
+  // of accumulator.  Measured on the Q1 shape with shared-memory
+  // accumulators it is slower (78-131 us over the shapes tried, against
+  // 52 us; 8 warps per SM spend their issue slots on the accumulators'
+  // shared-memory read-modify-write chains).
   const bool want_tma = ctx_.OptStr("KDB_DENSE_TMA") != nullptr && Streamable(op.child());
-  const int block = want_tma ? opt_int("KDB_TMA_BLOCK", 128) : opt_int("KDB_DENSE_BLOCK", 64);
-  const int min_blocks = want_tma ? opt_int("KDB_TMA_CTAS", 2) : opt_int("KDB_DENSE_MINB", 6);
-  const int grid_per_sm = want_tma ? opt_int("KDB_TMA_CTAS", 2) : opt_int("KDB_DENSE_GRID", 6);
-  // Accumulators in registers (every row updates every group's words under a
-  // predicate) or, for larger groups x words, in per-thread shared-memory
-  // slots indexed by the group id (a row touches only its own group's words).
   const char* smem_env = ctx_.OptStr("KDB_DENSE_SMEM");
+  const bool want_smem = smem_env ? std::atoi(smem_env) != 0 : K > 64;
+  const int block = want_tma ? opt_int("KDB_TMA_BLOCK", 128) : opt_int("KDB_DENSE_BLOCK", want_smem ? 64 : 256);
+  const int min_blocks = want_tma ? opt_int("KDB_TMA_CTAS", 2) : opt_int("KDB_DENSE_MINB", want_smem ? 6 : 1);
+  const int grid_per_sm = want_tma ? opt_int("KDB_TMA_CTAS", 2) : opt_int("KDB_DENSE_GRID", want_smem ? 6 : 1);
   const bool smem_fits = K * block * 8 <= 48 * 1024;  // static shared memory limit
-  const bool in_smem = smem_fits && (smem_env ? std::atoi(smem_env) != 0 : K > 16);
+  const bool in_smem = smem_fits && want_smem;
 
   auto reg = [&](int64_t g, int w) { return "a" + std::to_string(g) + "_" + std::to_string(w); };
   auto combine = [&](WordKind k, const std::string& a, const std::string& b) -> std::string {
@@ -2317,7 +2334,7 @@ MatBuffer Executor::RunGroupByDense(const Operator& op, const std::vector<AggPla
       }
     }
   };
-  if (want_tma && in_smem) {
+  if (want_tma) {
     tma_tile_ = opt_int("KDB_TMA_TILE", 512);
     tma_stages_ = opt_int("KDB_TMA_STAGES", 3);
   }
@@ -2398,19 +2415,6 @@ MatBuffer Executor::RunGroupByDense(const Operator& op, const std::vector<AggPla
     for (int64_t k = 0; k < K; k++) kinds[k] = words[k % W].kind;
     EmitPartialReduce(fk, FP, GW, static_cast<int>(K), kinds);
   }
-  fk.Open("if (threadIdx.x == 0)");
-  fk.L("int32_t ng = 0;");
-  fk.Open("for (int32_t g = 0; g < " + std::to_string(D) + "; g++)");
-  fk.Open("if ((int64_t)tot[g * " + std::to_string(W) + " + " + std::to_string(rows_w) + "] > 0)");
-  // insertion by first position
-  fk.L("int32_t j = ng++;");
-  fk.L("uint64_t fg = tot[g * " + std::to_string(W) + " + " + std::to_string(first_w) + "];");
-  fk.L("while (j > 0 && tot[order[j - 1] * " + std::to_string(W) + " + " + std::to_string(first_w) +
-       "] > fg) { order[j] = order[j - 1]; j--; }");
-  fk.L("order[j] = g;");
-  fk.Close();
-  fk.Close();
-  fk.L("*" + NG + " = (uint64_t)ng;");
   // A parent ORDER BY whose keys are all enum GROUP BY keys is done here:
   // the groups, in stream order, are re-ranked by the ORDER BY comparator
   // (enum string order, NULLs after values, ascending or descending) with
@@ -2435,6 +2439,35 @@ MatBuffer Executor::RunGroupByDense(const Operator& op, const std::vector<AggPla
       sort_asc.push_back(order_by->asc[k] ? 1 : 0);
     }
   }
+  const bool fuse_order_pre = !sort_key.empty();
+  // the sort keys' enum string ranks, staged in shared memory by all
+  // threads (thread 0's comparisons below then wait on no global load)
+  std::vector<std::string> rank_smem(op.group_by.size());
+  if (fuse_order_pre) {
+    for (int k : sort_key) {
+      if (!rank_smem[k].empty()) continue;
+      const std::string name = "kdb_rk" + std::to_string(k);
+      const int64_t card = static_cast<int64_t>(kl.card[k]);
+      fk.L("__shared__ int32_t " + name + "[" + std::to_string(std::max<int64_t>(card, 1)) + "];");
+      fk.L("for (int i = threadIdx.x; i < " + std::to_string(card) + "; i += blockDim.x) " + name + "[i] = " +
+           fg.EnumRank(op.group_by[k]->type, "i") + ";");
+      rank_smem[k] = name;
+    }
+    fk.L("__syncthreads();");
+  }
+  fk.Open("if (threadIdx.x == 0)");
+  fk.L("int32_t ng = 0;");
+  fk.Open("for (int32_t g = 0; g < " + std::to_string(D) + "; g++)");
+  fk.Open("if ((int64_t)tot[g * " + std::to_string(W) + " + " + std::to_string(rows_w) + "] > 0)");
+  // insertion by first position
+  fk.L("int32_t j = ng++;");
+  fk.L("uint64_t fg = tot[g * " + std::to_string(W) + " + " + std::to_string(first_w) + "];");
+  fk.L("while (j > 0 && tot[order[j - 1] * " + std::to_string(W) + " + " + std::to_string(first_w) +
+       "] > fg) { order[j] = order[j - 1]; j--; }");
+  fk.L("order[j] = g;");
+  fk.Close();
+  fk.Close();
+  fk.L("*" + NG + " = (uint64_t)ng;");
   const bool fuse_order = !sort_key.empty();
   if (fuse_order) {
     // digit of key k of group g, and its enum string rank (NULL: -1)
@@ -2443,7 +2476,7 @@ MatBuffer Executor::RunGroupByDense(const Operator& op, const std::vector<AggPla
       for (int j = 0; j < k; j++) stride *= static_cast<int64_t>(kl.card[j] + (kl.nullable[j] ? 1 : 0));
       const int64_t base = static_cast<int64_t>(kl.card[k] + (kl.nullable[k] ? 1 : 0));
       const std::string digit = "((" + g + " / " + std::to_string(stride) + ") % " + std::to_string(base) + ")";
-      const std::string rank = "(int64_t)" + fg.EnumRank(op.group_by[k]->type, "(int32_t)" + digit);
+      const std::string rank = "(int64_t)" + rank_smem[k] + "[(int32_t)" + digit + "]";
       if (!kl.nullable[k]) return rank;
       return "(" + digit + " == " + std::to_string(kl.card[k]) + " ? (int64_t)-1 : " + rank + ")";
     };

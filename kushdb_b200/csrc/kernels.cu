@@ -395,10 +395,14 @@ __device__ __forceinline__ void SortNetwork(SortItem (&x)[N]) {
 // every thread sorts ITEMS items in registers, then rounds of merge path in
 // shared memory double the sorted runs from ITEMS to TILE items.  Missing
 // items of the last tile are maximal padding and never written.
+// Tiles above 2048 items keep their items in dynamic shared memory.
 template <int TILE, int ITEMS>
 __global__ void __launch_bounds__(TILE / ITEMS) BlockSortItems(const SortItem* in, SortItem* out, int64_t n) {
   constexpr int kThreads = TILE / ITEMS;
-  __shared__ SortItem s[PaddedTile<TILE>()];
+  constexpr bool kDynamic = TILE > 2048;
+  extern __shared__ __align__(16) unsigned char sort_dyn[];
+  __shared__ SortItem s_static[kDynamic ? 1 : PaddedTile<TILE>()];
+  SortItem* s = kDynamic ? reinterpret_cast<SortItem*>(sort_dyn) : s_static;
   const int64_t base = static_cast<int64_t>(blockIdx.x) * TILE;
   const int cnt = static_cast<int>(n - base < TILE ? n - base : TILE);
   for (int i = threadIdx.x; i < TILE; i += kThreads)
@@ -581,7 +585,13 @@ struct SortShape {
 
 template <int TILE, int ITEMS>
 void LaunchBlockSort(const SortItem* in, SortItem* out, int64_t n, cudaStream_t s) {
-  BlockSortItems<TILE, ITEMS><<<static_cast<unsigned>((n + TILE - 1) / TILE), TILE / ITEMS, 0, s>>>(in, out, n);
+  const int dyn = TILE > 2048 ? static_cast<int>(sizeof(SortItem)) * PaddedTile<TILE>() : 0;
+  // set once, on the first (uncaptured) launch; replays reuse the attribute
+  static const bool attr = dyn == 0 || cudaFuncSetAttribute(BlockSortItems<TILE, ITEMS>,
+                                                           cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                           dyn) == cudaSuccess;
+  (void)attr;
+  BlockSortItems<TILE, ITEMS><<<static_cast<unsigned>((n + TILE - 1) / TILE), TILE / ITEMS, dyn, s>>>(in, out, n);
 }
 template <int TILE, int ITEMS>
 void LaunchMerge(const SortItem* in, SortItem* out, int64_t n, int64_t w, cudaStream_t s) {
@@ -796,6 +806,9 @@ void Context::MergeSortItems(void* items, int64_t n, Arena& arena) {
   SortShapes(*this, &bs, &ms);
   auto block_sort = [&]() -> void (*)(const SortItem*, SortItem*, int64_t, cudaStream_t) {
     switch (bs.tile * 16 + bs.items) {
+      case 8192 * 16 + 8: return LaunchBlockSort<8192, 8>;
+      case 4096 * 16 + 4: return LaunchBlockSort<4096, 4>;
+      case 4096 * 16 + 8: return LaunchBlockSort<4096, 8>;
       case 2048 * 16 + 2: return LaunchBlockSort<2048, 2>;
       case 2048 * 16 + 4: return LaunchBlockSort<2048, 4>;
       case 2048 * 16 + 8: return LaunchBlockSort<2048, 8>;

@@ -45,6 +45,7 @@ namespace ops {
 namespace {
 
 constexpr int kBlock = 256;
+constexpr int kPartBlock = 1024;                 // threads of a partitioned build / probe CTA
 constexpr int kMaxPartBits = 13;                 // at most 8192 sub-tables
 constexpr size_t kSmemTableMax = 128 << 10;      // a sub-table built in shared memory
 constexpr size_t kTableBuf = 64 << 10;           // a probe-side sub-table buffer (two of them)
@@ -52,7 +53,7 @@ constexpr int kProbeTile = 2048;                 // probe tuples per bulk-copied
 constexpr uint32_t kWaitLimit = 1u << 24;        // bounded mbarrier waits
 constexpr int kErrWait = 1;                      // device error word: a wait gave up
 constexpr int kErrFull = 2;                      // a table ran out of empty slots
-constexpr unsigned kOutStage = 2048;             // pairs a CTA stages before one global append
+constexpr unsigned kOutStage = 4096;             // pairs a CTA stages before one global append
 
 // ---- keys --------------------------------------------------------------------
 struct KeyCol {
@@ -305,7 +306,7 @@ __global__ void BuildFlat(KeyCol key, const int32_t* __restrict__ sel, int64_t n
 // fits shared memory is built there with shared-memory CAS and written out
 // with coalesced stores, a larger one is built in place in HBM.
 template <bool WIDE>
-__global__ void __launch_bounds__(kBlock) BuildParts(const typename Slot<WIDE>::T* __restrict__ staged,
+__global__ void __launch_bounds__(kPartBlock) BuildParts(const typename Slot<WIDE>::T* __restrict__ staged,
                                                      const unsigned long long* __restrict__ stage_off,
                                                      const unsigned* __restrict__ hist,
                                                      const unsigned long long* __restrict__ slot_off, int parts,
@@ -483,7 +484,7 @@ __global__ void __launch_bounds__(kBlock) ProbeFlat(KeyCol key, const int32_t* _
 // two table buffers, so a partition's table copy overlaps the probing of the
 // one before.  Sub-tables larger than a table buffer are probed in HBM.
 template <bool WIDE>
-__global__ void __launch_bounds__(kBlock) ProbeParts(const typename Slot<WIDE>::T* __restrict__ staged,
+__global__ void __launch_bounds__(kPartBlock) ProbeParts(const typename Slot<WIDE>::T* __restrict__ staged,
                                                      const unsigned long long* __restrict__ stage_off,
                                                      const unsigned* __restrict__ hist,
                                                      const typename Slot<WIDE>::T* __restrict__ slots,
@@ -570,9 +571,11 @@ __global__ void __launch_bounds__(kBlock) ProbeParts(const typename Slot<WIDE>::
         const T v = tiles[b][i];
         ProbeOne<WIDE>(tab, cap, S::Key(v), S::Row(v), st, out, out_cap, counter);
       }
-      // begins with a barrier: this tile's (and at the partition's end its
-      // table's) reads are done before those buffers are refilled
-      FlushPairs(st, out, out_cap, counter);
+      // a barrier: this tile's (and at the partition's end its table's)
+      // reads are done before those buffers are refilled; the staged pairs
+      // go out once the stage is half full (a tile adds at most kProbeTile
+      // pairs per distinct build key)
+      if (__syncthreads_or(threadIdx.x == 0 && st.count >= kOutStage / 2)) FlushPairs(st, out, out_cap, counter);
       j++;
     }
     if (fits) tb ^= 1;
@@ -741,11 +744,11 @@ std::unique_ptr<HashTable> HashBuild(Context& c, const std::string& table, const
     const int pgrid = std::min(parts, c.num_sms * 1);
     if (ht->wide) {
       KDB_CUDA(cudaFuncSetAttribute(BuildParts<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
-      BuildParts<true><<<pgrid, kBlock, smem, c.stream>>>(static_cast<const ulonglong2*>(staged), stage_off, hist,
+      BuildParts<true><<<pgrid, kPartBlock, smem, c.stream>>>(static_cast<const ulonglong2*>(staged), stage_off, hist,
                                                           ht->slot_off, parts, static_cast<ulonglong2*>(ht->slots), err);
     } else {
       KDB_CUDA(cudaFuncSetAttribute(BuildParts<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
-      BuildParts<false><<<pgrid, kBlock, smem, c.stream>>>(static_cast<const unsigned long long*>(staged), stage_off,
+      BuildParts<false><<<pgrid, kPartBlock, smem, c.stream>>>(static_cast<const unsigned long long*>(staged), stage_off,
                                                            hist, ht->slot_off, parts,
                                                            static_cast<unsigned long long*>(ht->slots), err);
     }
@@ -820,13 +823,13 @@ std::unique_ptr<Pairs> HashProbe(Context& c, const HashTable& ht, const std::str
         if (ht.wide) {
           KDB_CUDA(cudaFuncSetAttribute(ProbeParts<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                         static_cast<int>(smem)));
-          ProbeParts<true><<<pgrid, kBlock, smem, c.stream>>>(static_cast<const ulonglong2*>(staged), stage_off, hist,
+          ProbeParts<true><<<pgrid, kPartBlock, smem, c.stream>>>(static_cast<const ulonglong2*>(staged), stage_off, hist,
                                                               static_cast<const ulonglong2*>(ht.slots), ht.slot_off,
                                                               parts, out, cap, counter, err);
         } else {
           KDB_CUDA(cudaFuncSetAttribute(ProbeParts<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                         static_cast<int>(smem)));
-          ProbeParts<false><<<pgrid, kBlock, smem, c.stream>>>(
+          ProbeParts<false><<<pgrid, kPartBlock, smem, c.stream>>>(
               static_cast<const unsigned long long*>(staged), stage_off, hist,
               static_cast<const unsigned long long*>(ht.slots), ht.slot_off, parts, out, cap, counter, err);
         }

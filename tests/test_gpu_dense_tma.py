@@ -1,9 +1,9 @@
 """The small-domain group-by with its scan staged through shared memory by
-TMA bulk copies (KDB_DENSE_TMA) against the oracle and against the
-register-load scan: row counts around the tile size (ragged last tiles,
-fewer rows than one 16-byte unit), nullable keys and measures (their null
-arrays staged too), BOOLEAN, SMALLINT, ENUM and DATE columns, and several
-tile / stage shapes."""
+TMA bulk copies (KDB_DENSE_TMA; register and shared-memory accumulators)
+against the oracle and against the register-load scan: row counts around
+the tile size (ragged last tiles, fewer rows than one 16-byte unit),
+nullable keys and measures (their null arrays staged too), BOOLEAN,
+SMALLINT, ENUM and DATE columns, and several tile / stage shapes."""
 
 import numpy as np
 import pytest
@@ -70,8 +70,9 @@ def _run(engine, plan, opts):
 
 
 @pytest.mark.parametrize("rows", [1, 3, 15, 511, 512, 513, 4099, 200_003])
-@pytest.mark.parametrize("shape", [{}, {"KDB_TMA_TILE": "256", "KDB_TMA_STAGES": "2"},
-                                   {"KDB_TMA_TILE": "1024", "KDB_TMA_STAGES": "4", "KDB_TMA_BLOCK": "64"}])
+@pytest.mark.parametrize("shape", [{}, {"KDB_DENSE_SMEM": "1"}, {"KDB_TMA_TILE": "256", "KDB_TMA_STAGES": "2"},
+                                   {"KDB_TMA_TILE": "1024", "KDB_TMA_STAGES": "4", "KDB_TMA_BLOCK": "64",
+                                    "KDB_DENSE_SMEM": "1"}])
 def test_tma_dense_group_by_matches_oracle(engine, rows, shape):
     from oracle import Oracle
     t = _table(f"tma_{rows}", rows, rows)
