@@ -726,6 +726,8 @@ class Executor {
   // column loads, bound such a pipeline, and the 4-row vector's registers
   // cost occupancy)
   bool probe_side_scan_ = false;
+  // set while materialising a join's build side (rows in any order)
+  bool build_side_mat_ = false;
   // TMA-staged scan: set by a consumer before emitting its scan (rows per
   // tile, stages); the scan reports the dynamic shared memory it needs in
   // tma_smem_ (0 when it fell back to register loads).
@@ -1578,7 +1580,12 @@ JoinTable Executor::BuildGroupedIndex(const MatBuffer& m, int key_col) {
 
 void Executor::BuildJoin(const Operator& op) {
   if (joins_.count(&op)) return;
+  // a join's build rows need no particular buffer order (their stream
+  // positions travel with them): with KDB_BUILD_MAT_ATOMIC the build side
+  // is written in one pass with block-level slot claims
+  build_side_mat_ = ctx_.OptStr("KDB_BUILD_MAT_ATOMIC") != nullptr && Streamable(op.child(0));
   MatBuffer left = Materialize(op.child(0));
+  build_side_mat_ = false;
   std::vector<int> keys;
   for (const auto& k : op.left_keys) {
     if (k->kind != ExprKind::ColRef) throw Error(-5, "hash join keys must be column references");
@@ -1639,7 +1646,9 @@ MatBuffer Executor::MaterializeStream(const Operator& op, const uint32_t* order,
     return out;
   }
   Prepare(op);
-  if (!StreamHasJoin(op) && !ctx_.OptStr("KDB_MATERIALIZE_ATOMIC")) return MaterializeCounted(op);
+  const bool any_order = build_side_mat_;
+  build_side_mat_ = false;
+  if (!StreamHasJoin(op) && !any_order && !ctx_.OptStr("KDB_MATERIALIZE_ATOMIC")) return MaterializeCounted(op);
   int64_t cap = RowBound(op);
   for (int attempt = 0; attempt < 3; attempt++) {
     const auto mark = ctx_.RecordMark();
@@ -2201,13 +2210,14 @@ MatBuffer Executor::RunGroupByDense(const Operator& op, const std::vector<AggPla
     return v ? std::atoi(v) : dflt;
   };
   // Accumulators in registers (every row updates every group's words under a
-  // predicate) while groups x words <= 64: 256-thread CTAs, one per SM, so
+  // predicate) while groups x words <= 64: 128-thread CTAs, two per SM, so
   // a thread may hold them all plus two iterations of loads (measured on
-  // the Q1 shape, 42 words: 51.7 us against 53.8 us for the shared-memory
-  // form).  Beyond that, per-thread shared-memory slots indexed by the group
-  // id (a row touches only its own group's words) in 64-thread CTAs, 6 per
-  // SM.  KDB_DENSE_SMEM=0/1 forces either; KDB_DENSE_BLOCK/MINB/GRID set
-  // the shape.
+  // the Q1 shape, 42 words: 49.6 us, against 51.5 us for 256 x 1, 156 us
+  // for 512 x 1 and 53.6 us for the shared-memory form).  Beyond that,
+  // per-thread shared-memory slots indexed by the group id (a row touches
+  // only its own group's words) in 64-thread CTAs, 6 per SM.
+  // KDB_DENSE_SMEM=0/1 forces either; KDB_DENSE_BLOCK/MINB/GRID set the
+  // shape.
   // KDB_DENSE_TMA: the scan's tiles come into shared memory by TMA bulk
   // copies (persistent CTAs, KDB_TMA_CTAS per SM of KDB_TMA_BLOCK threads,
   // KDB_TMA_STAGES tiles of KDB_TMA_TILE rows in flight), with either kind
@@ -2218,9 +2228,9 @@ MatBuffer Executor::RunGroupByDense(const Operator& op, const std::vector<AggPla
   const bool want_tma = ctx_.OptStr("KDB_DENSE_TMA") != nullptr && Streamable(op.child());
   const char* smem_env = ctx_.OptStr("KDB_DENSE_SMEM");
   const bool want_smem = smem_env ? std::atoi(smem_env) != 0 : K > 64;
-  const int block = want_tma ? opt_int("KDB_TMA_BLOCK", 128) : opt_int("KDB_DENSE_BLOCK", want_smem ? 64 : 256);
-  const int min_blocks = want_tma ? opt_int("KDB_TMA_CTAS", 2) : opt_int("KDB_DENSE_MINB", want_smem ? 6 : 1);
-  const int grid_per_sm = want_tma ? opt_int("KDB_TMA_CTAS", 2) : opt_int("KDB_DENSE_GRID", want_smem ? 6 : 1);
+  const int block = want_tma ? opt_int("KDB_TMA_BLOCK", 128) : opt_int("KDB_DENSE_BLOCK", want_smem ? 64 : 128);
+  const int min_blocks = want_tma ? opt_int("KDB_TMA_CTAS", 2) : opt_int("KDB_DENSE_MINB", want_smem ? 6 : 2);
+  const int grid_per_sm = want_tma ? opt_int("KDB_TMA_CTAS", 2) : opt_int("KDB_DENSE_GRID", want_smem ? 6 : 2);
   const bool smem_fits = K * block * 8 <= 48 * 1024;  // static shared memory limit
   const bool in_smem = smem_fits && want_smem;
 
@@ -2455,6 +2465,10 @@ MatBuffer Executor::RunGroupByDense(const Operator& op, const std::vector<AggPla
     }
     fk.L("__syncthreads();");
   }
+  // thread 0 orders the present groups (shared memory only); all threads
+  // then write one output row each
+  fk.L("__shared__ int32_t kdb_ng;");
+  fk.L("__shared__ int32_t kdb_fin[" + std::to_string(D) + "];");
   fk.Open("if (threadIdx.x == 0)");
   fk.L("int32_t ng = 0;");
   fk.Open("for (int32_t g = 0; g < " + std::to_string(D) + "; g++)");
@@ -2493,21 +2507,25 @@ MatBuffer Executor::RunGroupByDense(const Operator& op, const std::vector<AggPla
     fk.L("return kdb_tie_path((uint64_t)ra, (uint64_t)ng) < kdb_tie_path((uint64_t)rb, (uint64_t)ng);");
     fk.indent--;
     fk.L("};");
-    fk.L("int32_t fin[" + std::to_string(D) + "];");
+    fk.L("int32_t* fin = kdb_fin;");
     fk.Open("for (int32_t r = 0; r < ng; r++)");
     fk.L("int32_t j = r;");
     fk.L("while (j > 0 && kless(r, fin[j - 1])) { fin[j] = fin[j - 1]; j--; }");
     fk.L("fin[j] = r;");
     fk.Close();
   }
+  fk.L("kdb_ng = ng;");
+  fk.Close();
+  fk.L("__syncthreads();");
   std::vector<std::string> optr, onull;
   for (const auto& c : out.cols) {
     optr.push_back(fk.Ptr(c.data, StoreType(c.type.id)));
     onull.push_back(c.nullable ? fk.Ptr(c.nulls, "int8_t") : "");
   }
   std::string posp = fk.Ptr(out.pos, "uint64_t");
-  fk.Open("for (int32_t r = 0; r < ng; r++)");
-  fk.L(fuse_order ? "int64_t g = order[fin[r]];" : "int64_t g = order[r];");
+  fk.L("const int32_t ng = kdb_ng;");
+  fk.Open("for (int32_t r = threadIdx.x; r < ng; r += blockDim.x)");
+  fk.L(fuse_order ? "int64_t g = order[kdb_fin[r]];" : "int64_t g = order[r];");
   fk.L("const uint64_t* t = tot + g * " + std::to_string(W) + ";");
   fk.L("int64_t rows = (int64_t)t[" + std::to_string(rows_w) + "];");
   fk.L("uint64_t fst = t[" + std::to_string(first_w) + "];");
@@ -2551,7 +2569,6 @@ MatBuffer Executor::RunGroupByDense(const Operator& op, const std::vector<AggPla
     if (!onull[c].empty()) fk.L(onull[c] + "[r] = (" + v.n + ") ? 1 : 0;");
   }
   fk.L(posp + "[r] = (uint64_t)r;");
-  fk.Close();
   fk.Close();
   {
     std::string src = fk.Kernel("kdb_group_by_finalize", 1024);

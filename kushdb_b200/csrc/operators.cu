@@ -53,7 +53,8 @@ constexpr int kProbeTile = 2048;                 // probe tuples per bulk-copied
 constexpr uint32_t kWaitLimit = 1u << 24;        // bounded mbarrier waits
 constexpr int kErrWait = 1;                      // device error word: a wait gave up
 constexpr int kErrFull = 2;                      // a table ran out of empty slots
-constexpr unsigned kOutStage = 4096;             // pairs a CTA stages before one global append
+constexpr unsigned kOutStage = 4096;             // pairs a partitioned-probe CTA stages
+constexpr unsigned kFlatStage = 2048;            // pairs a flat-probe CTA stages
 
 // ---- keys --------------------------------------------------------------------
 struct KeyCol {
@@ -392,9 +393,11 @@ __global__ void __launch_bounds__(kPartBlock) BuildParts(const typename Slot<WID
 // stage position (one shared-memory atomic per coalesced group) and the CTA
 // appends the whole stage to the output with one global atomic.  A match
 // that finds the stage full is appended on its own.
+template <unsigned N>
 struct OutStage {
-  unsigned long long buf[kOutStage];
-  unsigned count;  // may pass kOutStage; positions from kOutStage on went direct
+  static constexpr unsigned kCap = N;
+  unsigned long long buf[N];
+  unsigned count;  // may pass N; positions from N on went direct
   unsigned long long base;
 };
 
@@ -412,22 +415,24 @@ __device__ __forceinline__ void EmitPair(unsigned long long* out, unsigned long 
   if (base < cap) out[base] = v;
 }
 
-__device__ __forceinline__ void StagePair(OutStage& st, unsigned long long* out, unsigned long long cap,
+template <typename Stage>
+__device__ __forceinline__ void StagePair(Stage& st, unsigned long long* out, unsigned long long cap,
                                           unsigned long long* counter, unsigned long long v) {
   cg::coalesced_group g = cg::coalesced_threads();
   unsigned at = 0;
   if (g.thread_rank() == 0) at = atomicAdd(&st.count, g.size());
   at = g.shfl(at, 0) + g.thread_rank();
-  if (at < kOutStage) st.buf[at] = v;
+  if (at < Stage::kCap) st.buf[at] = v;
   else EmitPair(out, cap, counter, v);
 }
 
 // Every thread of the CTA calls it: the staged pairs are appended with one
 // global atomic and the stage is emptied.
-__device__ __forceinline__ void FlushPairs(OutStage& st, unsigned long long* out, unsigned long long cap,
+template <typename Stage>
+__device__ __forceinline__ void FlushPairs(Stage& st, unsigned long long* out, unsigned long long cap,
                                            unsigned long long* counter) {
   __syncthreads();
-  const unsigned n = st.count < kOutStage ? st.count : kOutStage;
+  const unsigned n = st.count < Stage::kCap ? st.count : Stage::kCap;
   if (n > 0) {
     if (threadIdx.x == 0) st.base = atomicAdd(counter, static_cast<unsigned long long>(n));
     __syncthreads();
@@ -440,9 +445,9 @@ __device__ __forceinline__ void FlushPairs(OutStage& st, unsigned long long* out
   __syncthreads();
 }
 
-template <bool WIDE>
+template <bool WIDE, typename Stage>
 __device__ __forceinline__ void ProbeOne(const typename Slot<WIDE>::T* tab, uint64_t cap, int64_t k,
-                                         int64_t probe_row, OutStage& st, unsigned long long* out,
+                                         int64_t probe_row, Stage& st, unsigned long long* out,
                                          unsigned long long out_cap, unsigned long long* counter) {
   using S = Slot<WIDE>;
   uint64_t i = Hash32(static_cast<uint64_t>(k)) & (cap - 1);
@@ -461,7 +466,7 @@ __global__ void __launch_bounds__(kBlock) ProbeFlat(KeyCol key, const int32_t* _
                                                     const typename Slot<WIDE>::T* __restrict__ tab, uint64_t cap,
                                                     unsigned long long* __restrict__ out,
                                                     unsigned long long out_cap, unsigned long long* counter) {
-  __shared__ OutStage st;
+  __shared__ OutStage<kFlatStage> st;
   if (threadIdx.x == 0) st.count = 0;
   __syncthreads();
   const int64_t stride = static_cast<int64_t>(gridDim.x) * blockDim.x;
@@ -472,7 +477,7 @@ __global__ void __launch_bounds__(kBlock) ProbeFlat(KeyCol key, const int32_t* _
       if (!KeyNull(key, r)) ProbeOne<WIDE>(tab, cap, LoadKey(key, r), r, st, out, out_cap, counter);
     }
     // every thread's matches of this round are staged before thread 0 looks
-    if (__syncthreads_or(threadIdx.x == 0 && st.count >= kOutStage / 2)) FlushPairs(st, out, out_cap, counter);
+    if (__syncthreads_or(threadIdx.x == 0 && st.count >= kFlatStage / 2)) FlushPairs(st, out, out_cap, counter);
   }
   FlushPairs(st, out, out_cap, counter);
 }
@@ -497,7 +502,7 @@ __global__ void __launch_bounds__(kPartBlock) ProbeParts(const typename Slot<WID
   extern __shared__ __align__(128) unsigned char smem[];
   // barriers 0-1: tile ring; 2-3: table buffers
   __shared__ __align__(8) uint64_t bar[4];
-  __shared__ OutStage st;
+  __shared__ OutStage<kOutStage> st;
   T* tiles[2] = {reinterpret_cast<T*>(smem), reinterpret_cast<T*>(smem + kProbeTile * sizeof(T))};
   T* tabs[2] = {reinterpret_cast<T*>(smem + 2 * kProbeTile * sizeof(T)),
                 reinterpret_cast<T*>(smem + 2 * kProbeTile * sizeof(T) + kTableBuf)};

@@ -1,7 +1,8 @@
 """The join probe's load schedules give the oracle's results: the default
 (one row per thread, next row's columns prefetched), the 4-row vector probe
 that loads each vector's join-filter words and first slots together
-(KDB_PROBE_VEC), and the row-ahead forms (KDB_PROBE_AHEAD=1 / word), on the
+(KDB_PROBE_VEC), the row-ahead forms (KDB_PROBE_AHEAD=1 / word) and the
+build side written in one unordered pass (KDB_BUILD_MAT_ATOMIC), on the
 Q3-shape join + group-by (uniform and Zipf foreign keys), a join whose probe
 keys are nullable SMALLINTs with duplicates on the build side, and a join
 materialised without a group-by."""
@@ -16,7 +17,8 @@ from parity import compare
 
 pytestmark = pytest.mark.gpu
 
-MODES = [{}, {"KDB_PROBE_VEC": "1"}, {"KDB_PROBE_AHEAD": "1"}, {"KDB_PROBE_AHEAD": "word"}]
+MODES = [{}, {"KDB_PROBE_VEC": "1"}, {"KDB_PROBE_AHEAD": "1"}, {"KDB_PROBE_AHEAD": "word"},
+         {"KDB_BUILD_MAT_ATOMIC": "1"}]
 
 
 @pytest.fixture(scope="module")
