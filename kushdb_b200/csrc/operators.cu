@@ -55,6 +55,8 @@ constexpr int kErrWait = 1;                      // device error word: a wait ga
 constexpr int kErrFull = 2;                      // a table ran out of empty slots
 constexpr unsigned kOutStage = 4096;             // pairs a partitioned-probe CTA stages
 constexpr unsigned kFlatStage = 2048;            // pairs a flat-probe CTA stages
+constexpr int kTupCap = 3072;                    // probe tuples per partition buffer (warp-level probe)
+constexpr int kWarpStage = 64;                   // pairs a warp stages before one global append
 
 // ---- keys --------------------------------------------------------------------
 struct KeyCol {
@@ -155,6 +157,20 @@ __device__ __forceinline__ void BulkLoad(void* dst, const void* src, uint32_t by
       "l"(src), "r"(bytes), "r"(SmemAddr(bar))
       : "memory");
 }
+// Several copies completing on one barrier phase: one thread announces their
+// total bytes (the phase's one arrival), then starts each copy.
+__device__ __forceinline__ void BarExpect(uint64_t* bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(SmemAddr(bar)), "r"(bytes)
+               : "memory");
+}
+__device__ __forceinline__ void BulkCopy(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+          SmemAddr(dst)),
+      "l"(src), "r"(bytes), "r"(SmemAddr(bar))
+      : "memory");
+}
+
 // Waits for phase `parity` of `bar` to complete; false when the wait gave up.
 __device__ __forceinline__ bool BarWait(uint64_t* bar, uint32_t parity) {
   for (uint32_t it = 0; it < kWaitLimit; it++) {
@@ -595,6 +611,137 @@ __global__ void __launch_bounds__(kPartBlock) ProbeParts(const typename Slot<WID
   FlushPairs(st, out, out_cap, counter);
 }
 
+// Partitioned probe with warp-level consumption (32-bit keys).  A CTA walks
+// its partitions through two buffers, each holding a partition's sub-table
+// (when it fits) and its probe tuples (up to kTupCap per copy): while one
+// partition is probed the next one's copy is in flight.  Inside a
+// partition the warps take their tuples without CTA barriers and stage
+// their pairs per warp (one global atomic per flush); one CTA barrier per
+// partition releases its buffer.
+__global__ void __launch_bounds__(kPartBlock) ProbePartsW(const unsigned long long* __restrict__ staged,
+                                                          const unsigned long long* __restrict__ stage_off,
+                                                          const unsigned* __restrict__ hist,
+                                                          const unsigned long long* __restrict__ slots,
+                                                          const unsigned long long* __restrict__ slot_off, int parts,
+                                                          unsigned long long* __restrict__ out,
+                                                          unsigned long long out_cap, unsigned long long* counter,
+                                                          int* err) {
+  using S = Slot<false>;
+  using T = S::T;
+  constexpr size_t kBuf = kTableBuf + kTupCap * sizeof(T);
+  extern __shared__ __align__(128) unsigned char smem[];
+  __shared__ __align__(8) uint64_t bar[2];
+  __shared__ unsigned long long wst[kPartBlock / 32][kWarpStage];
+  __shared__ unsigned wcount[kPartBlock / 32];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  if (threadIdx.x == 0) {
+    for (int b = 0; b < 2; b++) BarInit(&bar[b]);
+    FenceProxyAsync();
+  }
+  if (lane == 0) wcount[warp] = 0;
+  __syncthreads();
+  uint32_t issued[2] = {0, 0}, waited[2] = {0, 0};
+  auto next_part = [&](int q) {
+    for (q += gridDim.x; q < parts && hist[q] == 0; q += gridDim.x) {
+    }
+    return q;
+  };
+  auto tab_fits = [&](int q) { return (slot_off[q + 1] - slot_off[q]) * sizeof(T) <= kTableBuf; };
+  // partition q's table (when it fits; only with the first chunk) and its
+  // tuples from c0 on into buffer b
+  auto issue = [&](int q, int b, uint64_t c0) {
+    const uint64_t count = hist[q];
+    const uint32_t n = static_cast<uint32_t>(umin64(kTupCap, count - c0));
+    const uint32_t tb = (n * sizeof(T) + 15) & ~15u;
+    const bool with_tab = c0 == 0 && tab_fits(q);
+    const uint32_t ab = with_tab ? static_cast<uint32_t>((slot_off[q + 1] - slot_off[q]) * sizeof(T)) : 0u;
+    unsigned char* base = smem + b * kBuf;
+    FenceProxyAsync();
+    BarExpect(&bar[b], ab + tb);
+    if (with_tab) BulkCopy(base, slots + slot_off[q], ab, &bar[b]);
+    BulkCopy(base + kTableBuf, staged + stage_off[q] + c0, tb, &bar[b]);
+    issued[b]++;
+  };
+  auto warp_flush = [&]() {
+    const unsigned n = wcount[warp] < kWarpStage ? wcount[warp] : kWarpStage;
+    unsigned long long base = 0;
+    if (lane == 0 && n) base = atomicAdd(counter, static_cast<unsigned long long>(n));
+    base = __shfl_sync(0xffffffffu, base, 0);
+    for (unsigned i = lane; i < n; i += 32)
+      if (base + i < out_cap) out[base + i] = wst[warp][i];
+    __syncwarp();
+    if (lane == 0) wcount[warp] = 0;
+    __syncwarp();
+  };
+  int p = blockIdx.x;
+  if (p < parts && hist[p] == 0) p = next_part(p);
+  int pn = p < parts ? next_part(p) : parts;  // the partition in the other buffer
+  if (threadIdx.x == 0) {
+    if (p < parts) issue(p, 0, 0);
+    if (pn < parts) issue(pn, 1, 0);
+  }
+  bool failed = false;
+  int b = 0;
+  while (p < parts && !failed) {
+    const uint64_t cap = slot_off[p + 1] - slot_off[p];
+    const uint64_t count = hist[p];
+    const T* tab = tab_fits(p) ? reinterpret_cast<const T*>(smem + b * kBuf) : slots + slot_off[p];
+    const T* tup = reinterpret_cast<const T*>(smem + b * kBuf + kTableBuf);
+    for (uint64_t c0 = 0; c0 < count && !failed; c0 += kTupCap) {
+      if (c0 > 0) {
+        // a partition beyond one buffer of tuples: the next chunk into the
+        // same buffer once every warp is done with this one
+        __syncthreads();
+        if (threadIdx.x == 0) issue(p, b, c0);
+      }
+      if (!BarWaitAll(&bar[b], waited[b] & 1, err)) {
+        failed = true;
+        break;
+      }
+      waited[b]++;
+      const uint32_t n = static_cast<uint32_t>(umin64(kTupCap, count - c0));
+      for (uint32_t i0 = warp * 32; i0 < n; i0 += kPartBlock) {
+        const uint32_t i = i0 + lane;
+        if (i < n) {
+          const T v = tup[i];
+          const int64_t k = S::Key(v);
+          uint64_t j = Hash32(static_cast<uint64_t>(k)) & (cap - 1);
+          for (uint64_t step = 0; step < cap; step++) {
+            const T e = tab[j];
+            if (S::Empty(e)) break;
+            if (S::Key(e) == k) {
+              const unsigned long long pair = PackPair(S::Row(v), S::Row(e));
+              cg::coalesced_group g = cg::coalesced_threads();
+              unsigned at = 0;
+              if (g.thread_rank() == 0) at = atomicAdd(&wcount[warp], g.size());
+              at = g.shfl(at, 0) + g.thread_rank();
+              if (at < static_cast<unsigned>(kWarpStage)) wst[warp][at] = pair;
+              else EmitPair(out, out_cap, counter, pair);
+            }
+            j = (j + 1) & (cap - 1);
+          }
+        }
+        __syncwarp();
+        if (wcount[warp] >= kWarpStage / 2) warp_flush();
+      }
+    }
+    if (failed) break;
+    // buffer b is free once every warp is done with it
+    __syncthreads();
+    const int pnn = pn < parts ? next_part(pn) : parts;
+    if (threadIdx.x == 0 && pnn < parts) issue(pnn, b, 0);
+    p = pn;
+    pn = pnn;
+    b ^= 1;
+  }
+  if (failed && threadIdx.x == 0) {
+    for (int k = 0; k < 2; k++)
+      for (; waited[k] < issued[k]; waited[k]++) BarWait(&bar[k], waited[k] & 1);
+  }
+  __syncwarp();
+  warp_flush();
+}
+
 __global__ void SplitPairs(const unsigned long long* __restrict__ pairs, int64_t n, int32_t* __restrict__ probe,
                            int32_t* __restrict__ build) {
   for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < n;
@@ -825,7 +972,14 @@ std::unique_ptr<Pairs> HashProbe(Context& c, const HashTable& ht, const std::str
       } else {
         const size_t smem = 2 * kProbeTile * slot_bytes + 2 * kTableBuf;
         const int pgrid = std::min(parts, c.num_sms);
-        if (ht.wide) {
+        if (!ht.wide && !c.OptStr("KDB_PROBE_PARTS_TILED")) {
+          const size_t wsmem = 2 * (kTableBuf + kTupCap * sizeof(unsigned long long));
+          KDB_CUDA(cudaFuncSetAttribute(ProbePartsW, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        static_cast<int>(wsmem)));
+          ProbePartsW<<<pgrid, kPartBlock, wsmem, c.stream>>>(static_cast<const unsigned long long*>(staged), stage_off,
+                                                             hist, static_cast<const unsigned long long*>(ht.slots),
+                                                             ht.slot_off, parts, out, cap, counter, err);
+        } else if (ht.wide) {
           KDB_CUDA(cudaFuncSetAttribute(ProbeParts<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                         static_cast<int>(smem)));
           ProbeParts<true><<<pgrid, kPartBlock, smem, c.stream>>>(static_cast<const ulonglong2*>(staged), stage_off, hist,
