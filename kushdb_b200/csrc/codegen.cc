@@ -2210,9 +2210,10 @@ MatBuffer Executor::RunGroupByDense(const Operator& op, const std::vector<AggPla
     return v ? std::atoi(v) : dflt;
   };
   // Accumulators in registers (every row updates every group's words under a
-  // predicate) while groups x words <= 64: 128-thread CTAs, two per SM, so
+  // predicate) while groups x words <= 64: 256-thread CTAs, one per SM, so
   // a thread may hold them all plus two iterations of loads (measured on
-  // the Q1 shape, 42 words: 49.6 us, against 51.5 us for 256 x 1, 156 us
+  // the Q1 shape, 42 words: 51.5 us and a 97 us query, against 49.6 us and
+  // 103 us for 128 x 2 -- twice the partials for the finalize -- 156 us
   // for 512 x 1 and 53.6 us for the shared-memory form).  Beyond that,
   // per-thread shared-memory slots indexed by the group id (a row touches
   // only its own group's words) in 64-thread CTAs, 6 per SM.
@@ -2228,9 +2229,9 @@ MatBuffer Executor::RunGroupByDense(const Operator& op, const std::vector<AggPla
   const bool want_tma = ctx_.OptStr("KDB_DENSE_TMA") != nullptr && Streamable(op.child());
   const char* smem_env = ctx_.OptStr("KDB_DENSE_SMEM");
   const bool want_smem = smem_env ? std::atoi(smem_env) != 0 : K > 64;
-  const int block = want_tma ? opt_int("KDB_TMA_BLOCK", 128) : opt_int("KDB_DENSE_BLOCK", want_smem ? 64 : 128);
-  const int min_blocks = want_tma ? opt_int("KDB_TMA_CTAS", 2) : opt_int("KDB_DENSE_MINB", want_smem ? 6 : 2);
-  const int grid_per_sm = want_tma ? opt_int("KDB_TMA_CTAS", 2) : opt_int("KDB_DENSE_GRID", want_smem ? 6 : 2);
+  const int block = want_tma ? opt_int("KDB_TMA_BLOCK", 128) : opt_int("KDB_DENSE_BLOCK", want_smem ? 64 : 256);
+  const int min_blocks = want_tma ? opt_int("KDB_TMA_CTAS", 2) : opt_int("KDB_DENSE_MINB", want_smem ? 6 : 1);
+  const int grid_per_sm = want_tma ? opt_int("KDB_TMA_CTAS", 2) : opt_int("KDB_DENSE_GRID", want_smem ? 6 : 1);
   const bool smem_fits = K * block * 8 <= 48 * 1024;  // static shared memory limit
   const bool in_smem = smem_fits && want_smem;
 

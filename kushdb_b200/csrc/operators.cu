@@ -170,6 +170,14 @@ __device__ __forceinline__ void BulkCopy(void* dst, const void* src, uint32_t by
       "l"(src), "r"(bytes), "r"(SmemAddr(bar))
       : "memory");
 }
+// The same as several copies of at most `piece` bytes (a multiple of 16),
+// all in flight together.
+__device__ __forceinline__ void BulkCopyPieces(void* dst, const void* src, uint32_t bytes, uint64_t* bar,
+                                               uint32_t piece) {
+  for (uint32_t o = 0; o < bytes; o += piece)
+    BulkCopy(static_cast<char*>(dst) + o, static_cast<const char*>(src) + o, bytes - o < piece ? bytes - o : piece,
+             bar);
+}
 
 // Waits for phase `parity` of `bar` to complete; false when the wait gave up.
 __device__ __forceinline__ bool BarWait(uint64_t* bar, uint32_t parity) {
@@ -625,7 +633,7 @@ __global__ void __launch_bounds__(kPartBlock) ProbePartsW(const unsigned long lo
                                                           const unsigned long long* __restrict__ slot_off, int parts,
                                                           unsigned long long* __restrict__ out,
                                                           unsigned long long out_cap, unsigned long long* counter,
-                                                          int* err) {
+                                                          int* err, uint32_t piece) {
   using S = Slot<false>;
   using T = S::T;
   constexpr size_t kBuf = kTableBuf + kTupCap * sizeof(T);
@@ -658,8 +666,8 @@ __global__ void __launch_bounds__(kPartBlock) ProbePartsW(const unsigned long lo
     unsigned char* base = smem + b * kBuf;
     FenceProxyAsync();
     BarExpect(&bar[b], ab + tb);
-    if (with_tab) BulkCopy(base, slots + slot_off[q], ab, &bar[b]);
-    BulkCopy(base + kTableBuf, staged + stage_off[q] + c0, tb, &bar[b]);
+    if (with_tab) BulkCopyPieces(base, slots + slot_off[q], ab, &bar[b], piece);
+    BulkCopyPieces(base + kTableBuf, staged + stage_off[q] + c0, tb, &bar[b], piece);
     issued[b]++;
   };
   auto warp_flush = [&]() {
@@ -974,11 +982,16 @@ std::unique_ptr<Pairs> HashProbe(Context& c, const HashTable& ht, const std::str
         const int pgrid = std::min(parts, c.num_sms);
         if (!ht.wide && !c.OptStr("KDB_PROBE_PARTS_TILED")) {
           const size_t wsmem = 2 * (kTableBuf + kTupCap * sizeof(unsigned long long));
+          // KDB_TMA_PIECE: bytes per bulk copy (a partition's table and
+          // tuples go as several copies in flight together)
+          const char* pe = c.OptStr("KDB_TMA_PIECE");
+          const uint32_t piece = pe ? static_cast<uint32_t>(std::max(16, std::atoi(pe)) & ~15) : 4096u;
           KDB_CUDA(cudaFuncSetAttribute(ProbePartsW, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                         static_cast<int>(wsmem)));
           ProbePartsW<<<pgrid, kPartBlock, wsmem, c.stream>>>(static_cast<const unsigned long long*>(staged), stage_off,
                                                              hist, static_cast<const unsigned long long*>(ht.slots),
-                                                             ht.slot_off, parts, out, cap, counter, err);
+                                                             ht.slot_off, parts, out, cap, counter, err,
+                                                             piece);
         } else if (ht.wide) {
           KDB_CUDA(cudaFuncSetAttribute(ProbeParts<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                         static_cast<int>(smem)));
