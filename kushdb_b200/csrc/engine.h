@@ -327,6 +327,9 @@ class Context {
   // shared-memory sort per bucket); false, with the items untouched, when a
   // bucket came out too large (the caller then merge sorts)
   bool SampleSortItems(void* items, int64_t n, Arena& arena);
+  // (key, tie) order by key-range buckets; false (nothing done) when a
+  // bucket is too large for one CTA's shared memory
+  bool RangeSortItems(void* items, int64_t n, Arena& arena);
   // exclusive prefix sum of a[0..n) in place, the total into a[n]
   void ScanU64(uint64_t* a, int64_t n, const char* tag = "skinner scan");
   // the same over *n_ptr elements (a device word), skipped when *n_ptr > cap

@@ -755,6 +755,143 @@ __global__ void SampleBucketSort(const SortItem* __restrict__ src, const unsigne
 
 }  // namespace
 
+// ---------------------------------------------------------------------------
+// Range-bucket sort of 16-byte items by (key, tie): the keys' minimum and
+// maximum split the key range into kRangeBuckets equal-width buckets (a
+// bucket index never decreases with the key), one pass counts the buckets,
+// one block scans the counts, one pass scatters, and one CTA per bucket
+// sorts it in shared memory.  Equal keys share a bucket, so many ties (or a
+// skewed range) make a large bucket; the caller then uses the merge sort.
+// ---------------------------------------------------------------------------
+namespace {
+
+constexpr int kRangeBuckets = 1024;
+
+__global__ void RangeMinMax(const SortItem* __restrict__ items, int64_t n, unsigned long long* __restrict__ mm) {
+  unsigned long long lo = ~0ULL, hi = 0;
+  for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < n;
+       i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const unsigned long long k = items[i].key;
+    lo = k < lo ? k : lo;
+    hi = k > hi ? k : hi;
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    const unsigned long long a = __shfl_xor_sync(0xffffffffu, lo, o), b = __shfl_xor_sync(0xffffffffu, hi, o);
+    lo = a < lo ? a : lo;
+    hi = b > hi ? b : hi;
+  }
+  if ((threadIdx.x & 31) == 0) {
+    atomicMin(&mm[0], lo);
+    atomicMax(&mm[1], hi);
+  }
+}
+
+__device__ __forceinline__ int RangeBucket(unsigned long long k, const unsigned long long* mm) {
+  const unsigned long long lo = mm[0], range = mm[1] - mm[0];
+  // (k - lo) / (range + 1) * B in doubles: rounding keeps it monotonic
+  const double f = static_cast<double>(k - lo) / (static_cast<double>(range) + 1.0);
+  const int b = static_cast<int>(f * kRangeBuckets);
+  return b < 0 ? 0 : (b >= kRangeBuckets ? kRangeBuckets - 1 : b);
+}
+
+__global__ void RangeCount(const SortItem* __restrict__ items, int64_t n, const unsigned long long* __restrict__ mm,
+                           uint16_t* __restrict__ bucket_of, unsigned* __restrict__ counts) {
+  __shared__ unsigned cnt[kRangeBuckets];
+  __shared__ unsigned long long smm[2];
+  for (int j = threadIdx.x; j < kRangeBuckets; j += blockDim.x) cnt[j] = 0;
+  if (threadIdx.x < 2) smm[threadIdx.x] = mm[threadIdx.x];
+  __syncthreads();
+  for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < n;
+       i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const int b = RangeBucket(items[i].key, smm);
+    bucket_of[i] = static_cast<uint16_t>(b);
+    atomicAdd(&cnt[b], 1u);
+  }
+  __syncthreads();
+  for (int j = threadIdx.x; j < kRangeBuckets; j += blockDim.x)
+    if (cnt[j]) atomicAdd(&counts[j], cnt[j]);
+}
+
+// one block of kRangeBuckets threads: exclusive offsets (offs[B] = total),
+// cursors zeroed, the largest bucket into *largest
+__global__ void __launch_bounds__(kRangeBuckets) RangeOffsets(const unsigned* __restrict__ counts,
+                                                              unsigned* __restrict__ offs,
+                                                              unsigned* __restrict__ cursor,
+                                                              unsigned* __restrict__ largest) {
+  __shared__ unsigned ws[kRangeBuckets / 32];
+  __shared__ unsigned wmax[kRangeBuckets / 32];
+  const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
+  const unsigned c = counts[t];
+  unsigned incl = c, mx = c;
+  for (int o = 1; o < 32; o <<= 1) {
+    const unsigned y = __shfl_up_sync(0xffffffffu, incl, o);
+    if (lane >= o) incl += y;
+    const unsigned z = __shfl_xor_sync(0xffffffffu, mx, o);
+    mx = z > mx ? z : mx;
+  }
+  if (lane == 31) ws[warp] = incl;
+  if (lane == 0) wmax[warp] = mx;
+  __syncthreads();
+  if (warp == 0) {
+    unsigned v = ws[lane], m = wmax[lane];
+    for (int o = 1; o < 32; o <<= 1) {
+      const unsigned y = __shfl_up_sync(0xffffffffu, v, o);
+      if (lane >= o) v += y;
+      const unsigned z = __shfl_xor_sync(0xffffffffu, m, o);
+      m = z > m ? z : m;
+    }
+    ws[lane] = v;  // inclusive per warp
+    if (lane == 0) *largest = m;
+  }
+  __syncthreads();
+  const unsigned before = (warp ? ws[warp - 1] : 0u) + incl - c;
+  offs[t] = before;
+  if (t == kRangeBuckets - 1) offs[kRangeBuckets] = before + c;
+  cursor[t] = 0;
+}
+
+}  // namespace
+
+bool Context::RangeSortItems(void* items_v, int64_t n, Arena& arena) {
+  if (n <= 1 || dry) return true;
+  if (n > 0x7fffffffLL) return false;
+  SortItem* items = static_cast<SortItem*>(items_v);
+  SortItem* tmp = reinterpret_cast<SortItem*>(arena.Alloc(sizeof(SortItem) * n));
+  uint16_t* bof = reinterpret_cast<uint16_t*>(arena.Alloc(sizeof(uint16_t) * n));
+  unsigned long long* mm = arena.AllocT<unsigned long long>(2);
+  unsigned* counts = arena.AllocT<unsigned>(kRangeBuckets);
+  unsigned* offs = arena.AllocT<unsigned>(kRangeBuckets + 1);
+  unsigned* cursor = arena.AllocT<unsigned>(kRangeBuckets);
+  unsigned* largest = arena.AllocT<unsigned>(1);
+  Memset(mm, 0xff, sizeof(unsigned long long));
+  Memset(mm + 1, 0, sizeof(unsigned long long));
+  Memset(counts, 0, sizeof(unsigned) * kRangeBuckets);
+  const int grid = GridFor(n, 256);
+  TimedStart("sort range");
+  Issue([=](cudaStream_t s) { RangeMinMax<<<grid, 256, 0, s>>>(items, n, mm); });
+  Issue([=](cudaStream_t s) { RangeCount<<<grid, 256, 0, s>>>(items, n, mm, bof, counts); });
+  Issue([=](cudaStream_t s) { RangeOffsets<<<1, kRangeBuckets, 0, s>>>(counts, offs, cursor, largest); });
+  TimedStop();
+  KDB_CUDA(cudaGetLastError());
+  // the bucket sizes decide (at recording; a replay runs on the same data)
+  unsigned big = 0;
+  D2H(&big, largest, sizeof(big));
+  if (big > static_cast<unsigned>(kBucketCap)) return false;
+  int m = 1;
+  while (m < static_cast<int>(big)) m <<= 1;
+  const size_t smem_bucket = sizeof(SortItem) * std::max(m, 1);
+  TimedStart("sort buckets");
+  Issue([=](cudaStream_t s) { SampleScatter<<<grid, 256, 0, s>>>(items, n, bof, offs, cursor, tmp); });
+  if (smem_bucket > 48 * 1024)
+    KDB_CUDA(cudaFuncSetAttribute(SampleBucketSort, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  static_cast<int>(smem_bucket)));
+  const int threads = std::min(512, std::max(32, m / 2));
+  Issue([=](cudaStream_t s) { SampleBucketSort<<<kRangeBuckets, threads, smem_bucket, s>>>(tmp, offs, items); });
+  TimedStop();
+  KDB_CUDA(cudaGetLastError());
+  return true;
+}
+
 bool Context::SampleSortItems(void* items_v, int64_t n, Arena& arena) {
   if (n <= 1 || dry) return true;
   if (n > 0x7fffffffLL) return false;
