@@ -882,6 +882,7 @@ std::unique_ptr<HashTable> HashBuild(Context& c, const std::string& table, const
     PartHistogram<<<grid, kBlock, sizeof(unsigned) * parts, c.stream>>>(key, srows, n, ht->bits, hist);
     PartOffsets<<<1, 1024, 0, c.stream>>>(hist, parts, load_factor, stage_off, ht->slot_off, cursor);
     c.kernel_launches += 2;
+    c.TimedStop();
     unsigned long long totals[2];
     KDB_CUDA(cudaMemcpyAsync(&totals[0], stage_off + parts, 8, cudaMemcpyDeviceToHost, c.stream));
     KDB_CUDA(cudaMemcpyAsync(&totals[1], ht->slot_off + parts, 8, cudaMemcpyDeviceToHost, c.stream));
@@ -891,6 +892,7 @@ std::unique_ptr<HashTable> HashBuild(Context& c, const std::string& table, const
     // sub-tables too large for shared memory are built in place in HBM
     c.Memset(ht->slots, 0, totals[1] * slot_bytes);
     void* staged = arena.Alloc(std::max<unsigned long long>(totals[0], 2) * slot_bytes);
+    c.TimedStart("hash scatter");
     if (ht->wide)
       PartScatter<true><<<grid, kBlock, 0, c.stream>>>(key, srows, n, ht->bits, stage_off, cursor,
                                                       static_cast<ulonglong2*>(staged));
