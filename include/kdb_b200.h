@@ -254,6 +254,18 @@ int64_t kdb_selvec_get(const kdb_selvec* s, int32_t* rows, int64_t cap);
 const int32_t* kdb_selvec_device_rows(const kdb_selvec* s);
 void kdb_selvec_free(kdb_selvec* s);
 
+/* Sort of a table's rows: the rows of `table` (all, or those of `sel`) in
+ * ORDER BY order of nkeys key columns, asc[k] != 0 ascending, as a selection
+ * vector in that order (not ascending).  Replaces OrderByTranslator
+ * (compile/translators/order_by_translator.cc:35-110) over runtime::Vector's
+ * merge sort (runtime/vector.cc:45-110): a NULL key sorts after every value
+ * ascending and before every value descending (proxy::LessThan used both
+ * ways), ENUM keys in string order, and rows whose keys tie keep their input
+ * order.  Keys: SMALLINT/INT/BIGINT/DATE/BOOLEAN/ENUM/REAL columns (TEXT:
+ * KDB_ERR_UNSUPPORTED). */
+int kdb_sort(kdb_ctx* ctx, const char* table, const char* const* key_columns, const int8_t* asc, int32_t nkeys,
+             const kdb_selvec* sel, kdb_selvec** out);
+
 /* Hash join build / probe: runtime::HashTable::{Create,Insert,GetBucket}
  * (runtime/hash_table.h:22-38) as hash_join_translator.cc:79-139 drives it.
  * The key is one SMALLINT/INT/BIGINT/DATE/ENUM/BOOLEAN column; rows with a

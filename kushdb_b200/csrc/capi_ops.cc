@@ -133,6 +133,18 @@ int kdb_scan_select(kdb_ctx* ctx, const char* table, const char* const* columns,
   });
 }
 
+int kdb_sort(kdb_ctx* ctx, const char* table, const char* const* key_columns, const int8_t* asc, int32_t nkeys,
+             const kdb_selvec* sel, kdb_selvec** out) {
+  if (out) *out = nullptr;
+  return OpGuard(ctx, [&](kdb::Context& c) {
+    if (!table || !key_columns || !asc || !out || nkeys <= 0) throw kdb::Error(KDB_ERR_INVALID, "null argument");
+    std::vector<bool> dir;
+    for (int32_t k = 0; k < nkeys; k++) dir.push_back(asc[k] != 0);
+    auto sv = kdb::ops::SortRows(c, table, Names(key_columns, nkeys), dir, sel ? sel->s.get() : nullptr);
+    *out = new kdb_selvec{std::move(sv)};
+  });
+}
+
 int64_t kdb_selvec_size(const kdb_selvec* s) { return s ? s->s->n : -1; }
 
 const int32_t* kdb_selvec_device_rows(const kdb_selvec* s) { return s ? s->s->rows : nullptr; }

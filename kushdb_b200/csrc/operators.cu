@@ -815,6 +815,110 @@ static int64_t SelCount(const Context& c, const std::string& table, const SelVec
   return std::max<int64_t>(it->second.rows, 0);
 }
 
+// ---------------------------------------------------------------------------
+// Sort of a table's rows by key columns (ORDER BY outside a plan): one
+// stable radix sort of (order key, row) pairs per key column, from the last
+// key to the first, each pass keyed by the column's value in the current
+// row order.
+// ---------------------------------------------------------------------------
+namespace {
+
+// The order key of row r: an unsigned 64-bit value whose order is the
+// column's ORDER BY order ascending, NULL above every value; descending is
+// its complement (NULL then first).
+__global__ void SortKeyFill(const void* __restrict__ data, const int8_t* __restrict__ nulls, int kind,
+                            const int32_t* __restrict__ rank, const uint32_t* __restrict__ perm, int64_t n,
+                            bool desc, uint64_t* __restrict__ keys) {
+  for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < n;
+       i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const int64_t r = perm[i];
+    uint64_t k;
+    if (nulls && nulls[r]) {
+      k = ~0ULL;
+    } else {
+      switch (kind) {
+        case 0: k = static_cast<uint64_t>(static_cast<const int8_t*>(data)[r] != 0); break;
+        case 1: k = static_cast<uint64_t>(static_cast<int64_t>(static_cast<const int16_t*>(data)[r])) ^ (1ULL << 63); break;
+        case 2: k = static_cast<uint64_t>(static_cast<int64_t>(static_cast<const int32_t*>(data)[r])) ^ (1ULL << 63); break;
+        case 3: k = static_cast<uint64_t>(static_cast<const int64_t*>(data)[r]) ^ (1ULL << 63); break;
+        case 4: {
+          const uint64_t b = __double_as_longlong(static_cast<const double*>(data)[r]);
+          k = (b >> 63) ? ~b : (b | (1ULL << 63));
+          break;
+        }
+        default: k = static_cast<uint64_t>(rank[static_cast<const int32_t*>(data)[r]]); break;
+      }
+      // values stay below the NULL key
+      if (k == ~0ULL) k = ~0ULL - 1;
+    }
+    keys[i] = desc ? ~k : k;
+  }
+}
+
+__global__ void SortPermInit(const int32_t* __restrict__ sel, int64_t n, uint32_t* __restrict__ perm) {
+  for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < n;
+       i += static_cast<int64_t>(gridDim.x) * blockDim.x)
+    perm[i] = static_cast<uint32_t>(sel ? sel[i] : i);
+}
+
+}  // namespace
+
+std::unique_ptr<SelVec> SortRows(Context& c, const std::string& table, const std::vector<std::string>& keys,
+                                 const std::vector<bool>& asc, const SelVec* sel) {
+  if (c.dry) throw Error(KDB_ERR_UNSUPPORTED, "operators need a device context");
+  if (keys.empty() || keys.size() != asc.size()) throw Error(KDB_ERR_INVALID, "one direction per sort key");
+  const int64_t n = SelCount(c, table, sel);
+  if (n >= (int64_t(1) << 32)) throw Error(KDB_ERR_UNSUPPORTED, "sort of 2^32 rows or more");
+  struct KeyCol {
+    const DevColumn* col;
+    int kind;
+  };
+  std::vector<KeyCol> kc;
+  for (const auto& k : keys) {
+    const DevColumn& col = c.Column(table, k);
+    int kind;
+    switch (col.type.id) {
+      case plan::TypeId::BOOLEAN: kind = 0; break;
+      case plan::TypeId::SMALLINT: kind = 1; break;
+      case plan::TypeId::INT:
+      case plan::TypeId::DATE: kind = 2; break;
+      case plan::TypeId::BIGINT: kind = 3; break;
+      case plan::TypeId::REAL: kind = 4; break;
+      case plan::TypeId::ENUM: kind = 5; break;
+      default: throw Error(KDB_ERR_UNSUPPORTED, "sort keys must be integer, date, boolean, enum or real columns");
+    }
+    kc.push_back({&col, kind});
+  }
+  auto out = std::make_unique<SelVec>();
+  out->ctx = &c;
+  out->table = table;
+  out->n = n;
+  KDB_CUDA(cudaMallocAsync(&out->rows, sizeof(int32_t) * std::max<int64_t>(n, 1), c.stream));
+  if (n == 0) return out;
+  Arena arena(c);
+  uint64_t* kbuf = arena.AllocT<uint64_t>(n);
+  const int grid = c.GridFor(n, kBlock);
+  uint32_t* perm = reinterpret_cast<uint32_t*>(out->rows);
+  c.TimedStart("sort rows");
+  SortPermInit<<<grid, kBlock, 0, c.stream>>>(sel ? sel->rows : nullptr, n, perm);
+  c.kernel_launches++;
+  c.TimedStop();
+  for (size_t j = keys.size(); j-- > 0;) {
+    const DevColumn& col = *kc[j].col;
+    const int32_t* rank = kc[j].kind == 5 ? c.Enum(col.type.enum_id).d_rank : nullptr;
+    c.TimedStart("sort rows");
+    SortKeyFill<<<grid, kBlock, 0, c.stream>>>(col.data, col.nulls, kc[j].kind, rank, perm, n, !asc[j], kbuf);
+    c.kernel_launches++;
+    c.TimedStop();
+    KDB_CUDA(cudaGetLastError());
+    // stable: rows with equal keys keep the order of the previous pass
+    c.RadixSortPairs(kbuf, perm, n, arena, 64);
+  }
+  KDB_CUDA(cudaStreamSynchronize(c.stream));
+  return out;
+}
+
+
 int PartBitsFor(int64_t n, double lf, int slot_bytes, int32_t fanout) {
   if (fanout == 1) return 0;
   if (fanout > 1) {

@@ -54,6 +54,14 @@ std::unique_ptr<Pairs> HashProbe(Context& c, const HashTable& ht, const std::str
 // Sub-table bits the automatic fan-out chooses for n rows (host rule).
 int PartBitsFor(int64_t n, double load_factor, int slot_bytes, int32_t fanout);
 
+// Rows of `table` (all, or those of `sel`) in ORDER BY order of the key
+// columns (asc[k] per key; a NULL sorts after every value ascending and
+// before descending, as proxy::LessThan used both ways; ties keep the
+// input order, as runtime::Vector's merge sort does).  Keys: integer, date,
+// boolean, enum (string order) and real columns.
+std::unique_ptr<SelVec> SortRows(Context& c, const std::string& table, const std::vector<std::string>& keys,
+                                 const std::vector<bool>& asc, const SelVec* sel);
+
 // One aggregate of a group-by: op is a plan::AggType (SUM, MIN, MAX, AVG,
 // COUNT); an empty column under COUNT counts rows.
 struct AggSpec {

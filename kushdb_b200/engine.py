@@ -37,7 +37,7 @@ EXPORTS = [
     "kdb_mlp_last_error", "kdb_mlp_set_params", "kdb_mlp_get_params", "kdb_mlp_forward", "kdb_mlp_gradient",
     "kdb_mlp_train_step", "kdb_mlp_free", "kdb_ctx_set_skinner_policy", "kdb_last_skinner_samples",
     "kdb_ctx_set_prepared_queries",
-    "kdb_scan_select", "kdb_selvec_size", "kdb_selvec_get", "kdb_selvec_device_rows", "kdb_selvec_free",
+    "kdb_scan_select", "kdb_sort", "kdb_selvec_size", "kdb_selvec_get", "kdb_selvec_device_rows", "kdb_selvec_free",
     "kdb_hash_build", "kdb_hash_info", "kdb_hash_probe", "kdb_hash_free", "kdb_pairs_size", "kdb_pairs_get",
     "kdb_pairs_free", "kdb_agg_create", "kdb_agg_set_pre_aggregation", "kdb_agg_update", "kdb_agg_finalize",
     "kdb_agg_free", "kdb_index_build", "kdb_index_open_kdbindex", "kdb_index_num_keys", "kdb_index_num_rows",
@@ -134,6 +134,7 @@ def load_library(path: str = LIB_PATH):
     # per-operator boundary
     CP = ctypes.c_char_p
     L.kdb_scan_select.argtypes = [P, CP, P, I32, CP, ctypes.POINTER(P)]
+    L.kdb_sort.argtypes = [P, CP, P, P, I32, P, ctypes.POINTER(P)]
     L.kdb_selvec_size.restype = I64
     L.kdb_selvec_size.argtypes = [P]
     L.kdb_selvec_get.restype = I64

@@ -72,6 +72,21 @@ def scan_select(engine: Engine, table: str, columns: Sequence[str], filter_expr)
     return SelVec(engine, h)
 
 
+def sort_rows(engine: Engine, table: str, keys: Sequence[str], asc: Sequence[bool],
+              sel: Optional[SelVec] = None) -> SelVec:
+    """Rows of `table` (or of `sel`) in ORDER BY order of `keys` (kdb_sort):
+    NULL after values ascending, before them descending; ties keep the
+    input order."""
+    if len(keys) != len(asc) or not keys:
+        raise ValueError("one direction per key")
+    engine.register_enums()
+    dirs = (ctypes.c_int8 * len(asc))(*[1 if a else 0 for a in asc])
+    h = ctypes.c_void_p()
+    engine._check(engine.lib.kdb_sort(engine.ctx, table.encode(), _names(keys), dirs, len(keys),
+                                      sel.h if sel is not None else None, ctypes.byref(h)))
+    return SelVec(engine, h)
+
+
 class HashTable:
     """A device join table over one integer key column."""
 

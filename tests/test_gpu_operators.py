@@ -355,3 +355,59 @@ def test_skinner_operator_matches_plan(engine):
     for policy, seed in (("uct", 0), ("random", 3)):
         got = skinner_execute(engine, op, policy=policy, budget_per_episode=500, seed=seed)
         assert compare(got, want, ordered=False) == ""
+
+
+# ---------------------------------------------------------------------------
+# sort of a table's rows (kdb_sort)
+# ---------------------------------------------------------------------------
+
+
+def _sorted_rows(cols, keys, asc, rows):
+    """Python restatement of the ORDER BY order: per key, NULL after every
+    value ascending and before every value descending; a stable sort keeps
+    tied rows in input order."""
+    out = list(rows)
+    for k, a in reversed(list(zip(keys, asc))):
+        vals, nulls = cols[k]
+        if a:
+            out.sort(key=lambda r: (1, 0) if nulls[r] else (0, vals[r]))
+        else:
+            out.sort(key=lambda r: (0, 0) if nulls[r] else (1, vals[r]), reverse=True)
+    return out
+
+
+@pytest.mark.parametrize("keys,asc", [(["i"], [True]), (["i"], [False]), (["r", "i"], [False, True]),
+                                      (["e", "s", "b"], [True, False, True]), (["big"], [False]),
+                                      (["e"], [False])])
+@pytest.mark.parametrize("with_sel", [False, True])
+def test_sort_rows_matches_order_by_semantics(engine, keys, asc, with_sel):
+    from kushdb_b200.operators import scan_select, sort_rows
+    from kushdb_b200.plan import EnumRegistry
+    EnumRegistry.register(83, ["pear", "apple", "fig", "kiwi"])
+    rng = np.random.default_rng(len(keys) * 7 + int(with_sel))
+    n = 20_000
+    t = HostTable("sort_rows_t")
+    t.add(HostColumn("i", Type.Int(), values=rng.integers(-50, 50, n).astype(np.int32),
+                     nulls=(rng.random(n) < 0.1).astype(np.int8)))
+    t.add(HostColumn("r", Type.Real(), values=rng.integers(-20, 20, n).astype(np.float64) / 4.0,
+                     nulls=(rng.random(n) < 0.1).astype(np.int8)))
+    t.add(HostColumn("e", Type.Enum(83), values=rng.integers(0, 4, n).astype(np.int32)))
+    t.add(HostColumn("s", Type.SmallInt(), values=rng.integers(-3, 3, n).astype(np.int16)))
+    t.add(HostColumn("b", Type.Boolean(), values=(rng.random(n) < 0.5).astype(np.int8)))
+    t.add(HostColumn("big", Type.BigInt(), values=rng.integers(-(1 << 40), 1 << 40, n).astype(np.int64)))
+    t.add(HostColumn("v", Type.Int(), values=np.arange(n, dtype=np.int32)))
+    engine.register_table(t)
+    names = ["pear", "apple", "fig", "kiwi"]
+    cols = {}
+    for c in ("i", "r", "s", "b", "big"):
+        hc = t.columns[c]
+        cols[c] = (hc.values, hc.nulls if hc.nulls is not None else np.zeros(n, np.int8))
+    cols["e"] = ([names[x] for x in t.columns["e"].values], np.zeros(n, np.int8))
+    rows = list(range(n))
+    sel = None
+    if with_sel:
+        sel = scan_select(engine, t.name, ["v"], Geq(V(Type.Int(), 0), Literal(5000)))
+        rows = list(range(5000, n))
+    got = sort_rows(engine, t.name, keys, asc, sel=sel).rows()
+    assert list(got) == _sorted_rows(cols, keys, asc, rows)
+    engine.drop_table(t.name)
