@@ -21,6 +21,7 @@
 #include <cstring>
 #include <functional>
 #include <limits>
+#include <list>
 #include <map>
 #include <random>
 #include <set>
@@ -566,6 +567,9 @@ struct JoinTable {
   // loads the build row's key; `key_col` is that column
   bool key_in_slot = false;
   int key_col = -1;
+  // key-in-slot tables: device word set by the build when two non-NULL
+  // build rows share the key (the join key is then not unique)
+  uint64_t* dup = nullptr;
   // grouped form (Skinner indexes): rows sorted by key hash (`srow`, with
   // their hashes `sh`), and `slots` holding one entry per distinct hash
   // (hash << 32 | first sorted index + 1) with the group's length in `lens`
@@ -585,6 +589,87 @@ struct SkinnerAgg {
   int nw = 0;
 };
 
+}  // namespace
+
+// One cached Skinner child: its filtered rows and the grouped indexes of the
+// join columns, in device memory owned by the entry.  `ready` is recorded on
+// the building stream after the last kernel that fills them; a request that
+// finds the entry waits on it before its own kernels read the entry.
+struct BuildEntry {
+  explicit BuildEntry(Context& ctx) : arena(ctx) {
+    if (!ctx.dry) KDB_CUDA(cudaEventCreateWithFlags(&ready, cudaEventDisableTiming));
+  }
+  ~BuildEntry() {
+    if (ready) cudaEventDestroy(ready);
+  }
+  BuildEntry(const BuildEntry&) = delete;
+  BuildEntry& operator=(const BuildEntry&) = delete;
+  Arena arena;  // frees the entry's memory when the last holder lets go
+  MatBuffer mat;
+  std::vector<JoinTable> index;  // per child column (empty where none)
+  cudaEvent_t ready = nullptr;
+};
+
+// Shared by the slots of one server.  Entries leave the map oldest first
+// once the cached bytes pass max_bytes; their memory goes when the last
+// query holding them is destroyed, after its own synchronisation, so no
+// kernel still reads it.  The server's tables do not change while it runs
+// (a documented condition of the serving slots), so entries never go stale.
+struct BuildCache {
+  explicit BuildCache(size_t max) : max_bytes(max) {}
+  std::mutex mu;
+  size_t max_bytes;
+  size_t bytes = 0;
+  std::list<std::string> lru;  // least recently used first
+  struct Slot {
+    std::shared_ptr<BuildEntry> entry;
+    std::list<std::string>::iterator at;
+  };
+  std::unordered_map<std::string, Slot> map;
+  int64_t hits = 0, misses = 0;
+
+  std::shared_ptr<BuildEntry> Find(const std::string& key) {
+    std::lock_guard<std::mutex> lock(mu);
+    auto it = map.find(key);
+    if (it == map.end()) {
+      misses++;
+      return nullptr;
+    }
+    hits++;
+    lru.splice(lru.end(), lru, it->second.at);
+    return it->second.entry;
+  }
+  // Keeps `e` (or an entry another slot inserted for the same key first,
+  // which the caller then uses instead of its own).
+  std::shared_ptr<BuildEntry> Insert(const std::string& key, std::shared_ptr<BuildEntry> e) {
+    std::lock_guard<std::mutex> lock(mu);
+    auto it = map.find(key);
+    if (it != map.end()) return e;  // both built it; each uses its own
+    lru.push_back(key);
+    map[key] = Slot{e, std::prev(lru.end())};
+    bytes += e->arena.bytes();
+    while (bytes > max_bytes && lru.size() > 1) {
+      auto victim = map.find(lru.front());
+      bytes -= victim->second.entry->arena.bytes();
+      map.erase(victim);
+      lru.pop_front();
+    }
+    return e;
+  }
+};
+
+std::shared_ptr<BuildCache> MakeBuildCache(size_t max_bytes) { return std::make_shared<BuildCache>(max_bytes); }
+
+void BuildCacheStats(BuildCache& c, int64_t* hits, int64_t* misses, int64_t* bytes, int64_t* entries) {
+  std::lock_guard<std::mutex> lock(c.mu);
+  *hits = c.hits;
+  *misses = c.misses;
+  *bytes = static_cast<int64_t>(c.bytes);
+  *entries = static_cast<int64_t>(c.map.size());
+}
+
+namespace {
+
 class Executor {
  public:
   Executor(Context& ctx, Arena& arena) : ctx_(ctx), arena_(arena) {}
@@ -600,6 +685,10 @@ class Executor {
   Arena& arena_;
   std::map<const Operator*, MatBuffer> mats_;
   std::map<const Operator*, JoinTable> joins_;
+  // build-cache entries this query reads: kept until the executor (whose
+  // query has synchronised by then) is destroyed
+  std::vector<std::shared_ptr<BuildEntry>> held_;
+  std::string ChildSig(const Operator& child, const std::set<int>& index_cols) const;
 
   // --- helpers -----------------------------------------------------------
   // Upper bound (or, for joins, an estimate) of the rows a stream produces.
@@ -682,6 +771,9 @@ class Executor {
                   int64_t& src_rows);
   void EmitMatScan(KernelSource& ks, const MatBuffer& m, const uint32_t* indirection,
                    const Consume& consume, int64_t& src_rows);
+  // The output values of a SCAN / SCAN_SELECT at base-table row `row` (a
+  // row the scan's filters already passed), its columns read there.
+  std::vector<CVal> EmitScanRowAt(KernelSource& ks, ExprGen& eg, const Operator& op, const std::string& row);
   MatBuffer EmitOrderedMaterialize(KernelSource& ks, ExprGen& eg, const Operator& op, const uint32_t* order,
                                    const MatBuffer& src, int64_t& src_rows);
   std::vector<CVal> LoadMatRow(KernelSource& ks, ExprGen& eg, const MatBuffer& m,
@@ -691,7 +783,11 @@ class Executor {
   MatBuffer Materialize(const Operator& op);
   MatBuffer MaterializeStream(const Operator& op, const uint32_t* order = nullptr,
                               const MatBuffer* ordered_src = nullptr);
-  MatBuffer MaterializeCounted(const Operator& op);
+  // `on_count(rows)` runs between the counting and the writing pass; `on_row`
+  // emits extra per-row work into the writing pass (values, row index).
+  using RowHook = std::function<void(KernelSource&, ExprGen&, const std::vector<CVal>&, const std::string&)>;
+  MatBuffer MaterializeCounted(const Operator& op, const std::function<void(int64_t)>& on_count = nullptr,
+                               const RowHook& on_row = nullptr);
   // left rows of a CROSS_PRODUCT in the left child's stream order (null:
   // the buffer already is in that order)
   std::map<const Operator*, uint32_t*> cross_order_;
@@ -719,6 +815,11 @@ class Executor {
                                 const std::vector<int>& key_cols, bool any_order);
   void BuildJoin(const Operator& op);
   JoinTable BuildIndex(const MatBuffer& m, const std::vector<int>& key_cols);
+  // The table of BuildIndex for `rows` build rows of buffer m's layout
+  // (allocated and cleared), and the insert of one row into it.
+  JoinTable PrepareJoinTable(const MatBuffer& m, int64_t rows, const std::vector<int>& key_cols);
+  void EmitJoinInsert(KernelSource& ks, ExprGen& eg, const JoinTable& jt, const std::vector<CVal>& vals,
+                      const std::vector<int>& key_cols, const std::string& row);
   JoinTable BuildGroupedIndex(const MatBuffer& m, int key_col);
   std::string probe_br_;  // inside an on_match callback: the matched build row's index
   // set while emitting a join's probe side: its scan takes one row per
@@ -726,6 +827,9 @@ class Executor {
   // column loads, bound such a pipeline, and the 4-row vector's registers
   // cost occupancy)
   bool probe_side_scan_ = false;
+  // set with probe_side_scan_: the scan prefetches only these columns (the
+  // probe keys and the filters); the others load where they are used
+  const std::set<int>* prefetch_only_ = nullptr;
   // set while materialising a join's build side (rows in any order)
   bool build_side_mat_ = false;
   // TMA-staged scan: set by a consumer before emitting its scan (rows per
@@ -833,6 +937,31 @@ void Executor::EmitMatScan(KernelSource& ks, const MatBuffer& m, const uint32_t*
   ks.Close();
 }
 
+std::vector<CVal> Executor::EmitScanRowAt(KernelSource& ks, ExprGen& eg, const Operator& op,
+                                          const std::string& row) {
+  if (op.kind != OpKind::SCAN && op.kind != OpKind::SCAN_SELECT) throw Error(-1, "row access of a non-scan");
+  std::vector<CVal> scan;
+  for (const auto& sc : op.scan_columns) {
+    const DevColumn& c = ctx_.Column(op.relation, sc.name);
+    std::string v;
+    if (c.type.id == TypeId::TEXT) {
+      v = "kdb_text_at(" + ks.Ptr(c.toff, "int64_t", true) + ", " + ks.Ptr(c.tchars, "char", true) + ", " + row + ")";
+    } else {
+      v = ks.Ptr(c.data, StoreType(c.type.id), true) + "[" + row + "]";
+      if (c.type.id == TypeId::BOOLEAN) v = "(" + v + " != 0)";
+    }
+    const std::string nul = c.nulls ? "(" + ks.Ptr(c.nulls, "int8_t", true) + "[" + row + "] != 0)" : "false";
+    // bound where used: columns the consumer never reads are never loaded
+    scan.push_back(CVal{c.type, "(" + v + ")", nul});
+  }
+  Scope s;
+  if (op.kind == OpKind::SCAN) s.child.push_back(scan);
+  else s.virt = scan;
+  std::vector<CVal> out;
+  for (const auto& c : op.output) out.push_back(eg.Emit(*c.expr, s));
+  return out;
+}
+
 void Executor::EmitStream(KernelSource& ks, ExprGen& eg, const Operator& op, const Consume& consume,
                           int64_t& src_rows) {
   switch (op.kind) {
@@ -874,6 +1003,8 @@ void Executor::EmitStream(KernelSource& ks, ExprGen& eg, const Operator& op, con
       for (const DevColumn* c : cols) any_text |= c->type.id == TypeId::TEXT;
       const bool probe_side = probe_side_scan_;
       probe_side_scan_ = false;
+      const std::set<int>* prefetch_only = probe_side ? prefetch_only_ : nullptr;
+      prefetch_only_ = nullptr;
       // probe-ahead: the scan column that is the join's probe key
       const JoinTable* ajt = ahead_jt_;
       ahead_jt_ = nullptr;
@@ -1171,6 +1302,7 @@ void Executor::EmitStream(KernelSource& ks, ExprGen& eg, const Operator& op, con
           ks.L("const int64_t kdb_p0 = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;");
           for (size_t k = 0; k < cols.size(); k++) {
             if (cols[k]->type.id == TypeId::TEXT) continue;
+            if (prefetch_only && !prefetch_only->count(static_cast<int>(k))) continue;
             const std::string st = StoreType(cols[k]->type.id);
             nxt[k] = ks.Fresh("X");
             ks.L(st + " " + nxt[k] + " = kdb_p0 < (int64_t)" + n + " ? " + dp[k] + "[kdb_p0] : (" + st + ")0;");
@@ -1250,7 +1382,8 @@ void Executor::EmitStream(KernelSource& ks, ExprGen& eg, const Operator& op, con
           else v = raw;
           const std::string nul = np[k].empty() ? "false"
                                   : ncur[k].empty() ? "(" + np[k] + "[r] != 0)" : "(" + ncur[k] + " != 0)";
-          if (lazy) scan[k] = CVal{c.type, "(" + v + ")", nul};
+          if (lazy || (prefetch_only && !prefetch_only->count(static_cast<int>(k))))
+            scan[k] = CVal{c.type, "(" + v + ")", nul};
           else scan[k] = eg.Bind(c.type, v, nul);
           if (static_cast<int>(k) == ak) ahead_key_var_ = scan[k].v;
         };
@@ -1458,18 +1591,18 @@ void Executor::EmitProbe(KernelSource& ks, ExprGen& eg, const JoinTable& jt,
 // Join table over materialised rows (runtime::HashTable equivalent,
 // runtime/hash_table.cc:13-36): build rows with a NULL key are skipped
 // (hash_join_translator.cc:86-101).
-JoinTable Executor::BuildIndex(const MatBuffer& m, const std::vector<int>& key_cols) {
+JoinTable Executor::PrepareJoinTable(const MatBuffer& m, int64_t rows, const std::vector<int>& key_cols) {
   JoinTable jt;
   jt.build = m;
   uint64_t cap = 1024;
-  while (cap < static_cast<uint64_t>(m.rows) * 2) cap <<= 1;
+  while (cap < static_cast<uint64_t>(rows) * 2) cap <<= 1;
   if (cap > (uint64_t(1) << 31)) throw Error(-5, "join build side of more than 2^30 rows");
   jt.mask = cap - 1;
   jt.slots = arena_.AllocT<uint64_t>(cap);
   ctx_.Memset(jt.slots, 0, cap * sizeof(uint64_t));
   if (!ctx_.OptStr("KDB_NO_JOIN_FILTER")) {
     jt.bloom_log2 = 14;
-    while (jt.bloom_log2 < 26 && (int64_t(1) << jt.bloom_log2) < m.rows * 8) jt.bloom_log2++;
+    while (jt.bloom_log2 < 26 && (int64_t(1) << jt.bloom_log2) < rows * 8) jt.bloom_log2++;
     const size_t words = (size_t(1) << jt.bloom_log2) / 32;
     jt.bloom = arena_.AllocT<uint32_t>(words);
     ctx_.Memset(jt.bloom, 0, words * sizeof(uint32_t));
@@ -1479,30 +1612,47 @@ JoinTable Executor::BuildIndex(const MatBuffer& m, const std::vector<int>& key_c
     jt.key_in_slot = t == TypeId::INT || t == TypeId::DATE || t == TypeId::ENUM || t == TypeId::SMALLINT;
     jt.key_col = key_cols[0];
   }
-  if (m.rows == 0) return jt;
-  KernelSource ks;
-  ExprGen eg(ctx_, ks);
-  std::string n = ks.Word(static_cast<uint64_t>(m.rows));
+  if (jt.key_in_slot) {
+    jt.dup = arena_.AllocT<uint64_t>(1);
+    ctx_.Memset(jt.dup, 0, sizeof(uint64_t));
+  }
+  return jt;
+}
+
+void Executor::EmitJoinInsert(KernelSource& ks, ExprGen& eg, const JoinTable& jt, const std::vector<CVal>& vals,
+                              const std::vector<int>& key_cols, const std::string& row) {
   std::string slots = ks.Ptr(jt.slots, "uint64_t");
   std::string mask = ks.Word(jt.mask);
-  std::string bloom = jt.bloom ? ks.Ptr(jt.bloom, "uint32_t") : "";
-  ks.Open("for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < (int64_t)" + n +
-          "; r += (int64_t)gridDim.x * blockDim.x)");
-  auto vals = LoadMatRow(ks, eg, m, "r", nullptr);
   std::vector<CVal> keys;
   std::string nn = "true";
   for (int c : key_cols) {
     keys.push_back(vals.at(c));
     nn += " && !(" + vals.at(c).n + ")";
   }
+  // build rows with a NULL key are skipped (hash_join_translator.cc:86-101)
   ks.Open("if (" + nn + ")");
-  ks.L("const uint32_t h = " + JoinHash(eg, keys) + ";");
+  const std::string h = ks.Fresh("jh");
+  ks.L("const uint32_t " + h + " = " + JoinHash(eg, keys) + ";");
   if (jt.key_in_slot)
-    ks.L("kdb_join_insert_keyed(" + slots + ", " + mask + ", h, (uint32_t)(int32_t)" + keys[0].v + ", (uint32_t)r);");
+    ks.L("if (kdb_join_insert_keyed(" + slots + ", " + mask + ", " + h + ", (uint32_t)(int32_t)" + keys[0].v +
+         ", (uint32_t)(" + row + "))) atomicOr((unsigned long long*)" + ks.Ptr(jt.dup, "uint64_t") + ", 1ULL);");
   else
-    ks.L("kdb_join_insert(" + slots + ", " + mask + ", h, (uint32_t)r);");
-  if (jt.bloom) ks.L("kdb_bloom_set(" + bloom + ", h, " + std::to_string(jt.bloom_log2) + ");");
+    ks.L("kdb_join_insert(" + slots + ", " + mask + ", " + h + ", (uint32_t)(" + row + "));");
+  if (jt.bloom)
+    ks.L("kdb_bloom_set(" + ks.Ptr(jt.bloom, "uint32_t") + ", " + h + ", " + std::to_string(jt.bloom_log2) + ");");
   ks.Close();
+}
+
+JoinTable Executor::BuildIndex(const MatBuffer& m, const std::vector<int>& key_cols) {
+  JoinTable jt = PrepareJoinTable(m, m.rows, key_cols);
+  if (m.rows == 0) return jt;
+  KernelSource ks;
+  ExprGen eg(ctx_, ks);
+  std::string n = ks.Word(static_cast<uint64_t>(m.rows));
+  ks.Open("for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < (int64_t)" + n +
+          "; r += (int64_t)gridDim.x * blockDim.x)");
+  auto vals = LoadMatRow(ks, eg, m, "r", nullptr);
+  EmitJoinInsert(ks, eg, jt, vals, key_cols, "r");
   ks.Close();
   LaunchPipeline(ks, m.rows, "join build");
   return jt;
@@ -1583,14 +1733,38 @@ void Executor::BuildJoin(const Operator& op) {
   // a join's build rows need no particular buffer order (their stream
   // positions travel with them): with KDB_BUILD_MAT_ATOMIC the build side
   // is written in one pass with block-level slot claims
-  build_side_mat_ = ctx_.OptStr("KDB_BUILD_MAT_ATOMIC") != nullptr && Streamable(op.child(0));
-  MatBuffer left = Materialize(op.child(0));
-  build_side_mat_ = false;
   std::vector<int> keys;
   for (const auto& k : op.left_keys) {
     if (k->kind != ExprKind::ColRef) throw Error(-5, "hash join keys must be column references");
     keys.push_back(k->column_idx);
   }
+  const Operator& child = op.child(0);
+  if (Streamable(child) && !StreamHasJoin(child) && !ctx_.OptStr("KDB_BUILD_MAT_ATOMIC") &&
+      !ctx_.OptStr("KDB_MATERIALIZE_ATOMIC") && !ctx_.OptStr("KDB_JOIN_BUILD_PASS")) {
+    // The build side's writing pass inserts every row into the join table
+    // as it writes it (sized from the counting pass): no separate build
+    // kernel re-reads the rows.
+    Prepare(child);
+    JoinTable jt;
+    MatBuffer layout;  // column types only: the table is sized before the rows exist
+    for (const auto& c : child.output) {
+      MatCol mc;
+      mc.type = c.expr->type;
+      mc.nullable = c.expr->nullable;
+      layout.cols.push_back(mc);
+    }
+    auto on_count = [&](int64_t rows) { jt = PrepareJoinTable(layout, rows, keys); };
+    auto on_row = [&](KernelSource& ks, ExprGen& eg, const std::vector<CVal>& vals, const std::string& row) {
+      EmitJoinInsert(ks, eg, jt, vals, keys, row);
+    };
+    MatBuffer left = MaterializeCounted(child, on_count, on_row);
+    jt.build = left;
+    joins_[&op] = jt;
+    return;
+  }
+  build_side_mat_ = ctx_.OptStr("KDB_BUILD_MAT_ATOMIC") != nullptr && Streamable(child);
+  MatBuffer left = Materialize(child);
+  build_side_mat_ = false;
   joins_[&op] = BuildIndex(left, keys);
 }
 
@@ -1703,7 +1877,8 @@ MatBuffer Executor::MaterializeStream(const Operator& op, const uint32_t* order,
 // produced warp-row would serialise on the counter's L2 line (tens of
 // microseconds for a filtered scan of a few million rows); the count pass
 // reads only the filter columns.
-MatBuffer Executor::MaterializeCounted(const Operator& op) {
+MatBuffer Executor::MaterializeCounted(const Operator& op, const std::function<void(int64_t)>& on_count,
+                                       const RowHook& on_row) {
   const int block = 256;
   const auto& schema = op.output;
   const std::string shared_init =
@@ -1727,6 +1902,7 @@ MatBuffer Executor::MaterializeCounted(const Operator& op) {
   ctx_.ScanU64(offsets, grid, "materialize offsets");
   const int64_t produced = ReadU64(offsets + grid);
   ctx_.CheckDeviceError("materialize");
+  if (on_count) on_count(produced);
 
   KernelSource ks;
   ExprGen eg(ctx_, ks);
@@ -1752,6 +1928,7 @@ MatBuffer Executor::MaterializeCounted(const Operator& op) {
       if (!onull[c].empty()) ks.L(onull[c] + "[slot] = (" + v.n + ") ? 1 : 0;");
     }
     ks.L(posp + "[slot] = " + pos + ";");
+    if (on_row) on_row(ks, eg, vals, "slot");
     ks.Close();
     ks.Close();
   };
@@ -2156,6 +2333,31 @@ std::string ExprSig(const Expr& e) {
   for (const auto& k : e.kids) o << ExprSig(*k) << ";";
   for (int32_t v : e.in_values) o << v << ",";
   o << ")" << e.regex.size() << "'" << e.regex << "'";
+  return o.str();
+}
+
+// Identity of a Skinner child for the serving build cache: the relation
+// (and the device arrays it reads), its scan columns, filters and outputs,
+// and the columns indexed.
+std::string Executor::ChildSig(const Operator& child, const std::set<int>& index_cols) const {
+  std::ostringstream o;
+  o << static_cast<int>(child.kind) << "|" << child.relation << "|";
+  auto it = ctx_.tables.find(child.relation);
+  if (it != ctx_.tables.end()) o << it->second.rows << "|";
+  for (const auto& sc : child.scan_columns) {
+    o << sc.name << ":" << static_cast<int>(sc.type.id) << ":";
+    if (it != ctx_.tables.end()) {
+      auto c = it->second.cols.find(sc.name);
+      if (c != it->second.cols.end()) o << reinterpret_cast<uintptr_t>(c->second.data);
+    }
+    o << ",";
+  }
+  o << "|f";
+  for (const auto& f : child.filters) o << ExprSig(*f) << ";";
+  o << "|o";
+  for (const auto& c : child.output) o << ExprSig(*c.expr) << ";";
+  o << "|i";
+  for (int c : index_cols) o << c << ",";
   return o.str();
 }
 
@@ -2609,8 +2811,12 @@ bool Executor::BuildRowGroups(const Operator& op, std::vector<int>* key_cols) {
     if (std::find(key_cols->begin(), key_cols->end(), k->column_idx) == key_cols->end()) return false;
     bkeys.push_back(k->column_idx);
   }
-  // uniqueness of the build key: every non-NULL build row must find itself
-  // only (rows with a NULL key never join)
+  // uniqueness of the build key: a key-in-slot table found duplicates while
+  // it was built
+  if (jt.key_in_slot && jt.dup && bkeys.size() == 1 && bkeys[0] == jt.key_col && !ctx_.OptStr("KDB_KEY_CHECK_PASS"))
+    return ReadU64(jt.dup) == 0 || ctx_.dry;
+  // otherwise every non-NULL build row must find itself only (rows with a
+  // NULL key never join)
   uint64_t* dup = arena_.AllocT<uint64_t>(1);
   ctx_.Memset(dup, 0, sizeof(uint64_t));
   {
@@ -2644,32 +2850,141 @@ MatBuffer Executor::RunGroupByBuildRows(const Operator& op, const std::vector<Ag
     sv[j] = arena_.AllocT<uint64_t>(nb);
     sc[j] = arena_.AllocT<uint64_t>(nb);
   }
-  {
-    KernelSource ks;
-    std::string F = ks.Ptr(first, "uint64_t"), C = ks.Word(static_cast<uint64_t>(nb));
-    ks.Open("for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < (int64_t)" + C +
-            "; i += (int64_t)gridDim.x * blockDim.x)");
-    ks.L(F + "[i] = ~0ULL;");
-    for (size_t j = 0; j < plans.size(); j++) {
-      std::string V = ks.Ptr(sv[j], "uint64_t"), N = ks.Ptr(sc[j], "uint64_t");
-      bool min_init = plans[j].kind == StateKind::MinMaxKey && plans[j].is_min;
-      ks.L(V + "[i] = " + (min_init ? "~0ULL" : "0ULL") + "; " + N + "[i] = 0;");
-    }
-    ks.Close();
-    LaunchPipeline(ks, nb, "group init");
+  // initial states are byte patterns (all ones, or zero): memsets
+  ctx_.Memset(first, 0xff, sizeof(uint64_t) * nb);
+  for (size_t j = 0; j < plans.size(); j++) {
+    const bool min_init = plans[j].kind == StateKind::MinMaxKey && plans[j].is_min;
+    ctx_.Memset(sv[j], min_init ? 0xff : 0, sizeof(uint64_t) * nb);
+    ctx_.Memset(sc[j], 0, sizeof(uint64_t) * nb);
   }
   // probe pipeline: aggregate into the matched build row
-  {
+  std::vector<int> bkeys;
+  for (const auto& k : join.left_keys) bkeys.push_back(k->column_idx);
+  struct GroupPtrs {
+    std::string F;
+    std::vector<std::string> SV, SC;
+  };
+  auto group_ptrs = [&](KernelSource& ks) {
+    GroupPtrs gp;
+    gp.F = ks.Ptr(first, "uint64_t");
+    for (size_t j = 0; j < plans.size(); j++) {
+      gp.SV.push_back(ks.Ptr(sv[j], "uint64_t"));
+      gp.SC.push_back(ks.Ptr(sc[j], "uint64_t"));
+    }
+    return gp;
+  };
+  // one joined row folded into the state of build row g
+  auto fold = [&](KernelSource& ks, ExprGen& eg, const GroupPtrs& gp, const std::vector<CVal>& left,
+                  const std::vector<CVal>& right, const std::string& pos, const std::string& g) {
+    Scope s2;
+    s2.child.push_back(left);
+    s2.child.push_back(right);
+    std::vector<CVal> joined;
+    for (const auto& c : join.output) joined.push_back(eg.Emit(*c.expr, s2));
+    Scope s3;
+    s3.child.push_back(joined);
+    std::string fl = "0ULL";
+    for (size_t j = 0; j < plans.size(); j++) {
+      CVal c = eg.Emit(plans[j].agg->kid(0), s3);
+      if (plans[j].count_flag >= 0)
+        fl += " | ((" + c.n + ") ? " + std::to_string(1 << plans[j].count_flag) + "ULL : 0ULL)";
+      counted[j] = NeedsCount(plans[j], c);
+      EmitGroupUpdate(ks, eg, plans[j], c, gp.SV[j], gp.SC[j], g, counted[j]);
+    }
+    // every row of the group matches the same build row: the first
+    // position is the probe position alone (bits 40 and up)
+    ks.L("kdb_atomic_min_u64(&" + gp.F + "[" + g + "], ((uint64_t)(" + pos + ") << 40) | (" + fl + "));");
+  };
+  const Operator& probe_op = join.child(1);
+  const bool split = (probe_op.kind == OpKind::SCAN || probe_op.kind == OpKind::SCAN_SELECT) &&
+                     ctx_.OptStr("KDB_SPLIT_PROBE_GROUPS") && !ctx_.OptStr("KDB_VECTOR_PROBE_SCAN") &&
+                     !ctx_.OptStr("KDB_PROBE_AHEAD") && !ctx_.OptStr("KDB_PROBE_VEC") &&
+                     !ctx_.OptStr("KDB_LAZY_PROBE_COLUMNS");
+  if (split) {
+    // KDB_SPLIT_PROBE_GROUPS: two kernels.  Measured on the Q3 shape it is
+    // slower than the one fused kernel (probe 43 + aggregation 19 us against
+    // 52 us): the probe stays bound by its dependent table accesses however
+    // few bytes it streams.  The probe reads only the probe keys (and filter
+    // columns), probes the table and writes each match as a (build row,
+    // probe row) pair into its CTA's region of a pair buffer (a probe row
+    // matches at most one build row: the build key is unique, so a CTA's
+    // matches fit in the rows it scans); the aggregation then loads the
+    // measure columns for the matched rows only and folds them into the
+    // build rows.  Non-matching rows cost their key bytes alone.
+    const int block = 256;
+    const int64_t prow = std::max<int64_t>(ctx_.tables.at(probe_op.relation).rows, 1);
+    const int G = ctx_.GridFor(prow, block);
+    const int64_t per_cta = (prow + static_cast<int64_t>(G) * block - 1) / (static_cast<int64_t>(G) * block) * block;
+    uint64_t* pairs = arena_.AllocT<uint64_t>(static_cast<int64_t>(G) * per_cta);
+    uint32_t* pcount = arena_.AllocT<uint32_t>(G);
+    // scan columns the probe needs: its filters' and its keys'
+    std::set<int> key_cols_scan;
+    std::function<void(const Expr&)> scan_refs = [&](const Expr& e) {
+      if (e.kind == ExprKind::VirtColRef || e.kind == ExprKind::ColRef) key_cols_scan.insert(e.column_idx);
+      for (const auto& k : e.kids) scan_refs(*k);
+    };
+    for (const auto& f : probe_op.filters) scan_refs(*f);
+    std::function<void(const Expr&)> key_refs = [&](const Expr& e) {
+      if (e.kind == ExprKind::ColRef && e.child_idx == 1) scan_refs(*probe_op.output.at(e.column_idx).expr);
+      for (const auto& k : e.kids) key_refs(*k);
+    };
+    for (const auto& k : join.right_keys) key_refs(*k);
+    {
+      KernelSource ks;
+      ExprGen eg(ctx_, ks);
+      ks.pre << "  __shared__ unsigned kdb_block_rows;\n"
+                "  if (threadIdx.x == 0) kdb_block_rows = 0;\n"
+                "  __syncthreads();\n";
+      const std::string P = ks.Ptr(pairs, "uint64_t"), PC = ks.Ptr(pcount, "uint32_t");
+      const std::string RW = ks.Word(static_cast<uint64_t>(per_cta));
+      const std::string ERR = ks.Ptr(ctx_.d_err, "int");
+      int64_t src_rows = 0;
+      auto body = [&](const std::vector<CVal>& right, const std::string& pos) {
+        Scope s;
+        s.child.resize(2);
+        s.child[1] = right;
+        std::vector<CVal> pk;
+        for (const auto& k : join.right_keys) pk.push_back(eg.Emit(*k, s));
+        EmitProbe(ks, eg, jt, bkeys, pk, [&](const std::vector<CVal>&, const std::string&) {
+          ks.L("const uint32_t kdb_s = kdb_alloc_block_slot(&kdb_block_rows);");
+          ks.L("if (kdb_s < (uint32_t)" + RW + ") " + P + "[(int64_t)blockIdx.x * (int64_t)" + RW +
+               " + kdb_s] = ((uint64_t)(uint32_t)" + probe_br_ + " << 32) | (uint64_t)(uint32_t)(" + pos + ");");
+          ks.L("else kdb_set_error(" + ERR + ", 1);");
+        });
+      };
+      probe_side_scan_ = true;
+      prefetch_only_ = &key_cols_scan;
+      EmitStream(ks, eg, probe_op, body, src_rows);
+      probe_side_scan_ = false;
+      prefetch_only_ = nullptr;
+      ks.L("__syncthreads();");
+      ks.L("if (threadIdx.x == 0) " + PC + "[blockIdx.x] = kdb_block_rows < (unsigned)" + RW +
+           " ? kdb_block_rows : (unsigned)" + RW + ";");
+      LaunchPipeline(ks, src_rows, "join probe", block);
+    }
+    {
+      KernelSource ks;
+      ExprGen eg(ctx_, ks);
+      GroupPtrs gp = group_ptrs(ks);
+      const std::string P = ks.Ptr(pairs, "uint64_t", true), PC = ks.Ptr(pcount, "uint32_t", true);
+      const std::string RW = ks.Word(static_cast<uint64_t>(per_cta)), GW = ks.Word(static_cast<uint64_t>(G));
+      ks.Open("for (int64_t kdb_b = blockIdx.x; kdb_b < (int64_t)" + GW + "; kdb_b += gridDim.x)");
+      ks.L("const uint32_t kdb_n = " + PC + "[kdb_b];");
+      ks.Open("for (uint32_t kdb_i = threadIdx.x; kdb_i < kdb_n; kdb_i += blockDim.x)");
+      ks.L("const uint64_t kdb_pr = " + P + "[kdb_b * (int64_t)" + RW + " + kdb_i];");
+      ks.L("const int64_t r = (int64_t)(uint32_t)kdb_pr;");
+      ks.L("const int64_t kdb_br = (int64_t)(kdb_pr >> 32);");
+      std::vector<CVal> right = EmitScanRowAt(ks, eg, probe_op, "r");
+      std::vector<CVal> left = LoadMatRow(ks, eg, jt.build, "kdb_br", nullptr);
+      fold(ks, eg, gp, left, right, "(uint64_t)r", "kdb_br");
+      ks.Close();
+      ks.Close();
+      LaunchPipeline(ks, static_cast<int64_t>(G) * block, "group by", block);
+    }
+  } else {
     KernelSource ks;
     ExprGen eg(ctx_, ks);
-    std::string F = ks.Ptr(first, "uint64_t");
-    std::vector<std::string> SV(plans.size()), SC(plans.size());
-    for (size_t j = 0; j < plans.size(); j++) {
-      SV[j] = ks.Ptr(sv[j], "uint64_t");
-      SC[j] = ks.Ptr(sc[j], "uint64_t");
-    }
-    std::vector<int> bkeys;
-    for (const auto& k : join.left_keys) bkeys.push_back(k->column_idx);
+    GroupPtrs gp = group_ptrs(ks);
     int64_t src_rows = 0;
     auto body = [&](const std::vector<CVal>& right, const std::string& pos) {
       Scope s;
@@ -2677,27 +2992,8 @@ MatBuffer Executor::RunGroupByBuildRows(const Operator& op, const std::vector<Ag
       s.child[1] = right;
       std::vector<CVal> pk;
       for (const auto& k : join.right_keys) pk.push_back(eg.Emit(*k, s));
-      EmitProbe(ks, eg, jt, bkeys, pk, [&](const std::vector<CVal>& left, const std::string& bpos) {
-        const std::string g = probe_br_;
-        Scope s2;
-        s2.child.push_back(left);
-        s2.child.push_back(right);
-        std::vector<CVal> joined;
-        for (const auto& c : join.output) joined.push_back(eg.Emit(*c.expr, s2));
-        Scope s3;
-        s3.child.push_back(joined);
-        std::string fl = "0ULL";
-        for (size_t j = 0; j < plans.size(); j++) {
-          CVal c = eg.Emit(plans[j].agg->kid(0), s3);
-          if (plans[j].count_flag >= 0)
-            fl += " | ((" + c.n + ") ? " + std::to_string(1 << plans[j].count_flag) + "ULL : 0ULL)";
-          counted[j] = NeedsCount(plans[j], c);
-          EmitGroupUpdate(ks, eg, plans[j], c, SV[j], SC[j], g, counted[j]);
-        }
-        // every row of the group matches the same build row: the first
-        // position is the probe position alone (bits 40 and up)
-        (void)bpos;
-        ks.L("kdb_atomic_min_u64(&" + F + "[" + g + "], ((uint64_t)(" + pos + ") << 40) | (" + fl + "));");
+      EmitProbe(ks, eg, jt, bkeys, pk, [&](const std::vector<CVal>& left, const std::string&) {
+        fold(ks, eg, gp, left, right, pos, probe_br_);
       });
     };
     probe_side_scan_ = !ctx_.OptStr("KDB_VECTOR_PROBE_SCAN");
@@ -4673,10 +4969,6 @@ MatBuffer Executor::RunSkinner(const Operator& op, const SkinnerAgg* agg) {
   const int T = static_cast<int>(op.children.size());
   if (T > 16) throw Error(-5, "Skinner join of more than 16 tables");
   if (op.conditions.size() > 64) throw Error(-5, "Skinner join with more than 64 conditions");
-  for (int t = 0; t < T; t++)
-    if (!mats_.count(&op.child(t))) mats_[&op.child(t)] = Materialize(op.child(t));
-  std::vector<const MatBuffer*> mats;
-  for (int t = 0; t < T; t++) mats.push_back(&mats_.at(&op.child(t)));
   // equality predicates between two children: the join graph and indexes
   std::vector<SkinnerPred> preds;
   for (size_t c = 0; c < op.conditions.size(); c++) {
@@ -4687,8 +4979,51 @@ MatBuffer Executor::RunSkinner(const Operator& op, const SkinnerAgg* agg) {
     if (x.kind != ExprKind::ColRef || y.kind != ExprKind::ColRef || x.child_idx == y.child_idx) continue;
     preds.push_back({static_cast<int>(c), x.child_idx, x.column_idx, y.child_idx, y.column_idx});
   }
+  // the join columns each child needs an index on
+  std::vector<std::set<int>> index_cols(T);
+  for (const auto& pr : preds) {
+    index_cols[pr.tb].insert(pr.cb);
+    index_cols[pr.ta].insert(pr.ca);
+  }
   std::vector<std::vector<JoinTable>> index_for(T);
-  for (int t = 0; t < T; t++) index_for[t].resize(mats[t]->cols.size());
+  for (int t = 0; t < T; t++) {
+    const Operator& child = op.child(t);
+    // A serving slot reuses a child's rows and indexes built by an earlier
+    // request (the build cache waits on the event that follows their
+    // construction); a plain query builds them itself.
+    std::shared_ptr<BuildEntry> cached;
+    std::string key;
+    if (ctx_.build_cache && !ctx_.dry && !mats_.count(&child) &&
+        (child.kind == OpKind::SCAN || child.kind == OpKind::SCAN_SELECT)) {
+      key = ChildSig(child, index_cols[t]);
+      cached = ctx_.build_cache->Find(key);
+      if (cached) {
+        KDB_CUDA(cudaStreamWaitEvent(ctx_.stream, cached->ready, 0));
+      } else {
+        cached = std::make_shared<BuildEntry>(ctx_);
+        arena_.RedirectTo(&cached->arena);
+        try {
+          cached->mat = Materialize(child);
+          cached->index.resize(cached->mat.cols.size());
+          for (int c : index_cols[t]) cached->index[c] = BuildGroupedIndex(cached->mat, c);
+        } catch (...) {
+          arena_.RedirectTo(nullptr);
+          throw;
+        }
+        arena_.RedirectTo(nullptr);
+        KDB_CUDA(cudaEventRecord(cached->ready, ctx_.stream));
+        cached = ctx_.build_cache->Insert(key, cached);
+      }
+      held_.push_back(cached);  // until this query is done with it
+      mats_[&child] = cached->mat;
+      index_for[t] = cached->index;
+      continue;
+    }
+    if (!mats_.count(&child)) mats_[&child] = Materialize(child);
+    index_for[t].resize(mats_.at(&child).cols.size());
+  }
+  std::vector<const MatBuffer*> mats;
+  for (int t = 0; t < T; t++) mats.push_back(&mats_.at(&op.child(t)));
   for (const auto& pr : preds) {
     if (!index_for[pr.tb][pr.cb].slots) index_for[pr.tb][pr.cb] = BuildGroupedIndex(*mats[pr.tb], pr.cb);
     if (!index_for[pr.ta][pr.ca].slots) index_for[pr.ta][pr.ca] = BuildGroupedIndex(*mats[pr.ta], pr.ca);

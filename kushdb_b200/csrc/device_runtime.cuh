@@ -393,14 +393,22 @@ KDB_DEV bool kdb_bloom_test(const uint32_t* __restrict__ bits, uint32_t h, int l
 }
 
 // Same, storing the (32-bit) key in the slot's high word instead of the hash.
-KDB_DEV void kdb_join_insert_keyed(uint64_t* slots, uint64_t mask, uint32_t h, uint32_t key, uint32_t row) {
+// Returns whether the walk passed a slot holding the same key: of two rows
+// with equal keys (same hash, same walk; slots are only ever filled) the one
+// inserted second always passes the first one's slot, so a table with a
+// duplicate key reports it at least once.
+KDB_DEV bool kdb_join_insert_keyed(uint64_t* slots, uint64_t mask, uint32_t h, uint32_t key, uint32_t row) {
   uint64_t e = ((uint64_t)key << 32) | (uint64_t)(row + 1);
   const uint32_t m = (uint32_t)mask;
   uint32_t i = h & m;
+  bool dup = false;
   for (uint32_t k = 0; k <= m; k++) {
-    if (atomicCAS((unsigned long long*)&slots[i], 0ULL, (unsigned long long)e) == 0ULL) return;
+    const unsigned long long old = atomicCAS((unsigned long long*)&slots[i], 0ULL, (unsigned long long)e);
+    if (old == 0ULL) return dup;
+    dup |= (uint32_t)(old >> 32) == key;
     i = (i + 1) & m;
   }
+  return dup;
 }
 
 KDB_DEV void kdb_join_insert(uint64_t* slots, uint64_t mask, uint32_t h, uint32_t row) {

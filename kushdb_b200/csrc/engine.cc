@@ -75,6 +75,7 @@ Arena::~Arena() {
 }
 
 void* Arena::Alloc(size_t bytes) {
+  if (redirect_) return redirect_->Alloc(bytes);
   if (bytes == 0) bytes = 16;
   if (ctx_.dry) return ctx_.DevAlloc(bytes);
   void* p = nullptr;

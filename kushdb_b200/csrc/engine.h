@@ -157,12 +157,24 @@ class Arena {
     return static_cast<T*>(Alloc(count * sizeof(T) + 16));
   }
   size_t bytes() const { return bytes_; }
+  // While set, allocations are made by `to` (an owner that outlives this
+  // query, such as a serving build-cache entry) instead.
+  void RedirectTo(Arena* to) { redirect_ = to; }
 
  private:
   Context& ctx_;
   std::vector<void*> ptrs_;
   size_t bytes_ = 0;
+  Arena* redirect_ = nullptr;
 };
+
+// Build-side state a serving loop keeps on the device across requests
+// (defined with the executor): a Skinner join child's filtered rows and its
+// join-column indexes, keyed by what the child reads and filters.
+struct BuildCache;
+std::shared_ptr<BuildCache> MakeBuildCache(size_t max_bytes);
+// hits, misses, cached bytes and entries so far
+void BuildCacheStats(BuildCache& c, int64_t* hits, int64_t* misses, int64_t* bytes, int64_t* entries);
 
 class Context {
  public:
@@ -197,6 +209,9 @@ class Context {
   // 2 = uniformly random connected orders (training-data collection).
   int skinner_policy = 0;
   JoinPrior* join_prior = nullptr;
+  // Serving slots: children and indexes of Skinner joins reused across
+  // requests (null: every query builds its own, like the reference).
+  std::shared_ptr<BuildCache> build_cache;
   // (features, reward) of every (prefix, next table) step of every episode
   // of the last Skinner join, when logging is on
   bool skinner_log = false;

@@ -38,8 +38,15 @@ __global__ void __launch_bounds__(kSortBlock) RadixHistogram(const uint64_t* __r
   __syncthreads();
   int64_t base = static_cast<int64_t>(blockIdx.x) * tile;
   int64_t end = min(base + tile, n);
-  for (int64_t i = base + threadIdx.x; i < end; i += blockDim.x)
-    atomicAdd(&h[(keys[i] >> shift) & 0xff], 1u);
+  const int lane = threadIdx.x & 31;
+  // one shared-memory atomic per distinct digit in a warp: a skewed key
+  // column (many equal keys) would otherwise serialise the block on one counter
+  for (int64_t c = base; c < end; c += blockDim.x) {
+    const int64_t i = c + threadIdx.x;
+    const uint32_t d = i < end ? static_cast<uint32_t>((keys[i] >> shift) & 0xff) : 256u;
+    const unsigned peers = __match_any_sync(0xffffffffu, d);
+    if (d < 256u && lane == __ffs(peers) - 1) atomicAdd(&h[d], static_cast<uint32_t>(__popc(peers)));
+  }
   __syncthreads();
   for (int d = threadIdx.x; d < 256; d += blockDim.x) hist[d * nblocks + blockIdx.x] = h[d];
 }
@@ -51,10 +58,18 @@ __global__ void __launch_bounds__(kSortBlock) RadixDigitCounts(const uint64_t* _
   __shared__ uint32_t h[8][256];
   for (int i = threadIdx.x; i < 8 * 256; i += blockDim.x) (&h[0][0])[i] = 0;
   __syncthreads();
-  for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < n;
-       i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
-    const uint64_t k = keys[i];
-    for (int p = 0; p < passes; p++) atomicAdd(&h[p][(k >> (8 * p)) & 0xff], 1u);
+  const int lane = threadIdx.x & 31;
+  const int64_t stride = static_cast<int64_t>(gridDim.x) * blockDim.x;
+  // whole warps step together so that equal digits in a warp add once
+  for (int64_t c = blockIdx.x * static_cast<int64_t>(blockDim.x); c < n; c += stride) {
+    const int64_t i = c + threadIdx.x;
+    const bool valid = i < n;
+    const uint64_t k = valid ? keys[i] : 0;
+    for (int p = 0; p < passes; p++) {
+      const uint32_t d = valid ? static_cast<uint32_t>((k >> (8 * p)) & 0xff) : 256u;
+      const unsigned peers = __match_any_sync(0xffffffffu, d);
+      if (d < 256u && lane == __ffs(peers) - 1) atomicAdd(&h[p][d], static_cast<uint32_t>(__popc(peers)));
+    }
   }
   __syncthreads();
   for (int i = threadIdx.x; i < passes * 256; i += blockDim.x) {
@@ -246,12 +261,22 @@ __global__ void __launch_bounds__(kSortBlock) RadixScatter(
       total[d] = run;
     }
     __syncthreads();
+    const uint32_t dst = valid ? base[digit] + wcnt[warp][digit] + rank : 0u;
     if (valid) {
-      uint32_t dst = base[digit] + wcnt[warp][digit] + rank;
       kout[dst] = k;
       vout[dst] = v;
-      if (next_hist)
-        atomicAdd(&next_hist[static_cast<int64_t>((k >> next_shift) & 0xff) * nblocks + dst / tile], 1u);
+    }
+    if (next_hist) {
+      // one global atomic per distinct (next digit, destination tile) in the
+      // warp: equal keys land in consecutive slots of one tile, and a hot key
+      // would otherwise queue thousands of atomics on one counter
+      const uint32_t slot = valid ? (dst / static_cast<uint32_t>(tile)) * 256u +
+                                        static_cast<uint32_t>((k >> next_shift) & 0xff)
+                                  : 0xffffffffu;
+      const unsigned grp = __match_any_sync(0xffffffffu, slot);
+      if (valid && lane == __ffs(grp) - 1)
+        atomicAdd(&next_hist[static_cast<int64_t>(slot & 0xffu) * nblocks + (slot >> 8)],
+                  static_cast<uint32_t>(__popc(grp)));
     }
     __syncthreads();
     for (int d = threadIdx.x; d < 256; d += blockDim.x) base[d] += total[d];
@@ -758,16 +783,24 @@ __global__ void SampleBucketSort(const SortItem* __restrict__ src, const unsigne
 // ---------------------------------------------------------------------------
 // Range-bucket sort of 16-byte items by (key, tie): the keys' minimum and
 // maximum split the key range into kRangeBuckets equal-width buckets (a
-// bucket index never decreases with the key), one pass counts the buckets,
-// one block scans the counts, one pass scatters, and one CTA per bucket
-// sorts it in shared memory.  Equal keys share a bucket, so many ties (or a
-// skewed range) make a large bucket; the caller then uses the merge sort.
+// bucket index never decreases with the key).  A few large blocks count
+// their own slices into per-block histograms (no global atomics), one
+// block turns them into bucket offsets and per-block bases, the same blocks
+// scatter their items through shared-memory cursors, and one CTA per
+// bucket ranks its items in shared memory.
+// Equal keys share a bucket, so many ties (or a very skewed range) make a
+// bucket larger than kRangeBucketCap; the caller then uses the merge sort.
 // ---------------------------------------------------------------------------
 namespace {
 
 constexpr int kRangeBuckets = 1024;
+constexpr int kRangeBlocks = 32;       // blocks of the count and scatter passes
+constexpr int kRangeThreads = 1024;
+constexpr int kRangeBucketCap = 2048;  // items one CTA ranks (32 KiB of shared memory)
 
-__global__ void RangeMinMax(const SortItem* __restrict__ items, int64_t n, unsigned long long* __restrict__ mm) {
+__global__ void __launch_bounds__(kRangeThreads) RangeMinMax(const SortItem* __restrict__ items, int64_t n,
+                                                             unsigned long long* __restrict__ mm) {
+  __shared__ unsigned long long slo[kRangeThreads / 32], shi[kRangeThreads / 32];
   unsigned long long lo = ~0ULL, hi = 0;
   for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < n;
        i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
@@ -780,49 +813,66 @@ __global__ void RangeMinMax(const SortItem* __restrict__ items, int64_t n, unsig
     lo = a < lo ? a : lo;
     hi = b > hi ? b : hi;
   }
+  const int warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
   if ((threadIdx.x & 31) == 0) {
+    slo[warp] = lo;
+    shi[warp] = hi;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int w = 1; w < nw; w++) {
+      lo = slo[w] < lo ? slo[w] : lo;
+      hi = shi[w] > hi ? shi[w] : hi;
+    }
     atomicMin(&mm[0], lo);
     atomicMax(&mm[1], hi);
   }
 }
 
-__device__ __forceinline__ int RangeBucket(unsigned long long k, const unsigned long long* mm) {
-  const unsigned long long lo = mm[0], range = mm[1] - mm[0];
+__device__ __forceinline__ int RangeBucket(unsigned long long k, unsigned long long lo, unsigned long long range) {
   // (k - lo) / (range + 1) * B in doubles: rounding keeps it monotonic
   const double f = static_cast<double>(k - lo) / (static_cast<double>(range) + 1.0);
   const int b = static_cast<int>(f * kRangeBuckets);
   return b < 0 ? 0 : (b >= kRangeBuckets ? kRangeBuckets - 1 : b);
 }
 
-__global__ void RangeCount(const SortItem* __restrict__ items, int64_t n, const unsigned long long* __restrict__ mm,
-                           uint16_t* __restrict__ bucket_of, unsigned* __restrict__ counts) {
+// items of block blk: [blk * chunk, min(n, (blk + 1) * chunk))
+__device__ __forceinline__ int64_t RangeChunk(int64_t n) { return (n + kRangeBlocks - 1) / kRangeBlocks; }
+
+// per-block bucket histograms: bh[blk * kRangeBuckets + b]
+__global__ void __launch_bounds__(kRangeThreads) RangeCount(const SortItem* __restrict__ items, int64_t n,
+                                                            const unsigned long long* __restrict__ mm,
+                                                            uint16_t* __restrict__ bucket_of,
+                                                            unsigned* __restrict__ bh) {
   __shared__ unsigned cnt[kRangeBuckets];
-  __shared__ unsigned long long smm[2];
   for (int j = threadIdx.x; j < kRangeBuckets; j += blockDim.x) cnt[j] = 0;
-  if (threadIdx.x < 2) smm[threadIdx.x] = mm[threadIdx.x];
   __syncthreads();
-  for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < n;
-       i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
-    const int b = RangeBucket(items[i].key, smm);
+  const unsigned long long lo = mm[0], range = mm[1] - mm[0];
+  const int64_t c = RangeChunk(n), b0 = blockIdx.x * c, b1 = b0 + c < n ? b0 + c : n;
+  for (int64_t i = b0 + threadIdx.x; i < b1; i += blockDim.x) {
+    const int b = RangeBucket(items[i].key, lo, range);
     bucket_of[i] = static_cast<uint16_t>(b);
     atomicAdd(&cnt[b], 1u);
   }
   __syncthreads();
-  for (int j = threadIdx.x; j < kRangeBuckets; j += blockDim.x)
-    if (cnt[j]) atomicAdd(&counts[j], cnt[j]);
+  for (int j = threadIdx.x; j < kRangeBuckets; j += blockDim.x) bh[blockIdx.x * kRangeBuckets + j] = cnt[j];
 }
 
-// one block of kRangeBuckets threads: exclusive offsets (offs[B] = total),
-// cursors zeroed, the largest bucket into *largest
-__global__ void __launch_bounds__(kRangeBuckets) RangeOffsets(const unsigned* __restrict__ counts,
+// one block, one thread per bucket: bucket offsets (offs[B] = total), the
+// largest bucket, and in place of each block's histogram that block's first
+// slot in every bucket
+__global__ void __launch_bounds__(kRangeBuckets) RangeOffsets(unsigned* __restrict__ bh,
                                                               unsigned* __restrict__ offs,
-                                                              unsigned* __restrict__ cursor,
                                                               unsigned* __restrict__ largest) {
-  __shared__ unsigned ws[kRangeBuckets / 32];
-  __shared__ unsigned wmax[kRangeBuckets / 32];
+  static_assert(kRangeBuckets == 1024, "one thread per bucket");
+  __shared__ unsigned ws[32], wmax[32];
   const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
-  const unsigned c = counts[t];
-  unsigned incl = c, mx = c;
+  unsigned h[kRangeBlocks], tot = 0;
+#pragma unroll
+  for (int blk = 0; blk < kRangeBlocks; blk++) h[blk] = bh[blk * kRangeBuckets + t];
+#pragma unroll
+  for (int blk = 0; blk < kRangeBlocks; blk++) tot += h[blk];
+  unsigned incl = tot, mx = tot;
   for (int o = 1; o < 32; o <<= 1) {
     const unsigned y = __shfl_up_sync(0xffffffffu, incl, o);
     if (lane >= o) incl += y;
@@ -844,10 +894,50 @@ __global__ void __launch_bounds__(kRangeBuckets) RangeOffsets(const unsigned* __
     if (lane == 0) *largest = m;
   }
   __syncthreads();
-  const unsigned before = (warp ? ws[warp - 1] : 0u) + incl - c;
-  offs[t] = before;
-  if (t == kRangeBuckets - 1) offs[kRangeBuckets] = before + c;
-  cursor[t] = 0;
+  unsigned base = (warp ? ws[warp - 1] : 0u) + incl - tot;
+  offs[t] = base;
+#pragma unroll
+  for (int blk = 0; blk < kRangeBlocks; blk++) {
+    bh[blk * kRangeBuckets + t] = base;
+    base += h[blk];
+  }
+  if (t == kRangeBuckets - 1) offs[kRangeBuckets] = base;
+}
+
+// the count pass's blocks again: every item to its bucket's next slot
+__global__ void __launch_bounds__(kRangeThreads) RangeScatter(const SortItem* __restrict__ items, int64_t n,
+                                                              const uint16_t* __restrict__ bucket_of,
+                                                              const unsigned* __restrict__ bh,
+                                                              SortItem* __restrict__ out) {
+  __shared__ unsigned cur[kRangeBuckets];
+  for (int j = threadIdx.x; j < kRangeBuckets; j += blockDim.x) cur[j] = bh[blockIdx.x * kRangeBuckets + j];
+  __syncthreads();
+  const int64_t c = RangeChunk(n), b0 = blockIdx.x * c, b1 = b0 + c < n ? b0 + c : n;
+  for (int64_t i = b0 + threadIdx.x; i < b1; i += blockDim.x) {
+    const unsigned pos = atomicAdd(&cur[bucket_of[i]], 1u);
+    out[pos] = items[i];
+  }
+}
+
+// one CTA per bucket: the bucket's items in shared memory, and each item
+// written at its rank (the number of smaller items; (key, tie) pairs are
+// unique, so ranks are distinct).  Every thread reads the same item at the
+// same time (a broadcast), and the comparisons of one item are independent,
+// so they pipeline.
+__global__ void RangeRankSort(const SortItem* __restrict__ src, const unsigned* __restrict__ offs,
+                              SortItem* __restrict__ dst) {
+  extern __shared__ SortItem sr[];
+  const unsigned b0 = offs[blockIdx.x], cnt = offs[blockIdx.x + 1] - b0;
+  if (cnt == 0) return;
+  for (unsigned i = threadIdx.x; i < cnt; i += blockDim.x) sr[i] = src[b0 + i];
+  __syncthreads();
+  for (unsigned i = threadIdx.x; i < cnt; i += blockDim.x) {
+    const SortItem x = sr[i];
+    unsigned r = 0;
+#pragma unroll 4
+    for (unsigned j = 0; j < cnt; j++) r += ItemLess(sr[j], x) ? 1u : 0u;
+    dst[b0 + r] = x;
+  }
 }
 
 }  // namespace
@@ -859,34 +949,29 @@ bool Context::RangeSortItems(void* items_v, int64_t n, Arena& arena) {
   SortItem* tmp = reinterpret_cast<SortItem*>(arena.Alloc(sizeof(SortItem) * n));
   uint16_t* bof = reinterpret_cast<uint16_t*>(arena.Alloc(sizeof(uint16_t) * n));
   unsigned long long* mm = arena.AllocT<unsigned long long>(2);
-  unsigned* counts = arena.AllocT<unsigned>(kRangeBuckets);
+  unsigned* bh = arena.AllocT<unsigned>(kRangeBlocks * kRangeBuckets);
   unsigned* offs = arena.AllocT<unsigned>(kRangeBuckets + 1);
-  unsigned* cursor = arena.AllocT<unsigned>(kRangeBuckets);
   unsigned* largest = arena.AllocT<unsigned>(1);
   Memset(mm, 0xff, sizeof(unsigned long long));
   Memset(mm + 1, 0, sizeof(unsigned long long));
-  Memset(counts, 0, sizeof(unsigned) * kRangeBuckets);
-  const int grid = GridFor(n, 256);
+  const int mm_grid = static_cast<int>(std::min<int64_t>((n + kRangeThreads - 1) / kRangeThreads, 32));
   TimedStart("sort range");
-  Issue([=](cudaStream_t s) { RangeMinMax<<<grid, 256, 0, s>>>(items, n, mm); });
-  Issue([=](cudaStream_t s) { RangeCount<<<grid, 256, 0, s>>>(items, n, mm, bof, counts); });
-  Issue([=](cudaStream_t s) { RangeOffsets<<<1, kRangeBuckets, 0, s>>>(counts, offs, cursor, largest); });
+  Issue([=](cudaStream_t s) { RangeMinMax<<<mm_grid, kRangeThreads, 0, s>>>(items, n, mm); });
+  Issue([=](cudaStream_t s) { RangeCount<<<kRangeBlocks, kRangeThreads, 0, s>>>(items, n, mm, bof, bh); });
+  Issue([=](cudaStream_t s) { RangeOffsets<<<1, kRangeBuckets, 0, s>>>(bh, offs, largest); });
   TimedStop();
   KDB_CUDA(cudaGetLastError());
   // the bucket sizes decide (at recording; a replay runs on the same data)
   unsigned big = 0;
   D2H(&big, largest, sizeof(big));
-  if (big > static_cast<unsigned>(kBucketCap)) return false;
-  int m = 1;
-  while (m < static_cast<int>(big)) m <<= 1;
-  const size_t smem_bucket = sizeof(SortItem) * std::max(m, 1);
+  if (big > static_cast<unsigned>(kRangeBucketCap)) return false;
+  const size_t smem = sizeof(SortItem) * std::max<unsigned>(big, 1u);
+  if (smem > 48 * 1024)
+    KDB_CUDA(cudaFuncSetAttribute(RangeRankSort, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
+  const int threads = big > 512 ? 256 : 128;
   TimedStart("sort buckets");
-  Issue([=](cudaStream_t s) { SampleScatter<<<grid, 256, 0, s>>>(items, n, bof, offs, cursor, tmp); });
-  if (smem_bucket > 48 * 1024)
-    KDB_CUDA(cudaFuncSetAttribute(SampleBucketSort, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  static_cast<int>(smem_bucket)));
-  const int threads = std::min(512, std::max(32, m / 2));
-  Issue([=](cudaStream_t s) { SampleBucketSort<<<kRangeBuckets, threads, smem_bucket, s>>>(tmp, offs, items); });
+  Issue([=](cudaStream_t s) { RangeScatter<<<kRangeBlocks, kRangeThreads, 0, s>>>(items, n, bof, bh, tmp); });
+  Issue([=](cudaStream_t s) { RangeRankSort<<<kRangeBuckets, threads, smem, s>>>(tmp, offs, items); });
   TimedStop();
   KDB_CUDA(cudaGetLastError());
   return true;

@@ -61,9 +61,15 @@ int64_t EstimateFootprint(const Context& ctx, const plan::Operator& op) {
 class Server {
  public:
   Server(Context& parent, int slots, int64_t hbm_budget) : budget_(hbm_budget) {
+    // Build state kept across requests (Skinner children and their join
+    // indexes) takes up to a quarter of the budget; requests are admitted
+    // against the rest.
+    cache_ = MakeBuildCache(static_cast<size_t>(hbm_budget / 4));
+    budget_ = hbm_budget - hbm_budget / 4;
     for (int i = 0; i < slots; i++) {
       slots_.push_back(std::make_unique<Context>(parent));
       slots_.back()->ReserveHostBlocks(4, 16 << 20);  // pinned result blocks up front: no host-alloc syncs later
+      slots_.back()->build_cache = cache_;
     }
     for (int i = 0; i < slots; i++) workers_.emplace_back([this, i] { Loop(i); });
   }
@@ -75,6 +81,10 @@ class Server {
     }
     cv_.notify_all();
     for (auto& t : workers_) t.join();
+    // cached entries free their memory on the streams of the slots that
+    // built them: release them while those slots still exist
+    for (auto& s : slots_) s->build_cache.reset();
+    cache_.reset();
   }
 
   int64_t Submit(const std::string& plan_json, const Context& catalog) {
@@ -125,7 +135,11 @@ class Server {
       << ",\"p99_ms\":" << pct(lat, 0.99) << ",\"max_ms\":" << (lat.empty() ? 0 : lat.back())
       << ",\"service_p50_ms\":" << pct(svc, 0.5) << ",\"queries_per_second\":" << (span > 0 ? done / span : 0)
       << ",\"peak_in_flight\":" << peak_in_flight_ << ",\"slots\":" << slots_.size()
-      << ",\"hbm_budget\":" << budget_ << ",\"kernel_launches\":" << launches_ << "}";
+      << ",\"hbm_budget\":" << budget_ << ",\"kernel_launches\":" << launches_;
+    int64_t hits = 0, misses = 0, bytes = 0, entries = 0;
+    if (cache_) BuildCacheStats(*cache_, &hits, &misses, &bytes, &entries);
+    o << ",\"build_cache_hits\":" << hits << ",\"build_cache_misses\":" << misses
+      << ",\"build_cache_bytes\":" << bytes << ",\"build_cache_entries\":" << entries << "}";
     return o.str();
   }
 
@@ -192,6 +206,7 @@ class Server {
   }
 
   int64_t budget_;
+  std::shared_ptr<BuildCache> cache_;
   std::vector<std::unique_ptr<Context>> slots_;
   std::vector<std::thread> workers_;
   std::mutex mu_;

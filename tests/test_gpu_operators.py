@@ -363,16 +363,14 @@ def test_skinner_operator_matches_plan(engine):
 
 
 def _sorted_rows(cols, keys, asc, rows):
-    """Python restatement of the ORDER BY order: per key, NULL after every
-    value ascending and before every value descending; a stable sort keeps
-    tied rows in input order."""
+    """Python restatement of the ORDER BY order: NULL compares above every
+    value (compile/proxy/evaluate.cc:339-351), so it comes after every value
+    ascending and before every value descending; a stable sort keeps tied
+    rows in input order (Python's reverse=True sort is stable too)."""
     out = list(rows)
     for k, a in reversed(list(zip(keys, asc))):
         vals, nulls = cols[k]
-        if a:
-            out.sort(key=lambda r: (1, 0) if nulls[r] else (0, vals[r]))
-        else:
-            out.sort(key=lambda r: (0, 0) if nulls[r] else (1, vals[r]), reverse=True)
+        out.sort(key=lambda r: (1, 0) if nulls[r] else (0, vals[r]), reverse=not a)
     return out
 
 

@@ -73,6 +73,28 @@ def test_mix_matches_alone(setup, slots):
         assert st["peak_in_flight"] > 1
 
 
+def test_build_cache_reuses_skinner_children(setup):
+    """Requests after the first reuse the Skinner join's filtered children and
+    join indexes that the first built (build-cache hits, no new misses) and
+    return the query's plain result."""
+    from kushdb_b200.engine import Server
+    e, _, plans = setup
+    sk = plans[-1]
+    alone = e.execute(sk)
+    with Server(e, slots=2, hbm_budget_bytes=16 << 30) as srv:
+        first = srv.wait(srv.submit(sk))
+        st0 = srv.stats()
+        again = [srv.wait(srv.submit(sk)) for _ in range(3)]
+        st = srv.stats()
+    assert compare(first, alone) == ""
+    for r in again:
+        assert compare(r, alone) == ""
+    assert st0["build_cache_misses"] > 0 and st0["build_cache_hits"] == 0
+    assert st0["build_cache_bytes"] > 0 and st0["build_cache_entries"] == st0["build_cache_misses"]
+    assert st["build_cache_misses"] == st0["build_cache_misses"]
+    assert st["build_cache_hits"] == 3 * st0["build_cache_misses"]
+
+
 def test_admission_respects_budget(setup):
     """A budget below every request's footprint admits one query at a time."""
     from kushdb_b200.engine import Server
