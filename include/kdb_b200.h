@@ -398,7 +398,11 @@ void kdb_batch_free(kdb_batch* b);
  * its own CUDA stream, take queued plans as soon as a slot is free and the
  * request's estimated device footprint fits `hbm_budget_bytes` beside the
  * ones in flight, so queries of different shapes run concurrently.  Tables
- * must not be added or dropped while a server runs. */
+ * must not be added or dropped while a server runs.  A quarter of the budget
+ * holds build state kept across requests: the filtered children of Skinner
+ * joins and their join-column indexes, reused by later requests that read
+ * the same children (requests are admitted against the other three
+ * quarters). */
 typedef struct kdb_server kdb_server;
 int kdb_server_start(kdb_ctx* ctx, int32_t slots, int64_t hbm_budget_bytes, kdb_server** out);
 /* Queues a plan (same JSON as kdb_query_execute); returns a ticket > 0 or a
@@ -409,8 +413,9 @@ int64_t kdb_server_submit(kdb_server* s, const char* plan_json);
  * owning context).  Waits up to wait_ms for completion. */
 int kdb_server_poll(kdb_server* s, int64_t ticket, int64_t wait_ms, kdb_result** out);
 /* JSON: completed, failed, p50_ms, p99_ms, max_ms (submission to completion),
- * service_p50_ms, queries_per_second, peak_in_flight, slots, hbm_budget,
- * kernel_launches.
+ * service_p50_ms, queries_per_second, peak_in_flight, slots, hbm_budget (the
+ * admission budget), kernel_launches, build_cache_hits, build_cache_misses,
+ * build_cache_bytes, build_cache_entries.
  * Returns the size needed including the NUL. */
 int64_t kdb_server_stats(kdb_server* s, char* buf, int64_t cap);
 /* Finishes the requests in flight, drops queued ones, joins the workers. */

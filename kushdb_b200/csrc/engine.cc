@@ -28,6 +28,7 @@ struct Driver {
                            unsigned, CUstream, void**, void**) = nullptr;
   CUresult (*ModuleUnload)(CUmodule) = nullptr;
   CUresult (*FuncSetAttribute)(CUfunction, CUfunction_attribute, int) = nullptr;
+  CUresult (*LaunchKernelEx)(const CUlaunchConfig*, CUfunction, void**, void**) = nullptr;
   bool loaded = false;
 
   template <typename F>
@@ -46,6 +47,7 @@ struct Driver {
     Get("cuLaunchKernel", LaunchKernel);
     Get("cuModuleUnload", ModuleUnload);
     Get("cuFuncSetAttribute", FuncSetAttribute);
+    Get("cuLaunchKernelEx", LaunchKernelEx);
     loaded = true;
   }
 };
@@ -614,9 +616,40 @@ CUfunction Context::Kernel(const std::string& source, const std::string& name) {
     CUfunction fn;
     CuCheck(g_drv.ModuleGetFunction(&fn, prog.module, name.c_str()), "cuModuleGetFunction");
     f = prog.fns.emplace(name, fn).first;
+    // a kernel whose first statement waits for the preceding grid may be
+    // launched before that grid has finished (programmatic dependent launch)
+    if (source.find(kGridDependencyWait) != std::string::npos) cache_->waits.insert(fn);
   }
   return f->second;
 }
+
+namespace {
+
+// One kernel launch; `pdl`: with programmatic stream serialization, so the
+// kernel's CTAs may be scheduled while the previous kernel in the stream
+// drains (they wait at their first statement until it has completed and
+// its memory is visible).
+CUresult LaunchOne(CUfunction f, int grid, int block, size_t smem, CUstream s, void** params, bool pdl) {
+  if (!pdl)
+    return g_drv.LaunchKernel(f, grid, 1, 1, block, 1, 1, static_cast<unsigned>(smem), s, params, nullptr);
+  CUlaunchAttribute attr;
+  std::memset(&attr, 0, sizeof(attr));
+  attr.id = CU_LAUNCH_ATTRIBUTE_PROGRAMMATIC_STREAM_SERIALIZATION;
+  attr.value.programmaticStreamSerializationAllowed = 1;
+  CUlaunchConfig cfg;
+  std::memset(&cfg, 0, sizeof(cfg));
+  cfg.gridDimX = static_cast<unsigned>(grid);
+  cfg.gridDimY = cfg.gridDimZ = 1;
+  cfg.blockDimX = static_cast<unsigned>(block);
+  cfg.blockDimY = cfg.blockDimZ = 1;
+  cfg.sharedMemBytes = static_cast<unsigned>(smem);
+  cfg.hStream = s;
+  cfg.attrs = &attr;
+  cfg.numAttrs = 1;
+  return g_drv.LaunchKernelEx(&cfg, f, params, nullptr);
+}
+
+}  // namespace
 
 int Context::GridFor(int64_t n, int block) const {
   int64_t want = (n + block - 1) / block;
@@ -635,18 +668,20 @@ void Context::Launch(CUfunction f, int grid, int block, const KArgs& args, size_
     CuCheck(g_drv.FuncSetAttribute(f, CU_FUNC_ATTRIBUTE_MAX_DYNAMIC_SHARED_SIZE_BYTES,
                                    static_cast<int>(smem)),
             "cuFuncSetAttribute");
+  bool pdl = false;
+  if (!OptStr("KDB_NO_PDL")) {
+    std::lock_guard<std::mutex> lock(cache_->mu);
+    pdl = cache_->waits.count(f) != 0;
+  }
   TimedStart(tag);
-  CuCheck(g_drv.LaunchKernel(f, grid, 1, 1, block, 1, 1, static_cast<unsigned>(smem),
-                             reinterpret_cast<CUstream>(stream), params, nullptr),
-          "cuLaunchKernel");
+  CuCheck(LaunchOne(f, grid, block, smem, reinterpret_cast<CUstream>(stream), params, pdl), "cuLaunchKernel");
   TimedStop();
   if (rec) {
     rec->launches++;
     auto held = std::make_shared<KArgs>(args);
-    rec->ops.push_back([f, grid, block, smem, held](cudaStream_t s) {
+    rec->ops.push_back([f, grid, block, smem, held, pdl](cudaStream_t s) {
       void* p[] = {held.get()};
-      g_drv.LaunchKernel(f, grid, 1, 1, block, 1, 1, static_cast<unsigned>(smem), reinterpret_cast<CUstream>(s),
-                         p, nullptr);
+      LaunchOne(f, grid, block, smem, reinterpret_cast<CUstream>(s), p, pdl);
     });
   }
 }

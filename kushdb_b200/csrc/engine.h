@@ -18,6 +18,7 @@
 #include <stdexcept>
 #include <string>
 #include <unordered_map>
+#include <unordered_set>
 #include <vector>
 
 #include "host_result.h"
@@ -98,7 +99,17 @@ struct Program {
 struct ProgramCache {
   std::mutex mu;
   std::unordered_map<std::string, std::unique_ptr<Program>> programs;
+  // functions whose source starts with kGridDependencyWait (see Launch)
+  std::unordered_set<CUfunction> waits;
 };
+
+// First statement of every generated kernel: wait until the grid launched
+// before it in the stream has completed and its writes are visible (a no-op
+// unless the kernel was launched as a programmatic dependent), then let the
+// next kernel's CTAs be scheduled as this grid's CTAs finish.
+constexpr const char* kGridDependencyWait =
+    "  asm volatile(\"griddepcontrol.wait;\" ::: \"memory\");\n"
+    "  asm volatile(\"griddepcontrol.launch_dependents;\" ::: \"memory\");\n";
 
 // Host mirror of the device KArgs struct (passed by value).
 struct KArgs {

@@ -147,9 +147,11 @@ def declare_result_api(lib, prefix: str) -> None:
 
 
 def compare_tbl(expected: List[str], output: List[str], types: List[Type],
-                threshold: float = 1e-5) -> Optional[str]:
+                threshold: float = 1e-5, rel: float = 0.0) -> Optional[str]:
     """CHECK_EQ_TBL (util/test_util.h:82-175): ordered, REAL within an absolute
     threshold, TEXT/ENUM with surrounding quotes stripped, others exact.
+    `rel` > 0 also accepts a REAL within that relative distance (a parallel
+    summation order moves a sum of magnitude 1e9 by more than 1e-5).
     Returns None when equal, else a description of the first difference."""
     if len(expected) != len(output):
         return f"Differing table sizes: {len(expected)} vs {len(output)}"
@@ -171,7 +173,8 @@ def compare_tbl(expected: List[str], output: List[str], types: List[Type],
                     return f"({i},{j}) expected NULL got {ov!r}"
                 continue
             if t.type_id == "REAL":
-                if abs(float(ev) - float(ov)) >= threshold:
+                d = abs(float(ev) - float(ov))
+                if d >= threshold and d > rel * abs(float(ev)):
                     return f"({i},{j}) {ev} vs {ov}"
             elif t.type_id in ("TEXT", "ENUM"):
                 if len(ev) >= 2 and ev[0] == '"' and ev[-1] == '"':

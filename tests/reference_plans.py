@@ -448,9 +448,18 @@ _add("tpch/q06", tpch_q06, "tpch/q06_expected.tbl", "tbl")
 _add("tpch/q03_skinner", tpch_q03_skinner, "tpch/q03_expected.tbl", "tbl")
 
 
-def check(case: Case_, lines: List[str], types) -> str:
+# Float64 tolerance of GPU results against the reference's expected tables:
+# the reference's absolute 1e-5, or 1e-12 relative, whichever is larger.
+# Sums on the GPU add in another order than the reference's sequential loop
+# (atomics in the general group table, per-CTA partials elsewhere), and for a
+# sum near 1e9 an absolute 1e-5 is 1e-14 relative, a few dozen ulps.
+GPU_REL = 1e-12
+
+
+def check(case: Case_, lines: List[str], types, rel: float = 0.0) -> str:
     """Compare engine output lines with the expected table the way the
-    reference test does.  Returns '' when equal."""
+    reference test does (REAL also within `rel` relative, for GPU results).
+    Returns '' when equal."""
     from kushdb_b200.result import compare_tbl
     exp = case.expected_lines()
     if case.mode == "sorted":
@@ -468,5 +477,5 @@ def check(case: Case_, lines: List[str], types) -> str:
                     return f"line {i}: got {x!r} expected {y!r}"
             return f"line count {len(lines)} vs expected {len(exp)}"
         return ""
-    err = compare_tbl(exp, lines, types)
+    err = compare_tbl(exp, lines, types, rel=rel)
     return err or ""

@@ -30,7 +30,7 @@ def test_gpu_matches_reference_golden(engines, case):
     e, o = engines
     plan = case.build()
     res = e.execute(plan)
-    err = rp.check(case, res.lines, [c.type for c in res.columns])
+    err = rp.check(case, res.lines, [c.type for c in res.columns], rel=rp.GPU_REL)
     assert err == "", err
     ref = o.execute(plan)
     ordered = case.mode != "sorted"
@@ -50,7 +50,7 @@ def test_skinner_result_independent_of_budget_and_seed(engines, case, budget, se
     e.set_skinner(budget, seed)
     try:
         res = e.execute(case.build())
-        err = rp.check(case, res.lines, [c.type for c in res.columns])
+        err = rp.check(case, res.lines, [c.type for c in res.columns], rel=rp.GPU_REL)
         assert err == "", err
         if budget == 10:
             assert e.last_skinner_episodes() > 1

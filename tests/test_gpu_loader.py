@@ -66,7 +66,7 @@ def test_text_decoded_on_device_matches_fixture(engine):
                          ids=lambda c: c.name)
 def test_golden_case_on_files_read_from_disk(engine, case):
     res = engine.execute(case.build())
-    err = rp.check(case, res.lines, [c.type for c in res.columns])
+    err = rp.check(case, res.lines, [c.type for c in res.columns], rel=rp.GPU_REL)
     assert err == "", err
 
 
