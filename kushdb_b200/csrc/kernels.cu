@@ -783,20 +783,21 @@ __global__ void SampleBucketSort(const SortItem* __restrict__ src, const unsigne
 // ---------------------------------------------------------------------------
 // Range-bucket sort of 16-byte items by (key, tie): the keys' minimum and
 // maximum split the key range into kRangeBuckets equal-width buckets (a
-// bucket index never decreases with the key).  A few large blocks count
-// their own slices into per-block histograms (no global atomics), one
-// block turns them into bucket offsets and per-block bases, the same blocks
-// scatter their items through shared-memory cursors, and one CTA per
-// bucket ranks its items in shared memory.
-// Equal keys share a bucket, so many ties (or a very skewed range) make a
-// bucket larger than kRangeBucketCap; the caller then uses the merge sort.
+// bucket index never decreases with the key), one pass counts them, one
+// block scans the counts, one pass scatters every item into its bucket's
+// range, and then every item finds its final slot itself: its bucket's
+// start plus the number of items in the same bucket that order before it.
+// With many narrow buckets each item compares itself with a few dozen
+// others, all in parallel (no per-bucket sort whose largest bucket sets the
+// time).  Equal keys share a bucket, so many ties (or a very skewed range)
+// make a bucket larger than kRangeBucketCap; the caller then uses the merge
+// sort.
 // ---------------------------------------------------------------------------
 namespace {
 
-constexpr int kRangeBuckets = 1024;
-constexpr int kRangeBlocks = 32;       // blocks of the count and scatter passes
+constexpr int kRangeBuckets = 16384;
 constexpr int kRangeThreads = 1024;
-constexpr int kRangeBucketCap = 2048;  // items one CTA ranks (32 KiB of shared memory)
+constexpr unsigned kRangeBucketCap = 1024;  // items one bucket may hold
 
 __global__ void __launch_bounds__(kRangeThreads) RangeMinMax(const SortItem* __restrict__ items, int64_t n,
                                                              unsigned long long* __restrict__ mm) {
@@ -829,50 +830,51 @@ __global__ void __launch_bounds__(kRangeThreads) RangeMinMax(const SortItem* __r
   }
 }
 
-__device__ __forceinline__ int RangeBucket(unsigned long long k, unsigned long long lo, unsigned long long range) {
+__device__ __forceinline__ unsigned RangeBucket(unsigned long long k, unsigned long long lo, unsigned long long range) {
   // (k - lo) / (range + 1) * B in doubles: rounding keeps it monotonic
   const double f = static_cast<double>(k - lo) / (static_cast<double>(range) + 1.0);
   const int b = static_cast<int>(f * kRangeBuckets);
-  return b < 0 ? 0 : (b >= kRangeBuckets ? kRangeBuckets - 1 : b);
+  return b < 0 ? 0u : (b >= kRangeBuckets ? static_cast<unsigned>(kRangeBuckets - 1) : static_cast<unsigned>(b));
 }
 
-// items of block blk: [blk * chunk, min(n, (blk + 1) * chunk))
-__device__ __forceinline__ int64_t RangeChunk(int64_t n) { return (n + kRangeBlocks - 1) / kRangeBlocks; }
-
-// per-block bucket histograms: bh[blk * kRangeBuckets + b]
-__global__ void __launch_bounds__(kRangeThreads) RangeCount(const SortItem* __restrict__ items, int64_t n,
-                                                            const unsigned long long* __restrict__ mm,
-                                                            uint16_t* __restrict__ bucket_of,
-                                                            unsigned* __restrict__ bh) {
-  __shared__ unsigned cnt[kRangeBuckets];
-  for (int j = threadIdx.x; j < kRangeBuckets; j += blockDim.x) cnt[j] = 0;
-  __syncthreads();
+// bucket counts (global; few items per bucket, so the atomics rarely meet)
+__global__ void RangeCount(const SortItem* __restrict__ items, int64_t n, const unsigned long long* __restrict__ mm,
+                           uint16_t* __restrict__ bucket_of, unsigned* __restrict__ counts) {
   const unsigned long long lo = mm[0], range = mm[1] - mm[0];
-  const int64_t c = RangeChunk(n), b0 = blockIdx.x * c, b1 = b0 + c < n ? b0 + c : n;
-  for (int64_t i = b0 + threadIdx.x; i < b1; i += blockDim.x) {
-    const int b = RangeBucket(items[i].key, lo, range);
+  for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < n;
+       i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const unsigned b = RangeBucket(items[i].key, lo, range);
     bucket_of[i] = static_cast<uint16_t>(b);
-    atomicAdd(&cnt[b], 1u);
+    atomicAdd(&counts[b], 1u);
   }
-  __syncthreads();
-  for (int j = threadIdx.x; j < kRangeBuckets; j += blockDim.x) bh[blockIdx.x * kRangeBuckets + j] = cnt[j];
 }
 
-// one block, one thread per bucket: bucket offsets (offs[B] = total), the
-// largest bucket, and in place of each block's histogram that block's first
-// slot in every bucket
-__global__ void __launch_bounds__(kRangeBuckets) RangeOffsets(unsigned* __restrict__ bh,
+// one block: exclusive bucket offsets (offs[B] = total), each bucket's
+// cursor set to its offset, the largest bucket into *largest
+__global__ void __launch_bounds__(kRangeThreads) RangeOffsets(const unsigned* __restrict__ counts,
                                                               unsigned* __restrict__ offs,
+                                                              unsigned* __restrict__ cursor,
                                                               unsigned* __restrict__ largest) {
-  static_assert(kRangeBuckets == 1024, "one thread per bucket");
+  constexpr int kPer = kRangeBuckets / kRangeThreads;
   __shared__ unsigned ws[32], wmax[32];
   const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
-  unsigned h[kRangeBlocks], tot = 0;
+  static_assert(kPer % 4 == 0, "whole 16-byte vectors per thread");
+  unsigned c[kPer], tot = 0, mx = 0;
+  // a thread's buckets as 16-byte vectors (a warp reads 2 KiB contiguously)
 #pragma unroll
-  for (int blk = 0; blk < kRangeBlocks; blk++) h[blk] = bh[blk * kRangeBuckets + t];
+  for (int q = 0; q < kPer / 4; q++) {
+    const uint4 v = reinterpret_cast<const uint4*>(counts + t * kPer)[q];
+    c[4 * q] = v.x;
+    c[4 * q + 1] = v.y;
+    c[4 * q + 2] = v.z;
+    c[4 * q + 3] = v.w;
+  }
 #pragma unroll
-  for (int blk = 0; blk < kRangeBlocks; blk++) tot += h[blk];
-  unsigned incl = tot, mx = tot;
+  for (int q = 0; q < kPer; q++) {
+    tot += c[q];
+    mx = c[q] > mx ? c[q] : mx;
+  }
+  unsigned incl = tot;
   for (int o = 1; o < 32; o <<= 1) {
     const unsigned y = __shfl_up_sync(0xffffffffu, incl, o);
     if (lane >= o) incl += y;
@@ -894,49 +896,44 @@ __global__ void __launch_bounds__(kRangeBuckets) RangeOffsets(unsigned* __restri
     if (lane == 0) *largest = m;
   }
   __syncthreads();
-  unsigned base = (warp ? ws[warp - 1] : 0u) + incl - tot;
-  offs[t] = base;
+  unsigned run = (warp ? ws[warp - 1] : 0u) + incl - tot;
 #pragma unroll
-  for (int blk = 0; blk < kRangeBlocks; blk++) {
-    bh[blk * kRangeBuckets + t] = base;
-    base += h[blk];
+  for (int q = 0; q < kPer / 4; q++) {
+    uint4 v;
+    v.x = run;
+    v.y = v.x + c[4 * q];
+    v.z = v.y + c[4 * q + 1];
+    v.w = v.z + c[4 * q + 2];
+    run = v.w + c[4 * q + 3];
+    reinterpret_cast<uint4*>(offs + t * kPer)[q] = v;
+    reinterpret_cast<uint4*>(cursor + t * kPer)[q] = v;
   }
-  if (t == kRangeBuckets - 1) offs[kRangeBuckets] = base;
+  if (t == kRangeThreads - 1) offs[kRangeBuckets] = run;
 }
 
-// the count pass's blocks again: every item to its bucket's next slot
-__global__ void __launch_bounds__(kRangeThreads) RangeScatter(const SortItem* __restrict__ items, int64_t n,
-                                                              const uint16_t* __restrict__ bucket_of,
-                                                              const unsigned* __restrict__ bh,
-                                                              SortItem* __restrict__ out) {
-  __shared__ unsigned cur[kRangeBuckets];
-  for (int j = threadIdx.x; j < kRangeBuckets; j += blockDim.x) cur[j] = bh[blockIdx.x * kRangeBuckets + j];
-  __syncthreads();
-  const int64_t c = RangeChunk(n), b0 = blockIdx.x * c, b1 = b0 + c < n ? b0 + c : n;
-  for (int64_t i = b0 + threadIdx.x; i < b1; i += blockDim.x) {
-    const unsigned pos = atomicAdd(&cur[bucket_of[i]], 1u);
+// every item into its bucket's range (in any order within the bucket)
+__global__ void RangeScatter(const SortItem* __restrict__ items, int64_t n, const uint16_t* __restrict__ bucket_of,
+                             unsigned* __restrict__ cursor, SortItem* __restrict__ out, uint16_t* __restrict__ out_bucket) {
+  for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < n;
+       i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const unsigned b = bucket_of[i];
+    const unsigned pos = atomicAdd(&cursor[b], 1u);
     out[pos] = items[i];
+    out_bucket[pos] = static_cast<uint16_t>(b);
   }
 }
 
-// one CTA per bucket: the bucket's items in shared memory, and each item
-// written at its rank (the number of smaller items; (key, tie) pairs are
-// unique, so ranks are distinct).  Every thread reads the same item at the
-// same time (a broadcast), and the comparisons of one item are independent,
-// so they pipeline.
-__global__ void RangeRankSort(const SortItem* __restrict__ src, const unsigned* __restrict__ offs,
-                              SortItem* __restrict__ dst) {
-  extern __shared__ SortItem sr[];
-  const unsigned b0 = offs[blockIdx.x], cnt = offs[blockIdx.x + 1] - b0;
-  if (cnt == 0) return;
-  for (unsigned i = threadIdx.x; i < cnt; i += blockDim.x) sr[i] = src[b0 + i];
-  __syncthreads();
-  for (unsigned i = threadIdx.x; i < cnt; i += blockDim.x) {
-    const SortItem x = sr[i];
-    unsigned r = 0;
-#pragma unroll 4
-    for (unsigned j = 0; j < cnt; j++) r += ItemLess(sr[j], x) ? 1u : 0u;
-    dst[b0 + r] = x;
+// every item to its bucket's start plus the number of its bucket's items
+// that order before it ((key, tie) pairs are unique: distinct slots)
+__global__ void RangeRank(const SortItem* __restrict__ src, const uint16_t* __restrict__ bucket, int64_t n,
+                          const unsigned* __restrict__ offs, SortItem* __restrict__ dst) {
+  for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < n;
+       i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const SortItem x = src[i];
+    const unsigned b = bucket[i], b0 = offs[b], b1 = offs[b + 1];
+    unsigned r = b0;
+    for (unsigned j = b0; j < b1; j++) r += ItemLess(src[j], x) ? 1u : 0u;
+    dst[r] = x;
   }
 }
 
@@ -948,30 +945,35 @@ bool Context::RangeSortItems(void* items_v, int64_t n, Arena& arena) {
   SortItem* items = static_cast<SortItem*>(items_v);
   SortItem* tmp = reinterpret_cast<SortItem*>(arena.Alloc(sizeof(SortItem) * n));
   uint16_t* bof = reinterpret_cast<uint16_t*>(arena.Alloc(sizeof(uint16_t) * n));
+  uint16_t* tbof = reinterpret_cast<uint16_t*>(arena.Alloc(sizeof(uint16_t) * n));
   unsigned long long* mm = arena.AllocT<unsigned long long>(2);
-  unsigned* bh = arena.AllocT<unsigned>(kRangeBlocks * kRangeBuckets);
+  unsigned* counts = arena.AllocT<unsigned>(kRangeBuckets);
   unsigned* offs = arena.AllocT<unsigned>(kRangeBuckets + 1);
+  unsigned* cursor = arena.AllocT<unsigned>(kRangeBuckets);
   unsigned* largest = arena.AllocT<unsigned>(1);
+  // a fallback to the merge sort drops these passes from the recording
+  const auto mark = RecordMark();
   Memset(mm, 0xff, sizeof(unsigned long long));
   Memset(mm + 1, 0, sizeof(unsigned long long));
+  Memset(counts, 0, sizeof(unsigned) * kRangeBuckets);
   const int mm_grid = static_cast<int>(std::min<int64_t>((n + kRangeThreads - 1) / kRangeThreads, 32));
+  const int grid = GridFor(n, 256);
   TimedStart("sort range");
   Issue([=](cudaStream_t s) { RangeMinMax<<<mm_grid, kRangeThreads, 0, s>>>(items, n, mm); });
-  Issue([=](cudaStream_t s) { RangeCount<<<kRangeBlocks, kRangeThreads, 0, s>>>(items, n, mm, bof, bh); });
-  Issue([=](cudaStream_t s) { RangeOffsets<<<1, kRangeBuckets, 0, s>>>(bh, offs, largest); });
+  Issue([=](cudaStream_t s) { RangeCount<<<grid, 256, 0, s>>>(items, n, mm, bof, counts); });
+  Issue([=](cudaStream_t s) { RangeOffsets<<<1, kRangeThreads, 0, s>>>(counts, offs, cursor, largest); });
   TimedStop();
   KDB_CUDA(cudaGetLastError());
   // the bucket sizes decide (at recording; a replay runs on the same data)
   unsigned big = 0;
   D2H(&big, largest, sizeof(big));
-  if (big > static_cast<unsigned>(kRangeBucketCap)) return false;
-  const size_t smem = sizeof(SortItem) * std::max<unsigned>(big, 1u);
-  if (smem > 48 * 1024)
-    KDB_CUDA(cudaFuncSetAttribute(RangeRankSort, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
-  const int threads = big > 512 ? 256 : 128;
+  if (big > kRangeBucketCap) {
+    RecordTruncate(mark);
+    return false;
+  }
   TimedStart("sort buckets");
-  Issue([=](cudaStream_t s) { RangeScatter<<<kRangeBlocks, kRangeThreads, 0, s>>>(items, n, bof, bh, tmp); });
-  Issue([=](cudaStream_t s) { RangeRankSort<<<kRangeBuckets, threads, smem, s>>>(tmp, offs, items); });
+  Issue([=](cudaStream_t s) { RangeScatter<<<grid, 256, 0, s>>>(items, n, bof, cursor, tmp, tbof); });
+  Issue([=](cudaStream_t s) { RangeRank<<<grid, 256, 0, s>>>(tmp, tbof, n, offs, items); });
   TimedStop();
   KDB_CUDA(cudaGetLastError());
   return true;

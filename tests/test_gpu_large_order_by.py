@@ -50,21 +50,28 @@ def _plan(t, keys, asc):
                                       (["null_r"], [True]), (["null_r"], [False]),
                                       (["tied_r", "null_r"], [False, True]),
                                       (["tied_i"], [True]), (["tied_i"], [False]), (["id"], [False])])
-@pytest.mark.parametrize("sort", [None, "KDB_ORDER_SAMPLE", "KDB_ORDER_RANGE", "KDB_ORDER_RADIX",
-                                  "KDB_SORT_SHAPE=4096,8,512,2", "KDB_SORT_SHAPE=8192,8,1024,4"])
+@pytest.mark.parametrize("sort", [None, "KDB_ORDER_MERGE", "KDB_ORDER_SAMPLE", "KDB_ORDER_RADIX",
+                                  "KDB_ORDER_MERGE,KDB_SORT_SHAPE=4096,8,512,2",
+                                  "KDB_ORDER_MERGE,KDB_SORT_SHAPE=8192,8,1024,4"])
 def test_order_matches_reference_merge_sort(setup, keys, asc, sort):
-    """Each device sort (merge passes of several tile shapes, sample sort,
-    key-range bucket sort, radix passes) gives the reference merge sort's
-    order (the bucket sorts fall back to the merge passes when ties pile up
-    in one bucket)."""
+    """Each device sort (the default key-range bucket sort, merge passes of
+    several tile shapes, sample sort, radix passes) gives the reference merge
+    sort's order (the bucket sorts fall back to the merge passes when ties
+    pile up in one bucket)."""
     e, o, t = setup
     plan = _plan(t, keys, asc).to_json()
-    name, _, value = (sort or "").partition("=")
+    opts = []
     if sort:
-        e.set_option(name, value or "1")
+        first, _, shape = sort.partition(",")
+        opts.append((first, "1"))
+        if shape:
+            name, _, value = shape.partition("=")
+            opts.append((name, value))
+    for name, value in opts:
+        e.set_option(name, value)
     try:
         got = e.execute(plan)
     finally:
-        if sort:
+        for name, _ in opts:
             e.set_option(name, None)
     assert compare(got, o.execute(plan), ordered=True) == ""

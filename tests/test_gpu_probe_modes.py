@@ -1,8 +1,11 @@
 """The join probe's load schedules give the oracle's results: the default
 (one row per thread, next row's columns prefetched), the 4-row vector probe
 that loads each vector's join-filter words and first slots together
-(KDB_PROBE_VEC), the row-ahead forms (KDB_PROBE_AHEAD=1 / word) and the
-build side written in one unordered pass (KDB_BUILD_MAT_ATOMIC), on the
+(KDB_PROBE_VEC), the row-ahead forms (KDB_PROBE_AHEAD=1 / word), the build
+side written in one unordered pass (KDB_BUILD_MAT_ATOMIC), the join filter in
+shared memory (KDB_SMEM_BLOOM), the two-kernel probe and aggregation
+(KDB_SPLIT_PROBE_GROUPS), and the separate join build and key-check kernels
+(KDB_JOIN_BUILD_PASS, KDB_KEY_CHECK_PASS), on the
 Q3-shape join + group-by (uniform and Zipf foreign keys), a join whose probe
 keys are nullable SMALLINTs with duplicates on the build side, and a join
 materialised without a group-by."""
@@ -18,7 +21,8 @@ from parity import compare
 pytestmark = pytest.mark.gpu
 
 MODES = [{}, {"KDB_PROBE_VEC": "1"}, {"KDB_PROBE_AHEAD": "1"}, {"KDB_PROBE_AHEAD": "word"},
-         {"KDB_BUILD_MAT_ATOMIC": "1"}]
+         {"KDB_BUILD_MAT_ATOMIC": "1"}, {"KDB_SMEM_BLOOM": "1"}, {"KDB_SPLIT_PROBE_GROUPS": "1"},
+         {"KDB_JOIN_BUILD_PASS": "1", "KDB_KEY_CHECK_PASS": "1"}]
 
 
 @pytest.fixture(scope="module")
