@@ -339,6 +339,25 @@ def run_skinner(args):
                              "episodes": statistics.median(eps), "work": statistics.median(work)})
             per[policy] = rows
     eng.set_skinner_policy("uct")
+    timed_launches = eng.kernel_launches() - launches0
+    breakdown = None
+    if args.kernel_breakdown:
+        # per query (plain UCT): device time by kernel role, from CUDA events
+        # around every launch (profiling mode: one fresh execution each)
+        breakdown = {}
+        eng.set_skinner(budget, 0)
+        for name, _, plan in queries:
+            eng.set_profiling(True)
+            eng.execute(plan.to_json().encode(), fetch=False)
+            ks = eng.last_kernels()
+            eng.set_profiling(False)
+            tags = {}
+            for k in ks:
+                t = tags.setdefault(k["tag"], [0, 0.0])
+                t[0] += 1
+                t[1] += k["ms"]
+            breakdown[name] = {k: {"launches": v[0], "ms": round(v[1], 4)}
+                               for k, v in sorted(tags.items(), key=lambda kv: -kv[1][1])}
     total = {k: sum(r["ms"] for r in v) for k, v in per.items()}
     best = min(total, key=total.get)
     nq = len(queries)
@@ -355,7 +374,8 @@ def run_skinner(args):
                          "work_total": sum(r["work"] for r in v)} for k, v in per.items()},
         "prior_training": info,
         "per_query": per,
-        "gpu_launches": eng.kernel_launches() - launches0,
+        "kernel_breakdown_ms": breakdown,
+        "gpu_launches": timed_launches,
         "clocks": clocks.summary(),
     }
     print(json.dumps(line))
@@ -537,6 +557,8 @@ def main():
     ap.add_argument("--serving-budget-gb", type=int, default=32)
     ap.add_argument("--fanout", type=int, default=0,
                     help="op_hash_join: sub-tables of the build (1 = one table, 0 = automatic)")
+    ap.add_argument("--kernel-breakdown", action="store_true",
+                    help="skinner: also report each query's device time by kernel role (profiling mode)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-sub", action="store_true",

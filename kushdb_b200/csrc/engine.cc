@@ -273,6 +273,8 @@ Context::~Context() {
   if (copy_start_) cudaEventDestroy(copy_start_);
   if (stage_) cudaFreeHost(stage_);
   cudaSetDevice(device);
+  for (cudaEvent_t e : query_ev_)
+    if (e) cudaEventDestroy(e);
   if (dev_stage_) cudaFreeAsync(dev_stage_, stream);
   cudaStreamSynchronize(stream);
   if (owns_catalog_) {
@@ -668,8 +670,10 @@ void Context::Launch(CUfunction f, int grid, int block, const KArgs& args, size_
     CuCheck(g_drv.FuncSetAttribute(f, CU_FUNC_ATTRIBUTE_MAX_DYNAMIC_SHARED_SIZE_BYTES,
                                    static_cast<int>(smem)),
             "cuFuncSetAttribute");
+  // profiling runs time every kernel between two events: launched one
+  // after the other, without programmatic overlap
   bool pdl = false;
-  if (!OptStr("KDB_NO_PDL")) {
+  if (!OptStr("KDB_NO_PDL") && !profile) {
     std::lock_guard<std::mutex> lock(cache_->mu);
     pdl = cache_->waits.count(f) != 0;
   }
@@ -684,6 +688,13 @@ void Context::Launch(CUfunction f, int grid, int block, const KArgs& args, size_
       LaunchOne(f, grid, block, smem, reinterpret_cast<CUstream>(s), p, pdl);
     });
   }
+}
+
+void Context::QueryEvents(cudaEvent_t* start, cudaEvent_t* end) {
+  for (cudaEvent_t& e : query_ev_)
+    if (!e) KDB_CUDA(cudaEventCreate(&e));
+  *start = query_ev_[0];
+  *end = query_ev_[1];
 }
 
 void Context::TimedStart(const char* tag) {

@@ -323,6 +323,8 @@ class Context {
   std::vector<std::pair<std::string, float>> last_kernels;
   void BeginQueryProfile();
   void EndQueryProfile();
+  // the two events that time each query (made on first use)
+  void QueryEvents(cudaEvent_t* start, cudaEvent_t* end);
   void TimedStart(const char* tag);
   void TimedStop();
   int GridFor(int64_t n, int block) const;
@@ -371,6 +373,7 @@ class Context {
 
  private:
   std::shared_ptr<ProgramCache> cache_ = std::make_shared<ProgramCache>();
+  cudaEvent_t query_ev_[2] = {nullptr, nullptr};
   bool owns_catalog_ = true;
   void* stage_ = nullptr;
   size_t stage_bytes_ = 0;
