@@ -51,8 +51,8 @@ def _peaks():
 # each workload's dominant kernel at the default size, from one ncu capture
 # of the current kernels; other sizes scale it by the rows processed, the
 # traffic being proportional to them.
-MEASURED_TRAFFIC = {"group_by": 264_035_840 + 3_384_320,
-                    "join_group": 119_308_288 + 3_159_808,
+MEASURED_TRAFFIC = {"group_by": 264_039_168 + 3_074_816,
+                    "join_group": 126_673_152 + 3_196_672,
                     "scan_agg": 20_026_112}
 
 
