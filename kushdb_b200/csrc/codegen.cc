@@ -805,7 +805,11 @@ class Executor {
   MatBuffer RunSkinner(const Operator& op, const SkinnerAgg* agg = nullptr);
   MatBuffer SmallOrderBy(const Operator& op, MatBuffer& m);
   MatBuffer LargeOrderBy(const Operator& op, MatBuffer& m);
-  void SortItems(uint64_t* items, int64_t n);
+  // Returns true when it also counted ties into *ties (range sort taken).
+  bool SortItems(uint64_t* items, int64_t n, unsigned long long* ties = nullptr, uint32_t tie_mask = 0);
+  // set while materialising an ORDER BY's output: the sorted items, whose
+  // high words hold the rows (read by EmitMatScan instead of an index array)
+  const uint64_t* order_items_ = nullptr;
   MatBuffer RunGroupByDense(const Operator& op, const std::vector<AggPlan>& plans, const KeyLayout& kl,
                             const Operator* order_by = nullptr);
   // the ORDER BY was done by its GROUP BY child (dense path)
@@ -925,12 +929,19 @@ void Executor::EmitMatScan(KernelSource& ks, const MatBuffer& m, const uint32_t*
   ExprGen eg(ctx_, ks);
   src_rows = m.rows;
   std::string n = ks.Word(static_cast<uint64_t>(m.rows));
-  std::string ind = indirection ? ks.Ptr(indirection, "uint32_t", true) : "";
+  // sorted items instead of an index array: row = the item's high word
+  const uint64_t* items = indirection ? order_items_ : nullptr;
+  order_items_ = nullptr;
+  std::string ind = items ? ks.Ptr(items, "uint64_t", true)
+                          : indirection ? ks.Ptr(indirection, "uint32_t", true) : "";
   std::string pos = ks.Ptr(m.pos, "uint64_t", true);
   ks.Open("for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < (int64_t)" + n +
           "; r += (int64_t)gridDim.x * blockDim.x)");
   std::string row = "r";
-  if (indirection) {
+  if (items) {
+    ks.L("int64_t rr = (int64_t)(uint32_t)(" + ind + "[2 * r + 1] >> 32);");
+    row = "rr";
+  } else if (indirection) {
     ks.L("int64_t rr = (int64_t)" + ind + "[r];");
     row = "rr";
   }
@@ -3531,11 +3542,13 @@ MatBuffer Executor::SmallOrderBy(const Operator& op, MatBuffer& m) {
 // 134k-item ORDER BY of the Q3-shape query the query steps at 228 us with
 // the range sort against 241 us with the merge passes (198 / 211 us with
 // Zipf keys); the sample sort was slower than both.
-void Executor::SortItems(uint64_t* items, int64_t n) {
-  if (ctx_.OptStr("KDB_ORDER_SAMPLE") && ctx_.SampleSortItems(items, n, arena_)) return;
-  if (!ctx_.OptStr("KDB_ORDER_MERGE") && !ctx_.OptStr("KDB_ORDER_SAMPLE") && ctx_.RangeSortItems(items, n, arena_))
-    return;
+bool Executor::SortItems(uint64_t* items, int64_t n, unsigned long long* ties, uint32_t tie_mask) {
+  if (ctx_.OptStr("KDB_ORDER_SAMPLE") && ctx_.SampleSortItems(items, n, arena_)) return false;
+  if (!ctx_.OptStr("KDB_ORDER_MERGE") && !ctx_.OptStr("KDB_ORDER_SAMPLE") &&
+      ctx_.RangeSortItems(items, n, arena_, ctx_.OptStr("KDB_ORDER_TIE_PASS") ? nullptr : ties, tie_mask))
+    return ties != nullptr && !ctx_.OptStr("KDB_ORDER_TIE_PASS");
   ctx_.MergeSortItems(items, n, arena_);
+  return false;
 }
 
 MatBuffer Executor::LargeOrderBy(const Operator& op, MatBuffer& m) {
@@ -3636,15 +3649,28 @@ MatBuffer Executor::LargeOrderBy(const Operator& op, MatBuffer& m) {
         ks.Close();
         LaunchPipeline(ks, n, "order rows");
       };
+      // the output in sorted order, its rows read from the items' high words
+      // (KDB_ORDER_ROWS_PASS: through a separate row-index array)
+      auto sorted_output = [&]() {
+        if (ctx_.OptStr("KDB_ORDER_ROWS_PASS")) {
+          order_rows();
+          return MaterializeStream(op, idx, &m);
+        }
+        order_items_ = items;
+        MatBuffer out = MaterializeStream(op, idx, &m);
+        order_items_ = nullptr;
+        return out;
+      };
       if (!m.pos_is_index && !ctx_.OptStr("KDB_ORDER_TIE_SORT")) {
         // Rows not in stream order (groups in table order): sort by the key
         // alone and look for equal neighbours.  Without ties the tie rank
         // never decides, and the stream-order sort is not needed.
         make_items(false);
-        SortItems(items, n);
         uint64_t* ties = arena_.AllocT<uint64_t>(1);
         ctx_.Memset(ties, 0, sizeof(uint64_t));
-        {
+        // the range sort counts ties while it ranks (equal keys share a
+        // bucket); after the other sorts a pass compares neighbours
+        if (!SortItems(items, n, reinterpret_cast<unsigned long long*>(ties), mc.nullable ? 0x80000000u : 0u)) {
           KernelSource ks;
           std::string IT = ks.Ptr(items, "uint64_t", true), T = ks.Ptr(ties, "unsigned long long");
           std::string N = ks.Word(static_cast<uint64_t>(n));
@@ -3656,16 +3682,12 @@ MatBuffer Executor::LargeOrderBy(const Operator& op, MatBuffer& m) {
           ks.Close();
           LaunchPipeline(ks, n, "order ties");
         }
-        if (ReadU64(ties) == 0 && !ctx_.dry) {
-          order_rows();
-          return MaterializeStream(op, idx, &m);
-        }
+        if (ReadU64(ties) == 0 && !ctx_.dry) return sorted_output();
       }
       stream_order();
       make_items(true);
       SortItems(items, n);
-      order_rows();
-      return MaterializeStream(op, idx, &m);
+      return sorted_output();
     }
     stream_order();
     auto tie_sort = [&]() {

@@ -357,7 +357,10 @@ class Context {
   bool SampleSortItems(void* items, int64_t n, Arena& arena);
   // (key, tie) order by key-range buckets; false (nothing done) when a
   // bucket is too large for one CTA's shared memory
-  bool RangeSortItems(void* items, int64_t n, Arena& arena);
+  // With `ties` (zeroed by the caller), also counts the items whose key
+  // (and tie bits under `tie_mask`) another item shares.
+  bool RangeSortItems(void* items, int64_t n, Arena& arena, unsigned long long* ties = nullptr,
+                      uint32_t tie_mask = 0);
   // exclusive prefix sum of a[0..n) in place, the total into a[n]
   void ScanU64(uint64_t* a, int64_t n, const char* tag = "skinner scan");
   // the same over *n_ptr elements (a device word), skipped when *n_ptr > cap

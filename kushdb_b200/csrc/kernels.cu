@@ -924,22 +924,32 @@ __global__ void RangeScatter(const SortItem* __restrict__ items, int64_t n, cons
 }
 
 // every item to its bucket's start plus the number of its bucket's items
-// that order before it ((key, tie) pairs are unique: distinct slots)
+// that order before it ((key, tie) pairs are unique: distinct slots).  With
+// `ties`, an item whose key another item of its bucket shares (and, under
+// `tie_mask`, the same masked tie bits) counts into *ties: equal keys always
+// share a bucket, so this finds every tie of the sorted sequence.
 __global__ void RangeRank(const SortItem* __restrict__ src, const uint16_t* __restrict__ bucket, int64_t n,
-                          const unsigned* __restrict__ offs, SortItem* __restrict__ dst) {
+                          const unsigned* __restrict__ offs, SortItem* __restrict__ dst,
+                          unsigned long long* __restrict__ ties, uint32_t tie_mask) {
   for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < n;
        i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
     const SortItem x = src[i];
     const unsigned b = bucket[i], b0 = offs[b], b1 = offs[b + 1];
     unsigned r = b0;
-    for (unsigned j = b0; j < b1; j++) r += ItemLess(src[j], x) ? 1u : 0u;
+    bool tie = false;
+    for (unsigned j = b0; j < b1; j++) {
+      const SortItem y = src[j];
+      r += ItemLess(y, x) ? 1u : 0u;
+      tie |= j != static_cast<unsigned>(i) && y.key == x.key && ((y.tie ^ x.tie) & tie_mask) == 0;
+    }
     dst[r] = x;
+    if (ties && tie) atomicAdd(ties, 1ULL);
   }
 }
 
 }  // namespace
 
-bool Context::RangeSortItems(void* items_v, int64_t n, Arena& arena) {
+bool Context::RangeSortItems(void* items_v, int64_t n, Arena& arena, unsigned long long* ties, uint32_t tie_mask) {
   if (n <= 1 || dry) return true;
   if (n > 0x7fffffffLL) return false;
   SortItem* items = static_cast<SortItem*>(items_v);
@@ -973,7 +983,7 @@ bool Context::RangeSortItems(void* items_v, int64_t n, Arena& arena) {
   }
   TimedStart("sort buckets");
   Issue([=](cudaStream_t s) { RangeScatter<<<grid, 256, 0, s>>>(items, n, bof, cursor, tmp, tbof); });
-  Issue([=](cudaStream_t s) { RangeRank<<<grid, 256, 0, s>>>(tmp, tbof, n, offs, items); });
+  Issue([=](cudaStream_t s) { RangeRank<<<grid, 256, 0, s>>>(tmp, tbof, n, offs, items, ties, tie_mask); });
   TimedStop();
   KDB_CUDA(cudaGetLastError());
   return true;
