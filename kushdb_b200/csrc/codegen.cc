@@ -806,7 +806,16 @@ class Executor {
   MatBuffer SmallOrderBy(const Operator& op, MatBuffer& m);
   MatBuffer LargeOrderBy(const Operator& op, MatBuffer& m);
   // Returns true when it also counted ties into *ties (range sort taken).
-  bool SortItems(uint64_t* items, int64_t n, unsigned long long* ties = nullptr, uint32_t tie_mask = 0);
+  bool SortItems(uint64_t* items, int64_t n, unsigned long long* ties = nullptr, uint32_t tie_mask = 0,
+                 const unsigned long long* key_range = nullptr);
+  // KDB_ORDER_FUSED_RANGE: the kernel that makes the items also reduces
+  // their key range for the range-bucket sort (one 64-bit atomic min and max
+  // per warp).  Measured slower on the Q3 ORDER BY (step 217-219 against
+  // 214-216 us): thousands of warps' atomics queue on the two words, where
+  // the sort's own 32-CTA pass issues 64.
+  bool KeyRangeWanted() const {
+    return ctx_.OptStr("KDB_ORDER_FUSED_RANGE") && !ctx_.OptStr("KDB_ORDER_MERGE") && !ctx_.OptStr("KDB_ORDER_SAMPLE");
+  }
   // set while materialising an ORDER BY's output: the sorted items, whose
   // high words hold the rows (read by EmitMatScan instead of an index array)
   const uint64_t* order_items_ = nullptr;
@@ -3542,10 +3551,12 @@ MatBuffer Executor::SmallOrderBy(const Operator& op, MatBuffer& m) {
 // 134k-item ORDER BY of the Q3-shape query the query steps at 228 us with
 // the range sort against 241 us with the merge passes (198 / 211 us with
 // Zipf keys); the sample sort was slower than both.
-bool Executor::SortItems(uint64_t* items, int64_t n, unsigned long long* ties, uint32_t tie_mask) {
+bool Executor::SortItems(uint64_t* items, int64_t n, unsigned long long* ties, uint32_t tie_mask,
+                         const unsigned long long* key_range) {
   if (ctx_.OptStr("KDB_ORDER_SAMPLE") && ctx_.SampleSortItems(items, n, arena_)) return false;
   if (!ctx_.OptStr("KDB_ORDER_MERGE") && !ctx_.OptStr("KDB_ORDER_SAMPLE") &&
-      ctx_.RangeSortItems(items, n, arena_, ctx_.OptStr("KDB_ORDER_TIE_PASS") ? nullptr : ties, tie_mask))
+      ctx_.RangeSortItems(items, n, arena_, ctx_.OptStr("KDB_ORDER_TIE_PASS") ? nullptr : ties, tie_mask,
+                          KeyRangeWanted() ? key_range : nullptr))
     return ties != nullptr && !ctx_.OptStr("KDB_ORDER_TIE_PASS");
   ctx_.MergeSortItems(items, n, arena_);
   return false;
@@ -3604,12 +3615,22 @@ MatBuffer Executor::LargeOrderBy(const Operator& op, MatBuffer& m) {
       // stream_ties: rows in stream order (idx) with the reference merge
       // sort's tie rank; otherwise rows in buffer order with the row index
       // as a provisional (unique) tie
+      // the items' key range, reduced while they are made (the range-bucket
+      // sort then needs no pass of its own for it)
+      unsigned long long* key_range = KeyRangeWanted() ? arena_.AllocT<unsigned long long>(2) : nullptr;
       auto make_items = [&](bool stream_ties) {
         KernelSource ks;
         ExprGen eg(ctx_, ks);
         std::string IT = ks.Ptr(items, "uint64_t"), I = ks.Ptr(idx, "uint32_t", true);
         std::string D = ks.Ptr(mc.data, StoreType(t), true);
         std::string N = ks.Word(static_cast<uint64_t>(n));
+        std::string KR;
+        if (key_range) {
+          ctx_.Memset(key_range, 0xff, sizeof(unsigned long long));
+          ctx_.Memset(key_range + 1, 0, sizeof(unsigned long long));
+          KR = ks.Ptr(key_range, "unsigned long long");
+          ks.L("unsigned long long kdb_klo = ~0ULL, kdb_khi = 0ULL;");
+        }
         ks.Open("for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < (int64_t)" + N +
                 "; i += (int64_t)gridDim.x * blockDim.x)");
         ks.L(std::string("const uint32_t row = ") + (m.pos_is_index || !stream_ties ? "(uint32_t)i" : I + "[i]") +
@@ -3636,7 +3657,18 @@ MatBuffer Executor::LargeOrderBy(const Operator& op, MatBuffer& m) {
           ks.L(IT + "[2 * i] = (flag << 63) | (k >> 1);");
           ks.L(IT + "[2 * i + 1] = ((k & 1ULL) << 31) | " + tie + " | ((uint64_t)row << 32);");
         }
+        if (key_range) {
+          ks.L("{ const unsigned long long kk = " + IT + "[2 * i]; kdb_klo = kk < kdb_klo ? kk : kdb_klo; "
+               "kdb_khi = kk > kdb_khi ? kk : kdb_khi; }");
+        }
         ks.Close();
+        if (key_range) {
+          ks.L("for (int o = 16; o > 0; o >>= 1) { const unsigned long long a = __shfl_xor_sync(0xffffffffu, kdb_klo, o), "
+               "b = __shfl_xor_sync(0xffffffffu, kdb_khi, o); kdb_klo = a < kdb_klo ? a : kdb_klo; "
+               "kdb_khi = b > kdb_khi ? b : kdb_khi; }");
+          ks.L("if ((threadIdx.x & 31) == 0 && kdb_klo <= kdb_khi) { atomicMin(&" + KR + "[0], kdb_klo); atomicMax(&" + KR +
+               "[1], kdb_khi); }");
+        }
         LaunchPipeline(ks, n, "order key");
       };
       auto order_rows = [&]() {
@@ -3670,7 +3702,8 @@ MatBuffer Executor::LargeOrderBy(const Operator& op, MatBuffer& m) {
         ctx_.Memset(ties, 0, sizeof(uint64_t));
         // the range sort counts ties while it ranks (equal keys share a
         // bucket); after the other sorts a pass compares neighbours
-        if (!SortItems(items, n, reinterpret_cast<unsigned long long*>(ties), mc.nullable ? 0x80000000u : 0u)) {
+        if (!SortItems(items, n, reinterpret_cast<unsigned long long*>(ties), mc.nullable ? 0x80000000u : 0u,
+                       key_range)) {
           KernelSource ks;
           std::string IT = ks.Ptr(items, "uint64_t", true), T = ks.Ptr(ties, "unsigned long long");
           std::string N = ks.Word(static_cast<uint64_t>(n));
@@ -3686,7 +3719,7 @@ MatBuffer Executor::LargeOrderBy(const Operator& op, MatBuffer& m) {
       }
       stream_order();
       make_items(true);
-      SortItems(items, n);
+      SortItems(items, n, nullptr, 0, key_range);
       return sorted_output();
     }
     stream_order();

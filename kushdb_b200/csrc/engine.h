@@ -359,8 +359,10 @@ class Context {
   // bucket is too large for one CTA's shared memory
   // With `ties` (zeroed by the caller), also counts the items whose key
   // (and tie bits under `tie_mask`) another item shares.
+  // With `key_range` (min and max of the items' keys, already on the
+  // device), no pass computes it.
   bool RangeSortItems(void* items, int64_t n, Arena& arena, unsigned long long* ties = nullptr,
-                      uint32_t tie_mask = 0);
+                      uint32_t tie_mask = 0, const unsigned long long* key_range = nullptr);
   // exclusive prefix sum of a[0..n) in place, the total into a[n]
   void ScanU64(uint64_t* a, int64_t n, const char* tag = "skinner scan");
   // the same over *n_ptr elements (a device word), skipped when *n_ptr > cap

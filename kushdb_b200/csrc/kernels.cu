@@ -949,28 +949,32 @@ __global__ void RangeRank(const SortItem* __restrict__ src, const uint16_t* __re
 
 }  // namespace
 
-bool Context::RangeSortItems(void* items_v, int64_t n, Arena& arena, unsigned long long* ties, uint32_t tie_mask) {
+bool Context::RangeSortItems(void* items_v, int64_t n, Arena& arena, unsigned long long* ties, uint32_t tie_mask,
+                             const unsigned long long* key_range) {
   if (n <= 1 || dry) return true;
   if (n > 0x7fffffffLL) return false;
   SortItem* items = static_cast<SortItem*>(items_v);
   SortItem* tmp = reinterpret_cast<SortItem*>(arena.Alloc(sizeof(SortItem) * n));
   uint16_t* bof = reinterpret_cast<uint16_t*>(arena.Alloc(sizeof(uint16_t) * n));
   uint16_t* tbof = reinterpret_cast<uint16_t*>(arena.Alloc(sizeof(uint16_t) * n));
-  unsigned long long* mm = arena.AllocT<unsigned long long>(2);
+  unsigned long long* mm = key_range ? nullptr : arena.AllocT<unsigned long long>(2);
+  const unsigned long long* range = key_range ? key_range : mm;
   unsigned* counts = arena.AllocT<unsigned>(kRangeBuckets);
   unsigned* offs = arena.AllocT<unsigned>(kRangeBuckets + 1);
   unsigned* cursor = arena.AllocT<unsigned>(kRangeBuckets);
   unsigned* largest = arena.AllocT<unsigned>(1);
   // a fallback to the merge sort drops these passes from the recording
   const auto mark = RecordMark();
-  Memset(mm, 0xff, sizeof(unsigned long long));
-  Memset(mm + 1, 0, sizeof(unsigned long long));
+  if (mm) {
+    Memset(mm, 0xff, sizeof(unsigned long long));
+    Memset(mm + 1, 0, sizeof(unsigned long long));
+  }
   Memset(counts, 0, sizeof(unsigned) * kRangeBuckets);
   const int mm_grid = static_cast<int>(std::min<int64_t>((n + kRangeThreads - 1) / kRangeThreads, 32));
   const int grid = GridFor(n, 256);
   TimedStart("sort range");
-  Issue([=](cudaStream_t s) { RangeMinMax<<<mm_grid, kRangeThreads, 0, s>>>(items, n, mm); });
-  Issue([=](cudaStream_t s) { RangeCount<<<grid, 256, 0, s>>>(items, n, mm, bof, counts); });
+  if (mm) Issue([=](cudaStream_t s) { RangeMinMax<<<mm_grid, kRangeThreads, 0, s>>>(items, n, mm); });
+  Issue([=](cudaStream_t s) { RangeCount<<<grid, 256, 0, s>>>(items, n, range, bof, counts); });
   Issue([=](cudaStream_t s) { RangeOffsets<<<1, kRangeThreads, 0, s>>>(counts, offs, cursor, largest); });
   TimedStop();
   KDB_CUDA(cudaGetLastError());

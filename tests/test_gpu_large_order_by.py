@@ -51,7 +51,7 @@ def _plan(t, keys, asc):
                                       (["tied_r", "null_r"], [False, True]),
                                       (["tied_i"], [True]), (["tied_i"], [False]), (["id"], [False])])
 @pytest.mark.parametrize("sort", [None, "KDB_ORDER_MERGE", "KDB_ORDER_SAMPLE", "KDB_ORDER_RADIX",
-                                  "KDB_ORDER_TIE_PASS", "KDB_ORDER_ROWS_PASS",
+                                  "KDB_ORDER_TIE_PASS", "KDB_ORDER_ROWS_PASS", "KDB_ORDER_FUSED_RANGE",
                                   "KDB_ORDER_MERGE,KDB_SORT_SHAPE=4096,8,512,2",
                                   "KDB_ORDER_MERGE,KDB_SORT_SHAPE=8192,8,1024,4"])
 def test_order_matches_reference_merge_sort(setup, keys, asc, sort):
