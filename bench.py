@@ -146,6 +146,39 @@ def _ranks(values):
     return r
 
 
+def _host_llc_bytes() -> int:
+    """Largest CPU cache the host reports (sysfs), 0 when unknown."""
+    best = 0
+    base = "/sys/devices/system/cpu/cpu0/cache"
+    try:
+        for idx in os.listdir(base):
+            try:
+                with open(os.path.join(base, idx, "size")) as f:
+                    txt = f.read().strip().upper()
+                mult = 1 << 20 if txt.endswith("M") else (1 << 10 if txt.endswith("K") else 1)
+                best = max(best, int(txt.rstrip("KMG")) * mult)
+            except (OSError, ValueError):
+                continue
+    except OSError:
+        pass
+    return best
+
+
+class HostCacheFlush:
+    """Evicts the host caches between timed CPU steps (a write larger than
+    the last-level cache), as the GPU's L2 is flushed between GPU steps:
+    repeating a query over the same table would otherwise leave much of a
+    264 MB table in a large host cache and time warm reads."""
+
+    def __init__(self):
+        self.buf = np.zeros(max(1 << 30, 4 * _host_llc_bytes()), dtype=np.uint8)
+        self.k = 0
+
+    def __call__(self):
+        self.k = (self.k + 1) & 0xff
+        self.buf.fill(self.k)
+
+
 def run_cpu_baseline(name: str, tables, threads: int = 1):
     """One execution of the compiled CPU baseline loop for the workload
     (oracle/baseline.cc: the reference's generated-code loop + runtime
@@ -169,8 +202,14 @@ def cpu_baseline(name: str, tables, rows: int, repeats: int = 3):
     of `repeats`."""
     import oracle
     threads = oracle.host_threads()
-    secs = min(run_cpu_baseline(name, tables, threads) for _ in range(repeats))
-    secs1 = min(run_cpu_baseline(name, tables, 1) for _ in range(repeats))
+    flush = HostCacheFlush()
+
+    def timed(t):
+        flush()
+        return run_cpu_baseline(name, tables, t)
+    secs = min(timed(threads) for _ in range(repeats))
+    secs1 = min(timed(1) for _ in range(repeats))
+    del flush
     return rows / secs, {"rows": rows, "seconds": secs, "repeats": repeats, "threads": threads,
                          "single_thread_rows_per_second": rows / secs1}
 
@@ -184,10 +223,12 @@ def run_reference(args):
         return
     threads = oracle.host_threads()
     tables, plan, rows, _, _, cfg = make_workload(args.workload)
+    flush = HostCacheFlush()
     for _ in range(args.warmup):
         run_cpu_baseline(args.workload, tables, threads)
     total = 0.0
     for _ in range(args.steps):
+        flush()  # outside the timed region (the loop times itself)
         total += run_cpu_baseline(args.workload, tables, threads)
     value = rows * args.steps / total
     line = {
@@ -199,7 +240,8 @@ def run_reference(args):
                          "sample": f"the full {args.workload} workload ({rows} rows) per step: "
                                    "compiled restatement of the reference's generated loop and "
                                    f"runtime tables, rows split over {threads} host threads "
-                                   "(partial tables merged)"},
+                                   "(partial tables merged); host caches evicted between steps "
+                                   f"({flush.buf.nbytes >> 20} MiB write), as the GPU's L2 is"},
         "e2e": {"value": value, "unit": "rows/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line))
@@ -790,7 +832,8 @@ def measure(name, args, eng, stream, local, world, dist, scale, steps, warmup, w
                    "sample": f"full workload ({info['rows']} rows), best of {info['repeats']}: "
                              f"{info['seconds']:.4f} s on {info['threads']} host threads; compiled "
                              "restatement of the reference's generated loop + runtime tables "
-                             "(oracle/baseline.cc), rows split over the threads"}
+                             "(oracle/baseline.cc), rows split over the threads; host caches evicted "
+                             "before each run"}
         except Exception as ex:  # the oracle is a reported baseline, not the product
             cpu = {"value": None, "unit": "rows/s", "cores": 0, "kind": "port", "sample": f"failed: {ex}"}
     for t in tables:
