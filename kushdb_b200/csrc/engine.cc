@@ -47,7 +47,14 @@ struct Driver {
     Get("cuLaunchKernel", LaunchKernel);
     Get("cuModuleUnload", ModuleUnload);
     Get("cuFuncSetAttribute", FuncSetAttribute);
-    Get("cuLaunchKernelEx", LaunchKernelEx);
+    // optional: without it every kernel launches in plain stream order
+    void* ex = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuLaunchKernelEx", &ex, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess && ex)
+      LaunchKernelEx = reinterpret_cast<decltype(LaunchKernelEx)>(ex);
+    else
+      cudaGetLastError();
     loaded = true;
   }
 };
@@ -632,7 +639,7 @@ namespace {
 // drains (they wait at their first statement until it has completed and
 // its memory is visible).
 CUresult LaunchOne(CUfunction f, int grid, int block, size_t smem, CUstream s, void** params, bool pdl) {
-  if (!pdl)
+  if (!pdl || !g_drv.LaunchKernelEx)
     return g_drv.LaunchKernel(f, grid, 1, 1, block, 1, 1, static_cast<unsigned>(smem), s, params, nullptr);
   CUlaunchAttribute attr;
   std::memset(&attr, 0, sizeof(attr));
