@@ -5374,6 +5374,47 @@ HostResult ExecutePlan(Context& ctx, const plan::Operator& root, std::unique_ptr
     Executor ex(ctx, arena);
     return ex.Run(root);
   }
+  // Profiling a prepared query: its recorded launches replayed with an event
+  // pair around every kernel, queued behind a short delay so that the
+  // kernels run back to back as in the query's replay (a fresh execution
+  // leaves the GPU waiting for the host between a kernel's start event and
+  // its launch, and charges that wait to the kernel).
+  if (ctx.profile && prepared && *prepared && (*prepared)->catalog_version == ctx.catalog_version &&
+      (*prepared)->tags.size() == (*prepared)->ops.size() && !ctx.OptStr("KDB_PROFILE_FRESH")) {
+    PreparedQuery& pq = **prepared;
+    // a fixed delay first: the host queues every launch and event behind
+    // it, so the kernels then run back to back
+    ctx.DelayStream(std::min(2000.0, 20.0 + 10.0 * static_cast<double>(pq.ops.size())));
+    QueryTimer timer(ctx);
+    for (size_t i = 0; i < pq.ops.size(); i++) {
+      if (pq.tags[i].empty()) {
+        pq.ops[i](ctx.stream);
+        continue;
+      }
+      Context::LaunchTiming t;
+      t.tag = pq.tags[i];
+      KDB_CUDA(cudaEventCreate(&t.start));
+      KDB_CUDA(cudaEventCreate(&t.stop));
+      ctx.timings.push_back(t);
+      KDB_CUDA(cudaEventRecord(t.start, ctx.stream));
+      pq.ops[i](ctx.stream);
+      KDB_CUDA(cudaEventRecord(t.stop, ctx.stream));
+    }
+    KDB_CUDA(cudaGetLastError());
+    timer.Mark();
+    ctx.kernel_launches += pq.launches;
+    HostResult r;
+    try {
+      Arena arena(ctx);
+      Executor ex(ctx, arena);
+      r = ex.Download(pq.result, root, true);
+    } catch (...) {
+      cudaStreamSynchronize(ctx.stream);
+      throw;
+    }
+    timer.Done();
+    return r;
+  }
   const bool prepare = prepared != nullptr && !ctx.profile;
   if (prepare && *prepared) {
     PreparedQuery& pq = **prepared;
@@ -5444,6 +5485,7 @@ HostResult ExecutePlan(Context& ctx, const plan::Operator& root, std::unique_ptr
     pq->catalog_version = ctx.catalog_version;
     pq->launches = rec.launches;
     pq->ops = std::move(rec.ops);
+    pq->tags = std::move(rec.tags);
     *prepared = std::move(pq);
   }
   return r;

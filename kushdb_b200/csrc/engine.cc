@@ -116,7 +116,10 @@ void Context::DevFree(void* p) {
 void Context::Memset(void* d, int v, size_t bytes) {
   if (dry || !bytes) return;
   KDB_CUDA(cudaMemsetAsync(d, v, bytes, stream));
-  if (rec) rec->ops.push_back([d, v, bytes](cudaStream_t s) { cudaMemsetAsync(d, v, bytes, s); });
+  if (rec) {
+    rec->ops.push_back([d, v, bytes](cudaStream_t s) { cudaMemsetAsync(d, v, bytes, s); });
+    rec->tags.emplace_back();
+  }
 }
 
 void Context::H2D(void* d, const void* h, size_t bytes) {
@@ -694,6 +697,7 @@ void Context::Launch(CUfunction f, int grid, int block, const KArgs& args, size_
       void* p[] = {held.get()};
       LaunchOne(f, grid, block, smem, reinterpret_cast<CUstream>(s), p, pdl);
     });
+    rec->tags.emplace_back(tag ? tag : "");
   }
 }
 
@@ -705,6 +709,7 @@ void Context::QueryEvents(cudaEvent_t* start, cudaEvent_t* end) {
 }
 
 void Context::TimedStart(const char* tag) {
+  cur_tag_ = tag ? tag : "";
   if (!profile || dry) return;
   LaunchTiming t;
   t.tag = tag;
@@ -715,6 +720,7 @@ void Context::TimedStart(const char* tag) {
 }
 
 void Context::TimedStop() {
+  cur_tag_.clear();
   if (!profile || dry || timings.empty()) return;
   KDB_CUDA(cudaEventRecord(timings.back().stop, stream));
 }

@@ -153,6 +153,8 @@ struct PackSegs {
 // graph when the same plan runs again over unchanged tables.
 struct Recorder {
   std::vector<std::function<void(cudaStream_t)>> ops;
+  // per op: the kernel's role ("" for memsets), for profiled replays
+  std::vector<std::string> tags;
   int64_t launches = 0;
   bool replayable = true;
 };
@@ -256,6 +258,7 @@ class Context {
     if (rec) {
       rec->launches += is_kernel;
       rec->ops.push_back(std::move(op));
+      rec->tags.push_back(is_kernel ? cur_tag_ : std::string());
     }
   }
   // a retried step drops what its failed attempt recorded
@@ -265,6 +268,7 @@ class Context {
   void RecordTruncate(const std::pair<size_t, int64_t>& mark) {
     if (rec && rec->ops.size() > mark.first) {
       rec->ops.resize(mark.first);
+      rec->tags.resize(mark.first);
       rec->launches = mark.second;
     }
   }
@@ -320,9 +324,15 @@ class Context {
     cudaEvent_t start, stop;
   };
   std::vector<LaunchTiming> timings;
+  // the role of the kernels issued between TimedStart and TimedStop
+  std::string cur_tag_;
   std::vector<std::pair<std::string, float>> last_kernels;
   void BeginQueryProfile();
   void EndQueryProfile();
+  // Queues a kernel that spins on the SM clock for about `us` microseconds
+  // (a bounded cycle count; it touches no memory): profiled replays queue
+  // their launches behind it.
+  void DelayStream(double us);
   // the two events that time each query (made on first use)
   void QueryEvents(cudaEvent_t* start, cudaEvent_t* end);
   void TimedStart(const char* tag);
@@ -400,6 +410,7 @@ struct PreparedQuery {
   // instead of launching the graph when that measured faster at prepare
   // time (a short query pays the graph launch's fixed latency)
   std::vector<std::function<void(cudaStream_t)>> ops;
+  std::vector<std::string> tags;  // per op, as recorded
   bool direct = false;
   MatBuffer result;
   uint64_t catalog_version = 0;

@@ -552,6 +552,22 @@ __global__ void KdbTextGather(const char* __restrict__ raw, int64_t n, const int
 }
 }  // namespace
 
+namespace {
+__global__ void SpinDelay(long long cycles) {
+  const long long t0 = clock64();
+  while (clock64() - t0 < cycles) {
+  }
+}
+}  // namespace
+
+void Context::DelayStream(double us) {
+  if (dry || us <= 0) return;
+  // SM clock cycles at up to 2 GHz; at most 2 ms
+  const long long cycles = static_cast<long long>(std::min(us, 2000.0) * 2000.0);
+  SpinDelay<<<1, 1, 0, stream>>>(cycles);
+  KDB_CUDA(cudaGetLastError());
+}
+
 void Context::DecodeKdbText(const char* d_raw, int64_t n, int64_t* toff, char* tchars) {
   if (dry || n <= 0) return;
   TimedStart("text decode");

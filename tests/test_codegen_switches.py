@@ -18,7 +18,7 @@ SWITCHES = ["KDB_NO_SCAN_PREFETCH", "KDB_NO_VECTOR_SCAN", "KDB_VECTOR_PROBE_SCAN
             "KDB_AGG_MINB=4", "KDB_PROBE_VEC", "KDB_SORT_SHAPE=8192,8,1024,4", "KDB_SCAN_BATCH=4", "KDB_DENSE_SMEM=1", "KDB_BUILD_MAT_ATOMIC", "KDB_ORDER_MERGE",
             "KDB_SPLIT_PROBE_GROUPS", "KDB_KEY_CHECK_PASS", "KDB_JOIN_BUILD_PASS",
             "KDB_NO_PDL", "KDB_DENSE_SWITCH", "KDB_SMEM_BLOOM",
-            "KDB_ORDER_TIE_PASS", "KDB_ORDER_ROWS_PASS", "KDB_ORDER_FUSED_RANGE"]
+            "KDB_ORDER_TIE_PASS", "KDB_ORDER_ROWS_PASS", "KDB_ORDER_FUSED_RANGE", "KDB_PROFILE_FRESH"]
 
 
 @pytest.mark.parametrize("switch", SWITCHES)

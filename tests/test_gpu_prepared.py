@@ -95,3 +95,43 @@ def test_prepared_off_matches(engine):
     finally:
         engine.set_prepared_queries(True)
     assert compare(on, off) == ""
+
+
+@pytest.mark.parametrize("name", ["group_by", "join_group"])
+def test_profiled_replay_times_every_kernel(engine, name):
+    """Profiling a prepared query replays its recorded launches with an event
+    pair around each kernel: the same kernel roles as a profiled fresh run,
+    every time positive, and the query's result unchanged."""
+    if name == "group_by":
+        t = wl.group_by_table(300_000, seed=9, name="pq_prof_lineitem")
+        tables, plan = [t], wl.group_by_plan(t)
+    else:
+        b, p = wl.join_tables(60_000, 240_000, seed=10)
+        tables, plan = [b, p], wl.join_plan(b, p)
+    for t in tables:
+        try:  # an earlier test registered the join tables under these names
+            engine.drop_table(t.name)
+        except Exception:
+            pass
+        engine.register_table(t)
+    text = plan.to_json()
+    engine.set_profiling(True)
+    try:
+        fresh = engine.execute(text)  # profiling runs afresh when nothing is recorded
+        fresh_tags = {k["tag"] for k in engine.last_kernels()}
+    finally:
+        engine.set_profiling(False)
+    engine.execute(text)  # recorded
+    engine.execute(text)  # replayed
+    engine.set_profiling(True)
+    try:
+        replayed = engine.execute(text)
+        kernels = engine.last_kernels()
+    finally:
+        engine.set_profiling(False)
+    assert compare(replayed, fresh, ordered=True) == ""
+    tags = {k["tag"] for k in kernels}
+    assert "group by" in tags and tags <= fresh_tags
+    assert all(k["ms"] > 0 for k in kernels)
+    for t in tables:
+        engine.drop_table(t.name)
