@@ -7,7 +7,8 @@ available).  Metric: rows/s (whole job), with the roofline of the dominant
 kernel against the measured HBM copy bandwidth.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--workload group_by|scan_agg|join_group|batched|serving|skinner]
+                    [--workload group_by|scan_agg|join_group|join_group_zipf|batched|serving|skinner|op_hash_join]
+                    [--kernel-breakdown]   (skinner: device time per kernel role)
 
 A step is one execution of the query over the resident table.  The timed
 region covers exactly K steps on the engine's CUDA stream (events), bracketed
@@ -15,7 +16,8 @@ by a barrier and device synchronisation; multi-GPU runs are independent
 replicas (weak scaling, max time over ranks).  `--impl reference` times the
 CPU implementation of the path (the compiled restatement of the reference's
 generated loops and runtime tables, rows split over every host core) on the
-same workload.
+same workload, with the host caches evicted between its timed runs as the
+GPU's L2 is between GPU steps.
 """
 
 from __future__ import annotations
